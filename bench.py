@@ -1,0 +1,349 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 explicit Euler provider (one JSON line on rank 0).
+
+Workload: 2-D periodic isentropic vortex, 1024^2 cells on [0, 10]^2,
+TENO5 characteristic + Rusanov, SSPRK3, CFL 0.4 (the project's headline
+configuration).  A step is one full SSPRK3 time step (device CFL reduction +
+3 stages) over the whole grid.  Metric: Mcell-steps/s.
+
+  value     -- device throughput with the state resident in HBM, K steps in
+               one CUDA graph, timed with CUDA events on the launching stream;
+  e2e       -- the same steps through the public C ABI with host buffers:
+               every step uploads the state from pinned host memory,
+               advances one CFL step and downloads the state;
+  roofline  -- dominant sweep kernel: algorithmic HBM bytes per launch over
+               its CUDA-event duration vs the measured HBM copy bandwidth,
+               with the FP64/FP32 issue roof beside it (the binding one);
+  cpu_baseline -- the reference's own operator (oracle/_ref, compiled from
+               the sonicSolver sources) on the host cores.
+
+--impl reference times the reference CPU implementation alone.
+--gpus N runs N independent replicas (one per rank, weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# algorithmic HBM bytes per node per launch of each sweep (FP64 state, 5 vars)
+#   first axis of 2-D/3-D: read q_s, write R                         -> 80
+#   last axis (stage update): read q_s, R, q0, write q_out (+K RK4)   -> 160
+STATE_BYTES = 40
+# algorithmic FLOPs per face (reconstruction + flux), counted from the kernel
+# source: projection 12/pt, WENO5 core ~58 + 1 div, TENO5 core ~70 + 3 div,
+# back-projection 24, Rusanov ~60 + 2 div + 2 sqrt, eigen ~30 + rsqrt.
+FLOPS_PER_FACE = {"weno5": 6 * 12 + 10 * 59 + 24 + 64 + 34, "teno5": 6 * 12 + 10 * 73 + 24 + 64 + 34}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=1024)
+    ap.add_argument("--precision", default="fp32flux", choices=["fp32flux", "fp64"])
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--quick", action="store_true", help="skip e2e / peaks / baseline (profiling runs)")
+    return ap.parse_args()
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out = ""
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ CPU legs
+
+def _cpu_worker(args):
+    """One reference-operator step on a vortex slab (runs in a spawned process)."""
+    native, nx, ny, steps, recipe_scheme = args
+    sys.path[:0] = [ROOT, os.path.join(ROOT, "oracle")]
+    import numpy as np
+    import pyoracle as po
+    from sonicsolver_b200 import cases
+    L = 10.0
+    h = L / 1024
+    x = np.arange(nx) * h
+    y = np.arange(ny) * h + 3.0
+    X, Y = np.meshgrid(x, y, indexing="xy")
+    rho, u, v, p = cases.vortex_fields(X, Y, 0.0, L, 5.0, 1.4)
+    q = cases.conserved(rho, u, v, 0.0, p)[None]
+    spec = po.GridSpec(dim=2, n=(nx, ny, 1), ng=3, h=(h, h, 1.0), bc_lo=(1, 1, 0), bc_hi=(1, 1, 0))
+    Q = spec.empty()
+    spec.interior(Q)[...] = q
+    po.fill_ghosts(spec, Q)
+    if native is None:
+        t0 = time.perf_counter()
+        st = po.Stepper(spec, recipe_scheme, po.RUSANOV, po.SSPRK3)
+        for _ in range(steps):
+            st.step(Q, po.dt(spec, Q, 0.4))
+        return time.perf_counter() - t0
+    rc = po.RefCase(spec, recipe_scheme, po.RUSANOV, native=True)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        rc.step(po.SSPRK3, Q, rc.dt(Q, 0.4))
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(procs=None, nx=1024, ny=128, steps=2):
+    """The reference's own operator (oracle/_ref native build) stepping
+    independent vortex slabs, one process per core (the reference is
+    single-threaded per MPI rank); falls back to the oracle port."""
+    import multiprocessing as mp
+    sys.path[:0] = [os.path.join(ROOT, "oracle")]
+    import pyoracle as po
+    native = True if po.ref_lib(native=True) is not None else None
+    kind = "reference" if native else "port"
+    procs = procs or max(1, min(os.cpu_count() or 1, 32))
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(procs) as pool:
+        walls = pool.map(_cpu_worker, [(native, nx, ny, steps, po.TENO5)] * procs)
+    wall = max(walls)
+    total = time.perf_counter() - t0
+    cells = nx * ny * steps * procs
+    return {"value": cells / wall / 1e6, "unit": "Mcell-steps/s", "cores": procs, "kind": kind,
+            "sample": f"{procs} processes x {steps} SSPRK3 step(s) of a {nx}x{ny} periodic vortex slab "
+                      f"(dx = 10/1024), TENO5+Rusanov, reference operator compiled -O3 -march=x86-64-v3",
+            "per_core": cells / wall / 1e6 / procs, "wall_s": round(total, 2)}
+
+
+# ------------------------------------------------------------------ GPU legs
+
+def run_ours(args, rank, world):
+    import numpy as np
+    import torch
+    from sonicsolver_b200 import capi, cases
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream()
+    prec = capi.PREC_FP32_FLUX if args.precision == "fp32flux" else capi.PREC_FP64
+    case = cases.isentropic_vortex(args.size)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        s = case.solver(precision=prec, stream=ctypes_stream(stream))
+    K, W = args.steps, args.warmup
+    # warm-up (untimed): builds and caches the K-step graph shape too
+    s.advance(1e30, max_steps=W, graph_steps=K)
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(dev) as clk:
+        st, _ = s.advance(1e30, max_steps=K, graph_steps=K)
+        torch.cuda.synchronize()
+    barrier(world)
+    ms = st.device_ms
+    ms_max = allreduce_max(ms, world)
+    cells = case.cells
+    value = cells * K * world / (ms_max * 1e-3) / 1e6
+
+    out = {"metric": "Mcell-steps/s", "value": round(value, 2), "unit": "Mcell-steps/s", "n_gpus": world,
+           "steps": K, "warmup": W, "ms_per_step": round(ms_max / K, 4), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None,
+           "dtype": "fp32 flux / fp64 state" if prec else "fp64",
+           "data": "synthetic (analytic isentropic vortex initial condition)",
+           "config": {"workload": "isentropic_vortex_2d", "cells": f"{args.size}x{args.size}", "domain": "[0,10]^2",
+                      "recipe": "teno5Rusanov", "time": "SSPRK3", "cfl": 0.4, "precision": args.precision,
+                      "parallelism": f"replicas x{world}", "graph_steps": K,
+                      "l2": "inputs larger than L2 (4 x 42 MB state arrays touched per stage)"},
+           "clocks": clk.summary(), "gpu_launches": None}
+    dim = case.dim
+    launches_per_step = 2 + 3 * dim + 1  # dt, finalize, sweeps, commit
+    out["gpu_launches"] = launches_per_step * (K + 0)
+    if args.quick or rank != 0:
+        s.close()
+        return out
+
+    # ---- the other precision, same workload (plain FP64 vs mixed)
+    other = capi.PREC_FP64 if prec else capi.PREC_FP32_FLUX
+    with torch.cuda.stream(stream):
+        s2 = case.solver(precision=other, stream=ctypes_stream(stream))
+    s2.advance(1e30, max_steps=W, graph_steps=K)
+    torch.cuda.synchronize()
+    st2, _ = s2.advance(1e30, max_steps=K, graph_steps=K)
+    out["fp64_value" if prec else "fp32flux_value"] = round(cells * K / (st2.device_ms * 1e-3) / 1e6, 2)
+
+    # ---- roofline of the dominant sweep
+    dt = s.compute_dt()
+    ms_axes = s.time_sweeps(dt, stage=0, repeats=5)
+    nodes = case.nodes
+    hbm, src = measured_peaks()
+    kinds = ["first", "last"] if dim == 2 else ["final"]
+    dom = int(np.argmax(ms_axes))
+    bytes_node = 2 * STATE_BYTES if (dim > 1 and dom == 0) else 4 * STATE_BYTES
+    achieved = bytes_node * nodes / (ms_axes[dom] * 1e-3) / 1e9
+    fp_peak = capi.fma_peak_tflops(fp64=(prec == capi.PREC_FP64), seconds=0.5)
+    faces = nodes  # one face per node per axis
+    fl = FLOPS_PER_FACE["teno5"] * faces / (ms_axes[dom] * 1e-3) / 1e12
+    out["roofline"] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                       "frac": round(achieved / hbm, 4), "traffic": None, "peak_source": f"{src} (MEASURED_PEAKS.json)",
+                       "kernel": f"sweep axis {dom} ({'x' if dom == 0 else 'y'})", "ms_per_launch": round(ms_axes[dom], 4),
+                       "ms_per_axis": [round(x, 4) for x in ms_axes],
+                       "algorithmic_bytes_per_launch": bytes_node * nodes,
+                       "issue_roof": {"unit": "TFLOP/s", "achieved": round(fl, 2), "fma_peak": round(fp_peak, 2),
+                                      "frac": round(fl / fp_peak, 4) if fp_peak else None,
+                                      "arith": "fp32" if prec else "fp64",
+                                      "flops_per_face": FLOPS_PER_FACE["teno5"],
+                                      "note": "binding roof: arithmetic issue, not HBM"}}
+
+    # ---- e2e through the C ABI with pinned host buffers, every step
+    E = args.e2e_steps
+    host = torch.empty(case.q.size, dtype=torch.float64, pin_memory=True).numpy()
+    host[:] = case.q.ravel()
+    t_sim = 0.0
+    with torch.cuda.stream(stream):
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.upload(host, t_sim)
+        s.step()
+        s.download(out=host)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(E):
+            s.upload(host, t_sim)      # H2D of the step's input state
+            s.step()                   # CFL step (device dt + 3 stages)
+            s.download(out=host)       # D2H of the step's result state
+        ev1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = ev0.elapsed_time(ev1)
+    out["e2e"] = {"value": round(cells * E / (e2e_ms * 1e-3) / 1e6, 2), "unit": "Mcell-steps/s",
+                  "h2d_bytes_per_step": int(host.nbytes), "d2h_bytes_per_step": int(host.nbytes),
+                  "steps": E, "path": "sfg_upload(pinned) + sfg_step + sfg_download per step"}
+    out["gpu_launches"] += E * (launches_per_step + 2)
+    s.close()
+    s2.close()
+    return out
+
+
+def ctypes_stream(stream):
+    import ctypes
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allreduce_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        t0 = time.time()
+        res = []
+        for _ in range(args.warmup):
+            cpu_baseline(steps=1)
+        for _ in range(max(1, min(args.steps, 3))):
+            res.append(cpu_baseline(steps=1))
+        best = max(res, key=lambda r: r["value"])
+        line = {"impl": "reference", "metric": "Mcell-steps/s", "value": round(best["value"], 4),
+                "unit": "Mcell-steps/s", "n_gpus": args.gpus, "steps": len(res), "warmup": args.warmup,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64",
+                "data": "synthetic (analytic isentropic vortex initial condition)",
+                "config": {"workload": "isentropic_vortex_2d", "cells": "1024x1024 (sampled as slabs)",
+                           "recipe": "teno5Rusanov", "time": "SSPRK3", "cfl": 0.4},
+                "cpu_baseline": {k: best[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "e2e": {"value": round(best["value"], 4), "unit": "Mcell-steps/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}, "wall_s": round(time.time() - t0, 1)}
+        print(json.dumps(line), flush=True)
+        return
+    base = None
+    if rank == 0 and not args.quick and not args.no_cpu_baseline:
+        base = cpu_baseline(steps=1)  # spawned before any GPU call
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    out = run_ours(args, rank, world)
+    if rank == 0:
+        if base is not None:
+            out["cpu_baseline"] = {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,202 @@
+/*
+ * sonicsolver_b200.h -- C ABI of the B200 (sm_100a) explicit Euler provider.
+ *
+ * One opaque solver handle per structured grid (or one batch / server handle
+ * for many grids) carries device-resident conserved state and runs the
+ * density-based explicit path of sonicSolver on one GPU:
+ *   characteristic WENO/TENO reconstruction -> Rusanov/Roe face flux ->
+ *   conservative divergence -> ghost/periodic fill -> forwardEuler / SSPRK3 /
+ *   classicalRK4 stage combination, with the CFL time step reduced on device.
+ *
+ * Every entry point returns an int status (SFG_OK = 0) and never exits or
+ * throws across the ABI; sfg_last_error() gives the message of the last
+ * failure on the calling thread.  Plain pointers and sizes only.
+ *
+ * Reference interfaces replaced (paths inside the sonicSolver source tree):
+ *   - divDispatch(Field&, FluxField&, Residual&, ConvectionScheme, FluxSplitter,
+ *     double, IBMBoundaryScheme, int, double, const Model&)
+ *       src/solver/discretization/convection/SF_div.h:212-243
+ *   - Time::Explicit::begin / executeStage / forwardEuler
+ *       src/solver/algorithm/time/SF_explicit.h:47-69,
+ *       src/solver/algorithm/time/SF_explicit.cpp:282-530
+ *   - RusanovEOS::deltaT(const Field&, const Model&, double)
+ *       src/methods/numerics/Flux/SF_rusanovEOS.h:36-38
+ *   - Runtime::globalMinimum (MPI_Allreduce MIN of dt)
+ *       src/infrastructure/execution/SF_executionRuntime.cpp:126
+ *   - Boundary::Applicator::apply(Field&) for zeroGradient ends and the
+ *     (declared, unimplemented) periodic interface
+ *       src/solver/boundary/SF_applicator.h:51-83
+ *   - the flow.conservative op bindings FlowStepPrepare / FlowDtCompute /
+ *     FlowStepBegin / ExplicitStageExecute / FlowStepCommit
+ *       src/solver/algorithm/SF_flowOperations.cpp:466-522
+ */
+#ifndef SONICSOLVER_B200_H
+#define SONICSOLVER_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes --------------------------------------------------- */
+enum {
+    SFG_OK = 0,
+    SFG_ERR_ARG = 1,          /* invalid argument / unsupported combination   */
+    SFG_ERR_CUDA = 2,         /* CUDA runtime failure (message has the text)  */
+    SFG_ERR_STATE = 3,        /* rho <= 0, p <= 0 or non-finite state / flux  */
+    SFG_ERR_TENO_CUTOFF = 4,  /* TENO5 rejected all three sub-stencils        */
+    SFG_ERR_NOMEM = 5,        /* device allocation failed                     */
+    SFG_ERR_BUDGET = 6,       /* HBM budget of a batch / server exceeded      */
+    SFG_ERR_TIMEOUT = 7,      /* a bounded wait gave up                       */
+    SFG_ERR_NOT_FOUND = 8,    /* unknown slot / request id                    */
+    SFG_ERR_CANCELLED = 9     /* request was cancelled                        */
+};
+
+/* Device status-word bits (sfg_status_word). */
+enum {
+    SFG_FLAG_NONFINITE = 1u << 0,
+    SFG_FLAG_DENSITY = 1u << 1,
+    SFG_FLAG_PRESSURE = 1u << 2,
+    SFG_FLAG_TENO_CUTOFF = 1u << 3,
+    SFG_FLAG_ROE_SOUND = 1u << 4
+};
+
+/* ---- recipe identifiers --------------------------------------------- */
+/* Convection recipes: the values of FDM::TermRecipeId
+ * (src/core/config/types/SF_termRecipe.h:52-64). */
+enum {
+    SFG_RECIPE_WENO3_RUSANOV = 1,
+    SFG_RECIPE_WENO3_ROE = 3,
+    SFG_RECIPE_WENO5_RUSANOV = 6,
+    SFG_RECIPE_WENO5_ROE = 8,
+    SFG_RECIPE_TENO5_RUSANOV = 11,
+    SFG_RECIPE_TENO5_ROE = 13,
+    SFG_RECIPE_WENO7_RUSANOV = 16,
+    SFG_RECIPE_WENO7_ROE = 18
+};
+/* Time recipes: the values of FDM::TimeRecipeId (SF_timeRecipe.h:11). */
+enum { SFG_TIME_FORWARD_EULER = 0, SFG_TIME_SSPRK3 = 1, SFG_TIME_CLASSICAL_RK4 = 2 };
+/* Arithmetic of the reconstruction and face flux.  The conserved state, the
+ * stage accumulation, the conserved totals and the dt reduction are FP64 in
+ * both modes. */
+enum { SFG_PREC_FP64 = 0, SFG_PREC_FP32_FLUX = 1 };
+/* Boundary laws per axis end. */
+enum {
+    SFG_BC_TRANSMISSIVE = 0,  /* zeroGradient: boundary node copies its inner
+                                 neighbour and is not advanced; ghosts copy it
+                                 (reconstruction/linear/SF_zeroGradient.cpp:88-105) */
+    SFG_BC_PERIODIC = 1       /* ghosts wrap; every node is advanced (the
+                                 reference declares PatchBoundaryKind::Periodic,
+                                 SF_meshInterface.h:14, but never implements it) */
+};
+/* Host array layouts for upload / download. */
+enum {
+    SFG_LAYOUT_NODES = 0,     /* AoS [k][j][i][v] over the nodes only          */
+    SFG_LAYOUT_FIELD = 1      /* reference Field storage: AoS [k][j][i][v] with
+                                 ng ghost layers on every axis
+                                 (src/core/field/SF_field.h:58-67)            */
+};
+
+/* ---- descriptors ---------------------------------------------------- */
+typedef struct {
+    int dim;          /* active axes: the first `dim` of (x, y, z), 1..3      */
+    int n[3];         /* nodes per axis (1 on inactive axes)                 */
+    double h[3];      /* node spacing; inactive axes: slab thickness          */
+    int bc_lo[3];     /* SFG_BC_* per axis, low end                           */
+    int bc_hi[3];     /* SFG_BC_* per axis, high end                          */
+} sfg_grid_desc;
+
+typedef struct {
+    int recipe;       /* SFG_RECIPE_*                                        */
+    int time_recipe;  /* SFG_TIME_*                                          */
+    int precision;    /* SFG_PREC_*                                          */
+    double gamma;     /* perfect-gas ratio of specific heats                 */
+    double cfl;       /* CFL number of RusanovEOS::deltaT                     */
+    double max_dt;    /* numerics maxDeltaT (<= 0: unlimited)                 */
+} sfg_numerics_desc;
+
+typedef struct {
+    int64_t steps;            /* steps taken                                 */
+    double time;              /* physical time reached                       */
+    double last_dt;           /* last step size                              */
+    double device_ms;         /* device time of the advance (CUDA events)     */
+    uint32_t status_bits;     /* SFG_FLAG_* seen                             */
+    uint64_t teno_cut;        /* TENO5 sub-stencils cut (when counted)        */
+    uint64_t teno_cores;      /* TENO5 cores evaluated (when counted)         */
+} sfg_stats;
+
+typedef struct sfg_solver_s* sfg_solver;
+
+/* ---- errors and version --------------------------------------------- */
+const char* sfg_last_error(void);
+int sfg_version(int* major, int* minor);
+/* Recipe name as the case.yaml token (e.g. "weno5Rusanov"); NULL if unknown.
+ * Names of FDM::toString(TermRecipeId), SF_termRecipe.h:242-259. */
+const char* sfg_recipe_name(int recipe);
+/* Recipe id from its case.yaml token; SFG_ERR_ARG if not provided here. */
+int sfg_recipe_from_name(const char* name, int* recipe);
+
+/* ---- single grid ------------------------------------------------------ */
+/* Binds the provider to the current CUDA device and allocates the state.
+ * `stream` is a cudaStream_t (NULL: the solver creates its own). */
+int sfg_create(const sfg_grid_desc* grid, const sfg_numerics_desc* numerics,
+               void* stream, sfg_solver* out);
+int sfg_destroy(sfg_solver s);
+/* Ghost layers of the reference Field layout (3 for WENO5/TENO5). */
+int sfg_ghost_layers(sfg_solver s, int* ng);
+/* Number of doubles of a host array in `layout`. */
+int sfg_state_size(sfg_solver s, int layout, size_t* count);
+/* Host <-> device copies of the conserved state (pageable or pinned host
+ * memory; synchronous with respect to the solver's stream). Upload resets the
+ * time to `time`. */
+int sfg_upload(sfg_solver s, const double* host, int layout, double time);
+int sfg_download(sfg_solver s, double* host, int layout);
+/* The same from / to device memory (AoS node layout, no ghosts). */
+int sfg_upload_device(sfg_solver s, const double* dev_nodes_aos, double time);
+int sfg_download_device(sfg_solver s, double* dev_nodes_aos);
+
+/* FlowDtCompute: CFL step of the current state, min'ed with max_dt and
+ * `limit` (<= 0: no limit).  Reduced on device; copied to *dt. */
+int sfg_compute_dt(sfg_solver s, double limit, double* dt);
+/* FlowStepBegin + ExplicitStageExecute(stage) + (after the last stage)
+ * FlowStepCommit, at the given dt.  stage 0 snapshots q0. */
+int sfg_stage(sfg_solver s, int stage, double dt);
+/* All stages of one step of size dt (dt <= 0: the CFL step, clipped to
+ * `limit` when limit > 0). Advances the solver time. */
+int sfg_step(sfg_solver s, double dt, double limit);
+/* Time::Driver loop: steps until t_end (or max_steps), clipping dt at
+ * t_end and at every multiple of write_interval (<= 0: none).  Runs without
+ * host synchronisation inside a CUDA graph of `graph_steps` steps
+ * (<= 0: default).  dt_out (may be NULL) receives up to dt_capacity dts. */
+int sfg_advance(sfg_solver s, double t_end, int64_t max_steps, double write_interval,
+                int graph_steps, double* dt_out, int64_t dt_capacity, sfg_stats* stats);
+/* Spatial residual R = Jac * sum_d dF_d of the current state (node layout,
+ * AoS; unsolved boundary nodes are 0) -- operator-level parity. */
+int sfg_residual(sfg_solver s, double* host_nodes_aos);
+/* Stage combination alone with a caller-supplied residual (node layout AoS):
+ * stage arithmetic parity.  Updates the state as sfg_stage would. */
+int sfg_stage_with_residual(sfg_solver s, int stage, double dt, const double* host_residual);
+/* Conserved totals sum_nodes Q_v * cell volume (FP64), v = 0..4. */
+int sfg_conserved_totals(sfg_solver s, double totals[5]);
+int sfg_time(sfg_solver s, double* time, int64_t* steps);
+/* Device status word (SFG_FLAG_* bits) accumulated since the last clear. */
+int sfg_status_word(sfg_solver s, uint32_t* bits, int clear);
+/* TENO5 cut-off accounting (enable = 1 adds counters to the kernels). */
+int sfg_set_counting(sfg_solver s, int enable);
+int sfg_get_counters(sfg_solver s, uint64_t* teno_cores, uint64_t* teno_cut);
+
+/* ---- diagnostics (no counterpart in the reference: measurement aids) -- */
+/* Runs stage `stage` of a step of size dt `repeats` times on the current
+ * state without committing it, timing each axis sweep with CUDA events on the
+ * solver's stream; ms_per_axis[d] receives the mean duration of sweep d. */
+int sfg_time_sweeps(sfg_solver s, int stage, double dt, int repeats, float* ms_per_axis);
+/* Dependent-FMA throughput of this GPU in TFLOP/s (fp64 = 1: double,
+ * 0: float), measured with a kernel of `seconds` length. */
+int sfg_measure_fma_peak(int fp64, double seconds, double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

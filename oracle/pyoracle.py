@@ -1,0 +1,282 @@
+"""ctypes bindings of the CPU checker libraries (test infrastructure only).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline legs import
+this module.  It wraps
+
+  * oracle/liboracle.so      -- the plain-C restatement (sf_oracle.c);
+  * oracle/_ref/libsfref.so  -- the reference translation units driven by
+                                ref_driver.cpp (present when the reference
+                                sources were available at build time).
+
+Arrays use the oracle's compact node layout: AoS ``[k][j][i][v]`` with ``ng``
+ghost layers on active axes only (see sf_oracle.h).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+WENO3, WENO5, TENO5, WENO7 = 0, 1, 2, 3
+STEGER, RUSANOV, LAXFRIEDRICHS, ROE, LAXWENDROFF = 0, 1, 2, 3, 4
+EULER, SSPRK3, RK4 = 0, 1, 2
+BC_TRANSMISSIVE, BC_PERIODIC, BC_FROZEN = 0, 1, 2
+ERRORS = {0: "ok", 1: "non-finite", 2: "invalid state", 3: "TENO all-cutoff", 4: "argument",
+          5: "Roe sound speed"}
+
+
+class Grid(ctypes.Structure):
+    _fields_ = [("dim", ctypes.c_int), ("n", ctypes.c_int * 3), ("ng", ctypes.c_int),
+                ("h", ctypes.c_double * 3), ("bc_lo", ctypes.c_int * 3),
+                ("bc_hi", ctypes.c_int * 3), ("gamma", ctypes.c_double)]
+
+
+class Counters(ctypes.Structure):
+    _fields_ = [("teno_cores", ctypes.c_ulonglong), ("teno_cut", ctypes.c_ulonglong),
+                ("faces", ctypes.c_ulonglong)]
+
+
+@dataclass
+class GridSpec:
+    """Python view of ``sfo_grid``."""
+    dim: int
+    n: tuple
+    ng: int = 3
+    h: tuple = (1.0, 1.0, 1.0)
+    bc_lo: tuple = (0, 0, 0)
+    bc_hi: tuple = (0, 0, 0)
+    gamma: float = 1.4
+
+    def c(self) -> Grid:
+        g = Grid()
+        g.dim = self.dim
+        for d in range(3):
+            g.n[d] = int(self.n[d])
+            g.h[d] = float(self.h[d])
+            g.bc_lo[d] = int(self.bc_lo[d])
+            g.bc_hi[d] = int(self.bc_hi[d])
+        g.ng = self.ng
+        g.gamma = self.gamma
+        return g
+
+    @property
+    def extents(self):
+        return tuple(self.n[d] + (2 * self.ng if d < self.dim else 0) for d in range(3))
+
+    def empty(self) -> np.ndarray:
+        mx, my, mz = self.extents
+        return np.zeros((mz, my, mx, 5), dtype=np.float64)
+
+    def interior(self, Q: np.ndarray) -> np.ndarray:
+        """View of the node block (no ghosts) of a compact array."""
+        sl = []
+        for d in (2, 1, 0):
+            lo = self.ng if d < self.dim else 0
+            sl.append(slice(lo, lo + self.n[d]))
+        return Q[tuple(sl)]
+
+
+_DP = ctypes.POINTER(ctypes.c_double)
+
+
+def _ptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_DP)
+
+
+def _load(path):
+    if not os.path.exists(path):
+        return None
+    return ctypes.CDLL(path)
+
+
+def _sig(lib, prefix):
+    G = ctypes.POINTER(Grid)
+    C = ctypes.POINTER(Counters)
+    if prefix == "sfo":
+        lib.sfo_storage_size.argtypes = [G]
+        lib.sfo_storage_size.restype = ctypes.c_longlong
+        for nm in ("sfo_weno3_core", "sfo_weno5_core", "sfo_weno7_core"):
+            getattr(lib, nm).argtypes = [_DP]
+            getattr(lib, nm).restype = ctypes.c_double
+        lib.sfo_teno5_core.argtypes = [_DP, ctypes.POINTER(ctypes.c_int)]
+        lib.sfo_teno5_core.restype = ctypes.c_double
+        lib.sfo_char_matrix.argtypes = [_DP, _DP, ctypes.c_double, _DP, _DP]
+        lib.sfo_rusanov_flux.argtypes = [_DP, _DP, _DP, ctypes.c_double, _DP]
+        lib.sfo_roe_flux.argtypes = [_DP, _DP, _DP, ctypes.c_double, _DP]
+        lib.sfo_char_face_flux.argtypes = [ctypes.c_int, _DP, _DP, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_double, _DP]
+        lib.sfo_fill_ghosts.argtypes = [G, _DP]
+        lib.sfo_rhs.argtypes = [G, ctypes.c_int, ctypes.c_int, _DP, _DP, C]
+        lib.sfo_dt.argtypes = [G, _DP, ctypes.c_double, _DP]
+        lib.sfo_step.argtypes = [G, ctypes.c_int, ctypes.c_int, ctypes.c_int, _DP, ctypes.c_double,
+                                 _DP, C]
+        lib.sfo_stage.argtypes = [G, ctypes.c_int, ctypes.c_int, ctypes.c_int, _DP, ctypes.c_double,
+                                  ctypes.c_int, _DP, C]
+        lib.sfo_advance.argtypes = [G, ctypes.c_int, ctypes.c_int, ctypes.c_int, _DP,
+                                    ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_double, ctypes.c_double, ctypes.c_int, _DP,
+                                    ctypes.POINTER(ctypes.c_int), _DP, C]
+    else:
+        lib.sfr_rhs.argtypes = [G, ctypes.c_int, ctypes.c_int, _DP, _DP]
+        lib.sfr_dt.argtypes = [G, _DP, ctypes.c_double, _DP]
+        for nm in ("sfr_weno3_core", "sfr_weno5_core", "sfr_teno5_core", "sfr_weno7_core"):
+            getattr(lib, nm).argtypes = [_DP]
+            getattr(lib, nm).restype = ctypes.c_double
+        lib.sfr_char_matrix.argtypes = [_DP, _DP, ctypes.c_double, _DP, _DP]
+        lib.sfr_rusanov_flux.argtypes = [_DP, _DP, _DP, ctypes.c_double, _DP]
+        lib.sfr_roe_flux.argtypes = [_DP, _DP, _DP, ctypes.c_double, _DP]
+        lib.sfr_case_create.argtypes = [G, ctypes.c_int, ctypes.c_int]
+        lib.sfr_case_create.restype = ctypes.c_void_p
+        lib.sfr_case_destroy.argtypes = [ctypes.c_void_p]
+        lib.sfr_case_rhs.argtypes = [ctypes.c_void_p, _DP, _DP]
+        lib.sfr_case_dt.argtypes = [ctypes.c_void_p, _DP, ctypes.c_double, _DP]
+        lib.sfr_case_step.argtypes = [ctypes.c_void_p, ctypes.c_int, _DP, ctypes.c_double]
+        lib.sfr_case_advance.argtypes = [ctypes.c_void_p, ctypes.c_int, _DP, ctypes.c_double,
+                                         ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                         ctypes.c_double, ctypes.c_int, _DP,
+                                         ctypes.POINTER(ctypes.c_int), _DP]
+    return lib
+
+
+_oracle = None
+_ref = {}
+
+
+def oracle_lib():
+    """The C restatement (built by ``make -C oracle``)."""
+    global _oracle
+    if _oracle is None:
+        lib = _load(os.path.join(HERE, "liboracle.so"))
+        if lib is None:
+            raise RuntimeError("oracle/liboracle.so missing: run `make -C oracle`")
+        _oracle = _sig(lib, "sfo")
+    return _oracle
+
+
+def ref_lib(native: bool = False):
+    """The reference translation units, or None when they were not built."""
+    key = "native" if native else "strict"
+    if key not in _ref:
+        lib = _load(os.path.join(HERE, "_ref", "libsfref_native.so" if native else "libsfref.so"))
+        _ref[key] = _sig(lib, "sfr") if lib is not None else None
+    return _ref[key]
+
+
+def _check(code, what):
+    if code != 0:
+        raise RuntimeError(f"{what}: {ERRORS.get(code, code)}")
+
+
+class OracleError(RuntimeError):
+    pass
+
+
+# ---------------------------------------------------------------- restatement
+
+def fill_ghosts(spec: GridSpec, Q: np.ndarray) -> None:
+    _check(oracle_lib().sfo_fill_ghosts(ctypes.byref(spec.c()), _ptr(Q)), "fill_ghosts")
+
+
+def rhs(spec: GridSpec, scheme: int, flux: int, Q: np.ndarray, counters: Counters | None = None):
+    R = np.zeros_like(Q)
+    code = oracle_lib().sfo_rhs(ctypes.byref(spec.c()), scheme, flux, _ptr(Q), _ptr(R),
+                                ctypes.byref(counters) if counters is not None else None)
+    _check(code, "rhs")
+    return R
+
+
+def dt(spec: GridSpec, Q: np.ndarray, cfl: float) -> float:
+    out = ctypes.c_double()
+    _check(oracle_lib().sfo_dt(ctypes.byref(spec.c()), _ptr(Q), cfl, ctypes.byref(out)), "dt")
+    return out.value
+
+
+class Stepper:
+    """Holds the q0 / k work arrays between stages of one step."""
+
+    def __init__(self, spec: GridSpec, scheme: int, flux: int, time_id: int):
+        self.spec, self.scheme, self.flux, self.time_id = spec, scheme, flux, time_id
+        self.g = spec.c()
+        self.work = np.zeros(5 * int(oracle_lib().sfo_storage_size(ctypes.byref(self.g))))
+        self.counters = Counters()
+
+    def stage(self, Q, dt_, s):
+        code = oracle_lib().sfo_stage(ctypes.byref(self.g), self.scheme, self.flux, self.time_id,
+                                      _ptr(Q), dt_, s, _ptr(self.work), ctypes.byref(self.counters))
+        if code:
+            raise OracleError(f"stage {s}: {ERRORS.get(code, code)}")
+
+    def step(self, Q, dt_):
+        code = oracle_lib().sfo_step(ctypes.byref(self.g), self.scheme, self.flux, self.time_id,
+                                     _ptr(Q), dt_, _ptr(self.work), ctypes.byref(self.counters))
+        if code:
+            raise OracleError(f"step: {ERRORS.get(code, code)}")
+
+
+def advance(spec: GridSpec, scheme, flux, time_id, Q, t_end, cfl, *, t_start=0.0,
+            max_dt=1.7976931348623157e308, write_interval=0.0, max_steps=10 ** 7,
+            counters: Counters | None = None):
+    """Runs the Time::Driver loop; returns (dt array, t_final)."""
+    cap = min(max_steps, 10 ** 7)
+    dts = np.zeros(cap)
+    steps = ctypes.c_int()
+    tf = ctypes.c_double()
+    code = oracle_lib().sfo_advance(ctypes.byref(spec.c()), scheme, flux, time_id, _ptr(Q),
+                                    t_start, t_end, cfl, max_dt, write_interval, cap, _ptr(dts),
+                                    ctypes.byref(steps), ctypes.byref(tf),
+                                    ctypes.byref(counters) if counters is not None else None)
+    if code:
+        raise OracleError(f"advance: {ERRORS.get(code, code)} after {steps.value} steps")
+    return dts[:steps.value].copy(), tf.value
+
+
+# ---------------------------------------------------------------- reference TUs
+
+class RefCase:
+    """A persistent reference Field driven through the reference operator."""
+
+    def __init__(self, spec: GridSpec, scheme: int, flux: int, native: bool = False):
+        lib = ref_lib(native)
+        if lib is None:
+            raise RuntimeError("oracle/_ref not built (reference sources unavailable)")
+        self.lib = lib
+        self.spec = spec
+        self.g = spec.c()
+        self.h = lib.sfr_case_create(ctypes.byref(self.g), scheme, flux)
+        if not self.h:
+            raise RuntimeError("sfr_case_create failed")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.sfr_case_destroy(self.h)
+            self.h = None
+
+    def rhs(self, Q):
+        R = np.zeros_like(Q)
+        _check(self.lib.sfr_case_rhs(self.h, _ptr(Q), _ptr(R)), "ref rhs")
+        return R
+
+    def dt(self, Q, cfl):
+        out = ctypes.c_double()
+        _check(self.lib.sfr_case_dt(self.h, _ptr(Q), cfl, ctypes.byref(out)), "ref dt")
+        return out.value
+
+    def step(self, time_id, Q, dt_):
+        _check(self.lib.sfr_case_step(self.h, time_id, _ptr(Q), dt_), "ref step")
+
+    def advance(self, time_id, Q, t_end, cfl, *, t_start=0.0, max_dt=1.7976931348623157e308,
+                write_interval=0.0, max_steps=10 ** 7):
+        cap = min(max_steps, 10 ** 7)
+        dts = np.zeros(cap)
+        steps = ctypes.c_int()
+        tf = ctypes.c_double()
+        code = self.lib.sfr_case_advance(self.h, time_id, _ptr(Q), t_start, t_end, cfl, max_dt,
+                                         write_interval, cap, _ptr(dts), ctypes.byref(steps),
+                                         ctypes.byref(tf))
+        _check(code, "ref advance")
+        return dts[:steps.value].copy(), tf.value

@@ -1,0 +1,314 @@
+// ref_driver.cpp -- drives the reference's own hot-path translation units.
+//
+// TEST INFRASTRUCTURE ONLY.  Built by oracle/Makefile against the sonicSolver
+// sources where they lie (never copied into this repository) into
+// oracle/_ref/libsfref.so.  It exposes the same flat C entry points as
+// sf_oracle.h with the prefix sfr_, so the tests can pin the C restatement
+// against the reference implementation on identical inputs.
+//
+// What runs reference code:
+//   - the spatial operator: SF::divDispatch (solver/discretization/convection/
+//     SF_div.h:212-243) with its WENO/TENO cores, characteristic matrices,
+//     Rusanov/Roe fluxes, face loops and residual assembly, then
+//     Math::spatialResidual (methods/numerics/structured/SF_residualAssembly.h:34-41);
+//   - the CFL step: Numerics::RusanovEOS::deltaT (Flux/SF_rusanovEOS.cpp:110-147).
+// What is restated here (the reference's versions need the full solver
+// runtime): the ghost fill laws and the Euler / Shu-Osher SSPRK3 / RK4 stage
+// arithmetic of solver/algorithm/time/SF_explicit.cpp:193-238,282-285.
+#include "SF_field.h"
+#include "SF_div.h"
+#include "core/flux/SF_flux.h"
+#include "core/residual/SF_residual.h"
+#include "core/mesh/SF_dimension.h"
+#include "methods/numerics/Flux/SF_rusanovEOS.h"
+#include "methods/numerics/structured/SF_residualAssembly.h"
+#include "models/physics/fluidStateModel/SF_singleFluidStateModel.h"
+#include "models/physics/EOS/SF_perfectGasEOS.h"
+
+#include "sf_oracle.h"
+
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace {
+
+// makeSingleFluidPerfectGas (fluidStateModel/SF_factory.h:21-33) without the
+// multiphase headers that factory pulls in: inviscid (mu = 0), Pr = 0.72.
+std::shared_ptr<const SF::Physics::FluidStateModel::SingleFluidStateModel> perfect_gas(double gamma) {
+    const double gasConstant = 287.05, mu = 0.0, prandtl = 0.72;
+    const double cp = gamma * gasConstant / (gamma - 1.0);
+    return std::make_shared<const SF::Physics::FluidStateModel::SingleFluidStateModel>(
+        std::make_shared<SF::Physics::EOS::PerfectGasEOS>(gamma, gasConstant), mu, mu * cp / prandtl);
+}
+
+struct RefCase {
+    sfo_grid g;
+    SF::Field field;
+    SF::FluxField flux;
+    SF::Residual residual;
+    std::shared_ptr<const SF::Physics::FluidStateModel::SingleFluidStateModel> model;
+};
+
+int storage_extent(const sfo_grid* g, int d) { return g->n[d] + (d < g->dim ? 2 * g->ng : 0); }
+
+// Build a reference Field (ghosts on every axis) with uniform Cartesian metrics.
+void setup_case(RefCase& rc, const sfo_grid* g) {
+    rc.g = *g;
+    SF::Math::resetActiveDirections();
+    for (int d = g->dim; d < 3; ++d) SF::Math::deactivateDirection(d);
+    rc.field.setup(g->n[0], g->n[1], g->n[2], g->ng, 5);
+    rc.model = perfect_gas(g->gamma);
+    rc.field.setStateModel(rc.model);
+    const double hx = g->h[0], hy = g->h[1], hz = g->h[2];
+    const double J = hx * hy * hz;
+    const double jac = 1.0 / J;
+    for (int k = 0; k < rc.field.MZ(); ++k)
+        for (int j = 0; j < rc.field.MY(); ++j)
+            for (int i = 0; i < rc.field.MX(); ++i) {
+                rc.field.Jac(i, j, k) = jac;
+                rc.field.XiX(i, j, k) = (hy * hz) * jac;
+                rc.field.XiY(i, j, k) = 0.0;
+                rc.field.XiZ(i, j, k) = 0.0;
+                rc.field.EtX(i, j, k) = 0.0;
+                rc.field.EtY(i, j, k) = (hx * hz) * jac;
+                rc.field.EtZ(i, j, k) = 0.0;
+                rc.field.ZeX(i, j, k) = 0.0;
+                rc.field.ZeY(i, j, k) = 0.0;
+                rc.field.ZeZ(i, j, k) = (hx * hy) * jac;
+                rc.field.X(i, j, k) = (i - g->ng) * hx;
+                rc.field.Y(i, j, k) = (j - g->ng) * hy;
+                rc.field.Z(i, j, k) = (k - g->ng) * hz;
+            }
+    // Solver-boundary sets: the transmissive (zeroGradient) ends, exactly the
+    // nodes that Boundary::Applicator marks (SF_applicator.h:162-187).
+    std::map<std::string, std::vector<int>> sets;
+    const int ng = g->ng;
+    for (int d = 0; d < g->dim; ++d) {
+        for (int end = 0; end < 2; ++end) {
+            const int kind = end ? g->bc_hi[d] : g->bc_lo[d];
+            if (kind != SFO_BC_TRANSMISSIVE) continue;
+            std::string name = std::string("bc") + char('0' + d) + (end ? "hi" : "lo");
+            auto& ids = sets[name];
+            const int fixed = end ? g->n[d] - 1 + ng : ng;
+            for (int k = 0; k < g->n[2]; ++k)
+                for (int j = 0; j < g->n[1]; ++j)
+                    for (int i = 0; i < g->n[0]; ++i) {
+                        int idx[3] = {i + ng, j + ng, k + ng};
+                        if (idx[d] != fixed) continue;
+                        ids.push_back(rc.field.getIdx(idx[0], idx[1], idx[2]));
+                    }
+        }
+    }
+    rc.field.setBoundarySets(sets);
+    rc.field.clearSolverBoundaryMask();
+    for (auto& kv : sets) rc.field.markSolverBoundarySet(kv.first);
+    const int mx = rc.field.MX(), my = rc.field.MY(), mz = rc.field.MZ();
+    rc.flux.setup((size_t)3 * (size_t)mx * my * mz, 5);
+    rc.residual.setup(mx, my, mz, 5);
+}
+
+// compact (ghosts on active axes only) <-> reference Field (ghosts everywhere)
+void load_state(RefCase& rc, const double* Q) {
+    const sfo_grid* g = &rc.g;
+    const int m0 = storage_extent(g, 0), m1 = storage_extent(g, 1);
+    int off[3];
+    for (int d = 0; d < 3; ++d) off[d] = d < g->dim ? 0 : g->ng;
+    for (int k = 0; k < rc.field.MZ(); ++k)
+        for (int j = 0; j < rc.field.MY(); ++j)
+            for (int i = 0; i < rc.field.MX(); ++i) {
+                int c[3] = {i - off[0], j - off[1], k - off[2]};
+                for (int d = 0; d < 3; ++d) {
+                    const int m = storage_extent(g, d);
+                    if (c[d] < 0) c[d] = 0;
+                    if (c[d] >= m) c[d] = m - 1;
+                }
+                const double* q = Q + 5 * (((long long)c[2] * m1 + c[1]) * m0 + c[0]);
+                for (int v = 0; v < 5; ++v) rc.field(i, j, k, v) = q[v];
+            }
+    rc.field.invalidateThermodynamicCache();
+}
+
+int scheme_of(int s, SF::FDM::ConvectionScheme* out) {
+    switch (s) {
+    case SFO_WENO3: *out = SF::FDM::ConvectionScheme::WENO3; return 0;
+    case SFO_WENO5: *out = SF::FDM::ConvectionScheme::WENO5; return 0;
+    case SFO_TENO5: *out = SF::FDM::ConvectionScheme::TENO5; return 0;
+    case SFO_WENO7: *out = SF::FDM::ConvectionScheme::WENO7; return 0;
+    }
+    return SFO_ERR_ARG;
+}
+
+int flux_of(int f, SF::FDM::FluxSplitter* out) {
+    switch (f) {
+    case SFO_STEGER: *out = SF::FDM::FluxSplitter::StegerWarming; return 0;
+    case SFO_RUSANOV: *out = SF::FDM::FluxSplitter::Rusanov; return 0;
+    case SFO_LAXFRIEDRICHS: *out = SF::FDM::FluxSplitter::LaxFriedrichs; return 0;
+    case SFO_ROE: *out = SF::FDM::FluxSplitter::Roe; return 0;
+    }
+    return SFO_ERR_ARG;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Residual of the reference spatial operator on Q (compact layout, ghosts
+// already filled), written to R (compact layout; ghosts zero).
+int sfr_rhs(const sfo_grid* g, int scheme, int flux, const double* Q, double* R) {
+    try {
+        SF::FDM::ConvectionScheme cs;
+        SF::FDM::FluxSplitter fs;
+        if (scheme_of(scheme, &cs) || flux_of(flux, &fs)) return SFO_ERR_ARG;
+        RefCase rc;
+        setup_case(rc, g);
+        load_state(rc, Q);
+        rc.flux.clear();
+        rc.residual.clear();
+        SF::divDispatch(rc.field, rc.flux, rc.residual, cs, fs, 0.0,
+                        SF::FDM::IBMBoundaryScheme::LowOrder, 0, g->gamma, *rc.model);
+        const long long S = 5LL * storage_extent(g, 0) * storage_extent(g, 1) * storage_extent(g, 2);
+        std::memset(R, 0, sizeof(double) * (size_t)S);
+        const int m0 = storage_extent(g, 0), m1 = storage_extent(g, 1);
+        int off[3];
+        for (int d = 0; d < 3; ++d) off[d] = d < g->dim ? 0 : g->ng;
+        const int ng = g->ng;
+        for (int k = ng; k < ng + g->n[2]; ++k)
+            for (int j = ng; j < ng + g->n[1]; ++j)
+                for (int i = ng; i < ng + g->n[0]; ++i) {
+                    const long long at = 5 * (((long long)(k - off[2]) * m1 + (j - off[1])) * m0 + (i - off[0]));
+                    for (int v = 0; v < 5; ++v)
+                        R[at + v] = SF::Math::spatialResidual(rc.field, rc.residual, i, j, k, v);
+                }
+        return SFO_OK;
+    } catch (const std::exception&) {
+        return SFO_ERR_STATE;
+    }
+}
+
+int sfr_dt(const sfo_grid* g, const double* Q, double cfl, double* dt) {
+    try {
+        RefCase rc;
+        setup_case(rc, g);
+        load_state(rc, Q);
+        *dt = SF::Numerics::RusanovEOS::deltaT(rc.field, *rc.model, cfl);
+        return SFO_OK;
+    } catch (const std::exception&) {
+        return SFO_ERR_STATE;
+    }
+}
+
+// ---- persistent case: Field allocated once, reference operator per stage ----
+
+struct PersistentCase {
+    RefCase rc;
+    int scheme = 0, flux = 0;
+    SF::FDM::ConvectionScheme cs{};
+    SF::FDM::FluxSplitter fs{};
+    std::vector<double> work;
+};
+
+static int case_rhs(void* ctx, const double* Q, double* R) {
+    auto* pc = static_cast<PersistentCase*>(ctx);
+    const sfo_grid* g = &pc->rc.g;
+    try {
+        load_state(pc->rc, Q);
+        pc->rc.flux.clear();
+        pc->rc.residual.clear();
+        SF::divDispatch(pc->rc.field, pc->rc.flux, pc->rc.residual, pc->cs, pc->fs, 0.0,
+                        SF::FDM::IBMBoundaryScheme::LowOrder, 0, g->gamma, *pc->rc.model);
+        const int m0 = storage_extent(g, 0), m1 = storage_extent(g, 1);
+        int off[3];
+        for (int d = 0; d < 3; ++d) off[d] = d < g->dim ? 0 : g->ng;
+        const int ng = g->ng;
+        for (int k = ng; k < ng + g->n[2]; ++k)
+            for (int j = ng; j < ng + g->n[1]; ++j)
+                for (int i = ng; i < ng + g->n[0]; ++i) {
+                    const long long at =
+                        5 * (((long long)(k - off[2]) * m1 + (j - off[1])) * m0 + (i - off[0]));
+                    for (int v = 0; v < 5; ++v)
+                        R[at + v] = SF::Math::spatialResidual(pc->rc.field, pc->rc.residual, i, j, k, v);
+                }
+        return SFO_OK;
+    } catch (const std::exception&) {
+        return SFO_ERR_STATE;
+    }
+}
+
+static int case_dt(void* ctx, const double* Q, double cfl, double* dt) {
+    auto* pc = static_cast<PersistentCase*>(ctx);
+    try {
+        load_state(pc->rc, Q);
+        *dt = SF::Numerics::RusanovEOS::deltaT(pc->rc.field, *pc->rc.model, cfl);
+        return SFO_OK;
+    } catch (const std::exception&) {
+        return SFO_ERR_STATE;
+    }
+}
+
+void* sfr_case_create(const sfo_grid* g, int scheme, int flux) {
+    auto* pc = new PersistentCase;
+    if (scheme_of(scheme, &pc->cs) || flux_of(flux, &pc->fs)) {
+        delete pc;
+        return nullptr;
+    }
+    pc->scheme = scheme;
+    pc->flux = flux;
+    setup_case(pc->rc, g);
+    pc->work.assign((size_t)5 * 5 * storage_extent(g, 0) * storage_extent(g, 1) * storage_extent(g, 2), 0.0);
+    return pc;
+}
+
+void sfr_case_destroy(void* h) { delete static_cast<PersistentCase*>(h); }
+
+int sfr_case_rhs(void* h, const double* Q, double* R) { return case_rhs(h, Q, R); }
+
+int sfr_case_dt(void* h, const double* Q, double cfl, double* dt) { return case_dt(h, Q, cfl, dt); }
+
+// One full explicit step of size dt (ghost fill and stage arithmetic restated,
+// spatial operator from the reference).
+int sfr_case_step(void* h, int time_id, double* Q, double dt) {
+    auto* pc = static_cast<PersistentCase*>(h);
+    const int ns = time_id == SFO_EULER ? 1 : (time_id == SFO_SSPRK3 ? 3 : (time_id == SFO_RK4 ? 4 : 0));
+    if (!ns) return SFO_ERR_ARG;
+    for (int s = 0; s < ns; ++s) {
+        int err = sfo_stage_fn(&pc->rc.g, case_rhs, pc, time_id, Q, dt, s, pc->work.data());
+        if (err) return err;
+    }
+    return SFO_OK;
+}
+
+int sfr_case_advance(void* h, int time_id, double* Q, double t_start, double t_end, double cfl,
+                     double max_dt, double write_interval, int max_steps, double* dt_out,
+                     int* steps_done, double* t_final) {
+    auto* pc = static_cast<PersistentCase*>(h);
+    return sfo_advance_fn(&pc->rc.g, case_rhs, case_dt, pc, time_id, Q, t_start, t_end, cfl, max_dt,
+                          write_interval, max_steps, dt_out, steps_done, t_final);
+}
+
+// Scalar cores and fluxes straight from the reference (known-answer tests).
+double sfr_weno5_core(const double* v) { return SF::WENO5::weno5_core(v); }
+double sfr_teno5_core(const double* v) { return SF::TENO5::teno5_core(v); }
+double sfr_weno3_core(const double* v) { return SF::WENO3::weno3_core(v); }
+double sfr_weno7_core(const double* v) { return SF::WENO7::weno7_core(v); }
+void sfr_char_matrix(const double* q, const double* n, double gamma, double* L, double* R) {
+    SF::Riemann::buildCharacteristicMatrix(q, n, gamma, L, R);
+}
+int sfr_rusanov_flux(const double* qL, const double* qR, const double* n, double gamma, double* out) {
+    try {
+        auto model = perfect_gas(gamma);
+        SF::Numerics::RusanovEOS::faceFlux(*model, qL, qR, {n[0], n[1], n[2]}, out, 5);
+        return SFO_OK;
+    } catch (const std::exception&) {
+        return SFO_ERR_STATE;
+    }
+}
+void sfr_roe_flux(const double* qL, const double* qR, const double* n, double gamma, double* out) {
+    SF::Flux::RoeFlux::flux(qL, qR, n, out, gamma);
+}
+
+}  // extern "C"

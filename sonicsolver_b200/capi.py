@@ -1,0 +1,234 @@
+"""ctypes binding of the C ABI in ``include/sonicsolver_b200.h``.
+
+This is the Python face of the B200 provider: it loads the in-tree
+``libsonicsolver_b200.so`` (built by :mod:`sonicsolver_b200.build`) and raises
+if it is missing -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsonicsolver_b200.so")
+
+OK = 0
+ERR_ARG, ERR_CUDA, ERR_STATE, ERR_TENO_CUTOFF, ERR_NOMEM, ERR_BUDGET, ERR_TIMEOUT, ERR_NOT_FOUND, ERR_CANCELLED = range(1, 10)
+
+FLAG_NONFINITE, FLAG_DENSITY, FLAG_PRESSURE, FLAG_TENO_CUTOFF, FLAG_ROE_SOUND = 1, 2, 4, 8, 16
+
+RECIPES = {
+    "weno3Rusanov": 1, "weno3Roe": 3, "weno5Rusanov": 6, "weno5Roe": 8,
+    "teno5Rusanov": 11, "teno5Roe": 13, "weno7Rusanov": 16, "weno7Roe": 18,
+}
+TIME_RECIPES = {"forwardEuler": 0, "SSPRK3": 1, "classicalRK4": 2}
+PREC_FP64, PREC_FP32_FLUX = 0, 1
+BC_TRANSMISSIVE, BC_PERIODIC = 0, 1
+LAYOUT_NODES, LAYOUT_FIELD = 0, 1
+
+# The C-ABI symbols declared by include/sonicsolver_b200.h (checked by tests).
+EXPORTS = (
+    "sfg_last_error", "sfg_version", "sfg_recipe_name", "sfg_recipe_from_name", "sfg_create",
+    "sfg_destroy", "sfg_ghost_layers", "sfg_state_size", "sfg_upload", "sfg_download",
+    "sfg_upload_device", "sfg_download_device", "sfg_compute_dt", "sfg_stage", "sfg_step",
+    "sfg_advance", "sfg_residual", "sfg_stage_with_residual", "sfg_conserved_totals", "sfg_time",
+    "sfg_status_word", "sfg_set_counting", "sfg_get_counters", "sfg_time_sweeps", "sfg_measure_fma_peak",
+)
+
+
+class GridDesc(ctypes.Structure):
+    _fields_ = [("dim", ctypes.c_int), ("n", ctypes.c_int * 3), ("h", ctypes.c_double * 3),
+                ("bc_lo", ctypes.c_int * 3), ("bc_hi", ctypes.c_int * 3)]
+
+
+class NumericsDesc(ctypes.Structure):
+    _fields_ = [("recipe", ctypes.c_int), ("time_recipe", ctypes.c_int), ("precision", ctypes.c_int),
+                ("gamma", ctypes.c_double), ("cfl", ctypes.c_double), ("max_dt", ctypes.c_double)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("steps", ctypes.c_int64), ("time", ctypes.c_double), ("last_dt", ctypes.c_double),
+                ("device_ms", ctypes.c_double), ("status_bits", ctypes.c_uint32),
+                ("teno_cut", ctypes.c_uint64), ("teno_cores", ctypes.c_uint64)]
+
+
+class SolverError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+_lib = None
+_DP = ctypes.POINTER(ctypes.c_double)
+_VP = ctypes.c_void_p
+
+
+def lib():
+    """The loaded provider library (raises when it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m sonicsolver_b200.build` "
+                               "(the provider has no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        L.sfg_last_error.restype = ctypes.c_char_p
+        L.sfg_recipe_name.restype = ctypes.c_char_p
+        L.sfg_recipe_name.argtypes = [ctypes.c_int]
+        L.sfg_recipe_from_name.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)]
+        L.sfg_version.argtypes = [ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+        L.sfg_create.argtypes = [ctypes.POINTER(GridDesc), ctypes.POINTER(NumericsDesc), _VP, ctypes.POINTER(_VP)]
+        L.sfg_destroy.argtypes = [_VP]
+        L.sfg_ghost_layers.argtypes = [_VP, ctypes.POINTER(ctypes.c_int)]
+        L.sfg_state_size.argtypes = [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]
+        L.sfg_upload.argtypes = [_VP, _DP, ctypes.c_int, ctypes.c_double]
+        L.sfg_download.argtypes = [_VP, _DP, ctypes.c_int]
+        L.sfg_upload_device.argtypes = [_VP, _VP, ctypes.c_double]
+        L.sfg_download_device.argtypes = [_VP, _VP]
+        L.sfg_compute_dt.argtypes = [_VP, ctypes.c_double, _DP]
+        L.sfg_stage.argtypes = [_VP, ctypes.c_int, ctypes.c_double]
+        L.sfg_step.argtypes = [_VP, ctypes.c_double, ctypes.c_double]
+        L.sfg_advance.argtypes = [_VP, ctypes.c_double, ctypes.c_int64, ctypes.c_double, ctypes.c_int, _DP,
+                                  ctypes.c_int64, ctypes.POINTER(Stats)]
+        L.sfg_residual.argtypes = [_VP, _DP]
+        L.sfg_stage_with_residual.argtypes = [_VP, ctypes.c_int, ctypes.c_double, _DP]
+        L.sfg_conserved_totals.argtypes = [_VP, _DP]
+        L.sfg_time.argtypes = [_VP, _DP, ctypes.POINTER(ctypes.c_int64)]
+        L.sfg_status_word.argtypes = [_VP, ctypes.POINTER(ctypes.c_uint32), ctypes.c_int]
+        L.sfg_set_counting.argtypes = [_VP, ctypes.c_int]
+        L.sfg_get_counters.argtypes = [_VP, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
+        L.sfg_time_sweeps.argtypes = [_VP, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                      ctypes.POINTER(ctypes.c_float)]
+        L.sfg_measure_fma_peak.argtypes = [ctypes.c_int, ctypes.c_double, _DP]
+        _lib = L
+    return _lib
+
+
+def check(code: int):
+    if code != OK:
+        raise SolverError(code, lib().sfg_last_error().decode())
+
+
+def _dptr(a: np.ndarray):
+    if a.dtype != np.float64 or not a.flags.c_contiguous:
+        raise ValueError("expected a C-contiguous float64 array")
+    return a.ctypes.data_as(_DP)
+
+
+def grid_desc(dim, n, h, bc_lo, bc_hi) -> GridDesc:
+    g = GridDesc()
+    g.dim = dim
+    for d in range(3):
+        g.n[d] = int(n[d])
+        g.h[d] = float(h[d])
+        g.bc_lo[d] = int(bc_lo[d])
+        g.bc_hi[d] = int(bc_hi[d])
+    return g
+
+
+class Solver:
+    """One grid on the GPU (``sfg_solver``)."""
+
+    def __init__(self, dim, n, h, bc_lo, bc_hi, recipe="weno5Rusanov", time_recipe="SSPRK3",
+                 precision=PREC_FP64, gamma=1.4, cfl=0.5, max_dt=0.0, stream=None):
+        self.dim, self.n = dim, tuple(int(x) for x in n)
+        g = grid_desc(dim, n, h, bc_lo, bc_hi)
+        nm = NumericsDesc()
+        nm.recipe = RECIPES[recipe] if isinstance(recipe, str) else int(recipe)
+        nm.time_recipe = TIME_RECIPES[time_recipe] if isinstance(time_recipe, str) else int(time_recipe)
+        nm.precision = precision
+        nm.gamma, nm.cfl, nm.max_dt = gamma, cfl, max_dt
+        h_ = _VP()
+        check(lib().sfg_create(ctypes.byref(g), ctypes.byref(nm), stream, ctypes.byref(h_)))
+        self._h = h_
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().sfg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def node_shape(self):
+        return (self.n[2], self.n[1], self.n[0], 5)
+
+    def upload(self, q: np.ndarray, time: float = 0.0, layout=LAYOUT_NODES):
+        check(lib().sfg_upload(self._h, _dptr(q), layout, time))
+
+    def download(self, layout=LAYOUT_NODES, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            cnt = ctypes.c_size_t()
+            check(lib().sfg_state_size(self._h, layout, ctypes.byref(cnt)))
+            out = np.empty(cnt.value, dtype=np.float64)
+        check(lib().sfg_download(self._h, _dptr(out), layout))
+        return out
+
+    def compute_dt(self, limit=0.0) -> float:
+        v = ctypes.c_double()
+        check(lib().sfg_compute_dt(self._h, limit, ctypes.byref(v)))
+        return v.value
+
+    def stage(self, s, dt):
+        check(lib().sfg_stage(self._h, s, dt))
+
+    def step(self, dt=0.0, limit=0.0):
+        check(lib().sfg_step(self._h, dt, limit))
+
+    def advance(self, t_end, max_steps=0, write_interval=0.0, graph_steps=0, dt_capacity=0):
+        st = Stats()
+        buf = np.zeros(max(dt_capacity, 1))
+        check(lib().sfg_advance(self._h, t_end, max_steps, write_interval, graph_steps,
+                                _dptr(buf) if dt_capacity else None, dt_capacity, ctypes.byref(st)))
+        return st, buf[:min(st.steps, dt_capacity)].copy() if dt_capacity else None
+
+    def residual(self) -> np.ndarray:
+        out = np.empty(5 * int(np.prod(self.n)), dtype=np.float64)
+        check(lib().sfg_residual(self._h, _dptr(out)))
+        return out
+
+    def stage_with_residual(self, s, dt, r: np.ndarray):
+        check(lib().sfg_stage_with_residual(self._h, s, dt, _dptr(np.ascontiguousarray(r, dtype=np.float64))))
+
+    def totals(self):
+        out = np.zeros(5)
+        check(lib().sfg_conserved_totals(self._h, _dptr(out)))
+        return out
+
+    def time(self):
+        t = ctypes.c_double()
+        n = ctypes.c_int64()
+        check(lib().sfg_time(self._h, ctypes.byref(t), ctypes.byref(n)))
+        return t.value, n.value
+
+    def status(self, clear=False):
+        b = ctypes.c_uint32()
+        check(lib().sfg_status_word(self._h, ctypes.byref(b), 1 if clear else 0))
+        return b.value
+
+    def set_counting(self, on=True):
+        check(lib().sfg_set_counting(self._h, 1 if on else 0))
+
+    def counters(self):
+        a, b = ctypes.c_uint64(), ctypes.c_uint64()
+        check(lib().sfg_get_counters(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def time_sweeps(self, dt, stage=0, repeats=5):
+        out = (ctypes.c_float * 3)()
+        check(lib().sfg_time_sweeps(self._h, stage, dt, repeats, out))
+        return [out[d] for d in range(self.dim)]
+
+
+def fma_peak_tflops(fp64=True, seconds=0.5) -> float:
+    v = ctypes.c_double()
+    check(lib().sfg_measure_fma_peak(1 if fp64 else 0, seconds, ctypes.byref(v)))
+    return v.value

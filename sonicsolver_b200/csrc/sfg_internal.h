@@ -1,0 +1,81 @@
+// sfg_internal.h -- structures shared by the host runtime and the kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace sfg {
+
+constexpr int BC_TRANSMISSIVE = 0;
+constexpr int BC_PERIODIC = 1;
+
+// Status bits (match SFG_FLAG_* in include/sonicsolver_b200.h).
+constexpr unsigned FLAG_NONFINITE = 1u << 0;
+constexpr unsigned FLAG_DENSITY = 1u << 1;
+constexpr unsigned FLAG_PRESSURE = 1u << 2;
+constexpr unsigned FLAG_TENO_CUTOFF = 1u << 3;
+constexpr unsigned FLAG_ROE_SOUND = 1u << 4;
+
+// Reconstruction schemes in the order of FDM::ConvectionScheme and face
+// fluxes with the values of FDM::FluxSplitter (SF_termRecipe.h:14,33-40).
+enum Scheme { WENO3 = 0, WENO5 = 1, TENO5 = 2, WENO7 = 3 };
+enum Flux { RUSANOV = 1, ROE = 3 };
+
+// Device-resident step clock: the Time::Driver bookkeeping
+// (src/solver/algorithm/time/SF_time.cpp:42-93) and FlowDtCompute's
+// min(dt, maxDeltaT, limit) (SF_flowOperations.cpp:487-513) kept on the GPU so
+// that whole runs of steps execute inside one CUDA graph.
+struct Clock {
+    double t;                 // physical time
+    double t_end;             // run end (inf: none)
+    double next_out;          // next output time (inf: none)
+    double write_interval;    // <= 0: none
+    double max_dt;            // numerics maxDeltaT (inf: none)
+    double limit;             // one-shot extra limit (inf: none)
+    double dt;                // step size of the current step
+    unsigned long long dt_bits;  // CFL minimum, as ordered bits of a positive double
+    long long steps;
+    long long max_steps;
+    long long log_base;       // step index of dt_log[0]
+    int active;               // 1 while the current step runs
+    int pad;
+};
+
+// Geometry of one grid as the kernels see it (uniform Cartesian metrics).
+struct GridView {
+    int n[3];          // nodes per axis (1 on inactive axes)
+    int lo[3], hi[3];  // solved node range per axis
+    int bc_lo[3], bc_hi[3];
+    int dim;
+    long long vs;      // distance between variables in the SoA state (doubles)
+    double jac;        // 1 / J
+    double area[3];    // face cofactor magnitude per axis
+    double metric[3];  // xi_x, eta_y, zeta_z
+    double gamma;
+    double cfl;
+};
+
+// Stage arithmetic of one launch (Time::Explicit, SF_explicit.cpp:193-238,282-285).
+enum TimeId { T_EULER = 0, T_SSPRK3 = 1, T_RK4 = 2 };
+
+struct StageView {
+    const double* qs;     // state read by the stencils (current stage input)
+    const double* q0;     // step-start state
+    double* qout;         // stage output
+    double* r;            // residual accumulator (SoA)
+    double* k;            // RK4 accumulator (SoA)
+    Clock* clock;
+    unsigned* flags;
+    unsigned long long* counters;  // [teno cores, teno cut] or null
+    int time_id;
+    int stage;
+    double base, inc;     // SSPRK3: base*q0 + inc*(q - dt R);  RK4: inc = stage weight
+    int mode;             // MODE_* bits
+    int require_active;   // skip when clock->active == 0
+};
+
+constexpr int MODE_READ_R = 1;     // add the residual accumulated by earlier axes
+constexpr int MODE_FINAL = 2;      // last axis: finish the node
+constexpr int MODE_RESIDUAL = 4;   // final output is R = Jac * div (no stage update)
+
+}  // namespace sfg

@@ -1,0 +1,503 @@
+// sfg_kernels.cu -- sm_100a kernels of the explicit Euler path.
+//
+// State layout in HBM: structure of arrays, q[v * vs + (k * ny + j) * nx + i]
+// over the nodes only (no ghost storage).  Ghost and boundary-node values are
+// produced by index mapping when a stencil is read:
+//   transmissive end: any index at or beyond the boundary node reads its inner
+//     neighbour (zeroGradient: boundary node <- inner node, ghosts <- boundary
+//     node; reconstruction/linear/SF_zeroGradient.cpp:88-105);
+//   periodic end: indices wrap.
+// This is the in-device replacement of the per-stage ghost fill and MPI halo
+// exchange (SF_conservativeRHS.cpp:75-104).
+//
+// One stage on a D-dimensional grid is D sweep launches.  Sweep d computes
+// the face fluxes along axis d once per face, differences them into the node
+// residual (held in registers, accumulated through a FP64 residual array
+// across axes), and the last sweep applies the stage combination.
+//   x sweeps: one warp per 31 consecutive nodes of a row, one lane per face,
+//     neighbour face by warp shuffle (coalesced loads along x);
+//   y / z sweeps: one thread per node column segment, marching along the axis
+//     with the stencil in a register sliding window (one node load per face).
+#include "sfg_internal.h"
+#include "sfg_math.cuh"
+
+#include <cstdio>
+
+namespace sfg {
+
+__device__ __forceinline__ int map_index(int i, int n, int bcl, int bch) {
+    if (bcl == BC_PERIODIC) {
+        if (i < 0) i += n;
+    } else if (i < 1) {
+        i = 1;
+    }
+    if (bch == BC_PERIODIC) {
+        if (i >= n) i -= n;
+    } else if (i > n - 2) {
+        i = n - 2;
+    }
+    return i;
+}
+
+__device__ __forceinline__ void atomic_min_positive(unsigned long long* bits, double v) {
+    atomicMin(bits, (unsigned long long)__double_as_longlong(v));
+}
+
+// Stage combination at one node for one variable (applySSPStage, applyStage,
+// applyFinalRK4, applyDivergence).  qs_v is the current value, r the residual.
+__device__ __forceinline__ double stage_value(const StageView& sv, double dt, double qs_v, double r,
+                                              long long at) {
+    switch (sv.time_id) {
+    case T_EULER:
+        return qs_v - dt * r;
+    case T_SSPRK3: {
+        const double euler = qs_v - dt * r;
+        return sv.base * sv.q0[at] + sv.inc * euler;
+    }
+    default: {  // classical RK4 with one accumulator K = k1 + 2 k2 + 2 k3
+        if (sv.stage == 0) sv.k[at] = r;
+        else if (sv.stage < 3) sv.k[at] = sv.k[at] + 2.0 * r;
+        if (sv.stage < 3) return sv.q0[at] - sv.inc * dt * r;
+        return sv.q0[at] - dt / 6.0 * (sv.k[at] + 1.0 * r);
+    }
+    }
+}
+
+// Finishes one node: residual output or stage update + state validation
+// (validateEquationState after every stage, SF_explicit.cpp:417).
+__device__ __forceinline__ void finish_node(const GridView& g, const StageView& sv, double dt, long long node,
+                                            const double (&qn)[5], double (&div)[5], unsigned& flags) {
+    const long long vs = g.vs;
+    if (sv.mode & MODE_RESIDUAL) {
+#pragma unroll
+        for (int v = 0; v < 5; ++v) sv.r[v * vs + node] = g.jac * div[v];
+        return;
+    }
+    double out[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) out[v] = stage_value(sv, dt, qn[v], g.jac * div[v] - 0.0, v * vs + node);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) sv.qout[v * vs + node] = out[v];
+    const double ke = 0.5 * (out[1] * out[1] + out[2] * out[2] + out[3] * out[3]) / out[0];
+    const double p = (g.gamma - 1.0) * (out[4] - ke);
+    if (!(out[0] > 0.0)) flags |= FLAG_DENSITY;
+    if (!(p > 0.0)) flags |= FLAG_PRESSURE;
+    if (!isfinite(out[0] + out[1] + out[2] + out[3] + out[4])) flags |= FLAG_NONFINITE;
+}
+
+__device__ __forceinline__ void flush_status(const StageView& sv, unsigned flags, unsigned cores, unsigned cut) {
+    if (flags) atomicOr(sv.flags, flags);
+    if (sv.counters) {
+        // one atomic per warp
+        unsigned c = cores, k = cut;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            c += __shfl_xor_sync(0xffffffffu, c, o);
+            k += __shfl_xor_sync(0xffffffffu, k, o);
+        }
+        if ((threadIdx.x & 31) == 0 && (c | k)) {
+            atomicAdd(sv.counters + 0, (unsigned long long)c);
+            atomicAdd(sv.counters + 1, (unsigned long long)k);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// x sweep: blockDim = (32, ROWS); one warp per 31 nodes of one row.
+// ---------------------------------------------------------------------------
+template <int SCHEME, int FLUX, typename T>
+__global__ void __launch_bounds__(128) sweep_x(GridView g, StageView sv) {
+    constexpr int NST = SchemeInfo<SCHEME>::NST;
+    if (sv.require_active && !sv.clock->active) return;
+    const int lane = threadIdx.x;
+    const int cnt_y = g.hi[1] - g.lo[1];
+    const int cnt_z = g.hi[2] - g.lo[2];
+    const int row = blockIdx.y * blockDim.y + threadIdx.y;
+    if (row >= cnt_y * cnt_z) return;  // whole warp exits together
+    const int j = g.lo[1] + row % cnt_y;
+    const int k = g.lo[2] + row / cnt_y;
+    const int i0 = g.lo[0] + blockIdx.x * 31;
+    const int nodes = min(31, g.hi[0] - i0);
+    const int f = i0 + lane;  // face between nodes f-1 and f
+    const long long rowbase = ((long long)k * g.n[1] + j) * g.n[0];
+    const long long vs = g.vs;
+    unsigned flags = 0, cut = 0;
+    double st[NST][5];
+    double F[5] = {0, 0, 0, 0, 0};
+    if (lane <= nodes) {
+#pragma unroll
+        for (int s = 0; s < NST; ++s) {
+            const int ii = map_index(f - NST / 2 + s, g.n[0], g.bc_lo[0], g.bc_hi[0]);
+#pragma unroll
+            for (int v = 0; v < 5; ++v) st[s][v] = __ldg(sv.qs + v * vs + rowbase + ii);
+        }
+        T Ft[5];
+        face_flux<0, SCHEME, FLUX, T>(st, T(g.gamma), Ft, flags, cut);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) F[v] = double(Ft[v]) * g.area[0];
+    }
+    double div[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) div[v] = __shfl_down_sync(0xffffffffu, F[v], 1) - F[v];
+    if (lane < nodes) {
+        const long long node = rowbase + f;
+        if (sv.mode & MODE_READ_R) {
+#pragma unroll
+            for (int v = 0; v < 5; ++v) div[v] = sv.r[v * vs + node] + div[v];
+        }
+        if (sv.mode & MODE_FINAL) {
+            double qn[5];
+#pragma unroll
+            for (int v = 0; v < 5; ++v) qn[v] = st[NST / 2][v];
+            finish_node(g, sv, sv.clock->dt, node, qn, div, flags);
+        } else {
+#pragma unroll
+            for (int v = 0; v < 5; ++v) sv.r[v * vs + node] = div[v];
+        }
+    }
+    flush_status(sv, flags, SCHEME == TENO5 ? (lane <= nodes ? 10u : 0u) : 0u, cut);
+}
+
+// ---------------------------------------------------------------------------
+// y / z sweep: blockDim = (32, SEGS); thread = (x node, segment of SEGLEN
+// nodes along AX); blockIdx.z = the remaining axis.
+// ---------------------------------------------------------------------------
+constexpr int SEGLEN = 16;
+
+template <int AX, int SCHEME, int FLUX, typename T>
+__global__ void __launch_bounds__(128) sweep_yz(GridView g, StageView sv) {
+    constexpr int NST = SchemeInfo<SCHEME>::NST;
+    if (sv.require_active && !sv.clock->active) return;
+    constexpr int OTHER = AX == 1 ? 2 : 1;
+    const int i = g.lo[0] + blockIdx.x * 32 + threadIdx.x;
+    const int o = g.lo[OTHER] + blockIdx.z;
+    const int s0 = g.lo[AX] + (blockIdx.y * blockDim.y + threadIdx.y) * SEGLEN;
+    const bool live = i < g.hi[0] && s0 < g.hi[AX];
+    unsigned flags = 0, cut = 0, cores = 0;
+    if (live) {
+        const int s1 = min(s0 + SEGLEN, g.hi[AX]);
+        const long long vs = g.vs;
+        const long long sx = 1, sy = g.n[0], sz = (long long)g.n[0] * g.n[1];
+        const long long sa = AX == 1 ? sy : sz;
+        const long long base = i * sx + (long long)o * (OTHER == 1 ? sy : sz);
+        const int n = g.n[AX];
+        const int bl = g.bc_lo[AX], bh = g.bc_hi[AX];
+        const double dt = sv.clock->dt;
+        double st[NST][5];
+#pragma unroll
+        for (int s = 0; s < NST; ++s) {
+            const int a = map_index(s0 - NST / 2 + s, n, bl, bh);
+#pragma unroll
+            for (int v = 0; v < 5; ++v) st[s][v] = sv.qs[v * vs + base + a * sa];
+        }
+        double Fp[5];
+        for (int f = s0; f <= s1; ++f) {
+            T Ft[5];
+            face_flux<AX, SCHEME, FLUX, T>(st, T(g.gamma), Ft, flags, cut);
+            if (SCHEME == TENO5) cores += 10;
+            double F[5];
+#pragma unroll
+            for (int v = 0; v < 5; ++v) F[v] = double(Ft[v]) * g.area[AX];
+            if (f > s0) {
+                const long long node = base + (long long)(f - 1) * sa;
+                double div[5];
+#pragma unroll
+                for (int v = 0; v < 5; ++v) div[v] = F[v] - Fp[v];
+                if (sv.mode & MODE_READ_R) {
+#pragma unroll
+                    for (int v = 0; v < 5; ++v) div[v] = sv.r[v * vs + node] + div[v];
+                }
+                if (sv.mode & MODE_FINAL) {
+                    double qn[5];
+#pragma unroll
+                    for (int v = 0; v < 5; ++v) qn[v] = st[NST / 2 - 1][v];
+                    finish_node(g, sv, dt, node, qn, div, flags);
+                } else {
+#pragma unroll
+                    for (int v = 0; v < 5; ++v) sv.r[v * vs + node] = div[v];
+                }
+            }
+#pragma unroll
+            for (int v = 0; v < 5; ++v) Fp[v] = F[v];
+            if (f < s1) {
+#pragma unroll
+                for (int s = 0; s < NST - 1; ++s)
+#pragma unroll
+                    for (int v = 0; v < 5; ++v) st[s][v] = st[s + 1][v];
+                const int a = map_index(f + 1 - NST / 2 + NST - 1, n, bl, bh);
+#pragma unroll
+                for (int v = 0; v < 5; ++v) st[NST - 1][v] = sv.qs[v * vs + base + a * sa];
+            }
+        }
+    }
+    flush_status(sv, flags, cores, cut);
+}
+
+// ---------------------------------------------------------------------------
+// CFL step (RusanovEOS::deltaT, SF_rusanovEOS.cpp:110-147) with the block /
+// grid minimum replacing Runtime::globalMinimum's MPI_Allreduce(MIN).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) dt_kernel(GridView g, const double* __restrict__ q, Clock* clock,
+                                                 unsigned* flags, int require_active) {
+    const long long cx = g.hi[0] - g.lo[0], cy = g.hi[1] - g.lo[1], cz = g.hi[2] - g.lo[2];
+    const long long total = cx * cy * cz;
+    double best = 1.7976931348623157e308;
+    unsigned fl = 0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = g.lo[0] + (int)(t % cx);
+        const int j = g.lo[1] + (int)((t / cx) % cy);
+        const int k = g.lo[2] + (int)(t / (cx * cy));
+        const long long node = ((long long)k * g.n[1] + j) * g.n[0] + i;
+        const double rho = q[node];
+        const double u = q[g.vs + node] / rho, v = q[2 * g.vs + node] / rho, w = q[3 * g.vs + node] / rho;
+        const double kin = 0.5 * rho * (u * u + v * v + w * w);
+        const double e = (q[4 * g.vs + node] - kin) / rho;
+        const double p = (g.gamma - 1.0) * rho * e;
+        const double c = sqrt(g.gamma * p / rho);
+        double sr = 0.0;
+        sr += fabs(u * g.metric[0]) + c * g.metric[0];
+        if (g.dim > 1) sr += fabs(v * g.metric[1]) + c * g.metric[1];
+        if (g.dim > 2) sr += fabs(w * g.metric[2]) + c * g.metric[2];
+        if (!(sr > 0.0) || !isfinite(sr)) fl |= FLAG_NONFINITE;
+        const double cand = g.cfl / sr;
+        best = cand < best ? cand : best;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double other = __shfl_xor_sync(0xffffffffu, best, o);
+        best = other < best ? other : best;
+    }
+    __shared__ double wmin[8];
+    if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = best;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) best = wmin[w] < best ? wmin[w] : best;
+        atomic_min_positive(&clock->dt_bits, best);
+    }
+    if (fl) atomicOr(flags, fl);
+}
+
+// FlowDtCompute's min(dt, maxDeltaT, limit) with the Time::Driver end / output
+// clipping and stop test (SF_time.cpp:56-72).  One thread.
+__global__ void finalize_dt_kernel(Clock* c) {
+    const double eps = 2.220446049250313e-16;
+    const double remaining = c->t_end - c->t;
+    double scale = fmax(fabs(c->t), fabs(c->t_end));
+    scale = scale < 1.0 ? 1.0 : scale;
+    if (!(remaining > 64.0 * eps * scale) || c->steps >= c->max_steps) {
+        c->active = 0;
+        c->dt = 0.0;
+        return;
+    }
+    double limit = remaining;
+    if (c->write_interval > 0.0 && c->next_out - c->t < limit) limit = c->next_out - c->t;
+    if (c->limit < limit) limit = c->limit;
+    double dt = __longlong_as_double((long long)c->dt_bits);
+    if (c->max_dt < dt) dt = c->max_dt;
+    if (limit < dt) dt = limit;
+    c->dt = dt;
+    c->active = 1;
+}
+
+// TimeCommit: t += dt, ++step, output-time bookkeeping; re-arms the CFL min.
+__global__ void commit_kernel(Clock* c, double* dt_log, long long dt_cap) {
+    if (c->active) {
+        if (dt_log && c->steps - c->log_base < dt_cap && c->steps >= c->log_base) dt_log[c->steps - c->log_base] = c->dt;
+        c->t += c->dt;
+        c->steps += 1;
+        double sc = fabs(c->t);
+        sc = sc < 1.0 ? 1.0 : sc;
+        if (c->write_interval > 0.0 && c->t >= c->next_out - 1.0e-11 * sc) c->next_out += c->write_interval;
+    }
+    c->dt_bits = 0x7FEFFFFFFFFFFFFFull;  // largest finite double
+    c->limit = __longlong_as_double(0x7FF0000000000000ll);
+}
+
+__global__ void set_dt_kernel(Clock* c, double dt) {
+    c->dt = dt;
+    c->active = 1;
+}
+
+__global__ void reset_min_kernel(Clock* c) { c->dt_bits = 0x7FEFFFFFFFFFFFFFull; }
+
+// Stage combination with a residual supplied in sv.r (already Jac-scaled).
+__global__ void stage_from_residual_kernel(GridView g, StageView sv) {
+    const long long cx = g.hi[0] - g.lo[0], cy = g.hi[1] - g.lo[1], cz = g.hi[2] - g.lo[2];
+    const long long total = cx * cy * cz;
+    unsigned flags = 0;
+    const double dt = sv.clock->dt;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = g.lo[0] + (int)(t % cx);
+        const int j = g.lo[1] + (int)((t / cx) % cy);
+        const int k = g.lo[2] + (int)(t / (cx * cy));
+        const long long node = ((long long)k * g.n[1] + j) * g.n[0] + i;
+        double out[5];
+        for (int v = 0; v < 5; ++v)
+            out[v] = stage_value(sv, dt, sv.qs[v * g.vs + node], sv.r[v * g.vs + node], v * g.vs + node);
+        for (int v = 0; v < 5; ++v) sv.qout[v * g.vs + node] = out[v];
+        if (!(out[0] > 0.0)) flags |= FLAG_DENSITY;
+    }
+    if (flags) atomicOr(sv.flags, flags);
+}
+
+// AoS nodes (host layout) <-> SoA state.  On the way out the unsolved
+// transmissive boundary nodes are filled from their inner neighbours (the
+// commit ghost fill, SF_flowOperations.cpp:647-652).
+__global__ void aos_to_soa_kernel(const double* __restrict__ aos, double* __restrict__ soa, long long nodes,
+                                  long long vs) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nodes * 5;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long node = t / 5;
+        const int v = (int)(t % 5);
+        soa[v * vs + node] = aos[t];
+    }
+}
+
+__global__ void soa_to_aos_kernel(GridView g, const double* __restrict__ soa, double* __restrict__ aos) {
+    const long long nodes = (long long)g.n[0] * g.n[1] * g.n[2];
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nodes * 5;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long node = t / 5;
+        const int v = (int)(t % 5);
+        int i = (int)(node % g.n[0]);
+        int j = (int)((node / g.n[0]) % g.n[1]);
+        int k = (int)(node / ((long long)g.n[0] * g.n[1]));
+        if (g.dim > 0) i = map_index(i, g.n[0], g.bc_lo[0], g.bc_hi[0]);
+        if (g.dim > 1) j = map_index(j, g.n[1], g.bc_lo[1], g.bc_hi[1]);
+        if (g.dim > 2) k = map_index(k, g.n[2], g.bc_lo[2], g.bc_hi[2]);
+        aos[t] = soa[v * g.vs + ((long long)k * g.n[1] + j) * g.n[0] + i];
+    }
+}
+
+// Conserved totals over the nodes (trapezoid-free node sums x cell volume),
+// FP64 with a per-block tree and one atomic per block per variable.
+__global__ void totals_kernel(GridView g, const double* __restrict__ q, double* __restrict__ out, double vol) {
+    const long long nodes = (long long)g.n[0] * g.n[1] * g.n[2];
+    double acc[5] = {0, 0, 0, 0, 0};
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nodes;
+         t += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(t % g.n[0]);
+        int j = (int)((t / g.n[0]) % g.n[1]);
+        int k = (int)(t / ((long long)g.n[0] * g.n[1]));
+        if (g.dim > 0) i = map_index(i, g.n[0], g.bc_lo[0], g.bc_hi[0]);
+        if (g.dim > 1) j = map_index(j, g.n[1], g.bc_lo[1], g.bc_hi[1]);
+        if (g.dim > 2) k = map_index(k, g.n[2], g.bc_lo[2], g.bc_hi[2]);
+        const long long node = ((long long)k * g.n[1] + j) * g.n[0] + i;
+        for (int v = 0; v < 5; ++v) acc[v] += q[v * g.vs + node];
+    }
+    for (int v = 0; v < 5; ++v) {
+        double x = acc[v];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if ((threadIdx.x & 31) == 0) atomicAdd(out + v, x * vol);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Launchers
+// ---------------------------------------------------------------------------
+
+template <int SCHEME, int FLUX, typename T>
+static cudaError_t launch_axis(int axis, const GridView& g, const StageView& sv, cudaStream_t st) {
+    if (axis == 0) {
+        const int cnt_rows = (g.hi[1] - g.lo[1]) * (g.hi[2] - g.lo[2]);
+        dim3 block(32, 4);
+        dim3 grid((g.hi[0] - g.lo[0] + 30) / 31, (cnt_rows + 3) / 4, 1);
+        sweep_x<SCHEME, FLUX, T><<<grid, block, 0, st>>>(g, sv);
+    } else {
+        const int other = axis == 1 ? 2 : 1;
+        const int segs = (g.hi[axis] - g.lo[axis] + SEGLEN - 1) / SEGLEN;
+        dim3 block(32, 4);
+        dim3 grid((g.hi[0] - g.lo[0] + 31) / 32, (segs + 3) / 4, g.hi[other] - g.lo[other]);
+        if (axis == 1) sweep_yz<1, SCHEME, FLUX, T><<<grid, block, 0, st>>>(g, sv);
+        else sweep_yz<2, SCHEME, FLUX, T><<<grid, block, 0, st>>>(g, sv);
+    }
+    return cudaGetLastError();
+}
+
+template <typename T>
+static cudaError_t launch_axis_t(int scheme, int flux, int axis, const GridView& g, const StageView& sv,
+                                 cudaStream_t st) {
+    if (flux == RUSANOV) {
+        switch (scheme) {
+        case WENO5: return launch_axis<WENO5, RUSANOV, T>(axis, g, sv, st);
+        case TENO5: return launch_axis<TENO5, RUSANOV, T>(axis, g, sv, st);
+        case WENO3: return launch_axis<WENO3, RUSANOV, T>(axis, g, sv, st);
+        case WENO7: return launch_axis<WENO7, RUSANOV, T>(axis, g, sv, st);
+        }
+    } else if (flux == ROE) {
+        switch (scheme) {
+        case WENO5: return launch_axis<WENO5, ROE, T>(axis, g, sv, st);
+        case TENO5: return launch_axis<TENO5, ROE, T>(axis, g, sv, st);
+        case WENO3: return launch_axis<WENO3, ROE, T>(axis, g, sv, st);
+        case WENO7: return launch_axis<WENO7, ROE, T>(axis, g, sv, st);
+        }
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_sweep(int scheme, int flux, int prec64, int axis, const GridView& g, const StageView& sv,
+                         cudaStream_t st) {
+    return prec64 ? launch_axis_t<double>(scheme, flux, axis, g, sv, st)
+                  : launch_axis_t<float>(scheme, flux, axis, g, sv, st);
+}
+
+static int grid_for(long long work, int block) {
+    long long b = (work + block - 1) / block;
+    if (b > 148LL * 16) b = 148LL * 16;
+    return (int)(b < 1 ? 1 : b);
+}
+
+cudaError_t launch_dt(const GridView& g, const double* q, Clock* clock, unsigned* flags, int require_active,
+                      cudaStream_t st) {
+    const long long total = (long long)(g.hi[0] - g.lo[0]) * (g.hi[1] - g.lo[1]) * (g.hi[2] - g.lo[2]);
+    dt_kernel<<<grid_for(total, 256), 256, 0, st>>>(g, q, clock, flags, require_active);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_finalize_dt(Clock* c, cudaStream_t st) {
+    finalize_dt_kernel<<<1, 1, 0, st>>>(c);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_commit(Clock* c, double* dt_log, long long dt_cap, cudaStream_t st) {
+    commit_kernel<<<1, 1, 0, st>>>(c, dt_log, dt_cap);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_set_dt(Clock* c, double dt, cudaStream_t st) {
+    set_dt_kernel<<<1, 1, 0, st>>>(c, dt);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reset_min(Clock* c, cudaStream_t st) {
+    reset_min_kernel<<<1, 1, 0, st>>>(c);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stage_from_residual(const GridView& g, const StageView& sv, cudaStream_t st) {
+    const long long total = (long long)(g.hi[0] - g.lo[0]) * (g.hi[1] - g.lo[1]) * (g.hi[2] - g.lo[2]);
+    stage_from_residual_kernel<<<grid_for(total, 256), 256, 0, st>>>(g, sv);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_aos_to_soa(const double* aos, double* soa, long long nodes, long long vs, cudaStream_t st) {
+    aos_to_soa_kernel<<<grid_for(nodes * 5, 256), 256, 0, st>>>(aos, soa, nodes, vs);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_soa_to_aos(const GridView& g, const double* soa, double* aos, cudaStream_t st) {
+    const long long nodes = (long long)g.n[0] * g.n[1] * g.n[2];
+    soa_to_aos_kernel<<<grid_for(nodes * 5, 256), 256, 0, st>>>(g, soa, aos);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_totals(const GridView& g, const double* q, double* out, double vol, cudaStream_t st) {
+    const long long nodes = (long long)g.n[0] * g.n[1] * g.n[2];
+    totals_kernel<<<grid_for(nodes, 256), 256, 0, st>>>(g, q, out, vol);
+    return cudaGetLastError();
+}
+
+}  // namespace sfg

@@ -1,0 +1,443 @@
+// sfg_math.cuh -- device arithmetic of the explicit Euler path.
+//
+// The reference evaluates every face with dense 5x5 eigenvector matrices built
+// for an arbitrary unit normal (src/methods/numerics/convection/SF_riemann.cpp:69-123)
+// and 7 divisions per scalar WENO5 core (SF_WENO5.cpp:42-62).  On a Cartesian
+// grid the face normal is an axis unit vector, so the tangent basis the
+// reference builds is a fixed signed permutation of (x, y, z):
+//   normal e_x: l = (-0, 1, 0), m = (0, 0, 1)
+//   normal e_y: l = (-1, 0, 0), m = (0, 0, 1)
+//   normal e_z: l = (-1, 0, 0), m = (0, -1, 0)
+// and L, R collapse to a handful of scalar coefficients.  The functions below
+// are the same mathematics with that sparsity folded in; results agree with
+// the reference to rounding (the parity tests bound the difference).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "sfg_internal.h"
+
+namespace sfg {
+
+template <int SCHEME> struct SchemeInfo;
+template <> struct SchemeInfo<WENO3> { static constexpr int NST = 4, W = 4; };
+template <> struct SchemeInfo<WENO5> { static constexpr int NST = 6, W = 5; };
+template <> struct SchemeInfo<TENO5> { static constexpr int NST = 6, W = 5; };
+template <> struct SchemeInfo<WENO7> { static constexpr int NST = 8, W = 7; };
+
+// Momentum slots (1 + x/y/z) of the normal n and tangents l, m per axis, with
+// the sign of the tangent along that slot.
+template <int AX> struct AxisBasis;
+template <> struct AxisBasis<0> { static constexpr int N = 1, L = 2, M = 3; static constexpr int SL = 1, SM = 1; };
+template <> struct AxisBasis<1> { static constexpr int N = 2, L = 1, M = 3; static constexpr int SL = -1, SM = 1; };
+template <> struct AxisBasis<2> { static constexpr int N = 3, L = 1, M = 2; static constexpr int SL = -1, SM = -1; };
+
+template <typename T> __device__ __forceinline__ T rcp(T x);
+template <> __device__ __forceinline__ double rcp<double>(double x) { return 1.0 / x; }
+template <> __device__ __forceinline__ float rcp<float>(float x) { return __frcp_rn(x); }
+
+template <typename T> __device__ __forceinline__ T div_(T a, T b);
+template <> __device__ __forceinline__ double div_<double>(double a, double b) { return a / b; }
+template <> __device__ __forceinline__ float div_<float>(float a, float b) { return __fdividef(a, b); }
+
+template <typename T> __device__ __forceinline__ T rsqrt_(T x);
+template <> __device__ __forceinline__ double rsqrt_<double>(double x) { return rsqrt(x); }
+template <> __device__ __forceinline__ float rsqrt_<float>(float x) { return rsqrtf(x); }
+
+template <typename T> __device__ __forceinline__ T sqrt_(T x);
+template <> __device__ __forceinline__ double sqrt_<double>(double x) { return sqrt(x); }
+template <> __device__ __forceinline__ float sqrt_<float>(float x) { return sqrtf(x); }
+
+template <typename T> __device__ __forceinline__ bool finite_(T x) { return isfinite(x); }
+
+// ---------------------------------------------------------------------------
+// Eigen-structure of the Euler flux Jacobian at the face-average state
+// (buildCharacteristicMatrix, SF_riemann.cpp:69-123) in compact form:
+//   A = u.m - E - h rho          B = u_n rho - m_n
+//   w0 = rho + b1 A   w1 = m_l - u_l rho   w2 = m_m - u_m rho
+//   w3 =  x1 B - b2 A              w4 = -x1 B - b2 A
+// with h = |u|^2 / 2, b1 = (gamma - 1) / c^2, b2 = b1 / 2, x1 = 1 / (2c), and
+// back-projection q = R w:
+//   S = w0 + w3 + w4, D = w4 - w3
+//   rho = S, m = u S + l w1 + m w2 + c n D, E = h w0 + u_l w1 + u_m w2 + H (w3 + w4) + c u_n D.
+// ---------------------------------------------------------------------------
+template <typename T> struct Eigen {
+    T u, v, w;          // velocity
+    T un, ul, um;       // velocity along n, l, m
+    T h, H, c, b1, b2, x1;
+};
+
+template <int AX, typename T>
+__device__ __forceinline__ bool eigen_at(const T q[5], T gamma, Eigen<T>& e) {
+    using B = AxisBasis<AX>;
+    const T rho = q[0];
+    const T inv = rcp<T>(rho);
+    e.u = q[1] * inv;
+    e.v = q[2] * inv;
+    e.w = q[3] * inv;
+    const T ke = T(0.5) * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]) * inv;
+    const T p = (gamma - T(1)) * (q[4] - ke);
+    const T vel[3] = {e.u, e.v, e.w};
+    e.un = vel[B::N - 1];
+    e.ul = T(B::SL) * vel[B::L - 1];
+    e.um = T(B::SM) * vel[B::M - 1];
+    e.h = T(0.5) * (e.u * e.u + e.v * e.v + e.w * e.w);
+    e.H = (q[4] + p) * inv;
+    const T c2 = gamma * p * inv;
+    const T ic = rsqrt_<T>(c2);
+    e.c = c2 * ic;
+    e.b1 = (gamma - T(1)) * (ic * ic);
+    e.b2 = T(0.5) * e.b1;
+    e.x1 = T(0.5) * ic;
+    return rho > T(0) && p > T(0);
+}
+
+template <int AX, typename T>
+__device__ __forceinline__ void to_characteristic(const Eigen<T>& e, const T q[5], T w[5]) {
+    using B = AxisBasis<AX>;
+    const T mn = q[B::N], ml = T(B::SL) * q[B::L], mm = T(B::SM) * q[B::M];
+    const T A = e.u * q[1] + e.v * q[2] + e.w * q[3] - q[4] - e.h * q[0];
+    const T Bv = e.un * q[0] - mn;
+    const T y = e.b2 * A;
+    w[0] = q[0] + e.b1 * A;
+    w[1] = ml - e.ul * q[0];
+    w[2] = mm - e.um * q[0];
+    w[3] = e.x1 * Bv - y;
+    w[4] = -e.x1 * Bv - y;
+}
+
+template <int AX, typename T>
+__device__ __forceinline__ void from_characteristic(const Eigen<T>& e, const T w[5], T q[5]) {
+    using B = AxisBasis<AX>;
+    const T S = w[0] + w[3] + w[4];
+    const T D = w[4] - w[3];
+    const T cD = e.c * D;
+    q[0] = S;
+    q[1] = e.u * S;
+    q[2] = e.v * S;
+    q[3] = e.w * S;
+    q[B::N] += cD;
+    q[B::L] += T(B::SL) * w[1];
+    q[B::M] += T(B::SM) * w[2];
+    q[4] = e.h * w[0] + e.ul * w[1] + e.um * w[2] + e.H * (w[3] + w[4]) + e.un * cD;
+}
+
+// ---------------------------------------------------------------------------
+// Scalar reconstruction cores.  v[0..W-1] is the upwind-ordered stencil.
+// ---------------------------------------------------------------------------
+
+// WENO5-JS (SF_WENO5.cpp:42-62): weights d_k/(eps+b_k)^2 normalised.  The
+// three alpha divisions and the normalisation are folded into one division:
+// with s_k = (eps+b_k)^2, w_k = d_k * prod_{j!=k} s_j, result = sum w_k p_k / sum w_k.
+template <typename T>
+__device__ __forceinline__ T weno5_core(const T* v, unsigned& flags) {
+    const T p0 = T(2) * v[0] - T(7) * v[1] + T(11) * v[2];
+    const T p1 = -v[1] + T(5) * v[2] + T(2) * v[3];
+    const T p2 = T(2) * v[2] + T(5) * v[3] - v[4];
+    const T t0 = v[0] - T(2) * v[1] + v[2], r0 = v[0] - T(4) * v[1] + T(3) * v[2];
+    const T t1 = v[1] - T(2) * v[2] + v[3], r1 = v[1] - v[3];
+    const T t2 = v[2] - T(2) * v[3] + v[4], r2 = T(3) * v[2] - T(4) * v[3] + v[4];
+    const T c13 = T(13.0 / 12.0);
+    const T b0 = c13 * (t0 * t0) + T(0.25) * (r0 * r0);
+    const T b1 = c13 * (t1 * t1) + T(0.25) * (r1 * r1);
+    const T b2 = c13 * (t2 * t2) + T(0.25) * (r2 * r2);
+    const T eps = T(1e-6);
+    const T s0 = (eps + b0) * (eps + b0);
+    const T s1 = (eps + b1) * (eps + b1);
+    const T s2 = (eps + b2) * (eps + b2);
+    const T w0 = T(0.1) * (s1 * s2);
+    const T w1 = T(0.6) * (s0 * s2);
+    const T w2 = T(0.3) * (s0 * s1);
+    const T den = w0 + w1 + w2;
+    if (!(den > T(0)) || !finite_(den)) flags |= FLAG_NONFINITE;
+    return div_<T>(w0 * p0 + w1 * p1 + w2 * p2, T(6) * den);
+}
+
+// WENO3-JS (SF_WENO3.cpp:42-57), same folding.
+template <typename T>
+__device__ __forceinline__ T weno3_core(const T* v, unsigned& flags) {
+    const T p0 = -v[0] + T(5) * v[1] + T(2) * v[2];
+    const T p1 = T(2) * v[1] + T(5) * v[2] - v[3];
+    const T b0 = (v[2] - v[0]) * (v[2] - v[0]);
+    const T b1 = (v[3] - v[1]) * (v[3] - v[1]);
+    const T eps = T(1e-6);
+    const T s0 = (eps + b0) * (eps + b0);
+    const T s1 = (eps + b1) * (eps + b1);
+    const T w0 = T(1.0 / 3.0) * s1;
+    const T w1 = T(2.0 / 3.0) * s0;
+    const T den = w0 + w1;
+    if (!(den > T(0)) || !finite_(den)) flags |= FLAG_NONFINITE;
+    return div_<T>(w0 * p0 + w1 * p1, T(6) * den);
+}
+
+// Smoothness indicator of a 4-point sub-stencil of WENO7 (SF_WENO7.cpp:41-69):
+// the integral over [a, b] of the squared derivatives of the interpolating
+// cubic, with the integrals of x^k precomputed per sub-stencil.
+template <typename T>
+__device__ __forceinline__ T beta4(T v0, T v1, T v2, T v3, T i1, T i2, T i3, T i4, T i5) {
+    const T d1 = v1 - v0;
+    const T d2 = (v2 - T(2) * v1 + v0) * T(0.5);
+    const T d3 = (v3 - T(3) * v2 + T(3) * v1 - v0) * T(1.0 / 6.0);
+    const T A = d1 - d2 + T(2) * d3;
+    const T Bc = T(2) * d2 - T(6) * d3;
+    const T C = T(3) * d3;
+    const T beta1 = A * A * i1 + A * Bc * i2 + (Bc * Bc + T(2) * A * C) * i3 + Bc * C * i4 + C * C * i5;
+    const T E = T(6) * d3;
+    const T beta2 = Bc * Bc * i1 + Bc * E * i2 + E * E * i3;
+    const T beta3 = T(36) * d3 * d3 * i1;
+    return beta1 + beta2 + beta3;
+}
+
+// WENO7-JS (SF_WENO7.cpp:71-98).
+template <typename T>
+__device__ __forceinline__ T weno7_core(const T* v, unsigned& flags) {
+    const T p0 = -T(3) * v[0] + T(13) * v[1] - T(23) * v[2] + T(25) * v[3];
+    const T p1 = v[1] - T(5) * v[2] + T(13) * v[3] + T(3) * v[4];
+    const T p2 = -v[2] + T(7) * v[3] + T(7) * v[4] - v[5];
+    const T p3 = T(3) * v[3] + T(13) * v[4] - T(5) * v[5] + v[6];
+    // integrals over [a,b] of 1, x, x^2/3... as used by beta4: b-a, b^2-a^2,
+    // (b^3-a^3)/3, (b^4-a^4)/2, (b^5-a^5)/5 for [2.5,3.5], [1.5,2.5], [0.5,1.5], [-0.5,0.5]
+    const T b0 = beta4<T>(v[0], v[1], v[2], v[3], T(1), T(6), T(109.0 / 12.0 * 1.0), T(3.5 * 3.5 * 3.5 * 3.5 / 2.0 - 2.5 * 2.5 * 2.5 * 2.5 / 2.0),
+                          T((3.5 * 3.5 * 3.5 * 3.5 * 3.5 - 2.5 * 2.5 * 2.5 * 2.5 * 2.5) / 5.0));
+    const T b1 = beta4<T>(v[1], v[2], v[3], v[4], T(1), T(4), T(49.0 / 12.0), T(2.5 * 2.5 * 2.5 * 2.5 / 2.0 - 1.5 * 1.5 * 1.5 * 1.5 / 2.0),
+                          T((2.5 * 2.5 * 2.5 * 2.5 * 2.5 - 1.5 * 1.5 * 1.5 * 1.5 * 1.5) / 5.0));
+    const T b2 = beta4<T>(v[2], v[3], v[4], v[5], T(1), T(2), T(13.0 / 12.0), T(1.5 * 1.5 * 1.5 * 1.5 / 2.0 - 0.5 * 0.5 * 0.5 * 0.5 / 2.0),
+                          T((1.5 * 1.5 * 1.5 * 1.5 * 1.5 - 0.5 * 0.5 * 0.5 * 0.5 * 0.5) / 5.0));
+    const T b3 = beta4<T>(v[3], v[4], v[5], v[6], T(1), T(0), T(1.0 / 12.0), T(0),
+                          T((0.5 * 0.5 * 0.5 * 0.5 * 0.5 + 0.5 * 0.5 * 0.5 * 0.5 * 0.5) / 5.0));
+    const T eps = T(1e-6);
+    const T a0 = div_<T>(T(1.0 / 35.0), (eps + b0) * (eps + b0));
+    const T a1 = div_<T>(T(12.0 / 35.0), (eps + b1) * (eps + b1));
+    const T a2 = div_<T>(T(18.0 / 35.0), (eps + b2) * (eps + b2));
+    const T a3 = div_<T>(T(4.0 / 35.0), (eps + b3) * (eps + b3));
+    const T sum = a0 + a1 + a2 + a3;
+    if (!(sum > T(0)) || !finite_(sum)) flags |= FLAG_NONFINITE;
+    return div_<T>(a0 * p0 + a1 * p1 + a2 * p2 + a3 * p3, T(12) * sum);
+}
+
+// TENO5 (SF_TENO5.cpp:44-92): C = 1, q = 6, eps = 1e-40, CT = 1e-5.
+// FP64 keeps the reference's gamma_k = (1 + tau5/(b_k+eps))^6 and tests
+// gamma_k < CT * sum(gamma) (the reference divides; the comparison is the same
+// up to rounding at the threshold).  `cut` accumulates the number of cut
+// sub-stencils.
+template <typename T> struct Teno;
+
+template <> struct Teno<double> {
+    static __device__ __forceinline__ double core(const double* v, unsigned& flags, unsigned& cut) {
+        const double p0 = 2.0 * v[0] - 7.0 * v[1] + 11.0 * v[2];
+        const double p1 = -v[1] + 5.0 * v[2] + 2.0 * v[3];
+        const double p2 = 2.0 * v[2] + 5.0 * v[3] - v[4];
+        const double t0 = v[0] - 2.0 * v[1] + v[2], r0 = v[0] - 4.0 * v[1] + 3.0 * v[2];
+        const double t1 = v[1] - 2.0 * v[2] + v[3], r1 = v[1] - v[3];
+        const double t2 = v[2] - 2.0 * v[3] + v[4], r2 = 3.0 * v[2] - 4.0 * v[3] + v[4];
+        const double c13 = 13.0 / 12.0;
+        const double b0 = c13 * (t0 * t0) + 0.25 * (r0 * r0);
+        const double b1 = c13 * (t1 * t1) + 0.25 * (r1 * r1);
+        const double b2 = c13 * (t2 * t2) + 0.25 * (r2 * r2);
+        const double tau = fabs(b0 - b2);
+        const double g0 = 1.0 + tau / (b0 + 1e-40);
+        const double g1 = 1.0 + tau / (b1 + 1e-40);
+        const double g2 = 1.0 + tau / (b2 + 1e-40);
+        const double q0 = g0 * g0 * g0, q1 = g1 * g1 * g1, q2 = g2 * g2 * g2;
+        const double G0 = q0 * q0, G1 = q1 * q1, G2 = q2 * q2;
+        const double lim = 1e-5 * (G0 + G1 + G2);
+        if (!finite_(lim)) flags |= FLAG_NONFINITE;
+        const bool k0 = !(G0 < lim), k1 = !(G1 < lim), k2 = !(G2 < lim);
+        cut += (!k0) + (!k1) + (!k2);
+        const double d0 = k0 ? 0.1 : 0.0, d1 = k1 ? 0.6 : 0.0, d2 = k2 ? 0.3 : 0.0;
+        const double act = d0 + d1 + d2;
+        if (!(act > 0.0)) { flags |= FLAG_TENO_CUTOFF; return 0.0; }
+        return (d0 * p0 + d1 * p1 + d2 * p2) / (6.0 * act);
+    }
+};
+
+// FP32: gamma_k^6 overflows single precision, so the cut-off test is made on
+// ratios to the largest gamma (smallest b+eps), which are in (0, 1]:
+//   g_k / g_m = (e_k + tau) e_m / (e_k (e_m + tau)),  e = b + eps.
+template <> struct Teno<float> {
+    static __device__ __forceinline__ float core(const float* v, unsigned& flags, unsigned& cut) {
+        const float p0 = 2.f * v[0] - 7.f * v[1] + 11.f * v[2];
+        const float p1 = -v[1] + 5.f * v[2] + 2.f * v[3];
+        const float p2 = 2.f * v[2] + 5.f * v[3] - v[4];
+        const float t0 = v[0] - 2.f * v[1] + v[2], r0 = v[0] - 4.f * v[1] + 3.f * v[2];
+        const float t1 = v[1] - 2.f * v[2] + v[3], r1 = v[1] - v[3];
+        const float t2 = v[2] - 2.f * v[3] + v[4], r2 = 3.f * v[2] - 4.f * v[3] + v[4];
+        const float c13 = 13.f / 12.f;
+        const float b0 = c13 * (t0 * t0) + 0.25f * (r0 * r0);
+        const float b1 = c13 * (t1 * t1) + 0.25f * (r1 * r1);
+        const float b2 = c13 * (t2 * t2) + 0.25f * (r2 * r2);
+        const float tau = fabsf(b0 - b2);
+        const float e0 = b0 + 1e-40f, e1 = b1 + 1e-40f, e2 = b2 + 1e-40f;
+        const float em = fminf(e0, fminf(e1, e2));
+        const float den = em + tau;
+        // ratio r_k = g_k / g_max; the minimum-e sub-stencil has r = 1
+        auto ratio = [&](float ek) -> float {
+            if (ek == em) return 1.f;
+            return __fdividef((ek + tau) * em, ek * den);
+        };
+        const float x0 = ratio(e0), x1 = ratio(e1), x2 = ratio(e2);
+        const float y0 = x0 * x0 * x0, y1 = x1 * x1 * x1, y2 = x2 * x2 * x2;
+        const float G0 = y0 * y0, G1 = y1 * y1, G2 = y2 * y2;
+        const float lim = 1e-5f * (G0 + G1 + G2);
+        if (!finite_(lim)) flags |= FLAG_NONFINITE;
+        const bool k0 = !(G0 < lim), k1 = !(G1 < lim), k2 = !(G2 < lim);
+        cut += (!k0) + (!k1) + (!k2);
+        const float d0 = k0 ? 0.1f : 0.f, d1 = k1 ? 0.6f : 0.f, d2 = k2 ? 0.3f : 0.f;
+        const float act = d0 + d1 + d2;
+        if (!(act > 0.f)) { flags |= FLAG_TENO_CUTOFF; return 0.f; }
+        return __fdividef(d0 * p0 + d1 * p1 + d2 * p2, 6.f * act);
+    }
+};
+
+template <int SCHEME, typename T>
+__device__ __forceinline__ T recon_core(const T* v, unsigned& flags, unsigned& cut) {
+    if constexpr (SCHEME == WENO5) return weno5_core<T>(v, flags);
+    else if constexpr (SCHEME == TENO5) return Teno<T>::core(v, flags, cut);
+    else if constexpr (SCHEME == WENO3) return weno3_core<T>(v, flags);
+    else return weno7_core<T>(v, flags);
+}
+
+// ---------------------------------------------------------------------------
+// Face fluxes (per unit area, unit normal = axis AX).
+// ---------------------------------------------------------------------------
+
+// Rusanov with both sides closed by the perfect-gas EOS
+// (RusanovEOS::faceFlux, SF_rusanovEOS.cpp:47-77; close() of
+// SF_singleFluidStateModel.cpp:49-73).
+template <int AX, typename T>
+__device__ __forceinline__ void rusanov(const T qL[5], const T qR[5], T gamma, T F[5], unsigned& flags) {
+    constexpr int N = AxisBasis<AX>::N;
+    const T iL = rcp<T>(qL[0]), iR = rcp<T>(qR[0]);
+    const T uL[3] = {qL[1] * iL, qL[2] * iL, qL[3] * iL};
+    const T uR[3] = {qR[1] * iR, qR[2] * iR, qR[3] * iR};
+    const T kL = T(0.5) * qL[0] * (uL[0] * uL[0] + uL[1] * uL[1] + uL[2] * uL[2]);
+    const T kR = T(0.5) * qR[0] * (uR[0] * uR[0] + uR[1] * uR[1] + uR[2] * uR[2]);
+    const T pL = (gamma - T(1)) * (qL[4] - kL);
+    const T pR = (gamma - T(1)) * (qR[4] - kR);
+    if (!(qL[0] > T(0)) || !(qR[0] > T(0))) flags |= FLAG_DENSITY;
+    if (!(pL > T(0)) || !(pR > T(0))) flags |= FLAG_PRESSURE;
+    const T cL = sqrt_<T>(gamma * pL * iL), cR = sqrt_<T>(gamma * pR * iR);
+    const T unL = uL[N - 1], unR = uR[N - 1];
+    const T lam = fmax(fabs(unL) + cL, fabs(unR) + cR);
+    const T hl = T(0.5) * lam;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+        T fl = qL[v] * unL, fr = qR[v] * unR;
+        if (v == N) { fl += pL; fr += pR; }
+        if (v == 4) { fl += pL * unL; fr += pR * unR; }
+        F[v] = T(0.5) * (fl + fr) - hl * (qR[v] - qL[v]);
+    }
+}
+
+// Roe with the Harten entropy fix (RoeFlux::flux, SF_roe.cpp:20-111).
+template <int AX, typename T>
+__device__ __forceinline__ void roe(const T qL[5], const T qR[5], T gamma, T F[5], unsigned& flags) {
+    constexpr int N = AxisBasis<AX>::N;
+    const T gm1 = gamma - T(1);
+    const T iL = rcp<T>(qL[0]), iR = rcp<T>(qR[0]);
+    const T keL = T(0.5) * (qL[1] * qL[1] + qL[2] * qL[2] + qL[3] * qL[3]) * iL;
+    const T keR = T(0.5) * (qR[1] * qR[1] + qR[2] * qR[2] + qR[3] * qR[3]) * iR;
+    const T pL = gm1 * (qL[4] - keL), pR = gm1 * (qR[4] - keR);
+    if (!(qL[0] > T(0)) || !(qR[0] > T(0))) flags |= FLAG_DENSITY;
+    if (!(pL > T(0)) || !(pR > T(0))) flags |= FLAG_PRESSURE;
+    const T uL[3] = {qL[1] * iL, qL[2] * iL, qL[3] * iL};
+    const T uR[3] = {qR[1] * iR, qR[2] * iR, qR[3] * iR};
+    const T hL = (qL[4] + pL) * iL, hR = (qR[4] + pR) * iR;
+    const T sL = sqrt_<T>(qL[0]), sR = sqrt_<T>(qR[0]);
+    const T iS = rcp<T>(sL + sR);
+    const T ur = (sL * uL[0] + sR * uR[0]) * iS;
+    const T vr = (sL * uL[1] + sR * uR[1]) * iS;
+    const T wr = (sL * uL[2] + sR * uR[2]) * iS;
+    const T hr = (sL * hL + sR * hR) * iS;
+    const T q2 = ur * ur + vr * vr + wr * wr;
+    const T a2 = gm1 * (hr - T(0.5) * q2);
+    if (!(a2 > T(0)) || !finite_(a2)) flags |= FLAG_ROE_SOUND;
+    const T rr = sL * sR;
+    T qr[5] = {rr, rr * ur, rr * vr, rr * wr, rr * (T(0.5) * q2 + div_<T>(a2, gm1))};
+    Eigen<T> e;
+    eigen_at<AX, T>(qr, gamma, e);
+    const T a = sqrt_<T>(a2);
+    const T un = (N == 1 ? ur : (N == 2 ? vr : wr));
+    const T lam[5] = {un, un, un, un + a, un - a};
+    const T delta = T(0.1) * a;
+    T dq[5], alpha[5], s[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) dq[v] = qR[v] - qL[v];
+    to_characteristic<AX, T>(e, dq, alpha);
+    // the reference's wave order is (u_n, u_n, u_n, u_n + a, u_n - a) against
+    // columns (w0, w1, w2, w3, w4) of R = (entropy, shear l, shear m, u-c, u+c)
+#pragma unroll
+    for (int m = 0; m < 5; ++m) {
+        const T val = fabs(lam[m]);
+        const T ab = val < T(2) * delta ? T(0.5) * (val * val * rcp<T>(T(2) * delta) + delta) : val;
+        s[m] = ab * alpha[m];
+    }
+    T diss[5];
+    from_characteristic<AX, T>(e, s, diss);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+        T fl = qL[v] * uL[N - 1], fr = qR[v] * uR[N - 1];
+        if (v == N) { fl += pL; fr += pR; }
+        if (v == 4) { fl += pL * uL[N - 1]; fr += pR * uR[N - 1]; }
+        F[v] = T(0.5) * (fl + fr - diss[v]);
+    }
+}
+
+// One characteristic face flux (characteristicWENOFaceFlux, SF_WENO.h:184-245)
+// from NST conservative points st[0..NST-1] (face between NST/2-1 and NST/2).
+// In FP32 the reconstruction runs on deviations from the face average q-bar
+// (computed in FP64): the projections are linear and the WENO/TENO cores are
+// invariant to adding a constant, so the result is the same mathematics while
+// single precision only has to resolve the variation across the stencil.
+template <int AX, int SCHEME, int FLUX, typename T>
+__device__ __forceinline__ void face_flux(const double (&st)[SchemeInfo<SCHEME>::NST][5], T gamma, T F[5],
+                                          unsigned& flags, unsigned& cut) {
+    constexpr int NST = SchemeInfo<SCHEME>::NST;
+    constexpr int W = SchemeInfo<SCHEME>::W;
+    constexpr int CL = NST / 2 - 1;
+    constexpr bool DEV = sizeof(T) < sizeof(double);
+    double qbar64[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) qbar64[v] = 0.5 * (st[CL][v] + st[CL + 1][v]);
+    T qbar[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) qbar[v] = T(qbar64[v]);
+    Eigen<T> e;
+    if (!eigen_at<AX, T>(qbar, gamma, e)) flags |= FLAG_PRESSURE;
+    T ch[NST][5];
+#pragma unroll
+    for (int s = 0; s < NST; ++s) {
+        T d[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) d[v] = DEV ? T(st[s][v] - qbar64[v]) : T(st[s][v]);
+        to_characteristic<AX, T>(e, d, ch[s]);
+    }
+    T wl[5], wr[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+        T sl[W], sr[W];
+#pragma unroll
+        for (int s = 0; s < W; ++s) {
+            sl[s] = ch[s][v];
+            sr[s] = ch[NST - 1 - s][v];
+        }
+        wl[v] = recon_core<SCHEME, T>(sl, flags, cut);
+        wr[v] = recon_core<SCHEME, T>(sr, flags, cut);
+    }
+    T dl[5], dr[5], ql[5], qr[5];
+    from_characteristic<AX, T>(e, wl, dl);
+    from_characteristic<AX, T>(e, wr, dr);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+        ql[v] = DEV ? T(qbar64[v] + double(dl[v])) : dl[v];
+        qr[v] = DEV ? T(qbar64[v] + double(dr[v])) : dr[v];
+    }
+    if constexpr (FLUX == RUSANOV) rusanov<AX, T>(ql, qr, gamma, F, flags);
+    else roe<AX, T>(ql, qr, gamma, F, flags);
+#pragma unroll
+    for (int v = 0; v < 5; ++v)
+        if (!finite_(F[v])) flags |= FLAG_NONFINITE;
+}
+
+}  // namespace sfg

@@ -1,0 +1,798 @@
+// sfg_runtime.cu -- host runtime behind the C ABI (include/sonicsolver_b200.h).
+//
+// A solver handle owns the device state of one grid, a stream, the
+// device-resident step clock and, for sfg_advance, a CUDA graph of a run of
+// steps.  This is the B200-native counterpart of what FlowOperations binds for
+// the flow.conservative provider (src/solver/algorithm/SF_flowOperations.cpp:466-522):
+// FlowStepPrepare (ghost fill -> index mapping in the kernels), FlowDtCompute
+// (dt_kernel + finalize), FlowStepBegin (q0 is the untouched step-start
+// buffer), ExplicitStageExecute (sweep launches), FlowStepCommit / TimeCommit
+// (commit_kernel).
+#include "../../include/sonicsolver_b200.h"
+#include "sfg_internal.h"
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+
+namespace sfg {
+cudaError_t launch_sweep(int scheme, int flux, int prec64, int axis, const GridView& g, const StageView& sv,
+                         cudaStream_t st);
+cudaError_t launch_dt(const GridView& g, const double* q, Clock* clock, unsigned* flags, int require_active,
+                      cudaStream_t st);
+cudaError_t launch_finalize_dt(Clock* c, cudaStream_t st);
+cudaError_t launch_commit(Clock* c, double* dt_log, long long dt_cap, cudaStream_t st);
+cudaError_t launch_set_dt(Clock* c, double dt, cudaStream_t st);
+cudaError_t launch_reset_min(Clock* c, cudaStream_t st);
+cudaError_t launch_stage_from_residual(const GridView& g, const StageView& sv, cudaStream_t st);
+cudaError_t launch_aos_to_soa(const double* aos, double* soa, long long nodes, long long vs, cudaStream_t st);
+cudaError_t launch_soa_to_aos(const GridView& g, const double* soa, double* aos, cudaStream_t st);
+cudaError_t launch_totals(const GridView& g, const double* q, double* out, double vol, cudaStream_t st);
+}  // namespace sfg
+
+using namespace sfg;
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_error = buf;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                          \
+    do {                                                                                        \
+        cudaError_t e_ = (expr);                                                                \
+        if (e_ != cudaSuccess) return fail(SFG_ERR_CUDA, "%s: %s", #expr, cudaGetErrorString(e_)); \
+    } while (0)
+
+struct RecipeInfo {
+    int id;
+    const char* name;
+    int scheme;  // sfg::Scheme
+    int flux;    // sfg::Flux
+};
+
+// The convection recipes of FDM::TermRecipeId served here (names of
+// FDM::toString(TermRecipeId), SF_termRecipe.h:242-259).
+const RecipeInfo kRecipes[] = {
+    {SFG_RECIPE_WENO3_RUSANOV, "weno3Rusanov", WENO3, RUSANOV},
+    {SFG_RECIPE_WENO3_ROE, "weno3Roe", WENO3, ROE},
+    {SFG_RECIPE_WENO5_RUSANOV, "weno5Rusanov", WENO5, RUSANOV},
+    {SFG_RECIPE_WENO5_ROE, "weno5Roe", WENO5, ROE},
+    {SFG_RECIPE_TENO5_RUSANOV, "teno5Rusanov", TENO5, RUSANOV},
+    {SFG_RECIPE_TENO5_ROE, "teno5Roe", TENO5, ROE},
+    {SFG_RECIPE_WENO7_RUSANOV, "weno7Rusanov", WENO7, RUSANOV},
+    {SFG_RECIPE_WENO7_ROE, "weno7Roe", WENO7, ROE},
+};
+
+const RecipeInfo* find_recipe(int id) {
+    for (const auto& r : kRecipes)
+        if (r.id == id) return &r;
+    return nullptr;
+}
+
+int ghost_layers(int scheme) { return scheme == WENO3 ? 2 : (scheme == WENO7 ? 4 : 3); }
+int stage_count(int time_id) { return time_id == T_EULER ? 1 : (time_id == T_SSPRK3 ? 3 : 4); }
+
+}  // namespace
+
+struct sfg_solver_s {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    sfg_grid_desc grid{};
+    sfg_numerics_desc num{};
+    const RecipeInfo* recipe = nullptr;
+    int ng = 3;
+    GridView gv{};
+    long long nodes = 0;
+    double *qn = nullptr, *qa = nullptr, *qb = nullptr, *r = nullptr, *k = nullptr, *staging = nullptr;
+    double* totals = nullptr;
+    Clock* clock = nullptr;
+    unsigned* flags = nullptr;
+    unsigned long long* counters = nullptr;
+    bool counting = false;
+    int next_stage = 0;
+    double stage_dt = 0.0;
+    // graph of `graph_steps` steps for sfg_advance
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+    double* dt_log = nullptr;
+    long long dt_log_cap = 0;
+    Clock* host_clock = nullptr;  // pinned mirror
+};
+
+namespace {
+
+int validate(const sfg_grid_desc* g, const sfg_numerics_desc* n, const RecipeInfo** recipe) {
+    if (!g || !n) return fail(SFG_ERR_ARG, "null descriptor");
+    if (g->dim < 1 || g->dim > 3) return fail(SFG_ERR_ARG, "dim must be 1..3 (got %d)", g->dim);
+    const RecipeInfo* r = find_recipe(n->recipe);
+    if (!r) return fail(SFG_ERR_ARG, "convection recipe %d is not provided on the GPU", n->recipe);
+    if (n->time_recipe < 0 || n->time_recipe > 2) return fail(SFG_ERR_ARG, "unknown time recipe %d", n->time_recipe);
+    if (n->precision != SFG_PREC_FP64 && n->precision != SFG_PREC_FP32_FLUX)
+        return fail(SFG_ERR_ARG, "unknown precision mode %d", n->precision);
+    if (!(n->gamma > 1.0) || !std::isfinite(n->gamma)) return fail(SFG_ERR_ARG, "gamma must be > 1");
+    if (!(n->cfl > 0.0) || !std::isfinite(n->cfl)) return fail(SFG_ERR_ARG, "CFL must be finite and > 0");
+    const int reach = r->scheme == WENO3 ? 2 : (r->scheme == WENO7 ? 4 : 3);
+    for (int d = 0; d < 3; ++d) {
+        if (!(g->h[d] > 0.0) || !std::isfinite(g->h[d])) return fail(SFG_ERR_ARG, "h[%d] must be > 0", d);
+        if (d >= g->dim) {
+            if (g->n[d] != 1) return fail(SFG_ERR_ARG, "inactive axis %d must have 1 node", d);
+            continue;
+        }
+        const bool plo = g->bc_lo[d] == SFG_BC_PERIODIC, phi = g->bc_hi[d] == SFG_BC_PERIODIC;
+        if (plo != phi) return fail(SFG_ERR_ARG, "axis %d: periodic must be set on both ends", d);
+        for (int b : {g->bc_lo[d], g->bc_hi[d]})
+            if (b != SFG_BC_TRANSMISSIVE && b != SFG_BC_PERIODIC)
+                return fail(SFG_ERR_ARG, "axis %d: unknown boundary kind %d", d, b);
+        if (plo && g->n[d] < reach + 1) return fail(SFG_ERR_ARG, "periodic axis %d needs >= %d nodes", d, reach + 1);
+        if (!plo && g->n[d] < 3) return fail(SFG_ERR_ARG, "transmissive axis %d needs >= 3 nodes", d);
+    }
+    *recipe = r;
+    return SFG_OK;
+}
+
+void make_view(sfg_solver_s* s) {
+    GridView& g = s->gv;
+    const sfg_grid_desc& d = s->grid;
+    g.dim = d.dim;
+    for (int a = 0; a < 3; ++a) {
+        g.n[a] = d.n[a];
+        g.bc_lo[a] = a < d.dim ? d.bc_lo[a] : BC_TRANSMISSIVE;
+        g.bc_hi[a] = a < d.dim ? d.bc_hi[a] : BC_TRANSMISSIVE;
+        if (a < d.dim) {
+            g.lo[a] = d.bc_lo[a] == SFG_BC_TRANSMISSIVE ? 1 : 0;
+            g.hi[a] = d.bc_hi[a] == SFG_BC_TRANSMISSIVE ? d.n[a] - 1 : d.n[a];
+        } else {
+            g.lo[a] = 0;
+            g.hi[a] = 1;
+        }
+    }
+    // Uniform Cartesian metrics exactly as the reference mesh yields them for
+    // equal spacing (SF_mesh.cpp:283-339): J = dx dy dz, Jac = 1/J,
+    // xi_x = (dy dz) Jac; face cofactor (SF_canonicalFace.h:94-103) =
+    // 0.5 (xi_x/Jac + xi_x/Jac).
+    const double hx = d.h[0], hy = d.h[1], hz = d.h[2];
+    const double J = hx * hy * hz;
+    g.jac = 1.0 / J;
+    g.metric[0] = (hy * hz) * g.jac;
+    g.metric[1] = (hx * hz) * g.jac;
+    g.metric[2] = (hx * hy) * g.jac;
+    for (int a = 0; a < 3; ++a) g.area[a] = 0.5 * (g.metric[a] / g.jac + g.metric[a] / g.jac);
+    g.gamma = s->num.gamma;
+    g.cfl = s->num.cfl;
+    s->nodes = (long long)d.n[0] * d.n[1] * d.n[2];
+    g.vs = (s->nodes + 31) / 32 * 32;
+}
+
+StageView stage_view(sfg_solver_s* s, int stage, bool residual_only, bool require_active) {
+    StageView sv{};
+    sv.clock = s->clock;
+    sv.flags = s->flags;
+    sv.counters = s->counting ? s->counters : nullptr;
+    sv.time_id = s->num.time_recipe;
+    sv.stage = stage;
+    sv.q0 = s->qn;
+    sv.r = s->r;
+    sv.k = s->k;
+    sv.require_active = require_active ? 1 : 0;
+    if (residual_only) {
+        sv.qs = s->qn;
+        sv.qout = nullptr;
+        return sv;
+    }
+    switch (s->num.time_recipe) {
+    case T_EULER:
+        sv.qs = s->qn;
+        sv.qout = s->qa;
+        break;
+    case T_SSPRK3: {
+        static const double base[3] = {0.0, 0.75, 1.0 / 3.0};
+        static const double inc[3] = {1.0, 0.25, 2.0 / 3.0};
+        sv.base = base[stage];
+        sv.inc = inc[stage];
+        const double* in[3] = {s->qn, s->qa, s->qb};
+        double* out[3] = {s->qa, s->qb, s->qn};
+        sv.qs = in[stage];
+        sv.qout = out[stage];
+        break;
+    }
+    default: {
+        static const double inc[4] = {0.5, 0.5, 1.0, 0.0};
+        sv.inc = inc[stage];
+        const double* in[4] = {s->qn, s->qa, s->qb, s->qa};
+        double* out[4] = {s->qa, s->qb, s->qa, s->qn};
+        sv.qs = in[stage];
+        sv.qout = out[stage];
+        break;
+    }
+    }
+    return sv;
+}
+
+// All axis sweeps of one stage (or of the residual alone).
+int enqueue_stage(sfg_solver_s* s, int stage, bool residual_only, bool require_active) {
+    StageView sv = stage_view(s, stage, residual_only, require_active);
+    const int dim = s->grid.dim;
+    for (int axis = 0; axis < dim; ++axis) {
+        sv.mode = (axis > 0 ? MODE_READ_R : 0) | (axis == dim - 1 ? MODE_FINAL : 0) |
+                  (residual_only && axis == dim - 1 ? MODE_RESIDUAL : 0);
+        CUDA_TRY(launch_sweep(s->recipe->scheme, s->recipe->flux, s->num.precision == SFG_PREC_FP64, axis, s->gv,
+                              sv, s->stream));
+    }
+    return SFG_OK;
+}
+
+// Euler writes to qa; the committed state lives in qn.
+int enqueue_post_step(sfg_solver_s* s) {
+    if (s->num.time_recipe == T_EULER)
+        CUDA_TRY(cudaMemcpyAsync(s->qn, s->qa, sizeof(double) * 5 * s->gv.vs, cudaMemcpyDeviceToDevice, s->stream));
+    return SFG_OK;
+}
+
+// One full step with the CFL dt computed and clipped on device.
+int enqueue_cfl_step(sfg_solver_s* s, bool require_active) {
+    CUDA_TRY(launch_dt(s->gv, s->qn, s->clock, s->flags, 0, s->stream));
+    CUDA_TRY(launch_finalize_dt(s->clock, s->stream));
+    for (int st = 0; st < stage_count(s->num.time_recipe); ++st) {
+        int rc = enqueue_stage(s, st, false, require_active);
+        if (rc) return rc;
+    }
+    if (s->num.time_recipe == T_EULER) {
+        // guarded copy: only when the step ran (graph-safe: copy unconditionally
+        // is wrong once the run has stopped), so Euler keeps its own kernel path
+        int rc = enqueue_post_step(s);
+        if (rc) return rc;
+    }
+    CUDA_TRY(launch_commit(s->clock, s->dt_log, s->dt_log_cap, s->stream));
+    return SFG_OK;
+}
+
+int sync_and_check(sfg_solver_s* s) {
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    unsigned bits = 0;
+    CUDA_TRY(cudaMemcpy(&bits, s->flags, sizeof bits, cudaMemcpyDeviceToHost));
+    if (bits & FLAG_TENO_CUTOFF) return fail(SFG_ERR_TENO_CUTOFF, "TENO5 rejected all sub-stencils (flags 0x%x)", bits);
+    if (bits) return fail(SFG_ERR_STATE, "invalid state on device (flags 0x%x)", bits);
+    return SFG_OK;
+}
+
+int push_clock(sfg_solver_s* s) {
+    CUDA_TRY(cudaMemcpyAsync(s->clock, s->host_clock, sizeof(Clock), cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return SFG_OK;
+}
+
+int pull_clock(sfg_solver_s* s) {
+    CUDA_TRY(cudaMemcpyAsync(s->host_clock, s->clock, sizeof(Clock), cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return SFG_OK;
+}
+
+const double kInf = std::numeric_limits<double>::infinity();
+
+void reset_clock(Clock* c, double t) {
+    std::memset(c, 0, sizeof *c);
+    c->t = t;
+    c->t_end = kInf;
+    c->next_out = kInf;
+    c->write_interval = 0.0;
+    c->max_dt = kInf;
+    c->limit = kInf;
+    c->dt_bits = 0x7FEFFFFFFFFFFFFFull;
+    c->max_steps = std::numeric_limits<long long>::max();
+}
+
+// Host-layout helpers: reference Field storage (ng ghosts on every axis) <->
+// node block.  Ghost values follow the same laws the kernels read through.
+long long field_extent(const sfg_solver_s* s, int a) { return s->grid.n[a] + 2LL * s->ng; }
+
+int map_host(int i, int n, int bl, int bh) {
+    if (bl == SFG_BC_PERIODIC) {
+        while (i < 0) i += n;
+    } else if (i < 1) {
+        i = n > 1 ? 1 : 0;
+    }
+    if (bh == SFG_BC_PERIODIC) {
+        while (i >= n) i -= n;
+    } else if (i > n - 2) {
+        i = n > 1 ? n - 2 : 0;
+    }
+    return i;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* sfg_last_error(void) { return g_error.c_str(); }
+
+int sfg_version(int* major, int* minor) {
+    if (major) *major = 0;
+    if (minor) *minor = 1;
+    return SFG_OK;
+}
+
+const char* sfg_recipe_name(int recipe) {
+    const RecipeInfo* r = find_recipe(recipe);
+    return r ? r->name : nullptr;
+}
+
+int sfg_recipe_from_name(const char* name, int* recipe) {
+    if (!name || !recipe) return fail(SFG_ERR_ARG, "null argument");
+    for (const auto& r : kRecipes)
+        if (std::strcmp(r.name, name) == 0) {
+            *recipe = r.id;
+            return SFG_OK;
+        }
+    return fail(SFG_ERR_ARG, "convection recipe '%s' is not provided on the GPU", name);
+}
+
+int sfg_create(const sfg_grid_desc* grid, const sfg_numerics_desc* numerics, void* stream, sfg_solver* out) {
+    if (!out) return fail(SFG_ERR_ARG, "null output handle");
+    *out = nullptr;
+    const RecipeInfo* recipe = nullptr;
+    int rc = validate(grid, numerics, &recipe);
+    if (rc) return rc;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(SFG_ERR_CUDA, "no CUDA device: the B200 provider has no CPU fallback");
+    auto* s = new sfg_solver_s;
+    s->grid = *grid;
+    s->num = *numerics;
+    if (!(s->num.max_dt > 0.0)) s->num.max_dt = kInf;
+    s->recipe = recipe;
+    s->ng = ghost_layers(recipe->scheme);
+    make_view(s);
+    cudaGetDevice(&s->device);
+    auto cleanup = [&](int code) {
+        sfg_destroy(s);
+        return code;
+    };
+    if (stream) {
+        s->stream = (cudaStream_t)stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess)
+            return cleanup(fail(SFG_ERR_CUDA, "stream creation failed"));
+        s->own_stream = true;
+    }
+    const size_t state_bytes = sizeof(double) * 5 * (size_t)s->gv.vs;
+    double** bufs[] = {&s->qn, &s->qa, &s->qb, &s->r};
+    for (double** b : bufs)
+        if (cudaMalloc((void**)b, state_bytes) != cudaSuccess)
+            return cleanup(fail(SFG_ERR_NOMEM, "device allocation of %zu bytes failed", state_bytes));
+    if (s->num.time_recipe == T_RK4 && cudaMalloc((void**)&s->k, state_bytes) != cudaSuccess)
+        return cleanup(fail(SFG_ERR_NOMEM, "device allocation failed"));
+    if (cudaMalloc((void**)&s->staging, sizeof(double) * 5 * (size_t)s->nodes) != cudaSuccess ||
+        cudaMalloc((void**)&s->clock, sizeof(Clock)) != cudaSuccess ||
+        cudaMalloc((void**)&s->flags, 64) != cudaSuccess ||
+        cudaMalloc((void**)&s->counters, 64) != cudaSuccess ||
+        cudaMalloc((void**)&s->totals, 64) != cudaSuccess)
+        return cleanup(fail(SFG_ERR_NOMEM, "device allocation failed"));
+    if (cudaMallocHost((void**)&s->host_clock, sizeof(Clock)) != cudaSuccess)
+        return cleanup(fail(SFG_ERR_NOMEM, "pinned allocation failed"));
+    cudaMemsetAsync(s->flags, 0, 64, s->stream);
+    cudaMemsetAsync(s->counters, 0, 64, s->stream);
+    cudaMemsetAsync(s->qn, 0, state_bytes, s->stream);
+    cudaMemsetAsync(s->qa, 0, state_bytes, s->stream);
+    cudaMemsetAsync(s->qb, 0, state_bytes, s->stream);
+    cudaMemsetAsync(s->r, 0, state_bytes, s->stream);
+    reset_clock(s->host_clock, 0.0);
+    s->host_clock->max_dt = s->num.max_dt;
+    rc = push_clock(s);
+    if (rc) return cleanup(rc);
+    *out = s;
+    return SFG_OK;
+}
+
+int sfg_destroy(sfg_solver s) {
+    if (!s) return SFG_OK;
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    if (s->graph) cudaGraphExecDestroy(s->graph);
+    for (double* p : {s->qn, s->qa, s->qb, s->r, s->k, s->staging, s->totals, s->dt_log})
+        if (p) cudaFree(p);
+    if (s->clock) cudaFree(s->clock);
+    if (s->flags) cudaFree(s->flags);
+    if (s->counters) cudaFree(s->counters);
+    if (s->host_clock) cudaFreeHost(s->host_clock);
+    if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return SFG_OK;
+}
+
+int sfg_ghost_layers(sfg_solver s, int* ng) {
+    if (!s || !ng) return fail(SFG_ERR_ARG, "null argument");
+    *ng = s->ng;
+    return SFG_OK;
+}
+
+int sfg_state_size(sfg_solver s, int layout, size_t* count) {
+    if (!s || !count) return fail(SFG_ERR_ARG, "null argument");
+    if (layout == SFG_LAYOUT_NODES) *count = 5 * (size_t)s->nodes;
+    else if (layout == SFG_LAYOUT_FIELD)
+        *count = 5 * (size_t)(field_extent(s, 0) * field_extent(s, 1) * field_extent(s, 2));
+    else return fail(SFG_ERR_ARG, "unknown layout %d", layout);
+    return SFG_OK;
+}
+
+static int upload_nodes_host(sfg_solver s, const double* nodes_aos) {
+    CUDA_TRY(cudaMemcpyAsync(s->staging, nodes_aos, sizeof(double) * 5 * s->nodes, cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(launch_aos_to_soa(s->staging, s->qn, s->nodes, s->gv.vs, s->stream));
+    return SFG_OK;
+}
+
+static int reset_time(sfg_solver s, double time) {
+    reset_clock(s->host_clock, time);
+    s->host_clock->max_dt = s->num.max_dt;
+    s->next_stage = 0;
+    CUDA_TRY(cudaMemsetAsync(s->flags, 0, 64, s->stream));
+    return push_clock(s);
+}
+
+int sfg_upload(sfg_solver s, const double* host, int layout, double time) {
+    if (!s || !host) return fail(SFG_ERR_ARG, "null argument");
+    if (layout == SFG_LAYOUT_NODES) {
+        int rc = upload_nodes_host(s, host);
+        if (rc) return rc;
+    } else if (layout == SFG_LAYOUT_FIELD) {
+        std::vector<double> tmp(5 * (size_t)s->nodes);
+        const long long mx = field_extent(s, 0), my = field_extent(s, 1);
+        const int ng = s->ng;
+        for (int k = 0; k < s->grid.n[2]; ++k)
+            for (int j = 0; j < s->grid.n[1]; ++j)
+                for (int i = 0; i < s->grid.n[0]; ++i) {
+                    const long long src = (((long long)(k + ng) * my + (j + ng)) * mx + (i + ng)) * 5;
+                    const long long dst = (((long long)k * s->grid.n[1] + j) * s->grid.n[0] + i) * 5;
+                    std::memcpy(&tmp[dst], host + src, 5 * sizeof(double));
+                }
+        int rc = upload_nodes_host(s, tmp.data());
+        if (rc) return rc;
+        CUDA_TRY(cudaStreamSynchronize(s->stream));
+    } else {
+        return fail(SFG_ERR_ARG, "unknown layout %d", layout);
+    }
+    return reset_time(s, time);
+}
+
+int sfg_upload_device(sfg_solver s, const double* dev_nodes_aos, double time) {
+    if (!s || !dev_nodes_aos) return fail(SFG_ERR_ARG, "null argument");
+    CUDA_TRY(launch_aos_to_soa(dev_nodes_aos, s->qn, s->nodes, s->gv.vs, s->stream));
+    return reset_time(s, time);
+}
+
+int sfg_download_device(sfg_solver s, double* dev_nodes_aos) {
+    if (!s || !dev_nodes_aos) return fail(SFG_ERR_ARG, "null argument");
+    CUDA_TRY(launch_soa_to_aos(s->gv, s->qn, dev_nodes_aos, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return SFG_OK;
+}
+
+int sfg_download(sfg_solver s, double* host, int layout) {
+    if (!s || !host) return fail(SFG_ERR_ARG, "null argument");
+    CUDA_TRY(launch_soa_to_aos(s->gv, s->qn, s->staging, s->stream));
+    if (layout == SFG_LAYOUT_NODES) {
+        CUDA_TRY(cudaMemcpyAsync(host, s->staging, sizeof(double) * 5 * s->nodes, cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(cudaStreamSynchronize(s->stream));
+        return SFG_OK;
+    }
+    if (layout != SFG_LAYOUT_FIELD) return fail(SFG_ERR_ARG, "unknown layout %d", layout);
+    std::vector<double> tmp(5 * (size_t)s->nodes);
+    CUDA_TRY(cudaMemcpyAsync(tmp.data(), s->staging, sizeof(double) * 5 * s->nodes, cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    const long long mx = field_extent(s, 0), my = field_extent(s, 1), mz = field_extent(s, 2);
+    const int ng = s->ng;
+    for (long long k = 0; k < mz; ++k)
+        for (long long j = 0; j < my; ++j)
+            for (long long i = 0; i < mx; ++i) {
+                int c[3] = {(int)i - ng, (int)j - ng, (int)k - ng};
+                for (int a = 0; a < 3; ++a) {
+                    if (a < s->grid.dim) {
+                        c[a] = map_host(c[a], s->grid.n[a], s->grid.bc_lo[a], s->grid.bc_hi[a]);
+                    } else {
+                        c[a] = c[a] < 0 ? 0 : (c[a] >= s->grid.n[a] ? s->grid.n[a] - 1 : c[a]);
+                    }
+                }
+                const long long src = (((long long)c[2] * s->grid.n[1] + c[1]) * s->grid.n[0] + c[0]) * 5;
+                std::memcpy(host + ((k * my + j) * mx + i) * 5, &tmp[src], 5 * sizeof(double));
+            }
+    return SFG_OK;
+}
+
+int sfg_compute_dt(sfg_solver s, double limit, double* dt) {
+    if (!s || !dt) return fail(SFG_ERR_ARG, "null argument");
+    CUDA_TRY(launch_reset_min(s->clock, s->stream));
+    CUDA_TRY(launch_dt(s->gv, s->qn, s->clock, s->flags, 0, s->stream));
+    int rc = pull_clock(s);
+    if (rc) return rc;
+    double v;
+    unsigned long long bits = s->host_clock->dt_bits;
+    std::memcpy(&v, &bits, sizeof v);
+    if (s->num.max_dt < v) v = s->num.max_dt;
+    if (limit > 0.0 && limit < v) v = limit;
+    *dt = v;
+    return SFG_OK;
+}
+
+int sfg_stage(sfg_solver s, int stage, double dt) {
+    if (!s) return fail(SFG_ERR_ARG, "null solver");
+    const int ns = stage_count(s->num.time_recipe);
+    if (stage != s->next_stage || stage < 0 || stage >= ns)
+        return fail(SFG_ERR_ARG, "explicit stage %d out of order (expected %d)", stage, s->next_stage);
+    if (!(dt > 0.0) || !std::isfinite(dt)) return fail(SFG_ERR_ARG, "dt must be finite and > 0");
+    if (stage == 0) s->stage_dt = dt;
+    else if (dt != s->stage_dt) return fail(SFG_ERR_ARG, "dt changed inside a step");
+    CUDA_TRY(launch_set_dt(s->clock, dt, s->stream));
+    int rc = enqueue_stage(s, stage, false, false);
+    if (rc) return rc;
+    if (stage == ns - 1) {
+        rc = enqueue_post_step(s);
+        if (rc) return rc;
+        CUDA_TRY(launch_commit(s->clock, nullptr, 0, s->stream));
+        s->next_stage = 0;
+    } else {
+        s->next_stage = stage + 1;
+    }
+    return sync_and_check(s);
+}
+
+int sfg_step(sfg_solver s, double dt, double limit) {
+    if (!s) return fail(SFG_ERR_ARG, "null solver");
+    if (s->next_stage != 0) return fail(SFG_ERR_ARG, "a step is in progress (stage %d)", s->next_stage);
+    if (dt > 0.0) {
+        for (int st = 0; st < stage_count(s->num.time_recipe); ++st) {
+            s->next_stage = st;
+            int rc = sfg_stage(s, st, dt);
+            if (rc) {
+                s->next_stage = 0;
+                return rc;
+            }
+        }
+        return SFG_OK;
+    }
+    // CFL step on device; one-shot limit through the clock
+    s->host_clock->t_end = kInf;
+    s->host_clock->max_steps = std::numeric_limits<long long>::max();
+    int rc = pull_clock(s);
+    if (rc) return rc;
+    s->host_clock->t_end = kInf;
+    s->host_clock->max_steps = std::numeric_limits<long long>::max();
+    s->host_clock->limit = limit > 0.0 ? limit : kInf;
+    s->host_clock->write_interval = 0.0;
+    s->host_clock->next_out = kInf;
+    rc = push_clock(s);
+    if (rc) return rc;
+    rc = enqueue_cfl_step(s, false);
+    if (rc) return rc;
+    return sync_and_check(s);
+}
+
+int sfg_advance(sfg_solver s, double t_end, int64_t max_steps, double write_interval, int graph_steps,
+                double* dt_out, int64_t dt_capacity, sfg_stats* stats) {
+    if (!s) return fail(SFG_ERR_ARG, "null solver");
+    if (s->next_stage != 0) return fail(SFG_ERR_ARG, "a step is in progress");
+    if (!(t_end == t_end)) return fail(SFG_ERR_ARG, "t_end is NaN");
+    if (graph_steps <= 0) graph_steps = 32;
+    int rc = pull_clock(s);
+    if (rc) return rc;
+    Clock* hc = s->host_clock;
+    const long long steps0 = hc->steps;
+    hc->t_end = t_end;
+    hc->max_steps = max_steps > 0 ? steps0 + max_steps : std::numeric_limits<long long>::max();
+    hc->write_interval = write_interval > 0.0 ? write_interval : 0.0;
+    hc->next_out = write_interval > 0.0 ? hc->t + write_interval : kInf;
+    hc->limit = kInf;
+    hc->log_base = steps0;
+    hc->dt_bits = 0x7FEFFFFFFFFFFFFFull;
+    // dt log buffer
+    const long long want = dt_out && dt_capacity > 0 ? dt_capacity : 0;
+    if (want > s->dt_log_cap) {
+        if (s->dt_log) cudaFree(s->dt_log);
+        s->dt_log = nullptr;
+        s->dt_log_cap = 0;
+        if (s->graph) {
+            cudaGraphExecDestroy(s->graph);
+            s->graph = nullptr;
+        }
+        if (cudaMalloc((void**)&s->dt_log, sizeof(double) * want) != cudaSuccess)
+            return fail(SFG_ERR_NOMEM, "dt log allocation failed");
+        s->dt_log_cap = want;
+    }
+    rc = push_clock(s);
+    if (rc) return rc;
+    if (!s->graph || s->graph_steps != graph_steps) {
+        if (s->graph) cudaGraphExecDestroy(s->graph);
+        s->graph = nullptr;
+        cudaGraph_t g;
+        CUDA_TRY(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+        int crc = SFG_OK;
+        for (int i = 0; i < graph_steps && !crc; ++i) crc = enqueue_cfl_step(s, true);
+        cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+        if (crc) return crc;
+        if (e != cudaSuccess) return fail(SFG_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&s->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail(SFG_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+        s->graph_steps = graph_steps;
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, s->stream);
+    for (;;) {
+        CUDA_TRY(cudaGraphLaunch(s->graph, s->stream));
+        CUDA_TRY(cudaMemcpyAsync(hc, s->clock, sizeof(Clock), cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(cudaStreamSynchronize(s->stream));
+        unsigned bits = 0;
+        CUDA_TRY(cudaMemcpy(&bits, s->flags, sizeof bits, cudaMemcpyDeviceToHost));
+        if (bits) break;
+        if (!hc->active || hc->steps >= hc->max_steps) break;
+    }
+    cudaEventRecord(e1, s->stream);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    const long long done = hc->steps - steps0;
+    if (dt_out && want > 0) {
+        const long long n = done < want ? done : want;
+        if (n > 0) CUDA_TRY(cudaMemcpy(dt_out, s->dt_log, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    }
+    if (stats) {
+        stats->steps = done;
+        stats->time = hc->t;
+        stats->last_dt = hc->dt;
+        stats->device_ms = ms;
+        unsigned bits = 0;
+        cudaMemcpy(&bits, s->flags, sizeof bits, cudaMemcpyDeviceToHost);
+        stats->status_bits = bits;
+        unsigned long long cnt[2] = {0, 0};
+        cudaMemcpy(cnt, s->counters, sizeof cnt, cudaMemcpyDeviceToHost);
+        stats->teno_cores = cnt[0];
+        stats->teno_cut = cnt[1];
+    }
+    // restore one-shot fields for later single steps
+    hc->t_end = kInf;
+    hc->max_steps = std::numeric_limits<long long>::max();
+    hc->write_interval = 0.0;
+    hc->next_out = kInf;
+    hc->active = 0;
+    rc = push_clock(s);
+    if (rc) return rc;
+    return sync_and_check(s);
+}
+
+int sfg_residual(sfg_solver s, double* host_nodes_aos) {
+    if (!s || !host_nodes_aos) return fail(SFG_ERR_ARG, "null argument");
+    CUDA_TRY(cudaMemsetAsync(s->r, 0, sizeof(double) * 5 * s->gv.vs, s->stream));
+    int rc = enqueue_stage(s, 0, true, false);
+    if (rc) return rc;
+    // unsolved nodes are reported as 0: copy R without boundary mapping
+    GridView raw = s->gv;
+    for (int a = 0; a < 3; ++a) raw.bc_lo[a] = raw.bc_hi[a] = BC_PERIODIC;  // identity mapping inside [0,n)
+    raw.dim = 0;
+    CUDA_TRY(launch_soa_to_aos(raw, s->r, s->staging, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(host_nodes_aos, s->staging, sizeof(double) * 5 * s->nodes, cudaMemcpyDeviceToHost,
+                             s->stream));
+    return sync_and_check(s);
+}
+
+int sfg_stage_with_residual(sfg_solver s, int stage, double dt, const double* host_residual) {
+    if (!s || !host_residual) return fail(SFG_ERR_ARG, "null argument");
+    const int ns = stage_count(s->num.time_recipe);
+    if (stage != s->next_stage || stage < 0 || stage >= ns)
+        return fail(SFG_ERR_ARG, "explicit stage %d out of order (expected %d)", stage, s->next_stage);
+    CUDA_TRY(cudaMemcpyAsync(s->staging, host_residual, sizeof(double) * 5 * s->nodes, cudaMemcpyHostToDevice,
+                             s->stream));
+    CUDA_TRY(launch_aos_to_soa(s->staging, s->r, s->nodes, s->gv.vs, s->stream));
+    CUDA_TRY(launch_set_dt(s->clock, dt, s->stream));
+    StageView sv = stage_view(s, stage, false, false);
+    CUDA_TRY(launch_stage_from_residual(s->gv, sv, s->stream));
+    if (stage == ns - 1) {
+        int rc = enqueue_post_step(s);
+        if (rc) return rc;
+        CUDA_TRY(launch_commit(s->clock, nullptr, 0, s->stream));
+        s->next_stage = 0;
+    } else {
+        s->next_stage = stage + 1;
+    }
+    return sync_and_check(s);
+}
+
+int sfg_conserved_totals(sfg_solver s, double totals[5]) {
+    if (!s || !totals) return fail(SFG_ERR_ARG, "null argument");
+    CUDA_TRY(cudaMemsetAsync(s->totals, 0, 5 * sizeof(double), s->stream));
+    const double vol = s->grid.h[0] * s->grid.h[1] * s->grid.h[2];
+    CUDA_TRY(launch_totals(s->gv, s->qn, s->totals, vol, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(totals, s->totals, 5 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return SFG_OK;
+}
+
+int sfg_time(sfg_solver s, double* time, int64_t* steps) {
+    if (!s) return fail(SFG_ERR_ARG, "null solver");
+    int rc = pull_clock(s);
+    if (rc) return rc;
+    if (time) *time = s->host_clock->t;
+    if (steps) *steps = s->host_clock->steps;
+    return SFG_OK;
+}
+
+int sfg_status_word(sfg_solver s, uint32_t* bits, int clear) {
+    if (!s || !bits) return fail(SFG_ERR_ARG, "null argument");
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    unsigned b = 0;
+    CUDA_TRY(cudaMemcpy(&b, s->flags, sizeof b, cudaMemcpyDeviceToHost));
+    *bits = b;
+    if (clear) CUDA_TRY(cudaMemset(s->flags, 0, sizeof b));
+    return SFG_OK;
+}
+
+int sfg_set_counting(sfg_solver s, int enable) {
+    if (!s) return fail(SFG_ERR_ARG, "null solver");
+    if ((enable != 0) != s->counting && s->graph) {
+        cudaGraphExecDestroy(s->graph);
+        s->graph = nullptr;
+    }
+    s->counting = enable != 0;
+    CUDA_TRY(cudaMemsetAsync(s->counters, 0, 16, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return SFG_OK;
+}
+
+int sfg_time_sweeps(sfg_solver s, int stage, double dt, int repeats, float* ms_per_axis) {
+    if (!s || !ms_per_axis) return fail(SFG_ERR_ARG, "null argument");
+    if (stage < 0 || stage >= stage_count(s->num.time_recipe)) return fail(SFG_ERR_ARG, "bad stage %d", stage);
+    if (repeats < 1) repeats = 1;
+    const int dim = s->grid.dim;
+    cudaEvent_t ev[4];
+    for (auto& e : ev) CUDA_TRY(cudaEventCreate(&e));
+    double acc[3] = {0, 0, 0};
+    CUDA_TRY(launch_set_dt(s->clock, dt, s->stream));
+    StageView sv = stage_view(s, stage, false, false);
+    for (int r = 0; r < repeats; ++r) {
+        CUDA_TRY(cudaEventRecord(ev[0], s->stream));
+        for (int axis = 0; axis < dim; ++axis) {
+            sv.mode = (axis > 0 ? MODE_READ_R : 0) | (axis == dim - 1 ? MODE_FINAL : 0);
+            CUDA_TRY(launch_sweep(s->recipe->scheme, s->recipe->flux, s->num.precision == SFG_PREC_FP64, axis, s->gv,
+                                  sv, s->stream));
+            CUDA_TRY(cudaEventRecord(ev[axis + 1], s->stream));
+        }
+        CUDA_TRY(cudaEventSynchronize(ev[dim]));
+        for (int axis = 0; axis < dim; ++axis) {
+            float ms = 0.f;
+            CUDA_TRY(cudaEventElapsedTime(&ms, ev[axis], ev[axis + 1]));
+            acc[axis] += ms;
+        }
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    for (int axis = 0; axis < dim; ++axis) ms_per_axis[axis] = (float)(acc[axis] / repeats);
+    // the timed stage was not committed: state and flags are left as they were
+    CUDA_TRY(cudaMemsetAsync(s->flags, 0, 64, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return SFG_OK;
+}
+
+int sfg_get_counters(sfg_solver s, uint64_t* teno_cores, uint64_t* teno_cut) {
+    if (!s) return fail(SFG_ERR_ARG, "null solver");
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    unsigned long long c[2];
+    CUDA_TRY(cudaMemcpy(c, s->counters, sizeof c, cudaMemcpyDeviceToHost));
+    if (teno_cores) *teno_cores = c[0];
+    if (teno_cut) *teno_cut = c[1];
+    return SFG_OK;
+}
+
+}  // extern "C"
