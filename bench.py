@@ -222,12 +222,18 @@ def run_ours(args, rank, world):
 
     # ---- the other precision, same workload (plain FP64 vs mixed)
     other = capi.PREC_FP64 if prec else capi.PREC_FP32_FLUX
-    with torch.cuda.stream(stream):
-        s2 = case.solver(precision=other, stream=ctypes_stream(stream))
-    s2.advance(1e30, max_steps=W, graph_steps=K)
-    torch.cuda.synchronize()
-    st2, _ = s2.advance(1e30, max_steps=K, graph_steps=K)
-    out["fp64_value" if prec else "fp32flux_value"] = round(cells * K / (st2.device_ms * 1e-3) / 1e6, 2)
+    key = "fp64_value" if prec else "fp32flux_value"
+    s2 = None
+    try:
+        with torch.cuda.stream(stream):
+            s2 = case.solver(precision=other, stream=ctypes_stream(stream))
+        s2.advance(1e30, max_steps=W, graph_steps=K)
+        torch.cuda.synchronize()
+        st2, _ = s2.advance(1e30, max_steps=K, graph_steps=K)
+        out[key] = round(cells * K / (st2.device_ms * 1e-3) / 1e6, 2)
+    except capi.SolverError as e:
+        out[key] = None
+        out[key + "_error"] = str(e)
 
     # ---- roofline of the dominant sweep
     dt = s.compute_dt()
@@ -276,7 +282,8 @@ def run_ours(args, rank, world):
                   "steps": E, "path": "sfg_upload(pinned) + sfg_step + sfg_download per step"}
     out["gpu_launches"] += E * (launches_per_step + 2)
     s.close()
-    s2.close()
+    if s2 is not None:
+        s2.close()
     return out
 
 

@@ -252,9 +252,15 @@ template <> struct Teno<double> {
     }
 };
 
-// FP32: gamma_k^6 overflows single precision, so the cut-off test is made on
-// ratios to the largest gamma (smallest b+eps), which are in (0, 1]:
-//   g_k / g_m = (e_k + tau) e_m / (e_k (e_m + tau)),  e = b + eps.
+// FP32: gamma_k = g_k^6 leaves single-precision range long before FP64's, and
+// the smoothness indicators of a nearly uniform region (~1e-26) underflow any
+// product of two of them.  The cut-off test is therefore made on
+// r_k = g_k / max_j g_j in (0, 1]:
+//   tau = 0          -> every g_k = 1, nothing is cut;
+//   some g_k = +inf  -> those (the b_k ~ 0 sub-stencils) are kept, finite
+//                       ones cut (their ratio to the reference's huge gamma
+//                       is below the threshold);
+//   otherwise        -> r_k^6 < CT * sum_j r_j^6 with sum >= 1.
 template <> struct Teno<float> {
     static __device__ __forceinline__ float core(const float* v, unsigned& flags, unsigned& cut) {
         const float p0 = 2.f * v[0] - 7.f * v[1] + 11.f * v[2];
@@ -268,20 +274,29 @@ template <> struct Teno<float> {
         const float b1 = c13 * (t1 * t1) + 0.25f * (r1 * r1);
         const float b2 = c13 * (t2 * t2) + 0.25f * (r2 * r2);
         const float tau = fabsf(b0 - b2);
-        const float e0 = b0 + 1e-40f, e1 = b1 + 1e-40f, e2 = b2 + 1e-40f;
-        const float em = fminf(e0, fminf(e1, e2));
-        const float den = em + tau;
-        // ratio r_k = g_k / g_max; the minimum-e sub-stencil has r = 1
-        auto ratio = [&](float ek) -> float {
-            if (ek == em) return 1.f;
-            return __fdividef((ek + tau) * em, ek * den);
-        };
-        const float x0 = ratio(e0), x1 = ratio(e1), x2 = ratio(e2);
-        const float y0 = x0 * x0 * x0, y1 = x1 * x1 * x1, y2 = x2 * x2 * x2;
-        const float G0 = y0 * y0, G1 = y1 * y1, G2 = y2 * y2;
-        const float lim = 1e-5f * (G0 + G1 + G2);
-        if (!finite_(lim)) flags |= FLAG_NONFINITE;
-        const bool k0 = !(G0 < lim), k1 = !(G1 < lim), k2 = !(G2 < lim);
+        bool k0 = true, k1 = true, k2 = true;
+        if (tau > 0.f) {
+            // division by a subnormal b+eps gives +inf here: the "dominant" case
+            const float g0 = 1.f + __fdividef(tau, b0 + 1e-40f);
+            const float g1 = 1.f + __fdividef(tau, b1 + 1e-40f);
+            const float g2 = 1.f + __fdividef(tau, b2 + 1e-40f);
+            const float gm = fmaxf(g0, fmaxf(g1, g2));
+            if (!(gm <= 3.0e38f)) {
+                k0 = !(g0 <= 3.0e38f);
+                k1 = !(g1 <= 3.0e38f);
+                k2 = !(g2 <= 3.0e38f);
+            } else {
+                const float im = __frcp_rn(gm);
+                const float x0 = g0 * im, x1 = g1 * im, x2 = g2 * im;
+                const float y0 = x0 * x0 * x0, y1 = x1 * x1 * x1, y2 = x2 * x2 * x2;
+                const float G0 = y0 * y0, G1 = y1 * y1, G2 = y2 * y2;
+                const float lim = 1e-5f * (G0 + G1 + G2);
+                if (!finite_(lim)) flags |= FLAG_NONFINITE;
+                k0 = !(G0 < lim);
+                k1 = !(G1 < lim);
+                k2 = !(G2 < lim);
+            }
+        }
         cut += (!k0) + (!k1) + (!k2);
         const float d0 = k0 ? 0.1f : 0.f, d1 = k1 ? 0.6f : 0.f, d2 = k2 ? 0.3f : 0.f;
         const float act = d0 + d1 + d2;

@@ -1,0 +1,65 @@
+"""The FP32-flux / FP64-state path (reconstruction and face fluxes in FP32;
+state, stage accumulation, totals and dt in FP64) against the FP64 oracle.
+
+Tolerances (FP32 has a 6e-8 unit round-off):
+  * one step of a smooth or shocked state: relative L-infinity per variable
+    <= 2e-6 of the oracle's step (WENO5; TENO5 on smooth data);
+  * a vortex run: L1(rho) error against the exact solution within 1.5x of the
+    FP64 path's at the same grid and time.
+"""
+import numpy as np
+import pytest
+
+import pyoracle as po
+from conftest import rel_linf
+from helpers import FLUX_OF, SCHEME_OF, from_oracle, oracle_spec, smooth_state, split_recipe, to_oracle
+from sonicsolver_b200 import capi, cases
+
+pytestmark = pytest.mark.gpu
+
+STEP_TOL = 2e-6
+
+
+@pytest.mark.parametrize("recipe,shock", [("weno5Rusanov", False), ("weno5Rusanov", True), ("weno5Roe", True),
+                                          ("teno5Rusanov", False), ("weno3Rusanov", True), ("weno7Rusanov", False)])
+@pytest.mark.parametrize("dim,n,h", [(1, (61, 1, 1), (0.013, 1.0, 1.0)), (2, (37, 29, 1), (0.021, 0.017, 1.0)),
+                                     (3, (14, 12, 11), (0.05, 0.06, 0.07))])
+@pytest.mark.parametrize("bc", [capi.BC_TRANSMISSIVE, capi.BC_PERIODIC])
+def test_fp32_flux_step_close_to_fp64_oracle(recipe, shock, dim, n, h, bc):
+    bcs = (bc,) * 3
+    q = smooth_state(dim, n, seed=5, shock=shock)
+    spec = oracle_spec(dim, n, h, bcs, bcs, recipe)
+    s = capi.Solver(dim, n, h, bcs, bcs, recipe=recipe, time_recipe="SSPRK3", precision=capi.PREC_FP32_FLUX)
+    s.upload(np.ascontiguousarray(q))
+    scheme, flux = split_recipe(recipe)
+    Q = to_oracle(spec, q)
+    dt = po.dt(spec, Q, 0.5)
+    assert abs(s.compute_dt() - dt) <= 1e-14 * dt   # dt stays FP64
+    st = po.Stepper(spec, SCHEME_OF[scheme], FLUX_OF[flux], po.SSPRK3)
+    st.step(Q, dt)
+    s.step(dt)
+    err = rel_linf(s.download().reshape(q.shape), from_oracle(spec, Q))
+    assert err.max() <= STEP_TOL, err
+
+
+def test_fp32_vortex_l1_within_1p5x_of_fp64():
+    c = cases.isentropic_vortex(64, recipe="teno5Rusanov")
+    t_end = 1.0
+    errs = {}
+    for prec in (capi.PREC_FP64, capi.PREC_FP32_FLUX):
+        s = c.solver(precision=prec)
+        st, _ = s.advance(t_end)
+        assert abs(st.time - t_end) < 1e-12
+        q = s.download().reshape(c.q.shape)
+        ex = cases.vortex_exact(c, st.time)
+        errs[prec] = float(np.mean(np.abs(q[..., 0] - ex[..., 0])))
+    assert errs[capi.PREC_FP32_FLUX] <= 1.5 * errs[capi.PREC_FP64], errs
+
+
+def test_fp32_vortex_far_field_has_no_nonfinite_flags():
+    """Regression: near-uniform far field (smoothness indicators ~1e-26) must
+    not produce 0/0 in the FP32 TENO cut-off test."""
+    c = cases.isentropic_vortex(128, recipe="teno5Rusanov")
+    s = c.solver(precision=capi.PREC_FP32_FLUX)
+    st, _ = s.advance(1e30, max_steps=20)
+    assert st.status_bits == 0 and st.steps == 20

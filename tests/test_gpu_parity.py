@@ -44,8 +44,10 @@ def test_residual_parity(recipe, dim, n, h, bc, shock):
     Q = to_oracle(spec, q)
     R_ref = from_oracle(spec, po.rhs(spec, SCHEME_OF[scheme], FLUX_OF[flux], Q))
     R_gpu = s.residual().reshape(R_ref.shape)
-    # unsolved transmissive boundary nodes are reported as 0 by both
-    err = rel_linf(R_gpu, R_ref)
+    # compare on solved nodes: transmissive boundary nodes are not advanced
+    # (the GPU reports 0 there; the oracle evaluates them anyway)
+    sl = tuple(slice(1, -1) if (d < dim and bc == capi.BC_TRANSMISSIVE) else slice(None) for d in (2, 1, 0))
+    err = rel_linf(R_gpu[sl], R_ref[sl])
     assert err.max() <= TOL, (recipe, dim, bc, shock, err)
 
 
@@ -144,7 +146,7 @@ def test_invalid_state_reports_error():
     dim, n, h = GRIDS[0]
     s, spec, q = _pair(dim, n, h, capi.BC_TRANSMISSIVE, "weno5Rusanov")
     bad = q.copy()
-    bad[0, 0, 30, 4] = 0.01  # E below the kinetic energy -> p < 0
+    bad[0, 0, 30, 4] = -1.0  # negative total energy -> p < 0
     s.upload(np.ascontiguousarray(bad))
     with pytest.raises(capi.SolverError) as e:
         s.step(1e-4)
