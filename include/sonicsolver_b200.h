@@ -187,6 +187,33 @@ int sfg_status_word(sfg_solver s, uint32_t* bits, int clear);
 int sfg_set_counting(sfg_solver s, int enable);
 int sfg_get_counters(sfg_solver s, uint64_t* teno_cores, uint64_t* teno_cut);
 
+/* ---- residual without device allocation --------------------------------
+ * Has no counterpart in the reference.  Some callers cannot allocate device
+ * memory where they need an operator evaluation: a host application whose
+ * own memory manager owns the whole device budget and forbids plugins from
+ * allocating, a deployment with a fixed, pre-sized memory plan, or code on a
+ * latency-critical stream that must not take cudaMalloc's implicit device
+ * synchronisation.  sfg_residual_noalloc computes the same spatial residual
+ * as sfg_residual (R = Jac * sum_d dF_d; 0 on unsolved transmissive boundary
+ * nodes) for a caller-owned device state and writes it to a caller-owned
+ * device array, allocating nothing: its working memory is one fixed array in
+ * the library's device image, of 32 + 5 * SFG_NOALLOC_MAX_NODES doubles
+ * (~10 MiB), which every GPU that loads the library holds until the process
+ * exits.
+ *   dev_q, dev_r: device arrays, structure of arrays [5][nodes] with
+ *                 nodes = n[0] * n[1] * n[2] (x fastest), FP64.
+ *   stream:       cudaStream_t (NULL: the legacy default stream).
+ * Grids of more than SFG_NOALLOC_MAX_NODES nodes are rejected (SFG_ERR_ARG).
+ * The first call on each device looks up the array's device address with
+ * that device current; make that first call before any stream capture.
+ * All calls share the one array and it keeps the last call's contents, so
+ * calls whose work overlaps on the GPU (other streams, other host threads)
+ * race: serialise them.  The call returns after its work has finished on
+ * `stream` (it reads back the status word). */
+#define SFG_NOALLOC_MAX_NODES 262144
+int sfg_residual_noalloc(const sfg_grid_desc* grid, const sfg_numerics_desc* numerics,
+                         const double* dev_q, double* dev_r, void* stream);
+
 /* ---- diagnostics (no counterpart in the reference: measurement aids) -- */
 /* Runs stage `stage` of a step of size dt `repeats` times on the current
  * state without committing it, timing each axis sweep with CUDA events on the

@@ -101,6 +101,7 @@ def lib():
         L.sfg_time_sweeps.argtypes = [_VP, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                       ctypes.POINTER(ctypes.c_float)]
         L.sfg_measure_fma_peak.argtypes = [ctypes.c_int, ctypes.c_double, _DP]
+        L.sfg_residual_noalloc.argtypes = [ctypes.POINTER(GridDesc), ctypes.POINTER(NumericsDesc), _VP, _VP, _VP]
         _lib = L
     return _lib
 
@@ -226,6 +227,23 @@ class Solver:
         out = (ctypes.c_float * 3)()
         check(lib().sfg_time_sweeps(self._h, stage, dt, repeats, out))
         return [out[d] for d in range(self.dim)]
+
+
+NOALLOC_MAX_NODES = 262144  # SFG_NOALLOC_MAX_NODES in include/sonicsolver_b200.h
+
+
+def residual_noalloc(dim, n, h, bc_lo, bc_hi, dev_q: int, dev_r: int, recipe="weno5Rusanov",
+                     precision=PREC_FP64, gamma=1.4, stream=None):
+    """sfg_residual_noalloc on caller-owned device arrays (addresses as ints,
+    structure of arrays [5][nodes]).  For callers that cannot allocate device
+    memory themselves at this point; the library allocates nothing either."""
+    g = grid_desc(dim, n, h, bc_lo, bc_hi)
+    nm = NumericsDesc()
+    nm.recipe = RECIPES[recipe] if isinstance(recipe, str) else int(recipe)
+    nm.time_recipe = TIME_RECIPES["SSPRK3"]
+    nm.precision = precision
+    nm.gamma, nm.cfl, nm.max_dt = gamma, 0.5, 0.0
+    check(lib().sfg_residual_noalloc(ctypes.byref(g), ctypes.byref(nm), _VP(dev_q), _VP(dev_r), stream))
 
 
 def fma_peak_tflops(fp64=True, seconds=0.5) -> float:

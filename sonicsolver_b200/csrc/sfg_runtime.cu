@@ -87,6 +87,11 @@ int stage_count(int time_id) { return time_id == T_EULER ? 1 : (time_id == T_SSP
 
 }  // namespace
 
+namespace sfg {
+// Records a failure message for sfg_last_error() from other translation units.
+void set_last_error(const char* msg) { g_error = msg ? msg : ""; }
+}  // namespace sfg
+
 struct sfg_solver_s {
     int device = 0;
     cudaStream_t stream = nullptr;
