@@ -55,6 +55,11 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--quick", action="store_true", help="skip e2e / peaks / baseline (profiling runs)")
+    ap.add_argument("--batch-steps", type=int, default=200)
+    ap.add_argument("--serve-requests", type=int, default=96)
+    ap.add_argument("--serve-rate", type=float, default=8.0, help="Poisson arrivals per second")
+    ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--accuracy-t", type=float, default=10.0, help="vortex run length for the L1 check (0: skip)")
     return ap.parse_args()
 
 
@@ -210,11 +215,11 @@ def run_ours(args, rank, world):
            "data": "synthetic (analytic isentropic vortex initial condition)",
            "config": {"workload": "isentropic_vortex_2d", "cells": f"{args.size}x{args.size}", "domain": "[0,10]^2",
                       "recipe": "teno5Rusanov", "time": "SSPRK3", "cfl": 0.4, "precision": args.precision,
-                      "parallelism": f"replicas x{world}", "graph_steps": K,
+                      "parallelism": f"replicas x{world}", "graph_steps": K, "kernel_variant": s.variant,
                       "l2": "inputs larger than L2 (4 x 42 MB state arrays touched per stage)"},
            "clocks": clk.summary(), "gpu_launches": None}
     dim = case.dim
-    launches_per_step = 2 + 3 * dim + 1  # dt, finalize, sweeps, commit
+    launches_per_step = 2 + 3 * (1 if (dim == 2 and s.variant > 0) else dim) + 1  # dt, finalize, stages, commit
     out["gpu_launches"] = launches_per_step * (K + 0)
     if args.quick or rank != 0:
         s.close()
@@ -240,18 +245,24 @@ def run_ours(args, rank, world):
     ms_axes = s.time_sweeps(dt, stage=0, repeats=5)
     nodes = case.nodes
     hbm, src = measured_peaks()
-    kinds = ["first", "last"] if dim == 2 else ["final"]
     dom = int(np.argmax(ms_axes))
-    bytes_node = 2 * STATE_BYTES if (dim > 1 and dom == 0) else 4 * STATE_BYTES
+    fused = dim == 2 and s.variant > 0
+    if fused:
+        # one fused launch per stage: 320 B per cell-step (SSPRK3, FP64 state)
+        # over the 3 launches of a step
+        bytes_node = 320.0 / 3.0
+    else:
+        bytes_node = 2 * STATE_BYTES if (dim > 1 and dom == 0) else 4 * STATE_BYTES
     achieved = bytes_node * nodes / (ms_axes[dom] * 1e-3) / 1e9
     fp_peak = capi.fma_peak_tflops(fp64=(prec == capi.PREC_FP64), seconds=0.5)
-    faces = nodes  # one face per node per axis
+    faces = nodes * (dim if fused else 1)  # faces evaluated by one launch
     fl = FLOPS_PER_FACE["teno5"] * faces / (ms_axes[dom] * 1e-3) / 1e12
     out["roofline"] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                        "frac": round(achieved / hbm, 4), "traffic": None, "peak_source": f"{src} (MEASURED_PEAKS.json)",
-                       "kernel": f"sweep axis {dom} ({'x' if dom == 0 else 'y'})", "ms_per_launch": round(ms_axes[dom], 4),
+                       "kernel": ("tile2d fused stage" if fused else f"sweep axis {dom}"),
+                       "ms_per_launch": round(ms_axes[dom], 4),
                        "ms_per_axis": [round(x, 4) for x in ms_axes],
-                       "algorithmic_bytes_per_launch": bytes_node * nodes,
+                       "algorithmic_bytes_per_launch": int(bytes_node * nodes),
                        "issue_roof": {"unit": "TFLOP/s", "achieved": round(fl, 2), "fma_peak": round(fp_peak, 2),
                                       "frac": round(fl / fp_peak, 4) if fp_peak else None,
                                       "arith": "fp32" if prec else "fp64",
@@ -284,7 +295,123 @@ def run_ours(args, rank, world):
     s.close()
     if s2 is not None:
         s2.close()
+    if args.accuracy_t > 0:
+        out["accuracy"] = run_accuracy(args)
+    if not args.no_batch:
+        out["batched"] ={"fp32flux": run_batched(args, capi.PREC_FP32_FLUX), "fp64": run_batched(args, capi.PREC_FP64)}
+        cap = out["batched"]["fp64"]["value"]
+        out["served"] = {"fp32flux": run_served(args, capi.PREC_FP32_FLUX, capacity=cap),
+                         "fp64": run_served(args, capi.PREC_FP64, capacity=cap)}
     return out
+
+
+def run_accuracy(args):
+    """Matched-accuracy check on the headline workload: one full period
+    (t = 10) of the 1024^2 vortex, TENO5 + Rusanov, SSPRK3, CFL 0.4, in FP64
+    and FP32-flux; L1(rho) against the exact solution (the advected initial
+    field) and FP32 against FP64 (the FP64 path matches the CPU oracle to
+    <= 1e-12 per step in the parity tests; the oracle itself would need days
+    on the host for this run), plus the TENO5 cut-off flip rate."""
+    import numpy as np
+    from sonicsolver_b200 import capi, cases
+    case = cases.isentropic_vortex(args.size)
+    out = {"t_end": args.accuracy_t, "cells": f"{args.size}x{args.size}"}
+    res = {}
+    for name, prec in (("fp64", capi.PREC_FP64), ("fp32flux", capi.PREC_FP32_FLUX)):
+        s = case.solver(precision=prec)
+        d0, f0 = s.teno_flips()
+        st, _ = s.advance(args.accuracy_t, graph_steps=64)
+        q = s.download().reshape(case.q.shape)
+        d1, f1 = s.teno_flips()
+        ex = cases.vortex_exact(case, st.time)
+        res[name] = q
+        out[name] = {"steps": int(st.steps), "device_s": round(st.device_ms / 1e3, 3),
+                     "l1_rho_vs_exact": float(np.mean(np.abs(q[..., 0] - ex[..., 0]))),
+                     "linf_rho_vs_exact": float(np.max(np.abs(q[..., 0] - ex[..., 0])))}
+        if name == "fp64":
+            out["teno_flip_rate"] = {"initial": f0 / max(d0, 1), "final": f1 / max(d1, 1),
+                                     "decisions_per_eval": int(d0)}
+        s.close()
+    out["l1_rho_fp32flux_vs_fp64"] = float(np.mean(np.abs(res["fp32flux"][..., 0] - res["fp64"][..., 0])))
+    out["l1_ratio_fp32flux_over_fp64"] = out["fp32flux"]["l1_rho_vs_exact"] / out["fp64"]["l1_rho_vs_exact"]
+    return out
+
+
+def run_batched(args, precision):
+    """Batched shock tubes: 512 seeded instances (half 1-D N in [256, 16384],
+    half 2-D side in [64, 512]), WENO5 + Rusanov, SSPRK3, every grid with its
+    own CFL step; a bounded number of batch steps timed with CUDA events."""
+    import torch
+    from sonicsolver_b200 import capi, cases
+    tubes = cases.shock_tube_batch(count=512, seed=2024, t_end=0.15)
+    b = capi.Batch(8 << 30, 512, recipe="weno5Rusanov", precision=precision, cfl=0.5)
+    slots = [b.add(c) for c in tubes]
+    steps = args.batch_steps
+    b.step(3, graph_steps=16)                     # warm-up (graph capture)
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    before = {s: b.status(s)["steps"] for s in slots}
+    t0.record()
+    b.step(steps, graph_steps=16)
+    t1.record()
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1)
+    cell_steps = sum(c.cells * (b.status(s)["steps"] - before[s]) for c, s in zip(tubes, slots))
+    info = b.info()
+    b.close()
+    return {"value": round(cell_steps / (ms * 1e-3) / 1e6, 2), "unit": "Mcell-steps/s", "batch_steps": steps,
+            "instances": len(tubes), "cells_total": int(sum(c.cells for c in tubes)),
+            "tiles": info["items"], "ms": round(ms, 2),
+            "note": "default stream events around sfg_batch_step (graph of 16 steps, per-grid dt)"}
+
+
+def run_served(args, precision, seed=7, capacity=None):
+    """Served stream: Poisson arrivals of 2-D solves (isentropic vortex and
+    slanted shock tubes, grids 64^2..1024^2, 100..2000 steps), admission by a
+    60 GB HBM budget, continuous batching; latency = finish - submit."""
+    import numpy as np
+    from sonicsolver_b200 import capi, cases
+    rng = np.random.default_rng(seed)
+    nreq = args.serve_requests
+    reqs = []
+    for k in range(nreq):
+        side = int(round(np.exp(rng.uniform(np.log(64), np.log(1024)))))
+        steps = int(rng.integers(100, 2001))
+        if rng.random() < 0.5:
+            c = cases.isentropic_vortex(side, recipe="weno5Rusanov", cfl=0.5, t_end=1e9)
+        else:
+            c = cases.shock_tube_batch(count=2, seed=int(rng.integers(1 << 30)), t_end=1e9, max_2d=side)[1]
+        reqs.append((c, steps))
+    work = sum(c.cells * s for c, s in reqs)
+    srv = capi.Server(60 << 30, 256, recipe="weno5Rusanov", precision=precision, cfl=0.5, graph_steps=8)
+    # offered load: 1.2x the plain FP64 path's capacity for this request mix
+    rate = args.serve_rate if capacity is None else 1.2 * capacity * 1e6 / (work / nreq)
+    gaps = rng.exponential(1.0 / rate, nreq)
+    ids = []
+    start = srv.now()
+    t_next = start
+    for (c, steps), gap in zip(reqs, gaps):
+        t_next += gap
+        while srv.now() < t_next:
+            time.sleep(min(0.002, max(0.0, t_next - srv.now())))
+        ids.append(srv.submit(c, max_steps=steps))
+    srv.drain(600)
+    infos = [srv.poll(i) for i in ids]
+    end = max(i.finish_s for i in infos)
+    lat = np.array([i.finish_s - i.submit_s for i in infos])
+    wait = np.array([i.admit_s - i.submit_s for i in infos])
+    ok = sum(1 for i in infos if i.state == capi.REQ_DONE)
+    failed = [{"request": k, "cells": reqs[k][0].cells, "case": reqs[k][0].name, "flags": int(infos[k].flags),
+               "steps_done": int(infos[k].steps)} for k in range(nreq) if infos[k].state == capi.REQ_FAILED]
+    srv.close()
+    return {"requests": nreq, "completed": ok, "failed": failed, "arrival_rate_per_s": round(rate, 3),
+            "offered_load": "1.2x FP64 batched capacity" if capacity else "fixed rate",
+            "p50_latency_s": round(float(np.percentile(lat, 50)), 4),
+            "p99_latency_s": round(float(np.percentile(lat, 99)), 4),
+            "p50_queue_wait_s": round(float(np.percentile(wait, 50)), 4),
+            "throughput": {"value": round(work / (end - start) / 1e6, 2), "unit": "Mcell-steps/s"},
+            "wall_s": round(end - start, 2), "budget_gb": 60}
 
 
 def ctypes_stream(stream):

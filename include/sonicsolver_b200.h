@@ -187,6 +187,82 @@ int sfg_status_word(sfg_solver s, uint32_t* bits, int clear);
 int sfg_set_counting(sfg_solver s, int enable);
 int sfg_get_counters(sfg_solver s, uint64_t* teno_cores, uint64_t* teno_cut);
 
+/* ---- batches of independent grids ---------------------------------------
+ * Many 1-D / 2-D grids of uneven sizes, each with its own CFL step, end time
+ * and status, advanced together: per batch step one persistent kernel
+ * computes every grid's CFL minimum, one persistent kernel per stage works
+ * through a list of tiles of all grids, and a per-grid clock update follows;
+ * runs of steps execute as one CUDA graph.  Grids can be added and removed
+ * between calls without rebuilding the graph (continuous batching).  The
+ * reference has no batch layer: each sonicSolver run is one case; a batch is
+ * the GPU form of running many cases (test/Sod-style cases, MPI ranks on
+ * independent blocks) side by side.  All grids share one sfg_numerics_desc.
+ * State memory comes from one slab of `hbm_budget_bytes` reserved at create;
+ * sfg_batch_add returns SFG_ERR_BUDGET when a grid does not fit. */
+typedef struct sfg_batch_s* sfg_batch;
+int sfg_batch_create(const sfg_numerics_desc* numerics, size_t hbm_budget_bytes, int max_instances,
+                     void* stream, sfg_batch* out);
+int sfg_batch_destroy(sfg_batch b);
+/* Device bytes a grid would take from the budget. */
+int sfg_batch_instance_bytes(sfg_batch b, const sfg_grid_desc* grid, size_t* bytes);
+/* Uploads a grid (AoS nodes, time 0) that will run to t_end or max_steps
+ * (<= 0: no step limit); *slot identifies it. */
+int sfg_batch_add(sfg_batch b, const sfg_grid_desc* grid, const double* host_nodes_aos, double t_end,
+                  int64_t max_steps, int* slot);
+int sfg_batch_remove(sfg_batch b, int slot);
+/* Runs up to `steps` batch steps (graph of `graph_steps`, <= 0: 16); stops
+ * early when no grid is running.  *active = grids that stepped last. */
+int sfg_batch_step(sfg_batch b, int steps, int graph_steps, int* active);
+int sfg_batch_status(sfg_batch b, int slot, double* time, int64_t* steps, int* running, uint32_t* flags);
+int sfg_batch_download(sfg_batch b, int slot, double* host_nodes_aos);
+/* Tile shape of the 2-D work items: 1 = 30 x 16, 2 = 22 x 22. */
+int sfg_batch_set_variant(sfg_batch b, int variant);
+int sfg_batch_info(sfg_batch b, size_t* used_bytes, size_t* budget_bytes, int* live, int* items);
+/* Status of slots 0..count-1 in one read (running: 1 running, 0 finished or
+ * failed, -1 empty slot); any output pointer may be NULL. */
+int sfg_batch_snapshot(sfg_batch b, int count, int* running, double* time, int64_t* steps, uint32_t* flags);
+
+/* ---- serving -------------------------------------------------------------
+ * A request loop on its own host thread over one batch: submitted solves
+ * wait in a FIFO queue, are admitted while the HBM budget and the slot count
+ * allow, step with everything else in flight (state stays on the device),
+ * and are retired -- result downloaded, slot and memory released -- as soon
+ * as they finish.  Requests arriving while others run join the batch at the
+ * next graph boundary (continuous batching). */
+enum { SFG_REQ_QUEUED = 0, SFG_REQ_RUNNING = 1, SFG_REQ_DONE = 2, SFG_REQ_FAILED = 3, SFG_REQ_CANCELLED = 4 };
+typedef struct {
+    double submit_s, admit_s, finish_s;  /* seconds on the server's steady clock */
+    int64_t steps;
+    double time;
+    uint32_t flags;
+    int state;                           /* SFG_REQ_* */
+} sfg_request_info;
+typedef struct sfg_server_s* sfg_server;
+int sfg_server_create(const sfg_numerics_desc* numerics, size_t hbm_budget_bytes, int max_slots, int graph_steps,
+                      sfg_server* out);
+/* Stops the loop (pending requests are cancelled) and frees everything. */
+int sfg_server_destroy(sfg_server s);
+/* Copies the input; the request runs to t_end or max_steps. */
+int sfg_server_submit(sfg_server s, const sfg_grid_desc* grid, const double* host_nodes_aos, double t_end,
+                      int64_t max_steps, int64_t* request_id);
+int sfg_server_poll(sfg_server s, int64_t request_id, sfg_request_info* info);
+/* Result of a finished request (AoS nodes); SFG_ERR_ARG while not done. */
+int sfg_server_fetch(sfg_server s, int64_t request_id, double* host_nodes_aos);
+int sfg_server_cancel(sfg_server s, int64_t request_id);
+/* Blocks until every submitted request has left the system or timeout_s
+ * passes (SFG_ERR_TIMEOUT). */
+int sfg_server_drain(sfg_server s, double timeout_s);
+/* Seconds on the server's steady clock (same origin as sfg_request_info). */
+double sfg_server_now(sfg_server s);
+
+/* Kernel variant of the stage operator: 0 = one sweep launch per axis
+ * (any dimension), 1 = fused tile kernel (2-D: 30 x 16 tiles, 1-D: 511-node
+ * tiles), 2 = fused 2-D tile kernel with 22 x 22 tiles.  sfg_create picks 1
+ * for 1-D and 2-D grids and 0 for 3-D; results agree across variants to
+ * round-off, and variant 1 gives the same bits as a batch. */
+int sfg_set_kernel_variant(sfg_solver s, int variant);
+int sfg_get_kernel_variant(sfg_solver s, int* variant);
+
 /* ---- residual without device allocation --------------------------------
  * Has no counterpart in the reference.  Some callers cannot allocate device
  * memory where they need an operator evaluation: a host application whose
@@ -215,6 +291,10 @@ int sfg_residual_noalloc(const sfg_grid_desc* grid, const sfg_numerics_desc* num
                          const double* dev_q, double* dev_r, void* stream);
 
 /* ---- diagnostics (no counterpart in the reference: measurement aids) -- */
+/* TENO5 cut-off decisions of the current state's faces (3 per scalar core,
+ * 30 per face) evaluated in FP64 and in FP32: *flips counts those that
+ * differ.  Zero for non-TENO recipes. */
+int sfg_teno_flip_rate(sfg_solver s, uint64_t* decisions, uint64_t* flips);
 /* Runs stage `stage` of a step of size dt `repeats` times on the current
  * state without committing it, timing each axis sweep with CUDA events on the
  * solver's stream; ms_per_axis[d] receives the mean duration of sweep d. */

@@ -54,6 +54,15 @@ class Stats(ctypes.Structure):
                 ("teno_cut", ctypes.c_uint64), ("teno_cores", ctypes.c_uint64)]
 
 
+class RequestInfo(ctypes.Structure):
+    _fields_ = [("submit_s", ctypes.c_double), ("admit_s", ctypes.c_double), ("finish_s", ctypes.c_double),
+                ("steps", ctypes.c_int64), ("time", ctypes.c_double), ("flags", ctypes.c_uint32),
+                ("state", ctypes.c_int)]
+
+
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED, REQ_CANCELLED = range(5)
+
+
 class SolverError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"[{code}] {msg}")
@@ -102,6 +111,34 @@ def lib():
                                       ctypes.POINTER(ctypes.c_float)]
         L.sfg_measure_fma_peak.argtypes = [ctypes.c_int, ctypes.c_double, _DP]
         L.sfg_residual_noalloc.argtypes = [ctypes.POINTER(GridDesc), ctypes.POINTER(NumericsDesc), _VP, _VP, _VP]
+        L.sfg_set_kernel_variant.argtypes = [_VP, ctypes.c_int]
+        L.sfg_get_kernel_variant.argtypes = [_VP, ctypes.POINTER(ctypes.c_int)]
+        L.sfg_teno_flip_rate.argtypes = [_VP, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
+        PG, PN = ctypes.POINTER(GridDesc), ctypes.POINTER(NumericsDesc)
+        I64P = ctypes.POINTER(ctypes.c_int64)
+        L.sfg_batch_create.argtypes = [PN, ctypes.c_size_t, ctypes.c_int, _VP, ctypes.POINTER(_VP)]
+        L.sfg_batch_destroy.argtypes = [_VP]
+        L.sfg_batch_instance_bytes.argtypes = [_VP, PG, ctypes.POINTER(ctypes.c_size_t)]
+        L.sfg_batch_add.argtypes = [_VP, PG, _DP, ctypes.c_double, ctypes.c_int64, ctypes.POINTER(ctypes.c_int)]
+        L.sfg_batch_remove.argtypes = [_VP, ctypes.c_int]
+        L.sfg_batch_step.argtypes = [_VP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+        L.sfg_batch_status.argtypes = [_VP, ctypes.c_int, _DP, I64P, ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_uint32)]
+        L.sfg_batch_download.argtypes = [_VP, ctypes.c_int, _DP]
+        L.sfg_batch_set_variant.argtypes = [_VP, ctypes.c_int]
+        L.sfg_batch_info.argtypes = [_VP, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t),
+                                     ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+        L.sfg_batch_snapshot.argtypes = [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int), _DP, I64P,
+                                         ctypes.POINTER(ctypes.c_uint32)]
+        L.sfg_server_create.argtypes = [PN, ctypes.c_size_t, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_VP)]
+        L.sfg_server_destroy.argtypes = [_VP]
+        L.sfg_server_submit.argtypes = [_VP, PG, _DP, ctypes.c_double, ctypes.c_int64, I64P]
+        L.sfg_server_poll.argtypes = [_VP, ctypes.c_int64, ctypes.POINTER(RequestInfo)]
+        L.sfg_server_fetch.argtypes = [_VP, ctypes.c_int64, _DP]
+        L.sfg_server_cancel.argtypes = [_VP, ctypes.c_int64]
+        L.sfg_server_drain.argtypes = [_VP, ctypes.c_double]
+        L.sfg_server_now.argtypes = [_VP]
+        L.sfg_server_now.restype = ctypes.c_double
         _lib = L
     return _lib
 
@@ -223,10 +260,158 @@ class Solver:
         check(lib().sfg_get_counters(self._h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
 
+    @property
+    def variant(self) -> int:
+        v = ctypes.c_int()
+        check(lib().sfg_get_kernel_variant(self._h, ctypes.byref(v)))
+        return v.value
+
+    @variant.setter
+    def variant(self, v: int):
+        check(lib().sfg_set_kernel_variant(self._h, int(v)))
+
+    def teno_flips(self):
+        """(decisions, flips) of TENO5 cut-offs, FP64 vs FP32 on the current state."""
+        d, f = ctypes.c_uint64(), ctypes.c_uint64()
+        check(lib().sfg_teno_flip_rate(self._h, ctypes.byref(d), ctypes.byref(f)))
+        return d.value, f.value
+
     def time_sweeps(self, dt, stage=0, repeats=5):
         out = (ctypes.c_float * 3)()
         check(lib().sfg_time_sweeps(self._h, stage, dt, repeats, out))
         return [out[d] for d in range(self.dim)]
+
+
+def numerics_desc(recipe="weno5Rusanov", time_recipe="SSPRK3", precision=PREC_FP64, gamma=1.4, cfl=0.5,
+                  max_dt=0.0) -> NumericsDesc:
+    nm = NumericsDesc()
+    nm.recipe = RECIPES[recipe] if isinstance(recipe, str) else int(recipe)
+    nm.time_recipe = TIME_RECIPES[time_recipe] if isinstance(time_recipe, str) else int(time_recipe)
+    nm.precision = precision
+    nm.gamma, nm.cfl, nm.max_dt = gamma, cfl, max_dt
+    return nm
+
+
+class Batch:
+    """Many independent 1-D / 2-D grids stepped together (sfg_batch)."""
+
+    def __init__(self, budget_bytes, max_instances, recipe="weno5Rusanov", time_recipe="SSPRK3",
+                 precision=PREC_FP64, gamma=1.4, cfl=0.5, max_dt=0.0, stream=None):
+        nm = numerics_desc(recipe, time_recipe, precision, gamma, cfl, max_dt)
+        h = _VP()
+        check(lib().sfg_batch_create(ctypes.byref(nm), int(budget_bytes), int(max_instances), stream, ctypes.byref(h)))
+        self._h = h
+        self.shapes = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().sfg_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add(self, case, t_end=None, max_steps=0) -> int:
+        g = grid_desc(case.dim, case.n, case.h, case.bc_lo, case.bc_hi)
+        slot = ctypes.c_int()
+        q = np.ascontiguousarray(case.q, dtype=np.float64)
+        check(lib().sfg_batch_add(self._h, ctypes.byref(g), _dptr(q), case.t_end if t_end is None else t_end,
+                                  max_steps, ctypes.byref(slot)))
+        self.shapes[slot.value] = q.shape
+        return slot.value
+
+    def instance_bytes(self, case) -> int:
+        g = grid_desc(case.dim, case.n, case.h, case.bc_lo, case.bc_hi)
+        b = ctypes.c_size_t()
+        check(lib().sfg_batch_instance_bytes(self._h, ctypes.byref(g), ctypes.byref(b)))
+        return b.value
+
+    def remove(self, slot):
+        check(lib().sfg_batch_remove(self._h, slot))
+        self.shapes.pop(slot, None)
+
+    def step(self, steps, graph_steps=16) -> int:
+        a = ctypes.c_int()
+        check(lib().sfg_batch_step(self._h, int(steps), int(graph_steps), ctypes.byref(a)))
+        return a.value
+
+    def status(self, slot):
+        t, n, r, f = ctypes.c_double(), ctypes.c_int64(), ctypes.c_int(), ctypes.c_uint32()
+        check(lib().sfg_batch_status(self._h, slot, ctypes.byref(t), ctypes.byref(n), ctypes.byref(r), ctypes.byref(f)))
+        return {"time": t.value, "steps": n.value, "running": bool(r.value), "flags": f.value}
+
+    def download(self, slot) -> np.ndarray:
+        out = np.empty(self.shapes[slot], dtype=np.float64)
+        check(lib().sfg_batch_download(self._h, slot, _dptr(out)))
+        return out
+
+    @property
+    def variant(self):
+        raise AttributeError("write-only")
+
+    @variant.setter
+    def variant(self, v):
+        check(lib().sfg_batch_set_variant(self._h, int(v)))
+
+    def info(self):
+        u, b, l, i = ctypes.c_size_t(), ctypes.c_size_t(), ctypes.c_int(), ctypes.c_int()
+        check(lib().sfg_batch_info(self._h, ctypes.byref(u), ctypes.byref(b), ctypes.byref(l), ctypes.byref(i)))
+        return {"used": u.value, "budget": b.value, "live": l.value, "items": i.value}
+
+
+class Server:
+    """Continuous-batching request loop (sfg_server) on its own host thread."""
+
+    def __init__(self, budget_bytes, max_slots, recipe="weno5Rusanov", time_recipe="SSPRK3", precision=PREC_FP64,
+                 gamma=1.4, cfl=0.5, graph_steps=16):
+        nm = numerics_desc(recipe, time_recipe, precision, gamma, cfl)
+        h = _VP()
+        check(lib().sfg_server_create(ctypes.byref(nm), int(budget_bytes), int(max_slots), int(graph_steps),
+                                      ctypes.byref(h)))
+        self._h = h
+        self.shapes = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().sfg_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, case, t_end=None, max_steps=0) -> int:
+        g = grid_desc(case.dim, case.n, case.h, case.bc_lo, case.bc_hi)
+        q = np.ascontiguousarray(case.q, dtype=np.float64)
+        rid = ctypes.c_int64()
+        check(lib().sfg_server_submit(self._h, ctypes.byref(g), _dptr(q), case.t_end if t_end is None else t_end,
+                                      int(max_steps), ctypes.byref(rid)))
+        self.shapes[rid.value] = q.shape
+        return rid.value
+
+    def poll(self, rid) -> RequestInfo:
+        info = RequestInfo()
+        check(lib().sfg_server_poll(self._h, rid, ctypes.byref(info)))
+        return info
+
+    def fetch(self, rid) -> np.ndarray:
+        out = np.empty(self.shapes[rid], dtype=np.float64)
+        check(lib().sfg_server_fetch(self._h, rid, _dptr(out)))
+        return out
+
+    def cancel(self, rid):
+        check(lib().sfg_server_cancel(self._h, rid))
+
+    def drain(self, timeout_s=600.0):
+        check(lib().sfg_server_drain(self._h, float(timeout_s)))
+
+    def now(self) -> float:
+        return lib().sfg_server_now(self._h)
 
 
 NOALLOC_MAX_NODES = 262144  # SFG_NOALLOC_MAX_NODES in include/sonicsolver_b200.h

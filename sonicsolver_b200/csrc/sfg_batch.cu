@@ -1,0 +1,802 @@
+// sfg_batch.cu -- many independent grids of uneven sizes and dimensions
+// advanced together (sfg_batch_* in include/sonicsolver_b200.h).
+//
+// Device side:
+//   * an instance table: per grid its GridView, state buffers (carved out of
+//     one HBM slab), its own step clock (t, CFL dt, end time, step limit) and
+//     status word -- every grid keeps its own CFL step, exactly as if it ran
+//     alone;
+//   * a work list of tiles (2-D: TX x TY nodes, 1-D: 511 nodes) covering the
+//     solved nodes of every live instance, with its length in device memory;
+//   * persistent kernels, one block per SM slot, that take tiles from the
+//     list with an atomic counter: CFL reduction (per-instance 64-bit
+//     atomicMin), then each stage (the fused tile bodies of sfg_tile.cuh),
+//     then the per-instance clock update.
+// Host side: the batch step is captured once as a CUDA graph of G steps.
+// Adding or removing instances rewrites the table rows and the work list in
+// device memory between graph launches, so the graph never needs recapture
+// (continuous batching).
+#include "../../include/sonicsolver_b200.h"
+#include "sfg_tile.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstring>
+#include <limits>
+#include <map>
+#include <string>
+#include <vector>
+
+namespace sfg {
+void set_last_error(const char* msg);
+cudaError_t launch_soa_to_aos(const GridView& g, const double* soa, double* aos, cudaStream_t st);
+cudaError_t launch_aos_to_soa(const double* aos, double* soa, long long nodes, long long vs, cudaStream_t st);
+
+struct BatchInst {
+    GridView g;
+    double *qn, *qa, *qb, *k;
+    Clock clock;
+    unsigned flags;
+    int live;  // slot in use
+    int done;  // reached its end time / step limit or failed (set by finalize)
+    int pad;
+};
+
+struct WorkItem {
+    int inst, x0, y0, dim;
+};
+
+struct BatchCtl {
+    int n_items;
+    int n_inst;
+    int counters[8];  // work stealing: [0] dt, [1..4] stages, [5] copy
+    int active;       // instances stepping in the current step
+    int pad;
+};
+
+// ---------------------------------------------------------------- kernels
+
+__device__ __forceinline__ int steal(int* counter, int* slot) {
+    if (threadIdx.x == 0) *slot = atomicAdd(counter, 1);
+    __syncthreads();
+    const int item = *slot;
+    __syncthreads();
+    return item;
+}
+
+__device__ __forceinline__ StageView batch_stage_view(BatchInst& b, int stage, int time_id) {
+    StageView sv{};
+    sv.clock = &b.clock;
+    sv.flags = &b.flags;
+    sv.counters = nullptr;
+    sv.time_id = time_id;
+    sv.stage = stage;
+    sv.q0 = b.qn;
+    sv.r = nullptr;
+    sv.k = b.k;
+    sv.mode = MODE_FINAL;
+    sv.require_active = 0;
+    if (time_id == T_EULER) {
+        sv.qs = b.qn;
+        sv.qout = b.qa;
+    } else if (time_id == T_SSPRK3) {
+        const double base[3] = {0.0, 0.75, 1.0 / 3.0};
+        const double inc[3] = {1.0, 0.25, 2.0 / 3.0};
+        sv.base = base[stage];
+        sv.inc = inc[stage];
+        sv.qs = stage == 0 ? b.qn : (stage == 1 ? b.qa : b.qb);
+        sv.qout = stage == 0 ? b.qa : (stage == 1 ? b.qb : b.qn);
+    } else {
+        const double inc[4] = {0.5, 0.5, 1.0, 0.0};
+        sv.inc = inc[stage];
+        sv.qs = stage == 0 ? b.qn : (stage == 1 ? b.qa : (stage == 2 ? b.qb : b.qa));
+        sv.qout = stage == 0 ? b.qa : (stage == 1 ? b.qb : (stage == 2 ? b.qa : b.qn));
+    }
+    return sv;
+}
+
+template <int SCHEME, int FLUX, bool F32, int TX, int TY>
+__global__ void __launch_bounds__(TILE_THREADS, F32 ? 3 : 2)
+    batch_stage_kernel(BatchInst* inst, const WorkItem* items, BatchCtl* ctl, int stage, int time_id) {
+    using Tt = typename std::conditional<F32, float, double>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Tt* smem = reinterpret_cast<Tt*>(smem_raw);
+    __shared__ int slot;
+    const int n_items = ctl->n_items;
+    for (;;) {
+        const int it = steal(&ctl->counters[1 + stage], &slot);
+        if (it >= n_items) break;
+        const WorkItem w = items[it];
+        BatchInst& b = inst[w.inst];
+        if (!b.live || !b.clock.active) continue;  // uniform across the block
+        StageView sv = batch_stage_view(b, stage, time_id);
+        unsigned flags = 0, cut = 0, cores = 0;
+        if (w.dim == 2) {
+            if constexpr (F32) tile2d_f32_body<SCHEME, FLUX, TX, TY>(b.g, sv, w.x0, w.y0, smem, flags, cut, cores);
+            else tile2d_body<SCHEME, FLUX, TX, TY>(b.g, sv, w.x0, w.y0, smem, flags, cut, cores);
+        } else {
+            tile1d_body<SCHEME, FLUX, Tt>(b.g, sv, w.x0, smem, flags, cut, cores);
+        }
+        if (flags) atomicOr(&b.flags, flags);
+        __syncthreads();  // shared arrays are reused by the next tile
+    }
+}
+
+// CFL step per instance over its tiles (RusanovEOS::deltaT).
+template <int TX, int TY>
+__global__ void __launch_bounds__(TILE_THREADS) batch_dt_kernel(BatchInst* inst, const WorkItem* items, BatchCtl* ctl) {
+    __shared__ int slot;
+    __shared__ double wmin[TILE_THREADS / 32];
+    const int n_items = ctl->n_items;
+    for (;;) {
+        const int it = steal(&ctl->counters[0], &slot);
+        if (it >= n_items) break;
+        const WorkItem w = items[it];
+        BatchInst& b = inst[w.inst];
+        if (!b.live || b.done) continue;
+        const GridView& g = b.g;
+        const int cnt = w.dim == 2 ? TX * TY : TILE1D;
+        double best = 1.7976931348623157e308;
+        unsigned fl = 0;
+        for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
+            const int i = w.dim == 2 ? w.x0 + t % TX : w.x0 + t;
+            const int j = w.dim == 2 ? w.y0 + t / TX : 0;
+            if (i >= g.hi[0] || (w.dim == 2 && j >= g.hi[1])) continue;
+            const long long node = (long long)j * g.n[0] + i;
+            const double* q = b.qn;
+            const double rho = q[node];
+            const double u = q[g.vs + node] / rho, v = q[2 * g.vs + node] / rho, ww = q[3 * g.vs + node] / rho;
+            const double kin = 0.5 * rho * (u * u + v * v + ww * ww);
+            const double e = (q[4 * g.vs + node] - kin) / rho;
+            const double p = (g.gamma - 1.0) * rho * e;
+            const double c = sqrt(g.gamma * p / rho);
+            double sr = 0.0;
+            sr += fabs(u * g.metric[0]) + c * g.metric[0];
+            if (g.dim > 1) sr += fabs(v * g.metric[1]) + c * g.metric[1];
+            if (!(sr > 0.0) || !isfinite(sr)) fl |= FLAG_NONFINITE;
+            const double cand = g.cfl / sr;
+            best = cand < best ? cand : best;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double other = __shfl_xor_sync(0xffffffffu, best, o);
+            best = other < best ? other : best;
+        }
+        if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = best;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int k = 1; k < TILE_THREADS / 32; ++k) best = wmin[k] < best ? wmin[k] : best;
+            atomicMin(&b.clock.dt_bits, (unsigned long long)__double_as_longlong(best));
+        }
+        if (fl) atomicOr(&b.flags, fl);
+        __syncthreads();
+    }
+}
+
+// FlowDtCompute + Time::Driver clipping per instance (one thread each).
+__global__ void batch_finalize_kernel(BatchInst* inst, BatchCtl* ctl) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ctl->n_inst) return;
+    BatchInst& b = inst[i];
+    if (!b.live || b.done) return;
+    Clock* c = &b.clock;
+    const double eps = 2.220446049250313e-16;
+    const double remaining = c->t_end - c->t;
+    double scale = fmax(fabs(c->t), fabs(c->t_end));
+    scale = scale < 1.0 ? 1.0 : scale;
+    if (b.flags || !(remaining > 64.0 * eps * scale) || c->steps >= c->max_steps) {
+        c->active = 0;
+        c->dt = 0.0;
+        b.done = 1;
+        return;
+    }
+    double limit = remaining;
+    if (c->write_interval > 0.0 && c->next_out - c->t < limit) limit = c->next_out - c->t;
+    double dt = __longlong_as_double((long long)c->dt_bits);
+    if (c->max_dt < dt) dt = c->max_dt;
+    if (limit < dt) dt = limit;
+    c->dt = dt;
+    c->active = 1;
+    atomicAdd(&ctl->active, 1);
+}
+
+// Euler: the stage wrote qa; the committed state lives in qn.
+template <int TX, int TY>
+__global__ void __launch_bounds__(TILE_THREADS) batch_copy_kernel(BatchInst* inst, const WorkItem* items, BatchCtl* ctl) {
+    __shared__ int slot;
+    const int n_items = ctl->n_items;
+    for (;;) {
+        const int it = steal(&ctl->counters[5], &slot);
+        if (it >= n_items) break;
+        const WorkItem w = items[it];
+        BatchInst& b = inst[w.inst];
+        if (!b.live || !b.clock.active) continue;
+        const int cnt = w.dim == 2 ? TX * TY : TILE1D;
+        for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
+            const int i = w.dim == 2 ? w.x0 + t % TX : w.x0 + t;
+            const int j = w.dim == 2 ? w.y0 + t / TX : 0;
+            if (i >= b.g.hi[0] || (w.dim == 2 && j >= b.g.hi[1])) continue;
+            const long long node = (long long)j * b.g.n[0] + i;
+            for (int v = 0; v < 5; ++v) b.qn[v * b.g.vs + node] = b.qa[v * b.g.vs + node];
+        }
+    }
+}
+
+// TimeCommit per instance; re-arms the per-step counters (one grid).
+__global__ void batch_commit_kernel(BatchInst* inst, BatchCtl* ctl) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < ctl->n_inst) {
+        BatchInst& b = inst[i];
+        if (b.live) {
+            Clock* c = &b.clock;
+            if (c->active) {
+                c->t += c->dt;
+                c->steps += 1;
+                double sc = fabs(c->t);
+                sc = sc < 1.0 ? 1.0 : sc;
+                if (c->write_interval > 0.0 && c->t >= c->next_out - 1.0e-11 * sc) c->next_out += c->write_interval;
+            }
+            c->dt_bits = 0x7FEFFFFFFFFFFFFFull;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x < 8) ctl->counters[threadIdx.x] = 0;
+}
+
+__global__ void batch_reset_active_kernel(BatchCtl* ctl) { ctl->active = 0; }
+
+}  // namespace sfg
+
+using namespace sfg;
+
+// ---------------------------------------------------------------- host
+
+namespace {
+
+int bfail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    set_last_error(buf);
+    return code;
+}
+
+#define BCUDA(expr)                                                                              \
+    do {                                                                                         \
+        cudaError_t e_ = (expr);                                                                 \
+        if (e_ != cudaSuccess) return bfail(SFG_ERR_CUDA, "%s: %s", #expr, cudaGetErrorString(e_)); \
+    } while (0)
+
+struct RecipeParts {
+    int id, scheme, flux;
+};
+const RecipeParts kBatchRecipes[] = {
+    {SFG_RECIPE_WENO3_RUSANOV, WENO3, RUSANOV}, {SFG_RECIPE_WENO3_ROE, WENO3, ROE},
+    {SFG_RECIPE_WENO5_RUSANOV, WENO5, RUSANOV}, {SFG_RECIPE_WENO5_ROE, WENO5, ROE},
+    {SFG_RECIPE_TENO5_RUSANOV, TENO5, RUSANOV}, {SFG_RECIPE_TENO5_ROE, TENO5, ROE},
+    {SFG_RECIPE_WENO7_RUSANOV, WENO7, RUSANOV}, {SFG_RECIPE_WENO7_ROE, WENO7, ROE}};
+
+using StageKernel = void (*)(BatchInst*, const WorkItem*, BatchCtl*, int, int);
+using ItemKernel = void (*)(BatchInst*, const WorkItem*, BatchCtl*);
+
+template <int TX, int TY, bool F32>
+StageKernel pick_stage(int scheme, int flux) {
+#define SFG_PICK(S)                                                                              \
+    if (scheme == S) return flux == RUSANOV ? batch_stage_kernel<S, RUSANOV, F32, TX, TY>        \
+                                            : batch_stage_kernel<S, ROE, F32, TX, TY>;
+    SFG_PICK(WENO5)
+    SFG_PICK(TENO5)
+    SFG_PICK(WENO3)
+    SFG_PICK(WENO7)
+#undef SFG_PICK
+    return nullptr;
+}
+
+template <int TX, int TY>
+size_t stage_smem(int scheme, bool f32) {
+    size_t e2 = 0, e1 = 0;
+    switch (scheme) {
+    case WENO3: e2 = TileShape<WENO3, TX, TY>::ELEMS; e1 = Tile1Shape<WENO3>::ELEMS; break;
+    case WENO5: e2 = TileShape<WENO5, TX, TY>::ELEMS; e1 = Tile1Shape<WENO5>::ELEMS; break;
+    case TENO5: e2 = TileShape<TENO5, TX, TY>::ELEMS; e1 = Tile1Shape<TENO5>::ELEMS; break;
+    default: e2 = TileShape<WENO7, TX, TY>::ELEMS; e1 = Tile1Shape<WENO7>::ELEMS; break;
+    }
+    return std::max(e2, e1) * (f32 ? sizeof(float) : sizeof(double));
+}
+
+int stage_count_of(int time_id) { return time_id == T_EULER ? 1 : (time_id == T_SSPRK3 ? 3 : 4); }
+
+const double kInfB = std::numeric_limits<double>::infinity();
+
+}  // namespace
+
+struct sfg_batch_s {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    sfg_numerics_desc num{};
+    const RecipeParts* recipe = nullptr;
+    int variant = 1;  // 1: 30 x 16 tiles, 2: 22 x 22
+    int tx = 30, ty = 16;
+    int max_inst = 0;
+    // HBM slab for instance state, first-fit allocator over it
+    char* slab = nullptr;
+    size_t budget = 0, used = 0;
+    std::map<size_t, size_t> free_blocks;  // offset -> size
+    // tables
+    BatchInst* d_inst = nullptr;
+    std::vector<BatchInst> h_inst;
+    std::vector<size_t> inst_offset, inst_bytes;
+    WorkItem* d_items = nullptr;
+    size_t items_cap = 0;
+    std::vector<WorkItem> h_items;
+    BatchCtl* d_ctl = nullptr;
+    BatchCtl* h_ctl = nullptr;  // pinned
+    double* staging = nullptr;
+    size_t staging_cap = 0;
+    // kernels and graph
+    StageKernel stage_k = nullptr;
+    ItemKernel dt_k = nullptr, copy_k = nullptr;
+    size_t smem = 0;
+    int grid_stage = 0, grid_items = 0;
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+    long long batch_steps = 0;
+};
+
+namespace {
+
+int bind_kernels(sfg_batch_s* b) {
+    const bool f32 = b->num.precision == SFG_PREC_FP32_FLUX;
+    if (b->variant == 1) {
+        b->stage_k = f32 ? pick_stage<30, 16, true>(b->recipe->scheme, b->recipe->flux)
+                         : pick_stage<30, 16, false>(b->recipe->scheme, b->recipe->flux);
+        b->smem = stage_smem<30, 16>(b->recipe->scheme, f32);
+        b->dt_k = batch_dt_kernel<30, 16>;
+        b->copy_k = batch_copy_kernel<30, 16>;
+        b->tx = 30;
+        b->ty = 16;
+    } else {
+        b->stage_k = f32 ? pick_stage<22, 22, true>(b->recipe->scheme, b->recipe->flux)
+                         : pick_stage<22, 22, false>(b->recipe->scheme, b->recipe->flux);
+        b->smem = stage_smem<22, 22>(b->recipe->scheme, f32);
+        b->dt_k = batch_dt_kernel<22, 22>;
+        b->copy_k = batch_copy_kernel<22, 22>;
+        b->tx = 22;
+        b->ty = 22;
+    }
+    BCUDA(cudaFuncSetAttribute(b->stage_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
+    int sms = 0, per_sm = 0;
+    BCUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
+    BCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, b->stage_k, TILE_THREADS, b->smem));
+    if (per_sm < 1) return bfail(SFG_ERR_CUDA, "batched stage kernel does not fit an SM");
+    b->grid_stage = sms * per_sm;
+    b->grid_items = sms * 4;
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    return SFG_OK;
+}
+
+int slab_alloc(sfg_batch_s* b, size_t bytes, size_t* off) {
+    bytes = (bytes + 255) / 256 * 256;
+    for (auto it = b->free_blocks.begin(); it != b->free_blocks.end(); ++it) {
+        if (it->second >= bytes) {
+            *off = it->first;
+            const size_t rest = it->second - bytes;
+            const size_t roff = it->first + bytes;
+            b->free_blocks.erase(it);
+            if (rest) b->free_blocks[roff] = rest;
+            b->used += bytes;
+            return SFG_OK;
+        }
+    }
+    return bfail(SFG_ERR_BUDGET, "HBM budget exhausted: %zu bytes requested, %zu of %zu in use", bytes, b->used,
+                 b->budget);
+}
+
+void slab_free(sfg_batch_s* b, size_t off, size_t bytes) {
+    bytes = (bytes + 255) / 256 * 256;
+    b->used -= bytes;
+    auto it = b->free_blocks.emplace(off, bytes).first;
+    auto next = std::next(it);
+    if (next != b->free_blocks.end() && it->first + it->second == next->first) {
+        it->second += next->second;
+        b->free_blocks.erase(next);
+    }
+    if (it != b->free_blocks.begin()) {
+        auto prev = std::prev(it);
+        if (prev->first + prev->second == it->first) {
+            prev->second += it->second;
+            b->free_blocks.erase(it);
+        }
+    }
+}
+
+// Rebuilds the tile list of all live instances and publishes it (and the
+// instance count) to device memory.
+int publish_items(sfg_batch_s* b) {
+    b->h_items.clear();
+    for (int i = 0; i < (int)b->h_inst.size(); ++i) {
+        const BatchInst& r = b->h_inst[i];
+        if (!r.live || r.done) continue;
+        const GridView& g = r.g;
+        if (g.dim == 1) {
+            for (int x = g.lo[0]; x < g.hi[0]; x += TILE1D) b->h_items.push_back({i, x, 0, 1});
+        } else {
+            for (int y = g.lo[1]; y < g.hi[1]; y += b->ty)
+                for (int x = g.lo[0]; x < g.hi[0]; x += b->tx) b->h_items.push_back({i, x, y, 2});
+        }
+    }
+    if (b->h_items.size() > b->items_cap) {
+        size_t cap = std::max<size_t>(b->h_items.size() * 2, 1024);
+        if (b->d_items) cudaFree(b->d_items);
+        b->d_items = nullptr;
+        BCUDA(cudaMalloc((void**)&b->d_items, cap * sizeof(WorkItem)));
+        b->items_cap = cap;
+        if (b->graph) {  // the graph holds the old list address
+            cudaGraphExecDestroy(b->graph);
+            b->graph = nullptr;
+        }
+    }
+    if (!b->h_items.empty())
+        BCUDA(cudaMemcpyAsync(b->d_items, b->h_items.data(), b->h_items.size() * sizeof(WorkItem),
+                              cudaMemcpyHostToDevice, b->stream));
+    b->h_ctl->n_items = (int)b->h_items.size();
+    b->h_ctl->n_inst = (int)b->h_inst.size();
+    BCUDA(cudaMemcpyAsync(&b->d_ctl->n_items, &b->h_ctl->n_items, 2 * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+    BCUDA(cudaStreamSynchronize(b->stream));
+    return SFG_OK;
+}
+
+int enqueue_batch_step(sfg_batch_s* b) {
+    const int ni = std::max<int>(1, b->max_inst);
+    batch_reset_active_kernel<<<1, 1, 0, b->stream>>>(b->d_ctl);
+    b->dt_k<<<b->grid_items, TILE_THREADS, 0, b->stream>>>(b->d_inst, b->d_items, b->d_ctl);
+    batch_finalize_kernel<<<(ni + 127) / 128, 128, 0, b->stream>>>(b->d_inst, b->d_ctl);
+    const int ns = stage_count_of(b->num.time_recipe);
+    for (int s = 0; s < ns; ++s)
+        b->stage_k<<<b->grid_stage, TILE_THREADS, b->smem, b->stream>>>(b->d_inst, b->d_items, b->d_ctl, s,
+                                                                           b->num.time_recipe);
+    if (b->num.time_recipe == T_EULER) b->copy_k<<<b->grid_items, TILE_THREADS, 0, b->stream>>>(b->d_inst, b->d_items, b->d_ctl);
+    batch_commit_kernel<<<(ni + 127) / 128, 128, 0, b->stream>>>(b->d_inst, b->d_ctl);
+    BCUDA(cudaGetLastError());
+    return SFG_OK;
+}
+
+int batch_grid_view(const sfg_grid_desc* d, const sfg_numerics_desc* n, int reach, GridView* out, long long* nodes) {
+    if (!d) return bfail(SFG_ERR_ARG, "null grid");
+    if (d->dim < 1 || d->dim > 2) return bfail(SFG_ERR_ARG, "batched grids are 1-D or 2-D (got %d)", d->dim);
+    GridView g{};
+    g.dim = d->dim;
+    for (int a = 0; a < 3; ++a) {
+        if (!(d->h[a] > 0.0)) return bfail(SFG_ERR_ARG, "h[%d] must be > 0", a);
+        g.n[a] = d->n[a];
+        if (a >= d->dim) {
+            if (d->n[a] != 1) return bfail(SFG_ERR_ARG, "inactive axis %d must have 1 node", a);
+            g.lo[a] = 0;
+            g.hi[a] = 1;
+            continue;
+        }
+        const bool plo = d->bc_lo[a] == SFG_BC_PERIODIC, phi = d->bc_hi[a] == SFG_BC_PERIODIC;
+        if (plo != phi) return bfail(SFG_ERR_ARG, "axis %d: periodic must be set on both ends", a);
+        for (int bk : {d->bc_lo[a], d->bc_hi[a]})
+            if (bk != SFG_BC_TRANSMISSIVE && bk != SFG_BC_PERIODIC) return bfail(SFG_ERR_ARG, "unknown boundary kind");
+        if (plo ? d->n[a] < reach + 1 : d->n[a] < 3) return bfail(SFG_ERR_ARG, "axis %d has too few nodes", a);
+        g.bc_lo[a] = d->bc_lo[a];
+        g.bc_hi[a] = d->bc_hi[a];
+        g.lo[a] = plo ? 0 : 1;
+        g.hi[a] = plo ? d->n[a] : d->n[a] - 1;
+    }
+    const double hx = d->h[0], hy = d->h[1], hz = d->h[2];
+    g.jac = 1.0 / (hx * hy * hz);
+    g.metric[0] = (hy * hz) * g.jac;
+    g.metric[1] = (hx * hz) * g.jac;
+    g.metric[2] = (hx * hy) * g.jac;
+    for (int a = 0; a < 3; ++a) g.area[a] = 0.5 * (g.metric[a] / g.jac + g.metric[a] / g.jac);
+    g.gamma = n->gamma;
+    g.cfl = n->cfl;
+    *nodes = (long long)d->n[0] * d->n[1] * d->n[2];
+    g.vs = (*nodes + 31) / 32 * 32;
+    *out = g;
+    return SFG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sfg_batch_create(const sfg_numerics_desc* numerics, size_t hbm_budget_bytes, int max_instances, void* stream,
+                     sfg_batch* out) {
+    if (!numerics || !out) return bfail(SFG_ERR_ARG, "null argument");
+    *out = nullptr;
+    const RecipeParts* rp = nullptr;
+    for (const auto& r : kBatchRecipes)
+        if (r.id == numerics->recipe) rp = &r;
+    if (!rp) return bfail(SFG_ERR_ARG, "convection recipe %d is not provided on the GPU", numerics->recipe);
+    if (numerics->time_recipe < 0 || numerics->time_recipe > 2) return bfail(SFG_ERR_ARG, "unknown time recipe");
+    if (numerics->precision != SFG_PREC_FP64 && numerics->precision != SFG_PREC_FP32_FLUX)
+        return bfail(SFG_ERR_ARG, "unknown precision");
+    if (!(numerics->gamma > 1.0) || !(numerics->cfl > 0.0)) return bfail(SFG_ERR_ARG, "gamma > 1 and CFL > 0 required");
+    if (max_instances < 1 || max_instances > (1 << 20)) return bfail(SFG_ERR_ARG, "max_instances out of range");
+    if (hbm_budget_bytes < (1u << 20)) return bfail(SFG_ERR_ARG, "HBM budget below 1 MiB");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return bfail(SFG_ERR_CUDA, "no CUDA device: the B200 provider has no CPU fallback");
+    auto* b = new sfg_batch_s;
+    b->num = *numerics;
+    if (!(b->num.max_dt > 0.0)) b->num.max_dt = kInfB;
+    b->recipe = rp;
+    b->max_inst = max_instances;
+    cudaGetDevice(&b->device);
+    auto cleanup = [&](int code) {
+        sfg_batch_destroy(b);
+        return code;
+    };
+    if (stream) {
+        b->stream = (cudaStream_t)stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
+            return cleanup(bfail(SFG_ERR_CUDA, "stream creation failed"));
+        b->own_stream = true;
+    }
+    b->budget = hbm_budget_bytes / 256 * 256;
+    if (cudaMalloc((void**)&b->slab, b->budget) != cudaSuccess)
+        return cleanup(bfail(SFG_ERR_NOMEM, "cannot reserve the HBM budget of %zu bytes", b->budget));
+    b->free_blocks[0] = b->budget;
+    if (cudaMalloc((void**)&b->d_inst, sizeof(BatchInst) * (size_t)max_instances) != cudaSuccess ||
+        cudaMalloc((void**)&b->d_ctl, sizeof(BatchCtl)) != cudaSuccess ||
+        cudaMallocHost((void**)&b->h_ctl, sizeof(BatchCtl)) != cudaSuccess)
+        return cleanup(bfail(SFG_ERR_NOMEM, "device allocation failed"));
+    cudaMemsetAsync(b->d_inst, 0, sizeof(BatchInst) * (size_t)max_instances, b->stream);
+    cudaMemsetAsync(b->d_ctl, 0, sizeof(BatchCtl), b->stream);
+    std::memset(b->h_ctl, 0, sizeof(BatchCtl));
+    int rc = bind_kernels(b);
+    if (rc) return cleanup(rc);
+    rc = publish_items(b);
+    if (rc) return cleanup(rc);
+    *out = b;
+    return SFG_OK;
+}
+
+int sfg_batch_destroy(sfg_batch b) {
+    if (!b) return SFG_OK;
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    if (b->slab) cudaFree(b->slab);
+    if (b->d_inst) cudaFree(b->d_inst);
+    if (b->d_items) cudaFree(b->d_items);
+    if (b->d_ctl) cudaFree(b->d_ctl);
+    if (b->staging) cudaFree(b->staging);
+    if (b->h_ctl) cudaFreeHost(b->h_ctl);
+    if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return SFG_OK;
+}
+
+int sfg_batch_instance_bytes(sfg_batch b, const sfg_grid_desc* grid, size_t* bytes) {
+    if (!b || !grid || !bytes) return bfail(SFG_ERR_ARG, "null argument");
+    GridView g;
+    long long nodes = 0;
+    const int reach = b->recipe->scheme == WENO3 ? 2 : (b->recipe->scheme == WENO7 ? 4 : 3);
+    int rc = batch_grid_view(grid, &b->num, reach, &g, &nodes);
+    if (rc) return rc;
+    const int bufs = b->num.time_recipe == T_RK4 ? 4 : 3;
+    *bytes = ((sizeof(double) * 5 * (size_t)g.vs + 255) / 256 * 256) * bufs;
+    return SFG_OK;
+}
+
+int sfg_batch_add(sfg_batch b, const sfg_grid_desc* grid, const double* host_nodes_aos, double t_end,
+                  int64_t max_steps, int* slot) {
+    if (!b || !grid || !host_nodes_aos || !slot) return bfail(SFG_ERR_ARG, "null argument");
+    GridView g;
+    long long nodes = 0;
+    const int reach = b->recipe->scheme == WENO3 ? 2 : (b->recipe->scheme == WENO7 ? 4 : 3);
+    int rc = batch_grid_view(grid, &b->num, reach, &g, &nodes);
+    if (rc) return rc;
+    int idx = -1;
+    for (int i = 0; i < (int)b->h_inst.size(); ++i)
+        if (!b->h_inst[i].live) {
+            idx = i;
+            break;
+        }
+    if (idx < 0) {
+        if ((int)b->h_inst.size() >= b->max_inst) return bfail(SFG_ERR_BUDGET, "all %d instance slots in use", b->max_inst);
+        idx = (int)b->h_inst.size();
+        b->h_inst.push_back(BatchInst{});
+        b->inst_offset.push_back(0);
+        b->inst_bytes.push_back(0);
+    }
+    const size_t per = (sizeof(double) * 5 * (size_t)g.vs + 255) / 256 * 256;
+    const int bufs = b->num.time_recipe == T_RK4 ? 4 : 3;
+    size_t off = 0;
+    rc = slab_alloc(b, per * bufs, &off);
+    if (rc) return rc;
+    const size_t aos_bytes = sizeof(double) * 5 * (size_t)nodes;
+    if (aos_bytes > b->staging_cap) {
+        if (b->staging) cudaFree(b->staging);
+        b->staging = nullptr;
+        b->staging_cap = 0;
+        if (cudaMalloc((void**)&b->staging, aos_bytes) != cudaSuccess) {
+            slab_free(b, off, per * bufs);
+            return bfail(SFG_ERR_NOMEM, "staging allocation failed");
+        }
+        b->staging_cap = aos_bytes;
+    }
+    BatchInst r{};
+    r.g = g;
+    r.qn = reinterpret_cast<double*>(b->slab + off);
+    r.qa = reinterpret_cast<double*>(b->slab + off + per);
+    r.qb = reinterpret_cast<double*>(b->slab + off + 2 * per);
+    r.k = bufs == 4 ? reinterpret_cast<double*>(b->slab + off + 3 * per) : nullptr;
+    std::memset(&r.clock, 0, sizeof r.clock);
+    r.clock.t = 0.0;
+    r.clock.t_end = t_end;
+    r.clock.next_out = kInfB;
+    r.clock.max_dt = b->num.max_dt;
+    r.clock.limit = kInfB;
+    r.clock.dt_bits = 0x7FEFFFFFFFFFFFFFull;
+    r.clock.max_steps = max_steps > 0 ? max_steps : std::numeric_limits<long long>::max();
+    r.clock.active = 0;
+    r.flags = 0;
+    r.live = 1;
+    BCUDA(cudaMemcpyAsync(b->staging, host_nodes_aos, aos_bytes, cudaMemcpyHostToDevice, b->stream));
+    if (launch_aos_to_soa(b->staging, r.qn, nodes, g.vs, b->stream) != cudaSuccess)
+        return bfail(SFG_ERR_CUDA, "upload transpose failed");
+    BCUDA(cudaMemcpyAsync(b->d_inst + idx, &r, sizeof r, cudaMemcpyHostToDevice, b->stream));
+    b->h_inst[idx] = r;
+    b->inst_offset[idx] = off;
+    b->inst_bytes[idx] = per * bufs;
+    rc = publish_items(b);  // synchronises the stream
+    if (rc) return rc;
+    *slot = idx;
+    return SFG_OK;
+}
+
+int sfg_batch_remove(sfg_batch b, int slot) {
+    if (!b || slot < 0 || slot >= (int)b->h_inst.size() || !b->h_inst[slot].live)
+        return bfail(SFG_ERR_NOT_FOUND, "no live instance in slot %d", slot);
+    BCUDA(cudaStreamSynchronize(b->stream));
+    b->h_inst[slot].live = 0;
+    const int zero = 0;
+    BCUDA(cudaMemcpy(&b->d_inst[slot].live, &zero, sizeof zero, cudaMemcpyHostToDevice));
+    slab_free(b, b->inst_offset[slot], b->inst_bytes[slot]);
+    return publish_items(b);
+}
+
+int sfg_batch_step(sfg_batch b, int steps, int graph_steps, int* active) {
+    if (!b) return bfail(SFG_ERR_ARG, "null batch");
+    if (graph_steps <= 0) graph_steps = 16;
+    if (!b->graph || b->graph_steps != graph_steps) {
+        if (b->graph) cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+        cudaGraph_t g;
+        BCUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        int crc = SFG_OK;
+        for (int i = 0; i < graph_steps && !crc; ++i) crc = enqueue_batch_step(b);
+        cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+        if (crc) return crc;
+        if (e != cudaSuccess) return bfail(SFG_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&b->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return bfail(SFG_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+        b->graph_steps = graph_steps;
+    }
+    int done = 0, last_active = -1;
+    while (done < steps) {
+        if (steps - done >= graph_steps) {
+            BCUDA(cudaGraphLaunch(b->graph, b->stream));
+            done += graph_steps;
+        } else {
+            int rc = enqueue_batch_step(b);
+            if (rc) return rc;
+            done += 1;
+        }
+        BCUDA(cudaMemcpyAsync(b->h_ctl, b->d_ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, b->stream));
+        BCUDA(cudaStreamSynchronize(b->stream));
+        const int now = b->h_ctl->active;
+        if (last_active < 0 || now < last_active) {
+            // some instances finished: drop their tiles from the work list
+            std::vector<BatchInst> tmp(b->h_inst.size());
+            if (!tmp.empty()) {
+                BCUDA(cudaMemcpy(tmp.data(), b->d_inst, tmp.size() * sizeof(BatchInst), cudaMemcpyDeviceToHost));
+                bool changed = false;
+                for (size_t i = 0; i < tmp.size(); ++i)
+                    if (b->h_inst[i].live && tmp[i].done && !b->h_inst[i].done) {
+                        b->h_inst[i].done = 1;
+                        changed = true;
+                    }
+                if (changed) {
+                    int rc = publish_items(b);
+                    if (rc) return rc;
+                }
+            }
+        }
+        last_active = now;
+        if (now == 0) break;  // every live instance has finished
+    }
+    b->batch_steps += done;
+    if (active) *active = b->h_ctl->active;
+    return SFG_OK;
+}
+
+int sfg_batch_status(sfg_batch b, int slot, double* time, int64_t* steps, int* running, uint32_t* flags) {
+    if (!b || slot < 0 || slot >= (int)b->h_inst.size() || !b->h_inst[slot].live)
+        return bfail(SFG_ERR_NOT_FOUND, "no live instance in slot %d", slot);
+    BatchInst r;
+    BCUDA(cudaMemcpyAsync(&r, b->d_inst + slot, sizeof r, cudaMemcpyDeviceToHost, b->stream));
+    BCUDA(cudaStreamSynchronize(b->stream));
+    if (time) *time = r.clock.t;
+    if (steps) *steps = r.clock.steps;
+    if (flags) *flags = r.flags;
+    if (running) {
+        const double eps = 2.220446049250313e-16;
+        double scale = std::max({std::fabs(r.clock.t), std::fabs(r.clock.t_end), 1.0});
+        const bool finished = !(r.clock.t_end - r.clock.t > 64.0 * eps * scale) || r.clock.steps >= r.clock.max_steps;
+        *running = (finished || r.flags) ? 0 : 1;
+    }
+    return SFG_OK;
+}
+
+int sfg_batch_download(sfg_batch b, int slot, double* host_nodes_aos) {
+    if (!b || !host_nodes_aos) return bfail(SFG_ERR_ARG, "null argument");
+    if (slot < 0 || slot >= (int)b->h_inst.size() || !b->h_inst[slot].live)
+        return bfail(SFG_ERR_NOT_FOUND, "no live instance in slot %d", slot);
+    const BatchInst& r = b->h_inst[slot];
+    const long long nodes = (long long)r.g.n[0] * r.g.n[1] * r.g.n[2];
+    const size_t bytes = sizeof(double) * 5 * (size_t)nodes;
+    if (launch_soa_to_aos(r.g, r.qn, b->staging, b->stream) != cudaSuccess)
+        return bfail(SFG_ERR_CUDA, "download transpose failed");
+    BCUDA(cudaMemcpyAsync(host_nodes_aos, b->staging, bytes, cudaMemcpyDeviceToHost, b->stream));
+    BCUDA(cudaStreamSynchronize(b->stream));
+    return SFG_OK;
+}
+
+int sfg_batch_set_variant(sfg_batch b, int variant) {
+    if (!b) return bfail(SFG_ERR_ARG, "null batch");
+    if (variant != 1 && variant != 2) return bfail(SFG_ERR_ARG, "batched tile variant must be 1 or 2");
+    if (variant == b->variant) return SFG_OK;
+    b->variant = variant;
+    int rc = bind_kernels(b);
+    if (rc) return rc;
+    return publish_items(b);
+}
+
+int sfg_batch_snapshot(sfg_batch b, int count, int* running, double* time, int64_t* steps, uint32_t* flags) {
+    if (!b || count < 0) return bfail(SFG_ERR_ARG, "bad argument");
+    const int n = std::min<int>(count, (int)b->h_inst.size());
+    if (n == 0) return SFG_OK;
+    std::vector<BatchInst> tmp(n);
+    BCUDA(cudaMemcpyAsync(tmp.data(), b->d_inst, n * sizeof(BatchInst), cudaMemcpyDeviceToHost, b->stream));
+    BCUDA(cudaStreamSynchronize(b->stream));
+    for (int i = 0; i < n; ++i) {
+        const bool live = b->h_inst[i].live != 0;
+        const Clock& c = tmp[i].clock;
+        const double eps = 2.220446049250313e-16;
+        const double scale = std::max({std::fabs(c.t), std::fabs(c.t_end), 1.0});
+        const bool finished = !(c.t_end - c.t > 64.0 * eps * scale) || c.steps >= c.max_steps;
+        if (running) running[i] = live ? ((finished || tmp[i].flags) ? 0 : 1) : -1;
+        if (time) time[i] = c.t;
+        if (steps) steps[i] = c.steps;
+        if (flags) flags[i] = tmp[i].flags;
+    }
+    return SFG_OK;
+}
+
+int sfg_batch_info(sfg_batch b, size_t* used_bytes, size_t* budget_bytes, int* live, int* items) {
+    if (!b) return bfail(SFG_ERR_ARG, "null batch");
+    if (used_bytes) *used_bytes = b->used;
+    if (budget_bytes) *budget_bytes = b->budget;
+    if (live) {
+        int n = 0;
+        for (const auto& r : b->h_inst) n += r.live;
+        *live = n;
+    }
+    if (items) *items = (int)b->h_items.size();
+    return SFG_OK;
+}
+
+}  // extern "C"

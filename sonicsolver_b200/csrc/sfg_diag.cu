@@ -2,9 +2,113 @@
 // FP32 roof of the flux kernels) and per-sweep timing on the solver stream.
 #include "../../include/sonicsolver_b200.h"
 #include "sfg_internal.h"
+#include "sfg_math.cuh"
+#include "sfg_stage.cuh"
 
 #include <cstdio>
 #include <string>
+
+namespace sfg {
+
+// TENO5 cut-off decisions of the same stencils evaluated in FP64 (the plain
+// path) and in FP32 (the FP32-flux path's arithmetic: FP32 deviations from
+// the FP64 face average): out[0] += decisions (3 per scalar core, 30 per
+// face), out[1] += decisions that differ.
+template <int AX>
+__device__ __forceinline__ void teno_flips_face(const GridView& g, const double* q, int i, int j, int k,
+                                                unsigned long long& dec, unsigned long long& flips) {
+    constexpr int NST = 6, CL = 2;
+    double st[NST][5];
+    const int n = g.n[AX];
+    int base_idx[3] = {i, j, k};
+    for (int s = 0; s < NST; ++s) {
+        int c[3] = {base_idx[0], base_idx[1], base_idx[2]};
+        c[AX] = map_index(base_idx[AX] - 3 + s, n, g.bc_lo[AX], g.bc_hi[AX]);
+        const long long node = ((long long)c[2] * g.n[1] + c[1]) * g.n[0] + c[0];
+        for (int v = 0; v < 5; ++v) st[s][v] = q[v * g.vs + node];
+    }
+    double qbar[5];
+    float qbar32[5];
+    for (int v = 0; v < 5; ++v) {
+        qbar[v] = 0.5 * (st[CL][v] + st[CL + 1][v]);
+        qbar32[v] = float(qbar[v]);
+    }
+    Eigen<double> e64;
+    Eigen<float> e32;
+    eigen_at<AX, double>(qbar, g.gamma, e64);
+    eigen_at<AX, float>(qbar32, float(g.gamma), e32);
+    double c64[NST][5];
+    float c32[NST][5];
+    for (int s = 0; s < NST; ++s) {
+        float d[5];
+        for (int v = 0; v < 5; ++v) d[v] = float(st[s][v] - qbar[v]);
+        to_characteristic<AX, double>(e64, st[s], c64[s]);
+        to_characteristic<AX, float>(e32, d, c32[s]);
+    }
+    unsigned fl = 0;
+    for (int v = 0; v < 5; ++v)
+        for (int side = 0; side < 2; ++side) {
+            double a[5];
+            float b[5];
+            for (int s = 0; s < 5; ++s) {
+                a[s] = side ? c64[NST - 1 - s][v] : c64[s][v];
+                b[s] = side ? c32[NST - 1 - s][v] : c32[s][v];
+            }
+            double a0, a1, a2;
+            float b0, b1, b2;
+            teno_betas<double>(a, a0, a1, a2);
+            teno_betas<float>(b, b0, b1, b2);
+            const int m64 = Teno<double>::keep_mask(a0, a1, a2, fl);
+            const int m32 = Teno<float>::keep_mask(b0, b1, b2, fl);
+            dec += 3;
+            flips += __popc(m64 ^ m32);
+        }
+}
+
+__global__ void teno_flips_kernel(GridView g, const double* q, unsigned long long* out) {
+    unsigned long long dec = 0, flips = 0;
+    const long long cx = g.hi[0] - g.lo[0], cy = g.hi[1] - g.lo[1], cz = g.hi[2] - g.lo[2];
+    for (int ax = 0; ax < g.dim; ++ax) {
+        // faces between node f-1 and f for f in [lo, hi] along ax, solved nodes across
+        const long long fa = (ax == 0 ? cx : (ax == 1 ? cy : cz)) + 1;
+        const long long total = fa * (ax == 0 ? cy * cz : (ax == 1 ? cx * cz : cx * cy));
+        for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+             t += (long long)gridDim.x * blockDim.x) {
+            int i, j, k;
+            if (ax == 0) {
+                i = g.lo[0] + (int)(t % fa);
+                j = g.lo[1] + (int)((t / fa) % cy);
+                k = g.lo[2] + (int)(t / (fa * cy));
+                teno_flips_face<0>(g, q, i, j, k, dec, flips);
+            } else if (ax == 1) {
+                i = g.lo[0] + (int)(t % cx);
+                j = g.lo[1] + (int)((t / cx) % fa);
+                k = g.lo[2] + (int)(t / (cx * fa));
+                teno_flips_face<1>(g, q, i, j, k, dec, flips);
+            } else {
+                i = g.lo[0] + (int)(t % cx);
+                j = g.lo[1] + (int)((t / cx) % cy);
+                k = g.lo[2] + (int)(t / (cx * cy));
+                teno_flips_face<2>(g, q, i, j, k, dec, flips);
+            }
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        dec += __shfl_xor_sync(0xffffffffu, dec, o);
+        flips += __shfl_xor_sync(0xffffffffu, flips, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(out, dec);
+        atomicAdd(out + 1, flips);
+    }
+}
+
+cudaError_t launch_teno_flips(const GridView& g, const double* q, unsigned long long* out, cudaStream_t st) {
+    teno_flips_kernel<<<148 * 4, 256, 0, st>>>(g, q, out);
+    return cudaGetLastError();
+}
+
+}  // namespace sfg
 
 namespace {
 

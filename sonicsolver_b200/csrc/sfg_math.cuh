@@ -217,38 +217,57 @@ __device__ __forceinline__ T weno7_core(const T* v, unsigned& flags) {
 }
 
 // TENO5 (SF_TENO5.cpp:44-92): C = 1, q = 6, eps = 1e-40, CT = 1e-5.
-// FP64 keeps the reference's gamma_k = (1 + tau5/(b_k+eps))^6 and tests
-// gamma_k < CT * sum(gamma) (the reference divides; the comparison is the same
-// up to rounding at the threshold).  `cut` accumulates the number of cut
-// sub-stencils.
+// keep_mask() is the cut-off decision alone (bit k set = sub-stencil k kept);
+// core() is the reconstruction built on it.  `cut` accumulates the number of
+// cut sub-stencils.
+template <typename T>
+__device__ __forceinline__ void teno_betas(const T* v, T& b0, T& b1, T& b2) {
+    const T t0 = v[0] - T(2) * v[1] + v[2], r0 = v[0] - T(4) * v[1] + T(3) * v[2];
+    const T t1 = v[1] - T(2) * v[2] + v[3], r1 = v[1] - v[3];
+    const T t2 = v[2] - T(2) * v[3] + v[4], r2 = T(3) * v[2] - T(4) * v[3] + v[4];
+    const T c13 = T(13.0 / 12.0);
+    b0 = c13 * (t0 * t0) + T(0.25) * (r0 * r0);
+    b1 = c13 * (t1 * t1) + T(0.25) * (r1 * r1);
+    b2 = c13 * (t2 * t2) + T(0.25) * (r2 * r2);
+}
+
 template <typename T> struct Teno;
 
+// FP64 keeps the reference's gamma_k = (1 + tau5/(b_k+eps))^6 and tests
+// gamma_k < CT * sum(gamma) (the reference divides; the comparison is the same
+// up to rounding at the threshold).
 template <> struct Teno<double> {
-    static __device__ __forceinline__ double core(const double* v, unsigned& flags, unsigned& cut) {
-        const double p0 = 2.0 * v[0] - 7.0 * v[1] + 11.0 * v[2];
-        const double p1 = -v[1] + 5.0 * v[2] + 2.0 * v[3];
-        const double p2 = 2.0 * v[2] + 5.0 * v[3] - v[4];
-        const double t0 = v[0] - 2.0 * v[1] + v[2], r0 = v[0] - 4.0 * v[1] + 3.0 * v[2];
-        const double t1 = v[1] - 2.0 * v[2] + v[3], r1 = v[1] - v[3];
-        const double t2 = v[2] - 2.0 * v[3] + v[4], r2 = 3.0 * v[2] - 4.0 * v[3] + v[4];
-        const double c13 = 13.0 / 12.0;
-        const double b0 = c13 * (t0 * t0) + 0.25 * (r0 * r0);
-        const double b1 = c13 * (t1 * t1) + 0.25 * (r1 * r1);
-        const double b2 = c13 * (t2 * t2) + 0.25 * (r2 * r2);
+    static __device__ __forceinline__ int keep_mask(double b0, double b1, double b2, unsigned& flags) {
         const double tau = fabs(b0 - b2);
-        const double g0 = 1.0 + tau / (b0 + 1e-40);
-        const double g1 = 1.0 + tau / (b1 + 1e-40);
-        const double g2 = 1.0 + tau / (b2 + 1e-40);
+        // tau/e_k for the three sub-stencils from one reciprocal of the
+        // product e0 e1 e2 (>= 1e-120, no underflow in FP64)
+        const double e0 = b0 + 1e-40, e1 = b1 + 1e-40, e2 = b2 + 1e-40;
+        const double e12 = e1 * e2;
+        const double ti = tau / (e0 * e12);
+        const double g0 = 1.0 + ti * e12;
+        const double g1 = 1.0 + ti * (e0 * e2);
+        const double g2 = 1.0 + ti * (e0 * e1);
         const double q0 = g0 * g0 * g0, q1 = g1 * g1 * g1, q2 = g2 * g2 * g2;
         const double G0 = q0 * q0, G1 = q1 * q1, G2 = q2 * q2;
         const double lim = 1e-5 * (G0 + G1 + G2);
         if (!finite_(lim)) flags |= FLAG_NONFINITE;
-        const bool k0 = !(G0 < lim), k1 = !(G1 < lim), k2 = !(G2 < lim);
-        cut += (!k0) + (!k1) + (!k2);
-        const double d0 = k0 ? 0.1 : 0.0, d1 = k1 ? 0.6 : 0.0, d2 = k2 ? 0.3 : 0.0;
-        const double act = d0 + d1 + d2;
-        if (!(act > 0.0)) { flags |= FLAG_TENO_CUTOFF; return 0.0; }
-        return (d0 * p0 + d1 * p1 + d2 * p2) / (6.0 * act);
+        return int(!(G0 < lim)) | (int(!(G1 < lim)) << 1) | (int(!(G2 < lim)) << 2);
+    }
+    static __device__ __forceinline__ double core(const double* v, unsigned& flags, unsigned& cut) {
+        const double p0 = 2.0 * v[0] - 7.0 * v[1] + 11.0 * v[2];
+        const double p1 = -v[1] + 5.0 * v[2] + 2.0 * v[3];
+        const double p2 = 2.0 * v[2] + 5.0 * v[3] - v[4];
+        double b0, b1, b2;
+        teno_betas<double>(v, b0, b1, b2);
+        const int m = keep_mask(b0, b1, b2, flags);
+        cut += 3 - __popc(m);
+        if (m == 0) { flags |= FLAG_TENO_CUTOFF; return 0.0; }
+        // 1 / (6 * sum of the kept linear weights), by kept set (selects, no
+        // indexed local array)
+        const double inv6act = m == 7 ? 1.0 / 6.0 : m == 6 ? 1.0 / 5.4 : m == 5 ? 1.0 / 2.4 : m == 4 ? 1.0 / 1.8
+                             : m == 3 ? 1.0 / 4.2 : m == 2 ? 1.0 / 3.6 : 1.0 / 0.6;
+        const double d0 = (m & 1) ? 0.1 : 0.0, d1 = (m & 2) ? 0.6 : 0.0, d2 = (m & 4) ? 0.3 : 0.0;
+        return (d0 * p0 + d1 * p1 + d2 * p2) * inv6act;
     }
 };
 
@@ -262,43 +281,33 @@ template <> struct Teno<double> {
 //                       is below the threshold);
 //   otherwise        -> r_k^6 < CT * sum_j r_j^6 with sum >= 1.
 template <> struct Teno<float> {
+    static __device__ __forceinline__ int keep_mask(float b0, float b1, float b2, unsigned& flags) {
+        const float tau = fabsf(b0 - b2);
+        if (!(tau > 0.f)) return 7;
+        // division by a subnormal b+eps gives +inf here: the "dominant" case
+        const float g0 = 1.f + __fdividef(tau, b0 + 1e-40f);
+        const float g1 = 1.f + __fdividef(tau, b1 + 1e-40f);
+        const float g2 = 1.f + __fdividef(tau, b2 + 1e-40f);
+        const float gm = fmaxf(g0, fmaxf(g1, g2));
+        if (!(gm <= 3.0e38f))
+            return int(!(g0 <= 3.0e38f)) | (int(!(g1 <= 3.0e38f)) << 1) | (int(!(g2 <= 3.0e38f)) << 2);
+        const float im = __frcp_rn(gm);
+        const float x0 = g0 * im, x1 = g1 * im, x2 = g2 * im;
+        const float y0 = x0 * x0 * x0, y1 = x1 * x1 * x1, y2 = x2 * x2 * x2;
+        const float G0 = y0 * y0, G1 = y1 * y1, G2 = y2 * y2;
+        const float lim = 1e-5f * (G0 + G1 + G2);
+        if (!finite_(lim)) flags |= FLAG_NONFINITE;
+        return int(!(G0 < lim)) | (int(!(G1 < lim)) << 1) | (int(!(G2 < lim)) << 2);
+    }
     static __device__ __forceinline__ float core(const float* v, unsigned& flags, unsigned& cut) {
         const float p0 = 2.f * v[0] - 7.f * v[1] + 11.f * v[2];
         const float p1 = -v[1] + 5.f * v[2] + 2.f * v[3];
         const float p2 = 2.f * v[2] + 5.f * v[3] - v[4];
-        const float t0 = v[0] - 2.f * v[1] + v[2], r0 = v[0] - 4.f * v[1] + 3.f * v[2];
-        const float t1 = v[1] - 2.f * v[2] + v[3], r1 = v[1] - v[3];
-        const float t2 = v[2] - 2.f * v[3] + v[4], r2 = 3.f * v[2] - 4.f * v[3] + v[4];
-        const float c13 = 13.f / 12.f;
-        const float b0 = c13 * (t0 * t0) + 0.25f * (r0 * r0);
-        const float b1 = c13 * (t1 * t1) + 0.25f * (r1 * r1);
-        const float b2 = c13 * (t2 * t2) + 0.25f * (r2 * r2);
-        const float tau = fabsf(b0 - b2);
-        bool k0 = true, k1 = true, k2 = true;
-        if (tau > 0.f) {
-            // division by a subnormal b+eps gives +inf here: the "dominant" case
-            const float g0 = 1.f + __fdividef(tau, b0 + 1e-40f);
-            const float g1 = 1.f + __fdividef(tau, b1 + 1e-40f);
-            const float g2 = 1.f + __fdividef(tau, b2 + 1e-40f);
-            const float gm = fmaxf(g0, fmaxf(g1, g2));
-            if (!(gm <= 3.0e38f)) {
-                k0 = !(g0 <= 3.0e38f);
-                k1 = !(g1 <= 3.0e38f);
-                k2 = !(g2 <= 3.0e38f);
-            } else {
-                const float im = __frcp_rn(gm);
-                const float x0 = g0 * im, x1 = g1 * im, x2 = g2 * im;
-                const float y0 = x0 * x0 * x0, y1 = x1 * x1 * x1, y2 = x2 * x2 * x2;
-                const float G0 = y0 * y0, G1 = y1 * y1, G2 = y2 * y2;
-                const float lim = 1e-5f * (G0 + G1 + G2);
-                if (!finite_(lim)) flags |= FLAG_NONFINITE;
-                k0 = !(G0 < lim);
-                k1 = !(G1 < lim);
-                k2 = !(G2 < lim);
-            }
-        }
-        cut += (!k0) + (!k1) + (!k2);
-        const float d0 = k0 ? 0.1f : 0.f, d1 = k1 ? 0.6f : 0.f, d2 = k2 ? 0.3f : 0.f;
+        float b0, b1, b2;
+        teno_betas<float>(v, b0, b1, b2);
+        const int m = keep_mask(b0, b1, b2, flags);
+        cut += 3 - __popc(m);
+        const float d0 = (m & 1) ? 0.1f : 0.f, d1 = (m & 2) ? 0.6f : 0.f, d2 = (m & 4) ? 0.3f : 0.f;
         const float act = d0 + d1 + d2;
         if (!(act > 0.f)) { flags |= FLAG_TENO_CUTOFF; return 0.f; }
         return __fdividef(d0 * p0 + d1 * p1 + d2 * p2, 6.f * act);
@@ -453,6 +462,178 @@ __device__ __forceinline__ void face_flux(const double (&st)[SchemeInfo<SCHEME>:
 #pragma unroll
     for (int v = 0; v < 5; ++v)
         if (!finite_(F[v])) flags |= FLAG_NONFINITE;
+}
+
+// Reference state of a tile in FP32 with its velocity and pressure.
+struct Ref32 {
+    float q[5];
+    float u[3];
+    float p;
+};
+
+__device__ __forceinline__ Ref32 make_ref32(const double (&qref)[5], double gamma) {
+    Ref32 r;
+    const double inv = 1.0 / qref[0];
+    const double u0 = qref[1] * inv, u1 = qref[2] * inv, u2 = qref[3] * inv;
+    const double p = (gamma - 1.0) * (qref[4] - 0.5 * (qref[1] * u0 + qref[2] * u1 + qref[3] * u2));
+    for (int v = 0; v < 5; ++v) r.q[v] = float(qref[v]);
+    r.u[0] = float(u0);
+    r.u[1] = float(u1);
+    r.u[2] = float(u2);
+    r.p = float(p);
+    return r;
+}
+
+// Physical Euler flux along axis AX of q = q_ref + d, returned as the
+// deviation F(q) - F(q_ref), in algebra that never forms a small difference
+// of large terms:
+//   du = (d_m - u_ref d_rho) / rho,  u = u_ref + du
+//   d(m.u) = m_ref.du + d_m.u,  dp = (gamma - 1)(d_E - d(m.u)/2)
+//   dF_rho = d_m_n,  dF_m = m_ref du_n + d_m u_n + dp e_n,
+//   dF_E = (E_ref + p_ref) du_n + (d_E + dp) u_n.
+// Also gives u_n and the sound speed of q.
+template <int AX>
+__device__ __forceinline__ void phys_flux_dev(const Ref32& r, const float d[5], float gamma, float F[5], float& un,
+                                              float& c, float& p_out, unsigned& flags) {
+    constexpr int N = AxisBasis<AX>::N;
+    const float rho = r.q[0] + d[0];
+    const float irho = __frcp_rn(rho);
+    float du[3], u[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        du[k] = (d[1 + k] - r.u[k] * d[0]) * irho;
+        u[k] = r.u[k] + du[k];
+    }
+    const float dmu = r.q[1] * du[0] + r.q[2] * du[1] + r.q[3] * du[2] + d[1] * u[0] + d[2] * u[1] + d[3] * u[2];
+    const float dp = (gamma - 1.f) * (d[4] - 0.5f * dmu);
+    const float p = r.p + dp;
+    if (!(rho > 0.f)) flags |= FLAG_DENSITY;
+    if (!(p > 0.f)) flags |= FLAG_PRESSURE;
+    const float dun = du[N - 1];
+    un = u[N - 1];
+    F[0] = d[N];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) F[1 + k] = r.q[1 + k] * dun + d[1 + k] * un + (k == N - 1 ? dp : 0.f);
+    F[4] = (r.q[4] + r.p) * dun + (d[4] + dp) * un;
+    c = sqrtf(gamma * p * irho);
+    p_out = p;
+}
+
+// Rusanov flux deviation F-hat(q_ref + dL, q_ref + dR) - F(q_ref): the
+// central part from phys_flux_dev, the dissipation from dR - dL.
+template <int AX>
+__device__ __forceinline__ void rusanov_dev(const Ref32& r, const float dL[5], const float dR[5], float gamma,
+                                            float F[5], unsigned& flags) {
+    float fL[5], fR[5], unL, unR, cL, cR, pL, pR;
+    phys_flux_dev<AX>(r, dL, gamma, fL, unL, cL, pL, flags);
+    phys_flux_dev<AX>(r, dR, gamma, fR, unR, cR, pR, flags);
+    const float hl = 0.5f * fmaxf(fabsf(unL) + cL, fabsf(unR) + cR);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) F[v] = 0.5f * (fL[v] + fR[v]) - hl * (dR[v] - dL[v]);
+}
+
+// Roe flux deviation: Roe average and eigen-structure from the absolute
+// states, jump dR - dL, central part from phys_flux_dev.
+template <int AX>
+__device__ __forceinline__ void roe_dev(const Ref32& r, const float dL[5], const float dR[5], float gamma, float F[5],
+                                        unsigned& flags) {
+    constexpr int N = AxisBasis<AX>::N;
+    float qL[5], qR[5], fL[5], fR[5], unL, unR, cL, cR, pL, pR;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+        qL[v] = r.q[v] + dL[v];
+        qR[v] = r.q[v] + dR[v];
+    }
+    phys_flux_dev<AX>(r, dL, gamma, fL, unL, cL, pL, flags);
+    phys_flux_dev<AX>(r, dR, gamma, fR, unR, cR, pR, flags);
+    const float gm1 = gamma - 1.f;
+    const float iL = __frcp_rn(qL[0]), iR = __frcp_rn(qR[0]);
+    const float hL = (qL[4] + pL) * iL, hR = (qR[4] + pR) * iR;
+    const float sL = sqrtf(qL[0]), sR = sqrtf(qR[0]);
+    const float iS = __frcp_rn(sL + sR);
+    const float ur = (sL * qL[1] * iL + sR * qR[1] * iR) * iS;
+    const float vr = (sL * qL[2] * iL + sR * qR[2] * iR) * iS;
+    const float wr = (sL * qL[3] * iL + sR * qR[3] * iR) * iS;
+    const float hr = (sL * hL + sR * hR) * iS;
+    const float q2 = ur * ur + vr * vr + wr * wr;
+    const float a2 = gm1 * (hr - 0.5f * q2);
+    if (!(a2 > 0.f) || !isfinite(a2)) flags |= FLAG_ROE_SOUND;
+    const float rr = sL * sR;
+    float qr[5] = {rr, rr * ur, rr * vr, rr * wr, rr * (0.5f * q2 + __fdividef(a2, gm1))};
+    Eigen<float> e;
+    eigen_at<AX, float>(qr, gamma, e);
+    const float a = sqrtf(a2);
+    const float un = (N == 1 ? ur : (N == 2 ? vr : wr));
+    const float lam[5] = {un, un, un, un + a, un - a};
+    const float delta = 0.1f * a;
+    float dq[5], alpha[5], s[5], diss[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) dq[v] = dR[v] - dL[v];
+    to_characteristic<AX, float>(e, dq, alpha);
+#pragma unroll
+    for (int m = 0; m < 5; ++m) {
+        const float val = fabsf(lam[m]);
+        const float ab = val < 2.f * delta ? 0.5f * (val * val * __frcp_rn(2.f * delta) + delta) : val;
+        s[m] = ab * alpha[m];
+    }
+    from_characteristic<AX, float>(e, s, diss);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) F[v] = 0.5f * (fL[v] + fR[v] - diss[v]);
+}
+
+// FP32 face flux from a stencil held as FP32 deviations d_s = q_s - q_ref
+// from a reference state shared by a whole tile (q_ref is FP64 in HBM; only
+// the deviations are rounded to FP32, once per node when the tile is staged).
+// Same mathematics as face_flux: q-bar = q_ref + (d_CL + d_CL+1)/2, the
+// projection and reconstruction act on d_s - d-bar.  Returns the flux as a
+// deviation from F(q_ref) (rusanov_dev / roe_dev): within a tile the
+// reference flux cancels exactly in every difference dF, so FP32 rounding
+// scales with the variation across the tile, not with |F|.
+template <int AX, int SCHEME, int FLUX>
+__device__ __forceinline__ void face_flux_dev32(const float (&d)[SchemeInfo<SCHEME>::NST][5], const Ref32& ref,
+                                                float gamma, float F[5], unsigned& flags, unsigned& cut) {
+    const float (&qref)[5] = ref.q;
+    constexpr int NST = SchemeInfo<SCHEME>::NST;
+    constexpr int W = SchemeInfo<SCHEME>::W;
+    constexpr int CL = NST / 2 - 1;
+    float dbar[5], qbar[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+        dbar[v] = 0.5f * (d[CL][v] + d[CL + 1][v]);
+        qbar[v] = qref[v] + dbar[v];
+    }
+    Eigen<float> e;
+    if (!eigen_at<AX, float>(qbar, gamma, e)) flags |= FLAG_PRESSURE;
+    float ch[NST][5];
+#pragma unroll
+    for (int s = 0; s < NST; ++s) {
+        float dd[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) dd[v] = d[s][v] - dbar[v];
+        to_characteristic<AX, float>(e, dd, ch[s]);
+    }
+    float wl[5], wr[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+        float sl[W], sr[W];
+#pragma unroll
+        for (int s = 0; s < W; ++s) {
+            sl[s] = ch[s][v];
+            sr[s] = ch[NST - 1 - s][v];
+        }
+        wl[v] = recon_core<SCHEME, float>(sl, flags, cut);
+        wr[v] = recon_core<SCHEME, float>(sr, flags, cut);
+    }
+    float dl[5], dr[5], xl[5], xr[5];
+    from_characteristic<AX, float>(e, wl, dl);
+    from_characteristic<AX, float>(e, wr, dr);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {  // face states as deviations from q_ref
+        xl[v] = dbar[v] + dl[v];
+        xr[v] = dbar[v] + dr[v];
+    }
+    if constexpr (FLUX == RUSANOV) rusanov_dev<AX>(ref, xl, xr, gamma, F, flags);
+    else roe_dev<AX>(ref, xl, xr, gamma, F, flags);
 }
 
 }  // namespace sfg

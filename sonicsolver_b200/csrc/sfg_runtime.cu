@@ -32,6 +32,10 @@ cudaError_t launch_stage_from_residual(const GridView& g, const StageView& sv, c
 cudaError_t launch_aos_to_soa(const double* aos, double* soa, long long nodes, long long vs, cudaStream_t st);
 cudaError_t launch_soa_to_aos(const GridView& g, const double* soa, double* aos, cudaStream_t st);
 cudaError_t launch_totals(const GridView& g, const double* q, double* out, double vol, cudaStream_t st);
+cudaError_t launch_tile2d(int variant, int scheme, int flux, int prec64, const GridView& g, const StageView& sv,
+                          cudaStream_t st);
+cudaError_t launch_tile1d(int scheme, int flux, int prec64, const GridView& g, const StageView& sv, cudaStream_t st);
+cudaError_t launch_teno_flips(const GridView& g, const double* q, unsigned long long* out, cudaStream_t st);
 }  // namespace sfg
 
 using namespace sfg;
@@ -108,6 +112,7 @@ struct sfg_solver_s {
     unsigned* flags = nullptr;
     unsigned long long* counters = nullptr;
     bool counting = false;
+    int variant = 0;  // stage-operator kernel variant (sfg_set_kernel_variant)
     int next_stage = 0;
     double stage_dt = 0.0;
     // graph of `graph_steps` steps for sfg_advance
@@ -231,6 +236,18 @@ StageView stage_view(sfg_solver_s* s, int stage, bool residual_only, bool requir
 int enqueue_stage(sfg_solver_s* s, int stage, bool residual_only, bool require_active) {
     StageView sv = stage_view(s, stage, residual_only, require_active);
     const int dim = s->grid.dim;
+    if (dim == 2 && s->variant > 0) {
+        sv.mode = MODE_FINAL | (residual_only ? MODE_RESIDUAL : 0);
+        CUDA_TRY(launch_tile2d(s->variant, s->recipe->scheme, s->recipe->flux, s->num.precision == SFG_PREC_FP64,
+                               s->gv, sv, s->stream));
+        return SFG_OK;
+    }
+    if (dim == 1 && s->variant > 0) {
+        sv.mode = MODE_FINAL | (residual_only ? MODE_RESIDUAL : 0);
+        CUDA_TRY(launch_tile1d(s->recipe->scheme, s->recipe->flux, s->num.precision == SFG_PREC_FP64, s->gv, sv,
+                               s->stream));
+        return SFG_OK;
+    }
     for (int axis = 0; axis < dim; ++axis) {
         sv.mode = (axis > 0 ? MODE_READ_R : 0) | (axis == dim - 1 ? MODE_FINAL : 0) |
                   (residual_only && axis == dim - 1 ? MODE_RESIDUAL : 0);
@@ -361,6 +378,7 @@ int sfg_create(const sfg_grid_desc* grid, const sfg_numerics_desc* numerics, voi
     s->recipe = recipe;
     s->ng = ghost_layers(recipe->scheme);
     make_view(s);
+    s->variant = grid->dim <= 2 ? 1 : 0;
     cudaGetDevice(&s->device);
     auto cleanup = [&](int code) {
         sfg_destroy(s);
@@ -767,6 +785,24 @@ int sfg_time_sweeps(sfg_solver s, int stage, double dt, int repeats, float* ms_p
     double acc[3] = {0, 0, 0};
     CUDA_TRY(launch_set_dt(s->clock, dt, s->stream));
     StageView sv = stage_view(s, stage, false, false);
+    if (dim <= 2 && s->variant > 0) {  // one fused launch per stage
+        for (int r = 0; r < repeats; ++r) {
+            CUDA_TRY(cudaEventRecord(ev[0], s->stream));
+            int rc = enqueue_stage(s, stage, false, false);
+            if (rc) return rc;
+            CUDA_TRY(cudaEventRecord(ev[1], s->stream));
+            CUDA_TRY(cudaEventSynchronize(ev[1]));
+            float ms = 0.f;
+            CUDA_TRY(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+            acc[0] += ms;
+        }
+        for (auto& e : ev) cudaEventDestroy(e);
+        ms_per_axis[0] = (float)(acc[0] / repeats);
+        ms_per_axis[1] = 0.f;
+        CUDA_TRY(cudaMemsetAsync(s->flags, 0, 64, s->stream));
+        CUDA_TRY(cudaStreamSynchronize(s->stream));
+        return SFG_OK;
+    }
     for (int r = 0; r < repeats; ++r) {
         CUDA_TRY(cudaEventRecord(ev[0], s->stream));
         for (int axis = 0; axis < dim; ++axis) {
@@ -787,6 +823,40 @@ int sfg_time_sweeps(sfg_solver s, int stage, double dt, int repeats, float* ms_p
     // the timed stage was not committed: state and flags are left as they were
     CUDA_TRY(cudaMemsetAsync(s->flags, 0, 64, s->stream));
     CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return SFG_OK;
+}
+
+int sfg_teno_flip_rate(sfg_solver s, uint64_t* decisions, uint64_t* flips) {
+    if (!s || !decisions || !flips) return fail(SFG_ERR_ARG, "null argument");
+    *decisions = *flips = 0;
+    if (s->recipe->scheme != TENO5) return SFG_OK;
+    unsigned long long* out = reinterpret_cast<unsigned long long*>(s->totals);
+    CUDA_TRY(cudaMemsetAsync(out, 0, 2 * sizeof(unsigned long long), s->stream));
+    CUDA_TRY(launch_teno_flips(s->gv, s->qn, out, s->stream));
+    unsigned long long h[2];
+    CUDA_TRY(cudaMemcpyAsync(h, out, sizeof h, cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    *decisions = h[0];
+    *flips = h[1];
+    return SFG_OK;
+}
+
+int sfg_set_kernel_variant(sfg_solver s, int variant) {
+    if (!s) return fail(SFG_ERR_ARG, "null solver");
+    if (variant < 0 || variant > 2) return fail(SFG_ERR_ARG, "unknown kernel variant %d", variant);
+    if (variant > 0 && s->grid.dim == 3) return fail(SFG_ERR_ARG, "tile variants need a 1-D or 2-D grid");
+    if (variant == 2 && s->grid.dim != 2) return fail(SFG_ERR_ARG, "the 22 x 22 tile needs a 2-D grid");
+    if (variant != s->variant && s->graph) {
+        cudaGraphExecDestroy(s->graph);
+        s->graph = nullptr;
+    }
+    s->variant = variant;
+    return SFG_OK;
+}
+
+int sfg_get_kernel_variant(sfg_solver s, int* variant) {
+    if (!s || !variant) return fail(SFG_ERR_ARG, "null argument");
+    *variant = s->variant;
     return SFG_OK;
 }
 

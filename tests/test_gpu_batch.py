@@ -1,0 +1,147 @@
+"""Batched and served forms: every grid's result must be the same in the mix
+as alone (single-grid solver, same numerics) -- tolerance 1e-12 relative
+L-infinity per variable, the parity tolerance of the other GPU tests; step
+counts must match exactly."""
+import time
+
+import numpy as np
+import pytest
+
+from conftest import rel_linf
+from sonicsolver_b200 import capi, cases
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+
+
+def mix(seed=3, t_end=0.03):
+    """A small seeded mix: 1-D tubes of uneven length, 2-D slanted tubes, a
+    periodic vortex."""
+    tubes = cases.shock_tube_batch(count=8, seed=seed, t_end=t_end, max_1d=1500, max_2d=90)
+    vortex = cases.isentropic_vortex(48, recipe="weno5Rusanov", cfl=0.5, t_end=0.2)
+    return tubes + [vortex]
+
+
+def solo(case, precision=capi.PREC_FP64, recipe="weno5Rusanov", variant=1):
+    """The same grid alone.  FP32-flux results depend on the tile shape (the
+    per-tile reference state), so the solo run uses the batch's tile shape."""
+    s = capi.Solver(case.dim, case.n, case.h, case.bc_lo, case.bc_hi, recipe=recipe, time_recipe="SSPRK3",
+                    precision=precision, cfl=case.cfl)
+    if case.dim == 2:
+        s.variant = variant
+    s.upload(np.ascontiguousarray(case.q))
+    st, _ = s.advance(case.t_end)
+    return s.download().reshape(case.q.shape), st.steps
+
+
+@pytest.mark.parametrize("precision", [capi.PREC_FP64, capi.PREC_FP32_FLUX])
+@pytest.mark.parametrize("variant", [1, 2])
+def test_batch_results_equal_solo(precision, variant):
+    cs = mix()
+    b = capi.Batch(1 << 30, 64, recipe="weno5Rusanov", precision=precision, cfl=0.5)
+    b.variant = variant
+    slots = [b.add(c) for c in cs]
+    b.step(100000, graph_steps=8)
+    for c, slot in zip(cs, slots):
+        st = b.status(slot)
+        assert not st["running"] and st["flags"] == 0
+        assert abs(st["time"] - c.t_end) < 1e-12
+        want, steps = solo(c, precision, variant=variant)
+        assert st["steps"] == steps, c.name
+        assert rel_linf(b.download(slot), want).max() <= TOL, c.name
+
+
+def test_continuous_batching_add_and_remove_between_steps():
+    cs = mix(seed=5)
+    b = capi.Batch(1 << 30, 16)
+    first = {b.add(c): c for c in cs[:4]}
+    b.step(10, graph_steps=4)
+    later = {b.add(c): c for c in cs[4:]}
+    done = {}
+    for _ in range(10000):
+        active = b.step(8, graph_steps=8)
+        for slot in list(first) + list(later):
+            if slot in done:
+                continue
+            st = b.status(slot)
+            if not st["running"]:
+                done[slot] = (b.download(slot), st["steps"])
+                b.remove(slot)
+        if active == 0 and len(done) == len(cs):
+            break
+    assert len(done) == len(cs)
+    for slot, c in {**first, **later}.items():
+        want, steps = solo(c)
+        got, got_steps = done[slot]
+        assert got_steps == steps
+        assert rel_linf(got, want).max() <= TOL
+    assert b.info()["used"] == 0 and b.info()["live"] == 0
+
+
+def test_budget_rejects_and_others_continue():
+    c = cases.sod_1d(400, t_end=0.02)
+    b = capi.Batch(1 << 20, 64)   # 1 MiB, more slots than fit
+    need = b.instance_bytes(c)
+    fits = (1 << 20) // need
+    slots = [b.add(c) for _ in range(fits)]
+    with pytest.raises(capi.SolverError) as e:
+        b.add(c)
+    assert e.value.code == capi.ERR_BUDGET
+    b.step(100000)
+    want, steps = solo(c)
+    for s in slots:
+        assert rel_linf(b.download(s), want).max() <= TOL
+
+
+def test_failing_grid_is_isolated():
+    """A grid that goes invalid stops with its flags set; the others finish
+    exactly as alone (the reference would exit the whole process)."""
+    cs = mix(seed=7)
+    bad = cases.sod_1d(300, t_end=0.03)
+    bad.q[0, 0, 150, 4] = -1.0
+    b = capi.Batch(1 << 30, 32)
+    slots = [b.add(c) for c in cs]
+    bad_slot = b.add(bad)
+    b.step(100000)
+    st = b.status(bad_slot)
+    assert st["flags"] != 0 and not st["running"]
+    for c, slot in zip(cs, slots):
+        want, steps = solo(c)
+        assert b.status(slot)["steps"] == steps
+        assert rel_linf(b.download(slot), want).max() <= TOL
+
+
+def test_server_results_equal_solo_with_staggered_arrivals():
+    cs = mix(seed=11)
+    srv = capi.Server(1 << 30, 6, graph_steps=4)   # fewer slots than requests: queueing
+    ids = []
+    for c in cs:
+        ids.append(srv.submit(c))
+        time.sleep(0.002)                             # arrivals while others run
+    srv.drain(300)
+    for rid, c in zip(ids, cs):
+        info = srv.poll(rid)
+        assert info.state == capi.REQ_DONE
+        assert info.submit_s <= info.admit_s <= info.finish_s
+        want, steps = solo(c)
+        assert info.steps == steps
+        assert rel_linf(srv.fetch(rid), want).max() <= TOL
+    srv.close()
+
+
+def test_server_cancel_and_oversized_request():
+    c = cases.isentropic_vortex(48, t_end=5.0)
+    srv = capi.Server(64 << 20, 1, graph_steps=4)
+    a = srv.submit(c)
+    b = srv.submit(c)          # waits: one slot
+    srv.cancel(b)
+    srv.cancel(a)
+    srv.drain(120)
+    assert srv.poll(b).state == capi.REQ_CANCELLED
+    assert srv.poll(a).state == capi.REQ_CANCELLED
+    big = cases.isentropic_vortex(2048, t_end=1.0)
+    with pytest.raises(capi.SolverError) as e:
+        srv.submit(big)       # more than the whole budget
+    assert e.value.code == capi.ERR_BUDGET
+    srv.close()

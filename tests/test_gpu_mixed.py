@@ -56,6 +56,24 @@ def test_fp32_vortex_l1_within_1p5x_of_fp64():
     assert errs[capi.PREC_FP32_FLUX] <= 1.5 * errs[capi.PREC_FP64], errs
 
 
+def test_teno_flip_rate_diagnostic():
+    """30 decisions per face; a smooth vortex flips few of them, a shocked
+    state some; non-TENO recipes report none."""
+    c = cases.isentropic_vortex(64, recipe="teno5Rusanov")
+    s = c.solver()
+    dec, flips = s.teno_flips()
+    assert dec == 30 * 2 * 65 * 64   # faces f in [0, 64] per row (the wrap face counted at both ends)
+    assert flips <= dec * 0.02
+    q = smooth_state(2, (40, 30, 1), seed=2, shock=True)
+    s2 = capi.Solver(2, (40, 30, 1), (0.02, 0.02, 1.0), (0, 0, 0), (0, 0, 0), recipe="teno5Roe")
+    s2.upload(np.ascontiguousarray(q))
+    d2, f2 = s2.teno_flips()
+    assert d2 == 30 * ((38 + 1) * 28 + 38 * (28 + 1)) and 0 <= f2 < d2
+    s3 = capi.Solver(2, (40, 30, 1), (0.02, 0.02, 1.0), (0, 0, 0), (0, 0, 0), recipe="weno5Rusanov")
+    s3.upload(np.ascontiguousarray(q))
+    assert s3.teno_flips() == (0, 0)
+
+
 def test_fp32_vortex_far_field_has_no_nonfinite_flags():
     """Regression: near-uniform far field (smoothness indicators ~1e-26) must
     not produce 0/0 in the FP32 TENO cut-off test."""

@@ -51,6 +51,62 @@ def test_residual_parity(recipe, dim, n, h, bc, shock):
     assert err.max() <= TOL, (recipe, dim, bc, shock, err)
 
 
+@pytest.mark.parametrize("variant", [0, 1, 2])
+@pytest.mark.parametrize("recipe", ["weno5Rusanov", "teno5Roe", "weno7Rusanov", "weno3Rusanov"])
+@pytest.mark.parametrize("n", [(37, 29, 1), (64, 48, 1), (9, 40, 1)])
+@pytest.mark.parametrize("bc", [capi.BC_TRANSMISSIVE, capi.BC_PERIODIC])
+def test_2d_kernel_variants_match_oracle(variant, recipe, n, bc):
+    """Axis sweeps (0) and fused tile kernels (1: 30x16, 2: 22x22) on grids
+    smaller than, equal to and not a multiple of a tile, including periodic
+    axes shorter than the tile halo reach."""
+    h = (0.03, 0.02, 1.0)
+    s, spec, q = _pair(2, n, h, bc, recipe, shock=True, seed=9)
+    s.variant = variant
+    assert s.variant == variant
+    scheme, flux = split_recipe(recipe)
+    R_ref = from_oracle(spec, po.rhs(spec, SCHEME_OF[scheme], FLUX_OF[flux], to_oracle(spec, q)))
+    R_gpu = s.residual().reshape(R_ref.shape)
+    sl = tuple(slice(1, -1) if (d < 2 and bc == capi.BC_TRANSMISSIVE) else slice(None) for d in (2, 1, 0))
+    assert rel_linf(R_gpu[sl], R_ref[sl]).max() <= TOL
+    # one SSPRK3 step through the same variant
+    Q = to_oracle(spec, q)
+    dt = po.dt(spec, Q, 0.5)
+    po.Stepper(spec, SCHEME_OF[scheme], FLUX_OF[flux], po.SSPRK3).step(Q, dt)
+    s.step(dt)
+    assert rel_linf(s.download().reshape(q.shape), from_oracle(spec, Q)).max() <= TOL
+
+
+def test_variants_by_dimension():
+    s, _, _ = _pair(1, (61, 1, 1), (0.013, 1.0, 1.0), capi.BC_PERIODIC, "weno5Rusanov")
+    assert s.variant == 1
+    with pytest.raises(capi.SolverError):
+        s.variant = 2
+    s3, _, _ = _pair(3, (14, 12, 11), (0.05, 0.06, 0.07), capi.BC_PERIODIC, "weno5Rusanov")
+    assert s3.variant == 0
+    with pytest.raises(capi.SolverError):
+        s3.variant = 1
+
+
+@pytest.mark.parametrize("variant", [0, 1])
+@pytest.mark.parametrize("recipe", ["weno5Rusanov", "teno5Roe", "weno7Rusanov", "weno3Rusanov"])
+@pytest.mark.parametrize("n", [61, 511, 512, 1300])
+@pytest.mark.parametrize("bc", [capi.BC_TRANSMISSIVE, capi.BC_PERIODIC])
+def test_1d_kernel_variants_match_oracle(variant, recipe, n, bc):
+    """1-D sweeps (0) and 511-node tiles (1), grids below, at and above a tile."""
+    s, spec, q = _pair(1, (n, 1, 1), (1.0 / n, 1.0, 1.0), bc, recipe, shock=True, seed=4)
+    s.variant = variant
+    scheme, flux = split_recipe(recipe)
+    Q = to_oracle(spec, q)
+    R_ref = from_oracle(spec, po.rhs(spec, SCHEME_OF[scheme], FLUX_OF[flux], Q))
+    R_gpu = s.residual().reshape(R_ref.shape)
+    sl = (slice(None), slice(None), slice(1, -1) if bc == capi.BC_TRANSMISSIVE else slice(None))
+    assert rel_linf(R_gpu[sl], R_ref[sl]).max() <= TOL
+    dt = po.dt(spec, Q, 0.5)
+    po.Stepper(spec, SCHEME_OF[scheme], FLUX_OF[flux], po.SSPRK3).step(Q, dt)
+    s.step(dt)
+    assert rel_linf(s.download().reshape(q.shape), from_oracle(spec, Q)).max() <= TOL
+
+
 @pytest.mark.parametrize("time_recipe", ["forwardEuler", "SSPRK3", "classicalRK4"])
 @pytest.mark.parametrize("recipe", ["weno5Rusanov", "teno5Rusanov", "weno5Roe"])
 @pytest.mark.parametrize("dim,n,h", GRIDS)
