@@ -194,6 +194,8 @@ def run_ours(args, rank, world):
     torch.cuda.synchronize()
     with torch.cuda.stream(stream):
         s = case.solver(precision=prec, stream=ctypes_stream(stream))
+    from sonicsolver_b200 import autotune
+    tuned = autotune.tune_solver(s, "teno5Rusanov", prec)
     K, W = args.steps, args.warmup
     # warm-up (untimed): builds and caches the K-step graph shape too
     s.advance(1e30, max_steps=W, graph_steps=K)
@@ -216,6 +218,7 @@ def run_ours(args, rank, world):
            "config": {"workload": "isentropic_vortex_2d", "cells": f"{args.size}x{args.size}", "domain": "[0,10]^2",
                       "recipe": "teno5Rusanov", "time": "SSPRK3", "cfl": 0.4, "precision": args.precision,
                       "parallelism": f"replicas x{world}", "graph_steps": K, "kernel_variant": s.variant,
+                      "autotune_ms_per_stage": tuned.get("ms_per_stage"),
                       "l2": "inputs larger than L2 (4 x 42 MB state arrays touched per stage)"},
            "clocks": clk.summary(), "gpu_launches": None}
     dim = case.dim
@@ -343,8 +346,12 @@ def run_batched(args, precision):
     own CFL step; a bounded number of batch steps timed with CUDA events."""
     import torch
     from sonicsolver_b200 import capi, cases
+    from sonicsolver_b200 import autotune
     tubes = cases.shock_tube_batch(count=512, seed=2024, t_end=0.15)
+    variant = autotune.tune_batch(lambda: capi.Batch(8 << 30, 512, recipe="weno5Rusanov", precision=precision, cfl=0.5),
+                                  tubes[::8], "weno5Rusanov", precision)
     b = capi.Batch(8 << 30, 512, recipe="weno5Rusanov", precision=precision, cfl=0.5)
+    b.variant = variant
     slots = [b.add(c) for c in tubes]
     steps = args.batch_steps
     b.step(3, graph_steps=16)                     # warm-up (graph capture)
@@ -362,7 +369,7 @@ def run_batched(args, precision):
     b.close()
     return {"value": round(cell_steps / (ms * 1e-3) / 1e6, 2), "unit": "Mcell-steps/s", "batch_steps": steps,
             "instances": len(tubes), "cells_total": int(sum(c.cells for c in tubes)),
-            "tiles": info["items"], "ms": round(ms, 2),
+            "tiles": info["items"], "ms": round(ms, 2), "tile_variant": variant,
             "note": "default stream events around sfg_batch_step (graph of 16 steps, per-grid dt)"}
 
 

@@ -314,6 +314,78 @@ template <> struct Teno<float> {
     }
 };
 
+// FP64 left / right core pairs sharing one division: with x/a and y/b needed,
+// r = 1/(a b) gives x b r and y a r.  The WENO5 denominators lie in
+// [6e-25, ~1e33] and the TENO5 products e0 e1 e2 in [1e-120, ~1e24] for any
+// state the reference accepts, so a b stays inside FP64 range.
+__device__ __forceinline__ void weno5_pair64(const double* l, const double* r, double& wl, double& wr,
+                                             unsigned& flags) {
+    double num[2], den[2];
+    const double* v2[2] = {l, r};
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+        const double* v = v2[side];
+        const double p0 = 2.0 * v[0] - 7.0 * v[1] + 11.0 * v[2];
+        const double p1 = -v[1] + 5.0 * v[2] + 2.0 * v[3];
+        const double p2 = 2.0 * v[2] + 5.0 * v[3] - v[4];
+        const double t0 = v[0] - 2.0 * v[1] + v[2], r0 = v[0] - 4.0 * v[1] + 3.0 * v[2];
+        const double t1 = v[1] - 2.0 * v[2] + v[3], r1 = v[1] - v[3];
+        const double t2 = v[2] - 2.0 * v[3] + v[4], r2 = 3.0 * v[2] - 4.0 * v[3] + v[4];
+        const double c13 = 13.0 / 12.0;
+        const double b0 = c13 * (t0 * t0) + 0.25 * (r0 * r0);
+        const double b1 = c13 * (t1 * t1) + 0.25 * (r1 * r1);
+        const double b2 = c13 * (t2 * t2) + 0.25 * (r2 * r2);
+        const double s0 = (1e-6 + b0) * (1e-6 + b0), s1 = (1e-6 + b1) * (1e-6 + b1), s2 = (1e-6 + b2) * (1e-6 + b2);
+        const double w0 = 0.1 * (s1 * s2), w1 = 0.6 * (s0 * s2), w2 = 0.3 * (s0 * s1);
+        den[side] = 6.0 * (w0 + w1 + w2);
+        num[side] = w0 * p0 + w1 * p1 + w2 * p2;
+    }
+    const double inv = 1.0 / (den[0] * den[1]);
+    if (!(inv > 0.0) || !isfinite(inv)) flags |= FLAG_NONFINITE;
+    wl = num[0] * den[1] * inv;
+    wr = num[1] * den[0] * inv;
+}
+
+__device__ __forceinline__ void teno5_pair64(const double* l, const double* r, double& wl, double& wr,
+                                             unsigned& flags, unsigned& cut) {
+    double b[2][3], p[2][3], e[2][3], tau[2], prod[2];
+    const double* v2[2] = {l, r};
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+        const double* v = v2[side];
+        p[side][0] = 2.0 * v[0] - 7.0 * v[1] + 11.0 * v[2];
+        p[side][1] = -v[1] + 5.0 * v[2] + 2.0 * v[3];
+        p[side][2] = 2.0 * v[2] + 5.0 * v[3] - v[4];
+        teno_betas<double>(v, b[side][0], b[side][1], b[side][2]);
+        tau[side] = fabs(b[side][0] - b[side][2]);
+        for (int k = 0; k < 3; ++k) e[side][k] = b[side][k] + 1e-40;
+        prod[side] = e[side][0] * (e[side][1] * e[side][2]);
+    }
+    const double inv = 1.0 / (prod[0] * prod[1]);
+    double out[2];
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+        // tau / (e0 e1 e2) from the shared reciprocal
+        const double ti = tau[side] * prod[1 - side] * inv;
+        const double g0 = 1.0 + ti * (e[side][1] * e[side][2]);
+        const double g1 = 1.0 + ti * (e[side][0] * e[side][2]);
+        const double g2 = 1.0 + ti * (e[side][0] * e[side][1]);
+        const double q0 = g0 * g0 * g0, q1 = g1 * g1 * g1, q2 = g2 * g2 * g2;
+        const double G0 = q0 * q0, G1 = q1 * q1, G2 = q2 * q2;
+        const double lim = 1e-5 * (G0 + G1 + G2);
+        if (!isfinite(lim)) flags |= FLAG_NONFINITE;
+        const int m = int(!(G0 < lim)) | (int(!(G1 < lim)) << 1) | (int(!(G2 < lim)) << 2);
+        cut += 3 - __popc(m);
+        if (m == 0) flags |= FLAG_TENO_CUTOFF;
+        const double inv6act = m == 7 ? 1.0 / 6.0 : m == 6 ? 1.0 / 5.4 : m == 5 ? 1.0 / 2.4 : m == 4 ? 1.0 / 1.8
+                             : m == 3 ? 1.0 / 4.2 : m == 2 ? 1.0 / 3.6 : m == 1 ? 1.0 / 0.6 : 0.0;
+        const double d0 = (m & 1) ? 0.1 : 0.0, d1 = (m & 2) ? 0.6 : 0.0, d2 = (m & 4) ? 0.3 : 0.0;
+        out[side] = (d0 * p[side][0] + d1 * p[side][1] + d2 * p[side][2]) * inv6act;
+    }
+    wl = out[0];
+    wr = out[1];
+}
+
 template <int SCHEME, typename T>
 __device__ __forceinline__ T recon_core(const T* v, unsigned& flags, unsigned& cut) {
     if constexpr (SCHEME == WENO5) return weno5_core<T>(v, flags);
@@ -446,8 +518,14 @@ __device__ __forceinline__ void face_flux(const double (&st)[SchemeInfo<SCHEME>:
             sl[s] = ch[s][v];
             sr[s] = ch[NST - 1 - s][v];
         }
-        wl[v] = recon_core<SCHEME, T>(sl, flags, cut);
-        wr[v] = recon_core<SCHEME, T>(sr, flags, cut);
+        if constexpr (sizeof(T) == sizeof(double) && SCHEME == WENO5) {
+            weno5_pair64(sl, sr, wl[v], wr[v], flags);
+        } else if constexpr (sizeof(T) == sizeof(double) && SCHEME == TENO5) {
+            teno5_pair64(sl, sr, wl[v], wr[v], flags, cut);
+        } else {
+            wl[v] = recon_core<SCHEME, T>(sl, flags, cut);
+            wr[v] = recon_core<SCHEME, T>(sr, flags, cut);
+        }
     }
     T dl[5], dr[5], ql[5], qr[5];
     from_characteristic<AX, T>(e, wl, dl);
@@ -462,6 +540,107 @@ __device__ __forceinline__ void face_flux(const double (&st)[SchemeInfo<SCHEME>:
 #pragma unroll
     for (int v = 0; v < 5; ++v)
         if (!finite_(F[v])) flags |= FLAG_NONFINITE;
+}
+
+// ---------------------------------------------------------------------------
+// Paired FP32 arithmetic (sm_100 f32x2: one instruction, two lanes of work).
+// The left- and right-biased reconstructions of a face are the same
+// operations on mirrored stencils, so they run as the two halves of a float2.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 swap2(float2 a) { return make_float2(a.y, a.x); }
+
+// WENO5-JS on a (left, right) stencil pair; same folding as weno5_core.
+__device__ __forceinline__ float2 weno5_core2(const float2* v, unsigned& flags) {
+    const float2 p0 = fma2(f2(2.f), v[0], fma2(f2(-7.f), v[1], mul2(f2(11.f), v[2])));
+    const float2 p1 = fma2(f2(5.f), v[2], fma2(f2(2.f), v[3], sub2(f2(0.f), v[1])));
+    const float2 p2 = fma2(f2(2.f), v[2], fma2(f2(5.f), v[3], sub2(f2(0.f), v[4])));
+    const float2 t0 = add2(fma2(f2(-2.f), v[1], v[0]), v[2]);
+    const float2 r0 = fma2(f2(3.f), v[2], fma2(f2(-4.f), v[1], v[0]));
+    const float2 t1 = add2(fma2(f2(-2.f), v[2], v[1]), v[3]);
+    const float2 r1 = sub2(v[1], v[3]);
+    const float2 t2 = add2(fma2(f2(-2.f), v[3], v[2]), v[4]);
+    const float2 r2 = fma2(f2(3.f), v[2], fma2(f2(-4.f), v[3], v[4]));
+    const float2 c13 = f2(13.f / 12.f), q4 = f2(0.25f);
+    const float2 b0 = fma2(mul2(c13, t0), t0, mul2(mul2(q4, r0), r0));
+    const float2 b1 = fma2(mul2(c13, t1), t1, mul2(mul2(q4, r1), r1));
+    const float2 b2 = fma2(mul2(c13, t2), t2, mul2(mul2(q4, r2), r2));
+    const float2 e0 = add2(f2(1e-6f), b0), e1 = add2(f2(1e-6f), b1), e2 = add2(f2(1e-6f), b2);
+    const float2 s0 = mul2(e0, e0), s1 = mul2(e1, e1), s2 = mul2(e2, e2);
+    const float2 w0 = mul2(f2(0.1f), mul2(s1, s2));
+    const float2 w1 = mul2(f2(0.6f), mul2(s0, s2));
+    const float2 w2 = mul2(f2(0.3f), mul2(s0, s1));
+    const float2 den = mul2(f2(6.f), add2(add2(w0, w1), w2));
+    const float2 num = fma2(w0, p0, fma2(w1, p1, mul2(w2, p2)));
+    if (!(den.x > 0.f) || !(den.y > 0.f) || !isfinite(den.x) || !isfinite(den.y)) flags |= FLAG_NONFINITE;
+    return make_float2(__fdividef(num.x, den.x), __fdividef(num.y, den.y));
+}
+
+// TENO5 on a (left, right) stencil pair: polynomials and smoothness
+// indicators paired, the cut-off decision per side (Teno<float>::keep_mask).
+__device__ __forceinline__ float2 teno5_core2(const float2* v, unsigned& flags, unsigned& cut) {
+    const float2 p0 = fma2(f2(2.f), v[0], fma2(f2(-7.f), v[1], mul2(f2(11.f), v[2])));
+    const float2 p1 = fma2(f2(5.f), v[2], fma2(f2(2.f), v[3], sub2(f2(0.f), v[1])));
+    const float2 p2 = fma2(f2(2.f), v[2], fma2(f2(5.f), v[3], sub2(f2(0.f), v[4])));
+    const float2 t0 = add2(fma2(f2(-2.f), v[1], v[0]), v[2]);
+    const float2 r0 = fma2(f2(3.f), v[2], fma2(f2(-4.f), v[1], v[0]));
+    const float2 t1 = add2(fma2(f2(-2.f), v[2], v[1]), v[3]);
+    const float2 r1 = sub2(v[1], v[3]);
+    const float2 t2 = add2(fma2(f2(-2.f), v[3], v[2]), v[4]);
+    const float2 r2 = fma2(f2(3.f), v[2], fma2(f2(-4.f), v[3], v[4]));
+    const float2 c13 = f2(13.f / 12.f), q4 = f2(0.25f);
+    const float2 b0 = fma2(mul2(c13, t0), t0, mul2(mul2(q4, r0), r0));
+    const float2 b1 = fma2(mul2(c13, t1), t1, mul2(mul2(q4, r1), r1));
+    const float2 b2 = fma2(mul2(c13, t2), t2, mul2(mul2(q4, r2), r2));
+    const int mx = Teno<float>::keep_mask(b0.x, b1.x, b2.x, flags);
+    const int my = Teno<float>::keep_mask(b0.y, b1.y, b2.y, flags);
+    cut += 6 - __popc(mx) - __popc(my);
+    const float2 d0 = f2((mx & 1) ? 0.1f : 0.f, (my & 1) ? 0.1f : 0.f);
+    const float2 d1 = f2((mx & 2) ? 0.6f : 0.f, (my & 2) ? 0.6f : 0.f);
+    const float2 d2 = f2((mx & 4) ? 0.3f : 0.f, (my & 4) ? 0.3f : 0.f);
+    const float2 act = mul2(f2(6.f), add2(add2(d0, d1), d2));
+    if (!(act.x > 0.f) || !(act.y > 0.f)) flags |= FLAG_TENO_CUTOFF;
+    const float2 num = fma2(d0, p0, fma2(d1, p1, mul2(d2, p2)));
+    return make_float2(__fdividef(num.x, act.x), __fdividef(num.y, act.y));
+}
+
+// Characteristic projection of a pair of points (shared eigen-structure).
+template <int AX>
+__device__ __forceinline__ void to_characteristic2(const Eigen<float>& e, const float2 q[5], float2 w[5]) {
+    using B = AxisBasis<AX>;
+    const float2 mn = q[B::N];
+    const float2 ml = B::SL > 0 ? q[B::L] : sub2(f2(0.f), q[B::L]);
+    const float2 mm = B::SM > 0 ? q[B::M] : sub2(f2(0.f), q[B::M]);
+    const float2 A = fma2(f2(-e.h), q[0], sub2(fma2(f2(e.u), q[1], fma2(f2(e.v), q[2], mul2(f2(e.w), q[3]))), q[4]));
+    const float2 Bv = fma2(f2(e.un), q[0], sub2(f2(0.f), mn));
+    const float2 y = mul2(f2(e.b2), A);
+    w[0] = fma2(f2(e.b1), A, q[0]);
+    w[1] = fma2(f2(-e.ul), q[0], ml);
+    w[2] = fma2(f2(-e.um), q[0], mm);
+    w[3] = fma2(f2(e.x1), Bv, sub2(f2(0.f), y));
+    w[4] = fma2(f2(-e.x1), Bv, sub2(f2(0.f), y));
+}
+
+template <int AX>
+__device__ __forceinline__ void from_characteristic2(const Eigen<float>& e, const float2 w[5], float2 q[5]) {
+    using B = AxisBasis<AX>;
+    const float2 S = add2(add2(w[0], w[3]), w[4]);
+    const float2 D = sub2(w[4], w[3]);
+    const float2 cD = mul2(f2(e.c), D);
+    q[0] = S;
+    q[1] = mul2(f2(e.u), S);
+    q[2] = mul2(f2(e.v), S);
+    q[3] = mul2(f2(e.w), S);
+    q[B::N] = add2(q[B::N], cD);
+    q[B::L] = B::SL > 0 ? add2(q[B::L], w[1]) : sub2(q[B::L], w[1]);
+    q[B::M] = B::SM > 0 ? add2(q[B::M], w[2]) : sub2(q[B::M], w[2]);
+    q[4] = fma2(f2(e.h), w[0], fma2(f2(e.ul), w[1], fma2(f2(e.um), w[2], fma2(f2(e.H), add2(w[3], w[4]),
+                                                                                mul2(f2(e.un), cD)))));
 }
 
 // Reference state of a tile in FP32 with its velocity and pressure.
@@ -581,6 +760,96 @@ __device__ __forceinline__ void roe_dev(const Ref32& r, const float dL[5], const
     for (int v = 0; v < 5; ++v) F[v] = 0.5f * (fL[v] + fR[v] - diss[v]);
 }
 
+// phys_flux_dev for the (left, right) pair of face states.  Reciprocal and
+// square root use the SFU approximations (rcp, rsqrt): their ~1 ulp error
+// sits in front of quantities that are already deviations.
+template <int AX>
+__device__ __forceinline__ void phys_flux_dev2(const Ref32& r, const float2 d[5], float gamma, float2 F[5], float2& un,
+                                               float2& c, unsigned& flags) {
+    constexpr int N = AxisBasis<AX>::N;
+    const float2 rho = add2(f2(r.q[0]), d[0]);
+    const float2 irho = f2(__fdividef(1.f, rho.x), __fdividef(1.f, rho.y));
+    float2 du[3], u[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        du[k] = mul2(fma2(f2(-r.u[k]), d[0], d[1 + k]), irho);
+        u[k] = add2(f2(r.u[k]), du[k]);
+    }
+    const float2 dmu = fma2(f2(r.q[1]), du[0], fma2(f2(r.q[2]), du[1], fma2(f2(r.q[3]), du[2],
+                       fma2(d[1], u[0], fma2(d[2], u[1], mul2(d[3], u[2]))))));
+    const float2 dp = mul2(f2(gamma - 1.f), fma2(f2(-0.5f), dmu, d[4]));
+    const float2 p = add2(f2(r.p), dp);
+    if (!(rho.x > 0.f) || !(rho.y > 0.f)) flags |= FLAG_DENSITY;
+    if (!(p.x > 0.f) || !(p.y > 0.f)) flags |= FLAG_PRESSURE;
+    const float2 dun = du[N - 1];
+    un = u[N - 1];
+    F[0] = d[N];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        F[1 + k] = fma2(f2(r.q[1 + k]), dun, mul2(d[1 + k], un));
+        if (k == N - 1) F[1 + k] = add2(F[1 + k], dp);
+    }
+    F[4] = fma2(f2(r.q[4] + r.p), dun, mul2(add2(d[4], dp), un));
+    const float2 x = mul2(mul2(f2(gamma), p), irho);
+    c = f2(x.x * rsqrtf(x.x), x.y * rsqrtf(x.y));
+}
+
+template <int AX>
+__device__ __forceinline__ void rusanov_dev2(const Ref32& r, const float2 d[5], float gamma, float F[5],
+                                             unsigned& flags) {
+    float2 f[5], un, c;
+    phys_flux_dev2<AX>(r, d, gamma, f, un, c, flags);
+    const float hl = 0.5f * fmaxf(fabsf(un.x) + c.x, fabsf(un.y) + c.y);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) F[v] = 0.5f * (f[v].x + f[v].y) - hl * (d[v].y - d[v].x);
+}
+
+// face_flux_dev32 with the left / right work paired in float2 (WENO5, TENO5).
+template <int AX, int SCHEME, int FLUX>
+__device__ __forceinline__ void face_flux_dev32x2(const float (&d)[6][5], const Ref32& ref, float gamma, float F[5],
+                                                  unsigned& flags, unsigned& cut) {
+    float dbar[5], qbar[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+        dbar[v] = 0.5f * (d[2][v] + d[3][v]);
+        qbar[v] = ref.q[v] + dbar[v];
+    }
+    Eigen<float> e;
+    if (!eigen_at<AX, float>(qbar, gamma, e)) flags |= FLAG_PRESSURE;
+    // point pairs (k, 5-k): P[k][v] = (c_k, c_{5-k}) of component v
+    float2 P[3][5];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        float2 x[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) x[v] = sub2(f2(d[k][v], d[5 - k][v]), f2(dbar[v]));
+        to_characteristic2<AX>(e, x, P[k]);
+    }
+    float2 w[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+        // left stencil c0..c4 and right stencil c5..c1 as one paired stencil
+        const float2 st[5] = {P[0][v], P[1][v], P[2][v], swap2(P[2][v]), swap2(P[1][v])};
+        if constexpr (SCHEME == TENO5) w[v] = teno5_core2(st, flags, cut);
+        else w[v] = weno5_core2(st, flags);
+    }
+    float2 dq[5], x2[5];
+    from_characteristic2<AX>(e, w, dq);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) x2[v] = add2(f2(dbar[v]), dq[v]);  // (left, right) deviations from q_ref
+    if constexpr (FLUX == RUSANOV) {
+        rusanov_dev2<AX>(ref, x2, gamma, F, flags);
+    } else {
+        float xl[5], xr[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            xl[v] = x2[v].x;
+            xr[v] = x2[v].y;
+        }
+        roe_dev<AX>(ref, xl, xr, gamma, F, flags);
+    }
+}
+
 // FP32 face flux from a stencil held as FP32 deviations d_s = q_s - q_ref
 // from a reference state shared by a whole tile (q_ref is FP64 in HBM; only
 // the deviations are rounded to FP32, once per node when the tile is staged).
@@ -592,6 +861,10 @@ __device__ __forceinline__ void roe_dev(const Ref32& r, const float dL[5], const
 template <int AX, int SCHEME, int FLUX>
 __device__ __forceinline__ void face_flux_dev32(const float (&d)[SchemeInfo<SCHEME>::NST][5], const Ref32& ref,
                                                 float gamma, float F[5], unsigned& flags, unsigned& cut) {
+    if constexpr (SCHEME == WENO5 || SCHEME == TENO5) {
+        face_flux_dev32x2<AX, SCHEME, FLUX>(d, ref, gamma, F, flags, cut);
+        return;
+    }
     const float (&qref)[5] = ref.q;
     constexpr int NST = SchemeInfo<SCHEME>::NST;
     constexpr int W = SchemeInfo<SCHEME>::W;
