@@ -46,23 +46,25 @@ __device__ __forceinline__ void teno_flips_face(const GridView& g, const double*
         to_characteristic<AX, float>(e32, d, c32[s]);
     }
     unsigned fl = 0;
-    for (int v = 0; v < 5; ++v)
+    for (int v = 0; v < 5; ++v) {
+        // FP32: the (left, right) stencil pair through the paired indicators
+        // and cut-off of the FP32-flux kernels
+        float2 b2[5], B[3], q[3], keep[3];
+        for (int s = 0; s < 5; ++s) b2[s] = make_float2(c32[s][v], c32[NST - 1 - s][v]);
+        stencil5x2(b2, B, q);
+        teno_keep32x2(B[0], B[1], B[2], keep, fl);
         for (int side = 0; side < 2; ++side) {
             double a[5];
-            float b[5];
-            for (int s = 0; s < 5; ++s) {
-                a[s] = side ? c64[NST - 1 - s][v] : c64[s][v];
-                b[s] = side ? c32[NST - 1 - s][v] : c32[s][v];
-            }
+            for (int s = 0; s < 5; ++s) a[s] = side ? c64[NST - 1 - s][v] : c64[s][v];
             double a0, a1, a2;
-            float b0, b1, b2;
             teno_betas<double>(a, a0, a1, a2);
-            teno_betas<float>(b, b0, b1, b2);
             const int m64 = Teno<double>::keep_mask(a0, a1, a2, fl);
-            const int m32 = Teno<float>::keep_mask(b0, b1, b2, fl);
+            int m32 = 0;
+            for (int k = 0; k < 3; ++k) m32 |= int((side ? keep[k].y : keep[k].x) != 0.f) << k;
             dec += 3;
             flips += __popc(m64 ^ m32);
         }
+    }
 }
 
 __global__ void teno_flips_kernel(GridView g, const double* q, unsigned long long* out) {

@@ -33,9 +33,30 @@ template <> struct AxisBasis<0> { static constexpr int N = 1, L = 2, M = 3; stat
 template <> struct AxisBasis<1> { static constexpr int N = 2, L = 1, M = 3; static constexpr int SL = -1, SM = 1; };
 template <> struct AxisBasis<2> { static constexpr int N = 3, L = 1, M = 2; static constexpr int SL = -1, SM = -1; };
 
+// FP32 reciprocal as the single SFU instruction (PTX rcp.approx.ftz.f32,
+// about 1 ulp).  Every FP32 reciprocal of the path multiplies a deviation or
+// feeds a weight ratio, where 1 ulp is below the FP32 rounding already there.
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 template <typename T> __device__ __forceinline__ T rcp(T x);
 template <> __device__ __forceinline__ double rcp<double>(double x) { return 1.0 / x; }
-template <> __device__ __forceinline__ float rcp<float>(float x) { return __frcp_rn(x); }
+template <> __device__ __forceinline__ float rcp<float>(float x) { return rcp_approx(x); }
+
+// ---------------------------------------------------------------------------
+// Paired FP32 arithmetic (sm_100 f32x2: one instruction, two lanes of work).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 swap2(float2 a) { return make_float2(a.y, a.x); }
+__device__ __forceinline__ float2 rcp2(float2 a) { return make_float2(rcp_approx(a.x), rcp_approx(a.y)); }
 
 template <typename T> __device__ __forceinline__ T div_(T a, T b);
 template <> __device__ __forceinline__ double div_<double>(double a, double b) { return a / b; }
@@ -271,33 +292,40 @@ template <> struct Teno<double> {
     }
 };
 
-// FP32: gamma_k = g_k^6 leaves single-precision range long before FP64's, and
-// the smoothness indicators of a nearly uniform region (~1e-26) underflow any
-// product of two of them.  The cut-off test is therefore made on
-// r_k = g_k / max_j g_j in (0, 1]:
-//   tau = 0          -> every g_k = 1, nothing is cut;
-//   some g_k = +inf  -> those (the b_k ~ 0 sub-stencils) are kept, finite
-//                       ones cut (their ratio to the reference's huge gamma
-//                       is below the threshold);
-//   otherwise        -> r_k^6 < CT * sum_j r_j^6 with sum >= 1.
+// FP32 cut-off, for two independent sub-stencil triples at once (the two
+// lanes).  gamma_k = g_k^6 with g_k = 1 + tau/e_k leaves single-precision
+// range long before FP64's, so the test is made on the ratios to the largest
+// g, which belongs to the smallest e:
+//   x_k = g_k / g_max = t + s / e_k,   t = e_min / (e_min + tau),  s = tau t.
+// s <= e_min <= e_k, so every x_k lies in (0, 1] (x = 1 for e_min): nothing
+// overflows and no 0/0 or 0*inf arises, with no branch.  Keep k iff
+// x_k^6 >= CT * sum_j x_j^6 -- the reference's gamma_k / sum gamma >= CT
+// divided through by g_max^6.  eps is FLT_MIN: the reference's 1e-40 is
+// subnormal in FP32, whose reciprocal leaves the range.  keep[k] = 1 or 0.
+constexpr float TENO32_EPS = 1.17549435e-38f;
+
+__device__ __forceinline__ void teno_keep32x2(float2 b0, float2 b1, float2 b2, float2 (&keep)[3], unsigned& flags) {
+    const float2 e0 = add2(b0, f2(TENO32_EPS)), e1 = add2(b1, f2(TENO32_EPS)), e2 = add2(b2, f2(TENO32_EPS));
+    const float2 d02 = sub2(b0, b2);
+    const float2 tau = f2(fabsf(d02.x), fabsf(d02.y));
+    const float2 em = f2(fminf(e0.x, fminf(e1.x, e2.x)), fminf(e0.y, fminf(e1.y, e2.y)));
+    const float2 t = mul2(em, rcp2(add2(em, tau)));
+    const float2 s = mul2(tau, t);
+    const float2 x0 = fma2(s, rcp2(e0), t), x1 = fma2(s, rcp2(e1), t), x2 = fma2(s, rcp2(e2), t);
+    const float2 y0 = mul2(x0, x0), y1 = mul2(x1, x1), y2 = mul2(x2, x2);
+    const float2 G0 = mul2(mul2(y0, y0), y0), G1 = mul2(mul2(y1, y1), y1), G2 = mul2(mul2(y2, y2), y2);
+    const float2 lim = mul2(f2(1e-5f), add2(add2(G0, G1), G2));
+    if (!(lim.x < 1.f) || !(lim.y < 1.f)) flags |= FLAG_NONFINITE;  // NaN input (lim <= 3e-5 otherwise)
+    keep[0] = f2(G0.x < lim.x ? 0.f : 1.f, G0.y < lim.y ? 0.f : 1.f);
+    keep[1] = f2(G1.x < lim.x ? 0.f : 1.f, G1.y < lim.y ? 0.f : 1.f);
+    keep[2] = f2(G2.x < lim.x ? 0.f : 1.f, G2.y < lim.y ? 0.f : 1.f);
+}
+
 template <> struct Teno<float> {
     static __device__ __forceinline__ int keep_mask(float b0, float b1, float b2, unsigned& flags) {
-        const float tau = fabsf(b0 - b2);
-        if (!(tau > 0.f)) return 7;
-        // division by a subnormal b+eps gives +inf here: the "dominant" case
-        const float g0 = 1.f + __fdividef(tau, b0 + 1e-40f);
-        const float g1 = 1.f + __fdividef(tau, b1 + 1e-40f);
-        const float g2 = 1.f + __fdividef(tau, b2 + 1e-40f);
-        const float gm = fmaxf(g0, fmaxf(g1, g2));
-        if (!(gm <= 3.0e38f))
-            return int(!(g0 <= 3.0e38f)) | (int(!(g1 <= 3.0e38f)) << 1) | (int(!(g2 <= 3.0e38f)) << 2);
-        const float im = __frcp_rn(gm);
-        const float x0 = g0 * im, x1 = g1 * im, x2 = g2 * im;
-        const float y0 = x0 * x0 * x0, y1 = x1 * x1 * x1, y2 = x2 * x2 * x2;
-        const float G0 = y0 * y0, G1 = y1 * y1, G2 = y2 * y2;
-        const float lim = 1e-5f * (G0 + G1 + G2);
-        if (!finite_(lim)) flags |= FLAG_NONFINITE;
-        return int(!(G0 < lim)) | (int(!(G1 < lim)) << 1) | (int(!(G2 < lim)) << 2);
+        float2 k[3];
+        teno_keep32x2(f2(b0), f2(b1), f2(b2), k, flags);
+        return int(k[0].x != 0.f) | (int(k[1].x != 0.f) << 1) | (int(k[2].x != 0.f) << 2);
     }
     static __device__ __forceinline__ float core(const float* v, unsigned& flags, unsigned& cut) {
         const float p0 = 2.f * v[0] - 7.f * v[1] + 11.f * v[2];
@@ -543,104 +571,111 @@ __device__ __forceinline__ void face_flux(const double (&st)[SchemeInfo<SCHEME>:
 }
 
 // ---------------------------------------------------------------------------
-// Paired FP32 arithmetic (sm_100 f32x2: one instruction, two lanes of work).
-// The left- and right-biased reconstructions of a face are the same
-// operations on mirrored stencils, so they run as the two halves of a float2.
+// Paired FP32 cores.  The left- and right-biased reconstructions of a face
+// are the same operations on mirrored stencils, so they run as the two
+// halves of a float2.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
-__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
-__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-__device__ __forceinline__ float2 swap2(float2 a) { return make_float2(a.y, a.x); }
+
+// The 5-point stencil in first differences D_i = v_{i+1} - v_i (both lanes):
+//   t0 = D1 - D0, t1 = D2 - D1, t2 = D3 - D2          (second differences)
+//   r0 = 3 D1 - D0 = t0 + 2 D1, r1 = D1 + D2, r2 = D3 - 3 D2 = t2 - 2 D2
+//   B_k = 12 b_k = 13 t_k^2 + 3 r_k^2
+//   p_k - 6 v2 = q_k:  q0 = 5 D1 - 2 D0 = 2 t0 + 3 D1, q1 = D1 + 2 D2, q2 = 4 D2 - D3 = D2 - r2
+// (r1 is the reference's v1 - v3 up to sign, which the square removes), so a
+// reconstruction sum w_k p_k / (6 sum w_k) is v2 + sum w_k q_k / (6 sum w_k).
+// The indicators are scaled by 12 and the epsilons with them, which leaves
+// every weight unchanged; only differences of the stencil are rounded.
+__device__ __forceinline__ void stencil5x2(const float2* v, float2 (&B)[3], float2 (&q)[3]) {
+    const float2 D0 = sub2(v[1], v[0]), D1 = sub2(v[2], v[1]), D2 = sub2(v[3], v[2]), D3 = sub2(v[4], v[3]);
+    const float2 t0 = sub2(D1, D0), t1 = sub2(D2, D1), t2 = sub2(D3, D2);
+    const float2 r0 = fma2(f2(2.f), D1, t0), r1 = add2(D1, D2), r2 = fma2(f2(-2.f), D2, t2);
+    B[0] = fma2(mul2(f2(13.f), t0), t0, mul2(mul2(f2(3.f), r0), r0));
+    B[1] = fma2(mul2(f2(13.f), t1), t1, mul2(mul2(f2(3.f), r1), r1));
+    B[2] = fma2(mul2(f2(13.f), t2), t2, mul2(mul2(f2(3.f), r2), r2));
+    q[0] = fma2(f2(2.f), t0, mul2(f2(3.f), D1));
+    q[1] = fma2(f2(2.f), D2, D1);
+    q[2] = sub2(D2, r2);
+}
 
 // WENO5-JS on a (left, right) stencil pair; same folding as weno5_core.
 __device__ __forceinline__ float2 weno5_core2(const float2* v, unsigned& flags) {
-    const float2 p0 = fma2(f2(2.f), v[0], fma2(f2(-7.f), v[1], mul2(f2(11.f), v[2])));
-    const float2 p1 = fma2(f2(5.f), v[2], fma2(f2(2.f), v[3], sub2(f2(0.f), v[1])));
-    const float2 p2 = fma2(f2(2.f), v[2], fma2(f2(5.f), v[3], sub2(f2(0.f), v[4])));
-    const float2 t0 = add2(fma2(f2(-2.f), v[1], v[0]), v[2]);
-    const float2 r0 = fma2(f2(3.f), v[2], fma2(f2(-4.f), v[1], v[0]));
-    const float2 t1 = add2(fma2(f2(-2.f), v[2], v[1]), v[3]);
-    const float2 r1 = sub2(v[1], v[3]);
-    const float2 t2 = add2(fma2(f2(-2.f), v[3], v[2]), v[4]);
-    const float2 r2 = fma2(f2(3.f), v[2], fma2(f2(-4.f), v[3], v[4]));
-    const float2 c13 = f2(13.f / 12.f), q4 = f2(0.25f);
-    const float2 b0 = fma2(mul2(c13, t0), t0, mul2(mul2(q4, r0), r0));
-    const float2 b1 = fma2(mul2(c13, t1), t1, mul2(mul2(q4, r1), r1));
-    const float2 b2 = fma2(mul2(c13, t2), t2, mul2(mul2(q4, r2), r2));
-    const float2 e0 = add2(f2(1e-6f), b0), e1 = add2(f2(1e-6f), b1), e2 = add2(f2(1e-6f), b2);
+    float2 B[3], q[3];
+    stencil5x2(v, B, q);
+    const float2 eps = f2(12.f * 1e-6f);
+    const float2 e0 = add2(eps, B[0]), e1 = add2(eps, B[1]), e2 = add2(eps, B[2]);
     const float2 s0 = mul2(e0, e0), s1 = mul2(e1, e1), s2 = mul2(e2, e2);
     const float2 w0 = mul2(f2(0.1f), mul2(s1, s2));
     const float2 w1 = mul2(f2(0.6f), mul2(s0, s2));
     const float2 w2 = mul2(f2(0.3f), mul2(s0, s1));
     const float2 den = mul2(f2(6.f), add2(add2(w0, w1), w2));
-    const float2 num = fma2(w0, p0, fma2(w1, p1, mul2(w2, p2)));
-    if (!(den.x > 0.f) || !(den.y > 0.f) || !isfinite(den.x) || !isfinite(den.y)) flags |= FLAG_NONFINITE;
-    return make_float2(__fdividef(num.x, den.x), __fdividef(num.y, den.y));
+    const float2 num = fma2(w0, q[0], fma2(w1, q[1], mul2(w2, q[2])));
+    if (!(den.x > 0.f && den.x < INFINITY) || !(den.y > 0.f && den.y < INFINITY)) flags |= FLAG_NONFINITE;
+    return fma2(num, rcp2(den), v[2]);
 }
 
-// TENO5 on a (left, right) stencil pair: polynomials and smoothness
-// indicators paired, the cut-off decision per side (Teno<float>::keep_mask).
-__device__ __forceinline__ float2 teno5_core2(const float2* v, unsigned& flags, unsigned& cut) {
-    const float2 p0 = fma2(f2(2.f), v[0], fma2(f2(-7.f), v[1], mul2(f2(11.f), v[2])));
-    const float2 p1 = fma2(f2(5.f), v[2], fma2(f2(2.f), v[3], sub2(f2(0.f), v[1])));
-    const float2 p2 = fma2(f2(2.f), v[2], fma2(f2(5.f), v[3], sub2(f2(0.f), v[4])));
-    const float2 t0 = add2(fma2(f2(-2.f), v[1], v[0]), v[2]);
-    const float2 r0 = fma2(f2(3.f), v[2], fma2(f2(-4.f), v[1], v[0]));
-    const float2 t1 = add2(fma2(f2(-2.f), v[2], v[1]), v[3]);
-    const float2 r1 = sub2(v[1], v[3]);
-    const float2 t2 = add2(fma2(f2(-2.f), v[3], v[2]), v[4]);
-    const float2 r2 = fma2(f2(3.f), v[2], fma2(f2(-4.f), v[3], v[4]));
-    const float2 c13 = f2(13.f / 12.f), q4 = f2(0.25f);
-    const float2 b0 = fma2(mul2(c13, t0), t0, mul2(mul2(q4, r0), r0));
-    const float2 b1 = fma2(mul2(c13, t1), t1, mul2(mul2(q4, r1), r1));
-    const float2 b2 = fma2(mul2(c13, t2), t2, mul2(mul2(q4, r2), r2));
-    const int mx = Teno<float>::keep_mask(b0.x, b1.x, b2.x, flags);
-    const int my = Teno<float>::keep_mask(b0.y, b1.y, b2.y, flags);
-    cut += 6 - __popc(mx) - __popc(my);
-    const float2 d0 = f2((mx & 1) ? 0.1f : 0.f, (my & 1) ? 0.1f : 0.f);
-    const float2 d1 = f2((mx & 2) ? 0.6f : 0.f, (my & 2) ? 0.6f : 0.f);
-    const float2 d2 = f2((mx & 4) ? 0.3f : 0.f, (my & 4) ? 0.3f : 0.f);
-    const float2 act = mul2(f2(6.f), add2(add2(d0, d1), d2));
-    if (!(act.x > 0.f) || !(act.y > 0.f)) flags |= FLAG_TENO_CUTOFF;
-    const float2 num = fma2(d0, p0, fma2(d1, p1, mul2(d2, p2)));
-    return make_float2(__fdividef(num.x, act.x), __fdividef(num.y, act.y));
+// TENO5 on a (left, right) stencil pair, all of it paired: polynomials,
+// smoothness indicators, the cut-off (teno_keep32x2) and the weights.
+// `kept` accumulates the kept sub-stencils of each lane.
+__device__ __forceinline__ float2 teno5_core2(const float2* v, unsigned& flags, float2& kept) {
+    float2 B[3], q[3], k[3];
+    stencil5x2(v, B, q);
+    teno_keep32x2(B[0], B[1], B[2], k, flags);
+    kept = add2(kept, add2(add2(k[0], k[1]), k[2]));
+    const float2 d0 = mul2(f2(0.1f), k[0]), d1 = mul2(f2(0.6f), k[1]), d2 = mul2(f2(0.3f), k[2]);
+    // No all-cut check: the sub-stencil with x = 1 always passes (G ~ 1 >
+    // lim <= 3e-5, and a NaN lim fails every '<'), so act >= 0.6.
+    const float2 act = fma2(f2(6.f), d0, fma2(f2(6.f), d1, mul2(f2(6.f), d2)));
+    const float2 num = fma2(d0, q[0], fma2(d1, q[1], mul2(d2, q[2])));
+    return fma2(num, rcp2(act), v[2]);
 }
 
-// Characteristic projection of a pair of points (shared eigen-structure).
+// The eigen-structure as lane pairs, signs folded in, built once per face.
+// The tangential characteristic variables are taken with the raw Cartesian
+// components, w_t = m_t - u_t rho: the reference's signed tangents (+-e_t)
+// only negate w_t, and negation commutes exactly with the projection, every
+// reconstruction core (linear polynomials, squared indicators) and the
+// back-projection, so the face states are bit-identical.
+struct Eig2 {
+    float2 u[3], nu[3];  // velocity, negated velocity
+    float2 h, H, c, nb1, b2, x1, nx1;
+};
+
+__device__ __forceinline__ Eig2 eig2(const Eigen<float>& e) {
+    Eig2 p;
+    p.u[0] = f2(e.u), p.u[1] = f2(e.v), p.u[2] = f2(e.w);
+    p.nu[0] = f2(-e.u), p.nu[1] = f2(-e.v), p.nu[2] = f2(-e.w);
+    p.h = f2(e.h), p.H = f2(e.H), p.c = f2(e.c);
+    p.nb1 = f2(-e.b1), p.b2 = f2(e.b2), p.x1 = f2(e.x1), p.nx1 = f2(-e.x1);
+    return p;
+}
+
+// Characteristic projection of a pair of points:
+//   -A = E + h rho - u.m,  -B = m_n - u_n rho,
+//   w0 = rho - b1 (-A),  w3 = -x1 (-B) + b2 (-A),  w4 = x1 (-B) + b2 (-A).
 template <int AX>
-__device__ __forceinline__ void to_characteristic2(const Eigen<float>& e, const float2 q[5], float2 w[5]) {
+__device__ __forceinline__ void to_characteristic2(const Eig2& e, const float2 q[5], float2 w[5]) {
     using B = AxisBasis<AX>;
-    const float2 mn = q[B::N];
-    const float2 ml = B::SL > 0 ? q[B::L] : sub2(f2(0.f), q[B::L]);
-    const float2 mm = B::SM > 0 ? q[B::M] : sub2(f2(0.f), q[B::M]);
-    const float2 A = fma2(f2(-e.h), q[0], sub2(fma2(f2(e.u), q[1], fma2(f2(e.v), q[2], mul2(f2(e.w), q[3]))), q[4]));
-    const float2 Bv = fma2(f2(e.un), q[0], sub2(f2(0.f), mn));
-    const float2 y = mul2(f2(e.b2), A);
-    w[0] = fma2(f2(e.b1), A, q[0]);
-    w[1] = fma2(f2(-e.ul), q[0], ml);
-    w[2] = fma2(f2(-e.um), q[0], mm);
-    w[3] = fma2(f2(e.x1), Bv, sub2(f2(0.f), y));
-    w[4] = fma2(f2(-e.x1), Bv, sub2(f2(0.f), y));
+    const float2 nA = fma2(e.nu[0], q[1], fma2(e.nu[1], q[2], fma2(e.nu[2], q[3], fma2(e.h, q[0], q[4]))));
+    const float2 nB = fma2(e.nu[B::N - 1], q[0], q[B::N]);
+    const float2 b2nA = mul2(e.b2, nA);
+    w[0] = fma2(e.nb1, nA, q[0]);
+    w[1] = fma2(e.nu[B::L - 1], q[0], q[B::L]);
+    w[2] = fma2(e.nu[B::M - 1], q[0], q[B::M]);
+    w[3] = fma2(e.nx1, nB, b2nA);
+    w[4] = fma2(e.x1, nB, b2nA);
 }
 
 template <int AX>
-__device__ __forceinline__ void from_characteristic2(const Eigen<float>& e, const float2 w[5], float2 q[5]) {
+__device__ __forceinline__ void from_characteristic2(const Eig2& e, const float2 w[5], float2 q[5]) {
     using B = AxisBasis<AX>;
     const float2 S = add2(add2(w[0], w[3]), w[4]);
-    const float2 D = sub2(w[4], w[3]);
-    const float2 cD = mul2(f2(e.c), D);
+    const float2 cD = mul2(e.c, sub2(w[4], w[3]));
     q[0] = S;
-    q[1] = mul2(f2(e.u), S);
-    q[2] = mul2(f2(e.v), S);
-    q[3] = mul2(f2(e.w), S);
-    q[B::N] = add2(q[B::N], cD);
-    q[B::L] = B::SL > 0 ? add2(q[B::L], w[1]) : sub2(q[B::L], w[1]);
-    q[B::M] = B::SM > 0 ? add2(q[B::M], w[2]) : sub2(q[B::M], w[2]);
-    q[4] = fma2(f2(e.h), w[0], fma2(f2(e.ul), w[1], fma2(f2(e.um), w[2], fma2(f2(e.H), add2(w[3], w[4]),
-                                                                                mul2(f2(e.un), cD)))));
+    q[B::N] = fma2(e.u[B::N - 1], S, cD);
+    q[B::L] = fma2(e.u[B::L - 1], S, w[1]);
+    q[B::M] = fma2(e.u[B::M - 1], S, w[2]);
+    q[4] = fma2(e.h, w[0], fma2(e.u[B::L - 1], w[1], fma2(e.u[B::M - 1], w[2],
+                fma2(e.H, add2(w[3], w[4]), mul2(e.u[B::N - 1], cD)))));
 }
 
 // Reference state of a tile in FP32 with its velocity and pressure.
@@ -676,7 +711,7 @@ __device__ __forceinline__ void phys_flux_dev(const Ref32& r, const float d[5], 
                                               float& c, float& p_out, unsigned& flags) {
     constexpr int N = AxisBasis<AX>::N;
     const float rho = r.q[0] + d[0];
-    const float irho = __frcp_rn(rho);
+    const float irho = rcp_approx(rho);
     float du[3], u[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -726,10 +761,10 @@ __device__ __forceinline__ void roe_dev(const Ref32& r, const float dL[5], const
     phys_flux_dev<AX>(r, dL, gamma, fL, unL, cL, pL, flags);
     phys_flux_dev<AX>(r, dR, gamma, fR, unR, cR, pR, flags);
     const float gm1 = gamma - 1.f;
-    const float iL = __frcp_rn(qL[0]), iR = __frcp_rn(qR[0]);
+    const float iL = rcp_approx(qL[0]), iR = rcp_approx(qR[0]);
     const float hL = (qL[4] + pL) * iL, hR = (qR[4] + pR) * iR;
     const float sL = sqrtf(qL[0]), sR = sqrtf(qR[0]);
-    const float iS = __frcp_rn(sL + sR);
+    const float iS = rcp_approx(sL + sR);
     const float ur = (sL * qL[1] * iL + sR * qR[1] * iR) * iS;
     const float vr = (sL * qL[2] * iL + sR * qR[2] * iR) * iS;
     const float wr = (sL * qL[3] * iL + sR * qR[3] * iR) * iS;
@@ -752,7 +787,7 @@ __device__ __forceinline__ void roe_dev(const Ref32& r, const float dL[5], const
 #pragma unroll
     for (int m = 0; m < 5; ++m) {
         const float val = fabsf(lam[m]);
-        const float ab = val < 2.f * delta ? 0.5f * (val * val * __frcp_rn(2.f * delta) + delta) : val;
+        const float ab = val < 2.f * delta ? 0.5f * (val * val * rcp_approx(2.f * delta) + delta) : val;
         s[m] = ab * alpha[m];
     }
     from_characteristic<AX, float>(e, s, diss);
@@ -768,7 +803,7 @@ __device__ __forceinline__ void phys_flux_dev2(const Ref32& r, const float2 d[5]
                                                float2& c, unsigned& flags) {
     constexpr int N = AxisBasis<AX>::N;
     const float2 rho = add2(f2(r.q[0]), d[0]);
-    const float2 irho = f2(__fdividef(1.f, rho.x), __fdividef(1.f, rho.y));
+    const float2 irho = rcp2(rho);
     float2 du[3], u[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -799,9 +834,14 @@ __device__ __forceinline__ void rusanov_dev2(const Ref32& r, const float2 d[5], 
                                              unsigned& flags) {
     float2 f[5], un, c;
     phys_flux_dev2<AX>(r, d, gamma, f, un, c, flags);
-    const float hl = 0.5f * fmaxf(fabsf(un.x) + c.x, fabsf(un.y) + c.y);
+    // F = (f_L + f_R)/2 - lam/2 (d_R - d_L) = ((f_L + lam d_L) + (f_R - lam d_R)) / 2
+    const float lam = fmaxf(fabsf(un.x) + c.x, fabsf(un.y) + c.y);
+    const float2 lr = f2(lam, -lam);
 #pragma unroll
-    for (int v = 0; v < 5; ++v) F[v] = 0.5f * (f[v].x + f[v].y) - hl * (d[v].y - d[v].x);
+    for (int v = 0; v < 5; ++v) {
+        const float2 g = fma2(lr, d[v], f[v]);
+        F[v] = 0.5f * (g.x + g.y);
+    }
 }
 
 // face_flux_dev32 with the left / right work paired in float2 (WENO5, TENO5).
@@ -814,8 +854,9 @@ __device__ __forceinline__ void face_flux_dev32x2(const float (&d)[6][5], const 
         dbar[v] = 0.5f * (d[2][v] + d[3][v]);
         qbar[v] = ref.q[v] + dbar[v];
     }
-    Eigen<float> e;
-    if (!eigen_at<AX, float>(qbar, gamma, e)) flags |= FLAG_PRESSURE;
+    Eigen<float> es;
+    if (!eigen_at<AX, float>(qbar, gamma, es)) flags |= FLAG_PRESSURE;
+    const Eig2 e = eig2(es);
     // point pairs (k, 5-k): P[k][v] = (c_k, c_{5-k}) of component v
     float2 P[3][5];
 #pragma unroll
@@ -826,13 +867,15 @@ __device__ __forceinline__ void face_flux_dev32x2(const float (&d)[6][5], const 
         to_characteristic2<AX>(e, x, P[k]);
     }
     float2 w[5];
+    float2 kept = f2(0.f);
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
         // left stencil c0..c4 and right stencil c5..c1 as one paired stencil
         const float2 st[5] = {P[0][v], P[1][v], P[2][v], swap2(P[2][v]), swap2(P[1][v])};
-        if constexpr (SCHEME == TENO5) w[v] = teno5_core2(st, flags, cut);
+        if constexpr (SCHEME == TENO5) w[v] = teno5_core2(st, flags, kept);
         else w[v] = weno5_core2(st, flags);
     }
+    if constexpr (SCHEME == TENO5) cut += 30u - unsigned(kept.x + kept.y);
     float2 dq[5], x2[5];
     from_characteristic2<AX>(e, w, dq);
 #pragma unroll
