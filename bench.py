@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--serve-rate", type=float, default=8.0, help="Poisson arrivals per second")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--accuracy-t", type=float, default=10.0, help="vortex run length for the L1 check (0: skip)")
+    ap.add_argument("--tgv-t", type=float, default=0.25, help="Taylor-Green run length (0: skip)")
+    ap.add_argument("--tgv-size", type=int, default=256)
     return ap.parse_args()
 
 
@@ -300,6 +302,9 @@ def run_ours(args, rank, world):
         s2.close()
     if args.accuracy_t > 0:
         out["accuracy"] = run_accuracy(args)
+    out["sod_1d"] = run_sod(args)
+    if args.tgv_t > 0:
+        out["taylor_green"] = run_taylor_green(args)
     if not args.no_batch:
         out["batched"] ={"fp32flux": run_batched(args, capi.PREC_FP32_FLUX), "fp64": run_batched(args, capi.PREC_FP64)}
         cap = out["batched"]["fp64"]["value"]
@@ -337,6 +342,97 @@ def run_accuracy(args):
         s.close()
     out["l1_rho_fp32flux_vs_fp64"] = float(np.mean(np.abs(res["fp32flux"][..., 0] - res["fp64"][..., 0])))
     out["l1_ratio_fp32flux_over_fp64"] = out["fp32flux"]["l1_rho_vs_exact"] / out["fp64"]["l1_rho_vs_exact"]
+    return out
+
+
+def run_sod(args, repeats=5):
+    """Sod shock tube, 1000 cells, WENO5 + Rusanov, SSPRK3, CFL 0.5, t = 0.2,
+    FP64: the latency case.  Reports the device time of sfg_advance and the
+    wall time of one solve through the C ABI with host buffers (upload +
+    advance + download; the solver is created beforehand), median of
+    `repeats`, beside the reference operator (oracle/_ref, one host core)
+    running the same solve, and the largest relative difference between the
+    two final states (the per-step parity bar is in the tests)."""
+    import numpy as np
+    import torch
+    from sonicsolver_b200 import capi, cases
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    case = cases.sod_1d(1000)
+    q = np.ascontiguousarray(case.q)
+    host = np.empty_like(q)
+    walls, devs, steps = [], [], 0
+    for r in range(repeats + 1):
+        s = case.solver(precision=capi.PREC_FP64)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.upload(q)
+        st, _ = s.advance(case.t_end, graph_steps=32)
+        s.download(out=host)
+        wall = time.perf_counter() - t0
+        s.close()
+        if r:                                     # the first solve loads modules
+            walls.append(wall)
+            devs.append(st.device_ms / 1e3)
+        steps = int(st.steps)
+    out = {"cells": 1000, "t_end": case.t_end, "steps": steps, "recipe": "weno5Rusanov", "time": "SSPRK3",
+           "device_s": float(np.median(devs)), "wall_s_capi_host_buffers": float(np.median(walls))}
+    out["value"] = round(1000 * steps / out["wall_s_capi_host_buffers"] / 1e6, 3)
+    out["unit"] = "Mcell-steps/s"
+    try:
+        spec = po.GridSpec(dim=1, n=tuple(case.n), ng=3, h=tuple(case.h), bc_lo=tuple(case.bc_lo),
+                           bc_hi=tuple(case.bc_hi), gamma=case.gamma)
+        Q = spec.empty()
+        spec.interior(Q)[...] = q.reshape(spec.interior(Q).shape)
+        po.fill_ghosts(spec, Q)
+        rc = po.RefCase(spec, po.WENO5, po.RUSANOV, native=True)
+        t0 = time.perf_counter()
+        dts, tf = rc.advance(po.SSPRK3, Q, case.t_end, case.cfl)
+        ref_s = time.perf_counter() - t0
+        ref = np.ascontiguousarray(spec.interior(Q)).reshape(host.shape)
+        scale = np.maximum(np.abs(ref).reshape(-1, 5).max(axis=0), 1e-300)
+        diff = (np.abs(host - ref).reshape(-1, 5).max(axis=0) / scale)
+        out["reference_cpu"] = {"wall_s": ref_s, "steps": int(len(dts)), "cores": 1,
+                                "kind": "reference operator, -O3 -march=x86-64-v3"}
+        out["max_rel_diff_vs_reference"] = float(diff.max())
+        out["speedup_wall_vs_reference"] = round(ref_s / out["wall_s_capi_host_buffers"], 2)
+    except Exception as e:  # reference library missing on this host
+        out["reference_cpu"] = {"unavailable": str(e)}
+    return out
+
+
+def run_taylor_green(args):
+    """3-D inviscid Taylor-Green vortex, periodic [0, 2 pi]^3 (256^3 cells by
+    default), Mach 0.1, WENO5 + Rusanov, SSPRK3, CFL 0.5, advanced to
+    t = args.tgv_t in FP64 and in FP32-flux / FP64-state.  Reports the
+    device-timed throughput of each, the kinetic energy KE(t) / KE(0) and the
+    FP32-flux kinetic-energy drift relative to the FP64 path (which matches
+    the CPU oracle to <= 1e-12 per step in the parity tests)."""
+    import numpy as np
+    from sonicsolver_b200 import capi, cases
+    N = args.tgv_size
+    case = cases.taylor_green(N, t_end=args.tgv_t)
+    cells = N ** 3
+    ke0 = cases.kinetic_energy(case.q)
+    out = {"t_end": args.tgv_t, "cells": f"{N}^3", "recipe": "weno5Rusanov", "time": "SSPRK3", "cfl": case.cfl,
+           "mach": 0.1, "ke0": ke0}
+    res = {}
+    for name, prec in (("fp64", capi.PREC_FP64), ("fp32flux", capi.PREC_FP32_FLUX)):
+        s = case.solver(precision=prec)
+        st, _ = s.advance(args.tgv_t, graph_steps=32)
+        q = s.download().reshape(case.q.shape)
+        ke = cases.kinetic_energy(q)
+        res[name] = (q, ke)
+        out[name] = {"steps": int(st.steps), "device_s": round(st.device_ms / 1e3, 3),
+                     "value": round(cells * st.steps / (st.device_ms * 1e-3) / 1e6, 2), "unit": "Mcell-steps/s",
+                     "ke_over_ke0": ke / ke0}
+        s.close()
+    (q64, ke64), (q32, ke32) = res["fp64"], res["fp32flux"]
+    out["ke_drift_fp32flux_vs_fp64"] = (ke32 - ke64) / ke64
+    out["ke_change_fp64"] = (ke64 - ke0) / ke0
+    out["ke_drift_over_ke_change"] = (ke32 - ke64) / abs(ke64 - ke0) if ke64 != ke0 else None
+    out["l1_rho_fp32flux_vs_fp64"] = float(np.mean(np.abs(q32[..., 0] - q64[..., 0])))
+    out["fp32flux_over_fp64"] = round(out["fp32flux"]["value"] / out["fp64"]["value"], 3)
     return out
 
 

@@ -56,7 +56,21 @@ __global__ void __launch_bounds__(128) sweep_x(GridView g, StageView sv) {
             for (int v = 0; v < 5; ++v) st[s][v] = __ldg(sv.qs + v * vs + rowbase + ii);
         }
         T Ft[5];
-        face_flux<0, SCHEME, FLUX, T>(st, T(g.gamma), Ft, flags, cut);
+        if constexpr (sizeof(T) == sizeof(float)) {
+            // deviations from the chunk's first node, shared by the whole warp
+            double qref[5];
+#pragma unroll
+            for (int v = 0; v < 5; ++v) qref[v] = __ldg(sv.qs + v * vs + rowbase + i0);
+            const Ref32 ref = make_ref32(qref, g.gamma);
+            float d[NST][5];
+#pragma unroll
+            for (int s = 0; s < NST; ++s)
+#pragma unroll
+                for (int v = 0; v < 5; ++v) d[s][v] = float(st[s][v] - qref[v]);
+            face_flux_dev32<0, SCHEME, FLUX>(d, ref, float(g.gamma), Ft, flags, cut);
+        } else {
+            face_flux<0, SCHEME, FLUX, T>(st, T(g.gamma), Ft, flags, cut);
+        }
 #pragma unroll
         for (int v = 0; v < 5; ++v) F[v] = double(Ft[v]) * g.area[0];
     }
@@ -88,6 +102,77 @@ __global__ void __launch_bounds__(128) sweep_x(GridView g, StageView sv) {
 // ---------------------------------------------------------------------------
 constexpr int SEGLEN = 16;
 
+// FP32-flux segment: the register window holds FP32 deviations from the
+// segment's first node (one FP64 -> FP32 rounding per node), the face fluxes
+// are deviations F - F(q_ref) (face_flux_dev32).  Both faces of every node of
+// the segment share the reference, so F(q_ref) cancels from the divergence
+// exactly.  The FP64 node value for the stage update is re-read (L1 / L2).
+template <int AX, int SCHEME, int FLUX>
+__device__ __forceinline__ void sweep_yz_f32_segment(const GridView& g, const StageView& sv, int i, int o, int s0,
+                                                     unsigned& flags, unsigned& cut, unsigned& cores) {
+    constexpr int NST = SchemeInfo<SCHEME>::NST;
+    constexpr int OTHER = AX == 1 ? 2 : 1;
+    const int s1 = min(s0 + SEGLEN, g.hi[AX]);
+    const long long vs = g.vs;
+    const long long sy = g.n[0], sz = (long long)g.n[0] * g.n[1];
+    const long long sa = AX == 1 ? sy : sz;
+    const long long base = i + (long long)o * (OTHER == 1 ? sy : sz);
+    const int n = g.n[AX];
+    const int bl = g.bc_lo[AX], bh = g.bc_hi[AX];
+    const double dt = sv.clock->dt;
+    double qref[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) qref[v] = sv.qs[v * vs + base + (long long)s0 * sa];
+    const Ref32 ref = make_ref32(qref, g.gamma);
+    const float gamma = float(g.gamma);
+    float d[NST][5];
+#pragma unroll
+    for (int s = 0; s < NST; ++s) {
+        const int a = map_index(s0 - NST / 2 + s, n, bl, bh);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) d[s][v] = float(sv.qs[v * vs + base + a * sa] - qref[v]);
+    }
+    double Fp[5];
+    for (int f = s0; f <= s1; ++f) {
+        float Ft[5];
+        face_flux_dev32<AX, SCHEME, FLUX>(d, ref, gamma, Ft, flags, cut);
+        if (SCHEME == TENO5) cores += 10;
+        double F[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) F[v] = double(Ft[v]) * g.area[AX];
+        if (f > s0) {
+            const long long node = base + (long long)(f - 1) * sa;
+            double div[5];
+#pragma unroll
+            for (int v = 0; v < 5; ++v) div[v] = F[v] - Fp[v];
+            if (sv.mode & MODE_READ_R) {
+#pragma unroll
+                for (int v = 0; v < 5; ++v) div[v] = sv.r[v * vs + node] + div[v];
+            }
+            if (sv.mode & MODE_FINAL) {
+                double qn[5];
+#pragma unroll
+                for (int v = 0; v < 5; ++v) qn[v] = sv.qs[v * vs + node];
+                finish_node(g, sv, dt, node, qn, div, flags);
+            } else {
+#pragma unroll
+                for (int v = 0; v < 5; ++v) sv.r[v * vs + node] = div[v];
+            }
+        }
+#pragma unroll
+        for (int v = 0; v < 5; ++v) Fp[v] = F[v];
+        if (f < s1) {
+#pragma unroll
+            for (int s = 0; s < NST - 1; ++s)
+#pragma unroll
+                for (int v = 0; v < 5; ++v) d[s][v] = d[s + 1][v];
+            const int a = map_index(f + 1 - NST / 2 + NST - 1, n, bl, bh);
+#pragma unroll
+            for (int v = 0; v < 5; ++v) d[NST - 1][v] = float(sv.qs[v * vs + base + a * sa] - qref[v]);
+        }
+    }
+}
+
 template <int AX, int SCHEME, int FLUX, typename T>
 __global__ void __launch_bounds__(128) sweep_yz(GridView g, StageView sv) {
     constexpr int NST = SchemeInfo<SCHEME>::NST;
@@ -98,7 +183,9 @@ __global__ void __launch_bounds__(128) sweep_yz(GridView g, StageView sv) {
     const int s0 = g.lo[AX] + (blockIdx.y * blockDim.y + threadIdx.y) * SEGLEN;
     const bool live = i < g.hi[0] && s0 < g.hi[AX];
     unsigned flags = 0, cut = 0, cores = 0;
-    if (live) {
+    if constexpr (sizeof(T) == sizeof(float)) {
+        if (live) sweep_yz_f32_segment<AX, SCHEME, FLUX>(g, sv, i, o, s0, flags, cut, cores);
+    } else if (live) {
         const int s1 = min(s0 + SEGLEN, g.hi[AX]);
         const long long vs = g.vs;
         const long long sx = 1, sy = g.n[0], sz = (long long)g.n[0] * g.n[1];

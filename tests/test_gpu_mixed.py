@@ -81,3 +81,40 @@ def test_fp32_vortex_far_field_has_no_nonfinite_flags():
     s = c.solver(precision=capi.PREC_FP32_FLUX)
     st, _ = s.advance(1e30, max_steps=20)
     assert st.status_bits == 0 and st.steps == 20
+
+
+@pytest.mark.parametrize("recipe", ["weno5Rusanov", "teno5Rusanov", "weno5Roe"])
+def test_fp32_sweep_variant_step_close_to_fp64_oracle(recipe):
+    """The FP32-flux sweep kernels (2-D variant 0; the 3-D path) hold the
+    stencil as FP32 deviations from one reference node per warp chunk or
+    thread segment: one step within STEP_TOL of the oracle."""
+    n, h, bcs = (45, 38, 1), (0.021, 0.017, 1.0), (capi.BC_PERIODIC,) * 3
+    q = smooth_state(2, n, seed=9, shock=recipe != "teno5Rusanov")
+    spec = oracle_spec(2, n, h, bcs, bcs, recipe)
+    s = capi.Solver(2, n, h, bcs, bcs, recipe=recipe, time_recipe="SSPRK3", precision=capi.PREC_FP32_FLUX)
+    s.variant = 0
+    s.upload(np.ascontiguousarray(q))
+    scheme, flux = split_recipe(recipe)
+    Q = to_oracle(spec, q)
+    dt = po.dt(spec, Q, 0.5)
+    po.Stepper(spec, SCHEME_OF[scheme], FLUX_OF[flux], po.SSPRK3).step(Q, dt)
+    s.step(dt)
+    err = rel_linf(s.download().reshape(q.shape), from_oracle(spec, Q))
+    assert err.max() <= STEP_TOL, err
+
+
+def test_fp32_taylor_green_tracks_fp64():
+    """3-D Taylor-Green vortex (Mach 0.1, where p ~ 71 dwarfs the velocity
+    variation): 20 FP32-flux steps stay within 20 x STEP_TOL of the FP64 path
+    per variable, and the kinetic energy within 1e-6 relative."""
+    c = cases.taylor_green(24)
+    res = {}
+    for prec in (capi.PREC_FP64, capi.PREC_FP32_FLUX):
+        s = c.solver(precision=prec)
+        st, _ = s.advance(1e30, max_steps=20, graph_steps=4)
+        assert st.steps == 20 and st.status_bits == 0
+        res[prec] = s.download().reshape(c.q.shape)
+    q64, q32 = res[capi.PREC_FP64], res[capi.PREC_FP32_FLUX]
+    assert rel_linf(q32, q64).max() <= 20 * STEP_TOL
+    ke64, ke32 = cases.kinetic_energy(q64), cases.kinetic_energy(q32)
+    assert abs(ke32 - ke64) <= 1e-6 * ke64
