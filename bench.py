@@ -41,6 +41,11 @@ STATE_BYTES = 40
 # algorithmic FLOPs per face (reconstruction + flux), counted from the kernel
 # source: projection 12/pt, WENO5 core ~58 + 1 div, TENO5 core ~70 + 3 div,
 # back-projection 24, Rusanov ~60 + 2 div + 2 sqrt, eigen ~30 + rsqrt.
+# DRAM bytes (read + write) of one stage-1 launch of the fused 2-D tile kernel
+# on the 1024^2 vortex (22 x 22 tiles = variant 2), from one ncu --set full
+# capture per precision of the same command line with --quick.
+PROFILED_DRAM_BYTES = {("tile2d", 2, 1024, "fp32flux"): 42.036e6 + 4.637e6,
+                       ("tile2d", 2, 1024, "fp64"): 42.113e6 + 5.318e6}
 FLOPS_PER_FACE = {"weno5": 6 * 12 + 10 * 59 + 24 + 64 + 34, "teno5": 6 * 12 + 10 * 73 + 24 + 64 + 34}
 
 
@@ -253,17 +258,21 @@ def run_ours(args, rank, world):
     dom = int(np.argmax(ms_axes))
     fused = dim == 2 and s.variant > 0
     if fused:
-        # one fused launch per stage: 320 B per cell-step (SSPRK3, FP64 state)
-        # over the 3 launches of a step
-        bytes_node = 320.0 / 3.0
+        # one fused launch per stage; the timed launch is stage 1 (read Q^n,
+        # write Q1: 80 B per node; stages 2 and 3 also read Q^n: 120 B)
+        bytes_node = 2 * STATE_BYTES
     else:
         bytes_node = 2 * STATE_BYTES if (dim > 1 and dom == 0) else 4 * STATE_BYTES
     achieved = bytes_node * nodes / (ms_axes[dom] * 1e-3) / 1e9
     fp_peak = capi.fma_peak_tflops(fp64=(prec == capi.PREC_FP64), seconds=0.5)
     faces = nodes * (dim if fused else 1)  # faces evaluated by one launch
     fl = FLOPS_PER_FACE["teno5"] * faces / (ms_axes[dom] * 1e-3) / 1e12
+    traffic = PROFILED_DRAM_BYTES.get(("tile2d", s.variant, args.size, args.precision)) if fused else None
     out["roofline"] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
-                       "frac": round(achieved / hbm, 4), "traffic": None, "peak_source": f"{src} (MEASURED_PEAKS.json)",
+                       "frac": round(achieved / hbm, 4), "traffic": traffic,
+                       "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one stage-1 launch; "
+                                       "the output still resident in the write-back L2 at kernel end is not counted",
+                       "peak_source": f"{src} (MEASURED_PEAKS.json)",
                        "kernel": ("tile2d fused stage" if fused else f"sweep axis {dom}"),
                        "ms_per_launch": round(ms_axes[dom], 4),
                        "ms_per_axis": [round(x, 4) for x in ms_axes],
