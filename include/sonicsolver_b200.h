@@ -87,9 +87,17 @@ enum {
     SFG_BC_TRANSMISSIVE = 0,  /* zeroGradient: boundary node copies its inner
                                  neighbour and is not advanced; ghosts copy it
                                  (reconstruction/linear/SF_zeroGradient.cpp:88-105) */
-    SFG_BC_PERIODIC = 1       /* ghosts wrap; every node is advanced (the
+    SFG_BC_PERIODIC = 1,      /* ghosts wrap; every node is advanced (the
                                  reference declares PatchBoundaryKind::Periodic,
                                  SF_meshInterface.h:14, but never implements it) */
+    SFG_BC_FROZEN = 2         /* a patch with no boundary condition: the
+                                 boundary node is advanced and the ghosts keep
+                                 the values they were initialised with, the
+                                 boundary node's value at upload (or the
+                                 Field layout's first ghost layer)
+                                 (SF_applicator.h:162-187 with no BC for the
+                                 set; SF_mesh.cpp:544).  Single-grid solvers
+                                 only. */
 };
 /* Host array layouts for upload / download. */
 enum {

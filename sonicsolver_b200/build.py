@@ -72,7 +72,30 @@ def build(verbose: bool = False, force: bool = False) -> str:
         list(ex.map(run, jobs))
     if force or jobs or _stale(LIB, objs):
         run([nvcc, *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs])
+    build_host(verbose=verbose, force=force)
     return LIB
+
+
+HOST = os.path.join(HERE, "host")
+RUNNER = os.path.join(HERE, "sfg_run")
+
+
+def build_host(verbose: bool = False, force: bool = False) -> str:
+    """The C++17 host side (case reader, provider catalogs, plan, .vts writer)
+    linked into the ``sfg_run`` driver against the library (rpath $ORIGIN)."""
+    srcs = sorted(glob.glob(os.path.join(HOST, "*.cpp")))
+    deps = srcs + sorted(glob.glob(os.path.join(HOST, "*.hpp"))) + [os.path.join(ROOT, "include", "sonicsolver_b200.h"), LIB]
+    if not (force or _stale(RUNNER, deps)):
+        return RUNNER
+    cxx = shutil.which("g++") or "g++"
+    cmd = [cxx, "-std=c++17", "-O2", "-Wall", "-Wextra", "-o", RUNNER, *srcs, "-L", HERE, "-lsonicsolver_b200",
+           "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"host build failed:\n{' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    return RUNNER
 
 
 if __name__ == "__main__":

@@ -25,7 +25,7 @@ RECIPES = {
 }
 TIME_RECIPES = {"forwardEuler": 0, "SSPRK3": 1, "classicalRK4": 2}
 PREC_FP64, PREC_FP32_FLUX = 0, 1
-BC_TRANSMISSIVE, BC_PERIODIC = 0, 1
+BC_TRANSMISSIVE, BC_PERIODIC, BC_FROZEN = 0, 1, 2
 LAYOUT_NODES, LAYOUT_FIELD = 0, 1
 
 # The C-ABI symbols declared by include/sonicsolver_b200.h (checked by tests).

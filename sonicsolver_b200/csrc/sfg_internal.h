@@ -8,6 +8,9 @@ namespace sfg {
 
 constexpr int BC_TRANSMISSIVE = 0;
 constexpr int BC_PERIODIC = 1;
+// A frozen end: the device grid carries one extra, never advanced node at
+// that end holding the frozen ghost value, and ghost indices clamp to it.
+constexpr int BC_FROZEN = 2;
 
 // Status bits (match SFG_FLAG_* in include/sonicsolver_b200.h).
 constexpr unsigned FLAG_NONFINITE = 1u << 0;

@@ -389,13 +389,14 @@ __global__ void totals_kernel(GridView g, const double* __restrict__ q, double* 
     double acc[5] = {0, 0, 0, 0, 0};
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nodes;
          t += (long long)gridDim.x * blockDim.x) {
-        int i = (int)(t % g.n[0]);
-        int j = (int)((t / g.n[0]) % g.n[1]);
-        int k = (int)(t / ((long long)g.n[0] * g.n[1]));
-        if (g.dim > 0) i = map_index(i, g.n[0], g.bc_lo[0], g.bc_hi[0]);
-        if (g.dim > 1) j = map_index(j, g.n[1], g.bc_lo[1], g.bc_hi[1]);
-        if (g.dim > 2) k = map_index(k, g.n[2], g.bc_lo[2], g.bc_hi[2]);
-        const long long node = ((long long)k * g.n[1] + j) * g.n[0] + i;
+        int c[3] = {(int)(t % g.n[0]), (int)((t / g.n[0]) % g.n[1]), (int)(t / ((long long)g.n[0] * g.n[1]))};
+        bool extra = false;  // the frozen-ghost node of a frozen end is not a node of the case
+        for (int a = 0; a < g.dim; ++a) {
+            extra |= (g.bc_lo[a] == BC_FROZEN && c[a] == 0) || (g.bc_hi[a] == BC_FROZEN && c[a] == g.n[a] - 1);
+            c[a] = map_index(c[a], g.n[a], g.bc_lo[a], g.bc_hi[a]);
+        }
+        if (extra) continue;
+        const long long node = ((long long)c[2] * g.n[1] + c[1]) * g.n[0] + c[0];
         for (int v = 0; v < 5; ++v) acc[v] += q[v * g.vs + node];
     }
     for (int v = 0; v < 5; ++v) {

@@ -100,12 +100,18 @@ struct sfg_solver_s {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
-    sfg_grid_desc grid{};
+    sfg_grid_desc grid{};  // as the caller described it
+    // Device grid: `grid` plus one extra node at every frozen end, which
+    // holds the frozen ghost value and is never advanced.
+    sfg_grid_desc ig{};
+    int off_lo[3] = {0, 0, 0};  // 1 where the low end is frozen
+    bool frozen = false;
+    long long pub_nodes = 0;    // nodes of `grid`
     sfg_numerics_desc num{};
     const RecipeInfo* recipe = nullptr;
     int ng = 3;
     GridView gv{};
-    long long nodes = 0;
+    long long nodes = 0;        // nodes of the device grid
     double *qn = nullptr, *qa = nullptr, *qb = nullptr, *r = nullptr, *k = nullptr, *staging = nullptr;
     double* totals = nullptr;
     Clock* clock = nullptr;
@@ -145,26 +151,36 @@ int validate(const sfg_grid_desc* g, const sfg_numerics_desc* n, const RecipeInf
         const bool plo = g->bc_lo[d] == SFG_BC_PERIODIC, phi = g->bc_hi[d] == SFG_BC_PERIODIC;
         if (plo != phi) return fail(SFG_ERR_ARG, "axis %d: periodic must be set on both ends", d);
         for (int b : {g->bc_lo[d], g->bc_hi[d]})
-            if (b != SFG_BC_TRANSMISSIVE && b != SFG_BC_PERIODIC)
+            if (b != SFG_BC_TRANSMISSIVE && b != SFG_BC_PERIODIC && b != SFG_BC_FROZEN)
                 return fail(SFG_ERR_ARG, "axis %d: unknown boundary kind %d", d, b);
         if (plo && g->n[d] < reach + 1) return fail(SFG_ERR_ARG, "periodic axis %d needs >= %d nodes", d, reach + 1);
-        if (!plo && g->n[d] < 3) return fail(SFG_ERR_ARG, "transmissive axis %d needs >= 3 nodes", d);
+        const int extra = (g->bc_lo[d] == SFG_BC_FROZEN) + (g->bc_hi[d] == SFG_BC_FROZEN);
+        if (!plo && g->n[d] + extra < 3) return fail(SFG_ERR_ARG, "axis %d needs >= %d nodes", d, 3 - extra);
     }
     *recipe = r;
     return SFG_OK;
 }
 
 void make_view(sfg_solver_s* s) {
+    // device grid: one extra node per frozen end
+    s->ig = s->grid;
+    s->frozen = false;
+    s->pub_nodes = (long long)s->grid.n[0] * s->grid.n[1] * s->grid.n[2];
+    for (int a = 0; a < s->grid.dim; ++a) {
+        s->off_lo[a] = s->grid.bc_lo[a] == SFG_BC_FROZEN ? 1 : 0;
+        s->ig.n[a] += s->off_lo[a] + (s->grid.bc_hi[a] == SFG_BC_FROZEN ? 1 : 0);
+        s->frozen |= s->ig.n[a] != s->grid.n[a];
+    }
     GridView& g = s->gv;
-    const sfg_grid_desc& d = s->grid;
+    const sfg_grid_desc& d = s->ig;
     g.dim = d.dim;
     for (int a = 0; a < 3; ++a) {
         g.n[a] = d.n[a];
         g.bc_lo[a] = a < d.dim ? d.bc_lo[a] : BC_TRANSMISSIVE;
         g.bc_hi[a] = a < d.dim ? d.bc_hi[a] : BC_TRANSMISSIVE;
-        if (a < d.dim) {
-            g.lo[a] = d.bc_lo[a] == SFG_BC_TRANSMISSIVE ? 1 : 0;
-            g.hi[a] = d.bc_hi[a] == SFG_BC_TRANSMISSIVE ? d.n[a] - 1 : d.n[a];
+        if (a < d.dim) {  // transmissive boundary nodes and frozen extra nodes are not advanced
+            g.lo[a] = d.bc_lo[a] == SFG_BC_PERIODIC ? 0 : 1;
+            g.hi[a] = d.bc_hi[a] == SFG_BC_PERIODIC ? d.n[a] : d.n[a] - 1;
         } else {
             g.lo[a] = 0;
             g.hi[a] = 1;
@@ -321,18 +337,60 @@ void reset_clock(Clock* c, double t) {
 // node block.  Ghost values follow the same laws the kernels read through.
 long long field_extent(const sfg_solver_s* s, int a) { return s->grid.n[a] + 2LL * s->ng; }
 
+// Index map of the device grid (same laws as map_index in the kernels).
 int map_host(int i, int n, int bl, int bh) {
     if (bl == SFG_BC_PERIODIC) {
         while (i < 0) i += n;
+    } else if (bl == SFG_BC_FROZEN) {
+        if (i < 0) i = 0;
     } else if (i < 1) {
         i = n > 1 ? 1 : 0;
     }
     if (bh == SFG_BC_PERIODIC) {
         while (i >= n) i -= n;
+    } else if (bh == SFG_BC_FROZEN) {
+        if (i > n - 1) i = n - 1;
     } else if (i > n - 2) {
         i = n > 1 ? n - 2 : 0;
     }
     return i;
+}
+
+// Caller node layout -> device node layout (AoS).  A frozen end's extra node
+// takes the boundary node's value -- the reference initialises ghosts by
+// clamping to the interior (SF_mesh.cpp:544) -- or 0 with `zero_extra`.
+void nodes_to_device_layout(const sfg_solver_s* s, const double* pub, double* dev, bool zero_extra) {
+    const int* N = s->ig.n;
+    const int* P = s->grid.n;
+    for (int k = 0; k < N[2]; ++k)
+        for (int j = 0; j < N[1]; ++j)
+            for (int i = 0; i < N[0]; ++i) {
+                int c[3] = {i - s->off_lo[0], j - s->off_lo[1], k - s->off_lo[2]};
+                bool extra = false;
+                for (int a = 0; a < 3; ++a) {
+                    if (c[a] < 0) c[a] = 0, extra = true;
+                    if (c[a] >= P[a]) c[a] = P[a] - 1, extra = true;
+                }
+                double* out = dev + (((long long)k * N[1] + j) * N[0] + i) * 5;
+                if (extra && zero_extra) {
+                    std::memset(out, 0, 5 * sizeof(double));
+                    continue;
+                }
+                std::memcpy(out, pub + (((long long)c[2] * P[1] + c[1]) * P[0] + c[0]) * 5, 5 * sizeof(double));
+            }
+}
+
+// Device node layout -> caller node layout (drops the frozen extra nodes).
+void nodes_from_device_layout(const sfg_solver_s* s, const double* dev, double* pub) {
+    const int* N = s->ig.n;
+    const int* P = s->grid.n;
+    for (int k = 0; k < P[2]; ++k)
+        for (int j = 0; j < P[1]; ++j)
+            for (int i = 0; i < P[0]; ++i) {
+                const long long src =
+                    (((long long)(k + s->off_lo[2]) * N[1] + (j + s->off_lo[1])) * N[0] + (i + s->off_lo[0])) * 5;
+                std::memcpy(pub + (((long long)k * P[1] + j) * P[0] + i) * 5, dev + src, 5 * sizeof(double));
+            }
 }
 
 }  // namespace
@@ -443,7 +501,7 @@ int sfg_ghost_layers(sfg_solver s, int* ng) {
 
 int sfg_state_size(sfg_solver s, int layout, size_t* count) {
     if (!s || !count) return fail(SFG_ERR_ARG, "null argument");
-    if (layout == SFG_LAYOUT_NODES) *count = 5 * (size_t)s->nodes;
+    if (layout == SFG_LAYOUT_NODES) *count = 5 * (size_t)s->pub_nodes;
     else if (layout == SFG_LAYOUT_FIELD)
         *count = 5 * (size_t)(field_extent(s, 0) * field_extent(s, 1) * field_extent(s, 2));
     else return fail(SFG_ERR_ARG, "unknown layout %d", layout);
@@ -453,6 +511,14 @@ int sfg_state_size(sfg_solver s, int layout, size_t* count) {
 static int upload_nodes_host(sfg_solver s, const double* nodes_aos) {
     CUDA_TRY(cudaMemcpyAsync(s->staging, nodes_aos, sizeof(double) * 5 * s->nodes, cudaMemcpyHostToDevice, s->stream));
     CUDA_TRY(launch_aos_to_soa(s->staging, s->qn, s->nodes, s->gv.vs, s->stream));
+    if (s->frozen) {
+        // Stage kernels write solved nodes only, and stage outputs (and the
+        // Euler copy-back qa -> qn) are read as the next state: every stage
+        // buffer must hold the frozen ghost value in its extra nodes.
+        const size_t bytes = sizeof(double) * 5 * (size_t)s->gv.vs;
+        CUDA_TRY(cudaMemcpyAsync(s->qa, s->qn, bytes, cudaMemcpyDeviceToDevice, s->stream));
+        CUDA_TRY(cudaMemcpyAsync(s->qb, s->qn, bytes, cudaMemcpyDeviceToDevice, s->stream));
+    }
     return SFG_OK;
 }
 
@@ -466,18 +532,28 @@ static int reset_time(sfg_solver s, double time) {
 
 int sfg_upload(sfg_solver s, const double* host, int layout, double time) {
     if (!s || !host) return fail(SFG_ERR_ARG, "null argument");
-    if (layout == SFG_LAYOUT_NODES) {
+    if (layout == SFG_LAYOUT_NODES && !s->frozen) {
         int rc = upload_nodes_host(s, host);
         if (rc) return rc;
+    } else if (layout == SFG_LAYOUT_NODES) {
+        std::vector<double> tmp(5 * (size_t)s->nodes);
+        nodes_to_device_layout(s, host, tmp.data(), false);
+        int rc = upload_nodes_host(s, tmp.data());
+        if (rc) return rc;
+        CUDA_TRY(cudaStreamSynchronize(s->stream));
     } else if (layout == SFG_LAYOUT_FIELD) {
+        // device node (i, j, k) <- Field entry at caller node (i - off) + ng:
+        // a frozen end's extra node reads the Field's first ghost layer
         std::vector<double> tmp(5 * (size_t)s->nodes);
         const long long mx = field_extent(s, 0), my = field_extent(s, 1);
         const int ng = s->ng;
-        for (int k = 0; k < s->grid.n[2]; ++k)
-            for (int j = 0; j < s->grid.n[1]; ++j)
-                for (int i = 0; i < s->grid.n[0]; ++i) {
-                    const long long src = (((long long)(k + ng) * my + (j + ng)) * mx + (i + ng)) * 5;
-                    const long long dst = (((long long)k * s->grid.n[1] + j) * s->grid.n[0] + i) * 5;
+        const int* N = s->ig.n;
+        for (int k = 0; k < N[2]; ++k)
+            for (int j = 0; j < N[1]; ++j)
+                for (int i = 0; i < N[0]; ++i) {
+                    const long long fi = i - s->off_lo[0] + ng, fj = j - s->off_lo[1] + ng, fk = k - s->off_lo[2] + ng;
+                    const long long src = ((fk * my + fj) * mx + fi) * 5;
+                    const long long dst = (((long long)k * N[1] + j) * N[0] + i) * 5;
                     std::memcpy(&tmp[dst], host + src, 5 * sizeof(double));
                 }
         int rc = upload_nodes_host(s, tmp.data());
@@ -491,12 +567,14 @@ int sfg_upload(sfg_solver s, const double* host, int layout, double time) {
 
 int sfg_upload_device(sfg_solver s, const double* dev_nodes_aos, double time) {
     if (!s || !dev_nodes_aos) return fail(SFG_ERR_ARG, "null argument");
+    if (s->frozen) return fail(SFG_ERR_ARG, "frozen boundary ends need sfg_upload (host layouts)");
     CUDA_TRY(launch_aos_to_soa(dev_nodes_aos, s->qn, s->nodes, s->gv.vs, s->stream));
     return reset_time(s, time);
 }
 
 int sfg_download_device(sfg_solver s, double* dev_nodes_aos) {
     if (!s || !dev_nodes_aos) return fail(SFG_ERR_ARG, "null argument");
+    if (s->frozen) return fail(SFG_ERR_ARG, "frozen boundary ends need sfg_download (host layouts)");
     CUDA_TRY(launch_soa_to_aos(s->gv, s->qn, dev_nodes_aos, s->stream));
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     return SFG_OK;
@@ -505,29 +583,36 @@ int sfg_download_device(sfg_solver s, double* dev_nodes_aos) {
 int sfg_download(sfg_solver s, double* host, int layout) {
     if (!s || !host) return fail(SFG_ERR_ARG, "null argument");
     CUDA_TRY(launch_soa_to_aos(s->gv, s->qn, s->staging, s->stream));
-    if (layout == SFG_LAYOUT_NODES) {
+    if (layout == SFG_LAYOUT_NODES && !s->frozen) {
         CUDA_TRY(cudaMemcpyAsync(host, s->staging, sizeof(double) * 5 * s->nodes, cudaMemcpyDeviceToHost, s->stream));
         CUDA_TRY(cudaStreamSynchronize(s->stream));
         return SFG_OK;
     }
-    if (layout != SFG_LAYOUT_FIELD) return fail(SFG_ERR_ARG, "unknown layout %d", layout);
+    if (layout != SFG_LAYOUT_NODES && layout != SFG_LAYOUT_FIELD) return fail(SFG_ERR_ARG, "unknown layout %d", layout);
     std::vector<double> tmp(5 * (size_t)s->nodes);
     CUDA_TRY(cudaMemcpyAsync(tmp.data(), s->staging, sizeof(double) * 5 * s->nodes, cudaMemcpyDeviceToHost, s->stream));
     CUDA_TRY(cudaStreamSynchronize(s->stream));
+    if (layout == SFG_LAYOUT_NODES) {
+        nodes_from_device_layout(s, tmp.data(), host);
+        return SFG_OK;
+    }
+    // Field entry (i, j, k) <- device node map(caller node (i - ng) + off):
+    // ghosts follow the boundary laws, a frozen end's ghosts its extra node
     const long long mx = field_extent(s, 0), my = field_extent(s, 1), mz = field_extent(s, 2);
     const int ng = s->ng;
+    const int* N = s->ig.n;
     for (long long k = 0; k < mz; ++k)
         for (long long j = 0; j < my; ++j)
             for (long long i = 0; i < mx; ++i) {
                 int c[3] = {(int)i - ng, (int)j - ng, (int)k - ng};
                 for (int a = 0; a < 3; ++a) {
-                    if (a < s->grid.dim) {
-                        c[a] = map_host(c[a], s->grid.n[a], s->grid.bc_lo[a], s->grid.bc_hi[a]);
+                    if (a < s->ig.dim) {
+                        c[a] = map_host(c[a] + s->off_lo[a], N[a], s->ig.bc_lo[a], s->ig.bc_hi[a]);
                     } else {
-                        c[a] = c[a] < 0 ? 0 : (c[a] >= s->grid.n[a] ? s->grid.n[a] - 1 : c[a]);
+                        c[a] = c[a] < 0 ? 0 : (c[a] >= N[a] ? N[a] - 1 : c[a]);
                     }
                 }
-                const long long src = (((long long)c[2] * s->grid.n[1] + c[1]) * s->grid.n[0] + c[0]) * 5;
+                const long long src = (((long long)c[2] * N[1] + c[1]) * N[0] + c[0]) * 5;
                 std::memcpy(host + ((k * my + j) * mx + i) * 5, &tmp[src], 5 * sizeof(double));
             }
     return SFG_OK;
@@ -707,9 +792,17 @@ int sfg_residual(sfg_solver s, double* host_nodes_aos) {
     for (int a = 0; a < 3; ++a) raw.bc_lo[a] = raw.bc_hi[a] = BC_PERIODIC;  // identity mapping inside [0,n)
     raw.dim = 0;
     CUDA_TRY(launch_soa_to_aos(raw, s->r, s->staging, s->stream));
-    CUDA_TRY(cudaMemcpyAsync(host_nodes_aos, s->staging, sizeof(double) * 5 * s->nodes, cudaMemcpyDeviceToHost,
-                             s->stream));
-    return sync_and_check(s);
+    if (!s->frozen) {
+        CUDA_TRY(cudaMemcpyAsync(host_nodes_aos, s->staging, sizeof(double) * 5 * s->nodes, cudaMemcpyDeviceToHost,
+                                 s->stream));
+        return sync_and_check(s);
+    }
+    std::vector<double> tmp(5 * (size_t)s->nodes);
+    CUDA_TRY(cudaMemcpyAsync(tmp.data(), s->staging, sizeof(double) * 5 * s->nodes, cudaMemcpyDeviceToHost, s->stream));
+    rc = sync_and_check(s);
+    if (rc) return rc;
+    nodes_from_device_layout(s, tmp.data(), host_nodes_aos);
+    return SFG_OK;
 }
 
 int sfg_stage_with_residual(sfg_solver s, int stage, double dt, const double* host_residual) {
@@ -717,8 +810,15 @@ int sfg_stage_with_residual(sfg_solver s, int stage, double dt, const double* ho
     const int ns = stage_count(s->num.time_recipe);
     if (stage != s->next_stage || stage < 0 || stage >= ns)
         return fail(SFG_ERR_ARG, "explicit stage %d out of order (expected %d)", stage, s->next_stage);
+    std::vector<double> tmp;
+    if (s->frozen) {  // the extra nodes carry no residual
+        tmp.resize(5 * (size_t)s->nodes);
+        nodes_to_device_layout(s, host_residual, tmp.data(), true);
+        host_residual = tmp.data();
+    }
     CUDA_TRY(cudaMemcpyAsync(s->staging, host_residual, sizeof(double) * 5 * s->nodes, cudaMemcpyHostToDevice,
                              s->stream));
+    if (s->frozen) CUDA_TRY(cudaStreamSynchronize(s->stream));
     CUDA_TRY(launch_aos_to_soa(s->staging, s->r, s->nodes, s->gv.vs, s->stream));
     CUDA_TRY(launch_set_dt(s->clock, dt, s->stream));
     StageView sv = stage_view(s, stage, false, false);

@@ -10,15 +10,20 @@ namespace sfg {
 // Ghost and boundary-node values by index mapping (no ghost storage):
 // transmissive ends read the inner neighbour (zeroGradient: boundary node <-
 // inner node, ghosts <- boundary node; SF_zeroGradient.cpp:88-105), periodic
-// ends wrap.
+// ends wrap, frozen ends read the extra end node that holds the frozen ghost
+// value.
 __device__ __forceinline__ int map_index(int i, int n, int bcl, int bch) {
     if (bcl == BC_PERIODIC) {
         if (i < 0) i += n;
+    } else if (bcl == BC_FROZEN) {
+        if (i < 0) i = 0;
     } else if (i < 1) {
         i = 1;
     }
     if (bch == BC_PERIODIC) {
         if (i >= n) i -= n;
+    } else if (bch == BC_FROZEN) {
+        if (i > n - 1) i = n - 1;
     } else if (i > n - 2) {
         i = n - 2;
     }

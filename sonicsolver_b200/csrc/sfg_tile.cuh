@@ -54,14 +54,17 @@ struct Tile1Shape {
 // Halo index mapping for tile loads.  A partial tile at the high end of an
 // axis reaches up to TX - 1 + H nodes past the last node, which can exceed
 // one period on small periodic grids, so periodic indices take a full modulo
-// (both ends are periodic or neither); transmissive ones clamp.  Every result
-// lies in [0, n).
-__device__ __forceinline__ int map_tile_index(int i, int n, int bcl) {
+// (both ends are periodic or neither); transmissive ends clamp to the inner
+// neighbour of the boundary node, frozen ends to their extra end node.  Every
+// result lies in [0, n).
+__device__ __forceinline__ int map_tile_index(int i, int n, int bcl, int bch) {
     if (bcl == BC_PERIODIC) {
         i %= n;
         return i < 0 ? i + n : i;
     }
-    return i < 1 ? 1 : (i > n - 2 ? n - 2 : i);
+    const int lo = bcl == BC_FROZEN ? 0 : 1;
+    const int hi = bch == BC_FROZEN ? n - 1 : n - 2;
+    return i < lo ? lo : (i > hi ? hi : i);
 }
 
 // ------------------------------------------------------------------ 2-D FP64
@@ -78,8 +81,8 @@ __device__ __forceinline__ void tile2d_body(const GridView& g, const StageView& 
     for (int t = threadIdx.x; t < SX * SY; t += blockDim.x) {
         const int r = t / SX, c = t - r * SX;
         if ((r < H || r >= TY + H) && (c < H || c >= TX + H)) continue;  // corners are never read
-        const int gx = map_tile_index(x0 - H + c, g.n[0], g.bc_lo[0]);
-        const int gy = map_tile_index(y0 - H + r, g.n[1], g.bc_lo[1]);
+        const int gx = map_tile_index(x0 - H + c, g.n[0], g.bc_lo[0], g.bc_hi[0]);
+        const int gy = map_tile_index(y0 - H + r, g.n[1], g.bc_lo[1], g.bc_hi[1]);
         const long long at = (long long)gy * nx + gx;
 #pragma unroll
         for (int v = 0; v < 5; ++v) sq[v * SX * SY + t] = __ldg(sv.qs + v * vs + at);
@@ -155,8 +158,8 @@ __device__ __forceinline__ void tile2d_f32_body(const GridView& g, const StageVi
     for (int t = threadIdx.x; t < SX * SY; t += blockDim.x) {
         const int r = t / SX, c = t - r * SX;
         if ((r < H || r >= TY + H) && (c < H || c >= TX + H)) continue;
-        const int gx = map_tile_index(x0 - H + c, g.n[0], g.bc_lo[0]);
-        const int gy = map_tile_index(y0 - H + r, g.n[1], g.bc_lo[1]);
+        const int gx = map_tile_index(x0 - H + c, g.n[0], g.bc_lo[0], g.bc_hi[0]);
+        const int gy = map_tile_index(y0 - H + r, g.n[1], g.bc_lo[1], g.bc_hi[1]);
         const long long at = (long long)gy * nx + gx;
 #pragma unroll
         for (int v = 0; v < 5; ++v) sq[v * SX * SY + t] = float(__ldg(sv.qs + v * vs + at) - qref[v]);
@@ -231,7 +234,7 @@ __device__ __forceinline__ void tile1d_body(const GridView& g, const StageView& 
     }
     const Ref32 ref = F32 ? make_ref32(qref, g.gamma) : Ref32{};
     for (int t = threadIdx.x; t < SX; t += blockDim.x) {
-        const int gx = map_tile_index(x0 - H + t, g.n[0], g.bc_lo[0]);
+        const int gx = map_tile_index(x0 - H + t, g.n[0], g.bc_lo[0], g.bc_hi[0]);
 #pragma unroll
         for (int v = 0; v < 5; ++v) sq[v * SX + t] = T(__ldg(sv.qs + v * vs + gx) - qref[v]);
     }

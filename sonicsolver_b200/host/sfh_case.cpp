@@ -1,0 +1,306 @@
+// sfh_case.cpp -- case directory reader (see sfh_case.hpp).
+#include "sfh_case.hpp"
+
+#include <algorithm>
+#include <cctype>
+#include <cmath>
+#include <fstream>
+
+#include "sfh_yaml.hpp"
+
+namespace sfh {
+namespace {
+
+bool exists(const std::string& path) { return std::ifstream(path).good(); }
+
+std::string join(const std::string& dir, const std::string& rel) { return dir + "/" + rel; }
+
+// File of a registry entry (`entry: {type: ..., file: ...}`), else `fallback`.
+std::string registry_file(const std::string& dir, const std::string& registry, const std::string& entry,
+                          const std::string& fallback) {
+    const std::string reg = join(dir, registry);
+    if (exists(reg)) {
+        const Node r = load_yaml_file(reg);
+        if (const Node* e = r.get(entry))
+            if (const Node* f = e->get("file")) return join(dir, f->str());
+    }
+    return join(dir, fallback);
+}
+
+std::vector<double> numbers(const Node& n, size_t want, const std::string& what) {
+    std::vector<double> v;
+    if (n.is_scalar()) v.push_back(n.number());
+    else if (n.is_seq())
+        for (const auto& x : n.items) v.push_back(x.number());
+    if (v.size() != want)
+        throw ParseError(what + ": expected " + std::to_string(want) + " component(s)");
+    return v;
+}
+
+InitialValue initial_value(const Node& n, size_t comps, const std::string& var) {
+    InitialValue iv;
+    if (!n.is_map()) {  // bare value: uniform
+        iv.base = numbers(n, comps, var);
+        return iv;
+    }
+    for (const auto& kv : n.fields) {
+        if (kv.first == "uniform" || kv.first == "default") {
+            iv.base = numbers(kv.second, comps, var + "." + kv.first);
+        } else if (kv.second.is_map()) {
+            throw Unsupported("internalField " + var + "." + kv.first +
+                              ": generated set values (type: ...) are not supported for " + var);
+        } else {
+            iv.sets.emplace_back(kv.first, numbers(kv.second, comps, var + "." + kv.first));
+        }
+    }
+    if (iv.base.empty()) iv.base.assign(comps, 0.0);
+    return iv;
+}
+
+std::string lower(std::string s) {
+    for (auto& ch : s) ch = char(std::tolower((unsigned char)ch));
+    return s;
+}
+
+// The convection recipe token of a numerics file, in either form the
+// reference reads: `terms: {convection: weno5Rusanov}`, or
+// `convection: {default: WENO5, flux: Rusanov, reconstruction: ...}` whose
+// scheme and flux-splitter names compose the same token
+// (src/app/application/model/parsing/SF_numericsParser.h:11-162).
+std::string convection_token(const Node& nu) {
+    if (const Node* terms = nu.get("terms")) {
+        for (const auto& kv : terms->fields)
+            if (kv.first != "convection")
+                throw Unsupported("term '" + kv.first + "': the provider implements the convection term only");
+        return terms->at("convection").str();
+    }
+    const Node* cv = nu.get("convection");
+    if (!cv) throw Unsupported("numerics select no convection scheme");
+    if (const Node* r = cv->get("reconstruction"))
+        if (lower(r->str()) != "characteristic" && lower(r->str()) != "char")
+            throw Unsupported("reconstruction '" + r->str() + "': the provider reconstructs characteristic variables");
+    // a `diffusion:` block is inert while transport is disabled (checked by the caller)
+    const std::string scheme = lower(cv->at("default").str());
+    const std::string f = cv->get("flux") ? lower(cv->at("flux").str()) : "rusanov";
+    std::string flux;
+    if (f == "rusanov" || f == "localaxfriedrichs" || f == "llf") flux = "Rusanov";
+    else if (f == "roe") flux = "Roe";
+    else if (f == "laxfriedrichs" || f == "lf" || f == "lxf" || f == "laxf") flux = "LaxFriedrichs";
+    else if (f == "laxwendroff" || f == "lw") flux = "LaxWendroff";
+    else if (f == "stegerwarming" || f == "sw") flux = "StegerWarming";
+    else throw Unsupported("flux splitter '" + cv->at("flux").str() + "'");
+    return scheme + flux;
+}
+
+// Condition token of one patch entry: `zeroGradient` or `{type: zeroGradient}`.
+std::string condition(const Node& n) {
+    if (n.is_scalar()) return n.str();
+    if (const Node* t = n.get("type")) return t->str();
+    throw ParseError("boundary condition without a type");
+}
+
+}  // namespace
+
+CaseSpec load_case(const std::string& dir) {
+    CaseSpec c;
+    c.dir = dir;
+    if (exists(join(dir, "case.yaml"))) {
+        const Node cs = load_yaml_file(join(dir, "case.yaml"));
+        if (const Node* nm = cs.get("name")) c.name = nm->str();
+    }
+    // ---- solvers
+    const Node rt = load_yaml_file(registry_file(dir, "solvers/solvers.yaml", "runtime", "solvers/runtime.yaml"));
+    if (const Node* v = rt.get("startTime")) c.start_time = v->number();
+    c.end_time = rt.at("endTime").number();
+    if (const Node* v = rt.get("CFL")) c.cfl = v->number();
+    if (const Node* v = rt.get("writeControl")) c.write_control = v->str();
+    if (const Node* v = rt.get("writeInterval")) c.write_interval = v->number();
+    if (const Node* v = rt.get("writeInitial")) c.write_initial = v->boolean();
+    if (const Node* v = rt.get("maxDeltaT")) c.max_dt = v->number();
+    if (const Node* o = rt.get("output")) {
+        if (const Node* v = o->get("jobName")) c.job_name = v->str();
+        if (const Node* v = o->get("outputDir")) c.output_dir = v->str();
+    }
+    if (c.job_name.empty()) c.job_name = c.name.empty() ? "case" : c.name;
+    const Node nu = load_yaml_file(registry_file(dir, "solvers/solvers.yaml", "numerics", "solvers/numerics.yaml"));
+    c.time_recipe = nu.at("time").at("default").str();
+    c.convection = convection_token(nu);
+    if (const Node* tr = nu.get("transport"))
+        if (const Node* en = tr->get("enable"))
+            if (en->boolean()) throw Unsupported("transport enabled: viscous terms are outside the explicit Euler path");
+    const std::string alg = registry_file(dir, "solvers/solvers.yaml", "algorithm", "solvers/algorithm.yaml");
+    c.algorithm = exists(alg) ? load_yaml_file(alg).at("type").str() : "densityBase";
+    // ---- thermodynamics
+    const std::string th = registry_file(dir, "models/models.yaml", "thermoDynamics", "models/thermoDynamics.yaml");
+    if (exists(th)) {
+        const Node t = load_yaml_file(th);
+        if (const Node* td = t.get("thermoDynamics"))
+            if (const Node* eos = td->get("equationOfState"))
+                if (eos->str() != "perfectGas")
+                    throw Unsupported("equationOfState '" + eos->str() + "': the provider implements perfectGas");
+        if (const Node* pr = t.get("properties"))
+            if (const Node* eos = pr->get("equationOfState")) {
+                if (const Node* g = eos->get("gamma")) c.gamma = g->number();
+                if (const Node* r = eos->get("R")) c.gas_R = r->number();
+            }
+    }
+    // ---- mesh: one axis-aligned block
+    const Node gen = load_yaml_file(registry_file(dir, "mesh/mesh.yaml", "generation", "mesh/generation.yaml"));
+    const double scale = gen.get("scale") ? gen.at("scale").number() : 1.0;
+    if (const Node* ng = gen.get("nGhost")) c.ghost_layers = int(ng->integer());
+    const Node& verts = gen.at("vertices");
+    const Node& blocks = gen.at("blocks");
+    if (!blocks.is_seq() || blocks.items.size() != 1)
+        throw Unsupported("mesh: the provider runs a single structured block");
+    const Node& blk = blocks.items[0];
+    const auto cells = numbers(blk.at("cells"), 3, "blocks[0].cells");
+    for (int d = 0; d < 3; ++d) {
+        c.cells[d] = int(cells[d]);
+        c.lo[d] = 1e300;
+        c.hi[d] = -1e300;
+    }
+    for (const auto& v : verts.items) {
+        const auto x = numbers(v, 3, "vertex");
+        for (int d = 0; d < 3; ++d) {
+            c.lo[d] = std::min(c.lo[d], x[d] * scale);
+            c.hi[d] = std::max(c.hi[d], x[d] * scale);
+        }
+    }
+    for (const auto& v : verts.items) {  // every vertex on a corner of the box
+        const auto x = numbers(v, 3, "vertex");
+        for (int d = 0; d < 3; ++d)
+            if (std::fabs(x[d] * scale - c.lo[d]) > 1e-12 * (1 + std::fabs(c.lo[d])) &&
+                std::fabs(x[d] * scale - c.hi[d]) > 1e-12 * (1 + std::fabs(c.hi[d])))
+                throw Unsupported("mesh: curvilinear blocks need per-node metrics (not in this provider)");
+    }
+    if (const Node* gr = blk.get("grading")) {
+        for (double g : numbers(*gr, 3, "grading"))
+            if (g != 1.0) throw Unsupported("mesh: graded blocks need per-node metrics (not in this provider)");
+    }
+    // ---- fields
+    const std::string inf = registry_file(dir, "fields/fields.yaml", "internalField", "fields/internalField.yaml");
+    const Node in = load_yaml_file(inf);
+    c.rho = initial_value(in.at("rho"), 1, "rho");
+    c.U = initial_value(in.at("U"), 3, "U");
+    c.p = initial_value(in.at("p"), 1, "p");
+    const Node bc = load_yaml_file(registry_file(dir, "fields/fields.yaml", "boundaries", "fields/boundaries.yaml"));
+    for (const char* var : {"rho", "U", "p"}) {
+        const Node* vb = bc.get(var);
+        if (!vb) continue;
+        for (const auto& kv : vb->fields) {
+            const std::string cond = condition(kv.second);
+            auto it = c.patch_bc.find(kv.first);
+            if (it == c.patch_bc.end()) c.patch_bc[kv.first] = cond;
+            else if (it->second != cond)
+                throw Unsupported("patch '" + kv.first + "': rho, U and p carry different conditions (" + it->second +
+                                  " / " + cond + "); the provider applies one condition per patch");
+        }
+    }
+    return c;
+}
+
+namespace {
+
+// Boundary patches of the structured generator per axis (low end, high end)
+// and their aliases.
+struct AxisPatches {
+    const char* lo;
+    const char* hi;
+    const char* alt_lo;
+    const char* alt_hi;
+};
+const AxisPatches kPatches[3] = {{"Left", "Right", "inlet", "outlet"},
+                                 {"sideWalls", "sideWalls", "walls", "walls"},
+                                 {"frontBack", "frontBack", "walls", "walls"}};
+
+const std::string* patch_condition(const CaseSpec& c, const char* name, const char* alt) {
+    auto it = c.patch_bc.find(name);
+    if (it != c.patch_bc.end()) return &it->second;
+    it = c.patch_bc.find(alt);
+    return it != c.patch_bc.end() ? &it->second : nullptr;
+}
+
+int bc_kind(const std::string& token, const char* patch) {
+    if (token == "zeroGradient") return SFG_BC_TRANSMISSIVE;
+    if (token == "periodic" || token == "cyclic") return SFG_BC_PERIODIC;
+    throw Unsupported(std::string("patch '") + patch + "': condition '" + token +
+                      "' is not provided on the GPU (zeroGradient, periodic, empty are)");
+}
+
+}  // namespace
+
+GridSetup build_grid(const CaseSpec& c) {
+    if (c.algorithm != "densityBase")
+        throw Unsupported("algorithm '" + c.algorithm + "': the provider implements the densityBase explicit path");
+    GridSetup g;
+    bool active[3];
+    for (int d = 0; d < 3; ++d) {
+        const AxisPatches& P = kPatches[d];
+        const std::string* lo = patch_condition(c, P.lo, P.alt_lo);
+        const std::string* hi = patch_condition(c, P.hi, P.alt_hi);
+        const bool empty = (lo && *lo == "empty") || (hi && *hi == "empty");
+        if (empty || (c.cells[d] <= 1 && !lo && !hi)) {
+            active[d] = false;
+            continue;
+        }
+        // a patch without a condition keeps its initial ghost state and its
+        // boundary node is advanced (SF_applicator.h:162-187): SFG_BC_FROZEN
+        active[d] = true;
+        g.grid.bc_lo[d] = lo ? bc_kind(*lo, P.lo) : SFG_BC_FROZEN;
+        g.grid.bc_hi[d] = hi ? bc_kind(*hi, P.hi) : SFG_BC_FROZEN;
+        if ((g.grid.bc_lo[d] == SFG_BC_PERIODIC) != (g.grid.bc_hi[d] == SFG_BC_PERIODIC))
+            throw Unsupported(std::string("axis ") + "xyz"[d] + ": periodic must hold at both ends");
+    }
+    if ((active[1] && !active[0]) || (active[2] && !active[1]))
+        throw Unsupported("active axes must be x, x-y or x-y-z (the provider does not permute axes)");
+    g.grid.dim = int(active[0]) + int(active[1]) + int(active[2]);
+    if (g.grid.dim == 0) throw Unsupported("no active axis");
+    for (int d = 0; d < 3; ++d) {
+        const double len = c.hi[d] - c.lo[d];
+        g.origin[d] = c.lo[d];
+        if (active[d]) {
+            if (c.cells[d] < 2) throw Unsupported(std::string("axis ") + "xyz"[d] + " needs at least 2 cells");
+            g.nodes[d] = g.grid.bc_lo[d] == SFG_BC_PERIODIC ? c.cells[d] : c.cells[d] + 1;
+            g.grid.h[d] = len / c.cells[d];
+        } else {
+            g.nodes[d] = 1;
+            g.grid.h[d] = len > 0 ? len : 1.0;
+            g.grid.bc_lo[d] = g.grid.bc_hi[d] = SFG_BC_TRANSMISSIVE;
+        }
+        g.grid.n[d] = g.nodes[d];
+        if (!(g.grid.h[d] > 0)) throw Unsupported("degenerate block extent");
+    }
+    // initial state: base values, then the named sets in file order
+    const int nx = g.nodes[0], ny = g.nodes[1], nz = g.nodes[2];
+    const int split = nx / 2;  // leftHalf: i < nx / 2
+    auto value_at = [&](const InitialValue& iv, int i, size_t comp) {
+        double v = iv.base[comp];
+        for (const auto& s : iv.sets) {
+            bool in;
+            if (s.first == "leftHalf") in = i < split;
+            else if (s.first == "rightHalf") in = i >= split;
+            else if (s.first == "all") in = true;
+            else throw Unsupported("internalField set '" + s.first + "' is not a generated structured set");
+            if (in) v = s.second[comp];
+        }
+        return v;
+    };
+    g.q.resize(size_t(nx) * ny * nz * 5);
+    const double gm1 = c.gamma - 1.0;
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                const double rho = value_at(c.rho, i, 0), p = value_at(c.p, i, 0);
+                const double u[3] = {value_at(c.U, i, 0), value_at(c.U, i, 1), value_at(c.U, i, 2)};
+                if (!(rho > 0) || !(p > 0)) throw Unsupported("initial state has rho <= 0 or p <= 0");
+                double* q = &g.q[((size_t(k) * ny + j) * nx + i) * 5];
+                q[0] = rho;
+                q[1] = rho * u[0];
+                q[2] = rho * u[1];
+                q[3] = rho * u[2];
+                q[4] = p / gm1 + 0.5 * rho * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+            }
+    return g;
+}
+
+}  // namespace sfh

@@ -1,0 +1,370 @@
+// sfh_run.cpp -- `sfg_run`: runs a sonicSolver case directory on the GPU
+// provider, through the same selection steps the reference's compiled plan
+// takes:
+//   1. read the case (sfh_case), build the grid and the initial state;
+//   2. resolve the convection term in the TermCatalog and the plan's
+//      operations in the ProviderCatalog (exactly one provider each);
+//   3. build the conservative explicit plan, bind every operation id to a
+//      C-ABI call of this library, validate the bindings;
+//   4. run it, writing .vts output at the case's write times.
+//
+//   sfg_run CASE_DIR [--mode graph|plan] [--precision fp64|fp32flux]
+//                    [--graph-steps K] [--dump FILE] [--no-write] [--describe]
+//
+// --mode plan executes the plan operation by operation (one C-ABI call per
+// operation, host synchronous).  --mode graph (default) lowers the time loop
+// between two output times to one sfg_advance call: the device-resident
+// clock runs the same dt, stage and commit sequence inside CUDA graphs.
+// --describe stops after step 3 and touches no GPU.
+// Exit codes: 0 done, 1 error, 2 usage, 3 case not supported by the provider.
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <string>
+#include <sys/stat.h>
+#include <vector>
+
+#include "../../include/sonicsolver_b200.h"
+#include "sfh_case.hpp"
+#include "sfh_catalog.hpp"
+#include "sfh_plan.hpp"
+#include "sfh_vts.hpp"
+#include "sfh_yaml.hpp"
+
+namespace {
+
+using namespace sfh;
+
+struct Options {
+    std::string dir, mode = "graph", dump;
+    int precision = SFG_PREC_FP64;
+    int graph_steps = 32;
+    bool write = true, describe_only = false;
+};
+
+int usage() {
+    std::fprintf(stderr,
+                 "usage: sfg_run CASE_DIR [--mode graph|plan] [--precision fp64|fp32flux] [--graph-steps K]\n"
+                 "               [--dump FILE] [--no-write] [--describe]\n");
+    return 2;
+}
+
+int time_id(const std::string& token, int& stages) {
+    if (token == "forwardEuler") return stages = 1, SFG_TIME_FORWARD_EULER;
+    if (token == "SSPRK3") return stages = 3, SFG_TIME_SSPRK3;
+    if (token == "classicalRK4") return stages = 4, SFG_TIME_CLASSICAL_RK4;
+    throw Unsupported("time recipe '" + token + "': the provider implements forwardEuler, SSPRK3, classicalRK4");
+}
+
+std::string json_escape(const std::string& s) {
+    std::string o;
+    for (char c : s) {
+        if (c == '"' || c == '\\') o += '\\';
+        o += c;
+    }
+    return o;
+}
+
+// Everything the bound operations share.
+struct Run {
+    const CaseSpec* c = nullptr;
+    const GridSetup* g = nullptr;
+    sfg_solver s = nullptr;
+    bool write = true;
+    double next_out = 0.0;
+    int outputs = 0;
+    std::string out_dir;
+    std::vector<double> host;
+};
+
+bool at_or_past(double t, double mark) {
+    const double sc = std::fabs(t) < 1.0 ? 1.0 : std::fabs(t);
+    return t >= mark - 1e-11 * sc;
+}
+
+int write_output(Run& r, double t) {
+    if (!r.write) return 0;
+    if (int rc = sfg_download(r.s, r.host.data(), SFG_LAYOUT_NODES)) return rc;
+    char name[64];
+    std::snprintf(name, sizeof name, "_%04d.vts", r.outputs);
+    const std::string path = r.out_dir + "/" + r.c->job_name + name;
+    VtsGeometry geo{{r.g->nodes[0], r.g->nodes[1], r.g->nodes[2]},
+                    {r.g->origin[0], r.g->origin[1], r.g->origin[2]},
+                    {r.g->grid.h[0], r.g->grid.h[1], r.g->grid.h[2]}};
+    if (!write_vts(path, geo, r.host, r.c->gamma, t)) {
+        std::fprintf(stderr, "sfg_run: cannot write %s\n", path.c_str());
+        return SFG_ERR_ARG;
+    }
+    std::printf("write t=%.17g %s\n", t, path.c_str());
+    ++r.outputs;
+    return 0;
+}
+
+// Clock end / output clipping of Time::Driver (the rule the device clock
+// applies too): stop when the remaining time is round-off, else limit dt to
+// the end and to the next output time.
+bool remaining_limit(const Run& r, double t, double& limit) {
+    const double eps = 2.220446049250313e-16;
+    const double end = r.c->end_time;
+    double sc = std::fmax(std::fabs(t), std::fabs(end));
+    sc = sc < 1.0 ? 1.0 : sc;
+    const double remaining = end - t;
+    if (!(remaining > 64.0 * eps * sc)) return false;
+    limit = remaining;
+    if (r.c->write_interval > 0.0 && r.next_out - t < limit) limit = r.next_out - t;
+    return true;
+}
+
+void bind_ops(OperationTable& ops, const std::string& provider, Run& r) {
+    ops.bind(opid::FlowStepPrepare, provider, [&r](StepContext& ctx) {
+        // ghosts and periodic images are index maps inside the kernels
+        r.next_out = r.c->write_interval > 0.0 ? ctx.t + r.c->write_interval : 0.0;
+        return r.c->write_initial ? write_output(r, ctx.t) : 0;
+    });
+    ops.bind(opid::FlowDtCompute, provider, [&r](StepContext& ctx) {
+        double limit = 0.0;
+        if (!remaining_limit(r, ctx.t, limit)) {
+            ctx.stop = true;
+            return 0;
+        }
+        return sfg_compute_dt(r.s, limit, &ctx.dt);
+    });
+    ops.bind(opid::FlowStepBegin, provider, [](StepContext&) { return 0; });  // stage 0 snapshots q0
+    ops.bind(opid::ExplicitStageExecute, provider,
+             [&r](StepContext& ctx) { return sfg_stage(r.s, ctx.stage, ctx.dt); });
+    ops.bind(opid::FlowStepCommit, provider, [&r](StepContext&) {
+        uint32_t bits = 0;
+        if (int rc = sfg_status_word(r.s, &bits, 0)) return rc;
+        return bits ? int(SFG_ERR_STATE) : 0;
+    });
+    ops.bind(opid::TimeCommit, provider, [&r](StepContext& ctx) {
+        int64_t steps = 0;
+        if (int rc = sfg_time(r.s, &ctx.t, &steps)) return rc;
+        ctx.steps = steps;
+        if (r.c->write_interval > 0.0 && at_or_past(ctx.t, r.next_out)) {
+            r.next_out += r.c->write_interval;
+            return write_output(r, ctx.t);
+        }
+        return 0;
+    });
+}
+
+// The time loop between output times as one sfg_advance (device clock, CUDA
+// graphs of `graph_steps` steps).
+int run_graph(Run& r, int graph_steps, StepContext& ctx) {
+    r.next_out = r.c->write_interval > 0.0 ? ctx.t + r.c->write_interval : 0.0;
+    if (r.c->write_initial)
+        if (int rc = write_output(r, ctx.t)) return rc;
+    for (;;) {
+        double limit = 0.0;
+        if (!remaining_limit(r, ctx.t, limit)) return 0;
+        const double target =
+            r.c->write_interval > 0.0 && r.next_out < r.c->end_time ? r.next_out : r.c->end_time;
+        sfg_stats st{};
+        if (int rc = sfg_advance(r.s, target, 0, 0.0, graph_steps, nullptr, 0, &st)) return rc;
+        if (st.status_bits) return SFG_ERR_STATE;
+        int64_t steps = 0;
+        if (int rc = sfg_time(r.s, &ctx.t, &steps)) return rc;
+        ctx.steps = steps;
+        if (r.c->write_interval > 0.0 && at_or_past(ctx.t, r.next_out)) {
+            r.next_out += r.c->write_interval;
+            if (int rc = write_output(r, ctx.t)) return rc;
+        }
+    }
+}
+
+// Checks of the catalog and plan rules that need no case and no GPU.
+int selftest() {
+    int failed = 0;
+    auto check = [&](bool ok, const char* what) {
+        std::printf("%s %s\n", ok ? "ok" : "FAILED", what);
+        failed += !ok;
+    };
+    int weno5 = -1;
+    sfg_recipe_from_name("weno5Rusanov", &weno5);
+    TermMatch m{"Momentum", "ConservativeResidual", "div", "rhoU", weno5, "weno5Rusanov"};
+    TermCatalog gpu = TermCatalog::gpu();
+    check(gpu.resolve(m).status == BindingStatus::Resolved, "supported recipe resolves to one provider");
+    TermMatch sw = m;
+    sw.recipe = -1;
+    sw.recipe_token = "weno5StegerWarming";
+    const ResolvedTerm r_sw = gpu.resolve(sw);
+    check(r_sw.status == BindingStatus::Unsupported && r_sw.reason.find("no term provider") != std::string::npos,
+          "recipe without a GPU kernel is Unsupported");
+    TermMatch grad = m;
+    grad.operator_name = "grad";
+    check(gpu.resolve(grad).status == BindingStatus::Unsupported, "other operators are not matched");
+    check(gpu.resolve(m, "convection.other").status == BindingStatus::Unsupported, "binding to another id");
+    TermCatalog two = TermCatalog::gpu();
+    two.add({"convection.second", [](const TermMatch& t) { return t.operator_name == "div"; }, "test"});
+    const ResolvedTerm amb = two.resolve(m);
+    check(amb.status == BindingStatus::Invalid &&
+              amb.reason.find("convection.conservativeFlux, convection.second") != std::string::npos,
+          "two matching providers are Invalid (ambiguous, listed in id order)");
+    check(two.resolve(m, "convection.second").status == BindingStatus::Resolved, "a binding selects one of them");
+    bool threw = false;
+    try {
+        two.add({"convection.second", [](const TermMatch&) { return false; }, "test"});
+    } catch (const std::invalid_argument&) {
+        threw = true;
+    }
+    check(threw, "duplicate term provider id is refused");
+    const ProviderCatalog pc = ProviderCatalog::gpu();
+    const Operation op{opid::ExplicitStageExecute, {Capability::ConservativeExplicit}};
+    check(pc.resolve(op, "flow.conservative").status == BindingStatus::Resolved, "runtime provider resolves");
+    check(pc.resolve(op, "flow.pressure").reason.find("not registered") != std::string::npos,
+          "unknown runtime provider");
+    check(pc.resolve({opid::TimeCommit, {Capability::TemporalSynchronization}}, "flow.conservative")
+                  .reason.find("lacks a capability") != std::string::npos,
+          "missing capability");
+    check(pc.resolve(op, "").status == BindingStatus::Unsupported, "no provider selected");
+    const PlanNode plan = conservative_explicit_plan("flow.conservative", 3);
+    OperationTable ops;
+    ops.bind(opid::FlowStepPrepare, "flow.conservative", [](StepContext&) { return 0; });
+    bool unbound = false;
+    try {
+        ops.validate(plan);
+    } catch (const std::runtime_error& e) {
+        unbound = std::string(e.what()).find("flow.dt.compute @ flow.conservative") != std::string::npos;
+    }
+    check(unbound, "a plan with unbound operations is refused before it runs");
+    // a counting run of the plan: 2 steps of 3 stages
+    OperationTable cnt;
+    int stages = 0, dts = 0, commits = 0;
+    const std::string p = "flow.conservative";
+    cnt.bind(opid::FlowStepPrepare, p, [](StepContext&) { return 0; });
+    cnt.bind(opid::FlowDtCompute, p, [&](StepContext& c) {
+        c.stop = ++dts > 2;
+        return 0;
+    });
+    cnt.bind(opid::FlowStepBegin, p, [](StepContext&) { return 0; });
+    cnt.bind(opid::ExplicitStageExecute, p, [&](StepContext& c) { return c.stage == stages++ % 3 ? 0 : 1; });
+    cnt.bind(opid::FlowStepCommit, p, [](StepContext&) { return 0; });
+    cnt.bind(opid::TimeCommit, p, [&](StepContext&) { return ++commits, 0; });
+    StepContext ctx;
+    const int rc = PlanExecutor(cnt).run(plan, ctx);
+    check(rc == 0 && stages == 6 && commits == 2 && dts == 3, "plan runs stages 0..2 per step until dt stops it");
+    threw = false;
+    try {
+        cnt.bind(opid::TimeCommit, p, [](StepContext&) { return 0; });
+    } catch (const std::invalid_argument&) {
+        threw = true;
+    }
+    check(threw, "an operation is bound once");
+    std::printf("%s\n", failed ? "selftest FAILED" : "selftest passed");
+    return failed ? 1 : 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    if (argc == 2 && std::strcmp(argv[1], "--selftest") == 0) return selftest();
+    Options o;
+    for (int i = 1; i < argc; ++i) {
+        const std::string a = argv[i];
+        auto next = [&](void) -> std::string { return i + 1 < argc ? argv[++i] : std::string(); };
+        if (a == "--mode") o.mode = next();
+        else if (a == "--precision") {
+            const std::string p = next();
+            if (p == "fp64") o.precision = SFG_PREC_FP64;
+            else if (p == "fp32flux") o.precision = SFG_PREC_FP32_FLUX;
+            else return usage();
+        } else if (a == "--graph-steps") o.graph_steps = std::atoi(next().c_str());
+        else if (a == "--dump") o.dump = next();
+        else if (a == "--no-write") o.write = false;
+        else if (a == "--describe") o.describe_only = true;
+        else if (!a.empty() && a[0] == '-') return usage();
+        else o.dir = a;
+    }
+    if (o.dir.empty() || (o.mode != "graph" && o.mode != "plan")) return usage();
+    try {
+        const CaseSpec c = load_case(o.dir);
+        const GridSetup g = build_grid(c);
+        int stages = 0;
+        const int tid = time_id(c.time_recipe, stages);
+        // ---- provider selection
+        TermMatch term{"Momentum", "ConservativeResidual", "div", "rhoU", -1, c.convection};
+        int recipe = -1;
+        if (sfg_recipe_from_name(c.convection.c_str(), &recipe) == SFG_OK) term.recipe = recipe;
+        const ResolvedTerm rt = TermCatalog::gpu().resolve(term);
+        if (rt.status != BindingStatus::Resolved)
+            throw Unsupported(std::string(to_string(rt.status)) + ": " + rt.reason);
+        const std::string provider = "flow.conservative";
+        const ProviderCatalog pc = ProviderCatalog::gpu();
+        for (const char* op : {opid::FlowStepPrepare, opid::FlowDtCompute, opid::FlowStepBegin,
+                               opid::ExplicitStageExecute, opid::FlowStepCommit, opid::TimeCommit}) {
+            const ResolvedOperation ro = pc.resolve({op, {Capability::ConservativeExplicit}}, provider);
+            if (ro.status != BindingStatus::Resolved)
+                throw Unsupported(std::string(to_string(ro.status)) + ": " + ro.reason);
+        }
+        const PlanNode plan = conservative_explicit_plan(provider, stages);
+        std::printf("term %s -> %s (owner %s, recipe %s)\nplan:\n%s", "div", rt.id.c_str(), rt.owner.c_str(),
+                    c.convection.c_str(), describe(plan).c_str());
+        std::printf("grid dim=%d nodes=%d,%d,%d h=%.17g,%.17g,%.17g bc=%d%d/%d%d/%d%d\n", g.grid.dim, g.nodes[0],
+                    g.nodes[1], g.nodes[2], g.grid.h[0], g.grid.h[1], g.grid.h[2], g.grid.bc_lo[0], g.grid.bc_hi[0],
+                    g.grid.bc_lo[1], g.grid.bc_hi[1], g.grid.bc_lo[2], g.grid.bc_hi[2]);
+        if (o.describe_only) {
+            OperationTable ops;
+            Run dummy;
+            bind_ops(ops, provider, dummy);
+            ops.validate(plan);
+            std::printf("bindings valid\n");
+            return 0;
+        }
+        // ---- provider instance and bindings
+        sfg_numerics_desc nd{recipe, tid, o.precision, c.gamma, c.cfl, c.max_dt};
+        Run r;
+        r.c = &c;
+        r.g = &g;
+        r.write = o.write;
+        r.host.resize(g.q.size());
+        r.out_dir = c.dir + "/" + c.output_dir;
+        if (o.write) mkdir(r.out_dir.c_str(), 0755);
+        if (sfg_create(&g.grid, &nd, nullptr, &r.s) != SFG_OK) {
+            std::fprintf(stderr, "sfg_run: %s\n", sfg_last_error());
+            return 1;
+        }
+        int rc = sfg_upload(r.s, g.q.data(), SFG_LAYOUT_NODES, c.start_time);
+        StepContext ctx;
+        ctx.t = c.start_time;
+        const auto w0 = std::chrono::steady_clock::now();
+        if (!rc) {
+            if (o.mode == "plan") {
+                OperationTable ops;
+                bind_ops(ops, provider, r);
+                rc = PlanExecutor(ops).run(plan, ctx);
+            } else {
+                rc = run_graph(r, o.graph_steps, ctx);
+            }
+        }
+        const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - w0).count();
+        uint32_t bits = 0;
+        double totals[5] = {0, 0, 0, 0, 0};
+        if (!rc) rc = sfg_status_word(r.s, &bits, 0);
+        if (!rc) rc = sfg_conserved_totals(r.s, totals);
+        if (!rc && !o.dump.empty()) {
+            rc = sfg_download(r.s, r.host.data(), SFG_LAYOUT_NODES);
+            std::ofstream f(o.dump, std::ios::binary);
+            f.write(reinterpret_cast<const char*>(r.host.data()), std::streamsize(r.host.size() * sizeof(double)));
+        }
+        if (rc) std::fprintf(stderr, "sfg_run: status %d: %s\n", rc, sfg_last_error());
+        std::printf("{\"case\": \"%s\", \"mode\": \"%s\", \"term_provider\": \"%s\", \"runtime_provider\": \"%s\", "
+                    "\"recipe\": \"%s\", \"time_recipe\": \"%s\", \"dim\": %d, \"nodes\": [%d, %d, %d], "
+                    "\"steps\": %lld, \"time\": %.17g, \"status\": %d, \"status_bits\": %u, "
+                    "\"totals\": [%.17g, %.17g, %.17g, %.17g, %.17g], \"outputs\": %d, \"wall_s\": %.6f}\n",
+                    json_escape(c.name).c_str(), o.mode.c_str(), rt.id.c_str(), provider.c_str(),
+                    c.convection.c_str(), c.time_recipe.c_str(), g.grid.dim, g.nodes[0], g.nodes[1], g.nodes[2],
+                    (long long)ctx.steps, ctx.t, rc, bits, totals[0], totals[1], totals[2], totals[3], totals[4],
+                    r.outputs, wall);
+        sfg_destroy(r.s);
+        return rc ? 1 : 0;
+    } catch (const Unsupported& e) {
+        std::fprintf(stderr, "sfg_run: unsupported: %s\n", e.what());
+        return 3;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "sfg_run: error: %s\n", e.what());
+        return 1;
+    }
+}

@@ -1,0 +1,193 @@
+"""The host driver `sfg_run` on the GPU: a case directory in the reference's
+format goes through the provider catalogs and the compiled plan to the
+kernels, and the result matches the oracle run of the same case.
+
+Tolerances: 1e-11 relative L-infinity per variable after a whole run (the
+per-step bar of the parity tests is 1e-12; the run accumulates 875 steps);
+plan mode (one C-ABI call per operation) and graph mode (sfg_advance) take
+the same dt sequence, so their states agree to 1e-14.  The frozen-end golden
+case is held to the bars its oracle meets (tests/test_oracle.py): integrals
+2e-10, ranges 2e-7.
+"""
+import json
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import pyoracle as po
+from case_dirs import write_case
+from conftest import rel_linf
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+RUNNER = os.path.join(ROOT, "sonicsolver_b200", "sfg_run")
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def run_case(d, *args, dump=True):
+    out = os.path.join(d, "final.bin")
+    cmd = [RUNNER, d, *args] + (["--dump", out] if dump else [])
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    summary = json.loads(r.stdout.strip().splitlines()[-1])
+    q = np.fromfile(out, dtype=np.float64) if dump else None
+    return summary, q, r.stdout
+
+
+def sod_oracle(cells=1000, t_end=0.2, cfl=0.5, write_interval=0.05):
+    n = cells + 1
+    h = 1.0 / cells
+    spec = po.GridSpec(dim=1, n=(n, 1, 1), ng=3, h=(h, 0.1, 0.1), bc_lo=(0, 0, 0), bc_hi=(0, 0, 0))
+    Q = spec.empty()
+    I = spec.interior(Q)
+    i = np.arange(n)
+    I[0, 0, :, 0] = np.where(i < n // 2, 1.0, 0.125)
+    I[0, 0, :, 4] = np.where(i < n // 2, 1.0, 0.1) / 0.4
+    po.fill_ghosts(spec, Q)
+    dts, tf = po.advance(spec, po.WENO5, po.RUSANOV, po.SSPRK3, Q, t_end, cfl, write_interval=write_interval)
+    return np.ascontiguousarray(spec.interior(Q)).reshape(-1, 5), dts, tf
+
+
+@pytest.fixture(scope="module")
+def sod_dir(tmp_path_factory):
+    return write_case(str(tmp_path_factory.mktemp("cases")), "sod_c1", cells=(1000, 1, 1), box_hi=(1.0, 0.1, 0.1))
+
+
+def test_sod_c1_case_directory_matches_oracle(sod_dir):
+    s, q, out = run_case(sod_dir)
+    want, dts, tf = sod_oracle()
+    assert s["term_provider"] == "convection.conservativeFlux" and s["runtime_provider"] == "flow.conservative"
+    assert s["steps"] == len(dts) and abs(s["time"] - tf) <= 1e-14 and s["status"] == 0
+    assert rel_linf(q, want).max() <= 1e-11
+    assert s["outputs"] == 4 and len(re.findall(r"^write t=", out, re.M)) == 4
+
+
+def test_plan_mode_equals_graph_mode(sod_dir):
+    g, qg, _ = run_case(sod_dir, "--mode", "graph", "--no-write")
+    p, qp, _ = run_case(sod_dir, "--mode", "plan", "--no-write")
+    assert g["steps"] == p["steps"] and g["time"] == p["time"]
+    assert rel_linf(qp, qg).max() <= 1e-14
+
+
+def test_vts_output_carries_the_state(sod_dir):
+    s, q, _ = run_case(sod_dir)
+    path = os.path.join(sod_dir, "result", "sod_c1_0003.vts")
+    text = open(path).read()
+    assert 'WholeExtent="0 1000 0 0 0 0"' in text
+    m = re.search(r'Name="rho" NumberOfComponents="1" format="ascii">\n(.*?)</DataArray>', text, re.S)
+    rho = np.array(m.group(1).split(), dtype=np.float64)
+    np.testing.assert_array_equal(rho, q.reshape(-1, 5)[:, 0])   # 17 digits round-trip exactly
+    t = float(re.search(r'Name="TIME"[^>]*>([^<]*)<', text).group(1))
+    assert abs(t - 0.2) <= 1e-14
+
+
+# ------------------------------------------------- frozen end (no condition)
+
+def _weighted_integrals(q, nx, ny, gamma):
+    """Trapezoid node integrals of the reference's output check (2 z-nodes of
+    weight 0.5 at dz = 0.1), as tests/test_oracle.py computes them."""
+    I = q.reshape(ny, nx, 5)
+    rho = I[..., 0]
+    u, v, w = I[..., 1] / rho, I[..., 2] / rho, I[..., 3] / rho
+    p = (gamma - 1.0) * (I[..., 4] - 0.5 * rho * (u * u + v * v + w * w))
+    W = np.ones(rho.shape)
+    W[:, 0] *= 0.5
+    W[:, -1] *= 0.5
+    W[0, :] *= 0.5
+    W[-1, :] *= 0.5
+    W *= 0.5 * 0.1 * 2
+    sp = np.sqrt(u * u + v * v + w * w)
+    return {"rho": (rho.min(), rho.max()), "p": (p.min(), p.max()), "speed": (sp.min(), sp.max()),
+            "mass": (W * rho).sum(), "momentum": [(W * I[..., k]).sum() for k in (1, 2, 3)],
+            "energy": (W * I[..., 4]).sum()}
+
+
+def test_reference_sod_golden_case_through_the_plan(tmp_path):
+    """The reference's frozen-ghost WENO7 + Rusanov + forwardEuler Sod case
+    (100 x 20 cells, no Left condition), written as a case directory from the
+    committed fixture and run by sfg_run: 454 steps, t = 0.2, the baseline's
+    integrals and ranges, and the oracle's final state."""
+    with open(os.path.join(HERE, "golden", "sod_weno7_t0p2.json")) as f:
+        fx = json.load(f)
+    c, base = fx["case"], fx["baseline"]
+    L = c["left"], c["right"]
+    d = write_case(str(tmp_path), "sod_weno7", cells=tuple(c["cells"]), box_hi=tuple(c["length"]),
+                   n_ghost=c["n_ghost"], convection=c["recipe"], time=c["time"], end_time=c["t_end"], cfl=c["cfl"],
+                   write_interval=c["write_interval"], gamma=c["gamma"],
+                   left=(L[0]["rho"], L[0]["u"], L[0]["p"]), right=(L[1]["rho"], L[1]["u"], L[1]["p"]),
+                   boundaries={"Right": "zeroGradient", "sideWalls": "zeroGradient", "frontBack": "empty"})
+    s, q, out = run_case(d, "--no-write")
+    nx, ny, _ = c["nodes"]
+    assert "bc=20/00/00" in out and s["nodes"] == [nx, ny, 1]
+    assert s["steps"] == base["steps"] == 454 and abs(s["time"] - base["final_time"]) <= 5e-12
+    got = _weighted_integrals(q, nx, ny, c["gamma"])
+    for k in ("rho", "p", "speed"):
+        for a, b in zip(got[k], base["ranges"][k]):
+            assert abs(a - b) <= 2e-7 * abs(b), (k, a, b)
+    for k in ("mass", "energy"):
+        assert abs(got[k] - base["integrals"][k]) <= 2e-10 * base["integrals"][k], k
+    mx = base["integrals"]["momentum"][0]
+    assert abs(got["momentum"][0] - mx) <= 2e-10 * mx
+    assert abs(got["momentum"][1]) < 1e-7 and got["momentum"][2] == 0.0
+    from test_oracle import _sod_run
+    _, spec, Q, dts, tf = _sod_run()
+    want = np.ascontiguousarray(spec.interior(Q)).reshape(-1, 5)
+    assert len(dts) == s["steps"]
+    assert rel_linf(q, want).max() <= 1e-9
+
+
+def _frozen_pair(recipe="weno5Rusanov", n=(40, 12, 1), h=(0.02, 0.03, 1.0), ghost_state=None, seed=4):
+    from helpers import FLUX_OF, SCHEME_OF, smooth_state, split_recipe
+    from sonicsolver_b200 import capi
+    scheme, flux = split_recipe(recipe)
+    ng = 4 if scheme == "weno7" else 3
+    lo, hi = (po.BC_FROZEN, po.BC_TRANSMISSIVE, 0), (po.BC_TRANSMISSIVE, po.BC_TRANSMISSIVE, 0)
+    spec = po.GridSpec(dim=2, n=n, ng=ng, h=h, bc_lo=lo, bc_hi=hi)
+    q = smooth_state(2, n, seed=seed, shock=True)
+    Q = spec.empty()                   # oracle Field: (1, ny + 2 ng, nx + 2 ng, 5)
+    spec.interior(Q)[...] = q.reshape(spec.interior(Q).shape)
+    Q[:, :, :ng] = Q[:, :, ng:ng + 1] if ghost_state is None else ghost_state   # frozen x-low ghosts
+    po.fill_ghosts(spec, Q)
+    s = capi.Solver(2, n, h, (capi.BC_FROZEN, capi.BC_TRANSMISSIVE, 0), (capi.BC_TRANSMISSIVE,) * 2 + (0,),
+                    recipe=recipe, time_recipe="SSPRK3")
+    if ghost_state is None:
+        s.upload(np.ascontiguousarray(q))
+    else:                              # C-ABI Field layout: ng ghosts on every axis, z included
+        F = np.zeros((1 + 2 * ng,) + Q.shape[1:])
+        F[ng] = Q[0]
+        s.upload(np.ascontiguousarray(F), layout=capi.LAYOUT_FIELD)
+    return spec, Q, s, po.Stepper(spec, SCHEME_OF[scheme], FLUX_OF[flux], po.SSPRK3), q.shape
+
+
+@pytest.mark.parametrize("recipe", ["weno5Rusanov", "teno5Roe", "weno7Rusanov"])
+def test_frozen_end_steps_match_oracle(recipe):
+    spec, Q, s, st, shape = _frozen_pair(recipe)
+    for _ in range(5):
+        dt = po.dt(spec, Q, 0.5)
+        assert abs(s.compute_dt() - dt) <= 1e-14 * dt
+        st.step(Q, dt)
+        s.step(dt)
+    got = s.download().reshape(-1, 5)
+    assert got.shape[0] == 40 * 12     # the device's extra node is not part of the caller's grid
+    assert rel_linf(got, np.ascontiguousarray(spec.interior(Q)).reshape(-1, 5)).max() <= 1e-12
+
+
+def test_frozen_end_field_layout_ghosts_are_used():
+    """Field-layout upload: the frozen ghosts keep the values the caller
+    gave (here a different state from the boundary node), as the reference
+    does; download writes them back unchanged."""
+    from sonicsolver_b200 import capi
+    ghost = np.array([1.3, 0.2, 0.0, 0.0, 2.9])
+    spec, Q, s, st, shape = _frozen_pair(ghost_state=ghost)
+    dt = po.dt(spec, Q, 0.5)
+    assert abs(s.compute_dt() - dt) <= 1e-14 * dt
+    st.step(Q, dt)
+    s.step(dt)
+    ng = spec.ng
+    got = s.download(layout=capi.LAYOUT_FIELD).reshape((1 + 2 * ng,) + Q.shape[1:])[ng]
+    assert rel_linf(got[ng:-ng, ng:-ng], spec.interior(Q)[0]).max() <= 1e-12
+    np.testing.assert_array_equal(got[ng:-ng, :ng], np.broadcast_to(ghost, got[ng:-ng, :ng].shape))

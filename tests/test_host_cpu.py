@@ -1,0 +1,112 @@
+"""The C++17 host side (case reader, provider catalogs, plan, driver) on the
+CPU: `sfg_run --selftest` checks the catalog and plan rules, `--describe`
+reads a case directory, resolves its providers and validates the plan
+bindings without touching a GPU."""
+import os
+import subprocess
+
+import pytest
+
+from case_dirs import write_case
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+RUNNER = os.path.join(ROOT, "sonicsolver_b200", "sfg_run")
+REFERENCE_TESTS = "/root/reference/test"   # the reference's own case directories, read in place when present
+
+
+@pytest.fixture(scope="module")
+def runner():
+    from sonicsolver_b200 import build
+    build.build_host()
+    return RUNNER
+
+
+def run(runner, *args):
+    return subprocess.run([runner, *args], capture_output=True, text=True, timeout=60)
+
+
+def test_selftest(runner):
+    r = run(runner, "--selftest")
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "selftest passed" in r.stdout and "FAILED" not in r.stdout
+
+
+@pytest.mark.parametrize("form", ["terms", "scheme"])
+def test_describe_sod_case(runner, tmp_path, form):
+    d = write_case(str(tmp_path), "sod", cells=(1000, 1, 1), box_hi=(1.0, 0.1, 0.1), numerics_form=form)
+    r = run(runner, d, "--describe")
+    assert r.returncode == 0, r.stderr
+    assert "convection.conservativeFlux" in r.stdout and "recipe weno5Rusanov" in r.stdout
+    assert "grid dim=1 nodes=1001,1,1 h=0.001," in r.stdout and "bc=00/00/00" in r.stdout
+    for op in ("flow.step.prepare", "flow.dt.compute", "flow.step.begin", "explicit.stage.execute",
+               "flow.step.commit", "time.commit"):
+        assert f"[{op} @ flow.conservative]" in r.stdout
+    assert "stage-loop Explicit.stages x3" in r.stdout and "bindings valid" in r.stdout
+
+
+def test_describe_2d_frozen_and_periodic(runner, tmp_path):
+    d = write_case(str(tmp_path), "frozen", cells=(100, 20, 1), box_hi=(100.0, 20.0, 0.1), n_ghost=4,
+                   convection="weno7Rusanov", time="forwardEuler",
+                   boundaries={"Right": "zeroGradient", "sideWalls": "zeroGradient", "frontBack": "empty"})
+    r = run(runner, d, "--describe")
+    assert r.returncode == 0, r.stderr
+    assert "grid dim=2 nodes=101,21,1 h=1,1," in r.stdout and "bc=20/00/00" in r.stdout   # Left: frozen
+    d2 = write_case(str(tmp_path), "periodic", cells=(64, 32, 1), box_hi=(1.0, 0.5, 0.1),
+                    boundaries={"Left": "periodic", "Right": "periodic", "sideWalls": "periodic",
+                                "frontBack": "empty"})
+    r2 = run(runner, d2, "--describe")
+    assert r2.returncode == 0 and "nodes=64,32,1" in r2.stdout and "bc=11/11/00" in r2.stdout
+
+
+@pytest.mark.parametrize("convection,needle", [("weno5StegerWarming", "no term provider"),
+                                               ("upwind1Rusanov", "no term provider")])
+def test_unsupported_recipe(runner, tmp_path, convection, needle):
+    d = write_case(str(tmp_path), "c", cells=(50, 1, 1), box_hi=(1.0, 0.1, 0.1), convection=convection)
+    r = run(runner, d, "--describe")
+    assert r.returncode == 3 and needle in r.stderr
+
+
+def test_unsupported_condition_and_time(runner, tmp_path):
+    d = write_case(str(tmp_path), "a", cells=(50, 1, 1), box_hi=(1.0, 0.1, 0.1),
+                   boundaries={"Left": "fixedValue", "Right": "zeroGradient", "sideWalls": "empty",
+                               "frontBack": "empty"})
+    r = run(runner, d, "--describe")
+    assert r.returncode == 3 and "fixedValue" in r.stderr
+    d2 = write_case(str(tmp_path), "b", cells=(50, 1, 1), box_hi=(1.0, 0.1, 0.1), time="backwardEuler")
+    r2 = run(runner, d2, "--describe")
+    assert r2.returncode == 3 and "time recipe" in r2.stderr
+
+
+def test_parse_error_names_file_and_line(runner, tmp_path):
+    d = write_case(str(tmp_path), "bad", cells=(50, 1, 1), box_hi=(1.0, 0.1, 0.1))
+    with open(os.path.join(d, "solvers", "runtime.yaml"), "a") as f:
+        f.write("this line has no colon\n")
+    r = run(runner, d, "--describe")
+    assert r.returncode == 1 and "runtime.yaml:" in r.stderr
+
+
+@pytest.mark.skipif(not os.path.isdir(REFERENCE_TESTS), reason="reference case directories not present")
+def test_reference_case_directories(runner):
+    """Every case directory of the reference's test tree is read without a
+    parse error.  The Sod cases (no Left condition: frozen ghosts) resolve
+    and plan when their recipe has a GPU kernel (the WENO7 + Rusanov golden
+    case does; Steger-Warming has none yet); every other case is reported as
+    not supported by this provider, with its reason."""
+    dirs = sorted(os.path.dirname(os.path.join(dp, f)) for dp, _, fs in os.walk(REFERENCE_TESTS)
+                  for f in fs if f == "case.yaml")
+    assert len(dirs) > 10
+    resolved = []
+    for d in dirs:
+        r = run(runner, d, "--describe")
+        rel = os.path.relpath(d, REFERENCE_TESTS)
+        assert r.returncode in (0, 3), (rel, r.returncode, r.stderr)
+        if r.returncode == 0:
+            assert "bindings valid" in r.stdout
+            resolved.append(rel)
+            if rel.startswith("Sod" + os.sep):
+                assert "bc=20/00/00" in r.stdout
+        else:
+            assert "unsupported:" in r.stderr
+            if rel.startswith("Sod" + os.sep):
+                assert "no term provider" in r.stderr and "StegerWarming" in r.stderr
+    assert os.path.join("Sod", "sodCase_weno7_t0p2") in resolved
