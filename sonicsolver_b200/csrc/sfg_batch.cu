@@ -111,14 +111,18 @@ __global__ void __launch_bounds__(TILE_THREADS, F32 ? 3 : 2)
         BatchInst& b = inst[w.inst];
         if (!b.live || !b.clock.active) continue;  // uniform across the block
         StageView sv = batch_stage_view(b, stage, time_id);
+        const bool last = stage == (time_id == T_EULER ? 0 : (time_id == T_SSPRK3 ? 2 : 3));
+        if (last) sv.mode |= MODE_CFL;  // the step's result: reduce its CFL minimum here
         unsigned flags = 0, cut = 0, cores = 0;
+        double sr = 0.0;
         if (w.dim == 2) {
-            if constexpr (F32) tile2d_f32_body<SCHEME, FLUX, TX, TY>(b.g, sv, w.x0, w.y0, smem, flags, cut, cores);
-            else tile2d_body<SCHEME, FLUX, TX, TY>(b.g, sv, w.x0, w.y0, smem, flags, cut, cores);
+            if constexpr (F32) tile2d_f32_body<SCHEME, FLUX, TX, TY>(b.g, sv, w.x0, w.y0, smem, flags, cut, cores, sr);
+            else tile2d_body<SCHEME, FLUX, TX, TY>(b.g, sv, w.x0, w.y0, smem, flags, cut, cores, sr);
         } else {
-            tile1d_body<SCHEME, FLUX, Tt>(b.g, sv, w.x0, smem, flags, cut, cores);
+            tile1d_body<SCHEME, FLUX, Tt>(b.g, sv, w.x0, smem, flags, cut, cores, sr);
         }
         if (flags) atomicOr(&b.flags, flags);
+        if (last) flush_cfl_block(b.g, &b.clock, sr);
         __syncthreads();  // shared arrays are reused by the next tile
     }
 }
@@ -127,17 +131,16 @@ __global__ void __launch_bounds__(TILE_THREADS, F32 ? 3 : 2)
 template <int TX, int TY>
 __global__ void __launch_bounds__(TILE_THREADS) batch_dt_kernel(BatchInst* inst, const WorkItem* items, BatchCtl* ctl) {
     __shared__ int slot;
-    __shared__ double wmin[TILE_THREADS / 32];
     const int n_items = ctl->n_items;
     for (;;) {
         const int it = steal(&ctl->counters[0], &slot);
         if (it >= n_items) break;
         const WorkItem w = items[it];
         BatchInst& b = inst[w.inst];
-        if (!b.live || b.done) continue;
+        if (!b.live || b.done || b.clock.dt_ready) continue;  // ready: reduced by the last stage
         const GridView& g = b.g;
         const int cnt = w.dim == 2 ? TX * TY : TILE1D;
-        double best = 1.7976931348623157e308;
+        double best = 0.0;
         unsigned fl = 0;
         for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
             const int i = w.dim == 2 ? w.x0 + t % TX : w.x0 + t;
@@ -145,30 +148,12 @@ __global__ void __launch_bounds__(TILE_THREADS) batch_dt_kernel(BatchInst* inst,
             if (i >= g.hi[0] || (w.dim == 2 && j >= g.hi[1])) continue;
             const long long node = (long long)j * g.n[0] + i;
             const double* q = b.qn;
-            const double rho = q[node];
-            const double u = q[g.vs + node] / rho, v = q[2 * g.vs + node] / rho, ww = q[3 * g.vs + node] / rho;
-            const double kin = 0.5 * rho * (u * u + v * v + ww * ww);
-            const double e = (q[4 * g.vs + node] - kin) / rho;
-            const double p = (g.gamma - 1.0) * rho * e;
-            const double c = sqrt(g.gamma * p / rho);
-            double sr = 0.0;
-            sr += fabs(u * g.metric[0]) + c * g.metric[0];
-            if (g.dim > 1) sr += fabs(v * g.metric[1]) + c * g.metric[1];
+            const double qq[5] = {q[node], q[g.vs + node], q[2 * g.vs + node], q[3 * g.vs + node], q[4 * g.vs + node]};
+            const double sr = cfl_rate(g, qq);
             if (!(sr > 0.0) || !isfinite(sr)) fl |= FLAG_NONFINITE;
-            const double cand = g.cfl / sr;
-            best = cand < best ? cand : best;
+            best = fmax(best, sr);
         }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const double other = __shfl_xor_sync(0xffffffffu, best, o);
-            best = other < best ? other : best;
-        }
-        if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = best;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            for (int k = 1; k < TILE_THREADS / 32; ++k) best = wmin[k] < best ? wmin[k] : best;
-            atomicMin(&b.clock.dt_bits, (unsigned long long)__double_as_longlong(best));
-        }
+        flush_cfl_block(g, &b.clock, best);
         if (fl) atomicOr(&b.flags, fl);
         __syncthreads();
     }
@@ -198,6 +183,8 @@ __global__ void batch_finalize_kernel(BatchInst* inst, BatchCtl* ctl) {
     if (limit < dt) dt = limit;
     c->dt = dt;
     c->active = 1;
+    c->dt_bits = 0x7FEFFFFFFFFFFFFFull;  // consumed: re-armed for the last stage's reduction
+    c->dt_ready = 0;
     atomicAdd(&ctl->active, 1);
 }
 
@@ -237,7 +224,7 @@ __global__ void batch_commit_kernel(BatchInst* inst, BatchCtl* ctl) {
                 sc = sc < 1.0 ? 1.0 : sc;
                 if (c->write_interval > 0.0 && c->t >= c->next_out - 1.0e-11 * sc) c->next_out += c->write_interval;
             }
-            c->dt_bits = 0x7FEFFFFFFFFFFFFFull;
+            c->dt_ready = c->active ? 1 : 0;  // the last stage reduced the new state's CFL minimum
         }
     }
     if (blockIdx.x == 0 && threadIdx.x < 8) ctl->counters[threadIdx.x] = 0;

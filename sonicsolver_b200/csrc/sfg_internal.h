@@ -41,7 +41,8 @@ struct Clock {
     long long max_steps;
     long long log_base;       // step index of dt_log[0]
     int active;               // 1 while the current step runs
-    int pad;
+    int dt_ready;             // 1: dt_bits already holds the CFL minimum of the current
+                              // state (reduced by the previous step's last stage)
 };
 
 // Geometry of one grid as the kernels see it (uniform Cartesian metrics).
@@ -80,5 +81,7 @@ struct StageView {
 constexpr int MODE_READ_R = 1;     // add the residual accumulated by earlier axes
 constexpr int MODE_FINAL = 2;      // last axis: finish the node
 constexpr int MODE_RESIDUAL = 4;   // final output is R = Jac * div (no stage update)
+constexpr int MODE_CFL = 8;        // last stage of a step: also reduce the CFL minimum of
+                                   // the new state into clock->dt_bits (the next step's dt)
 
 }  // namespace sfg

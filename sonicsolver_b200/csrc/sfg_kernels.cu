@@ -46,6 +46,7 @@ __global__ void __launch_bounds__(128) sweep_x(GridView g, StageView sv) {
     const long long rowbase = ((long long)k * g.n[1] + j) * g.n[0];
     const long long vs = g.vs;
     unsigned flags = 0, cut = 0;
+    double sr = 0.0;
     double st[NST][5];
     double F[5] = {0, 0, 0, 0, 0};
     if (lane <= nodes) {
@@ -87,13 +88,14 @@ __global__ void __launch_bounds__(128) sweep_x(GridView g, StageView sv) {
             double qn[5];
 #pragma unroll
             for (int v = 0; v < 5; ++v) qn[v] = st[NST / 2][v];
-            finish_node(g, sv, sv.clock->dt, node, qn, div, flags);
+            finish_node(g, sv, sv.clock->dt, node, qn, div, flags, sr);
         } else {
 #pragma unroll
             for (int v = 0; v < 5; ++v) sv.r[v * vs + node] = div[v];
         }
     }
     flush_status(sv, flags, SCHEME == TENO5 ? (lane <= nodes ? 10u : 0u) : 0u, cut);
+    if (sv.mode & MODE_CFL) flush_cfl_warp(g, sv.clock, sr);
 }
 
 // ---------------------------------------------------------------------------
@@ -109,7 +111,8 @@ constexpr int SEGLEN = 16;
 // exactly.  The FP64 node value for the stage update is re-read (L1 / L2).
 template <int AX, int SCHEME, int FLUX>
 __device__ __forceinline__ void sweep_yz_f32_segment(const GridView& g, const StageView& sv, int i, int o, int s0,
-                                                     unsigned& flags, unsigned& cut, unsigned& cores) {
+                                                     unsigned& flags, unsigned& cut, unsigned& cores,
+                                                     double& sr_max) {
     constexpr int NST = SchemeInfo<SCHEME>::NST;
     constexpr int OTHER = AX == 1 ? 2 : 1;
     const int s1 = min(s0 + SEGLEN, g.hi[AX]);
@@ -153,7 +156,7 @@ __device__ __forceinline__ void sweep_yz_f32_segment(const GridView& g, const St
                 double qn[5];
 #pragma unroll
                 for (int v = 0; v < 5; ++v) qn[v] = sv.qs[v * vs + node];
-                finish_node(g, sv, dt, node, qn, div, flags);
+                finish_node(g, sv, dt, node, qn, div, flags, sr_max);
             } else {
 #pragma unroll
                 for (int v = 0; v < 5; ++v) sv.r[v * vs + node] = div[v];
@@ -183,8 +186,9 @@ __global__ void __launch_bounds__(128) sweep_yz(GridView g, StageView sv) {
     const int s0 = g.lo[AX] + (blockIdx.y * blockDim.y + threadIdx.y) * SEGLEN;
     const bool live = i < g.hi[0] && s0 < g.hi[AX];
     unsigned flags = 0, cut = 0, cores = 0;
+    double sr = 0.0;
     if constexpr (sizeof(T) == sizeof(float)) {
-        if (live) sweep_yz_f32_segment<AX, SCHEME, FLUX>(g, sv, i, o, s0, flags, cut, cores);
+        if (live) sweep_yz_f32_segment<AX, SCHEME, FLUX>(g, sv, i, o, s0, flags, cut, cores, sr);
     } else if (live) {
         const int s1 = min(s0 + SEGLEN, g.hi[AX]);
         const long long vs = g.vs;
@@ -222,7 +226,7 @@ __global__ void __launch_bounds__(128) sweep_yz(GridView g, StageView sv) {
                     double qn[5];
 #pragma unroll
                     for (int v = 0; v < 5; ++v) qn[v] = st[NST / 2 - 1][v];
-                    finish_node(g, sv, dt, node, qn, div, flags);
+                    finish_node(g, sv, dt, node, qn, div, flags, sr);
                 } else {
 #pragma unroll
                     for (int v = 0; v < 5; ++v) sv.r[v * vs + node] = div[v];
@@ -242,6 +246,7 @@ __global__ void __launch_bounds__(128) sweep_yz(GridView g, StageView sv) {
         }
     }
     flush_status(sv, flags, cores, cut);
+    if (sv.mode & MODE_CFL) flush_cfl_warp(g, sv.clock, sr);
 }
 
 // ---------------------------------------------------------------------------
@@ -249,10 +254,11 @@ __global__ void __launch_bounds__(128) sweep_yz(GridView g, StageView sv) {
 // grid minimum replacing Runtime::globalMinimum's MPI_Allreduce(MIN).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) dt_kernel(GridView g, const double* __restrict__ q, Clock* clock,
-                                                 unsigned* flags, int require_active) {
+                                                 unsigned* flags, int skip_if_ready) {
+    if (skip_if_ready && clock->dt_ready) return;  // the previous step's last stage reduced it
     const long long cx = g.hi[0] - g.lo[0], cy = g.hi[1] - g.lo[1], cz = g.hi[2] - g.lo[2];
     const long long total = cx * cy * cz;
-    double best = 1.7976931348623157e308;
+    double best = 0.0;  // largest spectral-radius sum; dt = CFL / best
     unsigned fl = 0;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
@@ -260,32 +266,12 @@ __global__ void __launch_bounds__(256) dt_kernel(GridView g, const double* __res
         const int j = g.lo[1] + (int)((t / cx) % cy);
         const int k = g.lo[2] + (int)(t / (cx * cy));
         const long long node = ((long long)k * g.n[1] + j) * g.n[0] + i;
-        const double rho = q[node];
-        const double u = q[g.vs + node] / rho, v = q[2 * g.vs + node] / rho, w = q[3 * g.vs + node] / rho;
-        const double kin = 0.5 * rho * (u * u + v * v + w * w);
-        const double e = (q[4 * g.vs + node] - kin) / rho;
-        const double p = (g.gamma - 1.0) * rho * e;
-        const double c = sqrt(g.gamma * p / rho);
-        double sr = 0.0;
-        sr += fabs(u * g.metric[0]) + c * g.metric[0];
-        if (g.dim > 1) sr += fabs(v * g.metric[1]) + c * g.metric[1];
-        if (g.dim > 2) sr += fabs(w * g.metric[2]) + c * g.metric[2];
+        const double qq[5] = {q[node], q[g.vs + node], q[2 * g.vs + node], q[3 * g.vs + node], q[4 * g.vs + node]};
+        const double sr = cfl_rate(g, qq);
         if (!(sr > 0.0) || !isfinite(sr)) fl |= FLAG_NONFINITE;
-        const double cand = g.cfl / sr;
-        best = cand < best ? cand : best;
+        best = fmax(best, sr);
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        const double other = __shfl_xor_sync(0xffffffffu, best, o);
-        best = other < best ? other : best;
-    }
-    __shared__ double wmin[8];
-    if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = best;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) best = wmin[w] < best ? wmin[w] : best;
-        atomic_min_positive(&clock->dt_bits, best);
-    }
+    flush_cfl_block(g, clock, best);
     if (fl) atomicOr(flags, fl);
 }
 
@@ -309,10 +295,13 @@ __global__ void finalize_dt_kernel(Clock* c) {
     if (limit < dt) dt = limit;
     c->dt = dt;
     c->active = 1;
+    c->dt_bits = 0x7FEFFFFFFFFFFFFFull;  // consumed: re-armed for the next minimum
+    c->dt_ready = 0;
 }
 
-// TimeCommit: t += dt, ++step, output-time bookkeeping; re-arms the CFL min.
-__global__ void commit_kernel(Clock* c, double* dt_log, long long dt_cap) {
+// TimeCommit: t += dt, ++step, output-time bookkeeping.  `cfl_next`: the
+// step's last stage reduced the CFL minimum of the new state into dt_bits.
+__global__ void commit_kernel(Clock* c, double* dt_log, long long dt_cap, int cfl_next) {
     if (c->active) {
         if (dt_log && c->steps - c->log_base < dt_cap && c->steps >= c->log_base) dt_log[c->steps - c->log_base] = c->dt;
         c->t += c->dt;
@@ -321,7 +310,7 @@ __global__ void commit_kernel(Clock* c, double* dt_log, long long dt_cap) {
         sc = sc < 1.0 ? 1.0 : sc;
         if (c->write_interval > 0.0 && c->t >= c->next_out - 1.0e-11 * sc) c->next_out += c->write_interval;
     }
-    c->dt_bits = 0x7FEFFFFFFFFFFFFFull;  // largest finite double
+    c->dt_ready = c->active && cfl_next ? 1 : 0;
     c->limit = __longlong_as_double(0x7FF0000000000000ll);
 }
 
@@ -462,10 +451,10 @@ static int grid_for(long long work, int block) {
     return (int)(b < 1 ? 1 : b);
 }
 
-cudaError_t launch_dt(const GridView& g, const double* q, Clock* clock, unsigned* flags, int require_active,
+cudaError_t launch_dt(const GridView& g, const double* q, Clock* clock, unsigned* flags, int skip_if_ready,
                       cudaStream_t st) {
     const long long total = (long long)(g.hi[0] - g.lo[0]) * (g.hi[1] - g.lo[1]) * (g.hi[2] - g.lo[2]);
-    dt_kernel<<<grid_for(total, 256), 256, 0, st>>>(g, q, clock, flags, require_active);
+    dt_kernel<<<grid_for(total, 256), 256, 0, st>>>(g, q, clock, flags, skip_if_ready);
     return cudaGetLastError();
 }
 
@@ -474,8 +463,8 @@ cudaError_t launch_finalize_dt(Clock* c, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_commit(Clock* c, double* dt_log, long long dt_cap, cudaStream_t st) {
-    commit_kernel<<<1, 1, 0, st>>>(c, dt_log, dt_cap);
+cudaError_t launch_commit(Clock* c, double* dt_log, long long dt_cap, int cfl_next, cudaStream_t st) {
+    commit_kernel<<<1, 1, 0, st>>>(c, dt_log, dt_cap, cfl_next);
     return cudaGetLastError();
 }
 

@@ -22,10 +22,10 @@
 namespace sfg {
 cudaError_t launch_sweep(int scheme, int flux, int prec64, int axis, const GridView& g, const StageView& sv,
                          cudaStream_t st);
-cudaError_t launch_dt(const GridView& g, const double* q, Clock* clock, unsigned* flags, int require_active,
+cudaError_t launch_dt(const GridView& g, const double* q, Clock* clock, unsigned* flags, int skip_if_ready,
                       cudaStream_t st);
 cudaError_t launch_finalize_dt(Clock* c, cudaStream_t st);
-cudaError_t launch_commit(Clock* c, double* dt_log, long long dt_cap, cudaStream_t st);
+cudaError_t launch_commit(Clock* c, double* dt_log, long long dt_cap, int cfl_next, cudaStream_t st);
 cudaError_t launch_set_dt(Clock* c, double dt, cudaStream_t st);
 cudaError_t launch_reset_min(Clock* c, cudaStream_t st);
 cudaError_t launch_stage_from_residual(const GridView& g, const StageView& sv, cudaStream_t st);
@@ -249,23 +249,26 @@ StageView stage_view(sfg_solver_s* s, int stage, bool residual_only, bool requir
 }
 
 // All axis sweeps of one stage (or of the residual alone).
-int enqueue_stage(sfg_solver_s* s, int stage, bool residual_only, bool require_active) {
+// `cfl`: the launch that finishes the nodes also reduces the CFL minimum of
+// the new state (the last stage of a step).
+int enqueue_stage(sfg_solver_s* s, int stage, bool residual_only, bool require_active, bool cfl = false) {
     StageView sv = stage_view(s, stage, residual_only, require_active);
     const int dim = s->grid.dim;
+    const int cfl_bit = cfl && !residual_only ? MODE_CFL : 0;
     if (dim == 2 && s->variant > 0) {
-        sv.mode = MODE_FINAL | (residual_only ? MODE_RESIDUAL : 0);
+        sv.mode = MODE_FINAL | (residual_only ? MODE_RESIDUAL : 0) | cfl_bit;
         CUDA_TRY(launch_tile2d(s->variant, s->recipe->scheme, s->recipe->flux, s->num.precision == SFG_PREC_FP64,
                                s->gv, sv, s->stream));
         return SFG_OK;
     }
     if (dim == 1 && s->variant > 0) {
-        sv.mode = MODE_FINAL | (residual_only ? MODE_RESIDUAL : 0);
+        sv.mode = MODE_FINAL | (residual_only ? MODE_RESIDUAL : 0) | cfl_bit;
         CUDA_TRY(launch_tile1d(s->recipe->scheme, s->recipe->flux, s->num.precision == SFG_PREC_FP64, s->gv, sv,
                                s->stream));
         return SFG_OK;
     }
     for (int axis = 0; axis < dim; ++axis) {
-        sv.mode = (axis > 0 ? MODE_READ_R : 0) | (axis == dim - 1 ? MODE_FINAL : 0) |
+        sv.mode = (axis > 0 ? MODE_READ_R : 0) | (axis == dim - 1 ? MODE_FINAL | cfl_bit : 0) |
                   (residual_only && axis == dim - 1 ? MODE_RESIDUAL : 0);
         CUDA_TRY(launch_sweep(s->recipe->scheme, s->recipe->flux, s->num.precision == SFG_PREC_FP64, axis, s->gv,
                               sv, s->stream));
@@ -280,12 +283,17 @@ int enqueue_post_step(sfg_solver_s* s) {
     return SFG_OK;
 }
 
-// One full step with the CFL dt computed and clipped on device.
+// One full step with the CFL dt computed and clipped on device.  The CFL
+// minimum of the step's result is reduced by its last stage (MODE_CFL) and
+// marked ready by the commit, so the next step's dt_kernel returns at once;
+// dt_kernel reads the state only when nothing reduced it (first step after
+// an upload, a host-driven stage or the start of sfg_advance).
 int enqueue_cfl_step(sfg_solver_s* s, bool require_active) {
-    CUDA_TRY(launch_dt(s->gv, s->qn, s->clock, s->flags, 0, s->stream));
+    CUDA_TRY(launch_dt(s->gv, s->qn, s->clock, s->flags, 1, s->stream));
     CUDA_TRY(launch_finalize_dt(s->clock, s->stream));
-    for (int st = 0; st < stage_count(s->num.time_recipe); ++st) {
-        int rc = enqueue_stage(s, st, false, require_active);
+    const int ns = stage_count(s->num.time_recipe);
+    for (int st = 0; st < ns; ++st) {
+        int rc = enqueue_stage(s, st, false, require_active, st == ns - 1);
         if (rc) return rc;
     }
     if (s->num.time_recipe == T_EULER) {
@@ -294,7 +302,7 @@ int enqueue_cfl_step(sfg_solver_s* s, bool require_active) {
         int rc = enqueue_post_step(s);
         if (rc) return rc;
     }
-    CUDA_TRY(launch_commit(s->clock, s->dt_log, s->dt_log_cap, s->stream));
+    CUDA_TRY(launch_commit(s->clock, s->dt_log, s->dt_log_cap, 1, s->stream));
     return SFG_OK;
 }
 
@@ -647,7 +655,7 @@ int sfg_stage(sfg_solver s, int stage, double dt) {
     if (stage == ns - 1) {
         rc = enqueue_post_step(s);
         if (rc) return rc;
-        CUDA_TRY(launch_commit(s->clock, nullptr, 0, s->stream));
+        CUDA_TRY(launch_commit(s->clock, nullptr, 0, 0, s->stream));
         s->next_stage = 0;
     } else {
         s->next_stage = stage + 1;
@@ -677,6 +685,8 @@ int sfg_step(sfg_solver s, double dt, double limit) {
     s->host_clock->t_end = kInf;
     s->host_clock->max_steps = std::numeric_limits<long long>::max();
     s->host_clock->limit = limit > 0.0 ? limit : kInf;
+    s->host_clock->dt_bits = 0x7FEFFFFFFFFFFFFFull;
+    s->host_clock->dt_ready = 0;
     s->host_clock->write_interval = 0.0;
     s->host_clock->next_out = kInf;
     rc = push_clock(s);
@@ -703,6 +713,7 @@ int sfg_advance(sfg_solver s, double t_end, int64_t max_steps, double write_inte
     hc->limit = kInf;
     hc->log_base = steps0;
     hc->dt_bits = 0x7FEFFFFFFFFFFFFFull;
+    hc->dt_ready = 0;  // the first step reduces the CFL minimum itself
     // dt log buffer
     const long long want = dt_out && dt_capacity > 0 ? dt_capacity : 0;
     if (want > s->dt_log_cap) {
@@ -826,7 +837,7 @@ int sfg_stage_with_residual(sfg_solver s, int stage, double dt, const double* ho
     if (stage == ns - 1) {
         int rc = enqueue_post_step(s);
         if (rc) return rc;
-        CUDA_TRY(launch_commit(s->clock, nullptr, 0, s->stream));
+        CUDA_TRY(launch_commit(s->clock, nullptr, 0, 0, s->stream));
         s->next_stage = 0;
     } else {
         s->next_stage = stage + 1;

@@ -34,6 +34,52 @@ __device__ __forceinline__ void atomic_min_positive(unsigned long long* bits, do
     atomicMin(bits, (unsigned long long)__double_as_longlong(v));
 }
 
+// Spectral-radius sum of one node for the CFL step (RusanovEOS::deltaT,
+// SF_rusanovEOS.cpp:110-147): sr = sum_active (|u_d| + c) metric_d, with the
+// state closed as SingleFluidStateModel::close does (u = m / rho,
+// p = (gamma - 1) rho (E - rho |u|^2 / 2) / rho, c = sqrt(gamma p / rho)).
+// Every operation is an explicit round-to-nearest intrinsic in the
+// reference's order, so the standalone reduction (dt_kernel) and the one fused
+// into a step's last stage give the same bits -- and the same bits as the
+// oracle's uncontracted C.  dt = CFL / max sr (division is monotonic, so this
+// equals the minimum of CFL / sr).
+__device__ __forceinline__ double cfl_rate(const GridView& g, const double (&q)[5]) {
+    const double rho = q[0];
+    const double u = __ddiv_rn(q[1], rho), v = __ddiv_rn(q[2], rho), w = __ddiv_rn(q[3], rho);
+    const double uu = __dadd_rn(__dadd_rn(__dmul_rn(u, u), __dmul_rn(v, v)), __dmul_rn(w, w));
+    const double kin = __dmul_rn(__dmul_rn(0.5, rho), uu);
+    const double e = __ddiv_rn(__dsub_rn(q[4], kin), rho);
+    const double p = __dmul_rn(__dmul_rn(g.gamma - 1.0, rho), e);
+    const double c = __dsqrt_rn(__ddiv_rn(__dmul_rn(g.gamma, p), rho));
+    double sr = __dadd_rn(fabs(__dmul_rn(u, g.metric[0])), __dmul_rn(c, g.metric[0]));
+    if (g.dim > 1) sr = __dadd_rn(sr, __dadd_rn(fabs(__dmul_rn(v, g.metric[1])), __dmul_rn(c, g.metric[1])));
+    if (g.dim > 2) sr = __dadd_rn(sr, __dadd_rn(fabs(__dmul_rn(w, g.metric[2])), __dmul_rn(c, g.metric[2])));
+    return sr;
+}
+
+// Largest sr of a warp, then one atomic: clock->dt_bits = min(.., CFL / sr).
+// Callers pass sr = 0 for threads without a node.
+__device__ __forceinline__ void flush_cfl_warp(const GridView& g, Clock* clock, double sr) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sr = fmax(sr, __shfl_xor_sync(0xffffffffu, sr, o));
+    if ((threadIdx.x & 31) == 0 && sr > 0.0) atomic_min_positive(&clock->dt_bits, __ddiv_rn(g.cfl, sr));
+}
+
+// The same for a whole block (every thread of the block must call it).
+__device__ __forceinline__ void flush_cfl_block(const GridView& g, Clock* clock, double sr) {
+    __shared__ double warp_max[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sr = fmax(sr, __shfl_xor_sync(0xffffffffu, sr, o));
+    const int warps = (blockDim.x + 31) >> 5;
+    __syncthreads();  // warp_max may still be read by a previous call
+    if ((threadIdx.x & 31) == 0) warp_max[threadIdx.x >> 5] = sr;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int i = 1; i < warps; ++i) sr = fmax(sr, warp_max[i]);
+        if (sr > 0.0) atomic_min_positive(&clock->dt_bits, __ddiv_rn(g.cfl, sr));
+    }
+}
+
 // Stage combination at one node for one variable (applySSPStage, applyStage,
 // applyFinalRK4, applyDivergence).  qs_v is the current value, r the residual.
 __device__ __forceinline__ double stage_value(const StageView& sv, double dt, double qs_v, double r,
@@ -55,9 +101,11 @@ __device__ __forceinline__ double stage_value(const StageView& sv, double dt, do
 }
 
 // Finishes one node: residual output or stage update + state validation
-// (validateEquationState after every stage, SF_explicit.cpp:417).
+// (validateEquationState after every stage, SF_explicit.cpp:417).  With
+// MODE_CFL, sr_max also takes the node's CFL rate of the new state.
 __device__ __forceinline__ void finish_node(const GridView& g, const StageView& sv, double dt, long long node,
-                                            const double (&qn)[5], double (&div)[5], unsigned& flags) {
+                                            const double (&qn)[5], double (&div)[5], unsigned& flags,
+                                            double& sr_max) {
     const long long vs = g.vs;
     if (sv.mode & MODE_RESIDUAL) {
 #pragma unroll
@@ -74,6 +122,7 @@ __device__ __forceinline__ void finish_node(const GridView& g, const StageView& 
     if (!(out[0] > 0.0)) flags |= FLAG_DENSITY;
     if (!(p > 0.0)) flags |= FLAG_PRESSURE;
     if (!isfinite(out[0] + out[1] + out[2] + out[3] + out[4])) flags |= FLAG_NONFINITE;
+    if (sv.mode & MODE_CFL) sr_max = fmax(sr_max, cfl_rate(g, out));
 }
 
 __device__ __forceinline__ void flush_status(const StageView& sv, unsigned flags, unsigned cores, unsigned cut) {

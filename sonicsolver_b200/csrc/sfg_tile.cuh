@@ -70,7 +70,7 @@ __device__ __forceinline__ int map_tile_index(int i, int n, int bcl, int bch) {
 // ------------------------------------------------------------------ 2-D FP64
 template <int SCHEME, int FLUX, int TX, int TY>
 __device__ __forceinline__ void tile2d_body(const GridView& g, const StageView& sv, int x0, int y0, double* smem,
-                                            unsigned& flags, unsigned& cut, unsigned& cores) {
+                                            unsigned& flags, unsigned& cut, unsigned& cores, double& sr_max) {
     using S = TileShape<SCHEME, TX, TY>;
     constexpr int NST = S::NST, H = S::H, SX = S::SX, SY = S::SY, NFX = S::NFX, NFY = S::NFY;
     constexpr int NFXP = S::NFXP, NFYP = S::NFYP;
@@ -133,14 +133,14 @@ __device__ __forceinline__ void tile2d_body(const GridView& g, const StageView& 
             div[v] = (fxv[1] - fxv[0]) + (fyv[TX] - fyv[0]);
             qn[v] = sq[v * SX * SY + (r + H) * SX + c + H];
         }
-        finish_node(g, sv, dt, node, qn, div, flags);
+        finish_node(g, sv, dt, node, qn, div, flags, sr_max);
     }
 }
 
 // ------------------------------------------------------------------ 2-D FP32 flux
 template <int SCHEME, int FLUX, int TX, int TY>
 __device__ __forceinline__ void tile2d_f32_body(const GridView& g, const StageView& sv, int x0, int y0, float* smem,
-                                                unsigned& flags, unsigned& cut, unsigned& cores) {
+                                                unsigned& flags, unsigned& cut, unsigned& cores, double& sr_max) {
     using S = TileShape<SCHEME, TX, TY>;
     constexpr int NST = S::NST, H = S::H, SX = S::SX, SY = S::SY, NFX = S::NFX, NFY = S::NFY;
     constexpr int NFXP = S::NFXP, NFYP = S::NFYP;
@@ -212,7 +212,7 @@ __device__ __forceinline__ void tile2d_f32_body(const GridView& g, const StageVi
             div[v] = (double(fxv[1]) - double(fxv[0])) + (double(fyv[TX]) - double(fyv[0]));
             qn[v] = __ldg(sv.qs + v * vs + node);
         }
-        finish_node(g, sv, dt, node, qn, div, flags);
+        finish_node(g, sv, dt, node, qn, div, flags, sr_max);
     }
 }
 
@@ -220,7 +220,7 @@ __device__ __forceinline__ void tile2d_f32_body(const GridView& g, const StageVi
 // T = double: FP64 stencil; T = float: FP32 deviations from the tile's first node.
 template <int SCHEME, int FLUX, typename T>
 __device__ __forceinline__ void tile1d_body(const GridView& g, const StageView& sv, int x0, T* smem, unsigned& flags,
-                                            unsigned& cut, unsigned& cores) {
+                                            unsigned& cut, unsigned& cores, double& sr_max) {
     using S = Tile1Shape<SCHEME>;
     constexpr int NST = S::NST, H = S::H, SX = S::SX, NF = S::NF;
     constexpr bool F32 = sizeof(T) == sizeof(float);
@@ -263,7 +263,7 @@ __device__ __forceinline__ void tile1d_body(const GridView& g, const StageView& 
             div[v] = double(fx[v * NF + c + 1]) - double(fx[v * NF + c]);
             qn[v] = F32 ? __ldg(sv.qs + v * vs + gx) : double(sq[v * SX + c + H]);
         }
-        finish_node(g, sv, dt, gx, qn, div, flags);
+        finish_node(g, sv, dt, gx, qn, div, flags, sr_max);
     }
 }
 

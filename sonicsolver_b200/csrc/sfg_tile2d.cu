@@ -11,8 +11,10 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) tile2d_kernel(GridView g, Sta
     const int ntx = (g.hi[0] - g.lo[0] + TX - 1) / TX;
     const int x0 = g.lo[0] + (blockIdx.x % ntx) * TX, y0 = g.lo[1] + (blockIdx.x / ntx) * TY;
     unsigned flags = 0, cut = 0, cores = 0;
-    tile2d_body<SCHEME, FLUX, TX, TY>(g, sv, x0, y0, smem, flags, cut, cores);
+    double sr = 0.0;
+    tile2d_body<SCHEME, FLUX, TX, TY>(g, sv, x0, y0, smem, flags, cut, cores, sr);
     flush_status(sv, flags, cores, cut);
+    if (sv.mode & MODE_CFL) flush_cfl_block(g, sv.clock, sr);
 }
 
 template <int SCHEME, int FLUX, int TX, int TY>
@@ -22,8 +24,10 @@ __global__ void __launch_bounds__(TILE_THREADS, 3) tile2d_f32_kernel(GridView g,
     const int ntx = (g.hi[0] - g.lo[0] + TX - 1) / TX;
     const int x0 = g.lo[0] + (blockIdx.x % ntx) * TX, y0 = g.lo[1] + (blockIdx.x / ntx) * TY;
     unsigned flags = 0, cut = 0, cores = 0;
-    tile2d_f32_body<SCHEME, FLUX, TX, TY>(g, sv, x0, y0, smemf, flags, cut, cores);
+    double sr = 0.0;
+    tile2d_f32_body<SCHEME, FLUX, TX, TY>(g, sv, x0, y0, smemf, flags, cut, cores, sr);
     flush_status(sv, flags, cores, cut);
+    if (sv.mode & MODE_CFL) flush_cfl_block(g, sv.clock, sr);
 }
 
 template <int SCHEME, int FLUX, typename T, int TX, int TY>
@@ -70,9 +74,11 @@ __global__ void __launch_bounds__(TILE_THREADS) tile1d_kernel(GridView g, StageV
     extern __shared__ __align__(16) unsigned char smem1[];
     if (sv.require_active && !sv.clock->active) return;
     unsigned flags = 0, cut = 0, cores = 0;
+    double sr = 0.0;
     tile1d_body<SCHEME, FLUX, T>(g, sv, g.lo[0] + blockIdx.x * TILE1D, reinterpret_cast<T*>(smem1), flags, cut,
-                                 cores);
+                                 cores, sr);
     flush_status(sv, flags, cores, cut);
+    if (sv.mode & MODE_CFL) flush_cfl_block(g, sv.clock, sr);
 }
 
 template <int SCHEME, int FLUX, typename T>
