@@ -97,7 +97,7 @@ __device__ __forceinline__ StageView batch_stage_view(BatchInst& b, int stage, i
 }
 
 template <int SCHEME, int FLUX, bool F32, int TX, int TY>
-__global__ void __launch_bounds__(TILE_THREADS, F32 ? 3 : 2)
+__global__ void __launch_bounds__(TILE_THREADS, F32 ? 4 : 2)
     batch_stage_kernel(BatchInst* inst, const WorkItem* items, BatchCtl* ctl, int stage, int time_id) {
     using Tt = typename std::conditional<F32, float, double>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];

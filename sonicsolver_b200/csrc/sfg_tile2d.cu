@@ -18,7 +18,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) tile2d_kernel(GridView g, Sta
 }
 
 template <int SCHEME, int FLUX, int TX, int TY>
-__global__ void __launch_bounds__(TILE_THREADS, 3) tile2d_f32_kernel(GridView g, StageView sv) {
+__global__ void __launch_bounds__(TILE_THREADS, 4) tile2d_f32_kernel(GridView g, StageView sv) {
     extern __shared__ __align__(16) float smemf[];
     if (sv.require_active && !sv.clock->active) return;
     const int ntx = (g.hi[0] - g.lo[0] + TX - 1) / TX;
