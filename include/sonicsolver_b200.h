@@ -4,7 +4,8 @@
  * One opaque solver handle per structured grid (or one batch / server handle
  * for many grids) carries device-resident conserved state and runs the
  * density-based explicit path of sonicSolver on one GPU:
- *   characteristic WENO/TENO reconstruction -> Rusanov/Roe face flux ->
+ *   characteristic WENO/TENO reconstruction -> Steger-Warming / Rusanov /
+ *   Lax-Friedrichs / Roe / Lax-Wendroff face flux ->
  *   conservative divergence -> ghost/periodic fill -> forwardEuler / SSPRK3 /
  *   classicalRK4 stage combination, with the CFL time step reduced on device.
  *
@@ -67,14 +68,26 @@ enum {
 /* Convection recipes: the values of FDM::TermRecipeId
  * (src/core/config/types/SF_termRecipe.h:52-64). */
 enum {
-    SFG_RECIPE_WENO3_RUSANOV = 1,
-    SFG_RECIPE_WENO3_ROE = 3,
+    SFG_RECIPE_WENO3_STEGER = 0,      /* Steger-Warming, Lax-Friedrichs and     */
+    SFG_RECIPE_WENO3_RUSANOV = 1,     /* Lax-Wendroff faces: FP64 single-grid   */
+    SFG_RECIPE_WENO3_LAXF = 2,        /* solvers only (SFG_PREC_FP32_FLUX and   */
+    SFG_RECIPE_WENO3_ROE = 3,         /* batches take Rusanov and Roe)          */
+    SFG_RECIPE_WENO3_LAXW = 4,
+    SFG_RECIPE_WENO5_STEGER = 5,
     SFG_RECIPE_WENO5_RUSANOV = 6,
+    SFG_RECIPE_WENO5_LAXF = 7,
     SFG_RECIPE_WENO5_ROE = 8,
+    SFG_RECIPE_WENO5_LAXW = 9,
+    SFG_RECIPE_TENO5_STEGER = 10,
     SFG_RECIPE_TENO5_RUSANOV = 11,
+    SFG_RECIPE_TENO5_LAXF = 12,
     SFG_RECIPE_TENO5_ROE = 13,
+    SFG_RECIPE_TENO5_LAXW = 14,
+    SFG_RECIPE_WENO7_STEGER = 15,
     SFG_RECIPE_WENO7_RUSANOV = 16,
-    SFG_RECIPE_WENO7_ROE = 18
+    SFG_RECIPE_WENO7_LAXF = 17,
+    SFG_RECIPE_WENO7_ROE = 18,
+    SFG_RECIPE_WENO7_LAXW = 19
 };
 /* Time recipes: the values of FDM::TimeRecipeId (SF_timeRecipe.h:11). */
 enum { SFG_TIME_FORWARD_EULER = 0, SFG_TIME_SSPRK3 = 1, SFG_TIME_CLASSICAL_RK4 = 2 };

@@ -97,6 +97,10 @@ def _load(path):
 def _sig(lib, prefix):
     G = ctypes.POINTER(Grid)
     C = ctypes.POINTER(Counters)
+    # both libraries hold the restatement's step-dt slot (the reference
+    # library links its own copy of sf_oracle.c)
+    lib.sfo_set_step_dt.argtypes = [ctypes.c_double]
+    lib.sfo_step_dt.restype = ctypes.c_double
     if prefix == "sfo":
         lib.sfo_storage_size.argtypes = [G]
         lib.sfo_storage_size.restype = ctypes.c_longlong
@@ -108,6 +112,11 @@ def _sig(lib, prefix):
         lib.sfo_char_matrix.argtypes = [_DP, _DP, ctypes.c_double, _DP, _DP]
         lib.sfo_rusanov_flux.argtypes = [_DP, _DP, _DP, ctypes.c_double, _DP]
         lib.sfo_roe_flux.argtypes = [_DP, _DP, _DP, ctypes.c_double, _DP]
+        lib.sfo_steger_flux.argtypes = [_DP, _DP, _DP, ctypes.c_double, _DP]
+        lib.sfo_lf_flux.argtypes = [_DP, _DP, _DP, ctypes.c_double, _DP]
+        lib.sfo_lw_flux.argtypes = [_DP, _DP, _DP, ctypes.c_double, ctypes.c_double, ctypes.c_double, _DP]
+        lib.sfo_char_face_flux_ex.argtypes = [ctypes.c_int, _DP, _DP, ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_double, ctypes.c_double, ctypes.c_double, _DP]
         lib.sfo_char_face_flux.argtypes = [ctypes.c_int, _DP, _DP, ctypes.c_int, ctypes.c_int,
                                            ctypes.c_double, _DP]
         lib.sfo_fill_ghosts.argtypes = [G, _DP]
@@ -130,6 +139,9 @@ def _sig(lib, prefix):
         lib.sfr_char_matrix.argtypes = [_DP, _DP, ctypes.c_double, _DP, _DP]
         lib.sfr_rusanov_flux.argtypes = [_DP, _DP, _DP, ctypes.c_double, _DP]
         lib.sfr_roe_flux.argtypes = [_DP, _DP, _DP, ctypes.c_double, _DP]
+        lib.sfr_steger_flux.argtypes = [_DP, _DP, _DP, ctypes.c_double, _DP]
+        lib.sfr_lf_flux.argtypes = [_DP, _DP, _DP, ctypes.c_double, _DP]
+        lib.sfr_lw_flux.argtypes = [_DP, _DP, _DP, ctypes.c_double, ctypes.c_double, ctypes.c_double, _DP]
         lib.sfr_case_create.argtypes = [G, ctypes.c_int, ctypes.c_int]
         lib.sfr_case_create.restype = ctypes.c_void_p
         lib.sfr_case_destroy.argtypes = [ctypes.c_void_p]
@@ -180,6 +192,17 @@ class OracleError(RuntimeError):
 
 def fill_ghosts(spec: GridSpec, Q: np.ndarray) -> None:
     _check(oracle_lib().sfo_fill_ghosts(ctypes.byref(spec.c()), _ptr(Q)), "fill_ghosts")
+
+
+def set_step_dt(dt: float) -> None:
+    """Step size the Lax-Wendroff flux sees in a bare rhs call (the stage
+    and step functions set it from their own dt), in the restatement and in
+    the reference library."""
+    oracle_lib().sfo_set_step_dt(dt)
+    ref_lib(False)
+    for ref in _ref.values():
+        if ref is not None:
+            ref.sfo_set_step_dt(dt)
 
 
 def rhs(spec: GridSpec, scheme: int, flux: int, Q: np.ndarray, counters: Counters | None = None):

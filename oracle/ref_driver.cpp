@@ -9,7 +9,8 @@
 // What runs reference code:
 //   - the spatial operator: SF::divDispatch (solver/discretization/convection/
 //     SF_div.h:212-243) with its WENO/TENO cores, characteristic matrices,
-//     Rusanov/Roe fluxes, face loops and residual assembly, then
+//     Steger-Warming / Rusanov / Lax-Friedrichs / Roe / Lax-Wendroff fluxes,
+//     face loops and residual assembly, then
 //     Math::spatialResidual (methods/numerics/structured/SF_residualAssembly.h:34-41);
 //   - the CFL step: Numerics::RusanovEOS::deltaT (Flux/SF_rusanovEOS.cpp:110-147).
 // What is restated here (the reference's versions need the full solver
@@ -21,6 +22,9 @@
 #include "core/residual/SF_residual.h"
 #include "core/mesh/SF_dimension.h"
 #include "methods/numerics/Flux/SF_rusanovEOS.h"
+#include "methods/numerics/Flux/SF_sw.h"
+#include "methods/numerics/Flux/SF_lxF.h"
+#include "methods/numerics/Flux/SF_lw.h"
 #include "methods/numerics/structured/SF_residualAssembly.h"
 #include "models/physics/fluidStateModel/SF_singleFluidStateModel.h"
 #include "models/physics/EOS/SF_perfectGasEOS.h"
@@ -149,6 +153,7 @@ int flux_of(int f, SF::FDM::FluxSplitter* out) {
     case SFO_RUSANOV: *out = SF::FDM::FluxSplitter::Rusanov; return 0;
     case SFO_LAXFRIEDRICHS: *out = SF::FDM::FluxSplitter::LaxFriedrichs; return 0;
     case SFO_ROE: *out = SF::FDM::FluxSplitter::Roe; return 0;
+    case SFO_LAXWENDROFF: *out = SF::FDM::FluxSplitter::LaxWendroff; return 0;
     }
     return SFO_ERR_ARG;
 }
@@ -169,7 +174,7 @@ int sfr_rhs(const sfo_grid* g, int scheme, int flux, const double* Q, double* R)
         load_state(rc, Q);
         rc.flux.clear();
         rc.residual.clear();
-        SF::divDispatch(rc.field, rc.flux, rc.residual, cs, fs, 0.0,
+        SF::divDispatch(rc.field, rc.flux, rc.residual, cs, fs, sfo_step_dt(),
                         SF::FDM::IBMBoundaryScheme::LowOrder, 0, g->gamma, *rc.model);
         const long long S = 5LL * storage_extent(g, 0) * storage_extent(g, 1) * storage_extent(g, 2);
         std::memset(R, 0, sizeof(double) * (size_t)S);
@@ -219,7 +224,7 @@ static int case_rhs(void* ctx, const double* Q, double* R) {
         load_state(pc->rc, Q);
         pc->rc.flux.clear();
         pc->rc.residual.clear();
-        SF::divDispatch(pc->rc.field, pc->rc.flux, pc->rc.residual, pc->cs, pc->fs, 0.0,
+        SF::divDispatch(pc->rc.field, pc->rc.flux, pc->rc.residual, pc->cs, pc->fs, sfo_step_dt(),
                         SF::FDM::IBMBoundaryScheme::LowOrder, 0, g->gamma, *pc->rc.model);
         const int m0 = storage_extent(g, 0), m1 = storage_extent(g, 1);
         int off[3];
@@ -309,6 +314,19 @@ int sfr_rusanov_flux(const double* qL, const double* qR, const double* n, double
 }
 void sfr_roe_flux(const double* qL, const double* qR, const double* n, double gamma, double* out) {
     SF::Flux::RoeFlux::flux(qL, qR, n, out, gamma);
+}
+// The reference's Steger-Warming, Lax-Friedrichs and Lax-Wendroff face
+// fluxes (Flux/SF_sw.cpp, SF_lxF.cpp, SF_lw.cpp).  They exit the process on an
+// invalid state, so callers pass valid states only.
+void sfr_steger_flux(const double* qL, const double* qR, const double* n, double gamma, double* out) {
+    SF::Flux::StegerWarmingFlux::flux(qL, qR, n, out, gamma);
+}
+void sfr_lf_flux(const double* qL, const double* qR, const double* n, double gamma, double* out) {
+    SF::Flux::LaxFriedrichsFlux::flux(qL, qR, n, out, gamma);
+}
+void sfr_lw_flux(const double* qL, const double* qR, const double* n, double dt, double spacing, double gamma,
+                 double* out) {
+    SF::Flux::LaxWendroffFlux::flux(qL, qR, n, dt, spacing, out, gamma);
 }
 
 }  // extern "C"

@@ -337,15 +337,131 @@ int sfo_roe_flux(const double* qL, const double* qR, const double* n, double gam
 
 /* ------------------------------------------------------------------ */
 /* Characteristic face flux                                            */
+/* Riemann::splitStegerWarming, SF_riemann.cpp:15-67: F+ and F- of one state
+ * with the entropy-fixed eigenvalue split (eps = 0.01). */
+static int steger_split(const double* Q, const double* n, double gamma, double* fpos, double* fneg) {
+    const double r = Q[0];
+    double p;
+    int err = physical_pressure(Q, gamma, &p);
+    if (err) return err;
+    const double invR = 1.0 / r;
+    const double u = Q[1] * invR, v = Q[2] * invR, w = Q[3] * invR;
+    const double q2 = u * u + v * v + w * w;
+    const double a = sqrt(gamma * p * invR);
+    const double un = u * n[0] + v * n[1] + w * n[2];
+    const double lam[5] = {un, un, un, un + a, un - a};
+    double lp[5], lm[5];
+    const double eps_sw = 0.01;
+    for (int i = 0; i < 5; ++i) {
+        if (fabs(lam[i]) < 2.0 * eps_sw) {
+            lp[i] = 0.5 * (lam[i] * lam[i] / (4.0 * eps_sw) + lam[i] + eps_sw);
+            lm[i] = lam[i] - lp[i];
+        } else {
+            lp[i] = 0.5 * (lam[i] + fabs(lam[i]));
+            lm[i] = 0.5 * (lam[i] - fabs(lam[i]));
+        }
+    }
+    const double common = r / (2.0 * gamma);
+    const double* l2[2] = {lp, lm};
+    double* out2[2] = {fpos, fneg};
+    for (int s = 0; s < 2; ++s) {
+        const double* l = l2[s];
+        double* f = out2[s];
+        const double W1 = 2.0 * (gamma - 1.0) * l[0] + l[3] + l[4];
+        const double W2 = l[3] - l[4];
+        const double W3 = l[3] + l[4];
+        f[0] = common * W1;
+        f[1] = common * (u * W1 + a * n[0] * W2);
+        f[2] = common * (v * W1 + a * n[1] * W2);
+        f[3] = common * (w * W1 + a * n[2] * W2);
+        f[4] = common * (0.5 * q2 * W1 + a * un * W2 + (a * a / (gamma - 1.0)) * W3);
+    }
+    return SFO_OK;
+}
+
+/* StegerWarmingFlux::flux, SF_sw.cpp:22-28: F+(qL) + F-(qR). */
+int sfo_steger_flux(const double* qL, const double* qR, const double* n, double gamma, double* out) {
+    double fp[5], fm[5], unused[5];
+    int err = steger_split(qL, n, gamma, fp, unused);
+    if (!err) err = steger_split(qR, n, gamma, unused, fm);
+    if (err) return err;
+    for (int v = 0; v < 5; ++v) out[v] = fp[v] + fm[v];
+    return SFO_OK;
+}
+
+/* Riemann::splitLaxFriedrichs, SF_riemann.cpp:125-152: (F +- lam_max Q) / 2
+ * with the state's own lam_max = |u.n| + a. */
+static int lf_split(const double* Q, const double* n, double gamma, double* fpos, double* fneg) {
+    const double r = Q[0];
+    double p;
+    int err = physical_pressure(Q, gamma, &p);
+    if (err) return err;
+    const double invR = 1.0 / r;
+    const double u = Q[1] * invR, v = Q[2] * invR, w = Q[3] * invR;
+    const double a = sqrt(gamma * p * invR);
+    const double un = u * n[0] + v * n[1] + w * n[2];
+    const double lam_max = fabs(un) + a;
+    double F[5];
+    F[0] = r * un;
+    F[1] = Q[1] * un + p * n[0];
+    F[2] = Q[2] * un + p * n[1];
+    F[3] = Q[3] * un + p * n[2];
+    F[4] = (Q[4] + p) * un;
+    for (int i = 0; i < 5; ++i) {
+        fpos[i] = 0.5 * (F[i] + lam_max * Q[i]);
+        fneg[i] = 0.5 * (F[i] - lam_max * Q[i]);
+    }
+    return SFO_OK;
+}
+
+/* LaxFriedrichsFlux::flux, SF_lxF.cpp: F+(qL) + F-(qR). */
+int sfo_lf_flux(const double* qL, const double* qR, const double* n, double gamma, double* out) {
+    double fp[5], fm[5], unused[5];
+    int err = lf_split(qL, n, gamma, fp, unused);
+    if (!err) err = lf_split(qR, n, gamma, unused, fm);
+    if (err) return err;
+    for (int v = 0; v < 5; ++v) out[v] = fp[v] + fm[v];
+    return SFO_OK;
+}
+
+/* LaxWendroffFlux::flux, SF_lw.cpp:17-40: the physical flux of the
+ * Richtmyer half-step state (qL + qR)/2 - dt/(2 s) (F(qR) - F(qL)), s the
+ * face spacing.  dt and s must be > 0 (the reference exits otherwise). */
+int sfo_lw_flux(const double* qL, const double* qR, const double* n, double dt, double spacing, double gamma,
+                double* out) {
+    if (!(dt > 0.0) || !(spacing > 0.0)) return SFO_ERR_ARG;
+    double fL[5], fR[5];
+    int err = physical_euler_flux(qL, n, gamma, fL);
+    if (!err) err = physical_euler_flux(qR, n, gamma, fR);
+    if (err) return err;
+    const double lambda = dt / spacing;
+    double qHalf[5];
+    for (int v = 0; v < 5; ++v) qHalf[v] = 0.5 * (qL[v] + qR[v]) - 0.5 * lambda * (fR[v] - fL[v]);
+    return physical_euler_flux(qHalf, n, gamma, out);
+}
+
 /* ------------------------------------------------------------------ */
 
 static __thread sfo_counters* g_counters = NULL;
+/* Step size seen by the Lax-Wendroff flux inside sfo_rhs: set by the stage
+ * driver from its dt (divDispatch receives the step's dt the same way). */
+static __thread double g_lw_dt = 0.0;
+
+void sfo_set_step_dt(double dt) { g_lw_dt = dt; }
+double sfo_step_dt(void) { return g_lw_dt; }
 
 /* characteristicWENOFaceFlux<NStencil>, SF_WENO.h:184-245, with the scalar
  * stencil gather of fillScalarWENOStencils (SF_WENO.h:79-98): the left state
  * reads points 0..w-1 and the right state the mirrored points N-1..N-w. */
 int sfo_char_face_flux(int nstencil, const double* stencil, const double* metrics, int scheme,
                        int flux, double gamma, double* out) {
+    return sfo_char_face_flux_ex(nstencil, stencil, metrics, scheme, flux, gamma, g_lw_dt, 0.0, out);
+}
+
+/* The same with the step size and face spacing the Lax-Wendroff flux needs
+ * (Flux::faceSpacing, SF_face.h:92-106). */
+int sfo_char_face_flux_ex(int nstencil, const double* stencil, const double* metrics, int scheme,
+                          int flux, double gamma, double dt, double spacing, double* out) {
     const int width = nstencil == 4 ? 4 : (nstencil == 6 ? 5 : 7);
     if (!(nstencil == 4 || nstencil == 6 || nstencil == 8)) return SFO_ERR_ARG;
     const double sx = metrics[0], sy = metrics[1], sz = metrics[2];
@@ -393,8 +509,11 @@ int sfo_char_face_flux(int nstencil, const double* stencil, const double* metric
     gemv5(R, wL, qL);
     gemv5(R, wR, qR);
     switch (flux) {
+    case SFO_STEGER: err = sfo_steger_flux(qL, qR, normal, gamma, f); break;
     case SFO_RUSANOV: err = sfo_rusanov_flux(qL, qR, normal, gamma, f); break;
+    case SFO_LAXFRIEDRICHS: err = sfo_lf_flux(qL, qR, normal, gamma, f); break;
     case SFO_ROE: err = sfo_roe_flux(qL, qR, normal, gamma, f); break;
+    case SFO_LAXWENDROFF: err = sfo_lw_flux(qL, qR, normal, dt, spacing, gamma, f); break;
     default: return SFO_ERR_ARG;
     }
     if (err) return err;
@@ -540,8 +659,14 @@ int sfo_rhs(const sfo_grid* g, int scheme, int flux, const double* Q, double* R,
                         const long long off = at + (long long)(s - (nst / 2 - 1)) * sd;
                         for (int v = 0; v < 5; ++v) st[s * 5 + v] = Q[off + v];
                     }
+                    /* faceSpacing on coordinates X = (index - ng) h, as the
+                     * reference Field of the harness holds them */
+                    const int li = d == 0 ? i : (d == 1 ? j : k);
+                    const double xl = (double)(li - g->ng) * g->h[d], xr = (double)(li + 1 - g->ng) * g->h[d];
+                    double spacing = fabs(xr - xl);
+                    spacing = spacing > 1e-14 ? spacing : 1e-14;
                     double f[5];
-                    err = sfo_char_face_flux(nst, st, metrics, scheme, flux, g->gamma, f);
+                    err = sfo_char_face_flux_ex(nst, st, metrics, scheme, flux, g->gamma, g_lw_dt, spacing, f);
                     if (err) break;
                     for (int v = 0; v < 5; ++v) {
                         if (!isfinite(f[v])) { err = SFO_ERR_NONFINITE; break; }
@@ -627,6 +752,7 @@ int sfo_stage_fn(const sfo_grid* g, sfo_rhs_fn rhs, void* ctx, int time_id, doub
                  int stage, double* work) {
     const int ns = stage_count(time_id);
     if (!ns || stage < 0 || stage >= ns) return SFO_ERR_ARG;
+    g_lw_dt = dt;  /* the spatial operator of this stage sees the step's dt */
     layout L;
     make_layout(g, &L);
     const long long S = sfo_storage_size(g);

@@ -81,11 +81,26 @@ int sfo_rusanov_flux(const double* qL, const double* qR, const double* n,
                      double gamma, double* out);
 int sfo_roe_flux(const double* qL, const double* qR, const double* n,
                  double gamma, double* out);
+int sfo_steger_flux(const double* qL, const double* qR, const double* n,
+                    double gamma, double* out);
+int sfo_lf_flux(const double* qL, const double* qR, const double* n,
+                double gamma, double* out);
+/* Lax-Wendroff needs the step size and the face spacing (both > 0). */
+int sfo_lw_flux(const double* qL, const double* qR, const double* n, double dt,
+                double spacing, double gamma, double* out);
 /* One characteristic face flux from a (2r)-point conservative stencil
  * (nstencil = 4, 6, 8) and the face metrics [sx, sy, sz, 1/J]; result is
  * multiplied by the face area (SF_WENO.h:184-245). */
 int sfo_char_face_flux(int nstencil, const double* stencil, const double* metrics,
                        int scheme, int flux, double gamma, double* out);
+/* The same with the Lax-Wendroff step size and face spacing. */
+int sfo_char_face_flux_ex(int nstencil, const double* stencil, const double* metrics,
+                          int scheme, int flux, double gamma, double dt, double spacing,
+                          double* out);
+/* Step size the Lax-Wendroff flux of sfo_rhs uses (set by the stage
+ * functions from their dt; sfo_rhs alone needs it set explicitly). */
+void sfo_set_step_dt(double dt);
+double sfo_step_dt(void);
 
 /* Apply the boundary laws of g to the ghost layers / boundary nodes of Q. */
 int sfo_fill_ghosts(const sfo_grid* g, double* Q);

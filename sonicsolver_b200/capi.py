@@ -19,10 +19,11 @@ ERR_ARG, ERR_CUDA, ERR_STATE, ERR_TENO_CUTOFF, ERR_NOMEM, ERR_BUDGET, ERR_TIMEOU
 
 FLAG_NONFINITE, FLAG_DENSITY, FLAG_PRESSURE, FLAG_TENO_CUTOFF, FLAG_ROE_SOUND = 1, 2, 4, 8, 16
 
-RECIPES = {
-    "weno3Rusanov": 1, "weno3Roe": 3, "weno5Rusanov": 6, "weno5Roe": 8,
-    "teno5Rusanov": 11, "teno5Roe": 13, "weno7Rusanov": 16, "weno7Roe": 18,
-}
+# FDM::TermRecipeId values: scheme * 5 + face flux (Steger, Rusanov,
+# LaxFriedrichs, Roe, LaxWendroff).
+RECIPES = {f"{sch}{flx}": 5 * i + j
+           for i, sch in enumerate(("weno3", "weno5", "teno5", "weno7"))
+           for j, flx in enumerate(("Steger", "Rusanov", "LaxFriedrichs", "Roe", "LaxWendroff"))}
 TIME_RECIPES = {"forwardEuler": 0, "SSPRK3": 1, "classicalRK4": 2}
 PREC_FP64, PREC_FP32_FLUX = 0, 1
 BC_TRANSMISSIVE, BC_PERIODIC, BC_FROZEN = 0, 1, 2

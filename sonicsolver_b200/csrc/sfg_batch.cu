@@ -485,6 +485,7 @@ int batch_grid_view(const sfg_grid_desc* d, const sfg_numerics_desc* n, int reac
     g.metric[2] = (hx * hy) * g.jac;
     for (int a = 0; a < 3; ++a) g.area[a] = 0.5 * (g.metric[a] / g.jac + g.metric[a] / g.jac);
     g.gamma = n->gamma;
+    for (int a = 0; a < 3; ++a) g.h[a] = d->h[a];
     g.cfl = n->cfl;
     *nodes = (long long)d->n[0] * d->n[1] * d->n[2];
     g.vs = (*nodes + 31) / 32 * 32;

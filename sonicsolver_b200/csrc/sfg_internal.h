@@ -22,7 +22,7 @@ constexpr unsigned FLAG_ROE_SOUND = 1u << 4;
 // Reconstruction schemes in the order of FDM::ConvectionScheme and face
 // fluxes with the values of FDM::FluxSplitter (SF_termRecipe.h:14,33-40).
 enum Scheme { WENO3 = 0, WENO5 = 1, TENO5 = 2, WENO7 = 3 };
-enum Flux { RUSANOV = 1, ROE = 3 };
+enum Flux { STEGER = 0, RUSANOV = 1, LAXF = 2, ROE = 3, LAXW = 4 };
 
 // Device-resident step clock: the Time::Driver bookkeeping
 // (src/solver/algorithm/time/SF_time.cpp:42-93) and FlowDtCompute's
@@ -57,6 +57,7 @@ struct GridView {
     double metric[3];  // xi_x, eta_y, zeta_z
     double gamma;
     double cfl;
+    double h[3];       // node spacing (the Lax-Wendroff face spacing)
 };
 
 // Stage arithmetic of one launch (Time::Explicit, SF_explicit.cpp:193-238,282-285).

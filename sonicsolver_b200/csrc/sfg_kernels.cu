@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(128) sweep_x(GridView g, StageView sv) {
                 for (int v = 0; v < 5; ++v) d[s][v] = float(st[s][v] - qref[v]);
             face_flux_dev32<0, SCHEME, FLUX>(d, ref, float(g.gamma), Ft, flags, cut);
         } else {
-            face_flux<0, SCHEME, FLUX, T>(st, T(g.gamma), Ft, flags, cut);
+            face_flux<0, SCHEME, FLUX, T>(st, T(g.gamma), Ft, flags, cut, T(FLUX == LAXW ? sv.clock->dt / g.h[0] : 0.0));
         }
 #pragma unroll
         for (int v = 0; v < 5; ++v) F[v] = double(Ft[v]) * g.area[0];
@@ -208,7 +208,8 @@ __global__ void __launch_bounds__(128) sweep_yz(GridView g, StageView sv) {
         double Fp[5];
         for (int f = s0; f <= s1; ++f) {
             T Ft[5];
-            face_flux<AX, SCHEME, FLUX, T>(st, T(g.gamma), Ft, flags, cut);
+            face_flux<AX, SCHEME, FLUX, T>(st, T(g.gamma), Ft, flags, cut,
+                                           T(FLUX == LAXW ? sv.clock->dt / g.h[AX] : 0.0));
             if (SCHEME == TENO5) cores += 10;
             double F[5];
 #pragma unroll
@@ -418,23 +419,28 @@ static cudaError_t launch_axis(int axis, const GridView& g, const StageView& sv,
     return cudaGetLastError();
 }
 
+template <int FLUX, typename T>
+static cudaError_t launch_axis_s(int scheme, int axis, const GridView& g, const StageView& sv, cudaStream_t st) {
+    switch (scheme) {
+    case WENO5: return launch_axis<WENO5, FLUX, T>(axis, g, sv, st);
+    case TENO5: return launch_axis<TENO5, FLUX, T>(axis, g, sv, st);
+    case WENO3: return launch_axis<WENO3, FLUX, T>(axis, g, sv, st);
+    case WENO7: return launch_axis<WENO7, FLUX, T>(axis, g, sv, st);
+    }
+    return cudaErrorInvalidValue;
+}
+
+// Rusanov and Roe in both precisions; Steger-Warming, Lax-Friedrichs and
+// Lax-Wendroff faces in FP64.
 template <typename T>
 static cudaError_t launch_axis_t(int scheme, int flux, int axis, const GridView& g, const StageView& sv,
                                  cudaStream_t st) {
-    if (flux == RUSANOV) {
-        switch (scheme) {
-        case WENO5: return launch_axis<WENO5, RUSANOV, T>(axis, g, sv, st);
-        case TENO5: return launch_axis<TENO5, RUSANOV, T>(axis, g, sv, st);
-        case WENO3: return launch_axis<WENO3, RUSANOV, T>(axis, g, sv, st);
-        case WENO7: return launch_axis<WENO7, RUSANOV, T>(axis, g, sv, st);
-        }
-    } else if (flux == ROE) {
-        switch (scheme) {
-        case WENO5: return launch_axis<WENO5, ROE, T>(axis, g, sv, st);
-        case TENO5: return launch_axis<TENO5, ROE, T>(axis, g, sv, st);
-        case WENO3: return launch_axis<WENO3, ROE, T>(axis, g, sv, st);
-        case WENO7: return launch_axis<WENO7, ROE, T>(axis, g, sv, st);
-        }
+    if (flux == RUSANOV) return launch_axis_s<RUSANOV, T>(scheme, axis, g, sv, st);
+    if (flux == ROE) return launch_axis_s<ROE, T>(scheme, axis, g, sv, st);
+    if constexpr (sizeof(T) == sizeof(double)) {
+        if (flux == STEGER) return launch_axis_s<STEGER, T>(scheme, axis, g, sv, st);
+        if (flux == LAXF) return launch_axis_s<LAXF, T>(scheme, axis, g, sv, st);
+        if (flux == LAXW) return launch_axis_s<LAXW, T>(scheme, axis, g, sv, st);
     }
     return cudaErrorInvalidValue;
 }

@@ -514,9 +514,119 @@ __device__ __forceinline__ void roe(const T qL[5], const T qR[5], T gamma, T F[5
 // (computed in FP64): the projections are linear and the WENO/TENO cores are
 // invariant to adding a constant, so the result is the same mathematics while
 // single precision only has to resolve the variation across the stencil.
+// Pressure of a conserved state as Numerics::pressure (SF_utility.h:24-29),
+// with the validation flags of requirePhysicalState.
+template <typename T>
+__device__ __forceinline__ T state_pressure(const T q[5], T gamma, T inv_rho, unsigned& flags) {
+    const T ke = T(0.5) * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]) * inv_rho;
+    const T p = (gamma - T(1)) * (q[4] - ke);
+    if (!(q[0] > T(0))) flags |= FLAG_DENSITY;
+    if (!(p > T(0))) flags |= FLAG_PRESSURE;
+    return p;
+}
+
+// Steger-Warming split of one state (Riemann::splitStegerWarming,
+// SF_riemann.cpp:15-67), the positive (POS) or negative part, for the unit
+// normal e_AX: eigenvalues u_n, u_n +- a split with the entropy fix of width
+// 2 eps, eps = 0.01.
+template <int AX, bool POS, typename T>
+__device__ __forceinline__ void steger_part(const T q[5], T gamma, T f[5], unsigned& flags) {
+    constexpr int N = AxisBasis<AX>::N;
+    const T r = q[0];
+    const T inv = rcp<T>(r);
+    const T p = state_pressure<T>(q, gamma, inv, flags);
+    const T vel[3] = {q[1] * inv, q[2] * inv, q[3] * inv};
+    const T q2 = vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2];
+    const T a = sqrt_<T>(gamma * p * inv);
+    const T un = vel[N - 1];
+    const T eps = T(0.01);
+    auto part = [&](T lam) {
+        if (fabs(lam) < T(2) * eps) {
+            const T lp = T(0.5) * (lam * lam / (T(4) * eps) + lam + eps);
+            return POS ? lp : lam - lp;
+        }
+        return POS ? T(0.5) * (lam + fabs(lam)) : T(0.5) * (lam - fabs(lam));
+    };
+    const T l0 = part(un), l3 = part(un + a), l4 = part(un - a);
+    const T common = r / (T(2) * gamma);
+    const T W1 = T(2) * (gamma - T(1)) * l0 + l3 + l4;
+    const T W2 = l3 - l4;
+    const T W3 = l3 + l4;
+    f[0] = common * W1;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) f[1 + k] = common * (vel[k] * W1 + (k == N - 1 ? a * W2 : T(0)));
+    f[4] = common * (T(0.5) * q2 * W1 + a * un * W2 + (a * a / (gamma - T(1))) * W3);
+}
+
+// StegerWarmingFlux::flux (Flux/SF_sw.cpp:22-28): F+(qL) + F-(qR).
+template <int AX, typename T>
+__device__ __forceinline__ void steger(const T qL[5], const T qR[5], T gamma, T F[5], unsigned& flags) {
+    T fp[5], fm[5];
+    steger_part<AX, true, T>(qL, gamma, fp, flags);
+    steger_part<AX, false, T>(qR, gamma, fm, flags);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) F[v] = fp[v] + fm[v];
+}
+
+// Lax-Friedrichs split (Riemann::splitLaxFriedrichs, SF_riemann.cpp:125-152)
+// and LaxFriedrichsFlux::flux (Flux/SF_lxF.cpp): (F(qL) + lam_L qL)/2 +
+// (F(qR) - lam_R qR)/2 with each state's own lam = |u_n| + a.
+template <int AX, typename T>
+__device__ __forceinline__ void laxf_part(const T q[5], T gamma, T sign, T f[5], unsigned& flags) {
+    constexpr int N = AxisBasis<AX>::N;
+    const T inv = rcp<T>(q[0]);
+    const T p = state_pressure<T>(q, gamma, inv, flags);
+    const T un = q[N] * inv;
+    const T lam = fabs(un) + sqrt_<T>(gamma * p * inv);
+    T Fp[5];
+    Fp[0] = q[0] * un;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) Fp[1 + k] = q[1 + k] * un + (k == N - 1 ? p : T(0));
+    Fp[4] = (q[4] + p) * un;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) f[v] = T(0.5) * (Fp[v] + sign * lam * q[v]);
+}
+
+template <int AX, typename T>
+__device__ __forceinline__ void laxf(const T qL[5], const T qR[5], T gamma, T F[5], unsigned& flags) {
+    T fp[5], fm[5];
+    laxf_part<AX, T>(qL, gamma, T(1), fp, flags);
+    laxf_part<AX, T>(qR, gamma, T(-1), fm, flags);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) F[v] = fp[v] + fm[v];
+}
+
+// physicalEulerFlux (Flux/SF_face.h:112-127) along e_AX.
+template <int AX, typename T>
+__device__ __forceinline__ void euler_flux(const T q[5], T gamma, T f[5], unsigned& flags) {
+    constexpr int N = AxisBasis<AX>::N;
+    const T rho = q[0];
+    const T inv = rcp<T>(rho);
+    const T p = state_pressure<T>(q, gamma, inv, flags);
+    const T vel[3] = {q[1] * inv, q[2] * inv, q[3] * inv};
+    const T un = vel[N - 1];
+    f[0] = rho * un;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) f[1 + k] = rho * vel[k] * un + (k == N - 1 ? p : T(0));
+    f[4] = (q[4] + p) * un;
+}
+
+// LaxWendroffFlux::flux (Flux/SF_lw.cpp:17-40): the physical flux of the
+// Richtmyer half-step state (qL + qR)/2 - lam/2 (F(qR) - F(qL)), lam = dt / h.
+template <int AX, typename T>
+__device__ __forceinline__ void laxw(const T qL[5], const T qR[5], T gamma, T lam, T F[5], unsigned& flags) {
+    T fL[5], fR[5], qh[5];
+    euler_flux<AX, T>(qL, gamma, fL, flags);
+    euler_flux<AX, T>(qR, gamma, fR, flags);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) qh[v] = T(0.5) * (qL[v] + qR[v]) - T(0.5) * lam * (fR[v] - fL[v]);
+    euler_flux<AX, T>(qh, gamma, F, flags);
+}
+
+// `lam` = dt / h along AX, used by the Lax-Wendroff flux only.
 template <int AX, int SCHEME, int FLUX, typename T>
 __device__ __forceinline__ void face_flux(const double (&st)[SchemeInfo<SCHEME>::NST][5], T gamma, T F[5],
-                                          unsigned& flags, unsigned& cut) {
+                                          unsigned& flags, unsigned& cut, T lam = T(0)) {
     constexpr int NST = SchemeInfo<SCHEME>::NST;
     constexpr int W = SchemeInfo<SCHEME>::W;
     constexpr int CL = NST / 2 - 1;
@@ -564,7 +674,10 @@ __device__ __forceinline__ void face_flux(const double (&st)[SchemeInfo<SCHEME>:
         qr[v] = DEV ? T(qbar64[v] + double(dr[v])) : dr[v];
     }
     if constexpr (FLUX == RUSANOV) rusanov<AX, T>(ql, qr, gamma, F, flags);
-    else roe<AX, T>(ql, qr, gamma, F, flags);
+    else if constexpr (FLUX == ROE) roe<AX, T>(ql, qr, gamma, F, flags);
+    else if constexpr (FLUX == STEGER) steger<AX, T>(ql, qr, gamma, F, flags);
+    else if constexpr (FLUX == LAXF) laxf<AX, T>(ql, qr, gamma, F, flags);
+    else laxw<AX, T>(ql, qr, gamma, lam, F, flags);
 #pragma unroll
     for (int v = 0; v < 5; ++v)
         if (!finite_(F[v])) flags |= FLAG_NONFINITE;

@@ -115,6 +115,7 @@ extern "C" int sfg_residual_noalloc(const sfg_grid_desc* grid, const sfg_numeric
     g.metric[2] = (hx * hy) * g.jac;
     for (int a = 0; a < 3; ++a) g.area[a] = 0.5 * (g.metric[a] / g.jac + g.metric[a] / g.jac);
     g.gamma = numerics->gamma;
+    for (int a = 0; a < 3; ++a) g.h[a] = grid->h[a];
     g.cfl = numerics->cfl;
     g.vs = nodes;
 

@@ -78,6 +78,18 @@ const RecipeInfo kRecipes[] = {
     {SFG_RECIPE_TENO5_ROE, "teno5Roe", TENO5, ROE},
     {SFG_RECIPE_WENO7_RUSANOV, "weno7Rusanov", WENO7, RUSANOV},
     {SFG_RECIPE_WENO7_ROE, "weno7Roe", WENO7, ROE},
+    {SFG_RECIPE_WENO3_STEGER, "weno3Steger", WENO3, STEGER},
+    {SFG_RECIPE_WENO3_LAXF, "weno3LaxFriedrichs", WENO3, LAXF},
+    {SFG_RECIPE_WENO3_LAXW, "weno3LaxWendroff", WENO3, LAXW},
+    {SFG_RECIPE_WENO5_STEGER, "weno5Steger", WENO5, STEGER},
+    {SFG_RECIPE_WENO5_LAXF, "weno5LaxFriedrichs", WENO5, LAXF},
+    {SFG_RECIPE_WENO5_LAXW, "weno5LaxWendroff", WENO5, LAXW},
+    {SFG_RECIPE_TENO5_STEGER, "teno5Steger", TENO5, STEGER},
+    {SFG_RECIPE_TENO5_LAXF, "teno5LaxFriedrichs", TENO5, LAXF},
+    {SFG_RECIPE_TENO5_LAXW, "teno5LaxWendroff", TENO5, LAXW},
+    {SFG_RECIPE_WENO7_STEGER, "weno7Steger", WENO7, STEGER},
+    {SFG_RECIPE_WENO7_LAXF, "weno7LaxFriedrichs", WENO7, LAXF},
+    {SFG_RECIPE_WENO7_LAXW, "weno7LaxWendroff", WENO7, LAXW},
 };
 
 const RecipeInfo* find_recipe(int id) {
@@ -139,6 +151,8 @@ int validate(const sfg_grid_desc* g, const sfg_numerics_desc* n, const RecipeInf
     if (n->time_recipe < 0 || n->time_recipe > 2) return fail(SFG_ERR_ARG, "unknown time recipe %d", n->time_recipe);
     if (n->precision != SFG_PREC_FP64 && n->precision != SFG_PREC_FP32_FLUX)
         return fail(SFG_ERR_ARG, "unknown precision mode %d", n->precision);
+    if (n->precision == SFG_PREC_FP32_FLUX && r->flux != RUSANOV && r->flux != ROE)
+        return fail(SFG_ERR_ARG, "%s: the FP32-flux mode implements Rusanov and Roe faces (use FP64)", r->name);
     if (!(n->gamma > 1.0) || !std::isfinite(n->gamma)) return fail(SFG_ERR_ARG, "gamma must be > 1");
     if (!(n->cfl > 0.0) || !std::isfinite(n->cfl)) return fail(SFG_ERR_ARG, "CFL must be finite and > 0");
     const int reach = r->scheme == WENO3 ? 2 : (r->scheme == WENO7 ? 4 : 3);
@@ -198,6 +212,7 @@ void make_view(sfg_solver_s* s) {
     g.metric[2] = (hx * hy) * g.jac;
     for (int a = 0; a < 3; ++a) g.area[a] = 0.5 * (g.metric[a] / g.jac + g.metric[a] / g.jac);
     g.gamma = s->num.gamma;
+    for (int a = 0; a < 3; ++a) g.h[a] = d.h[a];
     g.cfl = s->num.cfl;
     s->nodes = (long long)d.n[0] * d.n[1] * d.n[2];
     g.vs = (s->nodes + 31) / 32 * 32;

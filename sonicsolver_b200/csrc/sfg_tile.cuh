@@ -100,7 +100,7 @@ __device__ __forceinline__ void tile2d_body(const GridView& g, const StageView& 
             for (int s = 0; s < NST; ++s)
 #pragma unroll
                 for (int v = 0; v < 5; ++v) st[s][v] = base[v * SX * SY + s];
-            face_flux<0, SCHEME, FLUX, double>(st, gamma, Ft, flags, cut);
+            face_flux<0, SCHEME, FLUX, double>(st, gamma, Ft, flags, cut, FLUX == LAXW ? sv.clock->dt / g.h[0] : 0.0);
 #pragma unroll
             for (int v = 0; v < 5; ++v) fx[v * NFX + f] = Ft[v] * g.area[0];
         } else {
@@ -112,7 +112,7 @@ __device__ __forceinline__ void tile2d_body(const GridView& g, const StageView& 
             for (int s = 0; s < NST; ++s)
 #pragma unroll
                 for (int v = 0; v < 5; ++v) st[s][v] = base[v * SX * SY + s * SX];
-            face_flux<1, SCHEME, FLUX, double>(st, gamma, Ft, flags, cut);
+            face_flux<1, SCHEME, FLUX, double>(st, gamma, Ft, flags, cut, FLUX == LAXW ? sv.clock->dt / g.h[1] : 0.0);
 #pragma unroll
             for (int v = 0; v < 5; ++v) fy[v * NFY + k] = Ft[v] * g.area[1];
         }
@@ -247,7 +247,7 @@ __device__ __forceinline__ void tile1d_body(const GridView& g, const StageView& 
 #pragma unroll
             for (int v = 0; v < 5; ++v) st[s][v] = sq[v * SX + f + s];
         if constexpr (F32) face_flux_dev32<0, SCHEME, FLUX>(st, ref, T(g.gamma), Ft, flags, cut);
-        else face_flux<0, SCHEME, FLUX, double>(st, g.gamma, Ft, flags, cut);
+        else face_flux<0, SCHEME, FLUX, double>(st, g.gamma, Ft, flags, cut, FLUX == LAXW ? sv.clock->dt / g.h[0] : 0.0);
 #pragma unroll
         for (int v = 0; v < 5; ++v) fx[v * NF + f] = Ft[v] * T(g.area[0]);
         if (SCHEME == TENO5) cores += 10;

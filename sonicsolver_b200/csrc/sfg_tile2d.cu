@@ -47,22 +47,27 @@ static cudaError_t launch_tile(const GridView& g, const StageView& sv, cudaStrea
     return cudaGetLastError();
 }
 
+template <int FLUX, typename T, int TX, int TY>
+static cudaError_t launch_tile_s(int scheme, const GridView& g, const StageView& sv, cudaStream_t st) {
+    switch (scheme) {
+    case WENO5: return launch_tile<WENO5, FLUX, T, TX, TY>(g, sv, st);
+    case TENO5: return launch_tile<TENO5, FLUX, T, TX, TY>(g, sv, st);
+    case WENO3: return launch_tile<WENO3, FLUX, T, TX, TY>(g, sv, st);
+    case WENO7: return launch_tile<WENO7, FLUX, T, TX, TY>(g, sv, st);
+    }
+    return cudaErrorInvalidValue;
+}
+
+// Rusanov and Roe in both precisions; Steger-Warming, Lax-Friedrichs and
+// Lax-Wendroff faces in FP64 (the FP32 deviation form is Rusanov / Roe).
 template <typename T, int TX, int TY>
 static cudaError_t launch_tile_t(int scheme, int flux, const GridView& g, const StageView& sv, cudaStream_t st) {
-    if (flux == RUSANOV) {
-        switch (scheme) {
-        case WENO5: return launch_tile<WENO5, RUSANOV, T, TX, TY>(g, sv, st);
-        case TENO5: return launch_tile<TENO5, RUSANOV, T, TX, TY>(g, sv, st);
-        case WENO3: return launch_tile<WENO3, RUSANOV, T, TX, TY>(g, sv, st);
-        case WENO7: return launch_tile<WENO7, RUSANOV, T, TX, TY>(g, sv, st);
-        }
-    } else if (flux == ROE) {
-        switch (scheme) {
-        case WENO5: return launch_tile<WENO5, ROE, T, TX, TY>(g, sv, st);
-        case TENO5: return launch_tile<TENO5, ROE, T, TX, TY>(g, sv, st);
-        case WENO3: return launch_tile<WENO3, ROE, T, TX, TY>(g, sv, st);
-        case WENO7: return launch_tile<WENO7, ROE, T, TX, TY>(g, sv, st);
-        }
+    if (flux == RUSANOV) return launch_tile_s<RUSANOV, T, TX, TY>(scheme, g, sv, st);
+    if (flux == ROE) return launch_tile_s<ROE, T, TX, TY>(scheme, g, sv, st);
+    if constexpr (sizeof(T) == sizeof(double)) {
+        if (flux == STEGER) return launch_tile_s<STEGER, T, TX, TY>(scheme, g, sv, st);
+        if (flux == LAXF) return launch_tile_s<LAXF, T, TX, TY>(scheme, g, sv, st);
+        if (flux == LAXW) return launch_tile_s<LAXW, T, TX, TY>(scheme, g, sv, st);
     }
     return cudaErrorInvalidValue;
 }
@@ -95,22 +100,25 @@ static cudaError_t launch_tile1(const GridView& g, const StageView& sv, cudaStre
     return cudaGetLastError();
 }
 
+template <int FLUX, typename T>
+static cudaError_t launch_tile1_s(int scheme, const GridView& g, const StageView& sv, cudaStream_t st) {
+    switch (scheme) {
+    case WENO5: return launch_tile1<WENO5, FLUX, T>(g, sv, st);
+    case TENO5: return launch_tile1<TENO5, FLUX, T>(g, sv, st);
+    case WENO3: return launch_tile1<WENO3, FLUX, T>(g, sv, st);
+    case WENO7: return launch_tile1<WENO7, FLUX, T>(g, sv, st);
+    }
+    return cudaErrorInvalidValue;
+}
+
 template <typename T>
 static cudaError_t launch_tile1_t(int scheme, int flux, const GridView& g, const StageView& sv, cudaStream_t st) {
-    if (flux == RUSANOV) {
-        switch (scheme) {
-        case WENO5: return launch_tile1<WENO5, RUSANOV, T>(g, sv, st);
-        case TENO5: return launch_tile1<TENO5, RUSANOV, T>(g, sv, st);
-        case WENO3: return launch_tile1<WENO3, RUSANOV, T>(g, sv, st);
-        case WENO7: return launch_tile1<WENO7, RUSANOV, T>(g, sv, st);
-        }
-    } else if (flux == ROE) {
-        switch (scheme) {
-        case WENO5: return launch_tile1<WENO5, ROE, T>(g, sv, st);
-        case TENO5: return launch_tile1<TENO5, ROE, T>(g, sv, st);
-        case WENO3: return launch_tile1<WENO3, ROE, T>(g, sv, st);
-        case WENO7: return launch_tile1<WENO7, ROE, T>(g, sv, st);
-        }
+    if (flux == RUSANOV) return launch_tile1_s<RUSANOV, T>(scheme, g, sv, st);
+    if (flux == ROE) return launch_tile1_s<ROE, T>(scheme, g, sv, st);
+    if constexpr (sizeof(T) == sizeof(double)) {
+        if (flux == STEGER) return launch_tile1_s<STEGER, T>(scheme, g, sv, st);
+        if (flux == LAXF) return launch_tile1_s<LAXF, T>(scheme, g, sv, st);
+        if (flux == LAXW) return launch_tile1_s<LAXW, T>(scheme, g, sv, st);
     }
     return cudaErrorInvalidValue;
 }

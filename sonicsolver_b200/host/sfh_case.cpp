@@ -87,7 +87,7 @@ std::string convection_token(const Node& nu) {
     else if (f == "roe") flux = "Roe";
     else if (f == "laxfriedrichs" || f == "lf" || f == "lxf" || f == "laxf") flux = "LaxFriedrichs";
     else if (f == "laxwendroff" || f == "lw") flux = "LaxWendroff";
-    else if (f == "stegerwarming" || f == "sw") flux = "StegerWarming";
+    else if (f == "stegerwarming" || f == "sw" || f == "steger") flux = "Steger";  // TermRecipeId name
     else throw Unsupported("flux splitter '" + cv->at("flux").str() + "'");
     return scheme + flux;
 }

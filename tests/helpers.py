@@ -8,7 +8,8 @@ import pyoracle as po
 from sonicsolver_b200 import capi, cases
 
 SCHEME_OF = {"weno3": po.WENO3, "weno5": po.WENO5, "teno5": po.TENO5, "weno7": po.WENO7}
-FLUX_OF = {"Rusanov": po.RUSANOV, "Roe": po.ROE}
+FLUX_OF = {"Steger": po.STEGER, "Rusanov": po.RUSANOV, "LaxFriedrichs": po.LAXFRIEDRICHS, "Roe": po.ROE,
+           "LaxWendroff": po.LAXWENDROFF}
 TIME_OF = {"forwardEuler": po.EULER, "SSPRK3": po.SSPRK3, "classicalRK4": po.RK4}
 NG_OF = {"weno3": 2, "weno5": 3, "teno5": 3, "weno7": 4}
 

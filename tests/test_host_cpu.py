@@ -58,7 +58,7 @@ def test_describe_2d_frozen_and_periodic(runner, tmp_path):
     assert r2.returncode == 0 and "nodes=64,32,1" in r2.stdout and "bc=11/11/00" in r2.stdout
 
 
-@pytest.mark.parametrize("convection,needle", [("weno5StegerWarming", "no term provider"),
+@pytest.mark.parametrize("convection,needle", [("weno5Roeish", "no term provider"),
                                                ("upwind1Rusanov", "no term provider")])
 def test_unsupported_recipe(runner, tmp_path, convection, needle):
     d = write_case(str(tmp_path), "c", cells=(50, 1, 1), box_hi=(1.0, 0.1, 0.1), convection=convection)
@@ -88,10 +88,9 @@ def test_parse_error_names_file_and_line(runner, tmp_path):
 @pytest.mark.skipif(not os.path.isdir(REFERENCE_TESTS), reason="reference case directories not present")
 def test_reference_case_directories(runner):
     """Every case directory of the reference's test tree is read without a
-    parse error.  The Sod cases (no Left condition: frozen ghosts) resolve
-    and plan when their recipe has a GPU kernel (the WENO7 + Rusanov golden
-    case does; Steger-Warming has none yet); every other case is reported as
-    not supported by this provider, with its reason."""
+    parse error.  The three Sod cases (no Left condition: frozen ghosts;
+    TENO5 + Steger-Warming and WENO7 + Rusanov) resolve and plan; every other
+    case is reported as not supported by this provider, with its reason."""
     dirs = sorted(os.path.dirname(os.path.join(dp, f)) for dp, _, fs in os.walk(REFERENCE_TESTS)
                   for f in fs if f == "case.yaml")
     assert len(dirs) > 10
@@ -107,6 +106,5 @@ def test_reference_case_directories(runner):
                 assert "bc=20/00/00" in r.stdout
         else:
             assert "unsupported:" in r.stderr
-            if rel.startswith("Sod" + os.sep):
-                assert "no term provider" in r.stderr and "StegerWarming" in r.stderr
-    assert os.path.join("Sod", "sodCase_weno7_t0p2") in resolved
+    for case in ("sodCase", "sodCase_weno7", "sodCase_weno7_t0p2"):
+        assert os.path.join("Sod", case) in resolved

@@ -321,3 +321,119 @@ def _sod_perturbed(c):
     dts, tf = po.advance(spec, po.WENO7, po.RUSANOV, po.EULER, Q, c["t_end"], c["cfl"],
                          write_interval=c["write_interval"])
     return None, spec, Q, dts, tf
+
+
+# ------------------------------------- 4. Steger-Warming, Lax-Friedrichs, Lax-Wendroff
+
+NEW_FLUXES = {"Steger": po.STEGER, "LaxFriedrichs": po.LAXFRIEDRICHS, "LaxWendroff": po.LAXWENDROFF}
+
+
+def _flux(name, qL, qR, n, dt=1e-3, spacing=0.1):
+    out = np.zeros(5)
+    lib = po.oracle_lib()
+    if name == "Steger":
+        rc = lib.sfo_steger_flux(dp(qL), dp(qR), dp(n), GAMMA, dp(out))
+    elif name == "LaxFriedrichs":
+        rc = lib.sfo_lf_flux(dp(qL), dp(qR), dp(n), GAMMA, dp(out))
+    else:
+        rc = lib.sfo_lw_flux(dp(qL), dp(qR), dp(n), dt, spacing, GAMMA, dp(out))
+    assert rc == 0
+    return out
+
+
+@pytest.mark.parametrize("name", list(NEW_FLUXES))
+def test_new_fluxes_uniform_equal_physical_flux(oracle, name):
+    """Equal-state fluxes reduce to the physical flux (test_numericalFlux.cpp:185-199)."""
+    out = _flux(name, UNIFORM, UNIFORM, np.array([1.0, 0.0, 0.0]))
+    assert all(near(out[v], PHYS_UNIFORM[v]) for v in range(5))
+
+
+@pytest.mark.parametrize("name", ["Steger", "LaxFriedrichs"])
+def test_new_fluxes_reconstructed_on_constant_stencil(oracle, name):
+    """reconstructedConstantFlux with SW / LF (test_numericalFlux.cpp:201-224)."""
+    st = np.tile(UNIFORM, 6)
+    metrics = np.array([1.0, 0.0, 0.0, 1.0])
+    out = np.zeros(5)
+    assert po.oracle_lib().sfo_char_face_flux(6, dp(st), dp(metrics), po.WENO5, NEW_FLUXES[name], GAMMA,
+                                              dp(out)) == 0
+    assert all(near(out[v], PHYS_UNIFORM[v]) for v in range(5))
+
+
+def test_rusanov_steger_lf_distinct_on_riemann_data(oracle):
+    """Configured fluxes are observably distinct (test_numericalFlux.cpp:168-183)."""
+    left = perfect_gas_state(1.0, 2.0, 0.1, 0.0, 1.0)
+    right = perfect_gas_state(0.125, -0.5, 0.0, 0.0, 0.1)
+    n = np.array([1.0, 0.0, 0.0])
+    rus = np.zeros(5)
+    po.oracle_lib().sfo_rusanov_flux(dp(left), dp(right), dp(n), GAMMA, dp(rus))
+    sw, lf = _flux("Steger", left, right, n), _flux("LaxFriedrichs", left, right, n)
+    for a, b in ((rus, sw), (rus, lf), (sw, lf)):
+        assert not all(near(a[v], b[v], 1e-10) for v in range(5))
+
+
+def test_lax_wendroff_needs_positive_dt_and_spacing(oracle):
+    n = np.array([1.0, 0.0, 0.0])
+    out = np.zeros(5)
+    assert po.oracle_lib().sfo_lw_flux(dp(UNIFORM), dp(UNIFORM), dp(n), 0.0, 0.1, GAMMA, dp(out)) == po_err_arg()
+    assert po.oracle_lib().sfo_lw_flux(dp(UNIFORM), dp(UNIFORM), dp(n), 1e-3, 0.0, GAMMA, dp(out)) == po_err_arg()
+
+
+def po_err_arg():
+    return [k for k, v in po.ERRORS.items() if v == "argument"][0]
+
+
+@pytest.mark.skipif(not _ref_available(), reason="oracle/_ref not built (reference sources absent)")
+def test_new_fluxes_bitwise_equal_reference(oracle):
+    ref = po.ref_lib(False)
+    rng = np.random.default_rng(0)
+    for t in range(600):
+        a = perfect_gas_state(*rng.uniform([0.1, -3, -3, -3, 0.1], [5, 3, 3, 3, 5]))
+        b = perfect_gas_state(*rng.uniform([0.1, -3, -3, -3, 0.1], [5, 3, 3, 3, 5]))
+        n = np.zeros(3)
+        n[t % 3] = 1.0
+        for name in NEW_FLUXES:
+            want = np.zeros(5)
+            if name == "Steger":
+                ref.sfr_steger_flux(dp(a), dp(b), dp(n), GAMMA, dp(want))
+            elif name == "LaxFriedrichs":
+                ref.sfr_lf_flux(dp(a), dp(b), dp(n), GAMMA, dp(want))
+            else:
+                ref.sfr_lw_flux(dp(a), dp(b), dp(n), 1e-3, 0.1, GAMMA, dp(want))
+            np.testing.assert_array_equal(_flux(name, a, b, n), want)
+
+
+@pytest.mark.skipif(not _ref_available(), reason="oracle/_ref not built (reference sources absent)")
+@pytest.mark.parametrize("sname", ["weno3", "weno5", "teno5", "weno7"])
+@pytest.mark.parametrize("fname", list(NEW_FLUXES))
+def test_new_flux_operator_bitwise_equals_reference(oracle, sname, fname):
+    """divDispatch with Steger-Warming / Lax-Friedrichs / Lax-Wendroff faces
+    (the last with the step size set) against the restatement."""
+    po.set_step_dt(2.5e-3)
+    try:
+        for gi, (dim, n, h) in enumerate(GRIDS):
+            for bc in (po.BC_TRANSMISSIVE, po.BC_PERIODIC):
+                q = smooth_state(dim, n, seed=200 + gi, shock=True)
+                spec = po.GridSpec(dim=dim, n=n, ng=NG_OF[sname], h=h, bc_lo=(bc,) * 3, bc_hi=(bc,) * 3)
+                Q = spec.empty()
+                spec.interior(Q)[...] = q
+                po.fill_ghosts(spec, Q)
+                rc = po.RefCase(spec, SCHEMES[sname], NEW_FLUXES[fname])
+                np.testing.assert_array_equal(po.rhs(spec, SCHEMES[sname], NEW_FLUXES[fname], Q), rc.rhs(Q))
+    finally:
+        po.set_step_dt(0.0)
+
+
+@pytest.mark.skipif(not _ref_available(), reason="oracle/_ref not built (reference sources absent)")
+@pytest.mark.parametrize("fname", list(NEW_FLUXES))
+def test_new_flux_time_loop_equals_reference(oracle, fname):
+    spec = po.GridSpec(dim=1, n=(101, 1, 1), ng=3, h=(0.01, 1.0, 1.0))
+    Q = spec.empty()
+    x = np.arange(101) * 0.01
+    I = spec.interior(Q)
+    I[..., 0] = np.where(x < 0.5, 1.0, 0.125)
+    I[..., 4] = np.where(x < 0.5, 1.0, 0.1) / 0.4
+    Q2 = Q.copy()
+    d1, t1 = po.advance(spec, po.WENO5, NEW_FLUXES[fname], po.SSPRK3, Q, 0.05, 0.4)
+    d2, t2 = po.RefCase(spec, po.WENO5, NEW_FLUXES[fname]).advance(po.SSPRK3, Q2, 0.05, 0.4)
+    np.testing.assert_array_equal(d1, d2)
+    np.testing.assert_array_equal(Q, Q2)
