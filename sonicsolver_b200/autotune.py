@@ -3,8 +3,9 @@
 Picks the stage-operator kernel variant by timing the candidates on the
 device, per (GPU model, dimension, size class, recipe, precision):
 
-  * single grids: variant 0 (one sweep launch per axis), 1 (30 x 16 tiles or
-    511-node 1-D tiles), 2 (22 x 22 tiles, 2-D only), each timed with
+  * single grids: variant 0 (one sweep launch per axis), 1 (30 x 16 tiles,
+    511-node 1-D tiles, or 3-D 16 x 15 columns marching in z), 2 (22 x 22
+    tiles, 2-D only), each timed with
     sfg_time_sweeps (CUDA events on the solver's stream, stage 0 repeated);
   * batches: 2-D work-item tile 30 x 16 or 22 x 22, timed over a few batch
     steps of a sample of the batch's grids.
@@ -68,7 +69,7 @@ def size_class(nodes: int) -> int:
 
 
 def candidates(dim: int):
-    return {1: [0, 1], 2: [0, 1, 2], 3: [0]}[dim]
+    return {1: [0, 1], 2: [0, 1, 2], 3: [0, 1]}[dim]
 
 
 def tune_solver(solver: "capi.Solver", recipe: str, precision: int, repeats: int = 5, use_cache: bool = True) -> dict:

@@ -35,6 +35,7 @@ cudaError_t launch_totals(const GridView& g, const double* q, double* out, doubl
 cudaError_t launch_tile2d(int variant, int scheme, int flux, int prec64, const GridView& g, const StageView& sv,
                           cudaStream_t st);
 cudaError_t launch_tile1d(int scheme, int flux, int prec64, const GridView& g, const StageView& sv, cudaStream_t st);
+cudaError_t launch_tile3d(int scheme, int flux, int prec64, const GridView& g, const StageView& sv, cudaStream_t st);
 cudaError_t launch_teno_flips(const GridView& g, const double* q, unsigned long long* out, cudaStream_t st);
 }  // namespace sfg
 
@@ -274,6 +275,12 @@ int enqueue_stage(sfg_solver_s* s, int stage, bool residual_only, bool require_a
         sv.mode = MODE_FINAL | (residual_only ? MODE_RESIDUAL : 0) | cfl_bit;
         CUDA_TRY(launch_tile2d(s->variant, s->recipe->scheme, s->recipe->flux, s->num.precision == SFG_PREC_FP64,
                                s->gv, sv, s->stream));
+        return SFG_OK;
+    }
+    if (dim == 3 && s->variant > 0) {
+        sv.mode = MODE_FINAL | (residual_only ? MODE_RESIDUAL : 0) | cfl_bit;
+        CUDA_TRY(launch_tile3d(s->recipe->scheme, s->recipe->flux, s->num.precision == SFG_PREC_FP64, s->gv, sv,
+                               s->stream));
         return SFG_OK;
     }
     if (dim == 1 && s->variant > 0) {
@@ -911,7 +918,7 @@ int sfg_time_sweeps(sfg_solver s, int stage, double dt, int repeats, float* ms_p
     double acc[3] = {0, 0, 0};
     CUDA_TRY(launch_set_dt(s->clock, dt, s->stream));
     StageView sv = stage_view(s, stage, false, false);
-    if (dim <= 2 && s->variant > 0) {  // one fused launch per stage
+    if (s->variant > 0) {  // one fused launch per stage (1-D, 2-D and 3-D tiles)
         for (int r = 0; r < repeats; ++r) {
             CUDA_TRY(cudaEventRecord(ev[0], s->stream));
             int rc = enqueue_stage(s, stage, false, false);
@@ -970,7 +977,7 @@ int sfg_teno_flip_rate(sfg_solver s, uint64_t* decisions, uint64_t* flips) {
 int sfg_set_kernel_variant(sfg_solver s, int variant) {
     if (!s) return fail(SFG_ERR_ARG, "null solver");
     if (variant < 0 || variant > 2) return fail(SFG_ERR_ARG, "unknown kernel variant %d", variant);
-    if (variant > 0 && s->grid.dim == 3) return fail(SFG_ERR_ARG, "tile variants need a 1-D or 2-D grid");
+    if (variant > 1 && s->grid.dim == 3) return fail(SFG_ERR_ARG, "3-D grids have variants 0 (sweeps) and 1 (tiles)");
     if (variant == 2 && s->grid.dim != 2) return fail(SFG_ERR_ARG, "the 22 x 22 tile needs a 2-D grid");
     if (variant != s->variant && s->graph) {
         cudaGraphExecDestroy(s->graph);

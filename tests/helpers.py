@@ -43,8 +43,9 @@ def from_oracle(spec: po.GridSpec, Q: np.ndarray) -> np.ndarray:
     return np.ascontiguousarray(spec.interior(Q))
 
 
-def smooth_state(dim, n, seed=0, amp=0.2, gamma=1.4, shock=False):
-    """A seeded smooth (optionally with a contact/shock jump) positive state."""
+def smooth_state(dim, n, seed=0, amp=0.2, gamma=1.4, shock=False, noise=0.01):
+    """A seeded smooth (optionally with a contact/shock jump) positive state,
+    with `noise` relative random noise on the density."""
     rng = np.random.default_rng(seed)
     nz, ny, nx = n[2], n[1], n[0]
     z, y, x = np.meshgrid(np.linspace(0, 1, nz, endpoint=False), np.linspace(0, 1, ny, endpoint=False),
@@ -62,5 +63,5 @@ def smooth_state(dim, n, seed=0, amp=0.2, gamma=1.4, shock=False):
         jump = (x + 0.37 * y + 0.21 * z) > 0.55
         rho = np.where(jump, 0.5 * rho, rho)
         p = np.where(jump, 0.4 * p, p)
-    rho = rho * (1 + 0.01 * rng.random(rho.shape))
+    rho = rho * (1 + noise * rng.random(rho.shape))
     return cases.conserved(rho, u, v, w, p, gamma)
