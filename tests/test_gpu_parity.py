@@ -83,8 +83,10 @@ def test_variants_by_dimension():
         s.variant = 2
     s3, _, _ = _pair(3, (14, 12, 11), (0.05, 0.06, 0.07), capi.BC_PERIODIC, "weno5Rusanov")
     assert s3.variant == 0
+    s3.variant = 1                  # 3-D z-marching tiles
+    assert s3.variant == 1
     with pytest.raises(capi.SolverError):
-        s3.variant = 1
+        s3.variant = 2
 
 
 @pytest.mark.parametrize("variant", [0, 1])
