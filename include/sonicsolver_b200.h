@@ -103,7 +103,7 @@ enum {
     SFG_BC_PERIODIC = 1,      /* ghosts wrap; every node is advanced (the
                                  reference declares PatchBoundaryKind::Periodic,
                                  SF_meshInterface.h:14, but never implements it) */
-    SFG_BC_FROZEN = 2         /* a patch with no boundary condition: the
+    SFG_BC_FROZEN = 2,        /* a patch with no boundary condition: the
                                  boundary node is advanced and the ghosts keep
                                  the values they were initialised with, the
                                  boundary node's value at upload (or the
@@ -111,6 +111,24 @@ enum {
                                  (SF_applicator.h:162-187 with no BC for the
                                  set; SF_mesh.cpp:544).  Single-grid solvers
                                  only. */
+    SFG_BC_LAW = 3            /* physical boundary laws per field (density,
+                                 velocity, pressure with the energy rebuilt
+                                 from pressure), set by sfg_set_boundary_law;
+                                 default: zeroGradient for all three.  The
+                                 boundary node is written by the laws and not
+                                 advanced; every ghost layer is derived from
+                                 it (Boundary::Applicator::apply,
+                                 SF_applicator.h:51-83).  Single-grid solvers
+                                 only; needs >= 3 nodes on the axis. */
+};
+/* Law of one field at a SFG_BC_LAW end (BCType of SF_valueTypes.h:28). */
+enum {
+    SFG_LAW_ZERO_GRADIENT = 0,  /* SF_zeroGradient.cpp:88-131               */
+    SFG_LAW_FIXED_VALUE = 1,    /* SF_fixedValue.cpp:110-160                */
+    SFG_LAW_SYMMETRY = 2        /* SF_symmetry.cpp:78-136 (velocity: normal
+                                   component 0 on the boundary, mirrored in
+                                   the ghosts; density, pressure:
+                                   zeroGradient)                            */
 };
 /* Host array layouts for upload / download. */
 enum {
@@ -128,6 +146,19 @@ typedef struct {
     int bc_lo[3];     /* SFG_BC_* per axis, low end                           */
     int bc_hi[3];     /* SFG_BC_* per axis, high end                          */
 } sfg_grid_desc;
+
+/* The three laws of one SFG_BC_LAW end (the density / velocity / pressure
+ * BCSetting of one patch, FDM::BoundaryConfig); values are read by the
+ * fixedValue laws. */
+typedef struct {
+    int rho;                  /* SFG_LAW_* of density                        */
+    int velocity;             /* SFG_LAW_* of velocity                       */
+    int pressure;             /* SFG_LAW_* of pressure                       */
+    int reserved;             /* 0                                           */
+    double rho_value;         /* kg/m3                                       */
+    double velocity_value[3]; /* m/s                                         */
+    double pressure_value;    /* Pa                                          */
+} sfg_boundary_law;
 
 typedef struct {
     int recipe;       /* SFG_RECIPE_*                                        */
@@ -169,6 +200,18 @@ int sfg_destroy(sfg_solver s);
 int sfg_ghost_layers(sfg_solver s, int* ng);
 /* Number of doubles of a host array in `layout`. */
 int sfg_state_size(sfg_solver s, int layout, size_t* count);
+/* Laws of a SFG_BC_LAW end (axis 0..dim-1, end 0 = low, 1 = high).  They
+ * act from the next step on, where the reference applies its boundary
+ * conditions: at the start of every step (FlowStepPrepare, in sfg_step and
+ * sfg_advance), before every stage's RHS and after a step's last stage
+ * (FlowStepCommit).  A host plan that drives sfg_stage itself calls
+ * sfg_apply_boundary for FlowStepPrepare.  Boundary nodes on two or more
+ * law faces (box edges and corners) are read by no stencil of a solved node
+ * and are not maintained. */
+int sfg_set_boundary_law(sfg_solver s, int axis, int end, const sfg_boundary_law* law);
+/* Applies the laws of every SFG_BC_LAW end to the current state once (the
+ * reference's Boundary::Applicator::apply on the Field). */
+int sfg_apply_boundary(sfg_solver s);
 /* Host <-> device copies of the conserved state (pageable or pinned host
  * memory; synchronous with respect to the solver's stream). Upload resets the
  * time to `time`. */

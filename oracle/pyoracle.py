@@ -24,15 +24,44 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 WENO3, WENO5, TENO5, WENO7 = 0, 1, 2, 3
 STEGER, RUSANOV, LAXFRIEDRICHS, ROE, LAXWENDROFF = 0, 1, 2, 3, 4
 EULER, SSPRK3, RK4 = 0, 1, 2
-BC_TRANSMISSIVE, BC_PERIODIC, BC_FROZEN = 0, 1, 2
+BC_TRANSMISSIVE, BC_PERIODIC, BC_FROZEN, BC_LAW = 0, 1, 2, 3
+LAW_ZERO_GRADIENT, LAW_FIXED_VALUE, LAW_SYMMETRY = 0, 1, 2
 ERRORS = {0: "ok", 1: "non-finite", 2: "invalid state", 3: "TENO all-cutoff", 4: "argument",
           5: "Roe sound speed"}
+
+
+class Law(ctypes.Structure):
+    """``sfo_law``: density / velocity / pressure law of one LAW end."""
+    _fields_ = [("rho", ctypes.c_int), ("U", ctypes.c_int), ("p", ctypes.c_int), ("pad", ctypes.c_int),
+                ("rho_value", ctypes.c_double), ("U_value", ctypes.c_double * 3),
+                ("p_value", ctypes.c_double)]
 
 
 class Grid(ctypes.Structure):
     _fields_ = [("dim", ctypes.c_int), ("n", ctypes.c_int * 3), ("ng", ctypes.c_int),
                 ("h", ctypes.c_double * 3), ("bc_lo", ctypes.c_int * 3),
-                ("bc_hi", ctypes.c_int * 3), ("gamma", ctypes.c_double)]
+                ("bc_hi", ctypes.c_int * 3), ("gamma", ctypes.c_double),
+                ("law", ctypes.POINTER(Law))]
+
+
+@dataclass
+class LawSpec:
+    """Python view of ``sfo_law`` (values are used by fixedValue laws)."""
+    rho: int = LAW_ZERO_GRADIENT
+    U: int = LAW_ZERO_GRADIENT
+    p: int = LAW_ZERO_GRADIENT
+    rho_value: float = 0.0
+    U_value: tuple = (0.0, 0.0, 0.0)
+    p_value: float = 0.0
+
+    def c(self) -> Law:
+        law = Law()
+        law.rho, law.U, law.p = int(self.rho), int(self.U), int(self.p)
+        law.rho_value = float(self.rho_value)
+        for d in range(3):
+            law.U_value[d] = float(self.U_value[d])
+        law.p_value = float(self.p_value)
+        return law
 
 
 class Counters(ctypes.Structure):
@@ -50,6 +79,7 @@ class GridSpec:
     bc_lo: tuple = (0, 0, 0)
     bc_hi: tuple = (0, 0, 0)
     gamma: float = 1.4
+    laws: dict = field(default_factory=dict)   # (axis, end) -> LawSpec for BC_LAW ends
 
     def c(self) -> Grid:
         g = Grid()
@@ -61,6 +91,12 @@ class GridSpec:
             g.bc_hi[d] = int(self.bc_hi[d])
         g.ng = self.ng
         g.gamma = self.gamma
+        if self.laws:
+            arr = (Law * 6)()
+            for (axis, end), law in self.laws.items():
+                arr[2 * axis + end] = law.c()
+            g._laws = arr               # keeps the array alive with the struct
+            g.law = ctypes.cast(arr, ctypes.POINTER(Law))
         return g
 
     @property
@@ -132,6 +168,7 @@ def _sig(lib, prefix):
                                     ctypes.POINTER(ctypes.c_int), _DP, C]
     else:
         lib.sfr_rhs.argtypes = [G, ctypes.c_int, ctypes.c_int, _DP, _DP]
+        lib.sfr_fill_laws.argtypes = [G, _DP]
         lib.sfr_dt.argtypes = [G, _DP, ctypes.c_double, _DP]
         for nm in ("sfr_weno3_core", "sfr_weno5_core", "sfr_teno5_core", "sfr_weno7_core"):
             getattr(lib, nm).argtypes = [_DP]
@@ -192,6 +229,14 @@ class OracleError(RuntimeError):
 
 def fill_ghosts(spec: GridSpec, Q: np.ndarray) -> None:
     _check(oracle_lib().sfo_fill_ghosts(ctypes.byref(spec.c()), _ptr(Q)), "fill_ghosts")
+
+
+def ref_fill_laws(spec: GridSpec, Q: np.ndarray) -> None:
+    """The reference's own boundary laws of the LAW ends applied to Q."""
+    lib = ref_lib()
+    if lib is None:
+        raise RuntimeError("oracle/_ref/libsfref.so missing: run `make -C oracle`")
+    _check(lib.sfr_fill_laws(ctypes.byref(spec.c()), _ptr(Q)), "ref fill_laws")
 
 
 def set_step_dt(dt: float) -> None:

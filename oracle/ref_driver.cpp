@@ -14,8 +14,11 @@
 //     Math::spatialResidual (methods/numerics/structured/SF_residualAssembly.h:34-41);
 //   - the CFL step: Numerics::RusanovEOS::deltaT (Flux/SF_rusanovEOS.cpp:110-147).
 // What is restated here (the reference's versions need the full solver
-// runtime): the ghost fill laws and the Euler / Shu-Osher SSPRK3 / RK4 stage
-// arithmetic of solver/algorithm/time/SF_explicit.cpp:193-238,282-285.
+// runtime): the ghost fill laws inside the time loop and the Euler /
+// Shu-Osher SSPRK3 / RK4 stage arithmetic of
+// solver/algorithm/time/SF_explicit.cpp:193-238,282-285.  The physical
+// boundary laws themselves also run as reference code (sfr_fill_laws:
+// Boundary::update, updateEnergyFromPressure) to pin the restatement.
 #include "SF_field.h"
 #include "SF_div.h"
 #include "core/flux/SF_flux.h"
@@ -28,6 +31,8 @@
 #include "methods/numerics/structured/SF_residualAssembly.h"
 #include "models/physics/fluidStateModel/SF_singleFluidStateModel.h"
 #include "models/physics/EOS/SF_perfectGasEOS.h"
+#include "solver/boundary/SF_boundary.h"
+#include "solver/boundary/SF_thermodynamicClosure.h"
 
 #include "sf_oracle.h"
 
@@ -88,14 +93,16 @@ void setup_case(RefCase& rc, const sfo_grid* g) {
                 rc.field.Y(i, j, k) = (j - g->ng) * hy;
                 rc.field.Z(i, j, k) = (k - g->ng) * hz;
             }
-    // Solver-boundary sets: the transmissive (zeroGradient) ends, exactly the
-    // nodes that Boundary::Applicator marks (SF_applicator.h:162-187).
+    // Solver-boundary sets: the transmissive (zeroGradient) and LAW ends,
+    // exactly the nodes that Boundary::Applicator marks
+    // (SF_applicator.h:162-187).  Points are listed with the last axis
+    // outermost, the order the restatement visits them in.
     std::map<std::string, std::vector<int>> sets;
     const int ng = g->ng;
     for (int d = 0; d < g->dim; ++d) {
         for (int end = 0; end < 2; ++end) {
             const int kind = end ? g->bc_hi[d] : g->bc_lo[d];
-            if (kind != SFO_BC_TRANSMISSIVE) continue;
+            if (kind != SFO_BC_TRANSMISSIVE && kind != SFO_BC_LAW) continue;
             std::string name = std::string("bc") + char('0' + d) + (end ? "hi" : "lo");
             auto& ids = sets[name];
             const int fixed = end ? g->n[d] - 1 + ng : ng;
@@ -280,6 +287,8 @@ int sfr_case_step(void* h, int time_id, double* Q, double dt) {
     auto* pc = static_cast<PersistentCase*>(h);
     const int ns = time_id == SFO_EULER ? 1 : (time_id == SFO_SSPRK3 ? 3 : (time_id == SFO_RK4 ? 4 : 0));
     if (!ns) return SFO_ERR_ARG;
+    int prep = sfo_fill_ghosts(&pc->rc.g, Q);  // FlowStepPrepare
+    if (prep) return prep;
     for (int s = 0; s < ns; ++s) {
         int err = sfo_stage_fn(&pc->rc.g, case_rhs, pc, time_id, Q, dt, s, pc->work.data());
         if (err) return err;
@@ -293,6 +302,53 @@ int sfr_case_advance(void* h, int time_id, double* Q, double t_start, double t_e
     auto* pc = static_cast<PersistentCase*>(h);
     return sfo_advance_fn(&pc->rc.g, case_rhs, case_dt, pc, time_id, Q, t_start, t_end, cfl, max_dt,
                           write_interval, max_steps, dt_out, steps_done, t_final);
+}
+
+// The reference's own physical boundary laws on Q (compact layout): the
+// density, velocity and pressure settings of every LAW end, applied as
+// Boundary::Applicator::apply does (SF_applicator.h:51-83) between the cache
+// invalidations of the conservative RHS (SF_conservativeRHS.cpp:91-95).
+// Settings are listed x low, x high, y low, ... (the restatement's order).
+int sfr_fill_laws(const sfo_grid* g, double* Q) {
+    try {
+        RefCase rc;
+        setup_case(rc, g);
+        load_state(rc, Q);
+        std::vector<SF::BCSetting<double>> density, pressure;
+        std::vector<SF::BCSetting<SF::Vector3>> velocity;
+        auto type_of = [](int law) {
+            return law == SFO_LAW_FIXED_VALUE ? SF::FIXED_VALUE
+                   : law == SFO_LAW_SYMMETRY  ? SF::SYMMETRY
+                                              : SF::ZERO_GRADIENT;
+        };
+        for (int d = 0; d < g->dim; ++d)
+            for (int end = 0; end < 2; ++end) {
+                if ((end ? g->bc_hi[d] : g->bc_lo[d]) != SFO_BC_LAW) continue;
+                const sfo_law& law = g->law[2 * d + end];
+                const std::string name = std::string("bc") + char('0' + d) + (end ? "hi" : "lo");
+                density.push_back({name, type_of(law.rho), law.rho_value});
+                velocity.push_back({name, type_of(law.U), SF::Vector3(law.U_value[0], law.U_value[1], law.U_value[2])});
+                pressure.push_back({name, type_of(law.p), law.p_value});
+            }
+        rc.field.invalidateThermodynamicCache();
+        SF::Boundary::update<double>(rc.field, density, SF::RHO);
+        SF::Boundary::update<SF::Vector3>(rc.field, velocity, SF::RU);
+        SF::Boundary::updateEnergyFromPressure(rc.field, pressure);
+        rc.field.invalidateThermodynamicCache();
+        // reference Field -> compact layout (every compact storage position)
+        const int m0 = storage_extent(g, 0), m1 = storage_extent(g, 1), m2 = storage_extent(g, 2);
+        int off[3];
+        for (int d = 0; d < 3; ++d) off[d] = d < g->dim ? 0 : g->ng;
+        for (int k = 0; k < m2; ++k)
+            for (int j = 0; j < m1; ++j)
+                for (int i = 0; i < m0; ++i) {
+                    double* q = Q + 5 * (((long long)k * m1 + j) * m0 + i);
+                    for (int v = 0; v < 5; ++v) q[v] = rc.field(i + off[0], j + off[1], k + off[2], v);
+                }
+        return SFO_OK;
+    } catch (const std::exception&) {
+        return SFO_ERR_STATE;
+    }
 }
 
 // Scalar cores and fluxes straight from the reference (known-answer tests).

@@ -569,6 +569,8 @@ static int grid_ok(const sfo_grid* g) {
         if (g->n[d] < 1) return 0;
         if (d >= g->dim && g->n[d] != 1) return 0;
         if (!(g->h[d] > 0.0)) return 0;
+        if (d < g->dim && (g->bc_lo[d] == SFO_BC_LAW || g->bc_hi[d] == SFO_BC_LAW) && (!g->law || g->n[d] < 3))
+            return 0;
     }
     return g->gamma > 1.0;
 }
@@ -576,14 +578,17 @@ static int grid_ok(const sfo_grid* g) {
 static int node_solved(const sfo_grid* g, const layout* L, const int* idx) {
     for (int d = 0; d < g->dim; ++d) {
         int node = idx[d] - L->lo[d];
-        if (node == 0 && g->bc_lo[d] == SFO_BC_TRANSMISSIVE) return 0;
-        if (node == g->n[d] - 1 && g->bc_hi[d] == SFO_BC_TRANSMISSIVE) return 0;
+        if (node == 0 && (g->bc_lo[d] == SFO_BC_TRANSMISSIVE || g->bc_lo[d] == SFO_BC_LAW)) return 0;
+        if (node == g->n[d] - 1 && (g->bc_hi[d] == SFO_BC_TRANSMISSIVE || g->bc_hi[d] == SFO_BC_LAW)) return 0;
     }
     return 1;
 }
 
+static int fill_laws(const sfo_grid* g, const layout* L, double* Q);
+
 /* Boundary laws (SF_applicator.h:51-83 -> SF_zeroGradient.cpp:88-105 for
- * transmissive; wrap for periodic; nothing for frozen). */
+ * transmissive; wrap for periodic; nothing for frozen; fill_laws for the
+ * per-field laws of LAW ends). */
 int sfo_fill_ghosts(const sfo_grid* g, double* Q) {
     if (!grid_ok(g)) return SFO_ERR_ARG;
     layout L;
@@ -617,7 +622,232 @@ int sfo_fill_ghosts(const sfo_grid* g, double* Q) {
 #undef AT
             }
     }
+    return fill_laws(g, &L, Q);
+}
+
+/* ---- Per-field boundary laws of LAW ends -----------------------------------
+ * Boundary::Applicator::apply (SF_applicator.h:51-83) runs the density laws of
+ * every patch, then the velocity laws, then the pressure laws, each over the
+ * points of the patch's set.  Every ghost layer of a point is derived from the
+ * boundary node itself (forBoundaryGhostsAlongAxis, SF_boundary.h:95-121).
+ *
+ * Densities and pressures of some points are read through the Field's
+ * thermodynamic state cache (Field::thermodynamicState, SF_field.cpp:133-151;
+ * ThermodynamicStateCache, SF_thermodynamicStateCache.h): a direct-mapped
+ * table of min(storage points, 4096) entries indexed by the Field cell
+ * index.  It is emptied right before the laws run (SF_conservativeRHS.cpp:93)
+ * and the laws' own writes do not refresh it, so a state that the velocity
+ * fixedValue law caches before it writes the momentum is the state the
+ * pressure law later reads for the ghosts.  tcache reproduces that table.
+ * The Field of the reference carries ghosts on every axis; ref_cell maps a
+ * compact storage position to its cell index there. */
+
+#define SFO_GAS_CONSTANT 287.05  /* makeSingleFluidPerfectGas, fluidStateModel/SF_factory.h:21-33 */
+#define SFO_CACHE_MAX 4096       /* Field::setStateModel, SF_field.cpp:117-118 */
+
+typedef struct { long long cell; double rho, p; } tcache_entry;
+typedef struct {
+    tcache_entry e[SFO_CACHE_MAX];
+    long long cap, mx, my;
+    int off[3];
+    double gamma;
+} tcache;
+
+static long long ref_cell(const tcache* c, const int* at) {
+    return ((long long)(at[2] + c->off[2]) * c->my + (at[1] + c->off[1])) * c->mx + (at[0] + c->off[0]);
+}
+
+/* Field::thermodynamicState: SingleFluidStateModel::close
+ * (SF_singleFluidStateModel.cpp:49-73) with PerfectGasEOS::fromDensityEnergy
+ * and its checks (SF_perfectGasEOS.h:26-33,80-86), through the cache. */
+static int cached_state(tcache* c, const int* at, const double* q, double* rho, double* p) {
+    const long long cell = ref_cell(c, at);
+    tcache_entry* e = &c->e[cell % c->cap];
+    if (e->cell == cell) {
+        *rho = e->rho;
+        *p = e->p;
+        return SFO_OK;
+    }
+    if (!isfinite(q[0]) || q[0] <= 0.0) return SFO_ERR_STATE;       /* requireEnergyInput */
+    for (int d = 1; d < 4; ++d)
+        if (!isfinite(q[d])) return SFO_ERR_NONFINITE;
+    const double r = q[0];
+    double u[3];
+    for (int d = 0; d < 3; ++d) u[d] = q[1 + d] / r;
+    const double kinetic = 0.5 * r * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+    const double eint = q[4] - kinetic;
+    const double em = eint / r;
+    const double thermal = em - 0.0;
+    const double pp = (c->gamma - 1.0) * r * thermal;
+    const double T = thermal * (c->gamma - 1.0) / SFO_GAS_CONSTANT;
+    const double cs = sqrt(c->gamma * pp / r);
+    if (!isfinite(em) || !isfinite(pp) || pp <= 0.0 || !isfinite(T) || T <= 0.0 || !isfinite(cs) || cs <= 0.0)
+        return SFO_ERR_STATE;
+    e->cell = cell;
+    e->rho = r;
+    e->p = pp;
+    *rho = r;
+    *p = pp;
     return SFO_OK;
+}
+
+/* setEnergyFromPressure (SF_thermodynamicClosure.cpp:166-184) through
+ * SingleFluidStateModel::totalEnergyFromPressure / totalEnergyFromThermo
+ * (SF_singleFluidStateModel.cpp:75-102) and PerfectGasEOS::fromDensityPressure
+ * (SF_perfectGasEOS.h:43-53). */
+static int energy_from_pressure(double* q, double gamma, double p) {
+    if (!isfinite(p) || p <= 0.0) return SFO_ERR_STATE;
+    if (!isfinite(q[0]) || q[0] <= 0.0) return SFO_ERR_STATE;
+    for (int d = 1; d < 4; ++d)
+        if (!isfinite(q[d])) return SFO_ERR_NONFINITE;
+    const double thermal = p / ((gamma - 1.0) * q[0]);
+    const double e = 0.0 + thermal;
+    const double T = p / (q[0] * SFO_GAS_CONSTANT);
+    const double cs = sqrt(gamma * p / q[0]);
+    if (!isfinite(e) || !isfinite(T) || T <= 0.0 || !isfinite(cs) || cs <= 0.0) return SFO_ERR_STATE;
+    const double inv = 1.0 / q[0];
+    const double kinetic = 0.5 * inv * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+    q[4] = q[0] * e + kinetic;
+    return SFO_OK;
+}
+
+static int positive_density(const double* q) { return isfinite(q[0]) && q[0] > 0.0; }
+
+/* One family of laws (0 density, 1 velocity, 2 pressure) at one boundary
+ * point.  b, s: storage positions of the boundary node and of its inner
+ * sample (nearestInsideSample, SF_zeroGradient.cpp:35-52); gp: the ng ghost
+ * positions in the reference's visiting order. */
+static int law_point(tcache* c, const sfo_law* law, int family, int axis, double gamma, double* Q,
+                     const layout* L, const int* b, const int* s, int (*gp)[3], int ng) {
+#define PTR(at) (Q + (at)[0] * L->stride[0] + (at)[1] * L->stride[1] + (at)[2] * L->stride[2])
+    double* qb = PTR(b);
+    const double* qs = PTR(s);
+    double rr, pr;
+    int err;
+    if (family == 0) {
+        /* FixedValue::applyScalar (SF_fixedValue.cpp:110-127): ghost = 2 v - q_b;
+         * ZeroGradient / Symmetry::applyScalar (SF_zeroGradient.cpp:88-105) */
+        if (law->rho == SFO_LAW_FIXED_VALUE) {
+            qb[0] = law->rho_value;
+            for (int k = 0; k < ng; ++k) PTR(gp[k])[0] = 2.0 * law->rho_value - qb[0];
+        } else {
+            qb[0] = qs[0];
+            for (int k = 0; k < ng; ++k) PTR(gp[k])[0] = qb[0];
+        }
+        return SFO_OK;
+    }
+    if (family == 1) {
+        if (law->U == SFO_LAW_FIXED_VALUE) {
+            /* FixedValue::applyVector3 (SF_fixedValue.cpp:129-160) */
+            err = cached_state(c, b, qb, &rr, &pr);
+            if (err) return err;
+            for (int d = 0; d < 3; ++d) qb[1 + d] = rr * law->U_value[d];
+            for (int k = 0; k < ng; ++k) {
+                double* qg = PTR(gp[k]);
+                double rg, u[3];
+                err = cached_state(c, b, qb, &rr, &pr);
+                if (err) return err;
+                for (int d = 0; d < 3; ++d) u[d] = qb[1 + d] / rr;
+                err = cached_state(c, gp[k], qg, &rg, &pr);
+                if (err) return err;
+                for (int d = 0; d < 3; ++d) qg[1 + d] = rg * (2.0 * law->U_value[d] - u[d]);
+            }
+        } else if (law->U == SFO_LAW_SYMMETRY) {
+            /* Symmetry::applyVector3 (SF_symmetry.cpp:82-136): tangential
+             * velocity copied from the inner sample, normal component 0;
+             * ghosts mirror the normal component */
+            if (!positive_density(qb) || !positive_density(qs)) return SFO_ERR_STATE;
+            const double scale = qb[0] / qs[0];
+            double v[3];
+            for (int d = 0; d < 3; ++d) v[d] = qs[1 + d] * scale;
+            v[axis] = 0.0;
+            for (int d = 0; d < 3; ++d) qb[1 + d] = v[d];
+            for (int k = 0; k < ng; ++k) {
+                double* qg = PTR(gp[k]);
+                double m[3];
+                for (int d = 0; d < 3; ++d) m[d] = qb[1 + d];
+                m[axis] = -m[axis];
+                if (!positive_density(qg) || !positive_density(qb)) return SFO_ERR_STATE;
+                const double sg = qg[0] / qb[0];
+                for (int d = 0; d < 3; ++d) qg[1 + d] = m[d] * sg;
+            }
+        } else {
+            /* ZeroGradient::applyVector3 (SF_zeroGradient.cpp:107-131) */
+            for (int d = 1; d < 4; ++d) qb[d] = qs[d];
+            for (int k = 0; k < ng; ++k)
+                for (int d = 1; d < 4; ++d) PTR(gp[k])[d] = qb[d];
+        }
+        return SFO_OK;
+    }
+    /* updateEnergyFromPressure (SF_thermodynamicClosure.cpp:219-285) */
+    if (law->p == SFO_LAW_FIXED_VALUE) {
+        err = energy_from_pressure(qb, gamma, law->p_value);
+        if (err) return err;
+        for (int k = 0; k < ng; ++k) {
+            err = cached_state(c, b, qb, &rr, &pr);
+            if (err) return err;
+            err = energy_from_pressure(PTR(gp[k]), gamma, 2.0 * law->p_value - pr);
+            if (err) return err;
+        }
+    } else {
+        double rs, ps;
+        err = cached_state(c, s, qs, &rs, &ps);
+        if (err) return err;
+        err = energy_from_pressure(qb, gamma, ps);
+        if (err) return err;
+        for (int k = 0; k < ng; ++k) {
+            err = cached_state(c, b, qb, &rr, &pr);
+            if (err) return err;
+            err = energy_from_pressure(PTR(gp[k]), gamma, pr);
+            if (err) return err;
+        }
+    }
+    return SFO_OK;
+#undef PTR
+}
+
+/* The laws of every LAW end: density for all ends, then velocity, then
+ * pressure; ends in the order x low, x high, y low, ...; the points of an
+ * end's face with the last axis outermost. */
+static int fill_laws(const sfo_grid* g, const layout* L, double* Q) {
+    int any = 0;
+    for (int d = 0; d < g->dim; ++d) any |= g->bc_lo[d] == SFO_BC_LAW || g->bc_hi[d] == SFO_BC_LAW;
+    if (!any) return SFO_OK;
+    tcache* c = (tcache*)malloc(sizeof(tcache));
+    if (!c) return SFO_ERR_ARG;
+    const int ng = g->ng;
+    c->mx = g->n[0] + 2 * ng;
+    c->my = g->n[1] + 2 * ng;
+    const long long total = c->mx * c->my * (long long)(g->n[2] + 2 * ng);
+    c->cap = total < SFO_CACHE_MAX ? total : SFO_CACHE_MAX;
+    for (int d = 0; d < 3; ++d) c->off[d] = d < g->dim ? 0 : ng;
+    c->gamma = g->gamma;
+    for (long long i = 0; i < c->cap; ++i) c->e[i].cell = -1;
+    int err = SFO_OK;
+    for (int family = 0; family < 3 && !err; ++family)
+        for (int axis = 0; axis < g->dim && !err; ++axis)
+            for (int end = 0; end < 2 && !err; ++end) {
+                if ((end ? g->bc_hi[axis] : g->bc_lo[axis]) != SFO_BC_LAW) continue;
+                const sfo_law* law = &g->law[2 * axis + end];
+                const int n = g->n[axis];
+                const int bnode = end ? n - 1 : 0, snode = end ? n - 2 : 1;
+                int node[3];
+                for (node[2] = 0; node[2] < g->n[2] && !err; ++node[2])
+                    for (node[1] = 0; node[1] < g->n[1] && !err; ++node[1])
+                        for (node[0] = 0; node[0] < g->n[0] && !err; ++node[0]) {
+                            if (node[axis] != bnode) continue;
+                            int b[3], s[3], gp[4][3];
+                            for (int d = 0; d < 3; ++d) b[d] = s[d] = L->lo[d] + node[d];
+                            s[axis] = L->lo[axis] + snode;
+                            for (int k = 0; k < ng; ++k) {
+                                for (int d = 0; d < 3; ++d) gp[k][d] = b[d];
+                                gp[k][axis] = end ? b[axis] + 1 + k : k;
+                            }
+                            err = law_point(c, law, family, axis, g->gamma, Q, L, b, s, gp, ng);
+                        }
+            }
+    free(c);
+    return err;
 }
 
 static int stencil_points(int scheme) {
@@ -835,8 +1065,10 @@ int sfo_step(const sfo_grid* g, int scheme, int flux, int time_id, double* Q, do
              sfo_counters* counters) {
     const int ns = stage_count(time_id);
     if (!ns) return SFO_ERR_ARG;
+    int err = sfo_fill_ghosts(g, Q);   /* FlowStepPrepare (SF_flowOperations.cpp:471-485) */
+    if (err) return err;
     for (int s = 0; s < ns; ++s) {
-        int err = sfo_stage(g, scheme, flux, time_id, Q, dt, s, work, counters);
+        err = sfo_stage(g, scheme, flux, time_id, Q, dt, s, work, counters);
         if (err) return err;
     }
     return SFO_OK;
@@ -863,7 +1095,6 @@ int sfo_advance_fn(const sfo_grid* g, sfo_rhs_fn rhs, sfo_dt_fn dtf, void* ctx, 
     double next_out = write_interval > 0.0 ? t_start + write_interval : INFINITY;
     int step = 0, err = SFO_OK;
     const double eps = 2.220446049250313e-16;
-    err = sfo_fill_ghosts(g, Q);
     while (!err) {
         const double remaining = t_end - time;
         double scale = fabs(time) > fabs(t_end) ? fabs(time) : fabs(t_end);
@@ -872,6 +1103,10 @@ int sfo_advance_fn(const sfo_grid* g, sfo_rhs_fn rhs, sfo_dt_fn dtf, void* ctx, 
         if (step >= max_steps) break;
         double limit = remaining;
         if (write_interval > 0.0 && next_out - time < limit) limit = next_out - time;
+        /* every step opens with FlowStepPrepare (SF_flowOperations.cpp:471-485;
+         * the explicit fragment, SF_builtinProviders.cpp:63-81) */
+        err = sfo_fill_ghosts(g, Q);
+        if (err) break;
         double dt;
         err = dtf(ctx, Q, cfl, &dt);
         if (err) break;

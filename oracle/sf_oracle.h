@@ -35,8 +35,26 @@ enum { SFO_EULER = 0, SFO_SSPRK3 = 1, SFO_RK4 = 2 };
  *   PERIODIC:     ghosts wrap; every node is advanced (no reference code).
  *   FROZEN:       no boundary law: the boundary node is advanced and the
  *                 ghosts keep the values they were given (SF_applicator.h:162-187
- *                 with no BC configured for the set). */
-enum { SFO_BC_TRANSMISSIVE = 0, SFO_BC_PERIODIC = 1, SFO_BC_FROZEN = 2 };
+ *                 with no BC configured for the set).
+ *   LAW:          the reference's physical boundary laws per field
+ *                 (Boundary::Applicator::apply, SF_applicator.h:51-83): a
+ *                 density law, a velocity law and a pressure law (energy
+ *                 rebuilt from pressure), each fixedValue, zeroGradient or
+ *                 symmetry.  The boundary node is written by the laws and not
+ *                 advanced; every ghost layer is derived from it. */
+enum { SFO_BC_TRANSMISSIVE = 0, SFO_BC_PERIODIC = 1, SFO_BC_FROZEN = 2, SFO_BC_LAW = 3 };
+
+/* Field laws of one LAW end (FDM::BoundaryConfig density / velocity /
+ * pressure settings of one patch; BCSetting types FIXED_VALUE,
+ * ZERO_GRADIENT, SYMMETRY). */
+enum { SFO_LAW_ZERO_GRADIENT = 0, SFO_LAW_FIXED_VALUE = 1, SFO_LAW_SYMMETRY = 2 };
+typedef struct {
+    int rho, U, p;        /* SFO_LAW_* of density, velocity, pressure */
+    int pad;
+    double rho_value;     /* fixedValue density */
+    double U_value[3];    /* fixedValue velocity */
+    double p_value;       /* fixedValue pressure */
+} sfo_law;
 
 /* Error codes (the reference exits the process on these conditions). */
 enum {
@@ -56,6 +74,7 @@ typedef struct {
     int bc_lo[3];
     int bc_hi[3];
     double gamma;
+    const sfo_law* law;  /* law[2 * axis + end] of SFO_BC_LAW ends (end 0 = low) */
 } sfo_grid;
 
 /* Counters reported by the oracle (TENO cut-off decisions etc.). */

@@ -26,7 +26,8 @@ RECIPES = {f"{sch}{flx}": 5 * i + j
            for j, flx in enumerate(("Steger", "Rusanov", "LaxFriedrichs", "Roe", "LaxWendroff"))}
 TIME_RECIPES = {"forwardEuler": 0, "SSPRK3": 1, "classicalRK4": 2}
 PREC_FP64, PREC_FP32_FLUX = 0, 1
-BC_TRANSMISSIVE, BC_PERIODIC, BC_FROZEN = 0, 1, 2
+BC_TRANSMISSIVE, BC_PERIODIC, BC_FROZEN, BC_LAW = 0, 1, 2, 3
+LAW_ZERO_GRADIENT, LAW_FIXED_VALUE, LAW_SYMMETRY = 0, 1, 2
 LAYOUT_NODES, LAYOUT_FIELD = 0, 1
 
 # The C-ABI symbols declared by include/sonicsolver_b200.h (checked by tests).
@@ -42,6 +43,13 @@ EXPORTS = (
 class GridDesc(ctypes.Structure):
     _fields_ = [("dim", ctypes.c_int), ("n", ctypes.c_int * 3), ("h", ctypes.c_double * 3),
                 ("bc_lo", ctypes.c_int * 3), ("bc_hi", ctypes.c_int * 3)]
+
+
+class BoundaryLaw(ctypes.Structure):
+    """``sfg_boundary_law``: density / velocity / pressure law of one law end."""
+    _fields_ = [("rho", ctypes.c_int), ("velocity", ctypes.c_int), ("pressure", ctypes.c_int),
+                ("reserved", ctypes.c_int), ("rho_value", ctypes.c_double),
+                ("velocity_value", ctypes.c_double * 3), ("pressure_value", ctypes.c_double)]
 
 
 class NumericsDesc(ctypes.Structure):
@@ -91,6 +99,8 @@ def lib():
         L.sfg_create.argtypes = [ctypes.POINTER(GridDesc), ctypes.POINTER(NumericsDesc), _VP, ctypes.POINTER(_VP)]
         L.sfg_destroy.argtypes = [_VP]
         L.sfg_ghost_layers.argtypes = [_VP, ctypes.POINTER(ctypes.c_int)]
+        L.sfg_set_boundary_law.argtypes = [_VP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(BoundaryLaw)]
+        L.sfg_apply_boundary.argtypes = [_VP]
         L.sfg_state_size.argtypes = [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]
         L.sfg_upload.argtypes = [_VP, _DP, ctypes.c_int, ctypes.c_double]
         L.sfg_download.argtypes = [_VP, _DP, ctypes.c_int]
@@ -199,6 +209,22 @@ class Solver:
 
     def node_shape(self):
         return (self.n[2], self.n[1], self.n[0], 5)
+
+    def set_boundary_law(self, axis, end, rho=LAW_ZERO_GRADIENT, velocity=LAW_ZERO_GRADIENT,
+                         pressure=LAW_ZERO_GRADIENT, rho_value=0.0, velocity_value=(0.0, 0.0, 0.0),
+                         pressure_value=0.0):
+        """Laws of a BC_LAW end (axis, end 0 = low / 1 = high)."""
+        law = BoundaryLaw()
+        law.rho, law.velocity, law.pressure = int(rho), int(velocity), int(pressure)
+        law.rho_value = float(rho_value)
+        for d in range(3):
+            law.velocity_value[d] = float(velocity_value[d])
+        law.pressure_value = float(pressure_value)
+        check(lib().sfg_set_boundary_law(self._h, axis, end, ctypes.byref(law)))
+
+    def apply_boundary(self):
+        """Apply the laws of every law end to the current state once."""
+        check(lib().sfg_apply_boundary(self._h))
 
     def upload(self, q: np.ndarray, time: float = 0.0, layout=LAYOUT_NODES):
         check(lib().sfg_upload(self._h, _dptr(q), layout, time))

@@ -60,6 +60,24 @@ struct GridView {
     double h[3];       // node spacing (the Lax-Wendroff face spacing)
 };
 
+// Physical boundary laws of the law ends of one grid (SFG_BC_LAW; the
+// kernels see such an end as BC_FROZEN: one extra node holding the ghost
+// value, the boundary node outside the solved range).
+constexpr int LAW_ZERO_GRADIENT = 0, LAW_FIXED_VALUE = 1, LAW_SYMMETRY = 2;
+struct LawView {
+    int count;              // law ends
+    int axis[6], end[6];
+    int rho[6], U[6], p[6]; // LAW_* per field
+    double rho_value[6], U_value[6][3], p_value[6];
+    long long start[7];     // prefix sums of the face points per law end
+    // per face point: which state of its boundary node the pressure law reads
+    // (LAW_STATE_*), as the reference's state cache hands it out
+    const unsigned char* codes;
+};
+constexpr int LAW_STATE_FRESH = 0;   // the boundary node's new state
+constexpr int LAW_STATE_PRIMED = 1;  // new density, momentum and energy before the application
+constexpr int LAW_STATE_HALF = 2;    // new density and momentum, energy before the application
+
 // Stage arithmetic of one launch (Time::Explicit, SF_explicit.cpp:193-238,282-285).
 enum TimeId { T_EULER = 0, T_SSPRK3 = 1, T_RK4 = 2 };
 

@@ -17,6 +17,7 @@
 #include <cstring>
 #include <limits>
 #include <string>
+#include <unordered_set>
 #include <vector>
 
 namespace sfg {
@@ -36,6 +37,8 @@ cudaError_t launch_tile2d(int variant, int scheme, int flux, int prec64, const G
                           cudaStream_t st);
 cudaError_t launch_tile1d(int scheme, int flux, int prec64, const GridView& g, const StageView& sv, cudaStream_t st);
 cudaError_t launch_tile3d(int scheme, int flux, int prec64, const GridView& g, const StageView& sv, cudaStream_t st);
+cudaError_t launch_law_fill(const GridView& g, const LawView& lv, const double* old, double* q, const Clock* clock,
+                            int require_active, unsigned* flags, cudaStream_t st);
 cudaError_t launch_teno_flips(const GridView& g, const double* q, unsigned long long* out, cudaStream_t st);
 }  // namespace sfg
 
@@ -117,8 +120,12 @@ struct sfg_solver_s {
     // Device grid: `grid` plus one extra node at every frozen end, which
     // holds the frozen ghost value and is never advanced.
     sfg_grid_desc ig{};
-    int off_lo[3] = {0, 0, 0};  // 1 where the low end is frozen
-    bool frozen = false;
+    int off_lo[3] = {0, 0, 0};  // 1 where the low end is frozen or a law end
+    bool frozen = false;        // the device grid has extra nodes (frozen or law ends)
+    bool has_laws = false;      // some end is SFG_BC_LAW
+    sfg_boundary_law laws[6] = {};  // [2 * axis + end]
+    LawView lv{};
+    unsigned char* law_codes = nullptr;  // device: LAW_STATE_* per law face point
     long long pub_nodes = 0;    // nodes of `grid`
     sfg_numerics_desc num{};
     const RecipeInfo* recipe = nullptr;
@@ -166,36 +173,173 @@ int validate(const sfg_grid_desc* g, const sfg_numerics_desc* n, const RecipeInf
         const bool plo = g->bc_lo[d] == SFG_BC_PERIODIC, phi = g->bc_hi[d] == SFG_BC_PERIODIC;
         if (plo != phi) return fail(SFG_ERR_ARG, "axis %d: periodic must be set on both ends", d);
         for (int b : {g->bc_lo[d], g->bc_hi[d]})
-            if (b != SFG_BC_TRANSMISSIVE && b != SFG_BC_PERIODIC && b != SFG_BC_FROZEN)
+            if (b != SFG_BC_TRANSMISSIVE && b != SFG_BC_PERIODIC && b != SFG_BC_FROZEN && b != SFG_BC_LAW)
                 return fail(SFG_ERR_ARG, "axis %d: unknown boundary kind %d", d, b);
+        if ((g->bc_lo[d] == SFG_BC_LAW || g->bc_hi[d] == SFG_BC_LAW) && g->n[d] < 3)
+            return fail(SFG_ERR_ARG, "axis %d: a law end needs >= 3 nodes", d);
         if (plo && g->n[d] < reach + 1) return fail(SFG_ERR_ARG, "periodic axis %d needs >= %d nodes", d, reach + 1);
-        const int extra = (g->bc_lo[d] == SFG_BC_FROZEN) + (g->bc_hi[d] == SFG_BC_FROZEN);
+        const int extra = (g->bc_lo[d] == SFG_BC_FROZEN || g->bc_lo[d] == SFG_BC_LAW) +
+                          (g->bc_hi[d] == SFG_BC_FROZEN || g->bc_hi[d] == SFG_BC_LAW);
         if (!plo && g->n[d] + extra < 3) return fail(SFG_ERR_ARG, "axis %d needs >= %d nodes", d, 3 - extra);
     }
     *recipe = r;
     return SFG_OK;
 }
 
+// The reference reads the boundary node's state for a pressure law through
+// the Field's thermodynamic state cache (Field::thermodynamicState,
+// SF_field.cpp:133-151; ThermodynamicStateCache: min(storage points, 4096)
+// direct-mapped entries keyed by the Field cell index, emptied before each
+// application of the laws).  Which state a point's pressure law gets depends
+// only on the grid and the laws, so this replays the sequence of cache
+// queries of one application -- velocity laws of every law end, then
+// pressure laws, face points with the last axis outermost, corners included
+// (SF_fixedValue.cpp:129-160, SF_thermodynamicClosure.cpp:219-285) -- and
+// records LAW_STATE_* for each face point the kernel updates.
+void simulate_law_cache(const sfg_solver_s* s, std::vector<unsigned char>& codes) {
+    const LawView& lv = s->lv;
+    const sfg_grid_desc& G = s->grid;
+    const int ng = s->ng;
+    const long long mx = G.n[0] + 2LL * ng, my = G.n[1] + 2LL * ng, mz = G.n[2] + 2LL * ng;
+    const long long cap = std::min<long long>(mx * my * mz, 4096);
+    std::vector<long long> slot_cell((size_t)cap, -1);
+    std::vector<unsigned char> slot_kind((size_t)cap, 0);
+    codes.assign((size_t)lv.start[lv.count], (unsigned char)LAW_STATE_FRESH);
+    auto cell = [&](const int (&p)[3]) {
+        return ((long long)(p[2] + ng) * my + (p[1] + ng)) * mx + (p[0] + ng);
+    };
+    auto query = [&](long long c, unsigned char kind_if_miss) {
+        const size_t sl = (size_t)(c % cap);
+        if (slot_cell[sl] == c) return slot_kind[sl];
+        slot_cell[sl] = c;
+        slot_kind[sl] = kind_if_miss;
+        return kind_if_miss;
+    };
+    int pub_lo[3], pub_hi[3];
+    for (int d = 0; d < 3; ++d) {
+        pub_lo[d] = s->gv.lo[d] - s->off_lo[d];
+        pub_hi[d] = s->gv.hi[d] - s->off_lo[d];
+    }
+    // Boundary nodes whose energy this application has not written yet: an
+    // edge point's inner sample can be another end's boundary node, and the
+    // state cached for it then (new density and momentum, old energy) is the
+    // one that end's pressure law finds.
+    std::unordered_set<long long> pending;
+    for (int e = 0; e < lv.count; ++e) {
+        const int a = lv.axis[e], bnode = lv.end[e] ? G.n[a] - 1 : 0;
+        int p[3];
+        for (p[2] = 0; p[2] < G.n[2]; ++p[2])
+            for (p[1] = 0; p[1] < G.n[1]; ++p[1])
+                for (p[0] = 0; p[0] < G.n[0]; ++p[0])
+                    if (p[a] == bnode) pending.insert(cell(p));
+    }
+    for (int family = 1; family <= 2; ++family)   // density laws query nothing
+        for (int e = 0; e < lv.count; ++e) {
+            const int a = lv.axis[e], hi = lv.end[e], n = G.n[a];
+            if (family == 1 && lv.U[e] != LAW_FIXED_VALUE) continue;
+            int p[3];
+            for (p[2] = 0; p[2] < G.n[2]; ++p[2])
+                for (p[1] = 0; p[1] < G.n[1]; ++p[1])
+                    for (p[0] = 0; p[0] < G.n[0]; ++p[0]) {
+                        if (p[a] != (hi ? n - 1 : 0)) continue;
+                        const long long cb = cell(p);
+                        int q[3] = {p[0], p[1], p[2]};
+                        if (family == 1) {
+                            query(cb, LAW_STATE_PRIMED);              // setMomentumFromVelocity(b)
+                            for (int k = 0; k < ng; ++k) {
+                                query(cb, LAW_STATE_HALF);            // primitiveVelocity(b)
+                                q[a] = hi ? n + k : k - ng;
+                                query(cell(q), 3);                    // setMomentumFromVelocity(ghost)
+                            }
+                            continue;
+                        }
+                        if (lv.p[e] != LAW_FIXED_VALUE) {
+                            q[a] = hi ? n - 2 : 1;
+                            const long long cs = cell(q);               // pressureAt(inner sample)
+                            query(cs, pending.count(cs) ? LAW_STATE_HALF : LAW_STATE_FRESH);
+                        }
+                        pending.erase(cb);                              // setEnergyFromPressure(b)
+                        unsigned char kind = query(cb, LAW_STATE_FRESH);  // pressureAt(b), every layer alike
+                        bool face = true;
+                        long long at = 0, mult = 1;
+                        for (int d = 0; d < 3; ++d) {
+                            if (d == a) continue;
+                            face &= p[d] >= pub_lo[d] && p[d] < pub_hi[d];
+                            at += (long long)(p[d] - pub_lo[d]) * mult;
+                            mult *= pub_hi[d] - pub_lo[d];
+                        }
+                        if (face) codes[(size_t)(lv.start[e] + at)] = kind > LAW_STATE_HALF ? LAW_STATE_FRESH : kind;
+                    }
+        }
+}
+
+// Law ends in the order x low, x high, y low, ...; face points over the
+// solved range of the other axes.
+void build_law_view(sfg_solver_s* s) {
+    LawView& lv = s->lv;
+    lv = LawView{};
+    const GridView& g = s->gv;
+    for (int a = 0; a < s->grid.dim; ++a)
+        for (int end = 0; end < 2; ++end) {
+            if ((end ? s->grid.bc_hi[a] : s->grid.bc_lo[a]) != SFG_BC_LAW) continue;
+            const int e = lv.count++;
+            const sfg_boundary_law& law = s->laws[2 * a + end];
+            lv.axis[e] = a;
+            lv.end[e] = end;
+            lv.rho[e] = law.rho;
+            lv.U[e] = law.velocity;
+            lv.p[e] = law.pressure;
+            lv.rho_value[e] = law.rho_value;
+            for (int d = 0; d < 3; ++d) lv.U_value[e][d] = law.velocity_value[d];
+            lv.p_value[e] = law.pressure_value;
+            long long pts = 1;
+            for (int d = 0; d < 3; ++d)
+                if (d != a) pts *= g.hi[d] - g.lo[d];
+            lv.start[e + 1] = lv.start[e] + pts;
+        }
+    lv.codes = s->law_codes;
+}
+
+// Device copy of the cache replay for the current laws (the number of face
+// points never changes, so the buffer is allocated once).
+int upload_law_codes(sfg_solver_s* s) {
+    if (!s->lv.count) return SFG_OK;
+    std::vector<unsigned char> codes;
+    simulate_law_cache(s, codes);
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    if (!s->law_codes && cudaMalloc((void**)&s->law_codes, codes.size()) != cudaSuccess) {
+        s->law_codes = nullptr;
+        return fail(SFG_ERR_NOMEM, "device allocation of the law table failed");
+    }
+    CUDA_TRY(cudaMemcpy(s->law_codes, codes.data(), codes.size(), cudaMemcpyHostToDevice));
+    s->lv.codes = s->law_codes;
+    return SFG_OK;
+}
+
 void make_view(sfg_solver_s* s) {
-    // device grid: one extra node per frozen end
+    // device grid: one extra node per frozen or law end
     s->ig = s->grid;
     s->frozen = false;
+    s->has_laws = false;
     s->pub_nodes = (long long)s->grid.n[0] * s->grid.n[1] * s->grid.n[2];
+    auto extra_end = [](int b) { return b == SFG_BC_FROZEN || b == SFG_BC_LAW; };
     for (int a = 0; a < s->grid.dim; ++a) {
-        s->off_lo[a] = s->grid.bc_lo[a] == SFG_BC_FROZEN ? 1 : 0;
-        s->ig.n[a] += s->off_lo[a] + (s->grid.bc_hi[a] == SFG_BC_FROZEN ? 1 : 0);
+        s->off_lo[a] = extra_end(s->grid.bc_lo[a]) ? 1 : 0;
+        s->ig.n[a] += s->off_lo[a] + (extra_end(s->grid.bc_hi[a]) ? 1 : 0);
         s->frozen |= s->ig.n[a] != s->grid.n[a];
+        s->has_laws |= s->grid.bc_lo[a] == SFG_BC_LAW || s->grid.bc_hi[a] == SFG_BC_LAW;
     }
     GridView& g = s->gv;
     const sfg_grid_desc& d = s->ig;
     g.dim = d.dim;
     for (int a = 0; a < 3; ++a) {
         g.n[a] = d.n[a];
-        g.bc_lo[a] = a < d.dim ? d.bc_lo[a] : BC_TRANSMISSIVE;
-        g.bc_hi[a] = a < d.dim ? d.bc_hi[a] : BC_TRANSMISSIVE;
-        if (a < d.dim) {  // transmissive boundary nodes and frozen extra nodes are not advanced
-            g.lo[a] = d.bc_lo[a] == SFG_BC_PERIODIC ? 0 : 1;
-            g.hi[a] = d.bc_hi[a] == SFG_BC_PERIODIC ? d.n[a] : d.n[a] - 1;
+        // a law end reads like a frozen one: ghosts clamp to its extra node
+        g.bc_lo[a] = a < d.dim ? (d.bc_lo[a] == SFG_BC_LAW ? BC_FROZEN : d.bc_lo[a]) : BC_TRANSMISSIVE;
+        g.bc_hi[a] = a < d.dim ? (d.bc_hi[a] == SFG_BC_LAW ? BC_FROZEN : d.bc_hi[a]) : BC_TRANSMISSIVE;
+        if (a < d.dim) {  // transmissive and law boundary nodes and extra nodes are not advanced
+            g.lo[a] = d.bc_lo[a] == SFG_BC_PERIODIC ? 0 : (d.bc_lo[a] == SFG_BC_LAW ? 2 : 1);
+            g.hi[a] = d.bc_hi[a] == SFG_BC_PERIODIC ? d.n[a] : (d.bc_hi[a] == SFG_BC_LAW ? d.n[a] - 2 : d.n[a] - 1);
         } else {
             g.lo[a] = 0;
             g.hi[a] = 1;
@@ -217,6 +361,7 @@ void make_view(sfg_solver_s* s) {
     g.cfl = s->num.cfl;
     s->nodes = (long long)d.n[0] * d.n[1] * d.n[2];
     g.vs = (s->nodes + 31) / 32 * 32;
+    build_law_view(s);
 }
 
 StageView stage_view(sfg_solver_s* s, int stage, bool residual_only, bool require_active) {
@@ -270,6 +415,13 @@ StageView stage_view(sfg_solver_s* s, int stage, bool residual_only, bool requir
 int enqueue_stage(sfg_solver_s* s, int stage, bool residual_only, bool require_active, bool cfl = false) {
     StageView sv = stage_view(s, stage, residual_only, require_active);
     const int dim = s->grid.dim;
+    if (s->has_laws) {
+        // prepareBoundaryState before the RHS: the laws on the stage's input;
+        // the previous application's values sit in the previous stage's input
+        const double* old = stage == 0 || residual_only ? s->qn : stage_view(s, stage - 1, false, false).qs;
+        CUDA_TRY(launch_law_fill(s->gv, s->lv, old, const_cast<double*>(sv.qs), s->clock, require_active ? 1 : 0,
+                                 s->flags, s->stream));
+    }
     const int cfl_bit = cfl && !residual_only ? MODE_CFL : 0;
     if (dim == 2 && s->variant > 0) {
         sv.mode = MODE_FINAL | (residual_only ? MODE_RESIDUAL : 0) | cfl_bit;
@@ -298,6 +450,16 @@ int enqueue_stage(sfg_solver_s* s, int stage, bool residual_only, bool require_a
     return SFG_OK;
 }
 
+// FlowStepCommit's boundary application on the last stage's output (before
+// the Euler copy-back, which then carries it into qn).
+int enqueue_commit_laws(sfg_solver_s* s, bool require_active) {
+    if (!s->has_laws) return SFG_OK;
+    const StageView last = stage_view(s, stage_count(s->num.time_recipe) - 1, false, false);
+    CUDA_TRY(launch_law_fill(s->gv, s->lv, last.qs, last.qout, s->clock, require_active ? 1 : 0, s->flags,
+                             s->stream));
+    return SFG_OK;
+}
+
 // Euler writes to qa; the committed state lives in qn.
 int enqueue_post_step(sfg_solver_s* s) {
     if (s->num.time_recipe == T_EULER)
@@ -313,11 +475,17 @@ int enqueue_post_step(sfg_solver_s* s) {
 int enqueue_cfl_step(sfg_solver_s* s, bool require_active) {
     CUDA_TRY(launch_dt(s->gv, s->qn, s->clock, s->flags, 1, s->stream));
     CUDA_TRY(launch_finalize_dt(s->clock, s->stream));
+    // FlowStepPrepare opens the step (before its dt in the reference; the dt
+    // reads solved nodes only, which the laws never write)
+    if (s->has_laws)
+        CUDA_TRY(launch_law_fill(s->gv, s->lv, s->qn, s->qn, s->clock, require_active ? 1 : 0, s->flags, s->stream));
     const int ns = stage_count(s->num.time_recipe);
     for (int st = 0; st < ns; ++st) {
         int rc = enqueue_stage(s, st, false, require_active, st == ns - 1);
         if (rc) return rc;
     }
+    int rc = enqueue_commit_laws(s, require_active);
+    if (rc) return rc;
     if (s->num.time_recipe == T_EULER) {
         // guarded copy: only when the step ran (graph-safe: copy unconditionally
         // is wrong once the run has stopped), so Euler keeps its own kernel path
@@ -371,14 +539,14 @@ long long field_extent(const sfg_solver_s* s, int a) { return s->grid.n[a] + 2LL
 int map_host(int i, int n, int bl, int bh) {
     if (bl == SFG_BC_PERIODIC) {
         while (i < 0) i += n;
-    } else if (bl == SFG_BC_FROZEN) {
+    } else if (bl == SFG_BC_FROZEN || bl == SFG_BC_LAW) {
         if (i < 0) i = 0;
     } else if (i < 1) {
         i = n > 1 ? 1 : 0;
     }
     if (bh == SFG_BC_PERIODIC) {
         while (i >= n) i -= n;
-    } else if (bh == SFG_BC_FROZEN) {
+    } else if (bh == SFG_BC_FROZEN || bh == SFG_BC_LAW) {
         if (i > n - 1) i = n - 1;
     } else if (i > n - 2) {
         i = n > 1 ? n - 2 : 0;
@@ -504,6 +672,8 @@ int sfg_create(const sfg_grid_desc* grid, const sfg_numerics_desc* numerics, voi
     s->host_clock->max_dt = s->num.max_dt;
     rc = push_clock(s);
     if (rc) return cleanup(rc);
+    rc = upload_law_codes(s);
+    if (rc) return cleanup(rc);
     *out = s;
     return SFG_OK;
 }
@@ -515,12 +685,45 @@ int sfg_destroy(sfg_solver s) {
     for (double* p : {s->qn, s->qa, s->qb, s->r, s->k, s->staging, s->totals, s->dt_log})
         if (p) cudaFree(p);
     if (s->clock) cudaFree(s->clock);
+    if (s->law_codes) cudaFree(s->law_codes);
     if (s->flags) cudaFree(s->flags);
     if (s->counters) cudaFree(s->counters);
     if (s->host_clock) cudaFreeHost(s->host_clock);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return SFG_OK;
+}
+
+int sfg_set_boundary_law(sfg_solver s, int axis, int end, const sfg_boundary_law* law) {
+    if (!s || !law) return fail(SFG_ERR_ARG, "null argument");
+    if (axis < 0 || axis >= s->grid.dim || end < 0 || end > 1) return fail(SFG_ERR_ARG, "bad axis %d / end %d", axis, end);
+    if ((end ? s->grid.bc_hi[axis] : s->grid.bc_lo[axis]) != SFG_BC_LAW)
+        return fail(SFG_ERR_ARG, "axis %d end %d is not a SFG_BC_LAW end", axis, end);
+    for (int k : {law->rho, law->velocity, law->pressure})
+        if (k != SFG_LAW_ZERO_GRADIENT && k != SFG_LAW_FIXED_VALUE && k != SFG_LAW_SYMMETRY)
+            return fail(SFG_ERR_ARG, "unknown field law %d", k);
+    auto finite = [](double v) { return std::isfinite(v); };
+    if (!finite(law->rho_value) || !finite(law->pressure_value) || !finite(law->velocity_value[0]) ||
+        !finite(law->velocity_value[1]) || !finite(law->velocity_value[2]))
+        return fail(SFG_ERR_ARG, "law values must be finite");
+    if (law->rho == SFG_LAW_FIXED_VALUE && !(law->rho_value > 0.0))
+        return fail(SFG_ERR_ARG, "fixedValue density must be > 0");
+    if (law->pressure == SFG_LAW_FIXED_VALUE && !(law->pressure_value > 0.0))
+        return fail(SFG_ERR_ARG, "fixedValue pressure must be > 0");
+    s->laws[2 * axis + end] = *law;
+    build_law_view(s);
+    if (s->graph) {  // the captured launches hold the previous laws
+        cudaGraphExecDestroy(s->graph);
+        s->graph = nullptr;
+    }
+    return upload_law_codes(s);
+}
+
+int sfg_apply_boundary(sfg_solver s) {
+    if (!s) return fail(SFG_ERR_ARG, "null solver");
+    if (!s->has_laws) return SFG_OK;
+    CUDA_TRY(launch_law_fill(s->gv, s->lv, s->qn, s->qn, s->clock, 0, s->flags, s->stream));
+    return sync_and_check(s);
 }
 
 int sfg_ghost_layers(sfg_solver s, int* ng) {
@@ -675,6 +878,8 @@ int sfg_stage(sfg_solver s, int stage, double dt) {
     int rc = enqueue_stage(s, stage, false, false);
     if (rc) return rc;
     if (stage == ns - 1) {
+        rc = enqueue_commit_laws(s, false);
+        if (rc) return rc;
         rc = enqueue_post_step(s);
         if (rc) return rc;
         CUDA_TRY(launch_commit(s->clock, nullptr, 0, 0, s->stream));
@@ -689,6 +894,8 @@ int sfg_step(sfg_solver s, double dt, double limit) {
     if (!s) return fail(SFG_ERR_ARG, "null solver");
     if (s->next_stage != 0) return fail(SFG_ERR_ARG, "a step is in progress (stage %d)", s->next_stage);
     if (dt > 0.0) {
+        if (s->has_laws)  // FlowStepPrepare
+            CUDA_TRY(launch_law_fill(s->gv, s->lv, s->qn, s->qn, s->clock, 0, s->flags, s->stream));
         for (int st = 0; st < stage_count(s->num.time_recipe); ++st) {
             s->next_stage = st;
             int rc = sfg_stage(s, st, dt);

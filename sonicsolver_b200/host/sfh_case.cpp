@@ -92,11 +92,30 @@ std::string convection_token(const Node& nu) {
     return scheme + flux;
 }
 
-// Condition token of one patch entry: `zeroGradient` or `{type: zeroGradient}`.
-std::string condition(const Node& n) {
-    if (n.is_scalar()) return n.str();
-    if (const Node* t = n.get("type")) return t->str();
-    throw ParseError("boundary condition without a type");
+// One patch entry: `zeroGradient`, `{type: fixedValue, value: V}` or the
+// compact `{fixedValue: V}` (compactBoundary, SF_case.cpp:22-29).
+FieldCondition condition(const Node& n, const std::string& what) {
+    FieldCondition fc;
+    auto values = [&](const Node& v) {
+        std::vector<double> out;
+        if (v.is_scalar()) out.push_back(v.number());
+        else if (v.is_seq())
+            for (const auto& x : v.items) out.push_back(x.number());
+        else if (v.kind != Node::Null) throw ParseError(what + ": value must be a number or a list");
+        return out;
+    };
+    if (n.is_scalar()) {
+        fc.type = n.str();
+    } else if (n.is_map() && n.get("type")) {
+        fc.type = n.at("type").str();
+        if (const Node* v = n.get("value")) fc.value = values(*v);
+    } else if (n.is_map() && n.fields.size() == 1) {
+        fc.type = n.fields[0].first;
+        fc.value = values(n.fields[0].second);
+    } else {
+        throw ParseError(what + ": boundary condition must contain exactly one condition type");
+    }
+    return fc;
 }
 
 }  // namespace
@@ -188,12 +207,7 @@ CaseSpec load_case(const std::string& dir) {
         const Node* vb = bc.get(var);
         if (!vb) continue;
         for (const auto& kv : vb->fields) {
-            const std::string cond = condition(kv.second);
-            auto it = c.patch_bc.find(kv.first);
-            if (it == c.patch_bc.end()) c.patch_bc[kv.first] = cond;
-            else if (it->second != cond)
-                throw Unsupported("patch '" + kv.first + "': rho, U and p carry different conditions (" + it->second +
-                                  " / " + cond + "); the provider applies one condition per patch");
+            c.patch_bc[kv.first][var] = condition(kv.second, std::string(var) + "." + kv.first);
         }
     }
     return c;
@@ -213,18 +227,73 @@ const AxisPatches kPatches[3] = {{"Left", "Right", "inlet", "outlet"},
                                  {"sideWalls", "sideWalls", "walls", "walls"},
                                  {"frontBack", "frontBack", "walls", "walls"}};
 
-const std::string* patch_condition(const CaseSpec& c, const char* name, const char* alt) {
+using PatchConditions = std::map<std::string, FieldCondition>;
+
+const PatchConditions* patch_condition(const CaseSpec& c, const char* name, const char* alt) {
     auto it = c.patch_bc.find(name);
     if (it != c.patch_bc.end()) return &it->second;
     it = c.patch_bc.find(alt);
     return it != c.patch_bc.end() ? &it->second : nullptr;
 }
 
-int bc_kind(const std::string& token, const char* patch) {
-    if (token == "zeroGradient") return SFG_BC_TRANSMISSIVE;
-    if (token == "periodic" || token == "cyclic") return SFG_BC_PERIODIC;
-    throw Unsupported(std::string("patch '") + patch + "': condition '" + token +
-                      "' is not provided on the GPU (zeroGradient, periodic, empty are)");
+bool has_type(const PatchConditions& pc, const char* token) {
+    for (const auto& kv : pc)
+        if (lower(kv.second.type) == token) return true;
+    return false;
+}
+
+// Law of one field from its token (valueBCTypeValue,
+// app/application/model/compatibility/private/SF_valueParser.cpp:146-164:
+// case-insensitive; noSlip / slip are velocity laws: fixedValue 0 and
+// symmetry).
+int field_law(const FieldCondition& fc, bool velocity, const std::string& what, double* value) {
+    const std::string t = lower(fc.type);
+    const size_t want = velocity ? 3 : 1;
+    if (velocity && (t == "noslip" || t == "slip")) {
+        if (t == "noslip") value[0] = value[1] = value[2] = 0.0;
+        return t == "noslip" ? SFG_LAW_FIXED_VALUE : SFG_LAW_SYMMETRY;
+    }
+    if (t == "zerogradient" || t == "zero_gradient") return SFG_LAW_ZERO_GRADIENT;
+    if (t == "symmetry" || t == "symmetryplane") return SFG_LAW_SYMMETRY;
+    if (t == "fixedvalue" || t == "fixed_value") {
+        if (fc.value.size() != want)
+            throw ParseError(what + ": fixedValue needs " + std::to_string(want) + " number(s)");
+        for (size_t i = 0; i < want; ++i) value[i] = fc.value[i];
+        return SFG_LAW_FIXED_VALUE;
+    }
+    throw Unsupported(what + ": condition '" + fc.type +
+                      "' is not provided on the GPU (fixedValue, zeroGradient, symmetry, slip, noSlip, periodic, "
+                      "empty are)");
+}
+
+// Boundary kind (and laws) of one axis end.
+int end_kind(const PatchConditions& pc, const char* patch, sfg_boundary_law& law) {
+    if (has_type(pc, "periodic") || has_type(pc, "cyclic")) {
+        for (const auto& kv : pc) {
+            const std::string t = lower(kv.second.type);
+            if (t != "periodic" && t != "cyclic")
+                throw Unsupported(std::string("patch '") + patch + "': periodic must hold for every field");
+        }
+        return SFG_BC_PERIODIC;
+    }
+    const FieldCondition* f[3] = {nullptr, nullptr, nullptr};
+    const char* names[3] = {"rho", "U", "p"};
+    for (int i = 0; i < 3; ++i) {
+        auto it = pc.find(names[i]);
+        if (it == pc.end())
+            throw Unsupported(std::string("patch '") + patch + "': " + names[i] +
+                              " has no condition while other fields have one (the provider needs rho, U and p)");
+        f[i] = &it->second;
+    }
+    const std::string where = std::string("patch '") + patch + "' ";
+    law = sfg_boundary_law{};
+    law.rho = field_law(*f[0], false, where + "rho", &law.rho_value);
+    law.velocity = field_law(*f[1], true, where + "U", law.velocity_value);
+    law.pressure = field_law(*f[2], false, where + "p", &law.pressure_value);
+    if (law.rho == SFG_LAW_ZERO_GRADIENT && law.velocity == SFG_LAW_ZERO_GRADIENT &&
+        law.pressure == SFG_LAW_ZERO_GRADIENT)
+        return SFG_BC_TRANSMISSIVE;
+    return SFG_BC_LAW;
 }
 
 }  // namespace
@@ -236,9 +305,9 @@ GridSetup build_grid(const CaseSpec& c) {
     bool active[3];
     for (int d = 0; d < 3; ++d) {
         const AxisPatches& P = kPatches[d];
-        const std::string* lo = patch_condition(c, P.lo, P.alt_lo);
-        const std::string* hi = patch_condition(c, P.hi, P.alt_hi);
-        const bool empty = (lo && *lo == "empty") || (hi && *hi == "empty");
+        const PatchConditions* lo = patch_condition(c, P.lo, P.alt_lo);
+        const PatchConditions* hi = patch_condition(c, P.hi, P.alt_hi);
+        const bool empty = (lo && has_type(*lo, "empty")) || (hi && has_type(*hi, "empty"));
         if (empty || (c.cells[d] <= 1 && !lo && !hi)) {
             active[d] = false;
             continue;
@@ -246,8 +315,8 @@ GridSetup build_grid(const CaseSpec& c) {
         // a patch without a condition keeps its initial ghost state and its
         // boundary node is advanced (SF_applicator.h:162-187): SFG_BC_FROZEN
         active[d] = true;
-        g.grid.bc_lo[d] = lo ? bc_kind(*lo, P.lo) : SFG_BC_FROZEN;
-        g.grid.bc_hi[d] = hi ? bc_kind(*hi, P.hi) : SFG_BC_FROZEN;
+        g.grid.bc_lo[d] = lo ? end_kind(*lo, P.lo, g.laws[2 * d]) : SFG_BC_FROZEN;
+        g.grid.bc_hi[d] = hi ? end_kind(*hi, P.hi, g.laws[2 * d + 1]) : SFG_BC_FROZEN;
         if ((g.grid.bc_lo[d] == SFG_BC_PERIODIC) != (g.grid.bc_hi[d] == SFG_BC_PERIODIC))
             throw Unsupported(std::string("axis ") + "xyz"[d] + ": periodic must hold at both ends");
     }

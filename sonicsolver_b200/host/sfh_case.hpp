@@ -10,8 +10,8 @@
 //     nGhost; one axis-aligned box block);
 //   fields/fields.yaml -> internalField (rho, U, p: uniform / default plus
 //     the mesh sets leftHalf, rightHalf, all) and boundaries (per variable,
-//     per patch: zeroGradient, empty, none (frozen ghosts), and this
-//     provider's periodic).
+//     per patch: fixedValue, zeroGradient, symmetry, velocity noSlip / slip,
+//     empty, none (frozen ghosts), and this provider's periodic).
 // Mesh sets follow the structured generator
 // (src/infrastructure/mesh/createMesh/SF_meshGen.cpp:514-541): patches Left /
 // Right (i = 0 / nx-1), sideWalls (j ends), frontBack (k ends); leftHalf holds
@@ -30,6 +30,14 @@ namespace sfh {
 // A case the provider cannot run; the message says what and why.
 struct Unsupported : std::runtime_error {
     using std::runtime_error::runtime_error;
+};
+
+// One field's condition at one patch (compactBoundary,
+// src/infrastructure/io/case/SF_case.cpp:22-29): the law token as written
+// and its value (fixedValue: 1 number for rho and p, 3 for U).
+struct FieldCondition {
+    std::string type;
+    std::vector<double> value;
 };
 
 struct InitialValue {
@@ -52,8 +60,8 @@ struct CaseSpec {
     double start_time = 0.0, end_time = 0.0, cfl = 0.5, write_interval = 0.0;
     bool write_initial = false;
     std::string write_control = "runTime", output_dir = "result", job_name;
-    // one condition per patch (rho, U and p must agree)
-    std::map<std::string, std::string> patch_bc;
+    // patch -> field ("rho", "U", "p") -> condition
+    std::map<std::string, std::map<std::string, FieldCondition>> patch_bc;
     InitialValue rho, U, p;
 };
 
@@ -62,6 +70,7 @@ CaseSpec load_case(const std::string& dir);
 // The provider's grid and initial state for a case.
 struct GridSetup {
     sfg_grid_desc grid{};
+    sfg_boundary_law laws[6] = {};  // [2 * axis + end] of SFG_BC_LAW ends
     int nodes[3] = {1, 1, 1};
     double origin[3] = {0, 0, 0};
     std::vector<double> q;  // AoS [k][j][i][v] over the nodes, conserved
@@ -69,8 +78,10 @@ struct GridSetup {
 
 // An active patch with no condition becomes SFG_BC_FROZEN (the reference
 // keeps the initial ghost state there and advances the boundary node).
+// A patch whose rho, U and p are all zeroGradient is SFG_BC_TRANSMISSIVE;
+// one with fixedValue or symmetry laws is SFG_BC_LAW with those laws.
 // Throws Unsupported for what this provider does not run (curvilinear or
-// graded blocks; conditions other than zeroGradient, periodic and empty).
+// graded blocks; a patch with conditions for only some of rho, U, p).
 GridSetup build_grid(const CaseSpec& c);
 
 }  // namespace sfh

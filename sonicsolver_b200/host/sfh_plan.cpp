@@ -62,9 +62,12 @@ PlanNode conservative_explicit_plan(const std::string& provider, int stages) {
     stage_loop.name = "Explicit.stages";
     stage_loop.count = stages;
     stage_loop.children.push_back(op("Explicit.stage", opid::ExplicitStageExecute, provider));
+    // the explicit fragment of every step (SF_builtinProviders.cpp:63-81):
+    // prepare, dt, begin, stages; then the commits
     PlanNode step;
     step.kind = PlanKind::TimeLoop;
     step.name = "Explicit.step";
+    step.children.push_back(op("Explicit.prepare", opid::FlowStepPrepare, provider));
     step.children.push_back(op("Explicit.dt", opid::FlowDtCompute, provider));
     step.children.push_back(op("Explicit.begin", opid::FlowStepBegin, provider));
     step.children.push_back(std::move(stage_loop));
@@ -73,7 +76,6 @@ PlanNode conservative_explicit_plan(const std::string& provider, int stages) {
     PlanNode root;
     root.kind = PlanKind::Sequence;
     root.name = "ConservativeResidual";
-    root.children.push_back(op("Explicit.prepare", opid::FlowStepPrepare, provider));
     root.children.push_back(std::move(step));
     return root;
 }

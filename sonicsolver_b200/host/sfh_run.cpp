@@ -117,11 +117,23 @@ bool remaining_limit(const Run& r, double t, double& limit) {
     return true;
 }
 
+// Output schedule and the initial write, before the time loop.
+int start_output(Run& r, double t) {
+    r.next_out = r.c->write_interval > 0.0 ? t + r.c->write_interval : 0.0;
+    return r.c->write_initial ? write_output(r, t) : 0;
+}
+
 void bind_ops(OperationTable& ops, const std::string& provider, Run& r) {
     ops.bind(opid::FlowStepPrepare, provider, [&r](StepContext& ctx) {
-        // ghosts and periodic images are index maps inside the kernels
-        r.next_out = r.c->write_interval > 0.0 ? ctx.t + r.c->write_interval : 0.0;
-        return r.c->write_initial ? write_output(r, ctx.t) : 0;
+        // the time loop ends before a step's fragment once t_end is reached
+        double limit = 0.0;
+        if (!remaining_limit(r, ctx.t, limit)) {
+            ctx.stop = true;
+            return 0;
+        }
+        // the physical boundary laws of law ends; ghosts of the other ends
+        // are index maps inside the kernels
+        return sfg_apply_boundary(r.s);
     });
     ops.bind(opid::FlowDtCompute, provider, [&r](StepContext& ctx) {
         double limit = 0.0;
@@ -154,9 +166,7 @@ void bind_ops(OperationTable& ops, const std::string& provider, Run& r) {
 // The time loop between output times as one sfg_advance (device clock, CUDA
 // graphs of `graph_steps` steps).
 int run_graph(Run& r, int graph_steps, StepContext& ctx) {
-    r.next_out = r.c->write_interval > 0.0 ? ctx.t + r.c->write_interval : 0.0;
-    if (r.c->write_initial)
-        if (int rc = write_output(r, ctx.t)) return rc;
+    if (int rc = start_output(r, ctx.t)) return rc;
     for (;;) {
         double limit = 0.0;
         if (!remaining_limit(r, ctx.t, limit)) return 0;
@@ -305,6 +315,17 @@ int main(int argc, char** argv) {
         std::printf("grid dim=%d nodes=%d,%d,%d h=%.17g,%.17g,%.17g bc=%d%d/%d%d/%d%d\n", g.grid.dim, g.nodes[0],
                     g.nodes[1], g.nodes[2], g.grid.h[0], g.grid.h[1], g.grid.h[2], g.grid.bc_lo[0], g.grid.bc_hi[0],
                     g.grid.bc_lo[1], g.grid.bc_hi[1], g.grid.bc_lo[2], g.grid.bc_hi[2]);
+        for (int a = 0; a < 3; ++a)
+            for (int e = 0; e < 2; ++e) {
+                if ((e ? g.grid.bc_hi[a] : g.grid.bc_lo[a]) != SFG_BC_LAW) continue;
+                const sfg_boundary_law& L = g.laws[2 * a + e];
+                auto law_name = [](int k) {
+                    return k == SFG_LAW_FIXED_VALUE ? "fixedValue" : k == SFG_LAW_SYMMETRY ? "symmetry" : "zeroGradient";
+                };
+                std::printf("law %c%s rho=%s(%.17g) U=%s(%.17g,%.17g,%.17g) p=%s(%.17g)\n", "xyz"[a], e ? "hi" : "lo",
+                            law_name(L.rho), L.rho_value, law_name(L.velocity), L.velocity_value[0],
+                            L.velocity_value[1], L.velocity_value[2], law_name(L.pressure), L.pressure_value);
+            }
         if (o.describe_only) {
             OperationTable ops;
             Run dummy;
@@ -326,6 +347,14 @@ int main(int argc, char** argv) {
             std::fprintf(stderr, "sfg_run: %s\n", sfg_last_error());
             return 1;
         }
+        for (int a = 0; a < g.grid.dim; ++a)
+            for (int e = 0; e < 2; ++e)
+                if ((e ? g.grid.bc_hi[a] : g.grid.bc_lo[a]) == SFG_BC_LAW &&
+                    sfg_set_boundary_law(r.s, a, e, &g.laws[2 * a + e]) != SFG_OK) {
+                    std::fprintf(stderr, "sfg_run: %s\n", sfg_last_error());
+                    sfg_destroy(r.s);
+                    return 1;
+                }
         int rc = sfg_upload(r.s, g.q.data(), SFG_LAYOUT_NODES, c.start_time);
         StepContext ctx;
         ctx.t = c.start_time;
@@ -334,7 +363,8 @@ int main(int argc, char** argv) {
             if (o.mode == "plan") {
                 OperationTable ops;
                 bind_ops(ops, provider, r);
-                rc = PlanExecutor(ops).run(plan, ctx);
+                rc = start_output(r, ctx.t);
+                if (!rc) rc = PlanExecutor(ops).run(plan, ctx);
             } else {
                 rc = run_graph(r, o.graph_steps, ctx);
             }

@@ -4,6 +4,7 @@
 #include <cerrno>
 #include <cstdlib>
 #include <fstream>
+#include <regex>
 #include <sstream>
 
 namespace sfh {
@@ -366,12 +367,50 @@ Node parse_yaml(const std::string& text, const std::string& origin) {
     return Block(std::move(lines), origin).document();
 }
 
+// The two input conveniences of SonicFile, rewritten to plain YAML before
+// parsing as the reference does (normalizeSonicSyntax,
+// src/infrastructure/io/serialization/SF_serialization.cpp:35-60):
+//   `patch: fixedValue: V`  ->  `patch:` / `  fixedValue: V`
+//   `[1 0 0]`               ->  `[1, 0, 0]`
+std::string normalize_sonic_syntax(const std::string& text) {
+    static const std::regex compact(R"(^([ \t]*)([^:#\n][^:\n]*):[ \t]*([A-Za-z][A-Za-z0-9_-]*)[ \t]*:[ \t]*(.*)$)");
+    static const std::regex bracket(R"(\[([^\[\],#'"]+)\])");
+    std::istringstream in(text);
+    std::ostringstream out;
+    std::string line;
+    while (std::getline(in, line)) {
+        std::smatch m;
+        if (std::regex_match(line, m, compact))
+            line = m[1].str() + m[2].str() + ":\n" + m[1].str() + "  " + m[3].str() + ": " + m[4].str();
+        std::string fixed;
+        size_t pos = 0;
+        for (std::sregex_iterator it(line.begin(), line.end(), bracket), end; it != end; ++it) {
+            const std::smatch& b = *it;
+            fixed.append(line, pos, (size_t)b.position() - pos);
+            std::istringstream words(b[1].str());
+            std::vector<std::string> tok;
+            for (std::string w; words >> w;) tok.push_back(w);
+            if (tok.size() > 1) {
+                fixed += "[";
+                for (size_t i = 0; i < tok.size(); ++i) fixed += (i ? ", " : "") + tok[i];
+                fixed += "]";
+            } else {
+                fixed += b.str();
+            }
+            pos = (size_t)(b.position() + b.length());
+        }
+        fixed.append(line, pos, std::string::npos);
+        out << fixed << "\n";
+    }
+    return out.str();
+}
+
 Node load_yaml_file(const std::string& path) {
     std::ifstream f(path);
     if (!f) throw ParseError("cannot open " + path);
     std::stringstream ss;
     ss << f.rdbuf();
-    return parse_yaml(ss.str(), path);
+    return parse_yaml(normalize_sonic_syntax(ss.str()), path);
 }
 
 }  // namespace sfh

@@ -22,8 +22,10 @@ def write_case(root, name, *, cells, box_hi, box_lo=(0.0, 0.0, 0.0), n_ghost=3, 
                time="SSPRK3", end_time=0.2, cfl=0.5, write_interval=0.05, write_initial=False, gamma=1.4,
                left=(1.0, 0.0, 1.0), right=(0.125, 0.0, 0.1), boundaries=None, numerics_form="terms"):
     """A Riemann problem: leftHalf / rightHalf states (rho, u, p) split at
-    i < nx/2.  `boundaries` maps patch -> condition (omitted patches get
-    none); defaults to zeroGradient Left/Right and empty side patches."""
+    i < nx/2.  `boundaries` maps patch -> condition, or patch -> {field:
+    condition} for per-field laws (written verbatim, so the SonicFile form
+    `fixedValue: [1 0 0]` works); omitted patches get none.  Defaults to
+    zeroGradient Left/Right and empty side patches."""
     if boundaries is None:
         boundaries = {"Left": "zeroGradient", "Right": "zeroGradient", "sideWalls": "empty", "frontBack": "empty"}
     d = os.path.join(root, name)
@@ -75,7 +77,12 @@ def write_case(root, name, *, cells, box_hi, box_lo=(0.0, 0.0, 0.0), n_ghost=3, 
        f"U:\n  default: [0, 0, 0]\n  leftHalf: [{ul!r}, 0, 0]\n  rightHalf: [{ur!r}, 0, 0]\n"
        f"p:\n  default: 0\n  leftHalf: {pl!r}\n  rightHalf: {pr!r}\n"
        f"rho:\n  default: 0\n  leftHalf: {rl!r}\n  rightHalf: {rr!r}\n")
-    bc = "".join(f"  {patch}: {cond}\n" for patch, cond in boundaries.items())
-    _w(os.path.join(d, "fields", "boundaries.yaml"),
-       "SonicFile:\n  object: fields\n  type: boundaries\n" + "".join(f"{v}:\n{bc}" for v in ("U", "p", "rho")))
+    def cond_of(cond, var):
+        return cond[var] if isinstance(cond, dict) else cond
+    body = ""
+    for v in ("U", "p", "rho"):
+        lines = "".join(f"  {patch}: {cond_of(cond, v)}\n" for patch, cond in boundaries.items()
+                        if not isinstance(cond, dict) or v in cond)
+        body += f"{v}:\n{lines}"
+    _w(os.path.join(d, "fields", "boundaries.yaml"), "SonicFile:\n  object: fields\n  type: boundaries\n" + body)
     return d

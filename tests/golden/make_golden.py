@@ -10,6 +10,11 @@ source tree and oracle/_ref are available: ``python tests/golden/make_golden.py`
   (SF::divDispatch + Math::spatialResidual, run through oracle/_ref) on small
   seeded states, every provided recipe, 1-D / 2-D / 3-D, transmissive and
   periodic ends.
+* ref_laws.npz -- the reference's own physical boundary laws
+  (Boundary::update for density and velocity, updateEnergyFromPressure; run
+  through oracle/_ref `sfr_fill_laws`) applied to small seeded states with
+  law ends on every active axis: every density / velocity / pressure law
+  combination on a 1-D grid, a cycle of combinations on 2-D and 3-D grids.
 """
 import json
 import os
@@ -67,7 +72,57 @@ def ref_rhs_fixture():
     np.savez_compressed(os.path.join(HERE, "ref_rhs.npz"), **arrays)
 
 
+LAW_GRIDS = [(1, (9, 1, 1)), (2, (8, 7, 1)), (3, (5, 4, 4))]
+
+
+def law_state(spec, rng):
+    """Positive random state on every storage position (ghosts included: the
+    laws read the previous ghost and boundary values)."""
+    Q = spec.empty()
+    Q[..., 0] = rng.uniform(0.5, 2.0, Q.shape[:-1])
+    for d in range(3):
+        Q[..., 1 + d] = rng.uniform(-0.3, 0.3, Q.shape[:-1]) * Q[..., 0]
+    ke = 0.5 * (Q[..., 1] ** 2 + Q[..., 2] ** 2 + Q[..., 3] ** 2) / Q[..., 0]
+    Q[..., 4] = rng.uniform(0.5, 2.0, Q.shape[:-1]) / 0.4 + ke
+    return Q
+
+
+def law_specs():
+    """(name, GridSpec) of the ref_laws cases."""
+    import itertools
+    import pyoracle as po
+    kinds = [po.LAW_ZERO_GRADIENT, po.LAW_FIXED_VALUE, po.LAW_SYMMETRY]
+    combos = list(itertools.product(kinds, kinds, kinds))
+    out = []
+    for dim, n in LAW_GRIDS:
+        use = combos if dim == 1 else combos[::3] if dim == 2 else combos[1::13]
+        for combo in use:
+            laws = {}
+            for d in range(dim):
+                for e in (0, 1):
+                    laws[(d, e)] = po.LawSpec(*combo, rho_value=1.3 + 0.1 * d, U_value=(0.2 * e, -0.1, 0.05 * d),
+                                              p_value=2.2 + 0.2 * e)
+            bc = tuple(po.BC_LAW if d < dim else po.BC_TRANSMISSIVE for d in range(3))
+            spec = po.GridSpec(dim=dim, n=n, h=(0.1, 0.1, 0.1), bc_lo=bc, bc_hi=bc, laws=laws)
+            out.append((f"{dim}d_{combo[0]}{combo[1]}{combo[2]}", spec))
+    return out
+
+
+def ref_laws_fixture():
+    import pyoracle as po
+    rng = np.random.default_rng(2024)
+    arrays = {}
+    for name, spec in law_specs():
+        Q = law_state(spec, rng)
+        out = Q.copy()
+        po.ref_fill_laws(spec, out)
+        arrays[name + "_in"] = Q
+        arrays[name + "_out"] = out
+    np.savez_compressed(os.path.join(HERE, "ref_laws.npz"), **arrays)
+
+
 if __name__ == "__main__":
     sod_fixture()
     ref_rhs_fixture()
+    ref_laws_fixture()
     print("fixtures written to", HERE)

@@ -191,3 +191,50 @@ def test_frozen_end_field_layout_ghosts_are_used():
     got = s.download(layout=capi.LAYOUT_FIELD).reshape((1 + 2 * ng,) + Q.shape[1:])[ng]
     assert rel_linf(got[ng:-ng, ng:-ng], spec.interior(Q)[0]).max() <= 1e-12
     np.testing.assert_array_equal(got[ng:-ng, :ng], np.broadcast_to(ghost, got[ng:-ng, :ng].shape))
+
+
+LAW_CASE = {
+    "Left": {"rho": "fixedValue: 1.0", "U": "fixedValue: [0.3 0 0]", "p": "fixedValue: 1.0"},
+    "Right": {"rho": "zeroGradient", "U": "noSlip", "p": "zeroGradient"},
+    "sideWalls": "empty", "frontBack": "empty",
+}
+
+
+def law_oracle(cells=400, t_end=0.1, cfl=0.5, write_interval=0.05):
+    """The law case of LAW_CASE on the oracle: inflow on the left, a wall on
+    the right; ghosts start as copies of the boundary nodes, as the device's
+    upload holds them."""
+    n = cells + 1
+    h = 1.0 / cells
+    laws = {(0, 0): po.LawSpec(po.LAW_FIXED_VALUE, po.LAW_FIXED_VALUE, po.LAW_FIXED_VALUE, rho_value=1.0,
+                               U_value=(0.3, 0.0, 0.0), p_value=1.0),
+            (0, 1): po.LawSpec(po.LAW_ZERO_GRADIENT, po.LAW_FIXED_VALUE, po.LAW_ZERO_GRADIENT)}
+    spec = po.GridSpec(dim=1, n=(n, 1, 1), ng=3, h=(h, 0.1, 0.1), bc_lo=(po.BC_LAW, 0, 0),
+                       bc_hi=(po.BC_LAW, 0, 0), laws=laws)
+    Q = spec.empty()
+    i = np.arange(n)
+    Q[0, 0, 3:3 + n, 0] = np.where(i < n // 2, 1.0, 0.125)
+    Q[0, 0, 3:3 + n, 4] = np.where(i < n // 2, 1.0, 0.1) / 0.4
+    Q[0, 0, :3] = Q[0, 0, 3]
+    Q[0, 0, 3 + n:] = Q[0, 0, 2 + n]
+    dts, tf = po.advance(spec, po.WENO5, po.RUSANOV, po.SSPRK3, Q, t_end, cfl, write_interval=write_interval)
+    return np.ascontiguousarray(spec.interior(Q)).reshape(-1, 5), dts, tf
+
+
+@pytest.fixture(scope="module")
+def law_dir(tmp_path_factory):
+    return write_case(str(tmp_path_factory.mktemp("cases")), "law_c1", cells=(400, 1, 1), box_hi=(1.0, 0.1, 0.1),
+                      end_time=0.1, write_interval=0.05, boundaries=LAW_CASE)
+
+
+@pytest.mark.parametrize("mode", ["graph", "plan"])
+def test_law_case_directory_matches_oracle(law_dir, mode):
+    """fixedValue inflow and a noSlip wall from case.yaml through sfg_run:
+    the laws run before every step and stage and after each step, as the
+    reference's FlowStepPrepare / stage RHS / FlowStepCommit apply them."""
+    s, q, _ = run_case(law_dir, "--mode", mode, "--no-write")
+    want, dts, tf = law_oracle()
+    assert s["steps"] == len(dts) and abs(s["time"] - tf) <= 1e-14 and s["status"] == 0
+    assert rel_linf(q, want).max() <= 1e-11
+    q = q.reshape(-1, 5)
+    assert q[0, 0] == 1.0 and q[0, 1] == 0.3 and q[-1, 1] == 0.0

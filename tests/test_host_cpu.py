@@ -68,10 +68,10 @@ def test_unsupported_recipe(runner, tmp_path, convection, needle):
 
 def test_unsupported_condition_and_time(runner, tmp_path):
     d = write_case(str(tmp_path), "a", cells=(50, 1, 1), box_hi=(1.0, 0.1, 0.1),
-                   boundaries={"Left": "fixedValue", "Right": "zeroGradient", "sideWalls": "empty",
+                   boundaries={"Left": "inletOutlet", "Right": "zeroGradient", "sideWalls": "empty",
                                "frontBack": "empty"})
     r = run(runner, d, "--describe")
-    assert r.returncode == 3 and "fixedValue" in r.stderr
+    assert r.returncode == 3 and "inletOutlet" in r.stderr
     d2 = write_case(str(tmp_path), "b", cells=(50, 1, 1), box_hi=(1.0, 0.1, 0.1), time="backwardEuler")
     r2 = run(runner, d2, "--describe")
     assert r2.returncode == 3 and "time recipe" in r2.stderr
@@ -108,3 +108,45 @@ def test_reference_case_directories(runner):
             assert "unsupported:" in r.stderr
     for case in ("sodCase", "sodCase_weno7", "sodCase_weno7_t0p2"):
         assert os.path.join("Sod", case) in resolved
+
+
+LAW_BOUNDARIES = {
+    "Left": {"rho": "fixedValue: 1.2", "U": "fixedValue: [0.5 0 0]", "p": "fixedValue: 1.1"},
+    "Right": {"rho": "zeroGradient", "U": "noSlip", "p": "{type: zeroGradient}"},
+    "sideWalls": "empty", "frontBack": "empty",
+}
+
+
+def test_describe_law_patches(runner, tmp_path):
+    """fixedValue / noSlip / zeroGradient per field become SFG_BC_LAW ends
+    with those laws; the compact SonicFile syntax is read."""
+    d = write_case(str(tmp_path), "laws", cells=(40, 1, 1), box_hi=(1.0, 0.1, 0.1), boundaries=LAW_BOUNDARIES)
+    r = run(runner, d, "--describe")
+    assert r.returncode == 0, r.stderr
+    assert "bc=33/00/00" in r.stdout
+    assert "law xlo rho=fixedValue(1.2) U=fixedValue(0.5,0,0) p=fixedValue(1.1000000000000001)" in r.stdout
+    assert "law xhi rho=zeroGradient(0) U=fixedValue(0,0,0) p=zeroGradient(0)" in r.stdout
+    slip = dict(LAW_BOUNDARIES, Right={"rho": "zeroGradient", "U": "slip", "p": "symmetry"})
+    r2 = run(runner, write_case(str(tmp_path), "slip", cells=(40, 1, 1), box_hi=(1.0, 0.1, 0.1), boundaries=slip),
+             "--describe")
+    assert r2.returncode == 0 and "law xhi rho=zeroGradient(0) U=symmetry(0,0,0) p=symmetry(0)" in r2.stdout
+    # all-zeroGradient patches stay transmissive
+    zg = dict(LAW_BOUNDARIES, Left={"rho": "zeroGradient", "U": "zero_gradient", "p": "ZeroGradient"})
+    r3 = run(runner, write_case(str(tmp_path), "zg", cells=(40, 1, 1), box_hi=(1.0, 0.1, 0.1), boundaries=zg),
+             "--describe")
+    assert r3.returncode == 0 and "bc=03/00/00" in r3.stdout
+
+
+def test_law_patch_errors(runner, tmp_path):
+    partial = dict(LAW_BOUNDARIES, Right={"U": "noSlip"})
+    r = run(runner, write_case(str(tmp_path), "partial", cells=(40, 1, 1), box_hi=(1.0, 0.1, 0.1),
+                               boundaries=partial), "--describe")
+    assert r.returncode == 3 and "rho has no condition" in r.stderr
+    bad = dict(LAW_BOUNDARIES, Left={"rho": "fixedValue: 1.2", "U": "fixedValue: 0.5", "p": "fixedValue: 1.1"})
+    r2 = run(runner, write_case(str(tmp_path), "bad", cells=(40, 1, 1), box_hi=(1.0, 0.1, 0.1), boundaries=bad),
+             "--describe")
+    assert r2.returncode == 1 and "fixedValue needs 3 number(s)" in r2.stderr
+    noslip_p = dict(LAW_BOUNDARIES, Right={"rho": "zeroGradient", "U": "noSlip", "p": "noSlip"})
+    r3 = run(runner, write_case(str(tmp_path), "np", cells=(40, 1, 1), box_hi=(1.0, 0.1, 0.1),
+                                boundaries=noslip_p), "--describe")
+    assert r3.returncode == 3 and "noSlip" in r3.stderr
