@@ -212,6 +212,18 @@ int sfg_set_boundary_law(sfg_solver s, int axis, int end, const sfg_boundary_law
 /* Applies the laws of every SFG_BC_LAW end to the current state once (the
  * reference's Boundary::Applicator::apply on the Field). */
 int sfg_apply_boundary(sfg_solver s);
+/* Curvilinear grids: the per-node metrics of the reference Field, 10 doubles
+ * per node in the order Jac (= 1/J), XiX, XiY, XiZ, EtX, EtY, EtZ, ZeX, ZeY,
+ * ZeZ (src/core/field/SF_field.h metric arrays; computed by the mesh,
+ * src/infrastructure/mesh/SF_mesh.cpp:260-339), in SFG_LAYOUT_NODES (AoS over
+ * the nodes) or SFG_LAYOUT_FIELD (AoS with the ghost layers; a frozen end's
+ * ghost face reads them).  From then on every face takes the cofactor
+ * 0.5 (m_i / Jac_i + m_i+1 / Jac_i+1) as normal and area
+ * (SF_canonicalFace.h:56-118), the residual is Jac_node * sum_d dF_d, and the
+ * CFL rate uses the node's metric vectors; the grid's h[] is no longer read
+ * by the operator.  FP64; all fluxes but Lax-Wendroff (which needs node
+ * coordinates). */
+int sfg_set_metrics(sfg_solver s, const double* metrics, int layout);
 /* Host <-> device copies of the conserved state (pageable or pinned host
  * memory; synchronous with respect to the solver's stream). Upload resets the
  * time to `time`. */

@@ -41,7 +41,7 @@ class Grid(ctypes.Structure):
     _fields_ = [("dim", ctypes.c_int), ("n", ctypes.c_int * 3), ("ng", ctypes.c_int),
                 ("h", ctypes.c_double * 3), ("bc_lo", ctypes.c_int * 3),
                 ("bc_hi", ctypes.c_int * 3), ("gamma", ctypes.c_double),
-                ("law", ctypes.POINTER(Law))]
+                ("law", ctypes.POINTER(Law)), ("metrics", ctypes.POINTER(ctypes.c_double))]
 
 
 @dataclass
@@ -80,6 +80,7 @@ class GridSpec:
     bc_hi: tuple = (0, 0, 0)
     gamma: float = 1.4
     laws: dict = field(default_factory=dict)   # (axis, end) -> LawSpec for BC_LAW ends
+    metrics: np.ndarray | None = None          # curvilinear: (mz, my, mx, 10) over Q's layout
 
     def c(self) -> Grid:
         g = Grid()
@@ -97,6 +98,11 @@ class GridSpec:
                 arr[2 * axis + end] = law.c()
             g._laws = arr               # keeps the array alive with the struct
             g.law = ctypes.cast(arr, ctypes.POINTER(Law))
+        if self.metrics is not None:
+            m = np.ascontiguousarray(self.metrics, dtype=np.float64)
+            assert m.shape == self.extents[::-1] + (10,), (m.shape, self.extents)
+            g._metrics = m
+            g.metrics = m.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
         return g
 
     @property

@@ -93,6 +93,31 @@ void setup_case(RefCase& rc, const sfo_grid* g) {
                 rc.field.Y(i, j, k) = (j - g->ng) * hy;
                 rc.field.Z(i, j, k) = (k - g->ng) * hz;
             }
+    // Curvilinear grids: the caller's per-node metrics (compact layout; the
+    // Field's extra ghosts on inactive axes take the nearest compact point).
+    if (g->metrics) {
+        const int m0 = storage_extent(g, 0), m1 = storage_extent(g, 1), m2 = storage_extent(g, 2);
+        int off[3];
+        for (int d = 0; d < 3; ++d) off[d] = d < g->dim ? 0 : g->ng;
+        for (int k = 0; k < rc.field.MZ(); ++k)
+            for (int j = 0; j < rc.field.MY(); ++j)
+                for (int i = 0; i < rc.field.MX(); ++i) {
+                    int c[3] = {i - off[0], j - off[1], k - off[2]};
+                    const int m[3] = {m0, m1, m2};
+                    for (int d = 0; d < 3; ++d) c[d] = c[d] < 0 ? 0 : (c[d] >= m[d] ? m[d] - 1 : c[d]);
+                    const double* src = g->metrics + (((long long)c[2] * m1 + c[1]) * m0 + c[0]) * 10;
+                    rc.field.Jac(i, j, k) = src[0];
+                    rc.field.XiX(i, j, k) = src[1];
+                    rc.field.XiY(i, j, k) = src[2];
+                    rc.field.XiZ(i, j, k) = src[3];
+                    rc.field.EtX(i, j, k) = src[4];
+                    rc.field.EtY(i, j, k) = src[5];
+                    rc.field.EtZ(i, j, k) = src[6];
+                    rc.field.ZeX(i, j, k) = src[7];
+                    rc.field.ZeY(i, j, k) = src[8];
+                    rc.field.ZeZ(i, j, k) = src[9];
+                }
+    }
     // Solver-boundary sets: the transmissive (zeroGradient) and LAW ends,
     // exactly the nodes that Boundary::Applicator marks
     // (SF_applicator.h:162-187).  Points are listed with the last axis

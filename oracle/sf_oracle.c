@@ -870,9 +870,10 @@ int sfo_rhs(const sfo_grid* g, int scheme, int flux, const double* Q, double* R,
         F[d] = (double*)calloc((size_t)total * NV, sizeof(double));
         if (!F[d]) { err = SFO_ERR_ARG; goto done; }
     }
+    if (g->metrics && flux == SFO_LAXWENDROFF) { err = SFO_ERR_ARG; goto done; }  /* needs coordinates */
     for (int d = 0; d < g->dim && !err; ++d) {
-        const double metrics[4] = {d == 0 ? L.area[0] : 0.0, d == 1 ? L.area[1] : 0.0,
-                                   d == 2 ? L.area[2] : 0.0, L.jac};
+        double metrics[4] = {d == 0 ? L.area[0] : 0.0, d == 1 ? L.area[1] : 0.0,
+                             d == 2 ? L.area[2] : 0.0, L.jac};
         int lo[3], hi[3];
         for (int a = 0; a < 3; ++a) {
             lo[a] = L.lo[a];
@@ -896,6 +897,21 @@ int sfo_rhs(const sfo_grid* g, int scheme, int flux, const double* Q, double* R,
                     double spacing = fabs(xr - xl);
                     spacing = spacing > 1e-14 ? spacing : 1e-14;
                     double f[5];
+                    if (g->metrics) {
+                        /* canonicalFace::geometry without stored face metrics
+                         * (SF_canonicalFace.h:56-118): the cofactor averaged
+                         * from metricCofactor(m, Jac) = m / Jac of both nodes */
+                        const long long pa = at / NV, pb = (at + sd) / NV;
+                        const double* ma = g->metrics + pa * 10;
+                        const double* mb = g->metrics + pb * 10;
+                        if (!isfinite(ma[0]) || !isfinite(mb[0]) || fabs(ma[0]) < 1.0e-30 || fabs(mb[0]) < 1.0e-30) {
+                            err = SFO_ERR_ARG;
+                            break;
+                        }
+                        for (int c = 0; c < 3; ++c)
+                            metrics[c] = 0.5 * (ma[1 + 3 * d + c] / ma[0] + mb[1 + 3 * d + c] / mb[0]);
+                        metrics[3] = 0.5 * (ma[0] + mb[0]);
+                    }
                     err = sfo_char_face_flux_ex(nst, st, metrics, scheme, flux, g->gamma, g_lw_dt, spacing, f);
                     if (err) break;
                     for (int v = 0; v < 5; ++v) {
@@ -911,11 +927,12 @@ int sfo_rhs(const sfo_grid* g, int scheme, int flux, const double* Q, double* R,
         for (int j = L.lo[1]; j < L.lo[1] + g->n[1]; ++j)
             for (int i = L.lo[0]; i < L.lo[0] + g->n[0]; ++i) {
                 const long long at = i * L.stride[0] + j * L.stride[1] + k * L.stride[2];
+                const double jac = g->metrics ? g->metrics[(at / NV) * 10] : L.jac;
                 for (int v = 0; v < 5; ++v) {
                     double div = 0.0;
                     for (int d = 0; d < g->dim; ++d)
                         div += F[d][at + v] - F[d][at - L.stride[d] + v];
-                    R[at + v] = L.jac * div - 0.0;
+                    R[at + v] = jac * div - 0.0;
                 }
             }
 done:
@@ -939,14 +956,20 @@ int sfo_dt(const sfo_grid* g, const double* Q, double cfl, double* dt) {
                 closed_state s;
                 int err = close_state(q, g->gamma, &s);
                 if (err) return err;
-                /* metric vectors are (xi_x,0,0), (0,eta_y,0), (0,0,zeta_z) */
-                const double ux = fabs(s.vel[0] * L.metric[0] + s.vel[1] * 0.0 + s.vel[2] * 0.0);
-                const double ue = fabs(s.vel[0] * 0.0 + s.vel[1] * L.metric[1] + s.vel[2] * 0.0);
-                const double uz = fabs(s.vel[0] * 0.0 + s.vel[1] * 0.0 + s.vel[2] * L.metric[2]);
+                /* metric vectors: per node on curvilinear grids, else
+                 * (xi_x,0,0), (0,eta_y,0), (0,0,zeta_z) */
+                double mv[9] = {L.metric[0], 0.0, 0.0, 0.0, L.metric[1], 0.0, 0.0, 0.0, L.metric[2]};
+                if (g->metrics) {
+                    const double* m = g->metrics + ((idx[0] * L.stride[0] + idx[1] * L.stride[1] + idx[2] * L.stride[2]) / NV) * 10;
+                    for (int c = 0; c < 9; ++c) mv[c] = m[1 + c];
+                }
+                const double ux = fabs(s.vel[0] * mv[0] + s.vel[1] * mv[1] + s.vel[2] * mv[2]);
+                const double ue = fabs(s.vel[0] * mv[3] + s.vel[1] * mv[4] + s.vel[2] * mv[5]);
+                const double uz = fabs(s.vel[0] * mv[6] + s.vel[1] * mv[7] + s.vel[2] * mv[8]);
                 double sr = 0.0;
-                if (g->dim > 0) sr += ux + s.c * sqrt(L.metric[0] * L.metric[0] + 0.0 * 0.0 + 0.0 * 0.0);
-                if (g->dim > 1) sr += ue + s.c * sqrt(0.0 * 0.0 + L.metric[1] * L.metric[1] + 0.0 * 0.0);
-                if (g->dim > 2) sr += uz + s.c * sqrt(0.0 * 0.0 + 0.0 * 0.0 + L.metric[2] * L.metric[2]);
+                if (g->dim > 0) sr += ux + s.c * sqrt(mv[0] * mv[0] + mv[1] * mv[1] + mv[2] * mv[2]);
+                if (g->dim > 1) sr += ue + s.c * sqrt(mv[3] * mv[3] + mv[4] * mv[4] + mv[5] * mv[5]);
+                if (g->dim > 2) sr += uz + s.c * sqrt(mv[6] * mv[6] + mv[7] * mv[7] + mv[8] * mv[8]);
                 if (!isfinite(sr) || sr <= 0.0) return SFO_ERR_STATE;
                 const double cand = cfl / sr;
                 if (cand < result) result = cand;

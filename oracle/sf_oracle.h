@@ -75,6 +75,10 @@ typedef struct {
     int bc_hi[3];
     double gamma;
     const sfo_law* law;  /* law[2 * axis + end] of SFO_BC_LAW ends (end 0 = low) */
+    /* Curvilinear grids: 10 doubles per storage point of Q's layout (ghosts
+     * included): Jac (= 1/J), XiX, XiY, XiZ, EtX, EtY, EtZ, ZeX, ZeY, ZeZ, as
+     * the reference Field holds them.  NULL: uniform Cartesian metrics from h. */
+    const double* metrics;
 } sfo_grid;
 
 /* Counters reported by the oracle (TENO cut-off decisions etc.). */

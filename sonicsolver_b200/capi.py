@@ -101,6 +101,7 @@ def lib():
         L.sfg_ghost_layers.argtypes = [_VP, ctypes.POINTER(ctypes.c_int)]
         L.sfg_set_boundary_law.argtypes = [_VP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(BoundaryLaw)]
         L.sfg_apply_boundary.argtypes = [_VP]
+        L.sfg_set_metrics.argtypes = [_VP, _DP, ctypes.c_int]
         L.sfg_state_size.argtypes = [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]
         L.sfg_upload.argtypes = [_VP, _DP, ctypes.c_int, ctypes.c_double]
         L.sfg_download.argtypes = [_VP, _DP, ctypes.c_int]
@@ -221,6 +222,11 @@ class Solver:
             law.velocity_value[d] = float(velocity_value[d])
         law.pressure_value = float(pressure_value)
         check(lib().sfg_set_boundary_law(self._h, axis, end, ctypes.byref(law)))
+
+    def set_metrics(self, metrics: np.ndarray, layout=LAYOUT_NODES):
+        """Per-node metrics (Jac, xi_x..zeta_z: 10 per node) of a curvilinear grid."""
+        m = np.ascontiguousarray(metrics, dtype=np.float64)
+        check(lib().sfg_set_metrics(self._h, _dptr(m), layout))
 
     def apply_boundary(self):
         """Apply the laws of every law end to the current state once."""

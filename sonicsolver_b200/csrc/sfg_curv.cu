@@ -1,0 +1,463 @@
+// sfg_curv.cu -- the stage operator on curvilinear grids: per-node metrics
+// (Jac = 1/J and the xi / eta / zeta vectors the reference Field carries,
+// src/infrastructure/mesh/SF_mesh.cpp:260-339) and per-face geometry
+// (canonicalFace::geometry, methods/numerics/structured/SF_canonicalFace.h:56-118).
+//
+//   curv_geometry_kernel  once per sfg_set_metrics: for every face (i | i+1)
+//                         the cofactor 0.5 (m_i / Jac_i + m_i+1 / Jac_i+1),
+//                         its magnitude (the area) and the unit normal,
+//                         stored at the lower node i (4 x vs per axis).
+//   curv_face_kernel      per axis and stage: one thread per face; the
+//                         characteristic reconstruction with the full 5 x 5
+//                         left / right eigenvectors of the face normal
+//                         (Riemann::buildCharacteristicMatrix,
+//                         convection/SF_riemann.cpp:69-123), the face flux
+//                         along that normal, times the area.
+//   curv_stage_kernel     per stage: R = Jac_node * sum_d (F_d[i] - F_d[i-1])
+//                         and the stage update.
+//
+// FP64.  Reads per node and stage: the state (stencils, mostly from L2), 4
+// doubles of face geometry per axis, Jac; writes 5 face fluxes per axis.
+#include "sfg_internal.h"
+#include "sfg_stage.cuh"
+
+namespace sfg {
+
+namespace {
+
+// physical_pressure with the validity bits (requirePhysicalState).
+__device__ __forceinline__ double pressure_n(const double (&q)[5], double gamma, unsigned& flags) {
+    if (!isfinite(q[0] + q[1] + q[2] + q[3] + q[4])) flags |= FLAG_NONFINITE;
+    if (!(q[0] > 0.0)) flags |= FLAG_DENSITY;
+    const double inv = 1.0 / q[0];
+    const double ke = 0.5 * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]) * inv;
+    const double p = (gamma - 1.0) * (q[4] - ke);
+    if (!(p > 0.0)) flags |= FLAG_PRESSURE;
+    return p;
+}
+
+// Left / right eigenvectors of the flux Jacobian along the unit normal n
+// (Riemann::buildCharacteristicMatrix, SF_riemann.cpp:69-123): tangents l, m
+// from n, acoustic rows with the (gamma - 1)|u|^2 / (4 c^2) kinetic term.
+__device__ __forceinline__ void char_matrix_n(const double (&q)[5], const double (&n)[3], double gamma,
+                                              double (&L)[5][5], double (&R)[5][5], unsigned& flags) {
+    const double p = pressure_n(q, gamma, flags);
+    const double invR = 1.0 / q[0];
+    const double u = q[1] * invR, v = q[2] * invR, w = q[3] * invR;
+    const double q2 = u * u + v * v + w * w;
+    const double c = sqrt(gamma * p * invR);
+    const double H = (q[4] + p) * invR;
+    const double n1 = n[0], n2 = n[1], n3 = n[2];
+    double l1, l2, l3;
+    if (fabs(n3) <= fabs(n2)) {
+        const double ss = sqrt(n1 * n1 + n2 * n2);
+        l1 = -n2 / ss;
+        l2 = n1 / ss;
+        l3 = 0.0;
+    } else {
+        const double ss = sqrt(n1 * n1 + n3 * n3);
+        l1 = -n3 / ss;
+        l2 = 0.0;
+        l3 = n1 / ss;
+    }
+    const double m1 = n2 * l3 - n3 * l2, m2 = n3 * l1 - n1 * l3, m3 = n1 * l2 - n2 * l1;
+    const double un = u * n1 + v * n2 + w * n3;
+    const double ul = u * l1 + v * l2 + w * l3;
+    const double um = u * m1 + v * m2 + w * m3;
+    const double b1 = (gamma - 1.0) / (c * c);
+    const double b2 = 0.5 * b1;
+    const double x1 = 1.0 / (2.0 * c);
+    const double Lm[5][5] = {{1.0 - b2 * q2, b1 * u, b1 * v, b1 * w, -b1},
+                             {-ul, l1, l2, l3, 0.0},
+                             {-um, m1, m2, m3, 0.0},
+                             {0.5 * b2 * q2 + x1 * un, -x1 * n1 - b2 * u, -x1 * n2 - b2 * v, -x1 * n3 - b2 * w, b2},
+                             {0.5 * b2 * q2 - x1 * un, x1 * n1 - b2 * u, x1 * n2 - b2 * v, x1 * n3 - b2 * w, b2}};
+    const double Rm[5][5] = {{1.0, 0.0, 0.0, 1.0, 1.0},
+                             {u, l1, m1, u - c * n1, u + c * n1},
+                             {v, l2, m2, v - c * n2, v + c * n2},
+                             {w, l3, m3, w - c * n3, w + c * n3},
+                             {0.5 * q2, ul, um, H - c * un, H + c * un}};
+#pragma unroll
+    for (int r = 0; r < 5; ++r)
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+            L[r][k] = Lm[r][k];
+            R[r][k] = Rm[r][k];
+        }
+}
+
+__device__ __forceinline__ void gemv5(const double (&M)[5][5], const double (&x)[5], double (&y)[5]) {
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+        double acc = 0.0;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) acc += M[r][k] * x[k];
+        y[r] = acc;
+    }
+}
+
+// Physical flux along n (Euler flux of one state).
+__device__ __forceinline__ void euler_flux_n(const double (&q)[5], const double (&n)[3], double gamma,
+                                             double (&f)[5], unsigned& flags) {
+    const double p = pressure_n(q, gamma, flags);
+    const double rho = q[0];
+    const double u = q[1] / rho, v = q[2] / rho, w = q[3] / rho;
+    const double un = u * n[0] + v * n[1] + w * n[2];
+    f[0] = rho * un;
+    f[1] = rho * u * un + p * n[0];
+    f[2] = rho * v * un + p * n[1];
+    f[3] = rho * w * un + p * n[2];
+    f[4] = (q[4] + p) * un;
+}
+
+// Rusanov with both sides closed (RusanovEOS::faceFlux, SF_rusanovEOS.cpp:47-77).
+__device__ __forceinline__ void rusanov_n(const double (&qL)[5], const double (&qR)[5], const double (&n)[3],
+                                          double gamma, double (&F)[5], unsigned& flags) {
+    const double iL = 1.0 / qL[0], iR = 1.0 / qR[0];
+    const double uL[3] = {qL[1] * iL, qL[2] * iL, qL[3] * iL}, uR[3] = {qR[1] * iR, qR[2] * iR, qR[3] * iR};
+    const double eL = (qL[4] - 0.5 * qL[0] * (uL[0] * uL[0] + uL[1] * uL[1] + uL[2] * uL[2])) / qL[0];
+    const double eR = (qR[4] - 0.5 * qR[0] * (uR[0] * uR[0] + uR[1] * uR[1] + uR[2] * uR[2])) / qR[0];
+    const double pL = (gamma - 1.0) * qL[0] * eL, pR = (gamma - 1.0) * qR[0] * eR;
+    if (!(qL[0] > 0.0) || !(qR[0] > 0.0)) flags |= FLAG_DENSITY;
+    if (!(pL > 0.0) || !(pR > 0.0)) flags |= FLAG_PRESSURE;
+    const double cL = sqrt(gamma * pL / qL[0]), cR = sqrt(gamma * pR / qR[0]);
+    const double unL = uL[0] * n[0] + uL[1] * n[1] + uL[2] * n[2];
+    const double unR = uR[0] * n[0] + uR[1] * n[1] + uR[2] * n[2];
+    double fL[5], fR[5];
+    fL[0] = qL[0] * unL;
+    fR[0] = qR[0] * unR;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        fL[1 + d] = qL[1 + d] * unL + pL * n[d];
+        fR[1 + d] = qR[1 + d] * unR + pR * n[d];
+    }
+    fL[4] = (qL[4] + pL) * unL;
+    fR[4] = (qR[4] + pR) * unR;
+    const double lam = fmax(fabs(unL) + cL, fabs(unR) + cR);
+    if (!isfinite(lam) || !(lam > 0.0)) flags |= FLAG_NONFINITE;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) F[k] = 0.5 * (fL[k] + fR[k]) - 0.5 * lam * (qR[k] - qL[k]);
+}
+
+// Roe with the entropy fix and the reference's eigenvalue / eigenvector
+// pairing (Flux::RoeFlux::flux, SF_roe.cpp:10-90).
+__device__ __forceinline__ void roe_n(const double (&qL)[5], const double (&qR)[5], const double (&n)[3],
+                                      double gamma, double (&F)[5], unsigned& flags) {
+    const double gm1 = gamma - 1.0;
+    const double pL = pressure_n(qL, gamma, flags), pR = pressure_n(qR, gamma, flags);
+    const double iL = 1.0 / qL[0], iR = 1.0 / qR[0];
+    const double uL = qL[1] * iL, vL = qL[2] * iL, wL = qL[3] * iL, hL = (qL[4] + pL) * iL;
+    const double uR = qR[1] * iR, vR = qR[2] * iR, wR = qR[3] * iR, hR = (qR[4] + pR) * iR;
+    const double sL = sqrt(qL[0]), sR = sqrt(qR[0]), ss = sL + sR;
+    const double ur = (sL * uL + sR * uR) / ss, vr = (sL * vL + sR * vR) / ss, wr = (sL * wL + sR * wR) / ss;
+    const double hr = (sL * hL + sR * hR) / ss;
+    const double q2 = ur * ur + vr * vr + wr * wr;
+    const double a2 = gm1 * (hr - 0.5 * q2);
+    if (!isfinite(a2) || !(a2 > 0.0)) flags |= FLAG_ROE_SOUND;
+    const double a = sqrt(a2);
+    const double unr = ur * n[0] + vr * n[1] + wr * n[2];
+    const double lam[5] = {unr, unr, unr, unr + a, unr - a};
+    const double eps = 0.1 * a;
+    double al[5];
+#pragma unroll
+    for (int m = 0; m < 5; ++m) {
+        const double x = fabs(lam[m]);
+        al[m] = x < 2.0 * eps ? 0.5 * (x * x / (2.0 * eps) + eps) : x;
+    }
+    const double rr = sL * sR;
+    const double qRoe[5] = {rr, rr * ur, rr * vr, rr * wr, rr * (0.5 * q2 + a2 / gm1)};
+    double L[5][5], R[5][5];
+    char_matrix_n(qRoe, n, gamma, L, R, flags);
+    double dQ[5], alpha[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) dQ[k] = qR[k] - qL[k];
+    gemv5(L, dQ, alpha);
+    double diss[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int wv = 0; wv < 5; ++wv) {
+        const double strength = al[wv] * alpha[wv];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) diss[k] += R[k][wv] * strength;
+    }
+    double fL[5], fR[5];
+    euler_flux_n(qL, n, gamma, fL, flags);
+    euler_flux_n(qR, n, gamma, fR, flags);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) F[k] = 0.5 * (fL[k] + fR[k] - diss[k]);
+}
+
+// Steger-Warming split of one state (Flux::StegerWarmingFlux, SF_sw.cpp),
+// entropy-fixed eigenvalue parts; POS: the positive part.
+template <bool POS>
+__device__ __forceinline__ void steger_part_n(const double (&q)[5], const double (&n)[3], double gamma,
+                                              double (&f)[5], unsigned& flags) {
+    const double p = pressure_n(q, gamma, flags);
+    const double r = q[0], invR = 1.0 / r;
+    const double u = q[1] * invR, v = q[2] * invR, w = q[3] * invR;
+    const double q2 = u * u + v * v + w * w;
+    const double a = sqrt(gamma * p * invR);
+    const double un = u * n[0] + v * n[1] + w * n[2];
+    const double lam[5] = {un, un, un, un + a, un - a};
+    double l[5];
+    const double eps = 0.01;
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+        double lp, lm;
+        if (fabs(lam[i]) < 2.0 * eps) {
+            lp = 0.5 * (lam[i] * lam[i] / (4.0 * eps) + lam[i] + eps);
+            lm = lam[i] - lp;
+        } else {
+            lp = 0.5 * (lam[i] + fabs(lam[i]));
+            lm = 0.5 * (lam[i] - fabs(lam[i]));
+        }
+        l[i] = POS ? lp : lm;
+    }
+    const double common = r / (2.0 * gamma);
+    const double W1 = 2.0 * (gamma - 1.0) * l[0] + l[3] + l[4], W2 = l[3] - l[4], W3 = l[3] + l[4];
+    f[0] = common * W1;
+    f[1] = common * (u * W1 + a * n[0] * W2);
+    f[2] = common * (v * W1 + a * n[1] * W2);
+    f[3] = common * (w * W1 + a * n[2] * W2);
+    f[4] = common * (0.5 * q2 * W1 + a * un * W2 + (a * a / (gamma - 1.0)) * W3);
+}
+
+// Local Lax-Friedrichs split of one state (Flux::LaxFriedrichsFlux, SF_lxF.cpp).
+__device__ __forceinline__ void laxf_part_n(const double (&q)[5], const double (&n)[3], double gamma, double sign,
+                                            double (&f)[5], unsigned& flags) {
+    const double p = pressure_n(q, gamma, flags);
+    const double r = q[0], invR = 1.0 / r;
+    const double u = q[1] * invR, v = q[2] * invR, w = q[3] * invR;
+    const double a = sqrt(gamma * p * invR);
+    const double un = u * n[0] + v * n[1] + w * n[2];
+    const double lam = fabs(un) + a;
+    const double Fp[5] = {r * un, q[1] * un + p * n[0], q[2] * un + p * n[1], q[3] * un + p * n[2], (q[4] + p) * un};
+#pragma unroll
+    for (int i = 0; i < 5; ++i) f[i] = 0.5 * (Fp[i] + sign * lam * q[i]);
+}
+
+template <int FLUX>
+__device__ __forceinline__ void flux_n(const double (&qL)[5], const double (&qR)[5], const double (&n)[3],
+                                       double gamma, double (&F)[5], unsigned& flags) {
+    if constexpr (FLUX == RUSANOV) {
+        rusanov_n(qL, qR, n, gamma, F, flags);
+    } else if constexpr (FLUX == ROE) {
+        roe_n(qL, qR, n, gamma, F, flags);
+    } else if constexpr (FLUX == STEGER) {
+        double fp[5], fm[5];
+        steger_part_n<true>(qL, n, gamma, fp, flags);
+        steger_part_n<false>(qR, n, gamma, fm, flags);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) F[k] = fp[k] + fm[k];
+    } else {
+        double fp[5], fm[5];
+        laxf_part_n(qL, n, gamma, 1.0, fp, flags);
+        laxf_part_n(qR, n, gamma, -1.0, fm, flags);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) F[k] = fp[k] + fm[k];
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Face geometry from node metrics (SF_canonicalFace.h:56-118): stored for the
+// faces whose lower node is i; the upper node wraps on periodic axes and
+// does not exist past the last node of other axes (nothing stored).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) curv_geometry_kernel(GridView g, const double* __restrict__ nm,
+                                                            double* geom0, double* geom1, double* geom2,
+                                                            unsigned* flags) {
+    const long long nodes = (long long)g.n[0] * g.n[1] * g.n[2];
+    const long long vs = g.vs;
+    double* geom[3] = {geom0, geom1, geom2};
+    unsigned fl = 0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nodes;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int c[3] = {(int)(t % g.n[0]), (int)((t / g.n[0]) % g.n[1]), (int)(t / ((long long)g.n[0] * g.n[1]))};
+        for (int a = 0; a < g.dim; ++a) {
+            int cu[3] = {c[0], c[1], c[2]};
+            cu[a] = c[a] + 1;
+            if (cu[a] >= g.n[a]) {
+                if (g.bc_hi[a] != BC_PERIODIC) continue;
+                cu[a] = 0;
+            }
+            const long long up = ((long long)cu[2] * g.n[1] + cu[1]) * g.n[0] + cu[0];
+            const double ja = nm[t], jb = nm[up];
+            if (!isfinite(ja) || !isfinite(jb) || fabs(ja) < 1.0e-30 || fabs(jb) < 1.0e-30) fl |= FLAG_NONFINITE;
+            double cof[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+                cof[k] = 0.5 * (__ddiv_rn(nm[(1 + 3 * a + k) * vs + t], ja) + __ddiv_rn(nm[(1 + 3 * a + k) * vs + up], jb));
+            const double area = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(cof[0], cof[0]), __dmul_rn(cof[1], cof[1])),
+                                                     __dmul_rn(cof[2], cof[2])));
+            if (!isfinite(area) || !(area > 0.0)) fl |= FLAG_NONFINITE;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) geom[a][k * vs + t] = __ddiv_rn(cof[k], area);
+            geom[a][3 * vs + t] = area;
+        }
+    }
+    if (fl) atomicOr(flags, fl);
+}
+
+// ---------------------------------------------------------------------------
+// Face fluxes along one axis.  Faces: lower node over [lo - 1, hi - 1] on a
+// bounded axis, [0, n) on a periodic one; the other axes over the solved
+// range.  F (times the face area) goes to fl[axis][v] at the lower node.
+// ---------------------------------------------------------------------------
+template <int SCHEME, int FLUX>
+__global__ void __launch_bounds__(128) curv_face_kernel(GridView g, StageView sv, int axis, double* fl) {
+    if (sv.require_active && !sv.clock->active) return;
+    constexpr int NST = SchemeInfo<SCHEME>::NST, W = SchemeInfo<SCHEME>::W;
+    const int a = axis;
+    int base[3], span[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const bool per = d < g.dim && g.bc_lo[d] == BC_PERIODIC;
+        base[d] = d == a ? (per ? 0 : g.lo[d] - 1) : g.lo[d];
+        span[d] = d == a ? (per ? g.n[d] : g.hi[d] - g.lo[d] + 1) : g.hi[d] - g.lo[d];
+    }
+    const long long total = (long long)span[0] * span[1] * span[2];
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    unsigned flags = 0, cut = 0, cores = 0;
+    if (t < total) {
+        int c[3];
+        long long r = t;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            c[d] = base[d] + (int)(r % span[d]);
+            r /= span[d];
+        }
+        const long long vs = g.vs;
+        double st[NST][5];
+#pragma unroll
+        for (int s = 0; s < NST; ++s) {
+            int cc[3] = {c[0], c[1], c[2]};
+            cc[a] = map_index(c[a] - (NST / 2 - 1) + s, g.n[a], g.bc_lo[a], g.bc_hi[a]);
+            const long long node = ((long long)cc[2] * g.n[1] + cc[1]) * g.n[0] + cc[0];
+#pragma unroll
+            for (int v = 0; v < 5; ++v) st[s][v] = sv.qs[v * vs + node];
+        }
+        const long long face = ((long long)c[2] * g.n[1] + c[1]) * g.n[0] + c[0];
+        const double* gm = g.geom[a];
+        const double n[3] = {gm[face], gm[vs + face], gm[2 * vs + face]};
+        const double area = gm[3 * vs + face];
+        double qavg[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) qavg[v] = 0.5 * (st[NST / 2 - 1][v] + st[NST / 2][v]);
+        double L[5][5], R[5][5];
+        char_matrix_n(qavg, n, g.gamma, L, R, flags);
+        double ch[NST][5];
+#pragma unroll
+        for (int s = 0; s < NST; ++s) gemv5(L, st[s], ch[s]);
+        double wl[5], wr[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            double sl[8], sr[8];
+#pragma unroll
+            for (int s = 0; s < W; ++s) {
+                sl[s] = ch[s][v];
+                sr[s] = ch[NST - 1 - s][v];
+            }
+            wl[v] = recon_core<SCHEME, double>(sl, flags, cut);
+            wr[v] = recon_core<SCHEME, double>(sr, flags, cut);
+        }
+        if (SCHEME == TENO5) cores += 10;
+        double qL[5], qR[5], F[5];
+        gemv5(R, wl, qL);
+        gemv5(R, wr, qR);
+        flux_n<FLUX>(qL, qR, n, g.gamma, F, flags);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            const double x = F[v] * area;
+            if (!isfinite(x)) flags |= FLAG_NONFINITE;
+            fl[((long long)a * 5 + v) * vs + face] = x;
+        }
+    }
+    flush_status(sv, flags, cores, cut);
+}
+
+// Divergence and stage update of the solved nodes.
+__global__ void __launch_bounds__(256) curv_stage_kernel(GridView g, StageView sv, const double* __restrict__ fl) {
+    if (sv.require_active && !sv.clock->active) return;
+    const long long cx = g.hi[0] - g.lo[0], cy = g.hi[1] - g.lo[1], cz = g.hi[2] - g.lo[2];
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    unsigned flags = 0;
+    double sr = 0.0;
+    if (t < cx * cy * cz) {
+        const int c[3] = {g.lo[0] + (int)(t % cx), g.lo[1] + (int)((t / cx) % cy), g.lo[2] + (int)(t / (cx * cy))};
+        const long long vs = g.vs;
+        const long long node = ((long long)c[2] * g.n[1] + c[1]) * g.n[0] + c[0];
+        double div[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int d = 0; d < g.dim; ++d) {
+            // the lower face is stored at node i - 1 (a face index, not a
+            // value read: only the periodic wrap applies)
+            int cl[3] = {c[0], c[1], c[2]};
+            cl[d] = c[d] - 1 < 0 ? c[d] - 1 + g.n[d] : c[d] - 1;
+            const long long lower = ((long long)cl[2] * g.n[1] + cl[1]) * g.n[0] + cl[0];
+#pragma unroll
+            for (int v = 0; v < 5; ++v)
+                div[v] += fl[((long long)d * 5 + v) * vs + node] - fl[((long long)d * 5 + v) * vs + lower];
+        }
+        double qn[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) qn[v] = sv.qs[v * vs + node];
+        finish_node_j<true>(g, sv, sv.clock->dt, node, qn, div, g.node_jac[node], flags, sr);
+    }
+    if (flags) atomicOr(sv.flags, flags);
+    if (sv.mode & MODE_CFL) flush_cfl_block(g, sv.clock, sr);
+}
+
+// ---------------------------------------------------------------------------
+cudaError_t launch_curv_geometry(const GridView& g, const double* nm, double* const geom[3], unsigned* flags,
+                                 cudaStream_t st) {
+    const long long nodes = (long long)g.n[0] * g.n[1] * g.n[2];
+    const unsigned blocks = (unsigned)std::min<long long>((nodes + 255) / 256, 148LL * 16);
+    curv_geometry_kernel<<<blocks, 256, 0, st>>>(g, nm, geom[0], geom[1], geom[2], flags);
+    return cudaGetLastError();
+}
+
+template <int SCHEME, int FLUX>
+static cudaError_t launch_curv_faces(const GridView& g, const StageView& sv, int axis, double* fl, cudaStream_t st) {
+    long long total = 1;
+    for (int d = 0; d < 3; ++d) {
+        const bool per = d < g.dim && g.bc_lo[d] == BC_PERIODIC;
+        total *= d == axis ? (per ? g.n[d] : g.hi[d] - g.lo[d] + 1) : g.hi[d] - g.lo[d];
+    }
+    curv_face_kernel<SCHEME, FLUX><<<(unsigned)((total + 127) / 128), 128, 0, st>>>(g, sv, axis, fl);
+    return cudaGetLastError();
+}
+
+template <int SCHEME>
+static cudaError_t launch_curv_faces_f(int flux, const GridView& g, const StageView& sv, int axis, double* fl,
+                                       cudaStream_t st) {
+    switch (flux) {
+    case RUSANOV: return launch_curv_faces<SCHEME, RUSANOV>(g, sv, axis, fl, st);
+    case ROE: return launch_curv_faces<SCHEME, ROE>(g, sv, axis, fl, st);
+    case STEGER: return launch_curv_faces<SCHEME, STEGER>(g, sv, axis, fl, st);
+    case LAXF: return launch_curv_faces<SCHEME, LAXF>(g, sv, axis, fl, st);
+    }
+    return cudaErrorInvalidValue;
+}
+
+// One stage on a curvilinear grid: the face fluxes of every active axis, then
+// the divergence and stage update (sv.mode: MODE_FINAL with optional
+// MODE_RESIDUAL / MODE_CFL).
+cudaError_t launch_curv_stage(int scheme, int flux, const GridView& g, const StageView& sv, double* fl,
+                              cudaStream_t st) {
+    for (int axis = 0; axis < g.dim; ++axis) {
+        cudaError_t e;
+        switch (scheme) {
+        case WENO5: e = launch_curv_faces_f<WENO5>(flux, g, sv, axis, fl, st); break;
+        case TENO5: e = launch_curv_faces_f<TENO5>(flux, g, sv, axis, fl, st); break;
+        case WENO3: e = launch_curv_faces_f<WENO3>(flux, g, sv, axis, fl, st); break;
+        case WENO7: e = launch_curv_faces_f<WENO7>(flux, g, sv, axis, fl, st); break;
+        default: return cudaErrorInvalidValue;
+        }
+        if (e != cudaSuccess) return e;
+    }
+    const long long solved = (long long)(g.hi[0] - g.lo[0]) * (g.hi[1] - g.lo[1]) * (g.hi[2] - g.lo[2]);
+    curv_stage_kernel<<<(unsigned)((solved + 255) / 256), 256, 0, st>>>(g, sv, fl);
+    return cudaGetLastError();
+}
+
+}  // namespace sfg

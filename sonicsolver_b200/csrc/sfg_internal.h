@@ -58,6 +58,12 @@ struct GridView {
     double gamma;
     double cfl;
     double h[3];       // node spacing (the Lax-Wendroff face spacing)
+    // Curvilinear grids (curv = 1; sfg_set_metrics): per-node metrics and
+    // per-face geometry replace jac / area / metric.
+    int curv;
+    const double* node_jac;     // Jac = 1/J per node (vs doubles)
+    const double* node_metric;  // xi_x, xi_y, xi_z, eta_x, ..., zeta_z per node (9 x vs)
+    const double* geom[3];      // per axis, face (i | i+1) at its lower node i: unit normal, area (4 x vs)
 };
 
 // Physical boundary laws of the law ends of one grid (SFG_BC_LAW; the

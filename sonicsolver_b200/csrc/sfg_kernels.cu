@@ -268,7 +268,7 @@ __global__ void __launch_bounds__(256) dt_kernel(GridView g, const double* __res
         const int k = g.lo[2] + (int)(t / (cx * cy));
         const long long node = ((long long)k * g.n[1] + j) * g.n[0] + i;
         const double qq[5] = {q[node], q[g.vs + node], q[2 * g.vs + node], q[3 * g.vs + node], q[4 * g.vs + node]};
-        const double sr = cfl_rate(g, qq);
+        const double sr = cfl_rate_node(g, qq, node);
         if (!(sr > 0.0) || !isfinite(sr)) fl |= FLAG_NONFINITE;
         best = fmax(best, sr);
     }
@@ -387,7 +387,8 @@ __global__ void totals_kernel(GridView g, const double* __restrict__ q, double* 
         }
         if (extra) continue;
         const long long node = ((long long)c[2] * g.n[1] + c[1]) * g.n[0] + c[0];
-        for (int v = 0; v < 5; ++v) acc[v] += q[v * g.vs + node];
+        const double w = g.curv ? 1.0 / g.node_jac[node] : 1.0;  // node volume J on curvilinear grids
+        for (int v = 0; v < 5; ++v) acc[v] += q[v * g.vs + node] * w;
     }
     for (int v = 0; v < 5; ++v) {
         double x = acc[v];

@@ -39,6 +39,10 @@ cudaError_t launch_tile1d(int scheme, int flux, int prec64, const GridView& g, c
 cudaError_t launch_tile3d(int scheme, int flux, int prec64, const GridView& g, const StageView& sv, cudaStream_t st);
 cudaError_t launch_law_fill(const GridView& g, const LawView& lv, const double* old, double* q, const Clock* clock,
                             int require_active, unsigned* flags, cudaStream_t st);
+cudaError_t launch_curv_geometry(const GridView& g, const double* nm, double* const geom[3], unsigned* flags,
+                                 cudaStream_t st);
+cudaError_t launch_curv_stage(int scheme, int flux, const GridView& g, const StageView& sv, double* fl,
+                              cudaStream_t st);
 cudaError_t launch_teno_flips(const GridView& g, const double* q, unsigned long long* out, cudaStream_t st);
 }  // namespace sfg
 
@@ -126,6 +130,10 @@ struct sfg_solver_s {
     sfg_boundary_law laws[6] = {};  // [2 * axis + end]
     LawView lv{};
     unsigned char* law_codes = nullptr;  // device: LAW_STATE_* per law face point
+    // curvilinear grids (sfg_set_metrics)
+    double* node_metrics = nullptr;  // Jac then the 9 metric components per node (10 x vs)
+    double* face_geom = nullptr;     // unit normal and area per face, per axis (3 x 4 x vs)
+    double* face_flux = nullptr;     // face fluxes of one stage, per axis (3 x 5 x vs)
     long long pub_nodes = 0;    // nodes of `grid`
     sfg_numerics_desc num{};
     const RecipeInfo* recipe = nullptr;
@@ -415,12 +423,18 @@ StageView stage_view(sfg_solver_s* s, int stage, bool residual_only, bool requir
 int enqueue_stage(sfg_solver_s* s, int stage, bool residual_only, bool require_active, bool cfl = false) {
     StageView sv = stage_view(s, stage, residual_only, require_active);
     const int dim = s->grid.dim;
+    const int cfl_bit_all = cfl && !residual_only ? MODE_CFL : 0;
     if (s->has_laws) {
         // prepareBoundaryState before the RHS: the laws on the stage's input;
         // the previous application's values sit in the previous stage's input
         const double* old = stage == 0 || residual_only ? s->qn : stage_view(s, stage - 1, false, false).qs;
         CUDA_TRY(launch_law_fill(s->gv, s->lv, old, const_cast<double*>(sv.qs), s->clock, require_active ? 1 : 0,
                                  s->flags, s->stream));
+    }
+    if (s->gv.curv) {  // per-face geometry: face-flux launches per axis, then the stage
+        sv.mode = MODE_FINAL | (residual_only ? MODE_RESIDUAL : 0) | cfl_bit_all;
+        CUDA_TRY(launch_curv_stage(s->recipe->scheme, s->recipe->flux, s->gv, sv, s->face_flux, s->stream));
+        return SFG_OK;
     }
     const int cfl_bit = cfl && !residual_only ? MODE_CFL : 0;
     if (dim == 2 && s->variant > 0) {
@@ -686,6 +700,8 @@ int sfg_destroy(sfg_solver s) {
         if (p) cudaFree(p);
     if (s->clock) cudaFree(s->clock);
     if (s->law_codes) cudaFree(s->law_codes);
+    for (double* p : {s->node_metrics, s->face_geom, s->face_flux})
+        if (p) cudaFree(p);
     if (s->flags) cudaFree(s->flags);
     if (s->counters) cudaFree(s->counters);
     if (s->host_clock) cudaFreeHost(s->host_clock);
@@ -717,6 +733,72 @@ int sfg_set_boundary_law(sfg_solver s, int axis, int end, const sfg_boundary_law
         s->graph = nullptr;
     }
     return upload_law_codes(s);
+}
+
+// Caller metrics (10 per node: Jac, xi_x, xi_y, xi_z, eta_x, eta_y, eta_z,
+// zeta_x, zeta_y, zeta_z) in the node or Field layout -> device SoA over the
+// device grid (extra nodes: the Field's first ghost layer, or the boundary
+// node's metrics in the node layout).
+static void metrics_to_device(const sfg_solver_s* s, const double* host, int layout, std::vector<double>& soa) {
+    const int* N = s->ig.n;
+    const int* P = s->grid.n;
+    const long long vs = s->gv.vs;
+    soa.assign((size_t)10 * vs, 0.0);
+    const long long mx = field_extent(s, 0), my = field_extent(s, 1);
+    for (int k = 0; k < N[2]; ++k)
+        for (int j = 0; j < N[1]; ++j)
+            for (int i = 0; i < N[0]; ++i) {
+                int c[3] = {i - s->off_lo[0], j - s->off_lo[1], k - s->off_lo[2]};
+                const double* src;
+                if (layout == SFG_LAYOUT_FIELD) {
+                    const long long fi = c[0] + s->ng, fj = c[1] + s->ng, fk = c[2] + s->ng;
+                    src = host + ((fk * my + fj) * mx + fi) * 10;
+                } else {
+                    for (int a = 0; a < 3; ++a) c[a] = c[a] < 0 ? 0 : (c[a] >= P[a] ? P[a] - 1 : c[a]);
+                    src = host + (((long long)c[2] * P[1] + c[1]) * P[0] + c[0]) * 10;
+                }
+                const long long node = ((long long)k * N[1] + j) * N[0] + i;
+                for (int m = 0; m < 10; ++m) soa[(size_t)(m * vs + node)] = src[m];
+            }
+}
+
+int sfg_set_metrics(sfg_solver s, const double* host, int layout) {
+    if (!s || !host) return fail(SFG_ERR_ARG, "null argument");
+    if (layout != SFG_LAYOUT_NODES && layout != SFG_LAYOUT_FIELD) return fail(SFG_ERR_ARG, "unknown layout %d", layout);
+    if (s->num.precision != SFG_PREC_FP64) return fail(SFG_ERR_ARG, "curvilinear grids run in FP64");
+    if (s->recipe->flux == LAXW)
+        return fail(SFG_ERR_ARG, "%s: Lax-Wendroff needs node coordinates; curvilinear grids take the other fluxes",
+                    s->recipe->name);
+    std::vector<double> soa;
+    metrics_to_device(s, host, layout, soa);
+    for (double x : soa)
+        if (!std::isfinite(x)) return fail(SFG_ERR_ARG, "metrics must be finite");
+    const size_t vsb = sizeof(double) * (size_t)s->gv.vs;
+    if (!s->node_metrics && (cudaMalloc((void**)&s->node_metrics, 10 * vsb) != cudaSuccess ||
+                             cudaMalloc((void**)&s->face_geom, 12 * vsb) != cudaSuccess ||
+                             cudaMalloc((void**)&s->face_flux, 15 * vsb) != cudaSuccess))
+        return fail(SFG_ERR_NOMEM, "device allocation of the metric arrays failed");
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    CUDA_TRY(cudaMemcpy(s->node_metrics, soa.data(), 10 * vsb, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemset(s->face_geom, 0, 12 * vsb));
+    CUDA_TRY(cudaMemset(s->face_flux, 0, 15 * vsb));
+    GridView g = s->gv;
+    double* geom[3] = {s->face_geom, s->face_geom + 4 * s->gv.vs, s->face_geom + 8 * s->gv.vs};
+    CUDA_TRY(cudaMemsetAsync(s->flags, 0, 64, s->stream));
+    CUDA_TRY(launch_curv_geometry(g, s->node_metrics, geom, s->flags, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    unsigned bits = 0;
+    CUDA_TRY(cudaMemcpy(&bits, s->flags, sizeof bits, cudaMemcpyDeviceToHost));
+    if (bits) return fail(SFG_ERR_ARG, "metrics give a degenerate face (zero Jac or zero area)");
+    s->gv.curv = 1;
+    s->gv.node_jac = s->node_metrics;
+    s->gv.node_metric = s->node_metrics + s->gv.vs;
+    for (int a = 0; a < 3; ++a) s->gv.geom[a] = geom[a];
+    if (s->graph) {  // the captured launches hold the previous grid view
+        cudaGraphExecDestroy(s->graph);
+        s->graph = nullptr;
+    }
+    return SFG_OK;
 }
 
 int sfg_apply_boundary(sfg_solver s) {
@@ -1077,7 +1159,8 @@ int sfg_stage_with_residual(sfg_solver s, int stage, double dt, const double* ho
 int sfg_conserved_totals(sfg_solver s, double totals[5]) {
     if (!s || !totals) return fail(SFG_ERR_ARG, "null argument");
     CUDA_TRY(cudaMemsetAsync(s->totals, 0, 5 * sizeof(double), s->stream));
-    const double vol = s->grid.h[0] * s->grid.h[1] * s->grid.h[2];
+    // node volume: the cell volume, or J = 1 / Jac per node on curvilinear grids
+    const double vol = s->gv.curv ? 1.0 : s->grid.h[0] * s->grid.h[1] * s->grid.h[2];
     CUDA_TRY(launch_totals(s->gv, s->qn, s->totals, vol, s->stream));
     CUDA_TRY(cudaMemcpyAsync(totals, s->totals, 5 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
     CUDA_TRY(cudaStreamSynchronize(s->stream));
@@ -1125,7 +1208,7 @@ int sfg_time_sweeps(sfg_solver s, int stage, double dt, int repeats, float* ms_p
     double acc[3] = {0, 0, 0};
     CUDA_TRY(launch_set_dt(s->clock, dt, s->stream));
     StageView sv = stage_view(s, stage, false, false);
-    if (s->variant > 0) {  // one fused launch per stage (1-D, 2-D and 3-D tiles)
+    if (s->variant > 0 || s->gv.curv) {  // one stage operator (tiles, or the curvilinear launches)
         for (int r = 0; r < repeats; ++r) {
             CUDA_TRY(cudaEventRecord(ev[0], s->stream));
             int rc = enqueue_stage(s, stage, false, false);

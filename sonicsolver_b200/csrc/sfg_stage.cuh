@@ -57,6 +57,28 @@ __device__ __forceinline__ double cfl_rate(const GridView& g, const double (&q)[
     return sr;
 }
 
+// The same with the node's own metric vectors (curvilinear grids):
+// sr = sum_active (|u . m_d| + c |m_d|), in the reference's operation order.
+__device__ __forceinline__ double cfl_rate_node(const GridView& g, const double (&q)[5], long long node) {
+    if (!g.curv) return cfl_rate(g, q);
+    const double rho = q[0];
+    const double u = __ddiv_rn(q[1], rho), v = __ddiv_rn(q[2], rho), w = __ddiv_rn(q[3], rho);
+    const double uu = __dadd_rn(__dadd_rn(__dmul_rn(u, u), __dmul_rn(v, v)), __dmul_rn(w, w));
+    const double kin = __dmul_rn(__dmul_rn(0.5, rho), uu);
+    const double e = __ddiv_rn(__dsub_rn(q[4], kin), rho);
+    const double p = __dmul_rn(__dmul_rn(g.gamma - 1.0, rho), e);
+    const double c = __dsqrt_rn(__ddiv_rn(__dmul_rn(g.gamma, p), rho));
+    double sr = 0.0;
+    for (int d = 0; d < g.dim; ++d) {
+        const double mx = g.node_metric[(3 * d) * g.vs + node], my = g.node_metric[(3 * d + 1) * g.vs + node],
+                     mz = g.node_metric[(3 * d + 2) * g.vs + node];
+        const double un = fabs(__dadd_rn(__dadd_rn(__dmul_rn(u, mx), __dmul_rn(v, my)), __dmul_rn(w, mz)));
+        const double mag = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(mx, mx), __dmul_rn(my, my)), __dmul_rn(mz, mz)));
+        sr = __dadd_rn(sr, __dadd_rn(un, __dmul_rn(c, mag)));
+    }
+    return sr;
+}
+
 // Largest sr of a warp, then one atomic: clock->dt_bits = min(.., CFL / sr).
 // Callers pass sr = 0 for threads without a node.
 __device__ __forceinline__ void flush_cfl_warp(const GridView& g, Clock* clock, double sr) {
@@ -103,18 +125,21 @@ __device__ __forceinline__ double stage_value(const StageView& sv, double dt, do
 // Finishes one node: residual output or stage update + state validation
 // (validateEquationState after every stage, SF_explicit.cpp:417).  With
 // MODE_CFL, sr_max also takes the node's CFL rate of the new state.
-__device__ __forceinline__ void finish_node(const GridView& g, const StageView& sv, double dt, long long node,
-                                            const double (&qn)[5], double (&div)[5], unsigned& flags,
-                                            double& sr_max) {
+// `jac` is the node's 1/J (g.jac on uniform grids); CURV: the CFL rate uses
+// the node's metric vectors.
+template <bool CURV>
+__device__ __forceinline__ void finish_node_j(const GridView& g, const StageView& sv, double dt, long long node,
+                                              const double (&qn)[5], double (&div)[5], double jac, unsigned& flags,
+                                              double& sr_max) {
     const long long vs = g.vs;
     if (sv.mode & MODE_RESIDUAL) {
 #pragma unroll
-        for (int v = 0; v < 5; ++v) sv.r[v * vs + node] = g.jac * div[v];
+        for (int v = 0; v < 5; ++v) sv.r[v * vs + node] = jac * div[v];
         return;
     }
     double out[5];
 #pragma unroll
-    for (int v = 0; v < 5; ++v) out[v] = stage_value(sv, dt, qn[v], g.jac * div[v] - 0.0, v * vs + node);
+    for (int v = 0; v < 5; ++v) out[v] = stage_value(sv, dt, qn[v], jac * div[v] - 0.0, v * vs + node);
 #pragma unroll
     for (int v = 0; v < 5; ++v) sv.qout[v * vs + node] = out[v];
     const double ke = 0.5 * (out[1] * out[1] + out[2] * out[2] + out[3] * out[3]) / out[0];
@@ -122,7 +147,13 @@ __device__ __forceinline__ void finish_node(const GridView& g, const StageView& 
     if (!(out[0] > 0.0)) flags |= FLAG_DENSITY;
     if (!(p > 0.0)) flags |= FLAG_PRESSURE;
     if (!isfinite(out[0] + out[1] + out[2] + out[3] + out[4])) flags |= FLAG_NONFINITE;
-    if (sv.mode & MODE_CFL) sr_max = fmax(sr_max, cfl_rate(g, out));
+    if (sv.mode & MODE_CFL) sr_max = fmax(sr_max, CURV ? cfl_rate_node(g, out, node) : cfl_rate(g, out));
+}
+
+__device__ __forceinline__ void finish_node(const GridView& g, const StageView& sv, double dt, long long node,
+                                            const double (&qn)[5], double (&div)[5], unsigned& flags,
+                                            double& sr_max) {
+    finish_node_j<false>(g, sv, dt, node, qn, div, g.jac, flags, sr_max);
 }
 
 __device__ __forceinline__ void flush_status(const StageView& sv, unsigned flags, unsigned cores, unsigned cut) {

@@ -65,3 +65,40 @@ def smooth_state(dim, n, seed=0, amp=0.2, gamma=1.4, shock=False, noise=0.01):
         p = np.where(jump, 0.4 * p, p)
     rho = rho * (1 + noise * rng.random(rho.shape))
     return cases.conserved(rho, u, v, w, p, gamma)
+
+
+def curvilinear_metrics(dim, n, h, ng, amp=0.15, field_layout=False, seed=0):
+    """Metrics of the smooth map x = h i + amp h sin(...) of the index space
+    (i, j, k), 10 per point as the reference Field holds them: Jac = 1/J with
+    J = det(dx/di), and the rows of (dx/di)^-1 (XiX, XiY, XiZ, EtX, ...).
+    The displacement is periodic in every index over the node count, so the
+    same map serves periodic axes.  Points cover the oracle's compact layout
+    (ghosts on active axes), or with `field_layout` the Field layout (ghosts
+    on every axis).  Returns an array (mz, my, mx, 10)."""
+    rng = np.random.default_rng(seed)
+    ph = rng.uniform(0, 2 * np.pi, 6)
+    ext = [n[d] + (2 * ng if (d < dim or field_layout) else 0) for d in range(3)]
+    off = [ng if (d < dim or field_layout) else 0 for d in range(3)]
+    k, j, i = np.meshgrid(np.arange(ext[2]) - off[2], np.arange(ext[1]) - off[1], np.arange(ext[0]) - off[0],
+                          indexing="ij")
+    tw = [2 * np.pi / n[d] if d < dim else 0.0 for d in range(3)]
+    idx = [i, j, k]
+    # displacement component c depends on the index of axis (c + 1) % dim
+    A = np.zeros(i.shape + (3, 3))
+    for c in range(3):
+        A[..., c, c] = h[c]
+        if c >= dim:
+            continue
+        o = (c + 1) % dim
+        if o == c:
+            continue
+        A[..., c, o] += amp * h[c] * tw[o] * np.cos(tw[o] * idx[o] + ph[c])
+        # and a weak self term so the map stays curved in 1-D
+    if dim == 1:
+        A[..., 0, 0] = h[0] * (1.0 + 0.3 * amp * np.cos(tw[0] * i + ph[0]))
+    J = np.linalg.det(A)
+    inv = np.linalg.inv(A)
+    out = np.empty(i.shape + (10,))
+    out[..., 0] = 1.0 / J
+    out[..., 1:10] = inv.reshape(i.shape + (9,))
+    return out
