@@ -67,6 +67,7 @@ def parse():
     ap.add_argument("--accuracy-t", type=float, default=10.0, help="vortex run length for the L1 check (0: skip)")
     ap.add_argument("--tgv-t", type=float, default=0.25, help="Taylor-Green run length (0: skip)")
     ap.add_argument("--tgv-size", type=int, default=256)
+    ap.add_argument("--curv-t", type=float, default=1.0, help="curvilinear vortex run length (0: skip)")
     return ap.parse_args()
 
 
@@ -314,6 +315,8 @@ def run_ours(args, rank, world):
     out["sod_1d"] = run_sod(args)
     if args.tgv_t > 0:
         out["taylor_green"] = run_taylor_green(args)
+    if args.curv_t > 0:
+        out["curvilinear"] = run_curvilinear(args)
     if not args.no_batch:
         out["batched"] ={"fp32flux": run_batched(args, capi.PREC_FP32_FLUX), "fp64": run_batched(args, capi.PREC_FP64)}
         cap = out["batched"]["fp64"]["value"]
@@ -446,6 +449,43 @@ def run_taylor_green(args):
     out["ke_drift_over_ke_change"] = (ke32 - ke64) / abs(ke64 - ke0) if ke64 != ke0 else None
     out["l1_rho_fp32flux_vs_fp64"] = float(np.mean(np.abs(q32[..., 0] - q64[..., 0])))
     out["fp32flux_over_fp64"] = round(out["fp32flux"]["value"] / out["fp64"]["value"], 3)
+    return out
+
+
+def run_curvilinear(args):
+    """The curvilinear path (sfg_set_metrics: per-node metrics, full
+    eigenvector faces along each face normal, FP64) on the headline vortex
+    moved onto a sheared periodic mesh (cases.wavy_vortex, shear amplitude
+    0.3), TENO5 + Rusanov, SSPRK3, CFL 0.4, to t = args.curv_t: device-timed
+    throughput against the uniform FP64 path on the same node count, L1(rho)
+    of both against the exact solution at the nodes' physical coordinates,
+    and the time of one stage with its memory traffic estimate."""
+    import numpy as np
+    from sonicsolver_b200 import capi, cases
+    N = args.size
+    out = {"t_end": args.curv_t, "cells": f"{N}x{N}", "mesh": "x = i h + A sin(2 pi j/N), y = j h + A sin(2 pi i/N)",
+           "amp": 0.3, "recipe": "teno5Rusanov", "precision": "fp64"}
+    for name, case in (("curvilinear", cases.wavy_vortex(N)), ("uniform", cases.isentropic_vortex(N))):
+        s = case.solver(precision=capi.PREC_FP64)
+        stage_ms = s.time_sweeps(1e-4, 0, 10)[0]   # one stage (state restored below)
+        s.upload(np.ascontiguousarray(case.q))
+        st, _ = s.advance(args.curv_t, graph_steps=32)
+        q = s.download().reshape(case.q.shape)
+        ex = cases.vortex_exact(case, st.time)
+        out[name] = {"steps": int(st.steps), "device_s": round(st.device_ms / 1e3, 3),
+                     "value": round(N * N * st.steps / (st.device_ms * 1e-3) / 1e6, 2), "unit": "Mcell-steps/s",
+                     "l1_rho_vs_exact": float(np.mean(np.abs(q[..., 0] - ex[..., 0]))),
+                     "ms_per_stage": None if stage_ms is None else round(float(stage_ms), 4)}
+        s.close()
+    # bytes a curvilinear stage moves per node in 2-D: per axis the face
+    # launch reads the state (40 B) and the face geometry (32 B) and writes
+    # the face flux (40 B); the stage launch reads both axes' fluxes (80 B),
+    # the state, q0 and Jac (88 B) and writes the state (40 B)
+    out["bytes_per_node_stage"] = 2 * (40 + 32 + 40) + 80 + 88 + 40
+    c = out["curvilinear"]
+    if c["ms_per_stage"]:
+        out["hbm_gbs_per_stage"] = round(out["bytes_per_node_stage"] * N * N / (c["ms_per_stage"] * 1e-3) / 1e9, 1)
+    out["curvilinear_over_uniform"] = round(c["value"] / out["uniform"]["value"], 3)
     return out
 
 

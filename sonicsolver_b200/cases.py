@@ -35,6 +35,7 @@ class Case:
     recipe: str = "weno5Rusanov"
     time_recipe: str = "SSPRK3"
     meta: dict = field(default_factory=dict)
+    metrics: np.ndarray | None = None   # curvilinear: (nz, ny, nx, 10) per node (sfg_set_metrics)
 
     @property
     def cells(self) -> int:
@@ -53,6 +54,8 @@ class Case:
         s = capi.Solver(self.dim, self.n, self.h, self.bc_lo, self.bc_hi, recipe=kw.pop("recipe", self.recipe),
                         time_recipe=kw.pop("time_recipe", self.time_recipe), precision=precision,
                         gamma=self.gamma, cfl=kw.pop("cfl", self.cfl), **kw)
+        if self.metrics is not None:
+            s.set_metrics(self.metrics)
         s.upload(np.ascontiguousarray(self.q))
         return s
 
@@ -191,12 +194,45 @@ def isentropic_vortex(N=1024, L=10.0, beta=5.0, gamma=1.4, recipe="teno5Rusanov"
 
 
 def vortex_exact(case: Case, t: float) -> np.ndarray:
-    N = case.n[0]
-    h = case.h[0]
-    x = np.arange(N) * h
-    X, Y = np.meshgrid(x, x, indexing="xy")
+    if "X" in case.meta:   # curvilinear: the nodes' physical coordinates
+        X, Y = case.meta["X"], case.meta["Y"]
+    else:
+        N = case.n[0]
+        h = case.h[0]
+        x = np.arange(N) * h
+        X, Y = np.meshgrid(x, x, indexing="xy")
     rho, u, v, p = vortex_fields(X, Y, t, case.meta["L"], case.meta["beta"], case.gamma)
     return conserved(rho, u, v, 0.0, p, case.gamma)[None]
+
+
+def wavy_vortex(N=1024, L=10.0, amp=0.3, beta=5.0, gamma=1.4, recipe="teno5Rusanov", time_recipe="SSPRK3",
+                cfl=0.4, t_end=10.0) -> Case:
+    """The isentropic vortex on a sheared periodic mesh: node (i, j) sits at
+    x = i h + A sin(2 pi j / N), y = j h + A sin(2 pi i / N), A = amp L / (2 pi)
+    (amp < 1 keeps the map invertible).  Metrics are the map's exact ones
+    with respect to the node index: Jac = 1 / det(dx/di), the xi / eta / zeta
+    vectors the rows of (dx/di)^-1; the z slab is 1 thick."""
+    h = L / N
+    A = amp * L / (2 * math.pi)
+    i = np.arange(N)
+    I, J = np.meshgrid(i, i, indexing="xy")
+    k = 2 * math.pi / N
+    X = I * h + A * np.sin(k * J)
+    Y = J * h + A * np.sin(k * I)
+    dxdj = A * k * np.cos(k * J)
+    dydi = A * k * np.cos(k * I)
+    det = h * h - dxdj * dydi      # times the slab thickness 1
+    M = np.zeros((1, N, N, 10))
+    M[0, ..., 0] = 1.0 / det
+    M[0, ..., 1] = h / det         # xi_x, xi_y (inverse of [[h, dxdj], [dydi, h]])
+    M[0, ..., 2] = -dxdj / det
+    M[0, ..., 4] = -dydi / det     # eta_x, eta_y
+    M[0, ..., 5] = h / det
+    M[0, ..., 9] = 1.0             # zeta_z
+    rho, u, v, p = vortex_fields(X, Y, 0.0, L, beta, gamma)
+    q = conserved(rho, u, v, 0.0, p, gamma)[None]
+    return Case("wavy_vortex", 2, (N, N, 1), (h, h, 1.0), (1, 1, 0), (1, 1, 0), q, gamma, t_end, cfl, recipe,
+                time_recipe, meta={"L": L, "beta": beta, "amp": amp, "X": X, "Y": Y}, metrics=M)
 
 
 # ------------------------------------------------------------ Taylor-Green
