@@ -86,6 +86,114 @@ __device__ __forceinline__ void char_matrix_n(const double (&q)[5], const double
         }
 }
 
+// The same eigen-structure held as its basis scalars: row k of L and column k
+// of R are formed when field k is reconstructed, so the face kernel keeps
+// ~20 values live instead of two 5 x 5 matrices.
+struct CharBasis {
+    double u, v, w, c, H, q2, n1, n2, n3, l1, l2, l3, m1, m2, m3, un, ul, um, b1, b2, x1;
+};
+
+__device__ __forceinline__ void char_basis_n(const double (&q)[5], const double (&n)[3], double gamma, CharBasis& e,
+                                             unsigned& flags) {
+    const double p = pressure_n(q, gamma, flags);
+    const double invR = 1.0 / q[0];
+    e.u = q[1] * invR;
+    e.v = q[2] * invR;
+    e.w = q[3] * invR;
+    e.q2 = e.u * e.u + e.v * e.v + e.w * e.w;
+    e.c = sqrt(gamma * p * invR);
+    e.H = (q[4] + p) * invR;
+    e.n1 = n[0];
+    e.n2 = n[1];
+    e.n3 = n[2];
+    if (fabs(e.n3) <= fabs(e.n2)) {
+        const double ss = sqrt(e.n1 * e.n1 + e.n2 * e.n2);
+        e.l1 = -e.n2 / ss;
+        e.l2 = e.n1 / ss;
+        e.l3 = 0.0;
+    } else {
+        const double ss = sqrt(e.n1 * e.n1 + e.n3 * e.n3);
+        e.l1 = -e.n3 / ss;
+        e.l2 = 0.0;
+        e.l3 = e.n1 / ss;
+    }
+    e.m1 = e.n2 * e.l3 - e.n3 * e.l2;
+    e.m2 = e.n3 * e.l1 - e.n1 * e.l3;
+    e.m3 = e.n1 * e.l2 - e.n2 * e.l1;
+    e.un = e.u * e.n1 + e.v * e.n2 + e.w * e.n3;
+    e.ul = e.u * e.l1 + e.v * e.l2 + e.w * e.l3;
+    e.um = e.u * e.m1 + e.v * e.m2 + e.w * e.m3;
+    e.b1 = (gamma - 1.0) / (e.c * e.c);
+    e.b2 = 0.5 * e.b1;
+    e.x1 = 1.0 / (2.0 * e.c);
+}
+
+// Row K of L (as char_matrix_n builds it).
+template <int K>
+__device__ __forceinline__ void left_row(const CharBasis& e, double (&r)[5]) {
+    if constexpr (K == 0) {
+        r[0] = 1.0 - e.b2 * e.q2; r[1] = e.b1 * e.u; r[2] = e.b1 * e.v; r[3] = e.b1 * e.w; r[4] = -e.b1;
+    } else if constexpr (K == 1) {
+        r[0] = -e.ul; r[1] = e.l1; r[2] = e.l2; r[3] = e.l3; r[4] = 0.0;
+    } else if constexpr (K == 2) {
+        r[0] = -e.um; r[1] = e.m1; r[2] = e.m2; r[3] = e.m3; r[4] = 0.0;
+    } else if constexpr (K == 3) {
+        r[0] = 0.5 * e.b2 * e.q2 + e.x1 * e.un; r[1] = -e.x1 * e.n1 - e.b2 * e.u;
+        r[2] = -e.x1 * e.n2 - e.b2 * e.v; r[3] = -e.x1 * e.n3 - e.b2 * e.w; r[4] = e.b2;
+    } else {
+        r[0] = 0.5 * e.b2 * e.q2 - e.x1 * e.un; r[1] = e.x1 * e.n1 - e.b2 * e.u;
+        r[2] = e.x1 * e.n2 - e.b2 * e.v; r[3] = e.x1 * e.n3 - e.b2 * e.w; r[4] = e.b2;
+    }
+}
+
+// Column K of R.
+template <int K>
+__device__ __forceinline__ void right_col(const CharBasis& e, double (&r)[5]) {
+    if constexpr (K == 0) {
+        r[0] = 1.0; r[1] = e.u; r[2] = e.v; r[3] = e.w; r[4] = 0.5 * e.q2;
+    } else if constexpr (K == 1) {
+        r[0] = 0.0; r[1] = e.l1; r[2] = e.l2; r[3] = e.l3; r[4] = e.ul;
+    } else if constexpr (K == 2) {
+        r[0] = 0.0; r[1] = e.m1; r[2] = e.m2; r[3] = e.m3; r[4] = e.um;
+    } else if constexpr (K == 3) {
+        r[0] = 1.0; r[1] = e.u - e.c * e.n1; r[2] = e.v - e.c * e.n2; r[3] = e.w - e.c * e.n3; r[4] = e.H - e.c * e.un;
+    } else {
+        r[0] = 1.0; r[1] = e.u + e.c * e.n1; r[2] = e.v + e.c * e.n2; r[3] = e.w + e.c * e.n3; r[4] = e.H + e.c * e.un;
+    }
+}
+
+// Field K of the characteristic reconstruction: project the stencil on row
+// K, reconstruct both sides, add column K times the results to qL / qR.
+template <int K, int SCHEME, int NST, int W>
+__device__ __forceinline__ void recon_field(const CharBasis& e, const double (&st)[NST][5], double (&qL)[5],
+                                            double (&qR)[5], unsigned& flags, unsigned& cut) {
+    double row[5];
+    left_row<K>(e, row);
+    double ch[NST];
+#pragma unroll
+    for (int s = 0; s < NST; ++s) {
+        double acc = 0.0;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) acc += row[k] * st[s][k];
+        ch[s] = acc;
+    }
+    double sl[8], sr[8];
+#pragma unroll
+    for (int s = 0; s < W; ++s) {
+        sl[s] = ch[s];
+        sr[s] = ch[NST - 1 - s];
+    }
+    const double wl = recon_core<SCHEME, double>(sl, flags, cut);
+    const double wr = recon_core<SCHEME, double>(sr, flags, cut);
+    double col[5];
+    right_col<K>(e, col);
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+        qL[r] += col[r] * wl;
+        qR[r] += col[r] * wr;
+    }
+}
+
 __device__ __forceinline__ void gemv5(const double (&M)[5][5], const double (&x)[5], double (&y)[5]) {
 #pragma unroll
     for (int r = 0; r < 5; ++r) {
@@ -305,7 +413,7 @@ __global__ void __launch_bounds__(256) curv_geometry_kernel(GridView g, const do
 // range.  F (times the face area) goes to fl[axis][v] at the lower node.
 // ---------------------------------------------------------------------------
 template <int SCHEME, int FLUX>
-__global__ void __launch_bounds__(128) curv_face_kernel(GridView g, StageView sv, int axis, double* fl) {
+__global__ void __launch_bounds__(128, 4) curv_face_kernel(GridView g, StageView sv, int axis, double* fl) {
     if (sv.require_active && !sv.clock->active) return;
     constexpr int NST = SchemeInfo<SCHEME>::NST, W = SchemeInfo<SCHEME>::W;
     const int a = axis;
@@ -344,27 +452,15 @@ __global__ void __launch_bounds__(128) curv_face_kernel(GridView g, StageView sv
         double qavg[5];
 #pragma unroll
         for (int v = 0; v < 5; ++v) qavg[v] = 0.5 * (st[NST / 2 - 1][v] + st[NST / 2][v]);
-        double L[5][5], R[5][5];
-        char_matrix_n(qavg, n, g.gamma, L, R, flags);
-        double ch[NST][5];
-#pragma unroll
-        for (int s = 0; s < NST; ++s) gemv5(L, st[s], ch[s]);
-        double wl[5], wr[5];
-#pragma unroll
-        for (int v = 0; v < 5; ++v) {
-            double sl[8], sr[8];
-#pragma unroll
-            for (int s = 0; s < W; ++s) {
-                sl[s] = ch[s][v];
-                sr[s] = ch[NST - 1 - s][v];
-            }
-            wl[v] = recon_core<SCHEME, double>(sl, flags, cut);
-            wr[v] = recon_core<SCHEME, double>(sr, flags, cut);
-        }
+        CharBasis e;
+        char_basis_n(qavg, n, g.gamma, e, flags);
+        double qL[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, qR[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, F[5];
+        recon_field<0, SCHEME, NST, W>(e, st, qL, qR, flags, cut);
+        recon_field<1, SCHEME, NST, W>(e, st, qL, qR, flags, cut);
+        recon_field<2, SCHEME, NST, W>(e, st, qL, qR, flags, cut);
+        recon_field<3, SCHEME, NST, W>(e, st, qL, qR, flags, cut);
+        recon_field<4, SCHEME, NST, W>(e, st, qL, qR, flags, cut);
         if (SCHEME == TENO5) cores += 10;
-        double qL[5], qR[5], F[5];
-        gemv5(R, wl, qL);
-        gemv5(R, wr, qR);
         flux_n<FLUX>(qL, qR, n, g.gamma, F, flags);
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
