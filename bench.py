@@ -456,17 +456,21 @@ def run_curvilinear(args):
     """The curvilinear path (sfg_set_metrics: per-node metrics, full
     eigenvector faces along each face normal, FP64) on the headline vortex
     moved onto a sheared periodic mesh (cases.wavy_vortex, shear amplitude
-    0.3), TENO5 + Rusanov, SSPRK3, CFL 0.4, to t = args.curv_t: device-timed
-    throughput against the uniform FP64 path on the same node count, L1(rho)
-    of both against the exact solution at the nodes' physical coordinates,
-    and the time of one stage with its memory traffic estimate."""
+    0.3), TENO5 + Rusanov, SSPRK3, CFL 0.4, to t = args.curv_t, in FP64 and
+    in FP32-flux / FP64-state: device-timed throughput against the uniform
+    FP64 path on the same node count, L1(rho) of each against the exact
+    solution at the nodes' physical coordinates, and the time of one stage
+    with its memory traffic estimate."""
     import numpy as np
     from sonicsolver_b200 import capi, cases
     N = args.size
     out = {"t_end": args.curv_t, "cells": f"{N}x{N}", "mesh": "x = i h + A sin(2 pi j/N), y = j h + A sin(2 pi i/N)",
-           "amp": 0.3, "recipe": "teno5Rusanov", "precision": "fp64"}
-    for name, case in (("curvilinear", cases.wavy_vortex(N)), ("uniform", cases.isentropic_vortex(N))):
-        s = case.solver(precision=capi.PREC_FP64)
+           "amp": 0.3, "recipe": "teno5Rusanov"}
+    runs = (("curvilinear", cases.wavy_vortex(N), capi.PREC_FP64),
+            ("curvilinear_fp32flux", cases.wavy_vortex(N), capi.PREC_FP32_FLUX),
+            ("uniform", cases.isentropic_vortex(N), capi.PREC_FP64))
+    for name, case, prec in runs:
+        s = case.solver(precision=prec)
         stage_ms = s.time_sweeps(1e-4, 0, 10)[0]   # one stage (state restored below)
         s.upload(np.ascontiguousarray(case.q))
         st, _ = s.advance(args.curv_t, graph_steps=32)
@@ -486,6 +490,9 @@ def run_curvilinear(args):
     if c["ms_per_stage"]:
         out["hbm_gbs_per_stage"] = round(out["bytes_per_node_stage"] * N * N / (c["ms_per_stage"] * 1e-3) / 1e9, 1)
     out["curvilinear_over_uniform"] = round(c["value"] / out["uniform"]["value"], 3)
+    c32 = out["curvilinear_fp32flux"]
+    out["fp32flux_over_fp64"] = round(c32["value"] / c["value"], 3)
+    out["l1_ratio_fp32flux_over_fp64"] = c32["l1_rho_vs_exact"] / c["l1_rho_vs_exact"]
     return out
 
 

@@ -221,8 +221,8 @@ int sfg_apply_boundary(sfg_solver s);
  * 0.5 (m_i / Jac_i + m_i+1 / Jac_i+1) as normal and area
  * (SF_canonicalFace.h:56-118), the residual is Jac_node * sum_d dF_d, and the
  * CFL rate uses the node's metric vectors; the grid's h[] is no longer read
- * by the operator.  FP64; all fluxes but Lax-Wendroff (which needs node
- * coordinates). */
+ * by the operator.  FP64 with all fluxes but Lax-Wendroff (which needs node
+ * coordinates); FP32-flux with Rusanov and Roe. */
 int sfg_set_metrics(sfg_solver s, const double* metrics, int layout);
 /* Host <-> device copies of the conserved state (pageable or pinned host
  * memory; synchronous with respect to the solver's stream). Upload resets the

@@ -18,6 +18,9 @@
 //
 // FP64.  Reads per node and stage: the state (stencils, mostly from L2), 4
 // doubles of face geometry per axis, Jac; writes 5 face fluxes per axis.
+#include <algorithm>
+#include <type_traits>
+
 #include "sfg_internal.h"
 #include "sfg_stage.cuh"
 
@@ -89,32 +92,35 @@ __device__ __forceinline__ void char_matrix_n(const double (&q)[5], const double
 // The same eigen-structure held as its basis scalars: row k of L and column k
 // of R are formed when field k is reconstructed, so the face kernel keeps
 // ~20 values live instead of two 5 x 5 matrices.
-struct CharBasis {
-    double u, v, w, c, H, q2, n1, n2, n3, l1, l2, l3, m1, m2, m3, un, ul, um, b1, b2, x1;
+template <typename T>
+struct CharBasisT {
+    T u, v, w, c, H, q2, n1, n2, n3, l1, l2, l3, m1, m2, m3, un, ul, um, b1, b2, x1;
 };
+using CharBasis = CharBasisT<double>;
 
-__device__ __forceinline__ void char_basis_n(const double (&q)[5], const double (&n)[3], double gamma, CharBasis& e,
-                                             unsigned& flags) {
-    const double p = pressure_n(q, gamma, flags);
-    const double invR = 1.0 / q[0];
+// The basis of the state q with pressure p along the unit normal n.
+template <typename T>
+__device__ __forceinline__ void char_basis_p(const T (&q)[5], T p, const T (&n)[3], T gamma, CharBasisT<T>& e) {
+    const T one = T(1), half = T(0.5);
+    const T invR = one / q[0];
     e.u = q[1] * invR;
     e.v = q[2] * invR;
     e.w = q[3] * invR;
     e.q2 = e.u * e.u + e.v * e.v + e.w * e.w;
-    e.c = sqrt(gamma * p * invR);
+    e.c = sqrt_<T>(gamma * p * invR);
     e.H = (q[4] + p) * invR;
     e.n1 = n[0];
     e.n2 = n[1];
     e.n3 = n[2];
     if (fabs(e.n3) <= fabs(e.n2)) {
-        const double ss = sqrt(e.n1 * e.n1 + e.n2 * e.n2);
+        const T ss = sqrt_<T>(e.n1 * e.n1 + e.n2 * e.n2);
         e.l1 = -e.n2 / ss;
         e.l2 = e.n1 / ss;
-        e.l3 = 0.0;
+        e.l3 = T(0);
     } else {
-        const double ss = sqrt(e.n1 * e.n1 + e.n3 * e.n3);
+        const T ss = sqrt_<T>(e.n1 * e.n1 + e.n3 * e.n3);
         e.l1 = -e.n3 / ss;
-        e.l2 = 0.0;
+        e.l2 = T(0);
         e.l3 = e.n1 / ss;
     }
     e.m1 = e.n2 * e.l3 - e.n3 * e.l2;
@@ -123,70 +129,77 @@ __device__ __forceinline__ void char_basis_n(const double (&q)[5], const double 
     e.un = e.u * e.n1 + e.v * e.n2 + e.w * e.n3;
     e.ul = e.u * e.l1 + e.v * e.l2 + e.w * e.l3;
     e.um = e.u * e.m1 + e.v * e.m2 + e.w * e.m3;
-    e.b1 = (gamma - 1.0) / (e.c * e.c);
-    e.b2 = 0.5 * e.b1;
-    e.x1 = 1.0 / (2.0 * e.c);
+    e.b1 = (gamma - one) / (e.c * e.c);
+    e.b2 = half * e.b1;
+    e.x1 = one / (T(2) * e.c);
+}
+
+__device__ __forceinline__ void char_basis_n(const double (&q)[5], const double (&n)[3], double gamma, CharBasis& e,
+                                             unsigned& flags) {
+    char_basis_p<double>(q, pressure_n(q, gamma, flags), n, gamma, e);
 }
 
 // Row K of L (as char_matrix_n builds it).
-template <int K>
-__device__ __forceinline__ void left_row(const CharBasis& e, double (&r)[5]) {
+template <int K, typename T>
+__device__ __forceinline__ void left_row(const CharBasisT<T>& e, T (&r)[5]) {
+    const T half = T(0.5), zero = T(0), one = T(1);
     if constexpr (K == 0) {
-        r[0] = 1.0 - e.b2 * e.q2; r[1] = e.b1 * e.u; r[2] = e.b1 * e.v; r[3] = e.b1 * e.w; r[4] = -e.b1;
+        r[0] = one - e.b2 * e.q2; r[1] = e.b1 * e.u; r[2] = e.b1 * e.v; r[3] = e.b1 * e.w; r[4] = -e.b1;
     } else if constexpr (K == 1) {
-        r[0] = -e.ul; r[1] = e.l1; r[2] = e.l2; r[3] = e.l3; r[4] = 0.0;
+        r[0] = -e.ul; r[1] = e.l1; r[2] = e.l2; r[3] = e.l3; r[4] = zero;
     } else if constexpr (K == 2) {
-        r[0] = -e.um; r[1] = e.m1; r[2] = e.m2; r[3] = e.m3; r[4] = 0.0;
+        r[0] = -e.um; r[1] = e.m1; r[2] = e.m2; r[3] = e.m3; r[4] = zero;
     } else if constexpr (K == 3) {
-        r[0] = 0.5 * e.b2 * e.q2 + e.x1 * e.un; r[1] = -e.x1 * e.n1 - e.b2 * e.u;
+        r[0] = half * e.b2 * e.q2 + e.x1 * e.un; r[1] = -e.x1 * e.n1 - e.b2 * e.u;
         r[2] = -e.x1 * e.n2 - e.b2 * e.v; r[3] = -e.x1 * e.n3 - e.b2 * e.w; r[4] = e.b2;
     } else {
-        r[0] = 0.5 * e.b2 * e.q2 - e.x1 * e.un; r[1] = e.x1 * e.n1 - e.b2 * e.u;
+        r[0] = half * e.b2 * e.q2 - e.x1 * e.un; r[1] = e.x1 * e.n1 - e.b2 * e.u;
         r[2] = e.x1 * e.n2 - e.b2 * e.v; r[3] = e.x1 * e.n3 - e.b2 * e.w; r[4] = e.b2;
     }
 }
 
 // Column K of R.
-template <int K>
-__device__ __forceinline__ void right_col(const CharBasis& e, double (&r)[5]) {
+template <int K, typename T>
+__device__ __forceinline__ void right_col(const CharBasisT<T>& e, T (&r)[5]) {
+    const T half = T(0.5), zero = T(0), one = T(1);
     if constexpr (K == 0) {
-        r[0] = 1.0; r[1] = e.u; r[2] = e.v; r[3] = e.w; r[4] = 0.5 * e.q2;
+        r[0] = one; r[1] = e.u; r[2] = e.v; r[3] = e.w; r[4] = half * e.q2;
     } else if constexpr (K == 1) {
-        r[0] = 0.0; r[1] = e.l1; r[2] = e.l2; r[3] = e.l3; r[4] = e.ul;
+        r[0] = zero; r[1] = e.l1; r[2] = e.l2; r[3] = e.l3; r[4] = e.ul;
     } else if constexpr (K == 2) {
-        r[0] = 0.0; r[1] = e.m1; r[2] = e.m2; r[3] = e.m3; r[4] = e.um;
+        r[0] = zero; r[1] = e.m1; r[2] = e.m2; r[3] = e.m3; r[4] = e.um;
     } else if constexpr (K == 3) {
-        r[0] = 1.0; r[1] = e.u - e.c * e.n1; r[2] = e.v - e.c * e.n2; r[3] = e.w - e.c * e.n3; r[4] = e.H - e.c * e.un;
+        r[0] = one; r[1] = e.u - e.c * e.n1; r[2] = e.v - e.c * e.n2; r[3] = e.w - e.c * e.n3; r[4] = e.H - e.c * e.un;
     } else {
-        r[0] = 1.0; r[1] = e.u + e.c * e.n1; r[2] = e.v + e.c * e.n2; r[3] = e.w + e.c * e.n3; r[4] = e.H + e.c * e.un;
+        r[0] = one; r[1] = e.u + e.c * e.n1; r[2] = e.v + e.c * e.n2; r[3] = e.w + e.c * e.n3; r[4] = e.H + e.c * e.un;
     }
 }
 
 // Field K of the characteristic reconstruction: project the stencil on row
 // K, reconstruct both sides, add column K times the results to qL / qR.
-template <int K, int SCHEME, int NST, int W>
-__device__ __forceinline__ void recon_field(const CharBasis& e, const double (&st)[NST][5], double (&qL)[5],
-                                            double (&qR)[5], unsigned& flags, unsigned& cut) {
-    double row[5];
-    left_row<K>(e, row);
-    double ch[NST];
+template <int K, int SCHEME, int NST, int W, typename T>
+__device__ __forceinline__ void recon_field(const CharBasisT<T>& e, const T (&st)[NST][5], T (&qL)[5], T (&qR)[5],
+                                            unsigned& flags, unsigned& cut) {
+    T row[5];
+    left_row<K, T>(e, row);
+    T ch[NST];
 #pragma unroll
     for (int s = 0; s < NST; ++s) {
-        double acc = 0.0;
+        T acc = T(0);
 #pragma unroll
         for (int k = 0; k < 5; ++k) acc += row[k] * st[s][k];
         ch[s] = acc;
     }
-    double sl[8], sr[8];
+    T sl[8], sr[8];
 #pragma unroll
     for (int s = 0; s < W; ++s) {
         sl[s] = ch[s];
         sr[s] = ch[NST - 1 - s];
     }
-    const double wl = recon_core<SCHEME, double>(sl, flags, cut);
-    const double wr = recon_core<SCHEME, double>(sr, flags, cut);
-    double col[5];
-    right_col<K>(e, col);
+    const T wl = recon_core<SCHEME, T>(sl, flags, cut);
+    const T wr = recon_core<SCHEME, T>(sr, flags, cut);
+    T col[5];
+    right_col<K, T>(e, col);
 #pragma unroll
     for (int r = 0; r < 5; ++r) {
         qL[r] += col[r] * wl;
@@ -365,6 +378,108 @@ __device__ __forceinline__ void flux_n(const double (&qL)[5], const double (&qR)
     }
 }
 
+// ---- FP32-flux form -------------------------------------------------------
+// A face's stencil as FP32 deviations d = q - q_ref from its left node q_ref
+// (FP64); the reconstruction runs on the deviations (projections are linear,
+// the WENO / TENO cores shift invariant) and the face flux comes back as the
+// deviation F(q) - F(q_ref) in algebra that never subtracts large terms; the
+// FP64 flux of q_ref along the face normal is added in FP64.
+
+// Physical flux along the unit normal n of q = q_ref + d, as the deviation
+// F(q) - F(q_ref):
+//   du = (d_m - u_ref d_rho) / rho,  dp = (gamma - 1)(d_E - (m_ref.du + d_m.u) / 2)
+//   dF_rho = d_m.n,  dF_m = m_ref du_n + d_m u_n + dp n,  dF_E = (E_ref + p_ref) du_n + (d_E + dp) u_n.
+__device__ __forceinline__ void phys_flux_dev_n(const Ref32& r, const float (&d)[5], const float (&n)[3], float gamma,
+                                                float (&F)[5], float& un, float& c, float& p_out, unsigned& flags) {
+    const float rho = r.q[0] + d[0];
+    const float irho = rcp_approx(rho);
+    float du[3], u[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        du[k] = (d[1 + k] - r.u[k] * d[0]) * irho;
+        u[k] = r.u[k] + du[k];
+    }
+    const float dmu = r.q[1] * du[0] + r.q[2] * du[1] + r.q[3] * du[2] + d[1] * u[0] + d[2] * u[1] + d[3] * u[2];
+    const float dp = (gamma - 1.f) * (d[4] - 0.5f * dmu);
+    const float p = r.p + dp;
+    if (!(rho > 0.f)) flags |= FLAG_DENSITY;
+    if (!(p > 0.f)) flags |= FLAG_PRESSURE;
+    const float dun = du[0] * n[0] + du[1] * n[1] + du[2] * n[2];
+    un = u[0] * n[0] + u[1] * n[1] + u[2] * n[2];
+    F[0] = d[1] * n[0] + d[2] * n[1] + d[3] * n[2];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) F[1 + k] = r.q[1 + k] * dun + d[1 + k] * un + dp * n[k];
+    F[4] = (r.q[4] + r.p) * dun + (d[4] + dp) * un;
+    c = sqrtf(gamma * p * irho);
+    p_out = p;
+}
+
+template <int FLUX>
+__device__ __forceinline__ void flux_dev_n(const Ref32& r, const float (&dL)[5], const float (&dR)[5],
+                                           const float (&n)[3], float gamma, float (&F)[5], unsigned& flags) {
+    float fL[5], fR[5], unL, unR, cL, cR, pL, pR;
+    phys_flux_dev_n(r, dL, n, gamma, fL, unL, cL, pL, flags);
+    phys_flux_dev_n(r, dR, n, gamma, fR, unR, cR, pR, flags);
+    if constexpr (FLUX == RUSANOV) {
+        const float hl = 0.5f * fmaxf(fabsf(unL) + cL, fabsf(unR) + cR);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) F[v] = 0.5f * (fL[v] + fR[v]) - hl * (dR[v] - dL[v]);
+    } else {
+        // Roe: average and eigen-structure from the absolute states, the
+        // dissipation from the jump dR - dL (SF_roe.cpp:10-90)
+        float qL[5], qR[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            qL[v] = r.q[v] + dL[v];
+            qR[v] = r.q[v] + dR[v];
+        }
+        const float gm1 = gamma - 1.f;
+        const float iL = rcp_approx(qL[0]), iR = rcp_approx(qR[0]);
+        const float hL = (qL[4] + pL) * iL, hR = (qR[4] + pR) * iR;
+        const float sL = sqrtf(qL[0]), sR = sqrtf(qR[0]);
+        const float iS = rcp_approx(sL + sR);
+        const float ur = (sL * qL[1] * iL + sR * qR[1] * iR) * iS;
+        const float vr = (sL * qL[2] * iL + sR * qR[2] * iR) * iS;
+        const float wr = (sL * qL[3] * iL + sR * qR[3] * iR) * iS;
+        const float hr = (sL * hL + sR * hR) * iS;
+        const float q2 = ur * ur + vr * vr + wr * wr;
+        const float a2 = gm1 * (hr - 0.5f * q2);
+        if (!(a2 > 0.f) || !isfinite(a2)) flags |= FLAG_ROE_SOUND;
+        const float rr = sL * sR;
+        const float qRoe[5] = {rr, rr * ur, rr * vr, rr * wr, rr * (0.5f * q2 + __fdividef(a2, gm1))};
+        // the Roe state's own pressure, (gamma - 1)(E - rho q2 / 2) = rho a2, as
+        // the FP64 path closes it for the eigenvectors
+        CharBasisT<float> e;
+        char_basis_p<float>(qRoe, rr * a2, n, gamma, e);
+        const float a = sqrtf(a2);
+        const float unr = ur * n[0] + vr * n[1] + wr * n[2];
+        const float lam[5] = {unr, unr, unr, unr + a, unr - a};
+        const float delta = 0.1f * a;
+        float dq[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) dq[v] = dR[v] - dL[v];
+        float diss[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+        auto wave = [&](auto kc) {
+            constexpr int K = decltype(kc)::value;
+            float row[5], col[5];
+            left_row<K, float>(e, row);
+            right_col<K, float>(e, col);
+            const float alpha = row[0] * dq[0] + row[1] * dq[1] + row[2] * dq[2] + row[3] * dq[3] + row[4] * dq[4];
+            const float val = fabsf(lam[K]);
+            const float ab = val < 2.f * delta ? 0.5f * (val * val * rcp_approx(2.f * delta) + delta) : val;
+#pragma unroll
+            for (int v = 0; v < 5; ++v) diss[v] += col[v] * (ab * alpha);
+        };
+        wave(std::integral_constant<int, 0>{});
+        wave(std::integral_constant<int, 1>{});
+        wave(std::integral_constant<int, 2>{});
+        wave(std::integral_constant<int, 3>{});
+        wave(std::integral_constant<int, 4>{});
+#pragma unroll
+        for (int v = 0; v < 5; ++v) F[v] = 0.5f * (fL[v] + fR[v] - diss[v]);
+    }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -472,6 +587,81 @@ __global__ void __launch_bounds__(128, 4) curv_face_kernel(GridView g, StageView
     flush_status(sv, flags, cores, cut);
 }
 
+// The FP32-flux / FP64-state form of curv_face_kernel (Rusanov and Roe).
+template <int SCHEME, int FLUX>
+__global__ void __launch_bounds__(128, 4) curv_face_f32_kernel(GridView g, StageView sv, int axis, double* fl) {
+    if (sv.require_active && !sv.clock->active) return;
+    constexpr int NST = SchemeInfo<SCHEME>::NST, W = SchemeInfo<SCHEME>::W, CL = NST / 2 - 1;
+    const int a = axis;
+    int base[3], span[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const bool per = d < g.dim && g.bc_lo[d] == BC_PERIODIC;
+        base[d] = d == a ? (per ? 0 : g.lo[d] - 1) : g.lo[d];
+        span[d] = d == a ? (per ? g.n[d] : g.hi[d] - g.lo[d] + 1) : g.hi[d] - g.lo[d];
+    }
+    const long long total = (long long)span[0] * span[1] * span[2];
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    unsigned flags = 0, cut = 0, cores = 0;
+    if (t < total) {
+        int c[3];
+        long long r = t;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            c[d] = base[d] + (int)(r % span[d]);
+            r /= span[d];
+        }
+        const long long vs = g.vs;
+        long long node[NST];
+#pragma unroll
+        for (int s = 0; s < NST; ++s) {
+            int cc[3] = {c[0], c[1], c[2]};
+            cc[a] = map_index(c[a] - CL + s, g.n[a], g.bc_lo[a], g.bc_hi[a]);
+            node[s] = ((long long)cc[2] * g.n[1] + cc[1]) * g.n[0] + cc[0];
+        }
+        double qref[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) qref[v] = sv.qs[v * vs + node[CL]];
+        float d[NST][5];
+#pragma unroll
+        for (int s = 0; s < NST; ++s)
+#pragma unroll
+            for (int v = 0; v < 5; ++v) d[s][v] = float(sv.qs[v * vs + node[s]] - qref[v]);
+        const Ref32 ref = make_ref32(qref, g.gamma);
+        const long long face = ((long long)c[2] * g.n[1] + c[1]) * g.n[0] + c[0];
+        const double* gm = g.geom[a];
+        const double n64[3] = {gm[face], gm[vs + face], gm[2 * vs + face]};
+        const double area = gm[3 * vs + face];
+        const float n[3] = {float(n64[0]), float(n64[1]), float(n64[2])};
+        const float gamma = float(g.gamma);
+        // eigen basis at the face average (q_ref + d_CL+1 / 2)
+        float qa[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) qa[v] = ref.q[v] + 0.5f * d[CL + 1][v];
+        const float pa = (gamma - 1.f) * (qa[4] - 0.5f * (qa[1] * qa[1] + qa[2] * qa[2] + qa[3] * qa[3]) / qa[0]);
+        if (!(qa[0] > 0.f) || !(pa > 0.f)) flags |= FLAG_PRESSURE;
+        CharBasisT<float> e;
+        char_basis_p<float>(qa, pa, n, gamma, e);
+        float dL[5] = {0.f, 0.f, 0.f, 0.f, 0.f}, dR[5] = {0.f, 0.f, 0.f, 0.f, 0.f}, F[5];
+        recon_field<0, SCHEME, NST, W, float>(e, d, dL, dR, flags, cut);
+        recon_field<1, SCHEME, NST, W, float>(e, d, dL, dR, flags, cut);
+        recon_field<2, SCHEME, NST, W, float>(e, d, dL, dR, flags, cut);
+        recon_field<3, SCHEME, NST, W, float>(e, d, dL, dR, flags, cut);
+        recon_field<4, SCHEME, NST, W, float>(e, d, dL, dR, flags, cut);
+        if (SCHEME == TENO5) cores += 10;
+        flux_dev_n<FLUX>(ref, dL, dR, n, gamma, F, flags);
+        double fref[5];
+        euler_flux_n(qref, n64, g.gamma, fref, flags);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            const double x = (fref[v] + double(F[v])) * area;
+            if (!isfinite(x)) flags |= FLAG_NONFINITE;
+            fl[((long long)a * 5 + v) * vs + face] = x;
+        }
+    }
+    flush_status(sv, flags, cores, cut);
+}
+
 // Divergence and stage update of the solved nodes.
 __global__ void __launch_bounds__(256) curv_stage_kernel(GridView g, StageView sv, const double* __restrict__ fl) {
     if (sv.require_active && !sv.clock->active) return;
@@ -523,9 +713,25 @@ static cudaError_t launch_curv_faces(const GridView& g, const StageView& sv, int
     return cudaGetLastError();
 }
 
+template <int SCHEME, int FLUX>
+static cudaError_t launch_curv_faces32(const GridView& g, const StageView& sv, int axis, double* fl, cudaStream_t st) {
+    long long total = 1;
+    for (int d = 0; d < 3; ++d) {
+        const bool per = d < g.dim && g.bc_lo[d] == BC_PERIODIC;
+        total *= d == axis ? (per ? g.n[d] : g.hi[d] - g.lo[d] + 1) : g.hi[d] - g.lo[d];
+    }
+    curv_face_f32_kernel<SCHEME, FLUX><<<(unsigned)((total + 127) / 128), 128, 0, st>>>(g, sv, axis, fl);
+    return cudaGetLastError();
+}
+
 template <int SCHEME>
-static cudaError_t launch_curv_faces_f(int flux, const GridView& g, const StageView& sv, int axis, double* fl,
-                                       cudaStream_t st) {
+static cudaError_t launch_curv_faces_f(int flux, int prec64, const GridView& g, const StageView& sv, int axis,
+                                       double* fl, cudaStream_t st) {
+    if (!prec64) {
+        if (flux == RUSANOV) return launch_curv_faces32<SCHEME, RUSANOV>(g, sv, axis, fl, st);
+        if (flux == ROE) return launch_curv_faces32<SCHEME, ROE>(g, sv, axis, fl, st);
+        return cudaErrorInvalidValue;
+    }
     switch (flux) {
     case RUSANOV: return launch_curv_faces<SCHEME, RUSANOV>(g, sv, axis, fl, st);
     case ROE: return launch_curv_faces<SCHEME, ROE>(g, sv, axis, fl, st);
@@ -538,15 +744,15 @@ static cudaError_t launch_curv_faces_f(int flux, const GridView& g, const StageV
 // One stage on a curvilinear grid: the face fluxes of every active axis, then
 // the divergence and stage update (sv.mode: MODE_FINAL with optional
 // MODE_RESIDUAL / MODE_CFL).
-cudaError_t launch_curv_stage(int scheme, int flux, const GridView& g, const StageView& sv, double* fl,
+cudaError_t launch_curv_stage(int scheme, int flux, int prec64, const GridView& g, const StageView& sv, double* fl,
                               cudaStream_t st) {
     for (int axis = 0; axis < g.dim; ++axis) {
         cudaError_t e;
         switch (scheme) {
-        case WENO5: e = launch_curv_faces_f<WENO5>(flux, g, sv, axis, fl, st); break;
-        case TENO5: e = launch_curv_faces_f<TENO5>(flux, g, sv, axis, fl, st); break;
-        case WENO3: e = launch_curv_faces_f<WENO3>(flux, g, sv, axis, fl, st); break;
-        case WENO7: e = launch_curv_faces_f<WENO7>(flux, g, sv, axis, fl, st); break;
+        case WENO5: e = launch_curv_faces_f<WENO5>(flux, prec64, g, sv, axis, fl, st); break;
+        case TENO5: e = launch_curv_faces_f<TENO5>(flux, prec64, g, sv, axis, fl, st); break;
+        case WENO3: e = launch_curv_faces_f<WENO3>(flux, prec64, g, sv, axis, fl, st); break;
+        case WENO7: e = launch_curv_faces_f<WENO7>(flux, prec64, g, sv, axis, fl, st); break;
         default: return cudaErrorInvalidValue;
         }
         if (e != cudaSuccess) return e;

@@ -41,7 +41,7 @@ cudaError_t launch_law_fill(const GridView& g, const LawView& lv, const double* 
                             int require_active, unsigned* flags, cudaStream_t st);
 cudaError_t launch_curv_geometry(const GridView& g, const double* nm, double* const geom[3], unsigned* flags,
                                  cudaStream_t st);
-cudaError_t launch_curv_stage(int scheme, int flux, const GridView& g, const StageView& sv, double* fl,
+cudaError_t launch_curv_stage(int scheme, int flux, int prec64, const GridView& g, const StageView& sv, double* fl,
                               cudaStream_t st);
 cudaError_t launch_teno_flips(const GridView& g, const double* q, unsigned long long* out, cudaStream_t st);
 }  // namespace sfg
@@ -433,7 +433,8 @@ int enqueue_stage(sfg_solver_s* s, int stage, bool residual_only, bool require_a
     }
     if (s->gv.curv) {  // per-face geometry: face-flux launches per axis, then the stage
         sv.mode = MODE_FINAL | (residual_only ? MODE_RESIDUAL : 0) | cfl_bit_all;
-        CUDA_TRY(launch_curv_stage(s->recipe->scheme, s->recipe->flux, s->gv, sv, s->face_flux, s->stream));
+        CUDA_TRY(launch_curv_stage(s->recipe->scheme, s->recipe->flux, s->num.precision == SFG_PREC_FP64, s->gv, sv,
+                                   s->face_flux, s->stream));
         return SFG_OK;
     }
     const int cfl_bit = cfl && !residual_only ? MODE_CFL : 0;
@@ -765,7 +766,6 @@ static void metrics_to_device(const sfg_solver_s* s, const double* host, int lay
 int sfg_set_metrics(sfg_solver s, const double* host, int layout) {
     if (!s || !host) return fail(SFG_ERR_ARG, "null argument");
     if (layout != SFG_LAYOUT_NODES && layout != SFG_LAYOUT_FIELD) return fail(SFG_ERR_ARG, "unknown layout %d", layout);
-    if (s->num.precision != SFG_PREC_FP64) return fail(SFG_ERR_ARG, "curvilinear grids run in FP64");
     if (s->recipe->flux == LAXW)
         return fail(SFG_ERR_ARG, "%s: Lax-Wendroff needs node coordinates; curvilinear grids take the other fluxes",
                     s->recipe->name);
