@@ -23,6 +23,7 @@
 
 #include "sfg_internal.h"
 #include "sfg_stage.cuh"
+#include "sfg_tile.cuh"
 
 namespace sfg {
 
@@ -480,6 +481,30 @@ __device__ __forceinline__ void flux_dev_n(const Ref32& r, const float (&dL)[5],
     }
 }
 
+// One face in the FP32-flux form: stencil deviations d from the reference
+// ref, eigen basis at the face average, characteristic reconstruction, flux
+// deviation along the unit normal n (per unit area).
+template <int SCHEME, int FLUX>
+__device__ __forceinline__ void curv_face_dev32(const float (&d)[SchemeInfo<SCHEME>::NST][5], const Ref32& ref,
+                                                const float (&n)[3], float gamma, float (&F)[5], unsigned& flags,
+                                                unsigned& cut) {
+    constexpr int NST = SchemeInfo<SCHEME>::NST, W = SchemeInfo<SCHEME>::W, CL = NST / 2 - 1;
+    float qa[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) qa[v] = ref.q[v] + 0.5f * (d[CL][v] + d[CL + 1][v]);
+    const float pa = (gamma - 1.f) * (qa[4] - 0.5f * (qa[1] * qa[1] + qa[2] * qa[2] + qa[3] * qa[3]) / qa[0]);
+    if (!(qa[0] > 0.f) || !(pa > 0.f)) flags |= FLAG_PRESSURE;
+    CharBasisT<float> e;
+    char_basis_p<float>(qa, pa, n, gamma, e);
+    float dL[5] = {0.f, 0.f, 0.f, 0.f, 0.f}, dR[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+    recon_field<0, SCHEME, NST, W, float>(e, d, dL, dR, flags, cut);
+    recon_field<1, SCHEME, NST, W, float>(e, d, dL, dR, flags, cut);
+    recon_field<2, SCHEME, NST, W, float>(e, d, dL, dR, flags, cut);
+    recon_field<3, SCHEME, NST, W, float>(e, d, dL, dR, flags, cut);
+    recon_field<4, SCHEME, NST, W, float>(e, d, dL, dR, flags, cut);
+    flux_dev_n<FLUX>(ref, dL, dR, n, gamma, F, flags);
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -591,7 +616,7 @@ __global__ void __launch_bounds__(128, 4) curv_face_kernel(GridView g, StageView
 template <int SCHEME, int FLUX>
 __global__ void __launch_bounds__(128, 4) curv_face_f32_kernel(GridView g, StageView sv, int axis, double* fl) {
     if (sv.require_active && !sv.clock->active) return;
-    constexpr int NST = SchemeInfo<SCHEME>::NST, W = SchemeInfo<SCHEME>::W, CL = NST / 2 - 1;
+    constexpr int NST = SchemeInfo<SCHEME>::NST, CL = NST / 2 - 1;
     const int a = axis;
     int base[3], span[3];
 #pragma unroll
@@ -633,23 +658,9 @@ __global__ void __launch_bounds__(128, 4) curv_face_f32_kernel(GridView g, Stage
         const double n64[3] = {gm[face], gm[vs + face], gm[2 * vs + face]};
         const double area = gm[3 * vs + face];
         const float n[3] = {float(n64[0]), float(n64[1]), float(n64[2])};
-        const float gamma = float(g.gamma);
-        // eigen basis at the face average (q_ref + d_CL+1 / 2)
-        float qa[5];
-#pragma unroll
-        for (int v = 0; v < 5; ++v) qa[v] = ref.q[v] + 0.5f * d[CL + 1][v];
-        const float pa = (gamma - 1.f) * (qa[4] - 0.5f * (qa[1] * qa[1] + qa[2] * qa[2] + qa[3] * qa[3]) / qa[0]);
-        if (!(qa[0] > 0.f) || !(pa > 0.f)) flags |= FLAG_PRESSURE;
-        CharBasisT<float> e;
-        char_basis_p<float>(qa, pa, n, gamma, e);
-        float dL[5] = {0.f, 0.f, 0.f, 0.f, 0.f}, dR[5] = {0.f, 0.f, 0.f, 0.f, 0.f}, F[5];
-        recon_field<0, SCHEME, NST, W, float>(e, d, dL, dR, flags, cut);
-        recon_field<1, SCHEME, NST, W, float>(e, d, dL, dR, flags, cut);
-        recon_field<2, SCHEME, NST, W, float>(e, d, dL, dR, flags, cut);
-        recon_field<3, SCHEME, NST, W, float>(e, d, dL, dR, flags, cut);
-        recon_field<4, SCHEME, NST, W, float>(e, d, dL, dR, flags, cut);
+        float F[5];
+        curv_face_dev32<SCHEME, FLUX>(d, ref, n, float(g.gamma), F, flags, cut);
         if (SCHEME == TENO5) cores += 10;
-        flux_dev_n<FLUX>(ref, dL, dR, n, gamma, F, flags);
         double fref[5];
         euler_flux_n(qref, n64, g.gamma, fref, flags);
 #pragma unroll
@@ -660,6 +671,141 @@ __global__ void __launch_bounds__(128, 4) curv_face_f32_kernel(GridView g, Stage
         }
     }
     flush_status(sv, flags, cores, cut);
+}
+
+// ---------------------------------------------------------------------------
+// 2-D FP32-flux stage fused in one tile (the curvilinear form of
+// tile2d_f32_body): the tile and its halo staged as FP32 deviations from the
+// tile's first node q_ref; every x and y face of the tile from shared memory
+// with its own normal and area, as the flux deviation dF * area; per node
+// div = sum dF area (FP64) + (sum of the node's face cofactors) . F(q_ref),
+// the second term in FP64 (on a curved grid the reference flux does not
+// cancel between a node's faces).  No face fluxes round-trip through HBM.
+// ---------------------------------------------------------------------------
+template <int SCHEME, int FLUX, int TX, int TY>
+__global__ void __launch_bounds__(TILE_THREADS, 2) curv_tile2d_f32_kernel(GridView g, StageView sv) {
+    if (sv.require_active && !sv.clock->active) return;
+    extern __shared__ float smem_c[];
+    using S = TileShape<SCHEME, TX, TY>;
+    constexpr int NST = S::NST, H = S::H, SX = S::SX, SY = S::SY, NFX = S::NFX, NFY = S::NFY;
+    constexpr int NFXP = S::NFXP, NFYP = S::NFYP;
+    const int ntx = (g.hi[0] - g.lo[0] + TX - 1) / TX;
+    const int x0 = g.lo[0] + (blockIdx.x % ntx) * TX, y0 = g.lo[1] + (blockIdx.x / ntx) * TY;
+    float* sq = smem_c;             // [5][SY][SX] deviations from qref
+    float* fx = sq + 5 * SX * SY;   // [5][TY][TX+1]
+    float* fy = fx + 5 * NFX;       // [5][TY+1][TX]
+    const long long nx = g.n[0], vs = g.vs;
+    unsigned flags = 0, cut = 0, cores = 0;
+    double qref[5];
+    {
+        const long long at = (long long)y0 * nx + x0;
+#pragma unroll
+        for (int v = 0; v < 5; ++v) qref[v] = __ldg(sv.qs + v * vs + at);
+    }
+    const Ref32 ref = make_ref32(qref, g.gamma);
+    for (int t = threadIdx.x; t < SX * SY; t += blockDim.x) {
+        const int r = t / SX, c = t - r * SX;
+        if ((r < H || r >= TY + H) && (c < H || c >= TX + H)) continue;
+        const int gx = map_tile_index(x0 - H + c, g.n[0], g.bc_lo[0], g.bc_hi[0]);
+        const int gy = map_tile_index(y0 - H + r, g.n[1], g.bc_lo[1], g.bc_hi[1]);
+        const long long at = (long long)gy * nx + gx;
+#pragma unroll
+        for (int v = 0; v < 5; ++v) sq[v * SX * SY + t] = float(__ldg(sv.qs + v * vs + at) - qref[v]);
+    }
+    __syncthreads();
+    const float gamma = float(g.gamma);
+    // face (i | i+1) geometry sits at its lower node; only the periodic wrap
+    // applies to that index
+    auto lower = [&](int i, int a) { return i < 0 ? i + g.n[a] : i; };
+    for (int f = threadIdx.x; f < NFXP + NFYP; f += blockDim.x) {
+        float st[NST][5];
+        float Ft[5];
+        if (f < NFXP) {
+            if (f >= NFX) continue;
+            const int r = f / (TX + 1), c = f - r * (TX + 1);
+            const int gy = y0 + r, gl = x0 - 1 + c;  // face between nodes gl and gl + 1 of row gy
+            if (gy >= g.hi[1] || gl >= g.hi[0]) {
+#pragma unroll
+                for (int v = 0; v < 5; ++v) fx[v * NFX + f] = 0.f;
+                continue;
+            }
+            const float* base = sq + (r + H) * SX + c;
+#pragma unroll
+            for (int s = 0; s < NST; ++s)
+#pragma unroll
+                for (int v = 0; v < 5; ++v) st[s][v] = base[v * SX * SY + s];
+            const long long face = (long long)gy * nx + lower(gl, 0);
+            const float n[3] = {float(g.geom[0][face]), float(g.geom[0][vs + face]), float(g.geom[0][2 * vs + face])};
+            curv_face_dev32<SCHEME, FLUX>(st, ref, n, gamma, Ft, flags, cut);
+            const float area = float(g.geom[0][3 * vs + face]);
+#pragma unroll
+            for (int v = 0; v < 5; ++v) fx[v * NFX + f] = Ft[v] * area;
+        } else {
+            const int k = f - NFXP;
+            if (k >= NFY) continue;
+            const int r = k / TX, c = k - r * TX;
+            const int gx = x0 + c, gl = y0 - 1 + r;  // face between rows gl and gl + 1 of column gx
+            if (gx >= g.hi[0] || gl >= g.hi[1]) {
+#pragma unroll
+                for (int v = 0; v < 5; ++v) fy[v * NFY + k] = 0.f;
+                continue;
+            }
+            const float* base = sq + r * SX + (c + H);
+#pragma unroll
+            for (int s = 0; s < NST; ++s)
+#pragma unroll
+                for (int v = 0; v < 5; ++v) st[s][v] = base[v * SX * SY + s * SX];
+            const long long face = (long long)lower(gl, 1) * nx + gx;
+            const float n[3] = {float(g.geom[1][face]), float(g.geom[1][vs + face]), float(g.geom[1][2 * vs + face])};
+            curv_face_dev32<SCHEME, FLUX>(st, ref, n, gamma, Ft, flags, cut);
+            const float area = float(g.geom[1][3 * vs + face]);
+#pragma unroll
+            for (int v = 0; v < 5; ++v) fy[v * NFY + k] = Ft[v] * area;
+        }
+        if (SCHEME == TENO5) cores += 10;
+    }
+    __syncthreads();
+    // physical flux tensor of q_ref (FP64): Fc = flux along axis c
+    double Fc[3][5];
+    {
+        const double rho = qref[0];
+        const double u[3] = {qref[1] / rho, qref[2] / rho, qref[3] / rho};
+        const double p = (g.gamma - 1.0) * (qref[4] - 0.5 * (qref[1] * u[0] + qref[2] * u[1] + qref[3] * u[2]));
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            Fc[c][0] = qref[1 + c];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) Fc[c][1 + k] = qref[1 + k] * u[c] + (k == c ? p : 0.0);
+            Fc[c][4] = (qref[4] + p) * u[c];
+        }
+    }
+    const double dt = sv.clock->dt;
+    double sr = 0.0;
+    for (int nd = threadIdx.x; nd < TX * TY; nd += blockDim.x) {
+        const int r = nd / TX, c = nd - r * TX;
+        const int gx = x0 + c, gy = y0 + r;
+        if (gx >= g.hi[0] || gy >= g.hi[1]) continue;
+        const long long node = (long long)gy * nx + gx;
+        // the node's net face cofactor: upper minus lower face of each axis
+        const long long fxl = (long long)gy * nx + lower(gx - 1, 0), fyl = (long long)lower(gy - 1, 1) * nx + gx;
+        double gc[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            gc[k] = g.geom[0][k * vs + node] * g.geom[0][3 * vs + node] - g.geom[0][k * vs + fxl] * g.geom[0][3 * vs + fxl] +
+                    g.geom[1][k * vs + node] * g.geom[1][3 * vs + node] - g.geom[1][k * vs + fyl] * g.geom[1][3 * vs + fyl];
+        double div[5], qn[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            const float* fxv = fx + v * NFX + r * (TX + 1) + c;
+            const float* fyv = fy + v * NFY + r * TX + c;
+            div[v] = (double(fxv[1]) - double(fxv[0])) + (double(fyv[TX]) - double(fyv[0])) +
+                     (gc[0] * Fc[0][v] + gc[1] * Fc[1][v] + gc[2] * Fc[2][v]);
+            qn[v] = __ldg(sv.qs + v * vs + node);
+        }
+        finish_node_j<true>(g, sv, dt, node, qn, div, g.node_jac[node], flags, sr);
+    }
+    flush_status(sv, flags, cores, cut);
+    if (sv.mode & MODE_CFL) flush_cfl_block(g, sv.clock, sr);
 }
 
 // Divergence and stage update of the solved nodes.
@@ -741,11 +887,42 @@ static cudaError_t launch_curv_faces_f(int flux, int prec64, const GridView& g, 
     return cudaErrorInvalidValue;
 }
 
+template <int SCHEME, int FLUX>
+static cudaError_t launch_curv_tile2d(const GridView& g, const StageView& sv, cudaStream_t st) {
+    constexpr int TX = 22, TY = 22;
+    using S = TileShape<SCHEME, TX, TY>;
+    const int ntx = (g.hi[0] - g.lo[0] + TX - 1) / TX, nty = (g.hi[1] - g.lo[1] + TY - 1) / TY;
+    const size_t smem = sizeof(float) * S::ELEMS;
+    auto kern = curv_tile2d_f32_kernel<SCHEME, FLUX, TX, TY>;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    kern<<<ntx * nty, TILE_THREADS, smem, st>>>(g, sv);
+    return cudaGetLastError();
+}
+
+template <int SCHEME>
+static cudaError_t launch_curv_tile2d_f(int flux, const GridView& g, const StageView& sv, cudaStream_t st) {
+    if (flux == RUSANOV) return launch_curv_tile2d<SCHEME, RUSANOV>(g, sv, st);
+    if (flux == ROE) return launch_curv_tile2d<SCHEME, ROE>(g, sv, st);
+    return cudaErrorInvalidValue;
+}
+
 // One stage on a curvilinear grid: the face fluxes of every active axis, then
 // the divergence and stage update (sv.mode: MODE_FINAL with optional
-// MODE_RESIDUAL / MODE_CFL).
+// MODE_RESIDUAL / MODE_CFL); 2-D FP32-flux grids run the fused tile kernel.
 cudaError_t launch_curv_stage(int scheme, int flux, int prec64, const GridView& g, const StageView& sv, double* fl,
                               cudaStream_t st) {
+    if (!prec64 && g.dim == 2) {
+        switch (scheme) {
+        case WENO5: return launch_curv_tile2d_f<WENO5>(flux, g, sv, st);
+        case TENO5: return launch_curv_tile2d_f<TENO5>(flux, g, sv, st);
+        case WENO3: return launch_curv_tile2d_f<WENO3>(flux, g, sv, st);
+        case WENO7: return launch_curv_tile2d_f<WENO7>(flux, g, sv, st);
+        default: return cudaErrorInvalidValue;
+        }
+    }
     for (int axis = 0; axis < g.dim; ++axis) {
         cudaError_t e;
         switch (scheme) {

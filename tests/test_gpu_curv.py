@@ -183,10 +183,14 @@ def test_metric_arguments_are_checked():
         capi.Solver(1, n, h, bcs, bcs).set_metrics(zero)
 
 
-# FP32-flux / FP64-state on curvilinear grids: deviations from each face's
-# left node, FP32 reconstruction and flux deviation, FP64 reference flux.
-# Bars as for the uniform FP32 path: WENO5 2e-6 relative per step; TENO5's
-# cut-off decisions flip near its threshold in FP32 (max 1e-4, mean 1e-7).
+# FP32-flux / FP64-state on curvilinear grids: FP32 deviations from an FP64
+# reference (each face's left node in 1-D / 3-D; the tile's first node in
+# the fused 2-D tile kernel), FP32 reconstruction and flux deviation, the
+# reference's flux in FP64.  Steps: the uniform FP32 path's bar, 2e-6
+# relative; TENO5's cut-off decisions flip near its threshold in FP32 (max
+# 1e-4, mean 1e-7).  Residuals alone are the more sensitive measure -- their
+# FP32 error scales with the state's variation across a 22-node tile -- and
+# are held to 5e-6.
 
 @pytest.mark.parametrize("dim", [1, 2, 3])
 @pytest.mark.parametrize("bc", [capi.BC_TRANSMISSIVE, capi.BC_PERIODIC])
@@ -198,7 +202,7 @@ def test_curvilinear_fp32_residual_near_oracle(dim, bc, recipe):
     R_ref = from_oracle(spec, po.rhs(spec, SCHEME_OF[scheme], FLUX_OF[flux], Q))
     R_gpu = s.residual().reshape(R_ref.shape)
     sl = _solved(spec, bc)
-    assert rel_linf(R_gpu[sl], R_ref[sl]).max() <= 2e-6
+    assert rel_linf(R_gpu[sl], R_ref[sl]).max() <= 5e-6
 
 
 @pytest.mark.parametrize("dim", [1, 2, 3])
