@@ -460,7 +460,7 @@ def run_curvilinear(args):
     in FP32-flux / FP64-state: device-timed throughput against the uniform
     FP64 path on the same node count, L1(rho) of each against the exact
     solution at the nodes' physical coordinates, and the time of one stage
-    with its memory traffic estimate."""
+    (the fused 2-D tile kernel) with its algorithmic bytes."""
     import numpy as np
     from sonicsolver_b200 import capi, cases
     N = args.size
@@ -481,11 +481,10 @@ def run_curvilinear(args):
                      "l1_rho_vs_exact": float(np.mean(np.abs(q[..., 0] - ex[..., 0]))),
                      "ms_per_stage": None if stage_ms is None else round(float(stage_ms), 4)}
         s.close()
-    # bytes a curvilinear stage moves per node in 2-D: per axis the face
-    # launch reads the state (40 B) and the face geometry (32 B) and writes
-    # the face flux (40 B); the stage launch reads both axes' fluxes (80 B),
-    # the state, q0 and Jac (88 B) and writes the state (40 B)
-    out["bytes_per_node_stage"] = 2 * (40 + 32 + 40) + 80 + 88 + 40
+    # algorithmic bytes of one stage-1 launch of the fused 2-D tile kernel per
+    # node: the state in (40 B) and out (40 B), the face geometry of two
+    # axes (2 x 32 B) and Jac (8 B)
+    out["bytes_per_node_stage"] = 40 + 40 + 2 * 32 + 8
     c = out["curvilinear"]
     if c["ms_per_stage"]:
         out["hbm_gbs_per_stage"] = round(out["bytes_per_node_stage"] * N * N / (c["ms_per_stage"] * 1e-3) / 1e9, 1)

@@ -808,6 +808,123 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) curv_tile2d_f32_kernel(GridVi
     if (sv.mode & MODE_CFL) flush_cfl_block(g, sv.clock, sr);
 }
 
+// The FP64 form of the fused 2-D tile: the state staged as is, full face
+// fluxes (times the area) in shared memory, div = dFx + dFy per node.
+template <int SCHEME, int FLUX, int TX, int TY>
+__global__ void __launch_bounds__(TILE_THREADS, 2) curv_tile2d_kernel(GridView g, StageView sv) {
+    if (sv.require_active && !sv.clock->active) return;
+    extern __shared__ double smem_d[];
+    using S = TileShape<SCHEME, TX, TY>;
+    constexpr int NST = S::NST, W = S::NST == 8 ? 7 : (S::NST == 4 ? 4 : 5), H = S::H, SX = S::SX, SY = S::SY;
+    constexpr int NFX = S::NFX, NFY = S::NFY, NFXP = S::NFXP, NFYP = S::NFYP;
+    const int ntx = (g.hi[0] - g.lo[0] + TX - 1) / TX;
+    const int x0 = g.lo[0] + (blockIdx.x % ntx) * TX, y0 = g.lo[1] + (blockIdx.x / ntx) * TY;
+    double* sq = smem_d;            // [5][SY][SX]
+    double* fx = sq + 5 * SX * SY;  // [5][TY][TX+1]
+    double* fy = fx + 5 * NFX;      // [5][TY+1][TX]
+    const long long nx = g.n[0], vs = g.vs;
+    unsigned flags = 0, cut = 0, cores = 0;
+    for (int t = threadIdx.x; t < SX * SY; t += blockDim.x) {
+        const int r = t / SX, c = t - r * SX;
+        if ((r < H || r >= TY + H) && (c < H || c >= TX + H)) continue;
+        const int gx = map_tile_index(x0 - H + c, g.n[0], g.bc_lo[0], g.bc_hi[0]);
+        const int gy = map_tile_index(y0 - H + r, g.n[1], g.bc_lo[1], g.bc_hi[1]);
+        const long long at = (long long)gy * nx + gx;
+#pragma unroll
+        for (int v = 0; v < 5; ++v) sq[v * SX * SY + t] = __ldg(sv.qs + v * vs + at);
+    }
+    __syncthreads();
+    auto lower = [&](int i, int a) { return i < 0 ? i + g.n[a] : i; };
+    for (int f = threadIdx.x; f < NFXP + NFYP; f += blockDim.x) {
+        double st[NST][5];
+        const double* gm;
+        double* out;
+        long long face;
+        int slot, stride;
+        const double* base;
+        if (f < NFXP) {
+            if (f >= NFX) continue;
+            const int r = f / (TX + 1), c = f - r * (TX + 1);
+            const int gy = y0 + r, gl = x0 - 1 + c;
+            if (gy >= g.hi[1] || gl >= g.hi[0]) {
+#pragma unroll
+                for (int v = 0; v < 5; ++v) fx[v * NFX + f] = 0.0;
+                continue;
+            }
+            base = sq + (r + H) * SX + c;
+            stride = 1;
+            gm = g.geom[0];
+            face = (long long)gy * nx + lower(gl, 0);
+            out = fx;
+            slot = f;
+        } else {
+            const int k = f - NFXP;
+            if (k >= NFY) continue;
+            const int r = k / TX, c = k - r * TX;
+            const int gx = x0 + c, gl = y0 - 1 + r;
+            if (gx >= g.hi[0] || gl >= g.hi[1]) {
+#pragma unroll
+                for (int v = 0; v < 5; ++v) fy[v * NFY + k] = 0.0;
+                continue;
+            }
+            base = sq + r * SX + (c + H);
+            stride = SX;
+            gm = g.geom[1];
+            face = (long long)lower(gl, 1) * nx + gx;
+            out = fy;
+            slot = k;
+        }
+#pragma unroll
+        for (int s2 = 0; s2 < NST; ++s2)
+#pragma unroll
+            for (int v = 0; v < 5; ++v) st[s2][v] = base[v * SX * SY + s2 * stride];
+        const double n[3] = {gm[face], gm[vs + face], gm[2 * vs + face]};
+        const double area = gm[3 * vs + face];
+        double qavg[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) qavg[v] = 0.5 * (st[NST / 2 - 1][v] + st[NST / 2][v]);
+        CharBasis e;
+        char_basis_n(qavg, n, g.gamma, e, flags);
+        double qL[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, qR[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, F[5];
+        recon_field<0, SCHEME, NST, W, double>(e, st, qL, qR, flags, cut);
+        recon_field<1, SCHEME, NST, W, double>(e, st, qL, qR, flags, cut);
+        recon_field<2, SCHEME, NST, W, double>(e, st, qL, qR, flags, cut);
+        recon_field<3, SCHEME, NST, W, double>(e, st, qL, qR, flags, cut);
+        recon_field<4, SCHEME, NST, W, double>(e, st, qL, qR, flags, cut);
+        flux_n<FLUX>(qL, qR, n, g.gamma, F, flags);
+        const int nf = out == fx ? NFX : NFY;
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            const double x = F[v] * area;
+            if (!isfinite(x)) flags |= FLAG_NONFINITE;
+            out[v * nf + slot] = x;
+        }
+        if (SCHEME == TENO5) cores += 10;
+    }
+    __syncthreads();
+    const double dt = sv.clock->dt;
+    double sr = 0.0;
+    for (int nd = threadIdx.x; nd < TX * TY; nd += blockDim.x) {
+        const int r = nd / TX, c = nd - r * TX;
+        const int gx = x0 + c, gy = y0 + r;
+        if (gx >= g.hi[0] || gy >= g.hi[1]) continue;
+        const long long node = (long long)gy * nx + gx;
+        double div[5], qn[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            const double* fxv = fx + v * NFX + r * (TX + 1) + c;
+            const double* fyv = fy + v * NFY + r * TX + c;
+            div[v] = 0.0;
+            div[v] += fxv[1] - fxv[0];
+            div[v] += fyv[TX] - fyv[0];
+            qn[v] = sq[v * SX * SY + (r + H) * SX + (c + H)];
+        }
+        finish_node_j<true>(g, sv, dt, node, qn, div, g.node_jac[node], flags, sr);
+    }
+    flush_status(sv, flags, cores, cut);
+    if (sv.mode & MODE_CFL) flush_cfl_block(g, sv.clock, sr);
+}
+
 // Divergence and stage update of the solved nodes.
 __global__ void __launch_bounds__(256) curv_stage_kernel(GridView g, StageView sv, const double* __restrict__ fl) {
     if (sv.require_active && !sv.clock->active) return;
@@ -902,8 +1019,33 @@ static cudaError_t launch_curv_tile2d(const GridView& g, const StageView& sv, cu
     return cudaGetLastError();
 }
 
+template <int SCHEME, int FLUX>
+static cudaError_t launch_curv_tile2d64(const GridView& g, const StageView& sv, cudaStream_t st) {
+    constexpr int TX = 22, TY = 22;
+    using S = TileShape<SCHEME, TX, TY>;
+    const int ntx = (g.hi[0] - g.lo[0] + TX - 1) / TX, nty = (g.hi[1] - g.lo[1] + TY - 1) / TY;
+    const size_t smem = sizeof(double) * S::ELEMS;
+    auto kern = curv_tile2d_kernel<SCHEME, FLUX, TX, TY>;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    kern<<<ntx * nty, TILE_THREADS, smem, st>>>(g, sv);
+    return cudaGetLastError();
+}
+
 template <int SCHEME>
-static cudaError_t launch_curv_tile2d_f(int flux, const GridView& g, const StageView& sv, cudaStream_t st) {
+static cudaError_t launch_curv_tile2d_f(int flux, int prec64, const GridView& g, const StageView& sv,
+                                        cudaStream_t st) {
+    if (prec64) {
+        switch (flux) {
+        case RUSANOV: return launch_curv_tile2d64<SCHEME, RUSANOV>(g, sv, st);
+        case ROE: return launch_curv_tile2d64<SCHEME, ROE>(g, sv, st);
+        case STEGER: return launch_curv_tile2d64<SCHEME, STEGER>(g, sv, st);
+        case LAXF: return launch_curv_tile2d64<SCHEME, LAXF>(g, sv, st);
+        }
+        return cudaErrorInvalidValue;
+    }
     if (flux == RUSANOV) return launch_curv_tile2d<SCHEME, RUSANOV>(g, sv, st);
     if (flux == ROE) return launch_curv_tile2d<SCHEME, ROE>(g, sv, st);
     return cudaErrorInvalidValue;
@@ -912,14 +1054,14 @@ static cudaError_t launch_curv_tile2d_f(int flux, const GridView& g, const Stage
 // One stage on a curvilinear grid: the face fluxes of every active axis, then
 // the divergence and stage update (sv.mode: MODE_FINAL with optional
 // MODE_RESIDUAL / MODE_CFL); 2-D FP32-flux grids run the fused tile kernel.
-cudaError_t launch_curv_stage(int scheme, int flux, int prec64, const GridView& g, const StageView& sv, double* fl,
-                              cudaStream_t st) {
-    if (!prec64 && g.dim == 2) {
+cudaError_t launch_curv_stage(int scheme, int flux, int prec64, int tiles, const GridView& g, const StageView& sv,
+                              double* fl, cudaStream_t st) {
+    if (g.dim == 2 && tiles) {
         switch (scheme) {
-        case WENO5: return launch_curv_tile2d_f<WENO5>(flux, g, sv, st);
-        case TENO5: return launch_curv_tile2d_f<TENO5>(flux, g, sv, st);
-        case WENO3: return launch_curv_tile2d_f<WENO3>(flux, g, sv, st);
-        case WENO7: return launch_curv_tile2d_f<WENO7>(flux, g, sv, st);
+        case WENO5: return launch_curv_tile2d_f<WENO5>(flux, prec64, g, sv, st);
+        case TENO5: return launch_curv_tile2d_f<TENO5>(flux, prec64, g, sv, st);
+        case WENO3: return launch_curv_tile2d_f<WENO3>(flux, prec64, g, sv, st);
+        case WENO7: return launch_curv_tile2d_f<WENO7>(flux, prec64, g, sv, st);
         default: return cudaErrorInvalidValue;
         }
     }

@@ -41,8 +41,8 @@ cudaError_t launch_law_fill(const GridView& g, const LawView& lv, const double* 
                             int require_active, unsigned* flags, cudaStream_t st);
 cudaError_t launch_curv_geometry(const GridView& g, const double* nm, double* const geom[3], unsigned* flags,
                                  cudaStream_t st);
-cudaError_t launch_curv_stage(int scheme, int flux, int prec64, const GridView& g, const StageView& sv, double* fl,
-                              cudaStream_t st);
+cudaError_t launch_curv_stage(int scheme, int flux, int prec64, int tiles, const GridView& g, const StageView& sv,
+                              double* fl, cudaStream_t st);
 cudaError_t launch_teno_flips(const GridView& g, const double* q, unsigned long long* out, cudaStream_t st);
 }  // namespace sfg
 
@@ -433,8 +433,9 @@ int enqueue_stage(sfg_solver_s* s, int stage, bool residual_only, bool require_a
     }
     if (s->gv.curv) {  // per-face geometry: face-flux launches per axis, then the stage
         sv.mode = MODE_FINAL | (residual_only ? MODE_RESIDUAL : 0) | cfl_bit_all;
-        CUDA_TRY(launch_curv_stage(s->recipe->scheme, s->recipe->flux, s->num.precision == SFG_PREC_FP64, s->gv, sv,
-                                   s->face_flux, s->stream));
+        // 2-D: the fused tile unless variant 0 (face launches) is selected
+        CUDA_TRY(launch_curv_stage(s->recipe->scheme, s->recipe->flux, s->num.precision == SFG_PREC_FP64,
+                                   s->variant > 0, s->gv, sv, s->face_flux, s->stream));
         return SFG_OK;
     }
     const int cfl_bit = cfl && !residual_only ? MODE_CFL : 0;
