@@ -531,7 +531,8 @@ def run_batched(args, precision):
 def run_served(args, precision, seed=7, capacity=None):
     """Served stream: Poisson arrivals of 2-D solves (isentropic vortex and
     slanted shock tubes, grids 64^2..1024^2, 100..2000 steps), admission by a
-    60 GB HBM budget, continuous batching; latency = finish - submit."""
+    60 GB HBM budget, continuous batching; latency = finish - submit; the
+    served results of the smallest requests against the plain FP64 path."""
     import numpy as np
     from sonicsolver_b200 import capi, cases
     rng = np.random.default_rng(seed)
@@ -566,6 +567,19 @@ def run_served(args, precision, seed=7, capacity=None):
     ok = sum(1 for i in infos if i.state == capi.REQ_DONE)
     failed = [{"request": k, "cells": reqs[k][0].cells, "case": reqs[k][0].name, "flags": int(infos[k].flags),
                "steps_done": int(infos[k].steps)} for k in range(nreq) if infos[k].state == capi.REQ_FAILED]
+    # accuracy of served results: the four smallest finished requests rerun
+    # alone as plain FP64 single grids over the same steps; L1(rho) of the
+    # served state against them, relative to the mean |rho|
+    done = sorted((reqs[k][0].cells, k) for k in range(nreq) if infos[k].state == capi.REQ_DONE)[:4]
+    l1 = []
+    for _, k in done:
+        c, steps = reqs[k]
+        served_q = srv.fetch(ids[k]).reshape(c.q.shape)
+        alone = c.solver(precision=capi.PREC_FP64)
+        alone.advance(1e9, max_steps=steps, graph_steps=16)
+        ref = alone.download().reshape(c.q.shape)
+        alone.close()
+        l1.append(float(np.mean(np.abs(served_q[..., 0] - ref[..., 0])) / np.mean(np.abs(ref[..., 0]))))
     srv.close()
     return {"requests": nreq, "completed": ok, "failed": failed, "arrival_rate_per_s": round(rate, 3),
             "offered_load": "1.2x FP64 batched capacity" if capacity else "fixed rate",
@@ -573,7 +587,10 @@ def run_served(args, precision, seed=7, capacity=None):
             "p99_latency_s": round(float(np.percentile(lat, 99)), 4),
             "p50_queue_wait_s": round(float(np.percentile(wait, 50)), 4),
             "throughput": {"value": round(work / (end - start) / 1e6, 2), "unit": "Mcell-steps/s"},
-            "wall_s": round(end - start, 2), "budget_gb": 60}
+            "wall_s": round(end - start, 2), "budget_gb": 60,
+            "l1_rho_vs_fp64_alone": {"max": max(l1) if l1 else None, "requests": [k for _, k in done],
+                                     "note": "relative L1(rho) of the served state against the same request run "
+                                             "alone as a plain FP64 single grid"}}
 
 
 def ctypes_stream(stream):
