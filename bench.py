@@ -216,7 +216,7 @@ def run_ours(args, rank, world):
     ms = st.device_ms
     ms_max = allreduce_max(ms, world)
     cells = case.cells
-    value = cells * K * world / (ms_max * 1e-3) / 1e6
+    value = whole_job_rate(cells * K, ms_max, world) / 1e6
 
     out = {"metric": "Mcell-steps/s", "value": round(value, 2), "unit": "Mcell-steps/s", "n_gpus": world,
            "steps": K, "warmup": W, "ms_per_step": round(ms_max / K, 4), "higher_is_better": True,
@@ -232,10 +232,69 @@ def run_ours(args, rank, world):
     dim = case.dim
     launches_per_step = 2 + 3 * (1 if (dim == 2 and s.variant > 0) else dim) + 1  # dt, finalize, stages, commit
     out["gpu_launches"] = launches_per_step * (K + 0)
-    if args.quick or rank != 0:
+    if args.quick:
         s.close()
         return out
+    s2 = None
+    if rank == 0:
+        s2 = rank0_comparisons(args, out, s, case, prec, stream, K, W)
+    barrier(world)
 
+    # ---- e2e through the C ABI with pinned host buffers, every step, on
+    # every rank (replicas); the slowest rank's time counts
+    E = args.e2e_steps
+    host = torch.empty(case.q.size, dtype=torch.float64, pin_memory=True).numpy()
+    host[:] = case.q.ravel()
+    t_sim = 0.0
+    with torch.cuda.stream(stream):
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.upload(host, t_sim)
+        s.step()
+        s.download(out=host)
+        torch.cuda.synchronize()
+    barrier(world)
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+        for _ in range(E):
+            s.upload(host, t_sim)      # H2D of the step's input state
+            s.step()                   # CFL step (device dt + 3 stages)
+            s.download(out=host)       # D2H of the step's result state
+        ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    e2e_ms = allreduce_max(ev0.elapsed_time(ev1), world)
+    out["e2e"] = {"value": round(whole_job_rate(cells * E, e2e_ms, world) / 1e6, 2), "unit": "Mcell-steps/s",
+                  "h2d_bytes_per_step": int(host.nbytes), "d2h_bytes_per_step": int(host.nbytes),
+                  "steps": E, "path": "sfg_upload(pinned) + sfg_step + sfg_download per step"}
+    out["gpu_launches"] += E * (launches_per_step + 2)
+    s.close()
+    if s2 is not None:
+        s2.close()
+    if world > 1 or rank != 0:
+        return out   # the other workloads are measured by the one-GPU run
+    if args.accuracy_t > 0:
+        out["accuracy"] = run_accuracy(args)
+    out["sod_1d"] = run_sod(args)
+    if args.tgv_t > 0:
+        out["taylor_green"] = run_taylor_green(args)
+    if args.curv_t > 0:
+        out["curvilinear"] = run_curvilinear(args)
+    if not args.no_batch:
+        out["batched"] ={"fp32flux": run_batched(args, capi.PREC_FP32_FLUX), "fp64": run_batched(args, capi.PREC_FP64)}
+        cap = out["batched"]["fp64"]["value"]
+        out["served"] = {"fp32flux": run_served(args, capi.PREC_FP32_FLUX, capacity=cap),
+                         "fp64": run_served(args, capi.PREC_FP64, capacity=cap)}
+    return out
+
+
+def rank0_comparisons(args, out, s, case, prec, stream, K, W):
+    """Rank 0 only (no collectives): the other precision on the same
+    workload, and the roofline of the dominant launch.  Returns the
+    other-precision solver (closed by the caller)."""
+    import numpy as np
+    import torch
+    from sonicsolver_b200 import capi
+    cells, dim = case.cells, case.dim
     # ---- the other precision, same workload (plain FP64 vs mixed)
     other = capi.PREC_FP64 if prec else capi.PREC_FP32_FLUX
     key = "fp64_value" if prec else "fp32flux_value"
@@ -284,45 +343,7 @@ def run_ours(args, rank, world):
                                       "flops_per_face": FLOPS_PER_FACE["teno5"],
                                       "note": "binding roof: arithmetic issue, not HBM"}}
 
-    # ---- e2e through the C ABI with pinned host buffers, every step
-    E = args.e2e_steps
-    host = torch.empty(case.q.size, dtype=torch.float64, pin_memory=True).numpy()
-    host[:] = case.q.ravel()
-    t_sim = 0.0
-    with torch.cuda.stream(stream):
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s.upload(host, t_sim)
-        s.step()
-        s.download(out=host)
-        torch.cuda.synchronize()
-        ev0.record(stream)
-        for _ in range(E):
-            s.upload(host, t_sim)      # H2D of the step's input state
-            s.step()                   # CFL step (device dt + 3 stages)
-            s.download(out=host)       # D2H of the step's result state
-        ev1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = ev0.elapsed_time(ev1)
-    out["e2e"] = {"value": round(cells * E / (e2e_ms * 1e-3) / 1e6, 2), "unit": "Mcell-steps/s",
-                  "h2d_bytes_per_step": int(host.nbytes), "d2h_bytes_per_step": int(host.nbytes),
-                  "steps": E, "path": "sfg_upload(pinned) + sfg_step + sfg_download per step"}
-    out["gpu_launches"] += E * (launches_per_step + 2)
-    s.close()
-    if s2 is not None:
-        s2.close()
-    if args.accuracy_t > 0:
-        out["accuracy"] = run_accuracy(args)
-    out["sod_1d"] = run_sod(args)
-    if args.tgv_t > 0:
-        out["taylor_green"] = run_taylor_green(args)
-    if args.curv_t > 0:
-        out["curvilinear"] = run_curvilinear(args)
-    if not args.no_batch:
-        out["batched"] ={"fp32flux": run_batched(args, capi.PREC_FP32_FLUX), "fp64": run_batched(args, capi.PREC_FP64)}
-        cap = out["batched"]["fp64"]["value"]
-        out["served"] = {"fp32flux": run_served(args, capi.PREC_FP32_FLUX, capacity=cap),
-                         "fp64": run_served(args, capi.PREC_FP64, capacity=cap)}
-    return out
+    return s2
 
 
 def run_accuracy(args):
@@ -598,20 +619,7 @@ def ctypes_stream(stream):
     return ctypes.c_void_p(stream.cuda_stream)
 
 
-def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
-
-
-def allreduce_max(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+from sonicsolver_b200.replicas import barrier, max_over_ranks as allreduce_max, whole_job_rate  # noqa: E402
 
 
 def main():
@@ -642,20 +650,17 @@ def main():
     base = None
     if rank == 0 and not args.quick and not args.no_cpu_baseline:
         base = cpu_baseline(steps=1)  # spawned before any GPU call
+    from sonicsolver_b200 import replicas
     if world > 1:
         import torch
-        import torch.distributed as dist
-        from datetime import timedelta
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    replicas.init(world, "nccl", timeout_s=120)
     out = run_ours(args, rank, world)
     if rank == 0:
         if base is not None:
             out["cpu_baseline"] = {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")}
         print(json.dumps(out), flush=True)
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    replicas.finish(world)
 
 
 if __name__ == "__main__":
