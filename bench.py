@@ -408,8 +408,20 @@ def run_sod(args, repeats=5):
             walls.append(wall)
             devs.append(st.device_ms / 1e3)
         steps = int(st.steps)
+    # the same solve on the CUDA-graph path (1-D variant 1), for comparison
+    # with the whole-run cluster kernel the default variant 2 uses
+    graph_devs = []
+    for r in range(3):
+        s = case.solver(precision=capi.PREC_FP64)
+        s.variant = 1
+        s.upload(q)
+        st1, _ = s.advance(case.t_end, graph_steps=32)
+        graph_devs.append(st1.device_ms / 1e3)
+        s.close()
     out = {"cells": 1000, "t_end": case.t_end, "steps": steps, "recipe": "weno5Rusanov", "time": "SSPRK3",
-           "device_s": float(np.median(devs)), "wall_s_capi_host_buffers": float(np.median(walls))}
+           "path": "whole-run cluster kernel (1-D variant 2)",
+           "device_s": float(np.median(devs)), "wall_s_capi_host_buffers": float(np.median(walls)),
+           "device_s_graph_path": float(np.median(graph_devs[1:]))}
     out["value"] = round(1000 * steps / out["wall_s_capi_host_buffers"] / 1e6, 3)
     out["unit"] = "Mcell-steps/s"
     try:

@@ -334,8 +334,11 @@ double sfg_server_now(sfg_server s);
 /* Kernel variant of the stage operator: 0 = one sweep launch per axis
  * (any dimension), 1 = fused tile kernel (2-D: 30 x 16 tiles, 1-D: 511-node
  * tiles, 3-D: 16 x 15 columns marching up 32-plane chunks), 2 = fused 2-D
- * tile kernel with 22 x 22 tiles.  sfg_create picks 1 for 1-D and 2-D grids
- * and 0 for 3-D; results agree across variants to round-off (FP64; FP32-flux
+ * tile kernel with 22 x 22 tiles; for 1-D grids variant 2 runs sfg_advance
+ * in one thread-block cluster that steps the whole run on device (FP64, up to
+ * 8192 nodes, no boundary laws, not Lax-Wendroff; other 1-D grids and single
+ * stages use the 1-D tiles).  sfg_create picks 2 for 1-D, 1 for 2-D and 0
+ * for 3-D grids; results agree across variants to round-off (FP64; FP32-flux
  * results depend on the tile's reference state), and variant 1 gives the
  * same bits as a batch. */
 int sfg_set_kernel_variant(sfg_solver s, int variant);

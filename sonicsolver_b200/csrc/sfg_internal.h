@@ -109,4 +109,17 @@ constexpr int MODE_RESIDUAL = 4;   // final output is R = Jac * div (no stage up
 constexpr int MODE_CFL = 8;        // last stage of a step: also reduce the CFL minimum of
                                    // the new state into clock->dt_bits (the next step's dt)
 
+// One launch of the 1-D whole-run cluster kernel (sfg_cluster1d.cu): the
+// stage views of a step, the clock it advances and where it logs.
+struct ClusterRun {
+    StageView sv[4];         // the step's stages (Euler writes its stage in place)
+    int stages;
+    Clock* clock;
+    double* dt_log;
+    long long dt_cap;
+    double* faces;           // face fluxes x area, 5 x vs: face i between nodes i - 1 and i
+    unsigned* flags;
+    long long launch_steps;  // steps per launch at most (the host relaunches)
+};
+
 }  // namespace sfg

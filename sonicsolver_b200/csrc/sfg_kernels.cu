@@ -284,8 +284,7 @@ __global__ void finalize_dt_kernel(Clock* c) {
     double scale = fmax(fabs(c->t), fabs(c->t_end));
     scale = scale < 1.0 ? 1.0 : scale;
     if (!(remaining > 64.0 * eps * scale) || c->steps >= c->max_steps) {
-        c->active = 0;
-        c->dt = 0.0;
+        c->active = 0;  // dt keeps the last step's size
         return;
     }
     double limit = remaining;

@@ -44,6 +44,8 @@ cudaError_t launch_curv_geometry(const GridView& g, const double* nm, double* co
 cudaError_t launch_curv_stage(int scheme, int flux, int prec64, int tiles, const GridView& g, const StageView& sv,
                               double* fl, cudaStream_t st);
 cudaError_t launch_teno_flips(const GridView& g, const double* q, unsigned long long* out, cudaStream_t st);
+bool cluster1d_eligible(const GridView& g, int flux, int prec64);
+cudaError_t launch_cluster1d(int scheme, int flux, const GridView& g, const ClusterRun& run, cudaStream_t st);
 }  // namespace sfg
 
 using namespace sfg;
@@ -650,7 +652,7 @@ int sfg_create(const sfg_grid_desc* grid, const sfg_numerics_desc* numerics, voi
     s->recipe = recipe;
     s->ng = ghost_layers(recipe->scheme);
     make_view(s);
-    s->variant = grid->dim <= 2 ? 1 : 0;
+    s->variant = grid->dim == 1 ? 2 : grid->dim == 2 ? 1 : 0;
     cudaGetDevice(&s->device);
     auto cleanup = [&](int code) {
         sfg_destroy(s);
@@ -1008,6 +1010,96 @@ int sfg_step(sfg_solver s, double dt, double limit) {
     return sync_and_check(s);
 }
 
+// sfg_advance on the CUDA-graph path: graphs of `graph_steps` CFL steps,
+// relaunched until the clock stops.  `ms`: device time of the launches.
+static int advance_graph(sfg_solver_s* s, int graph_steps, float* ms) {
+    Clock* hc = s->host_clock;
+    if (!s->graph || s->graph_steps != graph_steps) {
+        if (s->graph) cudaGraphExecDestroy(s->graph);
+        s->graph = nullptr;
+        cudaGraph_t g;
+        CUDA_TRY(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+        int crc = SFG_OK;
+        for (int i = 0; i < graph_steps && !crc; ++i) crc = enqueue_cfl_step(s, true);
+        cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+        if (crc) return crc;
+        if (e != cudaSuccess) return fail(SFG_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&s->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail(SFG_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+        s->graph_steps = graph_steps;
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, s->stream);
+    for (;;) {
+        CUDA_TRY(cudaGraphLaunch(s->graph, s->stream));
+        CUDA_TRY(cudaMemcpyAsync(hc, s->clock, sizeof(Clock), cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(cudaStreamSynchronize(s->stream));
+        unsigned bits = 0;
+        CUDA_TRY(cudaMemcpy(&bits, s->flags, sizeof bits, cudaMemcpyDeviceToHost));
+        if (bits) break;
+        if (!hc->active || hc->steps >= hc->max_steps) break;
+    }
+    cudaEventRecord(e1, s->stream);
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return SFG_OK;
+}
+
+// sfg_advance of a small 1-D FP64 grid in the whole-run cluster kernel
+// (sfg_cluster1d.cu), relaunched every `launch_steps` steps until the clock
+// stops.  `ran` stays false when the device cannot place the cluster; the
+// caller then takes the graph path from the same state.
+static int advance_cluster(sfg_solver_s* s, float* ms, bool* ran) {
+    Clock* hc = s->host_clock;
+    ClusterRun run{};
+    run.stages = stage_count(s->num.time_recipe);
+    for (int st = 0; st < run.stages; ++st) {
+        run.sv[st] = stage_view(s, st, false, false);
+        // Euler updates qn in place (every face of the stage is formed before
+        // any node is written), which leaves no copy-back
+        if (s->num.time_recipe == T_EULER) run.sv[st].qout = s->qn;
+    }
+    run.clock = s->clock;
+    run.dt_log = s->dt_log;
+    run.dt_cap = s->dt_log_cap;
+    run.faces = s->r;
+    run.flags = s->flags;
+    run.launch_steps = 4096;
+    cudaEvent_t e0, e1;
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    CUDA_TRY(cudaEventRecord(e0, s->stream));
+    for (bool first = true;; first = false) {
+        cudaError_t e = launch_cluster1d(s->recipe->scheme, s->recipe->flux, s->gv, run, s->stream);
+        if (e != cudaSuccess) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            if (first) {  // not placed: nothing ran
+                (void)cudaGetLastError();
+                return SFG_OK;
+            }
+            return fail(SFG_ERR_CUDA, "cluster run: %s", cudaGetErrorString(e));
+        }
+        CUDA_TRY(cudaMemcpyAsync(hc, s->clock, sizeof(Clock), cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(cudaStreamSynchronize(s->stream));
+        unsigned bits = 0;
+        CUDA_TRY(cudaMemcpy(&bits, s->flags, sizeof bits, cudaMemcpyDeviceToHost));
+        if (bits || !hc->active || hc->steps >= hc->max_steps) break;
+    }
+    CUDA_TRY(cudaEventRecord(e1, s->stream));
+    CUDA_TRY(cudaEventSynchronize(e1));
+    cudaEventElapsedTime(ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ran = true;
+    return SFG_OK;
+}
+
 int sfg_advance(sfg_solver s, double t_end, int64_t max_steps, double write_interval, int graph_steps,
                 double* dt_out, int64_t dt_capacity, sfg_stats* stats) {
     if (!s) return fail(SFG_ERR_ARG, "null solver");
@@ -1042,40 +1134,17 @@ int sfg_advance(sfg_solver s, double t_end, int64_t max_steps, double write_inte
     }
     rc = push_clock(s);
     if (rc) return rc;
-    if (!s->graph || s->graph_steps != graph_steps) {
-        if (s->graph) cudaGraphExecDestroy(s->graph);
-        s->graph = nullptr;
-        cudaGraph_t g;
-        CUDA_TRY(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-        int crc = SFG_OK;
-        for (int i = 0; i < graph_steps && !crc; ++i) crc = enqueue_cfl_step(s, true);
-        cudaError_t e = cudaStreamEndCapture(s->stream, &g);
-        if (crc) return crc;
-        if (e != cudaSuccess) return fail(SFG_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
-        e = cudaGraphInstantiate(&s->graph, g, 0);
-        cudaGraphDestroy(g);
-        if (e != cudaSuccess) return fail(SFG_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
-        s->graph_steps = graph_steps;
-    }
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaEventRecord(e0, s->stream);
-    for (;;) {
-        CUDA_TRY(cudaGraphLaunch(s->graph, s->stream));
-        CUDA_TRY(cudaMemcpyAsync(hc, s->clock, sizeof(Clock), cudaMemcpyDeviceToHost, s->stream));
-        CUDA_TRY(cudaStreamSynchronize(s->stream));
-        unsigned bits = 0;
-        CUDA_TRY(cudaMemcpy(&bits, s->flags, sizeof bits, cudaMemcpyDeviceToHost));
-        if (bits) break;
-        if (!hc->active || hc->steps >= hc->max_steps) break;
-    }
-    cudaEventRecord(e1, s->stream);
-    cudaEventSynchronize(e1);
     float ms = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    bool ran = false;
+    if (s->grid.dim == 1 && s->variant == 2 && !s->has_laws &&
+        cluster1d_eligible(s->gv, s->recipe->flux, s->num.precision == SFG_PREC_FP64)) {
+        rc = advance_cluster(s, &ms, &ran);
+        if (rc) return rc;
+    }
+    if (!ran) {
+        rc = advance_graph(s, graph_steps, &ms);
+        if (rc) return rc;
+    }
     const long long done = hc->steps - steps0;
     if (dt_out && want > 0) {
         const long long n = done < want ? done : want;
@@ -1269,7 +1338,7 @@ int sfg_set_kernel_variant(sfg_solver s, int variant) {
     if (!s) return fail(SFG_ERR_ARG, "null solver");
     if (variant < 0 || variant > 2) return fail(SFG_ERR_ARG, "unknown kernel variant %d", variant);
     if (variant > 1 && s->grid.dim == 3) return fail(SFG_ERR_ARG, "3-D grids have variants 0 (sweeps) and 1 (tiles)");
-    if (variant == 2 && s->grid.dim != 2) return fail(SFG_ERR_ARG, "the 22 x 22 tile needs a 2-D grid");
+    // variant 2: the 22 x 22 tile (2-D), the whole-run cluster kernel (1-D)
     if (variant != s->variant && s->graph) {
         cudaGraphExecDestroy(s->graph);
         s->graph = nullptr;

@@ -152,7 +152,7 @@ def _run_steps(case, recipe, time_recipe, variant, steps, precision=capi.PREC_FP
     return rel_linf(got[keep], from_oracle(spec, Q)[keep]).max()
 
 
-@pytest.mark.parametrize("variant", [0, 1])
+@pytest.mark.parametrize("variant", [0, 1, 2])
 @pytest.mark.parametrize("recipe", ["weno5Rusanov", "teno5Roe", "weno7Rusanov", "weno3Rusanov"])
 @pytest.mark.parametrize("case", ["1d_inflow_wall", "1d_subsonic_slip", "1d_outflow_transmissive"])
 def test_1d_law_steps_match_oracle(case, recipe, variant):

@@ -78,9 +78,10 @@ def test_2d_kernel_variants_match_oracle(variant, recipe, n, bc):
 
 def test_variants_by_dimension():
     s, _, _ = _pair(1, (61, 1, 1), (0.013, 1.0, 1.0), capi.BC_PERIODIC, "weno5Rusanov")
-    assert s.variant == 1
+    assert s.variant == 2            # 1-D tiles + the whole-run cluster kernel
+    s.variant = 1
     with pytest.raises(capi.SolverError):
-        s.variant = 2
+        s.variant = 3
     s3, _, _ = _pair(3, (14, 12, 11), (0.05, 0.06, 0.07), capi.BC_PERIODIC, "weno5Rusanov")
     assert s3.variant == 0
     s3.variant = 1                  # 3-D z-marching tiles
@@ -89,7 +90,7 @@ def test_variants_by_dimension():
         s3.variant = 2
 
 
-@pytest.mark.parametrize("variant", [0, 1])
+@pytest.mark.parametrize("variant", [0, 1, 2])
 @pytest.mark.parametrize("recipe", ["weno5Rusanov", "teno5Roe", "weno7Rusanov", "weno3Rusanov"])
 @pytest.mark.parametrize("n", [61, 511, 512, 1300])
 @pytest.mark.parametrize("bc", [capi.BC_TRANSMISSIVE, capi.BC_PERIODIC])
