@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--tgv-t", type=float, default=0.25, help="Taylor-Green run length (0: skip)")
     ap.add_argument("--tgv-size", type=int, default=256)
     ap.add_argument("--curv-t", type=float, default=1.0, help="curvilinear vortex run length (0: skip)")
+    ap.add_argument("--survey", action="store_true",
+                    help="run every kernel family once on inputs larger than L2 (for a profiler launch list)")
     return ap.parse_args()
 
 
@@ -641,6 +643,72 @@ def run_served(args, precision, seed=7, capacity=None):
                                              "alone as a plain FP64 single grid"}}
 
 
+def run_survey(args):
+    """One CFL step (or the equivalent launch) of every kernel family of the
+    provider, each on a state larger than the 126 MB L2 where the kernel
+    streams the state, for a profiler launch list of device time and DRAM
+    bytes per kernel (achieved HBM GB/s against the peak).  Timing comes from
+    the profiler; this only runs the launches and says what ran."""
+    import numpy as np
+    from sonicsolver_b200 import capi, cases
+    F64, F32 = capi.PREC_FP64, capi.PREC_FP32_FLUX
+    ran = []
+
+    def steps(case, label, variants, precisions=(F64, F32)):
+        for prec in precisions:
+            for v in variants:
+                s = case.solver(precision=prec)          # upload (aos_to_soa; geometry when curvilinear)
+                s.variant = v
+                s.step()                                 # dt, finalize, the stages, commit
+                s.close()
+                ran.append(f"{label} variant {v} {'fp64' if prec == F64 else 'fp32flux'}: one CFL step")
+
+    # 2-D vortex 2048^2 (168 MB per state copy): axis sweeps, 30 x 16 and 22 x 22 tiles
+    vortex = cases.isentropic_vortex(2048)
+    steps(vortex, "2-D vortex 2048^2", (0, 1, 2))
+    s = vortex.solver()
+    s.totals()
+    s.teno_flips()
+    s.download()
+    r = s.residual()
+    s.stage_with_residual(0, 1e-4, r)
+    s.close()
+    ran.append("2-D vortex 2048^2: totals, TENO flip count, download, residual, stage from a given residual")
+    # 2-D channel with law ends (fixedValue inflow, zeroGradient outflow)
+    lo, hi = (capi.BC_LAW, capi.BC_TRANSMISSIVE, 0), (capi.BC_LAW, capi.BC_TRANSMISSIVE, 0)
+    s = capi.Solver(2, vortex.n, vortex.h, lo, hi, recipe="teno5Rusanov", cfl=0.4)
+    s.set_boundary_law(0, 0, rho=capi.LAW_FIXED_VALUE, velocity=capi.LAW_FIXED_VALUE, rho_value=1.0,
+                       velocity_value=(1.0, 0.0, 0.0))
+    s.set_boundary_law(0, 1)
+    s.upload(np.ascontiguousarray(vortex.q))
+    s.step()
+    s.close()
+    ran.append("2-D channel 2048^2 with law ends: one CFL step (law fill before each stage)")
+    del vortex
+    # 1-D tube of 4 M nodes (168 MB): 511-node tiles; Sod 1000 cells: the whole-run cluster kernel
+    steps(cases.sod_1d((1 << 22) - 1), "1-D tube 4M nodes", (1,))
+    sod = cases.sod_1d(1000)
+    s = sod.solver()
+    s.advance(sod.t_end, max_steps=50)
+    s.close()
+    ran.append("Sod 1000 cells: 50 steps in one cluster launch")
+    # 3-D Taylor-Green 160^3 (164 MB): axis sweeps and z-marching tiles
+    steps(cases.taylor_green(160), "3-D Taylor-Green 160^3", (0, 1))
+    # curvilinear vortex 1448^2 (84 MB state + 168 MB metrics): face launches and fused tiles
+    steps(cases.wavy_vortex(1448), "curvilinear vortex 1448^2", (0, 1))
+    # batch: every second tube of the batched workload
+    tubes = cases.shock_tube_batch(count=512, seed=2024, t_end=0.15)[::2]
+    for prec in (F64, F32):
+        b = capi.Batch(4 << 30, len(tubes), recipe="weno5Rusanov", precision=prec, cfl=0.5)
+        for c in tubes:
+            b.add(c)
+        b.step(2, graph_steps=2)
+        b.close()
+        ran.append(f"batch of {len(tubes)} tubes ({sum(c.cells for c in tubes)} cells) "
+                   f"{'fp64' if prec == F64 else 'fp32flux'}: two batch steps")
+    return {"survey": ran}
+
+
 def ctypes_stream(stream):
     import ctypes
     return ctypes.c_void_p(stream.cuda_stream)
@@ -673,6 +741,9 @@ def main():
                 "e2e": {"value": round(best["value"], 4), "unit": "Mcell-steps/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}, "wall_s": round(time.time() - t0, 1)}
         print(json.dumps(line), flush=True)
+        return
+    if args.survey:
+        print(json.dumps(run_survey(args)), flush=True)
         return
     base = None
     if rank == 0 and not args.quick and not args.no_cpu_baseline:

@@ -650,7 +650,8 @@ int sfg_batch_remove(sfg_batch b, int slot) {
     BCUDA(cudaStreamSynchronize(b->stream));
     b->h_inst[slot].live = 0;
     const int zero = 0;
-    BCUDA(cudaMemcpy(&b->d_inst[slot].live, &zero, sizeof zero, cudaMemcpyHostToDevice));
+    BCUDA(cudaMemcpyAsync(&b->d_inst[slot].live, &zero, sizeof zero, cudaMemcpyHostToDevice, b->stream));
+    BCUDA(cudaStreamSynchronize(b->stream));  // ordered on the batch's (non-blocking) stream
     slab_free(b, b->inst_offset[slot], b->inst_bytes[slot]);
     return publish_items(b);
 }

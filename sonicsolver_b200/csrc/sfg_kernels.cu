@@ -257,20 +257,34 @@ __global__ void __launch_bounds__(128) sweep_yz(GridView g, StageView sv) {
 __global__ void __launch_bounds__(256) dt_kernel(GridView g, const double* __restrict__ q, Clock* clock,
                                                  unsigned* flags, int skip_if_ready) {
     if (skip_if_ready && clock->dt_ready) return;  // the previous step's last stage reduced it
-    const long long cx = g.hi[0] - g.lo[0], cy = g.hi[1] - g.lo[1], cz = g.hi[2] - g.lo[2];
-    const long long total = cx * cy * cz;
+    // Work item = 64 consecutive solved nodes of one x row, taken by one
+    // warp (2 nodes a lane, loaded together): the node index needs integer
+    // divisions once per item, not once per node.
+    const int cx = g.hi[0] - g.lo[0], cy = g.hi[1] - g.lo[1], cz = g.hi[2] - g.lo[2];
+    const int chunks = (cx + 63) / 64;
+    const long long items = (long long)chunks * cy * cz;
+    const int lane = threadIdx.x & 31;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
     double best = 0.0;  // largest spectral-radius sum; dt = CFL / best
     unsigned fl = 0;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int i = g.lo[0] + (int)(t % cx);
-        const int j = g.lo[1] + (int)((t / cx) % cy);
-        const int k = g.lo[2] + (int)(t / (cx * cy));
-        const long long node = ((long long)k * g.n[1] + j) * g.n[0] + i;
-        const double qq[5] = {q[node], q[g.vs + node], q[2 * g.vs + node], q[3 * g.vs + node], q[4 * g.vs + node]};
-        const double sr = cfl_rate_node(g, qq, node);
-        if (!(sr > 0.0) || !isfinite(sr)) fl |= FLAG_NONFINITE;
-        best = fmax(best, sr);
+    for (long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < items; w += nwarps) {
+        const long long row = w / chunks;
+        const int i0 = g.lo[0] + (int)(w - row * chunks) * 64;
+        const int iend = min(g.hi[0], i0 + 64);
+        const int j = g.lo[1] + (int)(row % cy), k = g.lo[2] + (int)(row / cy);
+        const long long base = ((long long)k * g.n[1] + j) * g.n[0];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int i = i0 + 32 * u + lane;
+            if (i < iend) {
+                const long long node = base + i;
+                const double qq[5] = {q[node], q[g.vs + node], q[2 * g.vs + node], q[3 * g.vs + node],
+                                      q[4 * g.vs + node]};
+                const double sr = cfl_rate_node(g, qq, node);
+                if (!(sr > 0.0) || !isfinite(sr)) fl |= FLAG_NONFINITE;
+                best = fmax(best, sr);
+            }
+        }
     }
     flush_cfl_block(g, clock, best);
     if (fl) atomicOr(flags, fl);
@@ -347,27 +361,44 @@ __global__ void stage_from_residual_kernel(GridView g, StageView sv) {
 // commit ghost fill, SF_flowOperations.cpp:647-652).
 __global__ void aos_to_soa_kernel(const double* __restrict__ aos, double* __restrict__ soa, long long nodes,
                                   long long vs) {
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nodes * 5;
-         t += (long long)gridDim.x * blockDim.x) {
-        const long long node = t / 5;
-        const int v = (int)(t % 5);
-        soa[v * vs + node] = aos[t];
+    // one warp per 128 consecutive nodes, 4 a lane: SoA stores coalesced per variable
+    const int lane = threadIdx.x & 31;
+    const long long items = (nodes + 127) / 128, nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < items; w += nwarps) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const long long node = w * 128 + 32 * u + lane;
+            if (node < nodes) {
+#pragma unroll
+                for (int v = 0; v < 5; ++v) soa[v * vs + node] = aos[node * 5 + v];
+            }
+        }
     }
 }
 
 __global__ void soa_to_aos_kernel(GridView g, const double* __restrict__ soa, double* __restrict__ aos) {
-    const long long nodes = (long long)g.n[0] * g.n[1] * g.n[2];
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nodes * 5;
-         t += (long long)gridDim.x * blockDim.x) {
-        const long long node = t / 5;
-        const int v = (int)(t % 5);
-        int i = (int)(node % g.n[0]);
-        int j = (int)((node / g.n[0]) % g.n[1]);
-        int k = (int)(node / ((long long)g.n[0] * g.n[1]));
-        if (g.dim > 0) i = map_index(i, g.n[0], g.bc_lo[0], g.bc_hi[0]);
+    // one warp per 128 nodes of one x row, 4 a lane (index divisions once per
+    // row chunk); the row's source after the boundary mapping
+    const int lane = threadIdx.x & 31;
+    const int chunks = (g.n[0] + 127) / 128;
+    const long long items = (long long)chunks * g.n[1] * g.n[2], nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < items; w += nwarps) {
+        const long long row = w / chunks;
+        const int i0 = (int)(w - row * chunks) * 128;
+        int j = (int)(row % g.n[1]), k = (int)(row / g.n[1]);
+        const long long dst = ((long long)k * g.n[1] + j) * g.n[0];
         if (g.dim > 1) j = map_index(j, g.n[1], g.bc_lo[1], g.bc_hi[1]);
         if (g.dim > 2) k = map_index(k, g.n[2], g.bc_lo[2], g.bc_hi[2]);
-        aos[t] = soa[v * g.vs + ((long long)k * g.n[1] + j) * g.n[0] + i];
+        const long long src = ((long long)k * g.n[1] + j) * g.n[0];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int i = i0 + 32 * u + lane;
+            if (i < g.n[0]) {
+                const int im = g.dim > 0 ? map_index(i, g.n[0], g.bc_lo[0], g.bc_hi[0]) : i;
+#pragma unroll
+                for (int v = 0; v < 5; ++v) aos[(dst + i) * 5 + v] = soa[v * g.vs + src + im];
+            }
+        }
     }
 }
 
@@ -459,8 +490,9 @@ static int grid_for(long long work, int block) {
 
 cudaError_t launch_dt(const GridView& g, const double* q, Clock* clock, unsigned* flags, int skip_if_ready,
                       cudaStream_t st) {
-    const long long total = (long long)(g.hi[0] - g.lo[0]) * (g.hi[1] - g.lo[1]) * (g.hi[2] - g.lo[2]);
-    dt_kernel<<<grid_for(total, 256), 256, 0, st>>>(g, q, clock, flags, skip_if_ready);
+    // one warp per 64-node row chunk (8 chunks per 256-thread block)
+    const long long items = (long long)((g.hi[0] - g.lo[0] + 63) / 64) * (g.hi[1] - g.lo[1]) * (g.hi[2] - g.lo[2]);
+    dt_kernel<<<grid_for(items * 32, 256), 256, 0, st>>>(g, q, clock, flags, skip_if_ready);
     return cudaGetLastError();
 }
 
@@ -491,13 +523,13 @@ cudaError_t launch_stage_from_residual(const GridView& g, const StageView& sv, c
 }
 
 cudaError_t launch_aos_to_soa(const double* aos, double* soa, long long nodes, long long vs, cudaStream_t st) {
-    aos_to_soa_kernel<<<grid_for(nodes * 5, 256), 256, 0, st>>>(aos, soa, nodes, vs);
+    aos_to_soa_kernel<<<grid_for((nodes + 127) / 128 * 32, 256), 256, 0, st>>>(aos, soa, nodes, vs);
     return cudaGetLastError();
 }
 
 cudaError_t launch_soa_to_aos(const GridView& g, const double* soa, double* aos, cudaStream_t st) {
-    const long long nodes = (long long)g.n[0] * g.n[1] * g.n[2];
-    soa_to_aos_kernel<<<grid_for(nodes * 5, 256), 256, 0, st>>>(g, soa, aos);
+    const long long items = (long long)((g.n[0] + 127) / 128) * g.n[1] * g.n[2];  // one warp each
+    soa_to_aos_kernel<<<grid_for(items * 32, 256), 256, 0, st>>>(g, soa, aos);
     return cudaGetLastError();
 }
 

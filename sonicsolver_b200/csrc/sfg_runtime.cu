@@ -321,7 +321,10 @@ int upload_law_codes(sfg_solver_s* s) {
         s->law_codes = nullptr;
         return fail(SFG_ERR_NOMEM, "device allocation of the law table failed");
     }
-    CUDA_TRY(cudaMemcpy(s->law_codes, codes.data(), codes.size(), cudaMemcpyHostToDevice));
+    // on the solver's stream (non-blocking: the legacy stream does not order
+    // against it), complete before `codes` goes out of scope
+    CUDA_TRY(cudaMemcpyAsync(s->law_codes, codes.data(), codes.size(), cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
     s->lv.codes = s->law_codes;
     return SFG_OK;
 }
@@ -782,9 +785,12 @@ int sfg_set_metrics(sfg_solver s, const double* host, int layout) {
                              cudaMalloc((void**)&s->face_flux, 15 * vsb) != cudaSuccess))
         return fail(SFG_ERR_NOMEM, "device allocation of the metric arrays failed");
     CUDA_TRY(cudaStreamSynchronize(s->stream));
-    CUDA_TRY(cudaMemcpy(s->node_metrics, soa.data(), 10 * vsb, cudaMemcpyHostToDevice));
-    CUDA_TRY(cudaMemset(s->face_geom, 0, 12 * vsb));
-    CUDA_TRY(cudaMemset(s->face_flux, 0, 15 * vsb));
+    // every transfer on the solver's stream: it is non-blocking, so a copy or
+    // memset on the legacy stream would not be ordered before the geometry
+    // kernel (a late memset of face_geom would wipe the face areas)
+    CUDA_TRY(cudaMemcpyAsync(s->node_metrics, soa.data(), 10 * vsb, cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemsetAsync(s->face_geom, 0, 12 * vsb, s->stream));
+    CUDA_TRY(cudaMemsetAsync(s->face_flux, 0, 15 * vsb, s->stream));
     GridView g = s->gv;
     double* geom[3] = {s->face_geom, s->face_geom + 4 * s->gv.vs, s->face_geom + 8 * s->gv.vs};
     CUDA_TRY(cudaMemsetAsync(s->flags, 0, 64, s->stream));
@@ -1252,7 +1258,10 @@ int sfg_status_word(sfg_solver s, uint32_t* bits, int clear) {
     unsigned b = 0;
     CUDA_TRY(cudaMemcpy(&b, s->flags, sizeof b, cudaMemcpyDeviceToHost));
     *bits = b;
-    if (clear) CUDA_TRY(cudaMemset(s->flags, 0, sizeof b));
+    if (clear) {
+        CUDA_TRY(cudaMemsetAsync(s->flags, 0, sizeof b, s->stream));
+        CUDA_TRY(cudaStreamSynchronize(s->stream));
+    }
     return SFG_OK;
 }
 
