@@ -195,3 +195,32 @@ def test_default_variant_by_dimension():
     s.variant = 2
     c = capi.Solver(1, (61, 1, 1), (0.01, 1.0, 1.0), (PER, 0, 0), (PER, 0, 0))
     assert c.variant == 2
+
+
+@pytest.mark.parametrize("dim", [1, 2])
+def test_max_dt_clips_every_step_like_the_oracle(dim):
+    """numerics maxDeltaT (FlowDtCompute's min with the CFL dt): 1-D runs in
+    the cluster kernel, 2-D in the graph path; a dt log shorter than the run
+    keeps the first steps."""
+    n = (120, 1, 1) if dim == 1 else (40, 36, 1)
+    h = (1.0 / n[0], 1.0 / max(n[1], 1), 1.0)
+    bc = (TR, TR if dim > 1 else 0, 0)
+    q = np.ascontiguousarray(smooth_state(dim, n, seed=9, shock=True))
+    spec = po.GridSpec(dim=dim, n=n, ng=3, h=h, bc_lo=bc, bc_hi=bc)
+    Q = spec.empty()
+    spec.interior(Q)[...] = q.reshape(spec.interior(Q).shape)
+    po.fill_ghosts(spec, Q)
+    free_dt = po.dt(spec, Q, 0.5)
+    max_dt = 0.6 * free_dt
+    dts_ref, tf = po.advance(spec, po.WENO5, po.RUSANOV, po.SSPRK3, Q, 1e30, 0.5, max_dt=max_dt, max_steps=20)
+    s = capi.Solver(dim, n, h, bc, bc, recipe="weno5Rusanov", cfl=0.5, max_dt=max_dt)
+    s.upload(q)
+    st, dts = s.advance(1e30, max_steps=20, graph_steps=8, dt_capacity=5)
+    assert st.steps == 20 and len(dts) == 5
+    assert (dts_ref <= max_dt).all() and (dts_ref == max_dt).any()
+    np.testing.assert_allclose(dts, dts_ref[:5], rtol=1e-12, atol=0)
+    assert abs(st.time - tf) <= 1e-14
+    sl = (slice(None),) * (3 - dim) + (slice(1, -1),) * dim
+    got = s.download().reshape(q.shape)
+    ref = np.ascontiguousarray(spec.interior(Q)).reshape(q.shape)
+    assert rel_linf(got[sl], ref[sl]).max() <= 1e-11
