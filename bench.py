@@ -68,7 +68,7 @@ def parse():
     ap.add_argument("--tgv-t", type=float, default=0.25, help="Taylor-Green run length (0: skip)")
     ap.add_argument("--tgv-size", type=int, default=256)
     ap.add_argument("--curv-t", type=float, default=1.0, help="curvilinear vortex run length (0: skip)")
-    ap.add_argument("--survey", action="store_true",
+    ap.add_argument("--all-kernels", action="store_true",
                     help="run every kernel family once on inputs larger than L2 (for a profiler launch list)")
     return ap.parse_args()
 
@@ -654,7 +654,7 @@ def run_served(args, precision, seed=7, capacity=None, burst=False):
                                              "alone as a plain FP64 single grid"}}
 
 
-def run_survey(args):
+def run_all_kernels(args):
     """One CFL step (or the equivalent launch) of every kernel family of the
     provider, each on a state larger than the 126 MB L2 where the kernel
     streams the state, for a profiler launch list of device time and DRAM
@@ -717,7 +717,7 @@ def run_survey(args):
         b.close()
         ran.append(f"batch of {len(tubes)} tubes ({sum(c.cells for c in tubes)} cells) "
                    f"{'fp64' if prec == F64 else 'fp32flux'}: two batch steps")
-    return {"survey": ran}
+    return {"kernels_run": ran}
 
 
 def ctypes_stream(stream):
@@ -753,8 +753,8 @@ def main():
                         "d2h_bytes_per_step": 0}, "wall_s": round(time.time() - t0, 1)}
         print(json.dumps(line), flush=True)
         return
-    if args.survey:
-        print(json.dumps(run_survey(args)), flush=True)
+    if args.all_kernels:
+        print(json.dumps(run_all_kernels(args)), flush=True)
         return
     base = None
     if rank == 0 and not args.quick and not args.no_cpu_baseline:
