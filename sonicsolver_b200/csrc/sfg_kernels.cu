@@ -291,8 +291,14 @@ __global__ void __launch_bounds__(256) dt_kernel(GridView g, const double* __res
 }
 
 // FlowDtCompute's min(dt, maxDeltaT, limit) with the Time::Driver end / output
-// clipping and stop test (SF_time.cpp:56-72).  One thread.
-__global__ void finalize_dt_kernel(Clock* c) {
+// clipping and stop test (SF_time.cpp:56-72).  One thread.  A status word
+// with bits set stops the run (the reference exits on an invalid state): the
+// failing step is the last one counted, and the rest of a graph is no-ops.
+__global__ void finalize_dt_kernel(Clock* c, const unsigned* flags) {
+    if (*flags) {
+        c->active = 0;
+        return;
+    }
     const double eps = 2.220446049250313e-16;
     const double remaining = c->t_end - c->t;
     double scale = fmax(fabs(c->t), fabs(c->t_end));
@@ -496,8 +502,8 @@ cudaError_t launch_dt(const GridView& g, const double* q, Clock* clock, unsigned
     return cudaGetLastError();
 }
 
-cudaError_t launch_finalize_dt(Clock* c, cudaStream_t st) {
-    finalize_dt_kernel<<<1, 1, 0, st>>>(c);
+cudaError_t launch_finalize_dt(Clock* c, const unsigned* flags, cudaStream_t st) {
+    finalize_dt_kernel<<<1, 1, 0, st>>>(c, flags);
     return cudaGetLastError();
 }
 

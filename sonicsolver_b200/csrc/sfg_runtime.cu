@@ -25,7 +25,7 @@ cudaError_t launch_sweep(int scheme, int flux, int prec64, int axis, const GridV
                          cudaStream_t st);
 cudaError_t launch_dt(const GridView& g, const double* q, Clock* clock, unsigned* flags, int skip_if_ready,
                       cudaStream_t st);
-cudaError_t launch_finalize_dt(Clock* c, cudaStream_t st);
+cudaError_t launch_finalize_dt(Clock* c, const unsigned* flags, cudaStream_t st);
 cudaError_t launch_commit(Clock* c, double* dt_log, long long dt_cap, int cfl_next, cudaStream_t st);
 cudaError_t launch_set_dt(Clock* c, double dt, cudaStream_t st);
 cudaError_t launch_reset_min(Clock* c, cudaStream_t st);
@@ -495,7 +495,7 @@ int enqueue_post_step(sfg_solver_s* s) {
 // an upload, a host-driven stage or the start of sfg_advance).
 int enqueue_cfl_step(sfg_solver_s* s, bool require_active) {
     CUDA_TRY(launch_dt(s->gv, s->qn, s->clock, s->flags, 1, s->stream));
-    CUDA_TRY(launch_finalize_dt(s->clock, s->stream));
+    CUDA_TRY(launch_finalize_dt(s->clock, s->flags, s->stream));
     // FlowStepPrepare opens the step (before its dt in the reference; the dt
     // reads solved nodes only, which the laws never write)
     if (s->has_laws)

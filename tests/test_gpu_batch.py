@@ -2,11 +2,13 @@
 as alone (single-grid solver, same numerics) -- tolerance 1e-12 relative
 L-infinity per variable, the parity tolerance of the other GPU tests; step
 counts must match exactly."""
+import re
 import time
 
 import numpy as np
 import pytest
 
+import pyoracle as po
 from conftest import rel_linf
 from sonicsolver_b200 import capi, cases
 
@@ -145,3 +147,56 @@ def test_server_cancel_and_oversized_request():
         srv.submit(big)       # more than the whole budget
     assert e.value.code == capi.ERR_BUDGET
     srv.close()
+
+
+# A double rarefaction close to vacuum (rho ~ 3.6, u = -0.645 | +0.755,
+# p = 0.103 | 0.284): the scheme drives p below zero within a few steps, and
+# the reference stops on it (requirePhysicalState).  The GPU paths must stop
+# in the step where the oracle's time loop stops, and count that step.
+DOUBLE_RAREFACTION = dict(left=(3.569, -0.645, 0.103), right=(3.701, 0.755, 0.284))
+
+
+def _oracle_failure_step(c):
+    """Steps the oracle completes before the step that goes invalid."""
+    spec = po.GridSpec(dim=c.dim, n=tuple(c.n), ng=3, h=tuple(c.h), bc_lo=tuple(c.bc_lo), bc_hi=tuple(c.bc_hi),
+                       gamma=c.gamma)
+    Q = spec.empty()
+    spec.interior(Q)[...] = c.q.reshape(spec.interior(Q).shape)
+    po.fill_ghosts(spec, Q)
+    with pytest.raises(po.OracleError) as e:
+        po.advance(spec, po.WENO5, po.RUSANOV, po.SSPRK3, Q, 1e9, c.cfl, max_steps=2000)
+    return int(re.search(r"after (\d+) steps", str(e.value)).group(1))
+
+
+@pytest.mark.parametrize("variant", [1, 2])
+def test_near_vacuum_stops_where_the_oracle_stops(variant):
+    """Single grid: the graph path (1) and the whole-run cluster kernel (2)."""
+    c = cases.sod_1d(200, t_end=1e9, **DOUBLE_RAREFACTION)
+    done = _oracle_failure_step(c)
+    s = c.solver()
+    s.variant = variant
+    with pytest.raises(capi.SolverError) as e:
+        s.advance(1e9, max_steps=2000, graph_steps=16)
+    assert e.value.code == capi.ERR_STATE
+    assert s.time()[1] == done + 1
+
+
+def test_near_vacuum_request_stops_in_the_mix_where_the_oracle_stops():
+    """A 2-D double rarefaction (a slanted tube of the seeded generator) in a
+    batch: it stops at the oracle's step, the others finish as alone."""
+    tube = cases.shock_tube_batch(count=2, seed=557824790, t_end=1e9, max_2d=211)[1]
+    assert tube.dim == 2
+    done = _oracle_failure_step(tube)
+    others = mix(seed=5)
+    b = capi.Batch(1 << 30, 32)
+    slots = [b.add(c) for c in others]
+    bad = b.add(tube)
+    b.step(100000)
+    st = b.status(bad)
+    assert st["flags"] != 0 and not st["running"]
+    assert st["steps"] == done + 1
+    for c, slot in zip(others, slots):
+        want, steps = solo(c)
+        assert b.status(slot)["steps"] == steps
+        assert rel_linf(b.download(slot), want).max() <= TOL
+
