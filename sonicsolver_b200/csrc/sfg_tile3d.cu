@@ -24,6 +24,9 @@
 namespace sfg {
 
 constexpr int T3X = 16, T3Y = 15, T3Z = 32;
+// resident CTAs per SM of the FP32 kernel: 64 registers a thread and 48 KB
+// of shared memory each (with the full shared-memory carveout)
+constexpr int T3_F32_CTAS = 4;
 
 template <int SCHEME, typename T>
 struct Tile3Shape {
@@ -37,7 +40,7 @@ struct Tile3Shape {
 };
 
 template <int SCHEME, int FLUX, typename T>
-__global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == sizeof(float) ? 3 : 2)
+__global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == sizeof(float) ? T3_F32_CTAS : 2)
     tile3d_kernel(GridView g, StageView sv) {
     using S = Tile3Shape<SCHEME, T>;
     constexpr int NST = S::NST, H = S::H, R = S::R, COL = S::COL, SX = S::SX, SY = S::SY;
@@ -217,6 +220,10 @@ static cudaError_t launch_tile3(const GridView& g, const StageView& sv, cudaStre
     auto kern = tile3d_kernel<SCHEME, FLUX, T>;
     if (!configured) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        // the whole unified L1 / shared array as shared memory: four FP32
+        // CTAs of 48 KB per SM
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
         if (e != cudaSuccess) return e;
         configured = true;
     }
