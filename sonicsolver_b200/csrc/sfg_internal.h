@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 namespace sfg {
 
 constexpr int BC_TRANSMISSIVE = 0;
@@ -121,5 +123,15 @@ struct ClusterRun {
     unsigned* flags;
     long long launch_steps;  // steps per launch at most (the host relaunches)
 };
+
+// One-time kernel attribute setup per device: kernel attributes belong to a
+// device context, so each launcher keeps its own set of devices done (one bit
+// per device ordinal).  Sets `bit` to the current device's bit.
+inline bool attributes_pending(const std::atomic<unsigned long long>& done, unsigned long long& bit) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    bit = 1ull << (dev & 63);
+    return !(done.load(std::memory_order_acquire) & bit);
+}
 
 }  // namespace sfg

@@ -34,14 +34,15 @@ template <int SCHEME, int FLUX, typename T, int TX, int TY>
 static cudaError_t launch_tile(const GridView& g, const StageView& sv, cudaStream_t st) {
     using S = TileShape<SCHEME, TX, TY>;
     constexpr size_t smem = sizeof(T) * S::ELEMS;
-    static bool configured = false;
+    static std::atomic<unsigned long long> configured{0};
+    unsigned long long bit = 0;
     const int ntx = (g.hi[0] - g.lo[0] + TX - 1) / TX;
     const int nty = (g.hi[1] - g.lo[1] + TY - 1) / TY;
     auto kern = sizeof(T) == sizeof(float) ? tile2d_f32_kernel<SCHEME, FLUX, TX, TY> : tile2d_kernel<SCHEME, FLUX, TX, TY>;
-    if (!configured) {
+    if (attributes_pending(configured, bit)) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        configured = true;
+        configured.fetch_or(bit, std::memory_order_release);
     }
     kern<<<ntx * nty, TILE_THREADS, smem, st>>>(g, sv);
     return cudaGetLastError();
@@ -89,12 +90,13 @@ __global__ void __launch_bounds__(TILE_THREADS) tile1d_kernel(GridView g, StageV
 template <int SCHEME, int FLUX, typename T>
 static cudaError_t launch_tile1(const GridView& g, const StageView& sv, cudaStream_t st) {
     constexpr size_t smem = sizeof(T) * Tile1Shape<SCHEME>::ELEMS;
-    static bool configured = false;
+    static std::atomic<unsigned long long> configured{0};
+    unsigned long long bit = 0;
     auto kern = tile1d_kernel<SCHEME, FLUX, T>;
-    if (!configured) {
+    if (attributes_pending(configured, bit)) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        configured = true;
+        configured.fetch_or(bit, std::memory_order_release);
     }
     kern<<<(g.hi[0] - g.lo[0] + TILE1D - 1) / TILE1D, TILE_THREADS, smem, st>>>(g, sv);
     return cudaGetLastError();

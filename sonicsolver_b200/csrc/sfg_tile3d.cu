@@ -216,16 +216,17 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == sizeof(float) ? T3_
 template <int SCHEME, int FLUX, typename T>
 static cudaError_t launch_tile3(const GridView& g, const StageView& sv, cudaStream_t st) {
     constexpr size_t smem = sizeof(T) * Tile3Shape<SCHEME, T>::ELEMS;
-    static bool configured = false;
+    static std::atomic<unsigned long long> configured{0};
+    unsigned long long bit = 0;
     auto kern = tile3d_kernel<SCHEME, FLUX, T>;
-    if (!configured) {
+    if (attributes_pending(configured, bit)) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         // the whole unified L1 / shared array as shared memory: four FP32
         // CTAs of 48 KB per SM
         e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
         if (e != cudaSuccess) return e;
-        configured = true;
+        configured.fetch_or(bit, std::memory_order_release);
     }
     const int ntx = (g.hi[0] - g.lo[0] + T3X - 1) / T3X;
     const int nty = (g.hi[1] - g.lo[1] + T3Y - 1) / T3Y;
