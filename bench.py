@@ -432,6 +432,11 @@ def run_sod(args, repeats=5):
            "device_s_graph_path": float(np.median(graph_devs[1:]))}
     out["value"] = round(1000 * steps / out["wall_s_capi_host_buffers"] / 1e6, 3)
     out["unit"] = "Mcell-steps/s"
+    # L1(rho) against the exact Riemann solution at the final time (nodes
+    # x_i = i h); the diaphragm at 0.5
+    x = np.arange(case.n[0]) * case.h[0]
+    rho_exact = cases.sod_exact(x, case.t_end)[0]
+    out["l1_rho_vs_exact"] = float(np.mean(np.abs(host.reshape(-1, 5)[:, 0] - rho_exact)))
     try:
         spec = po.GridSpec(dim=1, n=tuple(case.n), ng=3, h=tuple(case.h), bc_lo=tuple(case.bc_lo),
                            bc_hi=tuple(case.bc_hi), gamma=case.gamma)
@@ -576,12 +581,18 @@ def run_batched(args, precision):
         ref = alone.download().reshape(c.q.shape)
         alone.close()
         l1[f"{dim}d_instance_{k}"] = float(np.mean(np.abs(got[..., 0] - ref[..., 0])) / np.mean(np.abs(ref[..., 0])))
+        if dim == 1:  # the 1-D tube against its exact Riemann solution (unit domain, diaphragm at 0.5)
+            x = np.arange(c.n[0]) * c.h[0]
+            ex = cases.sod_exact(x, st["time"], c.gamma, c.meta["left"], c.meta["right"])[0]
+            l1_exact = {"instance": k, "time": st["time"],
+                        "fp_under_test": float(np.mean(np.abs(got.reshape(-1, 5)[:, 0] - ex))),
+                        "plain_fp64_alone": float(np.mean(np.abs(ref.reshape(-1, 5)[:, 0] - ex)))}
     b.close()
     return {"value": round(cell_steps / (ms * 1e-3) / 1e6, 2), "unit": "Mcell-steps/s", "batch_steps": steps,
             "instances": len(tubes), "cells_total": int(sum(c.cells for c in tubes)),
             "tiles": info["items"], "ms": round(ms, 2), "tile_variant": variant,
             "note": "default stream events around sfg_batch_step (graph of 16 steps, per-grid dt)",
-            "l1_rho_vs_fp64_alone": l1}
+            "l1_rho_vs_fp64_alone": l1, "l1_rho_vs_exact_1d": l1_exact}
 
 
 def run_served(args, precision, seed=7, capacity=None, burst=False):
