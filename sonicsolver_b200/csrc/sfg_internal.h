@@ -114,12 +114,13 @@ constexpr int MODE_CFL = 8;        // last stage of a step: also reduce the CFL 
 // One launch of the 1-D whole-run cluster kernel (sfg_cluster1d.cu): the
 // stage views of a step, the clock it advances and where it logs.
 struct ClusterRun {
-    StageView sv[4];         // the step's stages (Euler writes its stage in place)
+    StageView sv[4];         // the step's stages: recipe and coefficients; sv[0].qs is qn,
+                             // loaded at the start and stored at the end (the stage
+                             // buffers themselves live in the cluster's shared memory)
     int stages;
     Clock* clock;
     double* dt_log;
     long long dt_cap;
-    double* faces;           // face fluxes x area, 5 x vs: face i between nodes i - 1 and i
     unsigned* flags;
     long long launch_steps;  // steps per launch at most (the host relaunches)
 };

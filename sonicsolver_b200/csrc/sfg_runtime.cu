@@ -1064,16 +1064,10 @@ static int advance_cluster(sfg_solver_s* s, float* ms, bool* ran) {
     Clock* hc = s->host_clock;
     ClusterRun run{};
     run.stages = stage_count(s->num.time_recipe);
-    for (int st = 0; st < run.stages; ++st) {
-        run.sv[st] = stage_view(s, st, false, false);
-        // Euler updates qn in place (every face of the stage is formed before
-        // any node is written), which leaves no copy-back
-        if (s->num.time_recipe == T_EULER) run.sv[st].qout = s->qn;
-    }
+    for (int st = 0; st < run.stages; ++st) run.sv[st] = stage_view(s, st, false, false);
     run.clock = s->clock;
     run.dt_log = s->dt_log;
     run.dt_cap = s->dt_log_cap;
-    run.faces = s->r;
     run.flags = s->flags;
     run.launch_steps = 4096;
     cudaEvent_t e0, e1;
