@@ -683,7 +683,7 @@ __global__ void __launch_bounds__(128, 4) curv_face_f32_kernel(GridView g, Stage
 // cancel between a node's faces).  No face fluxes round-trip through HBM.
 // ---------------------------------------------------------------------------
 template <int SCHEME, int FLUX, int TX, int TY>
-__global__ void __launch_bounds__(TILE_THREADS, 2) curv_tile2d_f32_kernel(GridView g, StageView sv) {
+__global__ void __launch_bounds__(TILE_THREADS, 3) curv_tile2d_f32_kernel(GridView g, StageView sv) {
     if (sv.require_active && !sv.clock->active) return;
     extern __shared__ float smem_c[];
     using S = TileShape<SCHEME, TX, TY>;
