@@ -177,7 +177,7 @@ __device__ __forceinline__ void sweep_yz_f32_segment(const GridView& g, const St
 }
 
 template <int AX, int SCHEME, int FLUX, typename T>
-__global__ void __launch_bounds__(128) sweep_yz(GridView g, StageView sv) {
+__global__ void __launch_bounds__(128, 4) sweep_yz(GridView g, StageView sv) {
     constexpr int NST = SchemeInfo<SCHEME>::NST;
     if (sv.require_active && !sv.clock->active) return;
     constexpr int OTHER = AX == 1 ? 2 : 1;
