@@ -30,7 +30,7 @@ namespace sfg {
 // x sweep: blockDim = (32, ROWS); one warp per 31 nodes of one row.
 // ---------------------------------------------------------------------------
 template <int SCHEME, int FLUX, typename T>
-__global__ void __launch_bounds__(128) sweep_x(GridView g, StageView sv) {
+__global__ void __launch_bounds__(128, 5) sweep_x(GridView g, StageView sv) {
     constexpr int NST = SchemeInfo<SCHEME>::NST;
     if (sv.require_active && !sv.clock->active) return;
     const int lane = threadIdx.x;
