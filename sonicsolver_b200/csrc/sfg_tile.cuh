@@ -263,7 +263,7 @@ __device__ __forceinline__ void tile1d_body(const GridView& g, const StageView& 
         double div[5], qn[5];
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
-            div[v] = double(fx[v * NF + c + 1]) - double(fx[v * NF + c]);
+            div[v] = double(fx[v * NF + c + 1] - fx[v * NF + c]);  // FP32: difference in FP32, one conversion
             qn[v] = F32 ? __ldg(sv.qs + v * vs + gx) : double(sq[v * SX + c + H]);
         }
         finish_node(g, sv, dt, gx, qn, div, flags, sr_max);

@@ -200,8 +200,10 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == sizeof(float) ? T3_
             for (int v = 0; v < 5; ++v) {
                 const T* fxv = fx + v * NFX + cj * (T3X + 1) + ci;
                 const T* fyv = fy + v * NFY + cj * T3X + ci;
-                div[v] = (double(fxv[1]) - double(fxv[0])) + (double(fyv[T3X]) - double(fyv[0])) +
-                         (double(Fup[v]) * g.area[2] - double(Fdn[v]) * g.area[2]);
+                if constexpr (F32)  // deviation differences in FP32, one conversion
+                    div[v] = double((fxv[1] - fxv[0]) + (fyv[T3X] - fyv[0]) + (Fup[v] - Fdn[v]) * T(g.area[2]));
+                else
+                    div[v] = (fxv[1] - fxv[0]) + (fyv[T3X] - fyv[0]) + (Fup[v] * g.area[2] - Fdn[v] * g.area[2]);
                 qn[v] = __ldg(sv.qs + v * vs + node);
             }
             finish_node(g, sv, dt, node, qn, div, flags, sr);
