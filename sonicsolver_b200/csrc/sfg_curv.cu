@@ -798,7 +798,9 @@ __global__ void __launch_bounds__(TILE_THREADS, 3) curv_tile2d_f32_kernel(GridVi
         for (int v = 0; v < 5; ++v) {
             const float* fxv = fx + v * NFX + r * (TX + 1) + c;
             const float* fyv = fy + v * NFY + r * TX + c;
-            div[v] = (double(fxv[1]) - double(fxv[0])) + (double(fyv[TX]) - double(fyv[0])) +
+            // deviation differences in FP32 (one conversion), the reference
+            // flux term in FP64
+            div[v] = double((fxv[1] - fxv[0]) + (fyv[TX] - fyv[0])) +
                      (gc[0] * Fc[0][v] + gc[1] * Fc[1][v] + gc[2] * Fc[2][v]);
             qn[v] = __ldg(sv.qs + v * vs + node);
         }
