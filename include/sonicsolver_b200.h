@@ -350,10 +350,13 @@ int sfg_get_kernel_variant(sfg_solver s, int* variant);
  * own memory manager owns the whole device budget and forbids plugins from
  * allocating, a deployment with a fixed, pre-sized memory plan, or code on a
  * latency-critical stream that must not take cudaMalloc's implicit device
- * synchronisation.  sfg_residual_noalloc computes the same spatial residual
- * as sfg_residual (R = Jac * sum_d dF_d; 0 on unsolved transmissive boundary
- * nodes) for a caller-owned device state and writes it to a caller-owned
- * device array, allocating nothing: its working memory is one fixed array in
+ * synchronisation.  sfg_residual_noalloc computes the spatial residual
+ * R = Jac * sum_d dF_d (0 on unsolved transmissive boundary nodes) of a
+ * caller-owned device state and writes it to a caller-owned device array.
+ * In FP64 it equals sfg_residual's to round-off; with SFG_PREC_FP32_FLUX it
+ * runs the axis-sweep form (one FP32 reference state per sweep segment), so
+ * it agrees with sfg_residual, whose tiles take other reference states, to
+ * FP32 round-off only.  It allocates nothing: its working memory is one fixed array in
  * the library's device image, of 32 + 5 * SFG_NOALLOC_MAX_NODES doubles
  * (~10 MiB), which every GPU that loads the library holds until the process
  * exits.
@@ -362,11 +365,12 @@ int sfg_get_kernel_variant(sfg_solver s, int* variant);
  *   stream:       cudaStream_t (NULL: the legacy default stream).
  * Grids of more than SFG_NOALLOC_MAX_NODES nodes are rejected (SFG_ERR_ARG).
  * The first call on each device looks up the array's device address with
- * that device current; make that first call before any stream capture.
- * All calls share the one array and it keeps the last call's contents, so
- * calls whose work overlaps on the GPU (other streams, other host threads)
- * race: serialise them.  The call returns after its work has finished on
- * `stream` (it reads back the status word). */
+ * that device current and keeps it for the life of the process; the entry
+ * point is not valid across cudaDeviceReset.  Every call waits for its work
+ * on `stream` and reads the status word back to the host, so it never runs
+ * on a stream that is being captured (SFG_ERR_ARG).  All calls share the one
+ * array and it keeps the last call's contents, so calls whose work overlaps
+ * on the GPU (other streams, other host threads) race: serialise them. */
 #define SFG_NOALLOC_MAX_NODES 262144
 int sfg_residual_noalloc(const sfg_grid_desc* grid, const sfg_numerics_desc* numerics,
                          const double* dev_q, double* dev_r, void* stream);

@@ -7,6 +7,9 @@
 // shadow of that array, never device memory: a kernel given it would fault or
 // silently use the wrong memory.  The device address is looked up once per
 // device with cudaGetSymbolAddress and that pointer is what the kernels get.
+// The cached address belongs to the device's current context: after
+// cudaDeviceReset the module is loaded again and the address may change, so
+// the entry point is not valid across a reset in the same process.
 #include "../../include/sonicsolver_b200.h"
 #include "sfg_internal.h"
 
@@ -74,14 +77,14 @@ extern "C" int sfg_residual_noalloc(const sfg_grid_desc* grid, const sfg_numeric
     if (!rp) return noalloc_fail(SFG_ERR_ARG, "convection recipe not provided on the GPU");
     if (numerics->precision != SFG_PREC_FP64 && numerics->precision != SFG_PREC_FP32_FLUX)
         return noalloc_fail(SFG_ERR_ARG, "unknown precision mode");
-    if (!(numerics->gamma > 1.0)) return noalloc_fail(SFG_ERR_ARG, "gamma must be > 1");
+    if (!(numerics->gamma > 1.0) || !std::isfinite(numerics->gamma)) return noalloc_fail(SFG_ERR_ARG, "gamma must be > 1");
     if (grid->dim < 1 || grid->dim > 3) return noalloc_fail(SFG_ERR_ARG, "dim must be 1..3");
     const int reach = rp->scheme == WENO3 ? 2 : (rp->scheme == WENO7 ? 4 : 3);
     GridView g{};
     g.dim = grid->dim;
     long long nodes = 1;
     for (int a = 0; a < 3; ++a) {
-        if (!(grid->h[a] > 0.0)) return noalloc_fail(SFG_ERR_ARG, "spacing must be > 0");
+        if (!(grid->h[a] > 0.0) || !std::isfinite(grid->h[a])) return noalloc_fail(SFG_ERR_ARG, "spacing must be > 0");
         g.n[a] = grid->n[a];
         if (a >= grid->dim) {
             if (grid->n[a] != 1) return noalloc_fail(SFG_ERR_ARG, "inactive axes must have 1 node");
@@ -99,12 +102,16 @@ extern "C" int sfg_residual_noalloc(const sfg_grid_desc* grid, const sfg_numeric
         g.bc_hi[a] = grid->bc_hi[a];
         g.lo[a] = plo ? 0 : 1;
         g.hi[a] = plo ? grid->n[a] : grid->n[a] - 1;
-        nodes *= grid->n[a];
+        // each factor is at most the cap before it is multiplied in, so the
+        // running product stays below cap^2 (< 2^37): no 64-bit overflow
+        if (grid->n[a] > SFG_NOALLOC_MAX_NODES || nodes > SFG_NOALLOC_MAX_NODES) nodes = SFG_NOALLOC_MAX_NODES + 1LL;
+        else nodes *= grid->n[a];
     }
     if (nodes > SFG_NOALLOC_MAX_NODES) {
         char msg[160];
-        snprintf(msg, sizeof msg, "grid of %lld nodes exceeds the fixed working array (SFG_NOALLOC_MAX_NODES = %d)",
-                 nodes, SFG_NOALLOC_MAX_NODES);
+        snprintf(msg, sizeof msg,
+                 "grid of %lld x %lld x %lld nodes exceeds the fixed working array (SFG_NOALLOC_MAX_NODES = %d)",
+                 (long long)grid->n[0], (long long)grid->n[1], (long long)grid->n[2], SFG_NOALLOC_MAX_NODES);
         return noalloc_fail(SFG_ERR_ARG, msg);
     }
     // uniform Cartesian metrics, formed exactly as sfg_create forms them
@@ -119,13 +126,20 @@ extern "C" int sfg_residual_noalloc(const sfg_grid_desc* grid, const sfg_numeric
     g.cfl = numerics->cfl;
     g.vs = nodes;
 
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // the call synchronises on `stream` and reads the status word back to
+    // pageable host memory, neither of which a capturing stream allows
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) {
+        cudaGetLastError();
+        return noalloc_fail(SFG_ERR_ARG, "sfg_residual_noalloc cannot run on a capturing stream");
+    }
     double* base = nullptr;
     int rc = scratch_address(&base);
     if (rc) return rc;
     Clock* clock = reinterpret_cast<Clock*>(base);
     unsigned* flags = reinterpret_cast<unsigned*>(base + 16);
     double* r = base + kHeaderDoubles;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
     const size_t rbytes = sizeof(double) * 5 * (size_t)nodes;
 
     // the array keeps the previous call's contents: clear what must start at 0

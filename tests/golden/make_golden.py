@@ -26,7 +26,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path[:0] = [ROOT, os.path.join(ROOT, "oracle"), os.path.join(ROOT, "tests")]
 
-REF_CASE = "/root/reference/test/Sod/sodCase_weno7_t0p2"
+# the reference tree, read in place (SONICSOLVER_REFERENCE overrides its location)
+REF_ROOT = os.environ.get("SONICSOLVER_REFERENCE", "/root/reference")
+REF_CASE = os.path.join(REF_ROOT, "test", "Sod", "sodCase_weno7_t0p2")
 
 
 def sod_fixture():

@@ -67,3 +67,19 @@ def test_no_cpu_fallback_without_device():
     with pytest.raises(capi.SolverError) as e:
         capi.Solver(1, (9, 1, 1), (0.1, 1.0, 1.0), (0, 0, 0), (0, 0, 0))
     assert e.value.code == capi.ERR_CUDA
+
+
+@pytest.mark.parametrize("n,gamma,h", [
+    ((1 << 22, 1 << 21, 1 << 21), 1.4, (0.1, 0.1, 0.1)),   # product wraps a signed 64-bit count to 0
+    ((70000, 70000, 3), 1.4, (0.1, 0.1, 0.1)),             # each axis below the cap, the product above it
+    ((16, 16, 16), float("inf"), (0.1, 0.1, 0.1)),
+    ((16, 16, 16), 1.4, (0.1, float("inf"), 0.1)),
+])
+def test_noalloc_arguments_rejected_before_any_launch(n, gamma, h):
+    """sfg_residual_noalloc checks every size against its fixed working array
+    (without overflowing the node count) and refuses non-finite gamma or
+    spacing, all before it touches the device: the pointers here are never
+    dereferenced."""
+    with pytest.raises(capi.SolverError) as e:
+        capi.residual_noalloc(3, n, h, (1, 1, 1), (1, 1, 1), 4096, 8192, gamma=gamma)
+    assert e.value.code == capi.ERR_ARG

@@ -11,7 +11,9 @@ from case_dirs import write_case
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 RUNNER = os.path.join(ROOT, "sonicsolver_b200", "sfg_run")
-REFERENCE_TESTS = "/root/reference/test"   # the reference's own case directories, read in place when present
+# the reference's own case directories, read in place when present
+# (SONICSOLVER_REFERENCE overrides the tree's location)
+REFERENCE_TESTS = os.path.join(os.environ.get("SONICSOLVER_REFERENCE", "/root/reference"), "test")
 
 
 @pytest.fixture(scope="module")
