@@ -166,27 +166,43 @@ def _cpu_worker(args):
     return time.perf_counter() - t0
 
 
-def cpu_baseline(procs=None, nx=1024, ny=128, steps=2):
-    """The reference's own operator (oracle/_ref native build) stepping
-    independent vortex slabs, one process per core (the reference is
-    single-threaded per MPI rank); falls back to the oracle port."""
+def host_cores() -> int:
+    """Cores this process may run on (its CPU affinity), not the machine's."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_baseline(procs=None, nx=1024, ny=128, steps=3, samples=1, warmup=0):
+    """The reference's own operator (oracle/_ref native build for this host's
+    CPU target) stepping independent vortex slabs, one process per core of
+    this process's affinity set (the reference is single-threaded per MPI
+    rank); falls back to the oracle port.  Each sample: every process times
+    `steps` SSPRK3 steps of its own slab; the sample's rate is all processes'
+    cell-steps over the slowest process's time.  Reports the median sample."""
     import multiprocessing as mp
     sys.path[:0] = [os.path.join(ROOT, "oracle")]
     import pyoracle as po
     native = True if po.ref_lib(native=True) is not None else None
     kind = "reference" if native else "port"
-    procs = procs or max(1, min(os.cpu_count() or 1, 32))
+    flags = po.ref_native_build()[1] if native else "the C oracle port, -O2"
+    procs = procs or max(1, min(host_cores(), 64))
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
+    rates = []
     with ctx.Pool(procs) as pool:
-        walls = pool.map(_cpu_worker, [(native, nx, ny, steps, po.TENO5)] * procs)
-    wall = max(walls)
+        for k in range(warmup + samples):
+            walls = pool.map(_cpu_worker, [(native, nx, ny, steps, po.TENO5)] * procs)
+            if k >= warmup:
+                rates.append(nx * ny * steps * procs / max(walls) / 1e6)
     total = time.perf_counter() - t0
-    cells = nx * ny * steps * procs
-    return {"value": cells / wall / 1e6, "unit": "Mcell-steps/s", "cores": procs, "kind": kind,
-            "sample": f"{procs} processes x {steps} SSPRK3 step(s) of a {nx}x{ny} periodic vortex slab "
-                      f"(dx = 10/1024), TENO5+Rusanov, reference operator compiled -O3 -march=x86-64-v3",
-            "per_core": cells / wall / 1e6 / procs, "wall_s": round(total, 2)}
+    value = statistics.median(rates)
+    return {"value": value, "unit": "Mcell-steps/s", "cores": procs, "kind": kind,
+            "sample": f"{procs} processes x {steps} SSPRK3 steps of a {nx}x{ny} periodic vortex slab each "
+                      f"(dx = 10/1024, the 1024^2 workload's spacing), TENO5+Rusanov, reference operator "
+                      f"compiled {flags}; median of {len(rates)} sample(s)",
+            "per_core": value / procs, "samples": [round(r, 4) for r in rates], "wall_s": round(total, 2)}
 
 
 # ------------------------------------------------------------------ GPU legs
@@ -271,6 +287,25 @@ def run_ours(args, rank, world):
     out["gpu_launches"] += E * (launches_per_step + 2)
     s.close()
     if s2 is not None:
+        # the other precision's e2e on the same path (rank 0): the FP64 e2e
+        # is the end-to-end figure at the reference's own precision
+        with torch.cuda.stream(stream):
+            host[:] = case.q.ravel()
+            s2.upload(host, t_sim)
+            s2.step()
+            s2.download(out=host)
+            torch.cuda.synchronize()
+            ev0.record(stream)
+            for _ in range(E):
+                s2.upload(host, t_sim)
+                s2.step()
+                s2.download(out=host)
+            ev1.record(stream)
+        torch.cuda.synchronize()
+        key = "e2e_fp64" if prec else "e2e_fp32flux"
+        out[key] = {"value": round(cells * E / (ev0.elapsed_time(ev1) * 1e-3) / 1e6, 2), "unit": "Mcell-steps/s",
+                    "h2d_bytes_per_step": int(host.nbytes), "d2h_bytes_per_step": int(host.nbytes), "steps": E,
+                    "path": "sfg_upload(pinned) + sfg_step + sfg_download per step, rank 0"}
         s2.close()
     if world > 1 or rank != 0:
         return out   # the other workloads are measured by the one-GPU run
@@ -282,7 +317,12 @@ def run_ours(args, rank, world):
     if args.curv_t > 0:
         out["curvilinear"] = run_curvilinear(args)
     if not args.no_batch:
-        out["batched"] ={"fp32flux": run_batched(args, capi.PREC_FP32_FLUX), "fp64": run_batched(args, capi.PREC_FP64)}
+        out["batched"] = {"fp32flux": run_batched(args, capi.PREC_FP32_FLUX), "fp64": run_batched(args, capi.PREC_FP64)}
+        out["batched_to_end"] = {
+            "fp32flux": run_batched_to_end(args, capi.PREC_FP32_FLUX, out["batched"]["fp32flux"]["tile_variant"]),
+            "fp64": run_batched_to_end(args, capi.PREC_FP64, out["batched"]["fp64"]["tile_variant"])}
+        e = out["batched_to_end"]
+        e["fp32flux_over_fp64"] = round(e["fp32flux"]["value"] / e["fp64"]["value"], 3)
         cap = out["batched"]["fp64"]["value"]
         out["served"] = {"fp32flux": run_served(args, capi.PREC_FP32_FLUX, capacity=cap),
                          "fp64": run_served(args, capi.PREC_FP64, capacity=cap)}
@@ -318,9 +358,10 @@ def rank0_comparisons(args, out, s, case, prec, stream, K, W):
         out[key] = None
         out[key + "_error"] = str(e)
 
-    # ---- roofline of the dominant sweep
+    # ---- roofline of the dominant launch (a fused stage is timed as 20
+    # back-to-back launches in one captured graph, as it runs in a step)
     dt = s.compute_dt()
-    ms_axes = s.time_sweeps(dt, stage=0, repeats=5)
+    ms_axes = s.time_sweeps(dt, stage=0, repeats=20)
     nodes = case.nodes
     hbm, src = measured_peaks()
     dom = int(np.argmax(ms_axes))
@@ -336,20 +377,31 @@ def rank0_comparisons(args, out, s, case, prec, stream, K, W):
     faces = nodes * (dim if fused else 1)  # faces evaluated by one launch
     fl = FLOPS_PER_FACE["teno5"] * faces / (ms_axes[dom] * 1e-3) / 1e12
     traffic = PROFILED_DRAM_BYTES.get(("tile2d", s.variant, args.size, args.precision)) if fused else None
-    out["roofline"] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+    ms_step = out["ms_per_step"]
+    step_gbs = 320 * cells / (ms_step * 1e-3) / 1e9   # SSPRK3, FP64 state: 80 + 120 + 120 B per cell-step
+    out["roofline"] = {"bound": "issue", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                        "frac": round(achieved / hbm, 4), "traffic": traffic,
                        "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one stage-1 launch; "
                                        "the output still resident in the write-back L2 at kernel end is not counted",
                        "peak_source": f"{src} (MEASURED_PEAKS.json)",
                        "kernel": ("tile2d fused stage" if fused else f"sweep axis {dom}"),
                        "ms_per_launch": round(ms_axes[dom], 4),
+                       "ms_per_launch_timing": ("20 stage-1 launches captured in one CUDA graph, events around "
+                                                "the graph" if fused else "launch by launch"),
                        "ms_per_axis": [round(x, 4) for x in ms_axes],
                        "algorithmic_bytes_per_launch": int(bytes_node * nodes),
+                       "hbm_step_average": {"achieved": round(step_gbs, 1), "frac": round(step_gbs / hbm, 4),
+                                            "bytes_per_cell_step": 320,
+                                            "note": "320 B per cell-step (stage 1 80 B, stages 2-3 120 B each) "
+                                                    "over the in-graph ms_per_step"},
                        "issue_roof": {"unit": "TFLOP/s", "achieved": round(fl, 2), "fma_peak": round(fp_peak, 2),
                                       "frac": round(fl / fp_peak, 4) if fp_peak else None,
                                       "arith": "fp32" if prec else "fp64",
                                       "flops_per_face": FLOPS_PER_FACE["teno5"],
-                                      "note": "binding roof: arithmetic issue, not HBM"}}
+                                      "peak_source": "measured (sfg_measure_fma_peak: dependent-FMA loop, "
+                                                     "this GPU, this run)"},
+                       "note": "bound = the binding roof: arithmetic issue (issue_roof), not HBM; achieved / "
+                               "peak / frac are the HBM figures on algorithmic bytes of the timed launch"}
 
     return s2
 
@@ -366,22 +418,38 @@ def run_accuracy(args):
     case = cases.isentropic_vortex(args.size)
     out = {"t_end": args.accuracy_t, "cells": f"{args.size}x{args.size}"}
     res = {}
+    import math
+
+    def sums(a):
+        a = a.reshape(-1, 5)
+        return [math.fsum(a[:, v]) for v in range(5)], np.abs(a).sum(axis=0)
+
+    tot0, scale = sums(case.q)
     for name, prec in (("fp64", capi.PREC_FP64), ("fp32flux", capi.PREC_FP32_FLUX)):
         s = case.solver(precision=prec)
         d0, f0 = s.teno_flips()
+        dev0 = s.totals()
         st, _ = s.advance(args.accuracy_t, graph_steps=64)
         q = s.download().reshape(case.q.shape)
+        tot1, _ = sums(q)
+        dev1 = s.totals()
         d1, f1 = s.teno_flips()
         ex = cases.vortex_exact(case, st.time)
         res[name] = q
         out[name] = {"steps": int(st.steps), "device_s": round(st.device_ms / 1e3, 3),
                      "l1_rho_vs_exact": float(np.mean(np.abs(q[..., 0] - ex[..., 0]))),
-                     "linf_rho_vs_exact": float(np.max(np.abs(q[..., 0] - ex[..., 0])))}
+                     "linf_rho_vs_exact": float(np.max(np.abs(q[..., 0] - ex[..., 0]))),
+                     # drift of the conserved totals over the run: (sum_t - sum_0) / sum |q_0| per
+                     # variable (rho, rho u, rho v, rho w, E), host fsum and sfg_conserved_totals (FP64)
+                     "totals_drift": [(a - b) / c if c > 0 else a - b for a, b, c in zip(tot1, tot0, scale)],
+                     "totals_drift_device": [(a - b) / abs(b) if b else a - b for a, b in zip(dev1, dev0)]}
         if name == "fp64":
             out["teno_flip_rate"] = {"initial": f0 / max(d0, 1), "final": f1 / max(d1, 1),
                                      "decisions_per_eval": int(d0)}
         s.close()
     out["l1_rho_fp32flux_vs_fp64"] = float(np.mean(np.abs(res["fp32flux"][..., 0] - res["fp64"][..., 0])))
+    out["totals_drift_fp32flux_minus_fp64"] = [a - b for a, b in zip(out["fp32flux"]["totals_drift"],
+                                                                      out["fp64"]["totals_drift"])]
     out["l1_ratio_fp32flux_over_fp64"] = out["fp32flux"]["l1_rho_vs_exact"] / out["fp64"]["l1_rho_vs_exact"]
     return out
 
@@ -451,7 +519,7 @@ def run_sod(args, repeats=5):
         scale = np.maximum(np.abs(ref).reshape(-1, 5).max(axis=0), 1e-300)
         diff = (np.abs(host - ref).reshape(-1, 5).max(axis=0) / scale)
         out["reference_cpu"] = {"wall_s": ref_s, "steps": int(len(dts)), "cores": 1,
-                                "kind": "reference operator, -O3 -march=x86-64-v3"}
+                                "kind": "reference operator, " + po.ref_native_build()[1]}
         out["max_rel_diff_vs_reference"] = float(diff.max())
         out["speedup_wall_vs_reference"] = round(ref_s / out["wall_s_capi_host_buffers"], 2)
     except Exception as e:  # reference library missing on this host
@@ -595,11 +663,62 @@ def run_batched(args, precision):
             "l1_rho_vs_fp64_alone": l1, "l1_rho_vs_exact_1d": l1_exact}
 
 
+def run_batched_to_end(args, precision, variant):
+    """The batched workload run to its end time: all 512 seeded tubes from
+    t = 0 to t_end = 0.15, every tube with its own CFL steps, finished tubes
+    dropping out of the work list (auto-compaction).  Reports the time to
+    solution of the whole batch (CUDA events around the run), the throughput
+    including the tail (every cell-step of every tube over that time), and
+    how many tubes and work items are live along the way."""
+    import numpy as np
+    import torch
+    from sonicsolver_b200 import capi, cases
+    tubes = cases.shock_tube_batch(count=512, seed=2024, t_end=0.15)
+    b = capi.Batch(8 << 30, 512, recipe="weno5Rusanov", precision=precision, cfl=0.5)
+    b.variant = variant
+    slots = [b.add(c) for c in tubes]
+    live0 = b.info()["items"]
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    wall0 = time.perf_counter()
+    t0.record()
+    timeline = []
+    calls = 0
+    while True:
+        active = b.step(64, graph_steps=16)
+        calls += 1
+        if calls % 8 == 0 or active == 0:
+            timeline.append((round(time.perf_counter() - wall0, 3), int(active), int(b.info()["items"])))
+        if active == 0:
+            break
+    t1.record()
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1)
+    st = [b.status(sl) for sl in slots]
+    steps = np.array([x["steps"] for x in st])
+    cell_steps = int(sum(c.cells * n for c, n in zip(tubes, steps)))
+    ok = all(abs(x["time"] - 0.15) < 1e-12 and x["flags"] == 0 for x in st)
+    b.close()
+    keep = np.unique(np.linspace(0, len(timeline) - 1, min(24, len(timeline))).astype(int))
+    return {"tubes": len(tubes), "t_end": 0.15, "all_reached_t_end": bool(ok),
+            "time_to_solution_s": round(ms / 1e3, 3), "cell_steps": cell_steps,
+            "value": round(cell_steps / (ms * 1e-3) / 1e6, 2), "unit": "Mcell-steps/s",
+            "steps_per_tube": {"min": int(steps.min()), "median": int(np.median(steps)), "max": int(steps.max())},
+            "work_items_at_start": int(live0), "tile_variant": variant,
+            "timeline": [{"wall_s": timeline[i][0], "running_tubes": timeline[i][1], "work_items": timeline[i][2]}
+                         for i in keep],
+            "note": "timeline sampled every 512 batch steps (graph launches of 16 steps, 64 per host call)"}
+
+
 def run_served(args, precision, seed=7, capacity=None, burst=False):
-    """Served stream: Poisson arrivals of 2-D solves (isentropic vortex and
-    slanted shock tubes, grids 64^2..1024^2, 100..2000 steps), admission by a
-    60 GB HBM budget, continuous batching; latency = finish - submit; the
-    served results of the smallest requests against the plain FP64 path.
+    """Served stream: Poisson arrivals of 2-D solves, a seeded mix of the
+    vortex workload's generator (isentropic vortex, TENO5 + Rusanov, CFL 0.4)
+    and the batched-tube workload's 2-D generator (slanted shock tubes,
+    WENO5 + Rusanov, CFL 0.5), each request with its own recipe and CFL in
+    one server; grids 64^2..1024^2, 100..2000 steps, admission by a 60 GB HBM
+    budget, continuous batching; latency = finish - submit; the served
+    results of the smallest requests against the plain FP64 path.
     `burst`: every request submitted at once (the server saturated), so the
     throughput is the server's capacity for this request mix."""
     import numpy as np
@@ -611,7 +730,7 @@ def run_served(args, precision, seed=7, capacity=None, burst=False):
         side = int(round(np.exp(rng.uniform(np.log(64), np.log(1024)))))
         steps = int(rng.integers(100, 2001))
         if rng.random() < 0.5:
-            c = cases.isentropic_vortex(side, recipe="weno5Rusanov", cfl=0.5, t_end=1e9)
+            c = cases.isentropic_vortex(side, recipe="teno5Rusanov", cfl=0.4, t_end=1e9)
         else:
             c = cases.shock_tube_batch(count=2, seed=int(rng.integers(1 << 30)), t_end=1e9, max_2d=side)[1]
         reqs.append((c, steps))
@@ -629,7 +748,7 @@ def run_served(args, precision, seed=7, capacity=None, burst=False):
         t_next += gap
         while srv.now() < t_next:
             time.sleep(min(0.002, max(0.0, t_next - srv.now())))
-        ids.append(srv.submit(c, max_steps=steps))
+        ids.append(srv.submit(c, max_steps=steps, recipe=c.recipe, cfl=c.cfl))
     srv.drain(600)
     infos = [srv.poll(i) for i in ids]
     end = max(i.finish_s for i in infos)
@@ -759,14 +878,11 @@ def main():
         if rank != 0:
             return
         t0 = time.time()
-        res = []
-        for _ in range(args.warmup):
-            cpu_baseline(steps=1)
-        for _ in range(max(1, min(args.steps, 3))):
-            res.append(cpu_baseline(steps=1))
-        best = max(res, key=lambda r: r["value"])
+        # each step a bounded sample (every host core, 3 steps of its slab)
+        best = cpu_baseline(steps=3, samples=max(1, min(args.steps, 10)), warmup=min(args.warmup, 1))
         line = {"impl": "reference", "metric": "Mcell-steps/s", "value": round(best["value"], 4),
-                "unit": "Mcell-steps/s", "n_gpus": args.gpus, "steps": len(res), "warmup": args.warmup,
+                "unit": "Mcell-steps/s", "n_gpus": args.gpus, "steps": len(best["samples"]),
+                "warmup": min(args.warmup, 1),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64",
                 "data": "synthetic (analytic isentropic vortex initial condition)",
                 "config": {"workload": "isentropic_vortex_2d", "cells": "1024x1024 (sampled as slabs)",
@@ -781,7 +897,7 @@ def main():
         return
     base = None
     if rank == 0 and not args.quick and not args.no_cpu_baseline:
-        base = cpu_baseline(steps=1)  # spawned before any GPU call
+        base = cpu_baseline(steps=3)  # spawned before any GPU call
     from sonicsolver_b200 import replicas
     if world > 1:
         import torch

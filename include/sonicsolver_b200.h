@@ -272,9 +272,12 @@ int sfg_get_counters(sfg_solver s, uint64_t* teno_cores, uint64_t* teno_cut);
  * between calls without rebuilding the graph (continuous batching).  The
  * reference has no batch layer: each sonicSolver run is one case; a batch is
  * the GPU form of running many cases (test/Sod-style cases, MPI ranks on
- * independent blocks) side by side.  All grids share one sfg_numerics_desc.
- * State memory comes from one slab of `hbm_budget_bytes` reserved at create;
- * sfg_batch_add returns SFG_ERR_BUDGET when a grid does not fit. */
+ * independent blocks) side by side.  Every grid can carry its own numerics
+ * (recipe, gamma, CFL, maxDeltaT: sfg_batch_add_ex), as every reference case
+ * directory selects its own TermRecipe; the time recipe and precision mode
+ * are the batch's.  State memory comes from one slab of `hbm_budget_bytes`
+ * reserved at create; sfg_batch_add returns SFG_ERR_BUDGET when a grid does
+ * not fit. */
 typedef struct sfg_batch_s* sfg_batch;
 int sfg_batch_create(const sfg_numerics_desc* numerics, size_t hbm_budget_bytes, int max_instances,
                      void* stream, sfg_batch* out);
@@ -285,6 +288,15 @@ int sfg_batch_instance_bytes(sfg_batch b, const sfg_grid_desc* grid, size_t* byt
  * (<= 0: no step limit); *slot identifies it. */
 int sfg_batch_add(sfg_batch b, const sfg_grid_desc* grid, const double* host_nodes_aos, double t_end,
                   int64_t max_steps, int* slot);
+/* sfg_batch_add with the grid's own numerics (NULL: the batch's): any recipe
+ * the batch kernels provide (WENO3/5/7, TENO5 x Rusanov/Roe) with its gamma,
+ * CFL and maxDeltaT; time_recipe and precision must equal the batch's
+ * (SFG_ERR_ARG otherwise).  Grids of one recipe share that recipe's stage
+ * kernel; up to 8 recipes per batch.  The reference binds one TermRecipe per
+ * case (core/config/types/SF_termRecipe.h:242-259): this is that choice, per
+ * grid of a batch. */
+int sfg_batch_add_ex(sfg_batch b, const sfg_grid_desc* grid, const sfg_numerics_desc* numerics,
+                     const double* host_nodes_aos, double t_end, int64_t max_steps, int* slot);
 int sfg_batch_remove(sfg_batch b, int slot);
 /* Runs up to `steps` batch steps (graph of `graph_steps`, <= 0: 16); stops
  * early when no grid is running.  *active = grids that stepped last. */
@@ -321,6 +333,10 @@ int sfg_server_destroy(sfg_server s);
 /* Copies the input; the request runs to t_end or max_steps. */
 int sfg_server_submit(sfg_server s, const sfg_grid_desc* grid, const double* host_nodes_aos, double t_end,
                       int64_t max_steps, int64_t* request_id);
+/* sfg_server_submit with the request's own numerics (NULL: the server's),
+ * under the rules of sfg_batch_add_ex, checked before the request queues. */
+int sfg_server_submit_ex(sfg_server s, const sfg_grid_desc* grid, const sfg_numerics_desc* numerics,
+                         const double* host_nodes_aos, double t_end, int64_t max_steps, int64_t* request_id);
 int sfg_server_poll(sfg_server s, int64_t request_id, sfg_request_info* info);
 /* Result of a finished request (AoS nodes); SFG_ERR_ARG while not done. */
 int sfg_server_fetch(sfg_server s, int64_t request_id, double* host_nodes_aos);
@@ -338,8 +354,9 @@ double sfg_server_now(sfg_server s);
  * in one thread-block cluster that steps the whole run on device (FP64, up to
  * 8192 nodes, no boundary laws, not Lax-Wendroff; other 1-D grids and single
  * stages use the 1-D tiles).  sfg_create picks 2 for 1-D, 1 for 2-D and 0
- * for 3-D grids; results agree across variants to round-off (FP64; FP32-flux
- * results depend on the tile's reference state), and variant 1 gives the
+ * for 3-D grids; results agree across variants to round-off (FP32-flux: every
+ * face takes the stage's one reference state; the sweeps scale face fluxes
+ * by the area in FP64, the tiles in FP32), and the tile variants give the
  * same bits as a batch. */
 int sfg_set_kernel_variant(sfg_solver s, int variant);
 int sfg_get_kernel_variant(sfg_solver s, int* variant);
@@ -354,9 +371,9 @@ int sfg_get_kernel_variant(sfg_solver s, int* variant);
  * R = Jac * sum_d dF_d (0 on unsolved transmissive boundary nodes) of a
  * caller-owned device state and writes it to a caller-owned device array.
  * In FP64 it equals sfg_residual's to round-off; with SFG_PREC_FP32_FLUX it
- * runs the axis-sweep form (one FP32 reference state per sweep segment), so
- * it agrees with sfg_residual, whose tiles take other reference states, to
- * FP32 round-off only.  It allocates nothing: its working memory is one fixed array in
+ * runs the axis-sweep form, which scales each face flux by its area in FP64
+ * where sfg_residual's tiles do it in FP32, so the two agree to FP32
+ * round-off only.  It allocates nothing: its working memory is one fixed array in
  * the library's device image, of 32 + 5 * SFG_NOALLOC_MAX_NODES doubles
  * (~10 MiB), which every GPU that loads the library holds until the process
  * exits.
@@ -382,7 +399,10 @@ int sfg_residual_noalloc(const sfg_grid_desc* grid, const sfg_numerics_desc* num
 int sfg_teno_flip_rate(sfg_solver s, uint64_t* decisions, uint64_t* flips);
 /* Runs stage `stage` of a step of size dt `repeats` times on the current
  * state without committing it, timing each axis sweep with CUDA events on the
- * solver's stream; ms_per_axis[d] receives the mean duration of sweep d. */
+ * solver's stream; ms_per_axis[d] receives the mean duration of sweep d.  A
+ * fused stage (tile kernels, curvilinear launches) is timed as `repeats`
+ * launches captured in one CUDA graph, as it runs inside a step's graph
+ * (ms_per_axis[0]; launch by launch on the legacy default stream). */
 int sfg_time_sweeps(sfg_solver s, int stage, double dt, int repeats, float* ms_per_axis);
 /* Dependent-FMA throughput of this GPU in TFLOP/s (fp64 = 1: double,
  * 0: float), measured with a kernel of `seconds` length. */

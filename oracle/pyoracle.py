@@ -213,11 +213,39 @@ def oracle_lib():
     return _oracle
 
 
+def host_march() -> str | None:
+    """The CPU target `gcc -march=native` selects on this host (None when gcc
+    cannot tell)."""
+    import subprocess
+    try:
+        out = subprocess.run(["gcc", "-march=native", "-Q", "--help=target"], capture_output=True, text=True,
+                             timeout=30).stdout
+    except Exception:
+        return None
+    for line in out.splitlines():
+        f = line.split()
+        if len(f) == 2 and f[0] == "-march=":
+            return f[1]
+    return None
+
+
+def ref_native_build() -> tuple[str, str]:
+    """(library file, gcc flags) of the timed reference build for this host:
+    the build for the target `gcc -march=native` selects here when oracle/_ref
+    has one (the reference's own -march=native), else the x86-64-v3 build."""
+    arch = host_march()
+    if arch:
+        name = f"libsfref_native_{arch}.so"
+        if os.path.exists(os.path.join(HERE, "_ref", name)):
+            return name, f"-O3 -march={arch} (gcc -march=native on this host)"
+    return "libsfref_native.so", "-O3 -march=x86-64-v3"
+
+
 def ref_lib(native: bool = False):
     """The reference translation units, or None when they were not built."""
     key = "native" if native else "strict"
     if key not in _ref:
-        lib = _load(os.path.join(HERE, "_ref", "libsfref_native.so" if native else "libsfref.so"))
+        lib = _load(os.path.join(HERE, "_ref", ref_native_build()[0] if native else "libsfref.so"))
         _ref[key] = _sig(lib, "sfr") if lib is not None else None
     return _ref[key]
 

@@ -132,6 +132,7 @@ def lib():
         L.sfg_batch_destroy.argtypes = [_VP]
         L.sfg_batch_instance_bytes.argtypes = [_VP, PG, ctypes.POINTER(ctypes.c_size_t)]
         L.sfg_batch_add.argtypes = [_VP, PG, _DP, ctypes.c_double, ctypes.c_int64, ctypes.POINTER(ctypes.c_int)]
+        L.sfg_batch_add_ex.argtypes = [_VP, PG, PN, _DP, ctypes.c_double, ctypes.c_int64, ctypes.POINTER(ctypes.c_int)]
         L.sfg_batch_remove.argtypes = [_VP, ctypes.c_int]
         L.sfg_batch_step.argtypes = [_VP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
         L.sfg_batch_status.argtypes = [_VP, ctypes.c_int, _DP, I64P, ctypes.POINTER(ctypes.c_int),
@@ -145,6 +146,7 @@ def lib():
         L.sfg_server_create.argtypes = [PN, ctypes.c_size_t, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_VP)]
         L.sfg_server_destroy.argtypes = [_VP]
         L.sfg_server_submit.argtypes = [_VP, PG, _DP, ctypes.c_double, ctypes.c_int64, I64P]
+        L.sfg_server_submit_ex.argtypes = [_VP, PG, PN, _DP, ctypes.c_double, ctypes.c_int64, I64P]
         L.sfg_server_poll.argtypes = [_VP, ctypes.c_int64, ctypes.POINTER(RequestInfo)]
         L.sfg_server_fetch.argtypes = [_VP, ctypes.c_int64, _DP]
         L.sfg_server_cancel.argtypes = [_VP, ctypes.c_int64]
@@ -325,11 +327,26 @@ def numerics_desc(recipe="weno5Rusanov", time_recipe="SSPRK3", precision=PREC_FP
     return nm
 
 
+def _own_numerics(defaults: dict, recipe, gamma, cfl, max_dt):
+    """A grid's own numerics (sfg_batch_add_ex / sfg_server_submit_ex): the
+    given fields over the batch's or server's, or None when none is given."""
+    if recipe is None and gamma is None and cfl is None and max_dt is None:
+        return None
+    d = dict(defaults)
+    for k, v in (("recipe", recipe), ("gamma", gamma), ("cfl", cfl), ("max_dt", max_dt)):
+        if v is not None:
+            d[k] = v
+    return numerics_desc(**d)
+
+
 class Batch:
-    """Many independent 1-D / 2-D grids stepped together (sfg_batch)."""
+    """Many independent 1-D / 2-D grids stepped together (sfg_batch).  A grid
+    added with its own recipe / gamma / CFL / maxDeltaT runs with them."""
 
     def __init__(self, budget_bytes, max_instances, recipe="weno5Rusanov", time_recipe="SSPRK3",
                  precision=PREC_FP64, gamma=1.4, cfl=0.5, max_dt=0.0, stream=None):
+        self.defaults = dict(recipe=recipe, time_recipe=time_recipe, precision=precision, gamma=gamma, cfl=cfl,
+                             max_dt=max_dt)
         nm = numerics_desc(recipe, time_recipe, precision, gamma, cfl, max_dt)
         h = _VP()
         check(lib().sfg_batch_create(ctypes.byref(nm), int(budget_bytes), int(max_instances), stream, ctypes.byref(h)))
@@ -347,12 +364,13 @@ class Batch:
         except Exception:
             pass
 
-    def add(self, case, t_end=None, max_steps=0) -> int:
+    def add(self, case, t_end=None, max_steps=0, recipe=None, gamma=None, cfl=None, max_dt=None) -> int:
         g = grid_desc(case.dim, case.n, case.h, case.bc_lo, case.bc_hi)
         slot = ctypes.c_int()
         q = np.ascontiguousarray(case.q, dtype=np.float64)
-        check(lib().sfg_batch_add(self._h, ctypes.byref(g), _dptr(q), case.t_end if t_end is None else t_end,
-                                  max_steps, ctypes.byref(slot)))
+        nm = _own_numerics(self.defaults, recipe, gamma, cfl, max_dt)
+        check(lib().sfg_batch_add_ex(self._h, ctypes.byref(g), ctypes.byref(nm) if nm is not None else None, _dptr(q),
+                                     case.t_end if t_end is None else t_end, max_steps, ctypes.byref(slot)))
         self.shapes[slot.value] = q.shape
         return slot.value
 
@@ -396,10 +414,14 @@ class Batch:
 
 
 class Server:
-    """Continuous-batching request loop (sfg_server) on its own host thread."""
+    """Continuous-batching request loop (sfg_server) on its own host thread.
+    A request submitted with its own recipe / gamma / CFL / maxDeltaT runs
+    with them."""
 
     def __init__(self, budget_bytes, max_slots, recipe="weno5Rusanov", time_recipe="SSPRK3", precision=PREC_FP64,
                  gamma=1.4, cfl=0.5, graph_steps=16):
+        self.defaults = dict(recipe=recipe, time_recipe=time_recipe, precision=precision, gamma=gamma, cfl=cfl,
+                             max_dt=0.0)
         nm = numerics_desc(recipe, time_recipe, precision, gamma, cfl)
         h = _VP()
         check(lib().sfg_server_create(ctypes.byref(nm), int(budget_bytes), int(max_slots), int(graph_steps),
@@ -418,12 +440,14 @@ class Server:
         except Exception:
             pass
 
-    def submit(self, case, t_end=None, max_steps=0) -> int:
+    def submit(self, case, t_end=None, max_steps=0, recipe=None, gamma=None, cfl=None, max_dt=None) -> int:
         g = grid_desc(case.dim, case.n, case.h, case.bc_lo, case.bc_hi)
         q = np.ascontiguousarray(case.q, dtype=np.float64)
         rid = ctypes.c_int64()
-        check(lib().sfg_server_submit(self._h, ctypes.byref(g), _dptr(q), case.t_end if t_end is None else t_end,
-                                      int(max_steps), ctypes.byref(rid)))
+        nm = _own_numerics(self.defaults, recipe, gamma, cfl, max_dt)
+        check(lib().sfg_server_submit_ex(self._h, ctypes.byref(g), ctypes.byref(nm) if nm is not None else None,
+                                         _dptr(q), case.t_end if t_end is None else t_end, int(max_steps),
+                                         ctypes.byref(rid)))
         self.shapes[rid.value] = q.shape
         return rid.value
 

@@ -12,10 +12,17 @@
 //     list with an atomic counter: CFL reduction (per-instance 64-bit
 //     atomicMin), then each stage (the fused tile bodies of sfg_tile.cuh),
 //     then the per-instance clock update.
+// Every grid carries its own numerics (convection recipe, gamma, CFL,
+// maxDeltaT), as every reference case directory selects its own TermRecipe.
+// Grids of one recipe form a group: the work list holds the groups' tiles in
+// contiguous ranges, and each stage runs one persistent kernel per group (the
+// recipe's template instance), the groups' kernels on parallel branches so
+// that one group's blocks fill the SMs that another's tail leaves idle.
 // Host side: the batch step is captured once as a CUDA graph of G steps.
 // Adding or removing instances rewrites the table rows and the work list in
-// device memory between graph launches, so the graph never needs recapture
-// (continuous batching).
+// device memory between graph launches, so the graph needs recapture only
+// when a grid brings a recipe the batch has not run yet (continuous
+// batching).
 #include "../../include/sonicsolver_b200.h"
 #include "sfg_tile.cuh"
 
@@ -47,12 +54,18 @@ struct WorkItem {
     int inst, x0, y0, dim;
 };
 
+constexpr int kMaxGroups = 8;  // one per convection recipe the batch kernels provide
+constexpr int kCounters = 8 + 4 * kMaxGroups;
+
 struct BatchCtl {
     int n_items;
     int n_inst;
-    int counters[8];  // work stealing: [0] dt, [1..4] stages, [5] copy
-    int active;       // instances stepping in the current step
+    int active;  // instances stepping in the current step
     int pad;
+    // work stealing: [0] dt, [5] copy, [8 + 4 g + s] stage s of recipe group g
+    int counters[kCounters];
+    // tile range of group g in the work list: [2 g] first item, [2 g + 1] count
+    int group_range[2 * kMaxGroups];
 };
 
 // ---------------------------------------------------------------- kernels
@@ -96,18 +109,20 @@ __device__ __forceinline__ StageView batch_stage_view(BatchInst& b, int stage, i
     return sv;
 }
 
+// One stage over the tiles of recipe group `group` (the grids whose recipe is
+// this instance's SCHEME and FLUX).
 template <int SCHEME, int FLUX, bool F32, int TX, int TY>
 __global__ void __launch_bounds__(TILE_THREADS, F32 ? 4 : 2)
-    batch_stage_kernel(BatchInst* inst, const WorkItem* items, BatchCtl* ctl, int stage, int time_id) {
+    batch_stage_kernel(BatchInst* inst, const WorkItem* items, BatchCtl* ctl, int stage, int time_id, int group) {
     using Tt = typename std::conditional<F32, float, double>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Tt* smem = reinterpret_cast<Tt*>(smem_raw);
     __shared__ int slot;
-    const int n_items = ctl->n_items;
+    const int first = ctl->group_range[2 * group], n_items = ctl->group_range[2 * group + 1];
     for (;;) {
-        const int it = steal(&ctl->counters[1 + stage], &slot);
+        const int it = steal(&ctl->counters[8 + 4 * group + stage], &slot);
         if (it >= n_items) break;
-        const WorkItem w = items[it];
+        const WorkItem w = items[first + it];
         BatchInst& b = inst[w.inst];
         if (!b.live || !b.clock.active) continue;  // uniform across the block
         StageView sv = batch_stage_view(b, stage, time_id);
@@ -227,7 +242,8 @@ __global__ void batch_commit_kernel(BatchInst* inst, BatchCtl* ctl) {
             c->dt_ready = c->active ? 1 : 0;  // the last stage reduced the new state's CFL minimum
         }
     }
-    if (blockIdx.x == 0 && threadIdx.x < 8) ctl->counters[threadIdx.x] = 0;
+    if (blockIdx.x == 0)
+        for (int c = threadIdx.x; c < kCounters; c += blockDim.x) ctl->counters[c] = 0;
 }
 
 __global__ void batch_reset_active_kernel(BatchCtl* ctl) { ctl->active = 0; }
@@ -265,7 +281,7 @@ const RecipeParts kBatchRecipes[] = {
     {SFG_RECIPE_TENO5_RUSANOV, TENO5, RUSANOV}, {SFG_RECIPE_TENO5_ROE, TENO5, ROE},
     {SFG_RECIPE_WENO7_RUSANOV, WENO7, RUSANOV}, {SFG_RECIPE_WENO7_ROE, WENO7, ROE}};
 
-using StageKernel = void (*)(BatchInst*, const WorkItem*, BatchCtl*, int, int);
+using StageKernel = void (*)(BatchInst*, const WorkItem*, BatchCtl*, int, int, int);
 using ItemKernel = void (*)(BatchInst*, const WorkItem*, BatchCtl*);
 
 template <int TX, int TY, bool F32>
@@ -299,12 +315,26 @@ const double kInfB = std::numeric_limits<double>::infinity();
 
 }  // namespace
 
+// The grids of one convection recipe: their stage kernel, its launch shape,
+// and the stream its branch of a stage runs on (group 0: the batch's stream).
+struct RecipeGroup {
+    const RecipeParts* recipe = nullptr;
+    StageKernel stage_k = nullptr;
+    size_t smem = 0;
+    int grid = 0;
+    cudaStream_t side = nullptr;
+    cudaEvent_t joined = nullptr;
+};
+
 struct sfg_batch_s {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     sfg_numerics_desc num{};
-    const RecipeParts* recipe = nullptr;
+    const RecipeParts* recipe = nullptr;  // the default recipe (group 0)
+    std::vector<RecipeGroup> groups;
+    std::vector<int> inst_group;          // per slot
+    cudaEvent_t fork = nullptr;
     int variant = 1;  // 1: 30 x 16 tiles, 2: 22 x 22
     int tx = 30, ty = 16;
     int max_inst = 0;
@@ -324,10 +354,8 @@ struct sfg_batch_s {
     double* staging = nullptr;
     size_t staging_cap = 0;
     // kernels and graph
-    StageKernel stage_k = nullptr;
     ItemKernel dt_k = nullptr, copy_k = nullptr;
-    size_t smem = 0;
-    int grid_stage = 0, grid_items = 0;
+    int grid_items = 0;
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
     long long batch_steps = 0;
@@ -335,36 +363,80 @@ struct sfg_batch_s {
 
 namespace {
 
-int bind_kernels(sfg_batch_s* b) {
+// Stage kernel of one recipe group for the batch's tile shape and precision.
+int bind_group(sfg_batch_s* b, RecipeGroup& grp) {
     const bool f32 = b->num.precision == SFG_PREC_FP32_FLUX;
+    const int scheme = grp.recipe->scheme, flux = grp.recipe->flux;
     if (b->variant == 1) {
-        b->stage_k = f32 ? pick_stage<30, 16, true>(b->recipe->scheme, b->recipe->flux)
-                         : pick_stage<30, 16, false>(b->recipe->scheme, b->recipe->flux);
-        b->smem = stage_smem<30, 16>(b->recipe->scheme, f32);
+        grp.stage_k = f32 ? pick_stage<30, 16, true>(scheme, flux) : pick_stage<30, 16, false>(scheme, flux);
+        grp.smem = stage_smem<30, 16>(scheme, f32);
+    } else {
+        grp.stage_k = f32 ? pick_stage<22, 22, true>(scheme, flux) : pick_stage<22, 22, false>(scheme, flux);
+        grp.smem = stage_smem<22, 22>(scheme, f32);
+    }
+    if (!grp.stage_k) return bfail(SFG_ERR_ARG, "no batched stage kernel for recipe %d", grp.recipe->id);
+    BCUDA(cudaFuncSetAttribute(grp.stage_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)grp.smem));
+    int sms = 0, per_sm = 0;
+    BCUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
+    BCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grp.stage_k, TILE_THREADS, grp.smem));
+    if (per_sm < 1) return bfail(SFG_ERR_CUDA, "batched stage kernel does not fit an SM");
+    grp.grid = sms * per_sm;
+    return SFG_OK;
+}
+
+int bind_kernels(sfg_batch_s* b) {
+    if (b->variant == 1) {
         b->dt_k = batch_dt_kernel<30, 16>;
         b->copy_k = batch_copy_kernel<30, 16>;
         b->tx = 30;
         b->ty = 16;
     } else {
-        b->stage_k = f32 ? pick_stage<22, 22, true>(b->recipe->scheme, b->recipe->flux)
-                         : pick_stage<22, 22, false>(b->recipe->scheme, b->recipe->flux);
-        b->smem = stage_smem<22, 22>(b->recipe->scheme, f32);
         b->dt_k = batch_dt_kernel<22, 22>;
         b->copy_k = batch_copy_kernel<22, 22>;
         b->tx = 22;
         b->ty = 22;
     }
-    BCUDA(cudaFuncSetAttribute(b->stage_k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
-    int sms = 0, per_sm = 0;
+    for (auto& grp : b->groups) {
+        int rc = bind_group(b, grp);
+        if (rc) return rc;
+    }
+    int sms = 0;
     BCUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
-    BCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, b->stage_k, TILE_THREADS, b->smem));
-    if (per_sm < 1) return bfail(SFG_ERR_CUDA, "batched stage kernel does not fit an SM");
-    b->grid_stage = sms * per_sm;
     b->grid_items = sms * 4;
     if (b->graph) {
         cudaGraphExecDestroy(b->graph);
         b->graph = nullptr;
     }
+    return SFG_OK;
+}
+
+// Group index of a recipe; a recipe the batch has not run yet opens a group
+// (its kernel bound, a stream for its branch), which the next captured graph
+// includes.
+int group_of(sfg_batch_s* b, const RecipeParts* rp, int* out) {
+    for (int g = 0; g < (int)b->groups.size(); ++g)
+        if (b->groups[g].recipe == rp) {
+            *out = g;
+            return SFG_OK;
+        }
+    if ((int)b->groups.size() >= kMaxGroups) return bfail(SFG_ERR_ARG, "too many recipes in one batch");
+    RecipeGroup grp;
+    grp.recipe = rp;
+    int rc = bind_group(b, grp);
+    if (rc) return rc;
+    if (!b->groups.empty()) {
+        BCUDA(cudaStreamCreateWithFlags(&grp.side, cudaStreamNonBlocking));
+        if (cudaEventCreateWithFlags(&grp.joined, cudaEventDisableTiming) != cudaSuccess) {
+            cudaStreamDestroy(grp.side);
+            return bfail(SFG_ERR_CUDA, "event creation failed");
+        }
+    }
+    b->groups.push_back(grp);
+    if (b->graph) {  // the graph has no branch for the new group
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    *out = (int)b->groups.size() - 1;
     return SFG_OK;
 }
 
@@ -407,16 +479,21 @@ void slab_free(sfg_batch_s* b, size_t off, size_t bytes) {
 // instance count) to device memory.
 int publish_items(sfg_batch_s* b) {
     b->h_items.clear();
-    for (int i = 0; i < (int)b->h_inst.size(); ++i) {
-        const BatchInst& r = b->h_inst[i];
-        if (!r.live || r.done) continue;
-        const GridView& g = r.g;
-        if (g.dim == 1) {
-            for (int x = g.lo[0]; x < g.hi[0]; x += TILE1D) b->h_items.push_back({i, x, 0, 1});
-        } else {
-            for (int y = g.lo[1]; y < g.hi[1]; y += b->ty)
-                for (int x = g.lo[0]; x < g.hi[0]; x += b->tx) b->h_items.push_back({i, x, y, 2});
+    for (int grp = 0; grp < kMaxGroups; ++grp) {
+        const int first = (int)b->h_items.size();
+        for (int i = 0; grp < (int)b->groups.size() && i < (int)b->h_inst.size(); ++i) {
+            const BatchInst& r = b->h_inst[i];
+            if (!r.live || r.done || b->inst_group[i] != grp) continue;
+            const GridView& g = r.g;
+            if (g.dim == 1) {
+                for (int x = g.lo[0]; x < g.hi[0]; x += TILE1D) b->h_items.push_back({i, x, 0, 1});
+            } else {
+                for (int y = g.lo[1]; y < g.hi[1]; y += b->ty)
+                    for (int x = g.lo[0]; x < g.hi[0]; x += b->tx) b->h_items.push_back({i, x, y, 2});
+            }
         }
+        b->h_ctl->group_range[2 * grp] = first;
+        b->h_ctl->group_range[2 * grp + 1] = (int)b->h_items.size() - first;
     }
     if (b->h_items.size() > b->items_cap) {
         size_t cap = std::max<size_t>(b->h_items.size() * 2, 1024);
@@ -435,6 +512,8 @@ int publish_items(sfg_batch_s* b) {
     b->h_ctl->n_items = (int)b->h_items.size();
     b->h_ctl->n_inst = (int)b->h_inst.size();
     BCUDA(cudaMemcpyAsync(&b->d_ctl->n_items, &b->h_ctl->n_items, 2 * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+    BCUDA(cudaMemcpyAsync(b->d_ctl->group_range, b->h_ctl->group_range, sizeof b->h_ctl->group_range,
+                          cudaMemcpyHostToDevice, b->stream));
     BCUDA(cudaStreamSynchronize(b->stream));
     return SFG_OK;
 }
@@ -445,12 +524,40 @@ int enqueue_batch_step(sfg_batch_s* b) {
     b->dt_k<<<b->grid_items, TILE_THREADS, 0, b->stream>>>(b->d_inst, b->d_items, b->d_ctl);
     batch_finalize_kernel<<<(ni + 127) / 128, 128, 0, b->stream>>>(b->d_inst, b->d_ctl);
     const int ns = stage_count_of(b->num.time_recipe);
-    for (int s = 0; s < ns; ++s)
-        b->stage_k<<<b->grid_stage, TILE_THREADS, b->smem, b->stream>>>(b->d_inst, b->d_items, b->d_ctl, s,
-                                                                           b->num.time_recipe);
+    const int ng = (int)b->groups.size();
+    for (int s = 0; s < ns; ++s) {
+        // group 0 on the batch's stream, every other group on a branch
+        // forked from it and joined back before the next stage
+        if (ng > 1) BCUDA(cudaEventRecord(b->fork, b->stream));
+        for (int g = 0; g < ng; ++g) {
+            const RecipeGroup& grp = b->groups[g];
+            cudaStream_t st = g == 0 ? b->stream : grp.side;
+            if (g > 0) BCUDA(cudaStreamWaitEvent(st, b->fork, 0));
+            grp.stage_k<<<grp.grid, TILE_THREADS, grp.smem, st>>>(b->d_inst, b->d_items, b->d_ctl, s,
+                                                                   b->num.time_recipe, g);
+            if (g > 0) BCUDA(cudaEventRecord(grp.joined, st));
+        }
+        for (int g = 1; g < ng; ++g) BCUDA(cudaStreamWaitEvent(b->stream, b->groups[g].joined, 0));
+    }
     if (b->num.time_recipe == T_EULER) b->copy_k<<<b->grid_items, TILE_THREADS, 0, b->stream>>>(b->d_inst, b->d_items, b->d_ctl);
     batch_commit_kernel<<<(ni + 127) / 128, 128, 0, b->stream>>>(b->d_inst, b->d_ctl);
     BCUDA(cudaGetLastError());
+    return SFG_OK;
+}
+
+// Checks a grid's own numerics against the batch (same time recipe and
+// precision; a recipe with a batched kernel; gamma, CFL and maxDeltaT as
+// sfg_create accepts them) and returns its recipe.
+int instance_numerics(const sfg_batch_s* b, const sfg_numerics_desc* n, const RecipeParts** rp) {
+    *rp = nullptr;
+    for (const auto& r : kBatchRecipes)
+        if (r.id == n->recipe) *rp = &r;
+    if (!*rp) return bfail(SFG_ERR_ARG, "convection recipe %d is not provided on the GPU", n->recipe);
+    if (n->time_recipe != b->num.time_recipe) return bfail(SFG_ERR_ARG, "a batch runs one time recipe");
+    if (n->precision != b->num.precision) return bfail(SFG_ERR_ARG, "a batch runs one precision mode");
+    if (!(n->gamma > 1.0) || !std::isfinite(n->gamma)) return bfail(SFG_ERR_ARG, "gamma must be > 1");
+    if (!(n->cfl > 0.0) || !std::isfinite(n->cfl)) return bfail(SFG_ERR_ARG, "CFL must be finite and > 0");
+    if (n->max_dt != n->max_dt) return bfail(SFG_ERR_ARG, "maxDeltaT is NaN");
     return SFG_OK;
 }
 
@@ -494,6 +601,14 @@ int batch_grid_view(const sfg_grid_desc* d, const sfg_numerics_desc* n, int reac
 }
 
 }  // namespace
+
+namespace sfg {
+// A request's own numerics, checked at submit before it queues (sfg_server.cu).
+int batch_check_numerics(sfg_batch b, const sfg_numerics_desc* n) {
+    const RecipeParts* rp = nullptr;
+    return instance_numerics(b, n, &rp);
+}
+}  // namespace sfg
 
 extern "C" {
 
@@ -542,7 +657,12 @@ int sfg_batch_create(const sfg_numerics_desc* numerics, size_t hbm_budget_bytes,
     cudaMemsetAsync(b->d_inst, 0, sizeof(BatchInst) * (size_t)max_instances, b->stream);
     cudaMemsetAsync(b->d_ctl, 0, sizeof(BatchCtl), b->stream);
     std::memset(b->h_ctl, 0, sizeof(BatchCtl));
+    if (cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess)
+        return cleanup(bfail(SFG_ERR_CUDA, "event creation failed"));
     int rc = bind_kernels(b);
+    if (rc) return cleanup(rc);
+    int g0 = 0;
+    rc = group_of(b, rp, &g0);  // the default recipe is group 0
     if (rc) return cleanup(rc);
     rc = publish_items(b);
     if (rc) return cleanup(rc);
@@ -560,6 +680,11 @@ int sfg_batch_destroy(sfg_batch b) {
     if (b->d_ctl) cudaFree(b->d_ctl);
     if (b->staging) cudaFree(b->staging);
     if (b->h_ctl) cudaFreeHost(b->h_ctl);
+    for (auto& grp : b->groups) {
+        if (grp.side) cudaStreamDestroy(grp.side);
+        if (grp.joined) cudaEventDestroy(grp.joined);
+    }
+    if (b->fork) cudaEventDestroy(b->fork);
     if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return SFG_OK;
@@ -579,11 +704,23 @@ int sfg_batch_instance_bytes(sfg_batch b, const sfg_grid_desc* grid, size_t* byt
 
 int sfg_batch_add(sfg_batch b, const sfg_grid_desc* grid, const double* host_nodes_aos, double t_end,
                   int64_t max_steps, int* slot) {
+    return sfg_batch_add_ex(b, grid, nullptr, host_nodes_aos, t_end, max_steps, slot);
+}
+
+int sfg_batch_add_ex(sfg_batch b, const sfg_grid_desc* grid, const sfg_numerics_desc* numerics,
+                     const double* host_nodes_aos, double t_end, int64_t max_steps, int* slot) {
     if (!b || !grid || !host_nodes_aos || !slot) return bfail(SFG_ERR_ARG, "null argument");
+    const sfg_numerics_desc& num = numerics ? *numerics : b->num;
+    const RecipeParts* rp = nullptr;
+    int rc = instance_numerics(b, &num, &rp);
+    if (rc) return rc;
     GridView g;
     long long nodes = 0;
-    const int reach = b->recipe->scheme == WENO3 ? 2 : (b->recipe->scheme == WENO7 ? 4 : 3);
-    int rc = batch_grid_view(grid, &b->num, reach, &g, &nodes);
+    const int reach = rp->scheme == WENO3 ? 2 : (rp->scheme == WENO7 ? 4 : 3);
+    rc = batch_grid_view(grid, &num, reach, &g, &nodes);
+    if (rc) return rc;
+    int group = 0;
+    rc = group_of(b, rp, &group);
     if (rc) return rc;
     int idx = -1;
     for (int i = 0; i < (int)b->h_inst.size(); ++i)
@@ -597,6 +734,7 @@ int sfg_batch_add(sfg_batch b, const sfg_grid_desc* grid, const double* host_nod
         b->h_inst.push_back(BatchInst{});
         b->inst_offset.push_back(0);
         b->inst_bytes.push_back(0);
+        b->inst_group.push_back(0);
     }
     const size_t per = (sizeof(double) * 5 * (size_t)g.vs + 255) / 256 * 256;
     const int bufs = b->num.time_recipe == T_RK4 ? 4 : 3;
@@ -624,7 +762,7 @@ int sfg_batch_add(sfg_batch b, const sfg_grid_desc* grid, const double* host_nod
     r.clock.t = 0.0;
     r.clock.t_end = t_end;
     r.clock.next_out = kInfB;
-    r.clock.max_dt = b->num.max_dt;
+    r.clock.max_dt = num.max_dt > 0.0 ? num.max_dt : kInfB;
     r.clock.limit = kInfB;
     r.clock.dt_bits = 0x7FEFFFFFFFFFFFFFull;
     r.clock.max_steps = max_steps > 0 ? max_steps : std::numeric_limits<long long>::max();
@@ -638,6 +776,7 @@ int sfg_batch_add(sfg_batch b, const sfg_grid_desc* grid, const double* host_nod
     b->h_inst[idx] = r;
     b->inst_offset[idx] = off;
     b->inst_bytes[idx] = per * bufs;
+    b->inst_group[idx] = group;
     rc = publish_items(b);  // synchronises the stream
     if (rc) return rc;
     *slot = idx;

@@ -676,7 +676,9 @@ __global__ void __launch_bounds__(128, 4) curv_face_f32_kernel(GridView g, Stage
 // ---------------------------------------------------------------------------
 // 2-D FP32-flux stage fused in one tile (the curvilinear form of
 // tile2d_f32_body): the tile and its halo staged as FP32 deviations from the
-// tile's first node q_ref; every x and y face of the tile from shared memory
+// stage's reference node q_ref (ref_node, shared by every tile, so a
+// tile-edge face has the same bits in both tiles); every x and y face of the
+// tile from shared memory
 // with its own normal and area, as the flux deviation dF * area; per node
 // div = sum dF area (FP64) + (sum of the node's face cofactors) . F(q_ref),
 // the second term in FP64 (on a curved grid the reference flux does not
@@ -697,11 +699,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 3) curv_tile2d_f32_kernel(GridVi
     const long long nx = g.n[0], vs = g.vs;
     unsigned flags = 0, cut = 0, cores = 0;
     double qref[5];
-    {
-        const long long at = (long long)y0 * nx + x0;
-#pragma unroll
-        for (int v = 0; v < 5; ++v) qref[v] = __ldg(sv.qs + v * vs + at);
-    }
+    load_ref(g, sv.qs, qref);
     const Ref32 ref = make_ref32(qref, g.gamma);
     for (int t = threadIdx.x; t < SX * SY; t += blockDim.x) {
         const int r = t / SX, c = t - r * SX;
@@ -798,9 +796,9 @@ __global__ void __launch_bounds__(TILE_THREADS, 3) curv_tile2d_f32_kernel(GridVi
         for (int v = 0; v < 5; ++v) {
             const float* fxv = fx + v * NFX + r * (TX + 1) + c;
             const float* fyv = fy + v * NFY + r * TX + c;
-            // deviation differences in FP32 (one conversion), the reference
+            // FP32 face deviations with exact FP64 differences, the reference
             // flux term in FP64
-            div[v] = double((fxv[1] - fxv[0]) + (fyv[TX] - fyv[0])) +
+            div[v] = (double(fxv[1]) - double(fxv[0])) + (double(fyv[TX]) - double(fyv[0])) +
                      (gc[0] * Fc[0][v] + gc[1] * Fc[1][v] + gc[2] * Fc[2][v]);
             qn[v] = __ldg(sv.qs + v * vs + node);
         }

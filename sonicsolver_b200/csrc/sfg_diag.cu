@@ -52,7 +52,9 @@ __device__ __forceinline__ void teno_flips_face(const GridView& g, const double*
         float2 b2[5], B[3], q[3], keep[3];
         for (int s = 0; s < 5; ++s) b2[s] = make_float2(c32[s][v], c32[NST - 1 - s][v]);
         stencil5x2(b2, B, q);
-        teno_keep32x2(B[0], B[1], B[2], keep, fl);
+        float2 bad = make_float2(0.f, 0.f);
+        teno_keep32x2(B[0], B[1], B[2], keep, bad);
+        flag_bad(bad, fl);
         for (int side = 0; side < 2; ++side) {
             double a[5];
             for (int s = 0; s < 5; ++s) a[s] = side ? c64[NST - 1 - s][v] : c64[s][v];

@@ -58,17 +58,16 @@ __global__ void __launch_bounds__(128, 5) sweep_x(GridView g, StageView sv) {
         }
         T Ft[5];
         if constexpr (sizeof(T) == sizeof(float)) {
-            // deviations from the chunk's first node, shared by the whole warp
+            // deviations from the stage's reference node (ref_node)
             double qref[5];
-#pragma unroll
-            for (int v = 0; v < 5; ++v) qref[v] = __ldg(sv.qs + v * vs + rowbase + i0);
+            load_ref(g, sv.qs, qref);
             const Ref32 ref = make_ref32(qref, g.gamma);
             float d[NST][5];
 #pragma unroll
             for (int s = 0; s < NST; ++s)
 #pragma unroll
                 for (int v = 0; v < 5; ++v) d[s][v] = float(st[s][v] - qref[v]);
-            face_flux_dev32<0, SCHEME, FLUX>(d, ref, float(g.gamma), Ft, flags, cut);
+            face_flux_dev32<0, SCHEME, FLUX>(d, ref, float(g.gamma), Ft, flags, cut, sv.counters != nullptr);
         } else {
             face_flux<0, SCHEME, FLUX, T>(st, T(g.gamma), Ft, flags, cut, T(FLUX == LAXW ? sv.clock->dt / g.h[0] : 0.0));
         }
@@ -105,10 +104,11 @@ __global__ void __launch_bounds__(128, 5) sweep_x(GridView g, StageView sv) {
 constexpr int SEGLEN = 16;
 
 // FP32-flux segment: the register window holds FP32 deviations from the
-// segment's first node (one FP64 -> FP32 rounding per node), the face fluxes
-// are deviations F - F(q_ref) (face_flux_dev32).  Both faces of every node of
-// the segment share the reference, so F(q_ref) cancels from the divergence
-// exactly.  The FP64 node value for the stage update is re-read (L1 / L2).
+// stage's reference node (ref_node; one FP64 -> FP32 rounding per node), the
+// face fluxes are deviations F - F(q_ref) (face_flux_dev32).  Every face of
+// the launch shares the reference, so F(q_ref) cancels from the divergence
+// exactly and a face on a segment boundary has the same bits in both
+// segments.  The FP64 node value for the stage update is re-read (L1 / L2).
 template <int AX, int SCHEME, int FLUX>
 __device__ __forceinline__ void sweep_yz_f32_segment(const GridView& g, const StageView& sv, int i, int o, int s0,
                                                      unsigned& flags, unsigned& cut, unsigned& cores,
@@ -124,8 +124,7 @@ __device__ __forceinline__ void sweep_yz_f32_segment(const GridView& g, const St
     const int bl = g.bc_lo[AX], bh = g.bc_hi[AX];
     const double dt = sv.clock->dt;
     double qref[5];
-#pragma unroll
-    for (int v = 0; v < 5; ++v) qref[v] = sv.qs[v * vs + base + (long long)s0 * sa];
+    load_ref(g, sv.qs, qref);
     const Ref32 ref = make_ref32(qref, g.gamma);
     const float gamma = float(g.gamma);
     float d[NST][5];
@@ -138,7 +137,7 @@ __device__ __forceinline__ void sweep_yz_f32_segment(const GridView& g, const St
     double Fp[5];
     for (int f = s0; f <= s1; ++f) {
         float Ft[5];
-        face_flux_dev32<AX, SCHEME, FLUX>(d, ref, gamma, Ft, flags, cut);
+        face_flux_dev32<AX, SCHEME, FLUX>(d, ref, gamma, Ft, flags, cut, sv.counters != nullptr);
         if (SCHEME == TENO5) cores += 10;
         double F[5];
 #pragma unroll

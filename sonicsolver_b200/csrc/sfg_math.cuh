@@ -58,6 +58,23 @@ __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __
 __device__ __forceinline__ float2 swap2(float2 a) { return make_float2(a.y, a.x); }
 __device__ __forceinline__ float2 rcp2(float2 a) { return make_float2(rcp_approx(a.x), rcp_approx(a.y)); }
 
+// 1.0f where a >= b, else 0.0f (also for NaN operands): PTX set with a
+// floating-point destination, one instruction instead of a compare and a
+// select.
+__device__ __forceinline__ float ge_one(float a, float b) {
+    float r;
+    asm("set.ge.f32.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+    return r;
+}
+
+// Non-finite watch over a face's paired FP32 work: bad + x * 0 stays exactly
+// 0 while every x is finite and turns NaN after an inf or a NaN, one paired
+// FMA per watched value and one test per face (flag_bad).
+__device__ __forceinline__ float2 watch2(float2 bad, float2 x) { return __ffma2_rn(x, make_float2(0.f, 0.f), bad); }
+__device__ __forceinline__ void flag_bad(float2 bad, unsigned& flags) {
+    if (!(bad.x == 0.f && bad.y == 0.f)) flags |= FLAG_NONFINITE;
+}
+
 template <typename T> __device__ __forceinline__ T div_(T a, T b);
 template <> __device__ __forceinline__ double div_<double>(double a, double b) { return a / b; }
 template <> __device__ __forceinline__ float div_<float>(float a, float b) { return __fdividef(a, b); }
@@ -301,10 +318,11 @@ template <> struct Teno<double> {
 // overflows and no 0/0 or 0*inf arises, with no branch.  Keep k iff
 // x_k^6 >= CT * sum_j x_j^6 -- the reference's gamma_k / sum gamma >= CT
 // divided through by g_max^6.  eps is FLT_MIN: the reference's 1e-40 is
-// subnormal in FP32, whose reciprocal leaves the range.  keep[k] = 1 or 0.
+// subnormal in FP32, whose reciprocal leaves the range.  keep[k] = 1 or 0
+// (0 for a NaN input, which `bad` reports).
 constexpr float TENO32_EPS = 1.17549435e-38f;
 
-__device__ __forceinline__ void teno_keep32x2(float2 b0, float2 b1, float2 b2, float2 (&keep)[3], unsigned& flags) {
+__device__ __forceinline__ void teno_keep32x2(float2 b0, float2 b1, float2 b2, float2 (&keep)[3], float2& bad) {
     const float2 e0 = add2(b0, f2(TENO32_EPS)), e1 = add2(b1, f2(TENO32_EPS)), e2 = add2(b2, f2(TENO32_EPS));
     const float2 d02 = sub2(b0, b2);
     const float2 tau = f2(fabsf(d02.x), fabsf(d02.y));
@@ -315,16 +333,18 @@ __device__ __forceinline__ void teno_keep32x2(float2 b0, float2 b1, float2 b2, f
     const float2 y0 = mul2(x0, x0), y1 = mul2(x1, x1), y2 = mul2(x2, x2);
     const float2 G0 = mul2(mul2(y0, y0), y0), G1 = mul2(mul2(y1, y1), y1), G2 = mul2(mul2(y2, y2), y2);
     const float2 lim = mul2(f2(1e-5f), add2(add2(G0, G1), G2));
-    if (!(lim.x < 1.f) || !(lim.y < 1.f)) flags |= FLAG_NONFINITE;  // NaN input (lim <= 3e-5 otherwise)
-    keep[0] = f2(G0.x < lim.x ? 0.f : 1.f, G0.y < lim.y ? 0.f : 1.f);
-    keep[1] = f2(G1.x < lim.x ? 0.f : 1.f, G1.y < lim.y ? 0.f : 1.f);
-    keep[2] = f2(G2.x < lim.x ? 0.f : 1.f, G2.y < lim.y ? 0.f : 1.f);
+    bad = watch2(bad, lim);  // NaN input (lim <= 3e-5 otherwise)
+    keep[0] = f2(ge_one(G0.x, lim.x), ge_one(G0.y, lim.y));
+    keep[1] = f2(ge_one(G1.x, lim.x), ge_one(G1.y, lim.y));
+    keep[2] = f2(ge_one(G2.x, lim.x), ge_one(G2.y, lim.y));
 }
 
 template <> struct Teno<float> {
     static __device__ __forceinline__ int keep_mask(float b0, float b1, float b2, unsigned& flags) {
         float2 k[3];
-        teno_keep32x2(f2(b0), f2(b1), f2(b2), k, flags);
+        float2 bad = f2(0.f);
+        teno_keep32x2(f2(b0), f2(b1), f2(b2), k, bad);
+        flag_bad(bad, flags);
         return int(k[0].x != 0.f) | (int(k[1].x != 0.f) << 1) | (int(k[2].x != 0.f) << 2);
     }
     static __device__ __forceinline__ float core(const float* v, unsigned& flags, unsigned& cut) {
@@ -696,25 +716,27 @@ __device__ __forceinline__ void face_flux(const double (&st)[SchemeInfo<SCHEME>:
 //   p_k - 6 v2 = q_k:  q0 = 5 D1 - 2 D0 = 2 t0 + 3 D1, q1 = D1 + 2 D2, q2 = 4 D2 - D3 = D2 - r2
 // (r1 is the reference's v1 - v3 up to sign, which the square removes), so a
 // reconstruction sum w_k p_k / (6 sum w_k) is v2 + sum w_k q_k / (6 sum w_k).
-// The indicators are scaled by 12 and the epsilons with them, which leaves
-// every weight unchanged; only differences of the stencil are rounded.
+// The indicators are returned as B_k / 3 = 4 b_k = 13/3 t_k^2 + r_k^2 (one
+// multiply fewer than 12 b_k) and the epsilons are scaled with them, which
+// leaves every weight unchanged; only differences of the stencil are rounded.
 __device__ __forceinline__ void stencil5x2(const float2* v, float2 (&B)[3], float2 (&q)[3]) {
     const float2 D0 = sub2(v[1], v[0]), D1 = sub2(v[2], v[1]), D2 = sub2(v[3], v[2]), D3 = sub2(v[4], v[3]);
     const float2 t0 = sub2(D1, D0), t1 = sub2(D2, D1), t2 = sub2(D3, D2);
     const float2 r0 = fma2(f2(2.f), D1, t0), r1 = add2(D1, D2), r2 = fma2(f2(-2.f), D2, t2);
-    B[0] = fma2(mul2(f2(13.f), t0), t0, mul2(mul2(f2(3.f), r0), r0));
-    B[1] = fma2(mul2(f2(13.f), t1), t1, mul2(mul2(f2(3.f), r1), r1));
-    B[2] = fma2(mul2(f2(13.f), t2), t2, mul2(mul2(f2(3.f), r2), r2));
+    const float2 c = f2(13.f / 3.f);
+    B[0] = fma2(mul2(c, t0), t0, mul2(r0, r0));
+    B[1] = fma2(mul2(c, t1), t1, mul2(r1, r1));
+    B[2] = fma2(mul2(c, t2), t2, mul2(r2, r2));
     q[0] = fma2(f2(2.f), t0, mul2(f2(3.f), D1));
     q[1] = fma2(f2(2.f), D2, D1);
     q[2] = sub2(D2, r2);
 }
 
 // WENO5-JS on a (left, right) stencil pair; same folding as weno5_core.
-__device__ __forceinline__ float2 weno5_core2(const float2* v, unsigned& flags) {
+__device__ __forceinline__ float2 weno5_core2(const float2* v, float2& bad) {
     float2 B[3], q[3];
     stencil5x2(v, B, q);
-    const float2 eps = f2(12.f * 1e-6f);
+    const float2 eps = f2(4.f * 1e-6f);  // the reference's 1e-6 on B_k / 3 = 4 b_k
     const float2 e0 = add2(eps, B[0]), e1 = add2(eps, B[1]), e2 = add2(eps, B[2]);
     const float2 s0 = mul2(e0, e0), s1 = mul2(e1, e1), s2 = mul2(e2, e2);
     const float2 w0 = mul2(f2(0.1f), mul2(s1, s2));
@@ -722,18 +744,19 @@ __device__ __forceinline__ float2 weno5_core2(const float2* v, unsigned& flags) 
     const float2 w2 = mul2(f2(0.3f), mul2(s0, s1));
     const float2 den = mul2(f2(6.f), add2(add2(w0, w1), w2));
     const float2 num = fma2(w0, q[0], fma2(w1, q[1], mul2(w2, q[2])));
-    if (!(den.x > 0.f && den.x < INFINITY) || !(den.y > 0.f && den.y < INFINITY)) flags |= FLAG_NONFINITE;
+    bad = watch2(bad, den);  // den >= 6 eps^4 > 0 unless an input was not finite
     return fma2(num, rcp2(den), v[2]);
 }
 
 // TENO5 on a (left, right) stencil pair, all of it paired: polynomials,
-// smoothness indicators, the cut-off (teno_keep32x2) and the weights.
-// `kept` accumulates the kept sub-stencils of each lane.
-__device__ __forceinline__ float2 teno5_core2(const float2* v, unsigned& flags, float2& kept) {
+// smoothness indicators, the cut-off (teno_keep32x2) and the weights.  With
+// `count` (a launch-uniform switch: the cut-off accounting of
+// sfg_set_counting), `kept` accumulates the kept sub-stencils of each lane.
+__device__ __forceinline__ float2 teno5_core2(const float2* v, float2& bad, bool count, float2& kept) {
     float2 B[3], q[3], k[3];
     stencil5x2(v, B, q);
-    teno_keep32x2(B[0], B[1], B[2], k, flags);
-    kept = add2(kept, add2(add2(k[0], k[1]), k[2]));
+    teno_keep32x2(B[0], B[1], B[2], k, bad);
+    if (count) kept = add2(kept, add2(add2(k[0], k[1]), k[2]));
     const float2 d0 = mul2(f2(0.1f), k[0]), d1 = mul2(f2(0.6f), k[1]), d2 = mul2(f2(0.3f), k[2]);
     // No all-cut check: the sub-stencil with x = 1 always passes (G ~ 1 >
     // lim <= 3e-5, and a NaN lim fails every '<'), so act >= 0.6.
@@ -960,7 +983,7 @@ __device__ __forceinline__ void rusanov_dev2(const Ref32& r, const float2 d[5], 
 // face_flux_dev32 with the left / right work paired in float2 (WENO5, TENO5).
 template <int AX, int SCHEME, int FLUX>
 __device__ __forceinline__ void face_flux_dev32x2(const float (&d)[6][5], const Ref32& ref, float gamma, float F[5],
-                                                  unsigned& flags, unsigned& cut) {
+                                                  unsigned& flags, unsigned& cut, bool count) {
     float dbar[5], qbar[5];
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
@@ -980,15 +1003,18 @@ __device__ __forceinline__ void face_flux_dev32x2(const float (&d)[6][5], const 
         to_characteristic2<AX>(e, x, P[k]);
     }
     float2 w[5];
-    float2 kept = f2(0.f);
+    float2 kept = f2(0.f), bad = f2(0.f);
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
         // left stencil c0..c4 and right stencil c5..c1 as one paired stencil
         const float2 st[5] = {P[0][v], P[1][v], P[2][v], swap2(P[2][v]), swap2(P[1][v])};
-        if constexpr (SCHEME == TENO5) w[v] = teno5_core2(st, flags, kept);
-        else w[v] = weno5_core2(st, flags);
+        if constexpr (SCHEME == TENO5) w[v] = teno5_core2(st, bad, count, kept);
+        else w[v] = weno5_core2(st, bad);
     }
-    if constexpr (SCHEME == TENO5) cut += 30u - unsigned(kept.x + kept.y);
+    flag_bad(bad, flags);
+    if constexpr (SCHEME == TENO5) {
+        if (count) cut += 30u - unsigned(kept.x + kept.y);
+    }
     float2 dq[5], x2[5];
     from_characteristic2<AX>(e, w, dq);
 #pragma unroll
@@ -1007,18 +1033,21 @@ __device__ __forceinline__ void face_flux_dev32x2(const float (&d)[6][5], const 
 }
 
 // FP32 face flux from a stencil held as FP32 deviations d_s = q_s - q_ref
-// from a reference state shared by a whole tile (q_ref is FP64 in HBM; only
-// the deviations are rounded to FP32, once per node when the tile is staged).
-// Same mathematics as face_flux: q-bar = q_ref + (d_CL + d_CL+1)/2, the
-// projection and reconstruction act on d_s - d-bar.  Returns the flux as a
-// deviation from F(q_ref) (rusanov_dev / roe_dev): within a tile the
-// reference flux cancels exactly in every difference dF, so FP32 rounding
-// scales with the variation across the tile, not with |F|.
+// from a reference state shared by a whole stage launch (q_ref is FP64 in
+// HBM; only the deviations are rounded to FP32, once per node when a tile is
+// staged).  Same mathematics as face_flux: q-bar = q_ref + (d_CL + d_CL+1)/2,
+// the projection and reconstruction act on d_s - d-bar.  Returns the flux as
+// a deviation from F(q_ref) (rusanov_dev / roe_dev): the reference flux
+// cancels exactly in every difference dF, so FP32 rounding scales with the
+// distance from the reference state, not with |F|.
+// `count`: the launch's TENO5 cut-off accounting is on (sfg_set_counting);
+// `cut` then receives the cut sub-stencils of the face.
 template <int AX, int SCHEME, int FLUX>
 __device__ __forceinline__ void face_flux_dev32(const float (&d)[SchemeInfo<SCHEME>::NST][5], const Ref32& ref,
-                                                float gamma, float F[5], unsigned& flags, unsigned& cut) {
+                                                float gamma, float F[5], unsigned& flags, unsigned& cut,
+                                                bool count = true) {
     if constexpr (SCHEME == WENO5 || SCHEME == TENO5) {
-        face_flux_dev32x2<AX, SCHEME, FLUX>(d, ref, gamma, F, flags, cut);
+        face_flux_dev32x2<AX, SCHEME, FLUX>(d, ref, gamma, F, flags, cut, count);
         return;
     }
     const float (&qref)[5] = ref.q;

@@ -1282,15 +1282,43 @@ int sfg_time_sweeps(sfg_solver s, int stage, double dt, int repeats, float* ms_p
     CUDA_TRY(launch_set_dt(s->clock, dt, s->stream));
     StageView sv = stage_view(s, stage, false, false);
     if (s->variant > 0 || s->gv.curv) {  // one stage operator (tiles, or the curvilinear launches)
-        for (int r = 0; r < repeats; ++r) {
-            CUDA_TRY(cudaEventRecord(ev[0], s->stream));
-            int rc = enqueue_stage(s, stage, false, false);
+        // `repeats` back-to-back launches captured as one CUDA graph, as the
+        // stages run inside a step's graph: the events bracket the graph,
+        // so host launch latency does not enter the per-launch time
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        CUDA_TRY(cudaStreamIsCapturing(s->stream, &cap));
+        cudaGraphExec_t exec = nullptr;
+        if (s->stream != nullptr && cap == cudaStreamCaptureStatusNone) {
+            cudaGraph_t graph;
+            CUDA_TRY(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+            int rc = SFG_OK;
+            for (int r = 0; r < repeats && !rc; ++r) rc = enqueue_stage(s, stage, false, false);
+            const cudaError_t ce = cudaStreamEndCapture(s->stream, &graph);
             if (rc) return rc;
+            CUDA_TRY(ce);
+            const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+            cudaGraphDestroy(graph);
+            CUDA_TRY(ie);
+            CUDA_TRY(cudaGraphLaunch(exec, s->stream));  // warm
+            CUDA_TRY(cudaEventRecord(ev[0], s->stream));
+            CUDA_TRY(cudaGraphLaunch(exec, s->stream));
             CUDA_TRY(cudaEventRecord(ev[1], s->stream));
             CUDA_TRY(cudaEventSynchronize(ev[1]));
+            cudaGraphExecDestroy(exec);
             float ms = 0.f;
             CUDA_TRY(cudaEventElapsedTime(&ms, ev[0], ev[1]));
-            acc[0] += ms;
+            acc[0] = ms;
+        } else {  // the legacy default stream cannot be captured: launch by launch
+            for (int r = 0; r < repeats; ++r) {
+                CUDA_TRY(cudaEventRecord(ev[0], s->stream));
+                int rc = enqueue_stage(s, stage, false, false);
+                if (rc) return rc;
+                CUDA_TRY(cudaEventRecord(ev[1], s->stream));
+                CUDA_TRY(cudaEventSynchronize(ev[1]));
+                float ms = 0.f;
+                CUDA_TRY(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+                acc[0] += ms;
+            }
         }
         for (auto& e : ev) cudaEventDestroy(e);
         ms_per_axis[0] = (float)(acc[0] / repeats);

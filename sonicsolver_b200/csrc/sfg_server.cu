@@ -26,6 +26,7 @@
 
 namespace sfg {
 void set_last_error(const char* msg);
+int batch_check_numerics(sfg_batch b, const sfg_numerics_desc* n);
 }
 
 namespace {
@@ -43,6 +44,8 @@ int sfail(int code, const char* fmt, ...) {
 struct Request {
     int64_t id = 0;
     sfg_grid_desc grid{};
+    sfg_numerics_desc num{};  // the request's own numerics (has_num)
+    bool has_num = false;
     std::vector<double> input, output;
     double t_end = 0.0;
     int64_t max_steps = 0;
@@ -129,7 +132,8 @@ void worker_loop(sfg_server_s* s) {
         }
         for (Request* r : admit) {
             int slot = -1;
-            int rc = sfg_batch_add(s->batch, &r->grid, r->input.data(), r->t_end, r->max_steps, &slot);
+            int rc = sfg_batch_add_ex(s->batch, &r->grid, r->has_num ? &r->num : nullptr, r->input.data(), r->t_end,
+                                      r->max_steps, &slot);
             std::lock_guard<std::mutex> lock(s->mu);
             if (rc == SFG_ERR_BUDGET) {  // fragmentation: retry at the queue head
                 s->queue.push_front(r->id);
@@ -235,7 +239,16 @@ int sfg_server_destroy(sfg_server s) {
 
 int sfg_server_submit(sfg_server s, const sfg_grid_desc* grid, const double* host_nodes_aos, double t_end,
                       int64_t max_steps, int64_t* request_id) {
+    return sfg_server_submit_ex(s, grid, nullptr, host_nodes_aos, t_end, max_steps, request_id);
+}
+
+int sfg_server_submit_ex(sfg_server s, const sfg_grid_desc* grid, const sfg_numerics_desc* numerics,
+                         const double* host_nodes_aos, double t_end, int64_t max_steps, int64_t* request_id) {
     if (!s || !grid || !host_nodes_aos || !request_id) return sfail(SFG_ERR_ARG, "null argument");
+    if (numerics) {
+        int rc = sfg::batch_check_numerics(s->batch, numerics);  // no device work
+        if (rc) return rc;
+    }
     size_t bytes = 0;
     int rc = sfg_batch_instance_bytes(s->batch, grid, &bytes);  // validates the grid; no device work
     if (rc) return rc;
@@ -246,6 +259,10 @@ int sfg_server_submit(sfg_server s, const sfg_grid_desc* grid, const double* hos
     Request r;
     r.id = s->next_id++;
     r.grid = *grid;
+    if (numerics) {
+        r.num = *numerics;
+        r.has_num = true;
+    }
     r.input.assign(host_nodes_aos, host_nodes_aos + count);
     r.t_end = t_end;
     r.max_steps = max_steps;

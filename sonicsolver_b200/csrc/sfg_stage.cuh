@@ -30,6 +30,22 @@ __device__ __forceinline__ int map_index(int i, int n, int bcl, int bch) {
     return i;
 }
 
+// FP32-flux reference state of a stage: the grid's first solved node of the
+// stage's input.  Every tile, chunk and segment of a launch takes the same
+// one, so a face that two of them evaluate (a tile edge, a chunk boundary)
+// gets the same FP32 inputs and the same bits on both sides, and every face
+// flux enters the divergence of its two nodes as one value.
+__device__ __forceinline__ long long ref_node(const GridView& g) {
+    return ((long long)g.lo[2] * g.n[1] + g.lo[1]) * g.n[0] + g.lo[0];
+}
+
+// Loads the FP64 reference state of a stage (ref_node of the stage input).
+__device__ __forceinline__ void load_ref(const GridView& g, const double* qs, double (&qref)[5]) {
+    const long long at = ref_node(g);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) qref[v] = __ldg(qs + v * g.vs + at);
+}
+
 __device__ __forceinline__ void atomic_min_positive(unsigned long long* bits, double v) {
     atomicMin(bits, (unsigned long long)__double_as_longlong(v));
 }
@@ -142,10 +158,12 @@ __device__ __forceinline__ void finish_node_j(const GridView& g, const StageView
     for (int v = 0; v < 5; ++v) out[v] = stage_value(sv, dt, qn[v], jac * div[v] - 0.0, v * vs + node);
 #pragma unroll
     for (int v = 0; v < 5; ++v) sv.qout[v * vs + node] = out[v];
-    const double ke = 0.5 * (out[1] * out[1] + out[2] * out[2] + out[3] * out[3]) / out[0];
-    const double p = (g.gamma - 1.0) * (out[4] - ke);
+    // p = (gamma - 1)(E - |m|^2 / (2 rho)) > 0 with rho > 0 is 2 E rho > |m|^2:
+    // the same test without a division (it differs only where p is within
+    // rounding of 0)
+    const double m2 = out[1] * out[1] + out[2] * out[2] + out[3] * out[3];
     if (!(out[0] > 0.0)) flags |= FLAG_DENSITY;
-    if (!(p > 0.0)) flags |= FLAG_PRESSURE;
+    else if (!(2.0 * out[4] * out[0] > m2)) flags |= FLAG_PRESSURE;
     if (!isfinite(out[0] + out[1] + out[2] + out[3] + out[4])) flags |= FLAG_NONFINITE;
     if (sv.mode & MODE_CFL) sr_max = fmax(sr_max, CURV ? cfl_rate_node(g, out, node) : cfl_rate(g, out));
 }

@@ -15,10 +15,14 @@
 // Faces on a tile edge are evaluated by both neighbouring tiles from the same
 // inputs, so both see the identical flux and the update stays conservative.
 //
-// FP32-flux bodies stage the tile as FP32 deviations from one FP64 reference
-// state per tile (its first node): the FP64 -> FP32 rounding happens once per
-// staged node, and the shared arrays are half the size.  Their fluxes are
-// FP32; flux differences, residual and stage update are FP64.
+// FP32-flux bodies stage the tile as FP32 deviations from the stage's FP64
+// reference state (ref_node: the grid's first solved node, the same for every
+// tile of a launch): the FP64 -> FP32 rounding happens once per staged node,
+// the shared arrays are half the size, and a tile-edge face gets the same
+// FP32 inputs, hence the same bits, in both tiles.  Their fluxes are FP32;
+// the flux differences (exact: a difference of two floats is exact in
+// double), residual and stage update are FP64, so the divergence telescopes
+// and the conserved totals drift only at FP64 round-off, as in the FP64 path.
 #pragma once
 
 #include <type_traits>
@@ -149,11 +153,7 @@ __device__ __forceinline__ void tile2d_f32_body(const GridView& g, const StageVi
     float* fy = fx + 5 * NFX;       // [5][TY+1][TX]
     const long long nx = g.n[0], vs = g.vs;
     double qref[5];
-    {
-        const long long at = (long long)y0 * nx + x0;
-#pragma unroll
-        for (int v = 0; v < 5; ++v) qref[v] = __ldg(sv.qs + v * vs + at);
-    }
+    load_ref(g, sv.qs, qref);
     const Ref32 ref = make_ref32(qref, g.gamma);
     for (int t = threadIdx.x; t < SX * SY; t += blockDim.x) {
         const int r = t / SX, c = t - r * SX;
@@ -177,7 +177,7 @@ __device__ __forceinline__ void tile2d_f32_body(const GridView& g, const StageVi
             for (int s = 0; s < NST; ++s)
 #pragma unroll
                 for (int v = 0; v < 5; ++v) st[s][v] = base[v * SX * SY + s];
-            face_flux_dev32<0, SCHEME, FLUX>(st, ref, gamma, Ft, flags, cut);
+            face_flux_dev32<0, SCHEME, FLUX>(st, ref, gamma, Ft, flags, cut, sv.counters != nullptr);
             const float a = float(g.area[0]);
 #pragma unroll
             for (int v = 0; v < 5; ++v) fx[v * NFX + f] = Ft[v] * a;
@@ -190,7 +190,7 @@ __device__ __forceinline__ void tile2d_f32_body(const GridView& g, const StageVi
             for (int s = 0; s < NST; ++s)
 #pragma unroll
                 for (int v = 0; v < 5; ++v) st[s][v] = base[v * SX * SY + s * SX];
-            face_flux_dev32<1, SCHEME, FLUX>(st, ref, gamma, Ft, flags, cut);
+            face_flux_dev32<1, SCHEME, FLUX>(st, ref, gamma, Ft, flags, cut, sv.counters != nullptr);
             const float a = float(g.area[1]);
 #pragma unroll
             for (int v = 0; v < 5; ++v) fy[v * NFY + k] = Ft[v] * a;
@@ -209,10 +209,9 @@ __device__ __forceinline__ void tile2d_f32_body(const GridView& g, const StageVi
         for (int v = 0; v < 5; ++v) {
             const float* fxv = fx + v * NFX + r * (TX + 1) + c;
             const float* fyv = fy + v * NFY + r * TX + c;
-            // the flux-deviation differences in FP32 (neighbouring faces'
-            // deviations are close, so each difference is nearly exact), one
-            // conversion to FP64 for the update
-            div[v] = double((fxv[1] - fxv[0]) + (fyv[TX] - fyv[0]));
+            // FP32 face values, differences in FP64: the difference of two
+            // floats is exact in double, so the divergence telescopes
+            div[v] = (double(fxv[1]) - double(fxv[0])) + (double(fyv[TX]) - double(fyv[0]));
             qn[v] = __ldg(sv.qs + v * vs + node);
         }
         finish_node(g, sv, dt, node, qn, div, flags, sr_max);
@@ -220,7 +219,7 @@ __device__ __forceinline__ void tile2d_f32_body(const GridView& g, const StageVi
 }
 
 // ------------------------------------------------------------------ 1-D
-// T = double: FP64 stencil; T = float: FP32 deviations from the tile's first node.
+// T = double: FP64 stencil; T = float: FP32 deviations from the stage's reference node.
 template <int SCHEME, int FLUX, typename T>
 __device__ __forceinline__ void tile1d_body(const GridView& g, const StageView& sv, int x0, T* smem, unsigned& flags,
                                             unsigned& cut, unsigned& cores, double& sr_max) {
@@ -231,10 +230,7 @@ __device__ __forceinline__ void tile1d_body(const GridView& g, const StageView& 
     T* fx = sq + 5 * SX;   // [5][NF]
     const long long vs = g.vs;
     double qref[5] = {0, 0, 0, 0, 0};
-    if (F32) {
-#pragma unroll
-        for (int v = 0; v < 5; ++v) qref[v] = __ldg(sv.qs + v * vs + x0);
-    }
+    if (F32) load_ref(g, sv.qs, qref);
     const Ref32 ref = F32 ? make_ref32(qref, g.gamma) : Ref32{};
     for (int t = threadIdx.x; t < SX; t += blockDim.x) {
         const int gx = map_tile_index(x0 - H + t, g.n[0], g.bc_lo[0], g.bc_hi[0]);
@@ -249,7 +245,7 @@ __device__ __forceinline__ void tile1d_body(const GridView& g, const StageView& 
         for (int s = 0; s < NST; ++s)
 #pragma unroll
             for (int v = 0; v < 5; ++v) st[s][v] = sq[v * SX + f + s];
-        if constexpr (F32) face_flux_dev32<0, SCHEME, FLUX>(st, ref, T(g.gamma), Ft, flags, cut);
+        if constexpr (F32) face_flux_dev32<0, SCHEME, FLUX>(st, ref, T(g.gamma), Ft, flags, cut, sv.counters != nullptr);
         else face_flux<0, SCHEME, FLUX, double>(st, g.gamma, Ft, flags, cut, FLUX == LAXW ? sv.clock->dt / g.h[0] : 0.0);
 #pragma unroll
         for (int v = 0; v < 5; ++v) fx[v * NF + f] = Ft[v] * T(g.area[0]);
@@ -263,7 +259,7 @@ __device__ __forceinline__ void tile1d_body(const GridView& g, const StageView& 
         double div[5], qn[5];
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
-            div[v] = double(fx[v * NF + c + 1] - fx[v * NF + c]);  // FP32: difference in FP32, one conversion
+            div[v] = double(fx[v * NF + c + 1]) - double(fx[v * NF + c]);  // FP32 faces: exact FP64 difference
             qn[v] = F32 ? __ldg(sv.qs + v * vs + gx) : double(sq[v * SX + c + H]);
         }
         finish_node(g, sv, dt, gx, qn, div, flags, sr_max);

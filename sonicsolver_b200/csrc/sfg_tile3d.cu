@@ -15,10 +15,12 @@
 // A face on a block edge (x, y, or the bottom z face of a chunk) is
 // evaluated by both neighbouring blocks from the same inputs.
 //
-// T = double: FP64 stencils.  T = float: FP32 deviations from the block's
-// first node (one FP64 -> FP32 rounding per staged node) and deviation
-// fluxes (face_flux_dev32): the reference flux cancels from every flux
-// difference of the block.  Divergence and stage update are FP64.
+// T = double: FP64 stencils.  T = float: FP32 deviations from the stage's
+// reference node (ref_node; one FP64 -> FP32 rounding per staged node) and
+// deviation fluxes (face_flux_dev32): the reference flux cancels from every
+// flux difference, and a block-edge face has the same bits in both blocks.
+// Divergence (exact FP64 differences of the FP32 faces) and stage update
+// are FP64.
 #include "sfg_tile.cuh"
 
 namespace sfg {
@@ -62,13 +64,9 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == sizeof(float) ? T3_
     const int t = threadIdx.x;
     const int ci = t % T3X, cj = t / T3X;  // this thread's column (t < COL)
 
-    // reference state of the block (FP32 deviations), none in FP64
+    // reference state of the stage (FP32 deviations), none in FP64
     double qref[5] = {0, 0, 0, 0, 0};
-    if (F32) {
-        const long long at = (long long)z0 * nxy + (long long)y0 * nx + x0;
-#pragma unroll
-        for (int v = 0; v < 5; ++v) qref[v] = __ldg(sv.qs + v * vs + at);
-    }
+    if (F32) load_ref(g, sv.qs, qref);
     const Ref32 ref = F32 ? make_ref32(qref, g.gamma) : Ref32{};
     auto load = [&](long long at, int v) -> T { return T(__ldg(sv.qs + v * vs + at) - qref[v]); };
 
@@ -94,7 +92,7 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == sizeof(float) ? T3_
 #pragma unroll
                 for (int v = 0; v < 5; ++v) d[s][v] = ring[(v * R + slot) * COL + t];
             }
-            face_flux_dev32<2, SCHEME, FLUX>(d, ref, float(g.gamma), Fz, flags, cut);
+            face_flux_dev32<2, SCHEME, FLUX>(d, ref, float(g.gamma), Fz, flags, cut, sv.counters != nullptr);
         } else {
             double st[NST][5];
 #pragma unroll
@@ -153,7 +151,7 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == sizeof(float) ? T3_
                 for (int s = 0; s < NST; ++s)
 #pragma unroll
                     for (int v = 0; v < 5; ++v) st[s][v] = base[v * SX * SY + s];
-                if constexpr (F32) face_flux_dev32<0, SCHEME, FLUX>(st, ref, float(g.gamma), Ft, flags, cut);
+                if constexpr (F32) face_flux_dev32<0, SCHEME, FLUX>(st, ref, float(g.gamma), Ft, flags, cut, sv.counters != nullptr);
                 else {
                     double sd[NST][5];
 #pragma unroll
@@ -172,7 +170,7 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == sizeof(float) ? T3_
                 for (int s = 0; s < NST; ++s)
 #pragma unroll
                     for (int v = 0; v < 5; ++v) st[s][v] = base[v * SX * SY + s * SX];
-                if constexpr (F32) face_flux_dev32<1, SCHEME, FLUX>(st, ref, float(g.gamma), Ft, flags, cut);
+                if constexpr (F32) face_flux_dev32<1, SCHEME, FLUX>(st, ref, float(g.gamma), Ft, flags, cut, sv.counters != nullptr);
                 else {
                     double sd[NST][5];
 #pragma unroll
@@ -200,8 +198,9 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == sizeof(float) ? T3_
             for (int v = 0; v < 5; ++v) {
                 const T* fxv = fx + v * NFX + cj * (T3X + 1) + ci;
                 const T* fyv = fy + v * NFY + cj * T3X + ci;
-                if constexpr (F32)  // deviation differences in FP32, one conversion
-                    div[v] = double((fxv[1] - fxv[0]) + (fyv[T3X] - fyv[0]) + (Fup[v] - Fdn[v]) * T(g.area[2]));
+                if constexpr (F32)  // FP32 face values, exact FP64 differences
+                    div[v] = (double(fxv[1]) - double(fxv[0])) + (double(fyv[T3X]) - double(fyv[0])) +
+                             (double(Fup[v]) - double(Fdn[v])) * g.area[2];
                 else
                     div[v] = (fxv[1] - fxv[0]) + (fyv[T3X] - fyv[0]) + (Fup[v] * g.area[2] - Fdn[v] * g.area[2]);
                 qn[v] = __ldg(sv.qs + v * vs + node);

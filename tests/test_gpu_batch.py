@@ -26,8 +26,7 @@ def mix(seed=3, t_end=0.03):
 
 
 def solo(case, precision=capi.PREC_FP64, recipe="weno5Rusanov", variant=1):
-    """The same grid alone.  FP32-flux results depend on the tile shape (the
-    per-tile reference state), so the solo run uses the batch's tile shape."""
+    """The same grid alone, on the tile kernel of the batch's tile shape."""
     s = capi.Solver(case.dim, case.n, case.h, case.bc_lo, case.bc_hi, recipe=recipe, time_recipe="SSPRK3",
                     precision=precision, cfl=case.cfl)
     if case.dim == 2:
@@ -52,6 +51,98 @@ def test_batch_results_equal_solo(precision, variant):
         want, steps = solo(c, precision, variant=variant)
         assert st["steps"] == steps, c.name
         assert rel_linf(b.download(slot), want).max() <= TOL, c.name
+
+
+def mixed_recipes(seed=13):
+    """Grids that each carry their own numerics, as reference case
+    directories do: tubes on WENO5 / WENO3 with Rusanov or Roe and TENO5 with
+    Roe (CFL 0.5), a TENO5 + Rusanov vortex at CFL 0.4 (the vortex workload's
+    numerics), a WENO7 vortex at CFL 0.45 with a maxDeltaT.  Each tube's
+    recipe is one the oracle's time loop runs to t_end on that tube (WENO3
+    drives some of these tubes to p < 0, as the reference does)."""
+    tubes = cases.shock_tube_batch(count=8, seed=seed, t_end=0.03, max_1d=1500, max_2d=90)
+    recipes = ("weno5Rusanov", "weno5Roe", "weno3Rusanov", "teno5Roe", "weno5Roe", "teno5Roe", "teno5Roe",
+               "weno5Rusanov")
+    for c, r in zip(tubes, recipes):
+        c.recipe = r
+    vortices = [cases.isentropic_vortex(48, recipe="teno5Rusanov", cfl=0.4, t_end=0.2),
+                cases.isentropic_vortex(40, recipe="weno7Rusanov", cfl=0.45, t_end=0.15)]
+    vortices[1].meta["max_dt"] = 2.5e-3
+    return tubes + vortices
+
+
+def solo_own(case, precision, variant):
+    """The grid alone with its own numerics."""
+    s = capi.Solver(case.dim, case.n, case.h, case.bc_lo, case.bc_hi, recipe=case.recipe, time_recipe="SSPRK3",
+                    precision=precision, cfl=case.cfl, max_dt=case.meta.get("max_dt", 0.0))
+    if case.dim == 2:
+        s.variant = variant
+    s.upload(np.ascontiguousarray(case.q))
+    st, _ = s.advance(case.t_end)
+    return s.download().reshape(case.q.shape), st.steps
+
+
+@pytest.mark.parametrize("precision", [capi.PREC_FP64, capi.PREC_FP32_FLUX])
+@pytest.mark.parametrize("variant", [1, 2])
+def test_batch_with_per_grid_recipes_equals_solo(precision, variant):
+    """One batch, five recipes and three CFL numbers: each grid's result and
+    step count equal the same grid run alone with its own numerics."""
+    cs = mixed_recipes()
+    b = capi.Batch(1 << 30, 64, recipe="weno5Rusanov", precision=precision, cfl=0.5)
+    b.variant = variant
+    slots = [b.add(c, recipe=c.recipe, cfl=c.cfl, max_dt=c.meta.get("max_dt")) for c in cs]
+    b.step(100000, graph_steps=8)
+    for c, slot in zip(cs, slots):
+        st = b.status(slot)
+        assert not st["running"] and st["flags"] == 0, c.name
+        assert abs(st["time"] - c.t_end) < 1e-12
+        want, steps = solo_own(c, precision, variant)
+        assert st["steps"] == steps, (c.name, c.recipe)
+        assert rel_linf(b.download(slot), want).max() <= TOL, (c.name, c.recipe)
+
+
+def test_server_with_per_request_recipes_equals_solo():
+    """Staggered arrivals of requests with their own recipes and CFL numbers,
+    fewer slots than requests: each result equals the grid alone."""
+    cs = mixed_recipes()
+    srv = capi.Server(1 << 30, 5, recipe="weno5Rusanov", graph_steps=4)
+    ids = []
+    for c in cs:
+        ids.append(srv.submit(c, recipe=c.recipe, cfl=c.cfl, max_dt=c.meta.get("max_dt")))
+        time.sleep(0.002)
+    srv.drain(300)
+    for rid, c in zip(ids, cs):
+        info = srv.poll(rid)
+        assert info.state == capi.REQ_DONE, (c.name, c.recipe)
+        want, steps = solo_own(c, capi.PREC_FP64, 1)
+        assert info.steps == steps
+        assert rel_linf(srv.fetch(rid), want).max() <= TOL
+    srv.close()
+
+
+def test_per_grid_numerics_are_checked():
+    """A grid's own numerics must keep the batch's time recipe and precision
+    and name a recipe with a batched kernel; the server checks at submit."""
+    import ctypes
+    c = cases.sod_1d(100, t_end=0.01)
+    b = capi.Batch(64 << 20, 4)
+    g = capi.grid_desc(c.dim, c.n, c.h, c.bc_lo, c.bc_hi)
+    q = np.ascontiguousarray(c.q)
+    slot = ctypes.c_int()
+    for kw in ({"time_recipe": "classicalRK4"}, {"precision": capi.PREC_FP32_FLUX}, {"recipe": "weno5Steger"},
+               {"cfl": float("nan")}):
+        nm = capi.numerics_desc(**{**b.defaults, **kw})
+        code = capi.lib().sfg_batch_add_ex(b._h, ctypes.byref(g), ctypes.byref(nm),
+                                           q.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 0.01, 0,
+                                           ctypes.byref(slot))
+        assert code == capi.ERR_ARG, kw
+    assert b.info()["live"] == 0
+    b.close()
+    srv = capi.Server(64 << 20, 2)
+    with pytest.raises(capi.SolverError) as e:
+        srv.submit(c, recipe="teno5LaxWendroff")
+    assert e.value.code == capi.ERR_ARG
+    srv.close()
 
 
 def test_continuous_batching_add_and_remove_between_steps():

@@ -3,7 +3,11 @@ state, stage accumulation, totals and dt in FP64) against the FP64 oracle.
 
 Tolerances (FP32 has a 6e-8 unit round-off):
   * one step of a smooth or shocked state: relative L-infinity per variable
-    <= 2e-6 of the oracle's step (WENO5; TENO5 on smooth data);
+    <= 2e-6 of the oracle's step (WENO3/5/7).  TENO5's cut-off is a
+    threshold test, and where the FP32 indicators fall on the other side of
+    it than the FP64 ones (a flip), that face's reconstruction changes by up
+    to a local difference of the state: TENO5 steps are held to 1e-4 relative
+    L-infinity and 1e-7 relative mean, the curvilinear FP32 tests' TENO bar;
   * a vortex run: L1(rho) error against the exact solution within 1.5x of the
     FP64 path's at the same grid and time.
 """
@@ -18,6 +22,7 @@ from sonicsolver_b200 import capi, cases
 pytestmark = pytest.mark.gpu
 
 STEP_TOL = 2e-6
+TENO_STEP_TOL, TENO_MEAN_TOL = 1e-4, 1e-7
 
 
 @pytest.mark.parametrize("recipe,shock", [("weno5Rusanov", False), ("weno5Rusanov", True), ("weno5Roe", True),
@@ -38,8 +43,14 @@ def test_fp32_flux_step_close_to_fp64_oracle(recipe, shock, dim, n, h, bc):
     st = po.Stepper(spec, SCHEME_OF[scheme], FLUX_OF[flux], po.SSPRK3)
     st.step(Q, dt)
     s.step(dt)
-    err = rel_linf(s.download().reshape(q.shape), from_oracle(spec, Q))
-    assert err.max() <= STEP_TOL, err
+    got, want = s.download().reshape(q.shape), from_oracle(spec, Q)
+    err = rel_linf(got, want)
+    if scheme == "teno5":
+        scale = np.abs(want).reshape(-1, 5).max(axis=0)
+        mean = np.abs(got - want).reshape(-1, 5).mean(axis=0) / np.where(scale > 0, scale, 1.0)
+        assert err.max() <= TENO_STEP_TOL and mean.max() <= TENO_MEAN_TOL, (err, mean)
+    else:
+        assert err.max() <= STEP_TOL, err
 
 
 def test_fp32_vortex_l1_within_1p5x_of_fp64():
@@ -99,8 +110,14 @@ def test_fp32_sweep_variant_step_close_to_fp64_oracle(recipe):
     dt = po.dt(spec, Q, 0.5)
     po.Stepper(spec, SCHEME_OF[scheme], FLUX_OF[flux], po.SSPRK3).step(Q, dt)
     s.step(dt)
-    err = rel_linf(s.download().reshape(q.shape), from_oracle(spec, Q))
-    assert err.max() <= STEP_TOL, err
+    got, want = s.download().reshape(q.shape), from_oracle(spec, Q)
+    err = rel_linf(got, want)
+    if scheme == "teno5":
+        scale = np.abs(want).reshape(-1, 5).max(axis=0)
+        mean = np.abs(got - want).reshape(-1, 5).mean(axis=0) / np.where(scale > 0, scale, 1.0)
+        assert err.max() <= TENO_STEP_TOL and mean.max() <= TENO_MEAN_TOL, (err, mean)
+    else:
+        assert err.max() <= STEP_TOL, err
 
 
 def test_fp32_taylor_green_tracks_fp64():

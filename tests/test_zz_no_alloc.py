@@ -80,10 +80,10 @@ def test_noalloc_matches_existing_entry_point_on_two_calls_in_a_row():
     (3, (20, 18, 16), (0.05, 0.06, 0.07), capi.BC_TRANSMISSIVE, "teno5Roe"),
 ])
 def test_noalloc_fp32_flux_within_fp32_tolerance(dim, n, h, bc, recipe):
-    """FP32-flux mode: the sweep form of the entry point and the tile form of
-    sfg_residual take different FP32 reference states, so they agree to FP32
-    round-off (and both stay that close to the FP64 oracle); two calls in a
-    row give the same bits."""
+    """FP32-flux mode: the sweep form of the entry point scales face fluxes by
+    the area in FP64, the tile form of sfg_residual in FP32, so they agree to
+    FP32 round-off (and both stay that close to the FP64 oracle); two calls
+    in a row give the same bits."""
     q = smooth_state(dim, n, seed=8, shock=False)
     got = _noalloc_residual(dim, n, h, bc, q, recipe, precision=capi.PREC_FP32_FLUX)
     again = _noalloc_residual(dim, n, h, bc, q, recipe, precision=capi.PREC_FP32_FLUX)
