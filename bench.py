@@ -698,10 +698,16 @@ def run_batched_to_end(args, precision, variant):
     st = [b.status(sl) for sl in slots]
     steps = np.array([x["steps"] for x in st])
     cell_steps = int(sum(c.cells * n for c, n in zip(tubes, steps)))
-    ok = all(abs(x["time"] - 0.15) < 1e-12 and x["flags"] == 0 for x in st)
+    reached = [k for k, x in enumerate(st) if abs(x["time"] - 0.15) < 1e-12 and x["flags"] == 0]
+    failed = [{"tube": k, "cells": tubes[k].cells, "flags": int(x["flags"]), "steps_done": int(x["steps"]) - 1,
+               "time": x["time"]} for k, x in enumerate(st) if x["flags"]]
     b.close()
     keep = np.unique(np.linspace(0, len(timeline) - 1, min(24, len(timeline))).astype(int))
-    return {"tubes": len(tubes), "t_end": 0.15, "all_reached_t_end": bool(ok),
+    return {"tubes": len(tubes), "t_end": 0.15, "reached_t_end": len(reached),
+            "failed": failed,
+            "failed_note": "tubes whose state went invalid (near-vacuum states of the seeded draw): each "
+                           "stops with its status bits and the others run on (the reference exits the process "
+                           "at that point)",
             "time_to_solution_s": round(ms / 1e3, 3), "cell_steps": cell_steps,
             "value": round(cell_steps / (ms * 1e-3) / 1e6, 2), "unit": "Mcell-steps/s",
             "steps_per_tube": {"min": int(steps.min()), "median": int(np.median(steps)), "max": int(steps.max())},
@@ -816,7 +822,7 @@ def run_all_kernels(args):
                 s.close()
                 ran.append(f"{label} variant {v} {'fp64' if prec == F64 else 'fp32flux'}: one CFL step")
 
-    # 2-D vortex 2048^2 (168 MB per state copy): axis sweeps, 30 x 16 and 22 x 22 tiles
+    # 2-D vortex 2048^2 (168 MB per state copy): axis sweeps, 32 x 15 and 22 x 22 tiles
     vortex = cases.isentropic_vortex(2048)
     steps(vortex, "2-D vortex 2048^2", (0, 1, 2))
     s = vortex.solver()
@@ -897,7 +903,7 @@ def main():
         return
     base = None
     if rank == 0 and not args.quick and not args.no_cpu_baseline:
-        base = cpu_baseline(steps=3)  # spawned before any GPU call
+        base = cpu_baseline(steps=3, samples=3)  # spawned before any GPU call
     from sonicsolver_b200 import replicas
     if world > 1:
         import torch

@@ -303,7 +303,7 @@ int sfg_batch_remove(sfg_batch b, int slot);
 int sfg_batch_step(sfg_batch b, int steps, int graph_steps, int* active);
 int sfg_batch_status(sfg_batch b, int slot, double* time, int64_t* steps, int* running, uint32_t* flags);
 int sfg_batch_download(sfg_batch b, int slot, double* host_nodes_aos);
-/* Tile shape of the 2-D work items: 1 = 30 x 16, 2 = 22 x 22. */
+/* Tile shape of the 2-D work items: 1 = 32 x 15, 2 = 22 x 22. */
 int sfg_batch_set_variant(sfg_batch b, int variant);
 int sfg_batch_info(sfg_batch b, size_t* used_bytes, size_t* budget_bytes, int* live, int* items);
 /* Status of slots 0..count-1 in one read (running: 1 running, 0 finished or
@@ -348,7 +348,7 @@ int sfg_server_drain(sfg_server s, double timeout_s);
 double sfg_server_now(sfg_server s);
 
 /* Kernel variant of the stage operator: 0 = one sweep launch per axis
- * (any dimension), 1 = fused tile kernel (2-D: 30 x 16 tiles, 1-D: 511-node
+ * (any dimension), 1 = fused tile kernel (2-D: 32 x 15 tiles, 1-D: 511-node
  * tiles, 3-D: 16 x 15 columns marching up 32-plane chunks), 2 = fused 2-D
  * tile kernel with 22 x 22 tiles; for 1-D grids variant 2 runs sfg_advance
  * in one thread-block cluster that steps the whole run on device (FP64, up to

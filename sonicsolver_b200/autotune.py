@@ -3,13 +3,13 @@
 Picks the stage-operator kernel variant by timing the candidates on the
 device, per (GPU model, dimension, size class, recipe, precision):
 
-  * single grids: variant 0 (one sweep launch per axis), 1 (30 x 16 tiles,
+  * single grids: variant 0 (one sweep launch per axis), 1 (32 x 15 tiles,
     511-node 1-D tiles, or 3-D 16 x 15 columns marching in z), 2 (22 x 22
     tiles, 2-D only), each timed with
     sfg_time_sweeps (CUDA events on the solver's stream, stage 0 repeated);
     a 1-D tile win selects 1-D variant 2, which runs the same tiles for
     single stages and adds the whole-run cluster kernel to sfg_advance;
-  * batches: 2-D work-item tile 30 x 16 or 22 x 22, timed over a few batch
+  * batches: 2-D work-item tile 32 x 15 or 22 x 22, timed over a few batch
     steps of a sample of the batch's grids.
 
 Results are cached in a JSON table (default ``~/.cache/sonicsolver_b200/

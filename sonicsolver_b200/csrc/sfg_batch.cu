@@ -335,8 +335,8 @@ struct sfg_batch_s {
     std::vector<RecipeGroup> groups;
     std::vector<int> inst_group;          // per slot
     cudaEvent_t fork = nullptr;
-    int variant = 1;  // 1: 30 x 16 tiles, 2: 22 x 22
-    int tx = 30, ty = 16;
+    int variant = 1;  // 1: 32 x 15 tiles, 2: 22 x 22
+    int tx = 32, ty = 15;
     int max_inst = 0;
     // HBM slab for instance state, first-fit allocator over it
     char* slab = nullptr;
@@ -368,8 +368,8 @@ int bind_group(sfg_batch_s* b, RecipeGroup& grp) {
     const bool f32 = b->num.precision == SFG_PREC_FP32_FLUX;
     const int scheme = grp.recipe->scheme, flux = grp.recipe->flux;
     if (b->variant == 1) {
-        grp.stage_k = f32 ? pick_stage<30, 16, true>(scheme, flux) : pick_stage<30, 16, false>(scheme, flux);
-        grp.smem = stage_smem<30, 16>(scheme, f32);
+        grp.stage_k = f32 ? pick_stage<32, 15, true>(scheme, flux) : pick_stage<32, 15, false>(scheme, flux);
+        grp.smem = stage_smem<32, 15>(scheme, f32);
     } else {
         grp.stage_k = f32 ? pick_stage<22, 22, true>(scheme, flux) : pick_stage<22, 22, false>(scheme, flux);
         grp.smem = stage_smem<22, 22>(scheme, f32);
@@ -386,10 +386,10 @@ int bind_group(sfg_batch_s* b, RecipeGroup& grp) {
 
 int bind_kernels(sfg_batch_s* b) {
     if (b->variant == 1) {
-        b->dt_k = batch_dt_kernel<30, 16>;
-        b->copy_k = batch_copy_kernel<30, 16>;
-        b->tx = 30;
-        b->ty = 16;
+        b->dt_k = batch_dt_kernel<32, 15>;
+        b->copy_k = batch_copy_kernel<32, 15>;
+        b->tx = 32;
+        b->ty = 15;
     } else {
         b->dt_k = batch_dt_kernel<22, 22>;
         b->copy_k = batch_copy_kernel<22, 22>;

@@ -9,7 +9,7 @@
 //   2. evaluates every face of the tile once from shared memory into
 //      shared-memory flux arrays.  The face list is warp aligned per axis, so
 //      no warp mixes the x and y template paths, and sized to whole rounds of
-//      256 threads (30 x 16 and 22 x 22 tiles: 4 rounds; 1-D 511 nodes: 2);
+//      256 threads (32 x 15 and 22 x 22 tiles: 4 rounds; 1-D 511 nodes: 2);
 //   3. forms div = dFx (+ dFy) per node and finishes it: stage combination
 //      with state validation, or R = Jac * div.
 // Faces on a tile edge are evaluated by both neighbouring tiles from the same
@@ -71,6 +71,33 @@ __device__ __forceinline__ int map_tile_index(int i, int n, int bcl, int bch) {
     return i < lo ? lo : (i > hi ? hi : i);
 }
 
+// Stages the tile and its cross-shaped halo row by row: a warp takes whole
+// rows, a lane the columns lane, lane + 32, ...  A lane maps its columns'
+// global indices once and a row's index once per row, and the loads of a row
+// are coalesced.  put(t, at) stores node `at` of the grid into shared slot t
+// (t = r * SX + c).
+template <int TX, int TY, int H, typename Put>
+__device__ __forceinline__ void stage_rows(const GridView& g, int x0, int y0, Put put) {
+    constexpr int SX = TX + 2 * H, SY = TY + 2 * H;
+    constexpr int CH = (SX + 31) / 32;  // column chunks of a row
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    int gx[CH];
+#pragma unroll
+    for (int k = 0; k < CH; ++k)
+        gx[k] = map_tile_index(x0 - H + min(lane + 32 * k, SX - 1), g.n[0], g.bc_lo[0], g.bc_hi[0]);
+    const long long nx = g.n[0];
+    for (int r = warp; r < SY; r += nwarps) {
+        const bool band = r >= H && r < TY + H;  // corners are never read
+        const long long row = (long long)map_tile_index(y0 - H + r, g.n[1], g.bc_lo[1], g.bc_hi[1]) * nx;
+#pragma unroll
+        for (int k = 0; k < CH; ++k) {
+            const int c = lane + 32 * k;
+            if (c >= SX || (!band && (c < H || c >= TX + H))) continue;
+            put(r * SX + c, row + gx[k]);
+        }
+    }
+}
+
 // ------------------------------------------------------------------ 2-D FP64
 template <int SCHEME, int FLUX, int TX, int TY>
 __device__ __forceinline__ void tile2d_body(const GridView& g, const StageView& sv, int x0, int y0, double* smem,
@@ -82,15 +109,13 @@ __device__ __forceinline__ void tile2d_body(const GridView& g, const StageView& 
     double* fx = sq + 5 * SX * SY;   // [5][TY][TX+1]
     double* fy = fx + 5 * NFX;       // [5][TY+1][TX]
     const long long nx = g.n[0], vs = g.vs;
-    for (int t = threadIdx.x; t < SX * SY; t += blockDim.x) {
-        const int r = t / SX, c = t - r * SX;
-        if ((r < H || r >= TY + H) && (c < H || c >= TX + H)) continue;  // corners are never read
-        const int gx = map_tile_index(x0 - H + c, g.n[0], g.bc_lo[0], g.bc_hi[0]);
-        const int gy = map_tile_index(y0 - H + r, g.n[1], g.bc_lo[1], g.bc_hi[1]);
-        const long long at = (long long)gy * nx + gx;
+    stage_rows<TX, TY, H>(g, x0, y0, [&](int t, long long at) {
+        double q[5];
 #pragma unroll
-        for (int v = 0; v < 5; ++v) sq[v * SX * SY + t] = __ldg(sv.qs + v * vs + at);
-    }
+        for (int v = 0; v < 5; ++v) q[v] = __ldg(sv.qs + v * vs + at);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) sq[v * SX * SY + t] = q[v];
+    });
     __syncthreads();
     const double gamma = g.gamma;
     for (int f = threadIdx.x; f < NFXP + NFYP; f += blockDim.x) {
@@ -155,15 +180,13 @@ __device__ __forceinline__ void tile2d_f32_body(const GridView& g, const StageVi
     double qref[5];
     load_ref(g, sv.qs, qref);
     const Ref32 ref = make_ref32(qref, g.gamma);
-    for (int t = threadIdx.x; t < SX * SY; t += blockDim.x) {
-        const int r = t / SX, c = t - r * SX;
-        if ((r < H || r >= TY + H) && (c < H || c >= TX + H)) continue;
-        const int gx = map_tile_index(x0 - H + c, g.n[0], g.bc_lo[0], g.bc_hi[0]);
-        const int gy = map_tile_index(y0 - H + r, g.n[1], g.bc_lo[1], g.bc_hi[1]);
-        const long long at = (long long)gy * nx + gx;
+    stage_rows<TX, TY, H>(g, x0, y0, [&](int t, long long at) {
+        double q[5];
 #pragma unroll
-        for (int v = 0; v < 5; ++v) sq[v * SX * SY + t] = float(__ldg(sv.qs + v * vs + at) - qref[v]);
-    }
+        for (int v = 0; v < 5; ++v) q[v] = __ldg(sv.qs + v * vs + at);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) sq[v * SX * SY + t] = float(q[v] - qref[v]);
+    });
     __syncthreads();
     const float gamma = float(g.gamma);
     for (int f = threadIdx.x; f < NFXP + NFYP; f += blockDim.x) {

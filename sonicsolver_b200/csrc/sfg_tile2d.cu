@@ -129,12 +129,12 @@ cudaError_t launch_tile1d(int scheme, int flux, int prec64, const GridView& g, c
     return prec64 ? launch_tile1_t<double>(scheme, flux, g, sv, st) : launch_tile1_t<float>(scheme, flux, g, sv, st);
 }
 
-// variant 1: 30 x 16 tile, variant 2: 22 x 22 tile (256 threads each).
+// variant 1: 32 x 15 tile, variant 2: 22 x 22 tile (256 threads each).
 cudaError_t launch_tile2d(int variant, int scheme, int flux, int prec64, const GridView& g, const StageView& sv,
                           cudaStream_t st) {
     if (variant == 1)
-        return prec64 ? launch_tile_t<double, 30, 16>(scheme, flux, g, sv, st)
-                      : launch_tile_t<float, 30, 16>(scheme, flux, g, sv, st);
+        return prec64 ? launch_tile_t<double, 32, 15>(scheme, flux, g, sv, st)
+                      : launch_tile_t<float, 32, 15>(scheme, flux, g, sv, st);
     if (variant == 2)
         return prec64 ? launch_tile_t<double, 22, 22>(scheme, flux, g, sv, st)
                       : launch_tile_t<float, 22, 22>(scheme, flux, g, sv, st);

@@ -56,7 +56,7 @@ def test_residual_parity(recipe, dim, n, h, bc, shock):
 @pytest.mark.parametrize("n", [(37, 29, 1), (64, 48, 1), (9, 40, 1)])
 @pytest.mark.parametrize("bc", [capi.BC_TRANSMISSIVE, capi.BC_PERIODIC])
 def test_2d_kernel_variants_match_oracle(variant, recipe, n, bc):
-    """Axis sweeps (0) and fused tile kernels (1: 30x16, 2: 22x22) on grids
+    """Axis sweeps (0) and fused tile kernels (1: 32x15, 2: 22x22) on grids
     smaller than, equal to and not a multiple of a tile, including periodic
     axes shorter than the tile halo reach."""
     h = (0.03, 0.02, 1.0)
