@@ -382,3 +382,126 @@ class RefCase:
                                          ctypes.byref(tf))
         _check(code, "ref advance")
         return dts[:steps.value].copy(), tf.value
+
+
+# ------------------------------------------------------------ block geometry
+
+_mesh = None
+
+
+def ref_mesh_lib():
+    """The reference's structured-block generator (oracle/_ref/libsfmesh.so),
+    or None when it was not built."""
+    global _mesh
+    if _mesh is None:
+        lib = _load(os.path.join(HERE, "_ref", "libsfmesh.so"))
+        if lib is None:
+            return None
+        IP = ctypes.POINTER(ctypes.c_int)
+        lib.sfr_mesh_points.argtypes = [ctypes.c_int, _DP, ctypes.c_double, IP, IP, _DP, ctypes.c_int, IP, _DP, _DP]
+        lib.sfr_mesh_points.restype = ctypes.c_int
+        _mesh = lib
+    return _mesh
+
+
+def ref_mesh_points(vertices, hex, cells, grading=(1.0, 1.0, 1.0), edges=(), scale=1.0):
+    """Node coordinates of one block from the reference's own generator
+    (MeshGen::generateStructuredMesh, SF_meshGen.cpp:76-110): trilinear with
+    grading, or transfinite interpolation when `edges` ((v0, v1, point) arcs)
+    are given.  Returns (nz, ny, nx, 3)."""
+    lib = ref_mesh_lib()
+    if lib is None:
+        raise RuntimeError("oracle/_ref/libsfmesh.so missing: run `make -C oracle`")
+    V = np.ascontiguousarray(vertices, dtype=np.float64).reshape(-1, 3)
+    H = np.ascontiguousarray(hex, dtype=np.int32)
+    C = np.ascontiguousarray(cells, dtype=np.int32)
+    G = np.ascontiguousarray(grading, dtype=np.float64)
+    E = np.ascontiguousarray([[a, b] for a, b, _ in edges] or [[0, 0]], dtype=np.int32)
+    P = np.ascontiguousarray([p for _, _, p in edges] or [[0.0, 0.0, 0.0]], dtype=np.float64)
+    out = np.zeros((C[2] + 1, C[1] + 1, C[0] + 1, 3))
+    IP = ctypes.POINTER(ctypes.c_int)
+    code = lib.sfr_mesh_points(len(V), _ptr(V), float(scale), H.ctypes.data_as(IP), C.ctypes.data_as(IP), _ptr(G),
+                               len(edges), E.ctypes.data_as(IP), _ptr(P), _ptr(out))
+    _check(code, "ref mesh points")
+    return out
+
+
+def field_metrics(points: np.ndarray, ng: int, active=(True, True, True)):
+    """The reference Field's metrics of a block (numpy restatement): ghost
+    coordinates extrapolated linearly along x, then y, then z
+    (Mesh::generateGhostCells, src/infrastructure/mesh/SF_mesh.cpp:491-533);
+    symmetric conservative cofactors and J = (r_xi.c_xi + r_eta.c_eta +
+    r_zeta.c_zeta) / 3 on every point one layer in, Jac = 1 / J and the
+    metric rows = cofactors * Jac (Mesh::computeMetrics, :219-345); the
+    outermost layer copied from its inner neighbour along x, then y, then z
+    (applyBoundaryMetrics, :439-474).  Returns (metrics (MZ, MY, MX, 10) with
+    ng ghost layers on every axis, identity residual, identity tolerance)
+    with the audit of Mesh::auditMetricIdentity (:348-437) over the nodes and
+    the active axes.  `points`: (nz, ny, nx, 3) node coordinates."""
+    nz, ny, nx, _ = points.shape
+    X = np.zeros((nz + 2 * ng, ny + 2 * ng, nx + 2 * ng, 3))
+    X[ng:ng + nz, ng:ng + ny, ng:ng + nx] = points
+    for ax in (2, 1, 0):                       # numpy axis of x, y, z
+        M = X.shape[ax]
+
+        def sl(i):
+            s = [slice(None)] * 4
+            s[ax] = i
+            return tuple(s)
+        for i in range(ng - 1, -1, -1):
+            X[sl(i)] = 2.0 * X[sl(i + 1)] - X[sl(i + 2)]
+        for i in range(M - ng, M):
+            X[sl(i)] = 2.0 * X[sl(i - 1)] - X[sl(i - 2)]
+    npax = {0: 2, 1: 1, 2: 0}                  # coordinate axis -> numpy axis
+
+    def shift(A, a, o):
+        return np.roll(A, -o, axis=npax[a])
+
+    def dco(A, a):                             # central difference along axis a (valid away from its ends)
+        return 0.5 * (shift(A, a, 1) - shift(A, a, -1))
+
+    D = {(c, a): dco(X[..., c], a) for c in range(3) for a in range(3)}
+
+    def dprod(p, q, inner, outer):
+        P = X[..., p] * D[(q, inner)]
+        return 0.5 * (shift(P, outer, 1) - shift(P, outer, -1))
+
+    after1, after2 = (1, 2, 0), (2, 0, 1)
+    cof = {}
+    for a_ in range(3):
+        a, b = after1[a_], after2[a_]
+        for c in range(3):
+            p, q = after1[c], after2[c]
+            curl1 = dprod(p, q, b, a) - dprod(p, q, a, b)
+            curl2 = dprod(q, p, a, b) - dprod(q, p, b, a)
+            cof[(a_, c)] = 0.5 * (curl1 + curl2)
+
+    def rowdot(a):
+        return D[(0, a)] * cof[(a, 0)] + D[(1, a)] * cof[(a, 1)] + D[(2, a)] * cof[(a, 2)]
+    J = (rowdot(0) + rowdot(1) + rowdot(2)) / 3.0
+    inner = (slice(1, -1),) * 3
+    Mt = np.zeros(X.shape[:3] + (10,))
+    Jac = 1.0 / J[inner]
+    Mt[inner + (0,)] = Jac
+    for a in range(3):
+        for c in range(3):
+            Mt[inner + (1 + 3 * a + c,)] = cof[(a, c)][inner] * Jac
+    Mt[:, :, 0] = Mt[:, :, 1]
+    Mt[:, :, -1] = Mt[:, :, -2]
+    Mt[:, 0] = Mt[:, 1]
+    Mt[:, -1] = Mt[:, -2]
+    Mt[0] = Mt[1]
+    Mt[-1] = Mt[-2]
+    nodes = (slice(ng, ng + nz), slice(ng, ng + ny), slice(ng, ng + nx))
+    div = np.zeros((nz, ny, nx, 3))
+    cmax = 0.0
+    for a in range(3):
+        if not active[a]:
+            continue
+        F = 0.5 * (Mt[..., 1 + 3 * a:4 + 3 * a] / Mt[..., :1] +
+                   shift(Mt[..., 1 + 3 * a:4 + 3 * a] / Mt[..., :1], a, 1))
+        fp, fm = F[nodes], shift(F, a, -1)[nodes]
+        cmax = max(cmax, float(np.abs(fp).max()), float(np.abs(fm).max()))
+        div = div + (fp - fm)
+    tol = 65536.0 * np.finfo(float).eps * max(cmax, np.finfo(float).tiny)
+    return Mt, float(np.abs(div).max()), tol

@@ -81,14 +81,16 @@ RUNNER = os.path.join(HERE, "sfg_run")
 
 
 def build_host(verbose: bool = False, force: bool = False) -> str:
-    """The C++17 host side (case reader, provider catalogs, plan, .vts writer)
-    linked into the ``sfg_run`` driver against the library (rpath $ORIGIN)."""
+    """The C++17 host side (case reader, mesh generator, provider catalogs,
+    plan, .vts writer) linked into the ``sfg_run`` driver against the library
+    (rpath $ORIGIN).  Multiply-adds are not contracted, so the generated
+    coordinates and metrics round as the reference's do."""
     srcs = sorted(glob.glob(os.path.join(HOST, "*.cpp")))
     deps = srcs + sorted(glob.glob(os.path.join(HOST, "*.hpp"))) + [os.path.join(ROOT, "include", "sonicsolver_b200.h"), LIB]
     if not (force or _stale(RUNNER, deps)):
         return RUNNER
     cxx = shutil.which("g++") or "g++"
-    cmd = [cxx, "-std=c++17", "-O2", "-Wall", "-Wextra", "-o", RUNNER, *srcs, "-L", HERE, "-lsonicsolver_b200",
+    cmd = [cxx, "-std=c++17", "-O2", "-ffp-contract=off", "-Wall", "-Wextra", "-o", RUNNER, *srcs, "-L", HERE, "-lsonicsolver_b200",
            "-Wl,-rpath,$ORIGIN"]
     if verbose:
         print(" ".join(cmd), flush=True)

@@ -163,39 +163,65 @@ CaseSpec load_case(const std::string& dir) {
                 if (const Node* r = eos->get("R")) c.gas_R = r->number();
             }
     }
-    // ---- mesh: one axis-aligned block
+    // ---- mesh: one block (structuredMesh generation, decodeParameters,
+    // src/infrastructure/io/mesh/SF_meshParameters.cpp:9-48)
     const Node gen = load_yaml_file(registry_file(dir, "mesh/mesh.yaml", "generation", "mesh/generation.yaml"));
-    const double scale = gen.get("scale") ? gen.at("scale").number() : 1.0;
+    MeshGeneration& m = c.mesh;
+    m.scale = gen.get("scale") ? gen.at("scale").number() : 1.0;
+    if (!(m.scale > 0) || !std::isfinite(m.scale)) throw ParseError("mesh: scale must be finite and > 0");
     if (const Node* ng = gen.get("nGhost")) c.ghost_layers = int(ng->integer());
+    m.n_ghost = c.ghost_layers;
     const Node& verts = gen.at("vertices");
     const Node& blocks = gen.at("blocks");
     if (!blocks.is_seq() || blocks.items.size() != 1)
         throw Unsupported("mesh: the provider runs a single structured block");
-    const Node& blk = blocks.items[0];
-    const auto cells = numbers(blk.at("cells"), 3, "blocks[0].cells");
-    for (int d = 0; d < 3; ++d) {
-        c.cells[d] = int(cells[d]);
-        c.lo[d] = 1e300;
-        c.hi[d] = -1e300;
-    }
     for (const auto& v : verts.items) {
         const auto x = numbers(v, 3, "vertex");
-        for (int d = 0; d < 3; ++d) {
-            c.lo[d] = std::min(c.lo[d], x[d] * scale);
-            c.hi[d] = std::max(c.hi[d], x[d] * scale);
-        }
+        m.vertices.push_back({x[0], x[1], x[2]});
     }
-    for (const auto& v : verts.items) {  // every vertex on a corner of the box
-        const auto x = numbers(v, 3, "vertex");
-        for (int d = 0; d < 3; ++d)
-            if (std::fabs(x[d] * scale - c.lo[d]) > 1e-12 * (1 + std::fabs(c.lo[d])) &&
-                std::fabs(x[d] * scale - c.hi[d]) > 1e-12 * (1 + std::fabs(c.hi[d])))
-                throw Unsupported("mesh: curvilinear blocks need per-node metrics (not in this provider)");
+    const Node& blk = blocks.items[0];
+    const auto hex = numbers(blk.at("vertices"), 8, "blocks[0].vertices");
+    for (int i = 0; i < 8; ++i) {
+        m.verts[i] = int(hex[i]);
+        if (m.verts[i] < 0 || m.verts[i] >= int(m.vertices.size()) || double(m.verts[i]) != hex[i])
+            throw ParseError("mesh: blocks[0].vertices holds an invalid vertex index");
+    }
+    const auto cells = numbers(blk.at("cells"), 3, "blocks[0].cells");
+    for (int d = 0; d < 3; ++d) {
+        c.cells[d] = m.cells[d] = int(cells[d]);
+        if (m.cells[d] < 1 || double(m.cells[d]) != cells[d]) throw ParseError("mesh: cells must be positive integers");
     }
     if (const Node* gr = blk.get("grading")) {
-        for (double g : numbers(*gr, 3, "grading"))
-            if (g != 1.0) throw Unsupported("mesh: graded blocks need per-node metrics (not in this provider)");
+        const auto g = numbers(*gr, 3, "grading");
+        for (int d = 0; d < 3; ++d) {
+            m.grading[d] = g[d];
+            if (!(g[d] > 0) || !std::isfinite(g[d])) throw ParseError("mesh: grading must be finite and > 0");
+        }
     }
+    if (const Node* edges = gen.get("edges")) {
+        for (const auto& e : edges->items) {
+            if (e.at("type").str() != "arc")
+                throw Unsupported("mesh: edge type '" + e.at("type").str() + "' (the generator builds arcs)");
+            const auto ends = numbers(e.at("vertices"), 2, "edges[].vertices");
+            const auto pt = numbers(e.at("point"), 3, "edges[].point");
+            ArcEdge a;
+            a.v0 = int(ends[0]);
+            a.v1 = int(ends[1]);
+            for (int d = 0; d < 3; ++d) a.point[d] = pt[d];
+            if (a.v0 < 0 || a.v1 < 0 || a.v0 >= int(m.vertices.size()) || a.v1 >= int(m.vertices.size()))
+                throw ParseError("mesh: edges[].vertices holds an invalid vertex index");
+            m.edges.push_back(a);
+        }
+    }
+    for (int d = 0; d < 3; ++d) {  // the block's bounding box
+        c.lo[d] = 1e300;
+        c.hi[d] = -1e300;
+        for (int i = 0; i < 8; ++i) {
+            c.lo[d] = std::min(c.lo[d], m.vertices[m.verts[i]][d] * m.scale);
+            c.hi[d] = std::max(c.hi[d], m.vertices[m.verts[i]][d] * m.scale);
+        }
+    }
+    c.curvilinear = !m.uniform_box();
     // ---- fields
     const std::string inf = registry_file(dir, "fields/fields.yaml", "internalField", "fields/internalField.yaml");
     const Node in = load_yaml_file(inf);
@@ -338,6 +364,8 @@ GridSetup build_grid(const CaseSpec& c) {
         }
         g.grid.n[d] = g.nodes[d];
         if (!(g.grid.h[d] > 0)) throw Unsupported("degenerate block extent");
+        if (c.curvilinear && g.grid.bc_lo[d] == SFG_BC_PERIODIC)
+            throw Unsupported("periodic ends on a graded or curved block (the reference has no periodic boundary)");
     }
     // initial state: base values, then the named sets in file order
     const int nx = g.nodes[0], ny = g.nodes[1], nz = g.nodes[2];

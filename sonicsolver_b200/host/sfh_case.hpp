@@ -6,8 +6,10 @@
 //     writeInterval, writeInitial, output.jobName / outputDir, maxDeltaT),
 //     numerics (time.default, terms.convection), algorithm (type);
 //   models/models.yaml -> thermoDynamics (perfectGas gamma, R);
-//   mesh/mesh.yaml -> generation (JSON: vertices, blocks[0].cells, scale,
-//     nGhost; one axis-aligned box block);
+//   mesh/mesh.yaml -> generation (JSON: vertices, blocks[0].vertices /
+//     cells / grading, scale, nGhost, arc edges; one block: an axis-aligned
+//     box runs on the uniform Cartesian path, a graded or curved block with
+//     the generator's node coordinates and metrics, sfh_mesh.hpp);
 //   fields/fields.yaml -> internalField (rho, U, p: uniform / default plus
 //     the mesh sets leftHalf, rightHalf, all) and boundaries (per variable,
 //     per patch: fixedValue, zeroGradient, symmetry, velocity noSlip / slip,
@@ -24,6 +26,7 @@
 #include <vector>
 
 #include "../../include/sonicsolver_b200.h"
+#include "sfh_mesh.hpp"
 
 namespace sfh {
 
@@ -51,6 +54,8 @@ struct CaseSpec {
     double lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
     int cells[3] = {1, 1, 1};
     int ghost_layers = 3;
+    MeshGeneration mesh;       // the block as generated
+    bool curvilinear = false;  // not a uniform axis-aligned box: metrics from `mesh`
     // physics
     double gamma = 1.4, gas_R = 287.05;
     // numerics
@@ -80,8 +85,9 @@ struct GridSetup {
 // keeps the initial ghost state there and advances the boundary node).
 // A patch whose rho, U and p are all zeroGradient is SFG_BC_TRANSMISSIVE;
 // one with fixedValue or symmetry laws is SFG_BC_LAW with those laws.
-// Throws Unsupported for what this provider does not run (curvilinear or
-// graded blocks; a patch with conditions for only some of rho, U, p).
+// Throws Unsupported for what this provider does not run (periodic ends on
+// a graded or curved block; a patch with conditions for only some of rho, U,
+// p).
 GridSetup build_grid(const CaseSpec& c);
 
 }  // namespace sfh

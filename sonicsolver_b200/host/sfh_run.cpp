@@ -9,13 +9,19 @@
 //   4. run it, writing .vts output at the case's write times.
 //
 //   sfg_run CASE_DIR [--mode graph|plan] [--precision fp64|fp32flux]
-//                    [--graph-steps K] [--dump FILE] [--no-write] [--describe]
+//                    [--graph-steps K] [--dump FILE] [--dump-points FILE]
+//                    [--dump-metrics FILE] [--no-write] [--describe]
 //
 // --mode plan executes the plan operation by operation (one C-ABI call per
 // operation, host synchronous).  --mode graph (default) lowers the time loop
 // between two output times to one sfg_advance call: the device-resident
 // clock runs the same dt, stage and commit sequence inside CUDA graphs.
-// --describe stops after step 3 and touches no GPU.
+// --describe stops after step 3 and touches no GPU.  A graded or curved
+// block gets the generator's node coordinates and the reference Field's
+// metrics (sfh_mesh.hpp); --dump-points writes the node coordinates (x, y, z
+// per node, x fastest) and --dump-metrics the metrics handed to the provider
+// (10 per point of the Field layout: the recipe's ghost layers on every
+// axis), both as raw float64, also under --describe.
 // Exit codes: 0 done, 1 error, 2 usage, 3 case not supported by the provider.
 #include <chrono>
 #include <cmath>
@@ -38,7 +44,7 @@ namespace {
 using namespace sfh;
 
 struct Options {
-    std::string dir, mode = "graph", dump;
+    std::string dir, mode = "graph", dump, dump_points, dump_metrics;
     int precision = SFG_PREC_FP64;
     int graph_steps = 32;
     bool write = true, describe_only = false;
@@ -47,7 +53,7 @@ struct Options {
 int usage() {
     std::fprintf(stderr,
                  "usage: sfg_run CASE_DIR [--mode graph|plan] [--precision fp64|fp32flux] [--graph-steps K]\n"
-                 "               [--dump FILE] [--no-write] [--describe]\n");
+                 "               [--dump FILE] [--dump-points FILE] [--dump-metrics FILE] [--no-write] [--describe]\n");
     return 2;
 }
 
@@ -77,7 +83,65 @@ struct Run {
     int outputs = 0;
     std::string out_dir;
     std::vector<double> host;
+    std::vector<double> points;  // node coordinates of a graded or curved block (else empty)
 };
+
+// Ghost layers of the provider's Field layout for a recipe (WENO3: 2,
+// WENO5 / TENO5: 3, WENO7: 4; sfg_ghost_layers).
+int recipe_ghosts(const std::string& convection) {
+    if (convection.rfind("weno3", 0) == 0) return 2;
+    if (convection.rfind("weno7", 0) == 0) return 4;
+    return 3;
+}
+
+// The geometry of a graded or curved block for the provider: node
+// coordinates (x, y, z per node) and the metrics in the provider's Field
+// layout (ng_s ghosts on every axis, 10 per point), taken from the
+// reference Field (the case's nGhost layers) at the same node offsets.  On
+// an inactive axis the provider's one node plane is the block's first.
+void block_geometry(const CaseSpec& c, const GridSetup& g, int ng_s, std::vector<double>& points,
+                    std::vector<double>& metrics, double* residual, double* tolerance) {
+    bool active[3];
+    for (int d = 0; d < 3; ++d) active[d] = d < g.grid.dim;
+    const int ng_c = c.ghost_layers;
+    if (ng_s > ng_c)
+        throw Unsupported("mesh: the case's nGhost " + std::to_string(ng_c) + " is below the recipe's " +
+                          std::to_string(ng_s) + " ghost layers");
+    const FieldGeometry F = field_geometry(c.mesh, ng_c, active);
+    *residual = F.identity_residual;
+    *tolerance = F.identity_tolerance;
+    if (!std::isfinite(F.identity_tolerance) || !(F.identity_tolerance > 0) ||
+        F.identity_residual > F.identity_tolerance)
+        throw Unsupported("mesh: the discrete metric identity is violated (max residual " +
+                          std::to_string(F.identity_residual) + ", tolerance " +
+                          std::to_string(F.identity_tolerance) + "), as the reference's audit reports");
+    const int* n = g.nodes;
+    points.resize(size_t(n[0]) * n[1] * n[2] * 3);
+    for (int k = 0; k < n[2]; ++k)
+        for (int j = 0; j < n[1]; ++j)
+            for (int i = 0; i < n[0]; ++i) {
+                const long long t = F.at(i + ng_c, j + ng_c, k + ng_c);
+                double* p = &points[(((size_t)k * n[1] + j) * n[0] + i) * 3];
+                p[0] = F.x[t];
+                p[1] = F.y[t];
+                p[2] = F.z[t];
+            }
+    const int e[3] = {n[0] + 2 * ng_s, n[1] + 2 * ng_s, n[2] + 2 * ng_s};
+    metrics.resize(size_t(e[0]) * e[1] * e[2] * 10);
+    for (int k = 0; k < e[2]; ++k)
+        for (int j = 0; j < e[1]; ++j)
+            for (int i = 0; i < e[0]; ++i) {
+                const long long t = F.at(i - ng_s + ng_c, j - ng_s + ng_c, k - ng_s + ng_c);
+                std::memcpy(&metrics[(((size_t)k * e[1] + j) * e[0] + i) * 10], &F.metrics[t * 10],
+                            10 * sizeof(double));
+            }
+}
+
+void write_doubles(const std::string& path, const std::vector<double>& v) {
+    std::ofstream f(path, std::ios::binary);
+    f.write(reinterpret_cast<const char*>(v.data()), std::streamsize(v.size() * sizeof(double)));
+    if (!f) throw std::runtime_error("cannot write " + path);
+}
 
 bool at_or_past(double t, double mark) {
     const double sc = std::fabs(t) < 1.0 ? 1.0 : std::fabs(t);
@@ -92,7 +156,8 @@ int write_output(Run& r, double t) {
     const std::string path = r.out_dir + "/" + r.c->job_name + name;
     VtsGeometry geo{{r.g->nodes[0], r.g->nodes[1], r.g->nodes[2]},
                     {r.g->origin[0], r.g->origin[1], r.g->origin[2]},
-                    {r.g->grid.h[0], r.g->grid.h[1], r.g->grid.h[2]}};
+                    {r.g->grid.h[0], r.g->grid.h[1], r.g->grid.h[2]},
+                    r.points.empty() ? nullptr : &r.points};
     if (!write_vts(path, geo, r.host, r.c->gamma, t)) {
         std::fprintf(stderr, "sfg_run: cannot write %s\n", path.c_str());
         return SFG_ERR_ARG;
@@ -283,6 +348,8 @@ int main(int argc, char** argv) {
             else return usage();
         } else if (a == "--graph-steps") o.graph_steps = std::atoi(next().c_str());
         else if (a == "--dump") o.dump = next();
+        else if (a == "--dump-points") o.dump_points = next();
+        else if (a == "--dump-metrics") o.dump_metrics = next();
         else if (a == "--no-write") o.write = false;
         else if (a == "--describe") o.describe_only = true;
         else if (!a.empty() && a[0] == '-') return usage();
@@ -326,6 +393,16 @@ int main(int argc, char** argv) {
                             law_name(L.rho), L.rho_value, law_name(L.velocity), L.velocity_value[0],
                             L.velocity_value[1], L.velocity_value[2], law_name(L.pressure), L.pressure_value);
             }
+        // a graded or curved block: the generator's node coordinates and metrics
+        std::vector<double> points, metrics;
+        if (c.curvilinear) {
+            double res = 0, tol = 0;
+            block_geometry(c, g, recipe_ghosts(c.convection), points, metrics, &res, &tol);
+            std::printf("mesh curvilinear (%s): metric identity residual %.3g, tolerance %.3g\n",
+                        c.mesh.edges.empty() ? "trilinear, graded" : "transfinite, arc edges", res, tol);
+            if (!o.dump_points.empty()) write_doubles(o.dump_points, points);
+            if (!o.dump_metrics.empty()) write_doubles(o.dump_metrics, metrics);
+        }
         if (o.describe_only) {
             OperationTable ops;
             Run dummy;
@@ -341,6 +418,7 @@ int main(int argc, char** argv) {
         r.g = &g;
         r.write = o.write;
         r.host.resize(g.q.size());
+        r.points = points;
         r.out_dir = c.dir + "/" + c.output_dir;
         if (o.write) mkdir(r.out_dir.c_str(), 0755);
         if (sfg_create(&g.grid, &nd, nullptr, &r.s) != SFG_OK) {
@@ -355,6 +433,11 @@ int main(int argc, char** argv) {
                     sfg_destroy(r.s);
                     return 1;
                 }
+        if (c.curvilinear && sfg_set_metrics(r.s, metrics.data(), SFG_LAYOUT_FIELD) != SFG_OK) {
+            std::fprintf(stderr, "sfg_run: %s\n", sfg_last_error());
+            sfg_destroy(r.s);
+            return 1;
+        }
         int rc = sfg_upload(r.s, g.q.data(), SFG_LAYOUT_NODES, c.start_time);
         StepContext ctx;
         ctx.t = c.start_time;

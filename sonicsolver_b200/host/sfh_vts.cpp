@@ -26,9 +26,15 @@ bool write_vts(const std::string& path, const VtsGeometry& geo, const std::vecto
         << "        <DataArray type=\"Float64\" NumberOfComponents=\"3\" format=\"ascii\">\n";
     for (int k = 0; k < nz; ++k)
         for (int j = 0; j < ny; ++j) {
-            for (int i = 0; i < nx; ++i)
-                out << geo.origin[0] + i * geo.h[0] << ' ' << geo.origin[1] + j * geo.h[1] << ' '
-                    << geo.origin[2] + k * geo.h[2] << ' ';
+            for (int i = 0; i < nx; ++i) {
+                if (geo.points) {
+                    const double* p = &(*geo.points)[((size_t(k) * ny + j) * nx + i) * 3];
+                    out << p[0] << ' ' << p[1] << ' ' << p[2] << ' ';
+                } else {
+                    out << geo.origin[0] + i * geo.h[0] << ' ' << geo.origin[1] + j * geo.h[1] << ' '
+                        << geo.origin[2] + k * geo.h[2] << ' ';
+                }
+            }
             out << '\n';
         }
     out << "        </DataArray>\n      </Points>\n      <PointData Scalars=\"rho\" Vectors=\"U\">\n";

@@ -16,6 +16,9 @@ struct VtsGeometry {
     int nodes[3];       // nodes per axis (1 on inactive axes)
     double origin[3];   // coordinate of node (0, 0, 0)
     double h[3];        // node spacing (unused on inactive axes)
+    // node coordinates x, y, z per node (x fastest) of a graded or curved
+    // block; null: origin + (i, j, k) h
+    const std::vector<double>* points = nullptr;
 };
 
 // q: conserved AoS [k][j][i][v] over the nodes.  Returns false when the file

@@ -20,12 +20,17 @@ def _w(path, text):
 
 def write_case(root, name, *, cells, box_hi, box_lo=(0.0, 0.0, 0.0), n_ghost=3, convection="weno5Rusanov",
                time="SSPRK3", end_time=0.2, cfl=0.5, write_interval=0.05, write_initial=False, gamma=1.4,
-               left=(1.0, 0.0, 1.0), right=(0.125, 0.0, 0.1), boundaries=None, numerics_form="terms"):
+               left=(1.0, 0.0, 1.0), right=(0.125, 0.0, 0.1), boundaries=None, numerics_form="terms",
+               vertices=None, hex=tuple(range(8)), grading=(1.0, 1.0, 1.0), edges=(), scale=1.0):
     """A Riemann problem: leftHalf / rightHalf states (rho, u, p) split at
     i < nx/2.  `boundaries` maps patch -> condition, or patch -> {field:
     condition} for per-field laws (written verbatim, so the SonicFile form
     `fixedValue: [1 0 0]` works); omitted patches get none.  Defaults to
-    zeroGradient Left/Right and empty side patches."""
+    zeroGradient Left/Right and empty side patches.  The block is the box
+    box_lo..box_hi unless `vertices` (with the block's `hex` of vertex
+    indices) is given; `grading` per axis and arc `edges` ((v0, v1, point)
+    each) go to the generation file as the reference's generator reads
+    them."""
     if boundaries is None:
         boundaries = {"Left": "zeroGradient", "Right": "zeroGradient", "sideWalls": "empty", "frontBack": "empty"}
     d = os.path.join(root, name)
@@ -62,11 +67,16 @@ def write_case(root, name, *, cells, box_hi, box_lo=(0.0, 0.0, 0.0), n_ghost=3, 
     _w(os.path.join(d, "mesh", "mesh.yaml"), "SonicFile:\n  object: mesh\n  type: registry\n"
        "generation:\n  type: structuredMesh\n  file: mesh/generation.yaml\n")
     (x0, y0, z0), (x1, y1, z1) = box_lo, box_hi
-    gen = {"SonicFile": {"object": "mesh", "type": "generation"}, "scale": 1.0, "nGhost": n_ghost,
-           "vertices": [[x0, y0, z0], [x1, y0, z0], [x1, y1, z0], [x0, y1, z0],
-                        [x0, y0, z1], [x1, y0, z1], [x1, y1, z1], [x0, y1, z1]],
-           "blocks": [{"vertices": list(range(8)), "cells": list(cells), "grading": [1.0, 1.0, 1.0]}],
-           "edges": [], "patches": []}
+    if vertices is None:
+        vertices = [[x0, y0, z0], [x1, y0, z0], [x1, y1, z0], [x0, y1, z0],
+                    [x0, y0, z1], [x1, y0, z1], [x1, y1, z1], [x0, y1, z1]]
+    gen = {"SonicFile": {"object": "mesh", "type": "generation"}, "scale": float(scale), "nGhost": n_ghost,
+           "vertices": [[float(c) for c in v] for v in vertices],
+           "blocks": [{"vertices": [int(i) for i in hex], "cells": [int(c) for c in cells],
+                       "grading": [float(g) for g in grading]}],
+           "edges": [{"type": "arc", "vertices": [int(a), int(b)], "point": [float(c) for c in pt]}
+                     for a, b, pt in edges],
+           "patches": []}
     _w(os.path.join(d, "mesh", "generation.yaml"), json.dumps(gen, indent=2) + "\n")
     _w(os.path.join(d, "fields", "fields.yaml"), "SonicFile:\n  object: fields\n  type: registry\n"
        "internalField:\n  type: internalField\n  file: fields/internalField.yaml\n"

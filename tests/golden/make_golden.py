@@ -15,6 +15,13 @@ source tree and oracle/_ref are available: ``python tests/golden/make_golden.py`
   through oracle/_ref `sfr_fill_laws`) applied to small seeded states with
   law ends on every active axis: every density / velocity / pressure law
   combination on a 1-D grid, a cycle of combinations on 2-D and 3-D grids.
+* createmesh_blocks.npz -- the reference generator's node coordinates of
+  blocks 0, 1 and 2 of its test/createMesh case (block 0: a 40 x 40 x 190
+  box whose hex runs against the axes; blocks 1 and 2: 40 x 20 x 190 hexes
+  with two arc edges each, transfinite interpolation), read from the
+  mesh_block00N.vts files that case holds, on the z planes k = 0, 1, 95,
+  190; with the vertices, hexes, cells, grading and arc edges of its
+  mesh/generation.yaml.
 """
 import json
 import os
@@ -123,8 +130,35 @@ def ref_laws_fixture():
     np.savez_compressed(os.path.join(HERE, "ref_laws.npz"), **arrays)
 
 
+def createmesh_fixture(blocks=(0, 1, 2), planes=(0, 1, 95, 190)):
+    import re
+    case = os.path.join(REF_ROOT, "test", "createMesh", "mesh")
+    with open(os.path.join(case, "generation.yaml")) as f:
+        gen = json.load(f)
+    assert all(e["type"] == "arc" for e in gen["edges"])
+    out = {"vertices": np.array(gen["vertices"], dtype=np.float64), "planes": np.array(planes),
+           "scale": np.array(gen.get("scale", 1.0)),
+           "edge_vertices": np.array([e["vertices"] for e in gen["edges"]]),
+           "edge_points": np.array([e["point"] for e in gen["edges"]], dtype=np.float64)}
+    for b in blocks:
+        blk = gen["blocks"][b]
+        with open(os.path.join(case, f"mesh_block{b:03d}.vts")) as f:
+            text = f.read()
+        ext = [int(x) for x in re.search(r'WholeExtent="([^"]+)"', text).group(1).split()]
+        nx, ny, nz = ext[1] + 1, ext[3] + 1, ext[5] + 1
+        body = re.search(r"<Points>\s*<DataArray[^>]*>(.*?)</DataArray>", text, re.S).group(1)
+        pts = np.array(body.split(), dtype=np.float64).reshape(nz, ny, nx, 3)
+        assert (nx - 1, ny - 1, nz - 1) == tuple(blk["cells"])
+        out[f"points_{b}"] = pts[list(planes)]
+        out[f"hex_{b}"] = np.array(blk["vertices"])
+        out[f"cells_{b}"] = np.array(blk["cells"])
+        out[f"grading_{b}"] = np.array(blk["grading"], dtype=np.float64)
+    np.savez_compressed(os.path.join(HERE, "createmesh_blocks.npz"), **out)
+
+
 if __name__ == "__main__":
     sod_fixture()
     ref_rhs_fixture()
     ref_laws_fixture()
+    createmesh_fixture()
     print("fixtures written to", HERE)

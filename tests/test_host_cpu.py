@@ -5,6 +5,8 @@ bindings without touching a GPU."""
 import os
 import subprocess
 
+import numpy as np
+
 import pytest
 
 from case_dirs import write_case
@@ -152,3 +154,149 @@ def test_law_patch_errors(runner, tmp_path):
     r3 = run(runner, write_case(str(tmp_path), "np", cells=(40, 1, 1), box_hi=(1.0, 0.1, 0.1),
                                 boundaries=noslip_p), "--describe")
     assert r3.returncode == 3 and "noSlip" in r3.stderr
+
+
+# ---- graded and curved blocks: the generator's node coordinates and metrics
+
+CREATEMESH = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "createmesh_blocks.npz"))
+ALL_ZG = {"Left": "zeroGradient", "Right": "zeroGradient", "sideWalls": "zeroGradient", "frontBack": "zeroGradient"}
+TWO_D = {"Left": "zeroGradient", "Right": "zeroGradient", "sideWalls": "zeroGradient", "frontBack": "empty"}
+
+
+def _dump(runner, d, *flags):
+    r = run(runner, d, "--describe", *flags)
+    assert r.returncode == 0, r.stdout + r.stderr
+    return r.stdout
+
+
+def _sixth_digit(want):
+    """One unit in the sixth significant digit of each value (the
+    reference's .vts files print coordinates with six digits)."""
+    a = np.abs(want)
+    return np.where(a > 0, 10.0 ** (np.floor(np.log10(np.where(a > 0, a, 1.0))) - 5), 0.0) + 1e-12
+
+
+@pytest.mark.parametrize("block", [0, 1, 2])
+def test_createmesh_blocks_match_the_reference_generator(runner, tmp_path, block):
+    """Blocks 0-2 of the reference's createMesh case (a box whose hex runs
+    against the axes; two 40 x 20 x 190 hexes with arc edges, transfinite
+    interpolation): the node coordinates equal the reference generator's
+    own .vts output to its six printed digits."""
+    g = CREATEMESH
+    edges = [(int(a), int(b), p) for (a, b), p in zip(g["edge_vertices"], g["edge_points"])]
+    c = g[f"cells_{block}"]
+    d = write_case(str(tmp_path), f"blk{block}", cells=tuple(int(x) for x in c), box_hi=(1, 1, 1),
+                   vertices=g["vertices"], hex=g[f"hex_{block}"], grading=g[f"grading_{block}"], edges=edges,
+                   boundaries=ALL_ZG)
+    f = os.path.join(str(tmp_path), "points.bin")
+    out = _dump(runner, d, "--dump-points", f)
+    assert "mesh curvilinear (transfinite, arc edges)" in out
+    P = np.fromfile(f).reshape(c[2] + 1, c[1] + 1, c[0] + 1, 3)[g["planes"]]
+    want = g[f"points_{block}"]
+    assert (np.abs(P - want) <= _sixth_digit(want)).all()
+    # the printed digits themselves agree almost everywhere (the rest sit on
+    # a rounding boundary or are round-off around zero)
+    printed = np.array([float("%g" % v) for v in P.ravel()]).reshape(P.shape)
+    assert (printed == want).mean() > 0.98
+
+
+def test_graded_block_points_and_metrics(runner, tmp_path):
+    """A graded box (no edges: trilinear interpolation with the generator's
+    geometric grading): node coordinates follow x_i = x0 + L (1 - g^i) /
+    (1 - g^n), and the symmetric conservative metrics of the orthogonal
+    grid are xi_x = 2 / (x_i+1 - x_i-1) (likewise eta_y, zeta_z), zero
+    cross terms, Jac = 1 / J the product of the central spacings; the
+    metric identity audit passes."""
+    cells, grading, lo, hi = (12, 8, 6), (2.0, 0.5, 1.3), (-0.5, 0.25, 1.0), (1.5, 1.0, 1.6)
+    d = write_case(str(tmp_path), "graded", cells=cells, box_lo=lo, box_hi=hi, grading=grading, boundaries=ALL_ZG)
+    fp, fm = os.path.join(str(tmp_path), "p.bin"), os.path.join(str(tmp_path), "m.bin")
+    out = _dump(runner, d, "--dump-points", fp, "--dump-metrics", fm)
+    assert "mesh curvilinear (trilinear, graded)" in out
+    nodes = [c + 1 for c in cells]
+    P = np.fromfile(fp).reshape(nodes[2], nodes[1], nodes[0], 3)
+    axes = []
+    for a in range(3):
+        t = (1 - grading[a] ** np.arange(nodes[a])) / (1 - grading[a] ** cells[a])
+        axes.append(lo[a] + (hi[a] - lo[a]) * t)
+    Z, Y, X = np.meshgrid(axes[2], axes[1], axes[0], indexing="ij")
+    for a, want in enumerate((X, Y, Z)):
+        assert np.abs(P[..., a] - want).max() <= 4e-14
+    e = [n + 6 for n in nodes]
+    M = np.fromfile(fm).reshape(e[2], e[1], e[0], 10)[3:-3, 3:-3, 3:-3]     # the nodes
+    dc = [(ax[2:] - ax[:-2]) / 2 for ax in axes]                            # central spacings of inner nodes
+    DZ, DY, DX = np.meshgrid(dc[2], dc[1], dc[0], indexing="ij")
+    Mi = M[1:-1, 1:-1, 1:-1]
+    for comp, dd in ((1, DX), (5, DY), (9, DZ)):
+        assert np.abs(Mi[..., comp] * dd - 1).max() <= 1e-13
+    for comp in (2, 3, 4, 6, 7, 8):
+        assert np.abs(Mi[..., comp]).max() <= 1e-12 * np.abs(Mi[..., (1, 5, 9)]).max()
+    assert np.abs(Mi[..., 0] * DX * DY * DZ - 1).max() <= 1e-13
+    line = out.split("metric identity residual ")[1].splitlines()[0]
+    res, tol = [float(v) for v in line.split(", tolerance ")]
+    assert res <= tol
+
+
+def test_block_orientation_and_curved_limits(runner, tmp_path):
+    """A box listed in the canonical corner order runs on the uniform path;
+    the same box with its hex listed against the axes takes the generated
+    coordinates; periodic ends on a curved block are refused (the reference
+    has no periodic boundary there)."""
+    out = _dump(runner, write_case(str(tmp_path), "box", cells=(16, 8, 1), box_hi=(2.0, 1.0, 0.1),
+                                   boundaries=TWO_D))
+    assert "mesh curvilinear" not in out and "dim=2 nodes=17,9,1 h=0.125,0.125," in out
+    verts = [[2.0, 0.0, 0.0], [0.0, 0.0, 0.0], [0.0, 1.0, 0.0], [2.0, 1.0, 0.0],
+             [2.0, 0.0, 0.1], [0.0, 0.0, 0.1], [0.0, 1.0, 0.1], [2.0, 1.0, 0.1]]
+    out2 = _dump(runner, write_case(str(tmp_path), "flipped", cells=(16, 8, 1), box_hi=(1, 1, 1), vertices=verts,
+                                    boundaries=TWO_D))
+    assert "mesh curvilinear (trilinear, graded)" in out2
+    arc = [(0, 1, (0.0, 1.5, 0.0)), (4, 5, (0.0, 1.5, 1.0))]
+    ring = [[1.0, 1.0, 0.0], [-1.0, 1.0, 0.0], [-0.5, 0.5, 0.0], [0.5, 0.5, 0.0],
+            [1.0, 1.0, 1.0], [-1.0, 1.0, 1.0], [-0.5, 0.5, 1.0], [0.5, 0.5, 1.0]]
+    per = {"Left": "periodic", "Right": "periodic", "sideWalls": "zeroGradient", "frontBack": "empty"}
+    r = run(runner, write_case(str(tmp_path), "ring", cells=(20, 10, 1), box_hi=(1, 1, 1), vertices=ring,
+                               edges=arc, boundaries=per), "--describe")
+    assert r.returncode == 3 and "periodic ends on a graded or curved block" in r.stderr
+
+
+PIN_BLOCKS = {
+    # arc block 1 of createMesh, shortened in z and scaled (edges scale with it)
+    "arc": dict(cells=(40, 20, 30), vertices=CREATEMESH["vertices"], hex=CREATEMESH["hex_1"], scale=0.01,
+                edges=[(int(a), int(b), p) for (a, b), p in zip(CREATEMESH["edge_vertices"], CREATEMESH["edge_points"])]),
+    # the centre box of createMesh, listed against the axes (TFI: the file has edges)
+    "centre": dict(cells=(20, 20, 10), vertices=CREATEMESH["vertices"], hex=CREATEMESH["hex_0"],
+                   edges=[(int(a), int(b), p) for (a, b), p in zip(CREATEMESH["edge_vertices"],
+                                                                  CREATEMESH["edge_points"])]),
+    "graded": dict(cells=(12, 8, 6), vertices=[[-0.5, 0.25, 1.0], [1.5, 0.25, 1.0], [1.5, 1.0, 1.0], [-0.5, 1.0, 1.0],
+                                               [-0.5, 0.25, 1.6], [1.5, 0.25, 1.6], [1.5, 1.0, 1.6], [-0.5, 1.0, 1.6]],
+                   grading=(2.0, 0.5, 1.3)),
+    "skewed": dict(cells=(14, 9, 7), grading=(1.2, 0.9, 1.1),
+                   vertices=[[0, 0, 0], [1.2, 0.15, 0.1], [1.35, 0.95, -0.05], [-0.1, 0.8, 0], [0.05, 0.02, 0.5],
+                             [1.1, 0.2, 0.6], [1.3, 1.0, 0.55], [0, 0.9, 0.45]]),
+}
+
+
+@pytest.mark.parametrize("name", sorted(PIN_BLOCKS))
+def test_block_geometry_is_the_reference_generators(runner, tmp_path, name):
+    """The host's node coordinates equal, bit for bit, those of the
+    reference's own generator compiled from its sources (oracle/_ref), for
+    arc-edged, graded and skewed blocks; the metrics handed to the provider
+    equal, bit for bit, the oracle's restatement of the reference Field's
+    metrics from those coordinates (ghost extrapolation, symmetric
+    conservative cofactors, outer-layer copies), with the same identity
+    residual."""
+    import pyoracle as po
+    if po.ref_mesh_lib() is None:
+        pytest.skip("oracle/_ref/libsfmesh.so not built (reference sources unavailable)")
+    kw = PIN_BLOCKS[name]
+    d = write_case(str(tmp_path), name, box_hi=(1, 1, 1), boundaries=ALL_ZG, **kw)
+    fp, fm = os.path.join(d, "p.bin"), os.path.join(d, "m.bin")
+    out = _dump(runner, d, "--dump-points", fp, "--dump-metrics", fm)
+    c = kw["cells"]
+    P = np.fromfile(fp).reshape(c[2] + 1, c[1] + 1, c[0] + 1, 3)
+    R = po.ref_mesh_points(kw["vertices"], kw.get("hex", range(8)), c, kw.get("grading", (1.0, 1.0, 1.0)),
+                           kw.get("edges", ()), kw.get("scale", 1.0))
+    assert np.array_equal(P, R)
+    want, res, tol = po.field_metrics(R, 3)
+    assert np.array_equal(np.fromfile(fm).reshape(want.shape), want)
+    line = out.split("metric identity residual ")[1].splitlines()[0]
+    assert float(line.split(",")[0]) == float("%.3g" % res) and res <= tol
