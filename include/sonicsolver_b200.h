@@ -229,6 +229,17 @@ int sfg_set_metrics(sfg_solver s, const double* metrics, int layout);
  * time to `time`. */
 int sfg_upload(sfg_solver s, const double* host, int layout, double time);
 int sfg_download(sfg_solver s, double* host, int layout);
+/* Resume: sfg_upload plus the step counter (the time and step count that
+ * sfg_time reported when the state was downloaded).  A run downloaded
+ * between two steps and restored into a solver with the same grid, numerics
+ * and metrics continues with the same dt sequence and the same bits as the
+ * run that was never interrupted: between steps the device keeps nothing
+ * but the state and the clock, and the CFL minimum is recomputed from the
+ * state.  The reference restarts from a state file and the case's start
+ * time (CheckpointIO::read, src/infrastructure/io/checkpoint/SF_checkpoint.h:6;
+ * initializeSingleFluidRestart, src/models/physics/fluidStateModel/
+ * SF_factory.h:137-150). */
+int sfg_restore(sfg_solver s, const double* host, int layout, double time, int64_t steps);
 /* The same from / to device memory (AoS node layout, no ghosts). */
 int sfg_upload_device(sfg_solver s, const double* dev_nodes_aos, double time);
 int sfg_download_device(sfg_solver s, double* dev_nodes_aos);
@@ -297,6 +308,19 @@ int sfg_batch_add(sfg_batch b, const sfg_grid_desc* grid, const double* host_nod
  * grid of a batch. */
 int sfg_batch_add_ex(sfg_batch b, const sfg_grid_desc* grid, const sfg_numerics_desc* numerics,
                      const double* host_nodes_aos, double t_end, int64_t max_steps, int* slot);
+/* sfg_batch_add_ex for a grid with boundary ends of every kind a single-grid
+ * solver takes: frozen ends (SFG_BC_FROZEN: a patch without a condition)
+ * and law ends (SFG_BC_LAW) whose laws are laws[2 * axis + end] (read only
+ * at those ends; may be NULL when the grid has none), checked as
+ * sfg_set_boundary_law checks them.  The laws run where the single-grid
+ * solver runs them (the step's start, before every stage's RHS, after the
+ * last stage) with the same arithmetic, so a grid gives the same results in
+ * a batch as alone: a reference case with a fixedValue inflow, a noSlip wall
+ * or an unconditioned patch (Boundary::Applicator, solver/boundary/
+ * SF_applicator.h:51-83, 162-187) runs batched as written. */
+int sfg_batch_add_laws(sfg_batch b, const sfg_grid_desc* grid, const sfg_numerics_desc* numerics,
+                       const sfg_boundary_law* laws, const double* host_nodes_aos, double t_end, int64_t max_steps,
+                       int* slot);
 int sfg_batch_remove(sfg_batch b, int slot);
 /* Runs up to `steps` batch steps (graph of `graph_steps`, <= 0: 16); stops
  * early when no grid is running.  *active = grids that stepped last. */
@@ -337,6 +361,12 @@ int sfg_server_submit(sfg_server s, const sfg_grid_desc* grid, const double* hos
  * under the rules of sfg_batch_add_ex, checked before the request queues. */
 int sfg_server_submit_ex(sfg_server s, const sfg_grid_desc* grid, const sfg_numerics_desc* numerics,
                          const double* host_nodes_aos, double t_end, int64_t max_steps, int64_t* request_id);
+/* sfg_server_submit_ex with the grid's boundary laws (laws[2 * axis + end]
+ * for its SFG_BC_LAW ends; NULL when it has none), under the rules of
+ * sfg_batch_add_laws, checked before the request queues. */
+int sfg_server_submit_laws(sfg_server s, const sfg_grid_desc* grid, const sfg_numerics_desc* numerics,
+                           const sfg_boundary_law* laws, const double* host_nodes_aos, double t_end,
+                           int64_t max_steps, int64_t* request_id);
 int sfg_server_poll(sfg_server s, int64_t request_id, sfg_request_info* info);
 /* Result of a finished request (AoS nodes); SFG_ERR_ARG while not done. */
 int sfg_server_fetch(sfg_server s, int64_t request_id, double* host_nodes_aos);

@@ -33,7 +33,7 @@ LAYOUT_NODES, LAYOUT_FIELD = 0, 1
 # The C-ABI symbols declared by include/sonicsolver_b200.h (checked by tests).
 EXPORTS = (
     "sfg_last_error", "sfg_version", "sfg_recipe_name", "sfg_recipe_from_name", "sfg_create",
-    "sfg_destroy", "sfg_ghost_layers", "sfg_state_size", "sfg_upload", "sfg_download",
+    "sfg_destroy", "sfg_ghost_layers", "sfg_state_size", "sfg_upload", "sfg_restore", "sfg_download",
     "sfg_upload_device", "sfg_download_device", "sfg_compute_dt", "sfg_stage", "sfg_step",
     "sfg_advance", "sfg_residual", "sfg_stage_with_residual", "sfg_conserved_totals", "sfg_time",
     "sfg_status_word", "sfg_set_counting", "sfg_get_counters", "sfg_time_sweeps", "sfg_measure_fma_peak",
@@ -50,6 +50,26 @@ class BoundaryLaw(ctypes.Structure):
     _fields_ = [("rho", ctypes.c_int), ("velocity", ctypes.c_int), ("pressure", ctypes.c_int),
                 ("reserved", ctypes.c_int), ("rho_value", ctypes.c_double),
                 ("velocity_value", ctypes.c_double * 3), ("pressure_value", ctypes.c_double)]
+
+
+def law_array(laws):
+    """The laws of a grid's law ends as the C ABI takes them
+    (laws[2 * axis + end]) from {(axis, end): dict(rho=, velocity=, pressure=,
+    rho_value=, velocity_value=, pressure_value=)}; None when `laws` is
+    empty."""
+    if not laws:
+        return None
+    arr = (BoundaryLaw * 6)()
+    for (axis, end), kw in laws.items():
+        law = arr[2 * axis + end]
+        law.rho = int(kw.get("rho", LAW_ZERO_GRADIENT))
+        law.velocity = int(kw.get("velocity", LAW_ZERO_GRADIENT))
+        law.pressure = int(kw.get("pressure", LAW_ZERO_GRADIENT))
+        law.rho_value = float(kw.get("rho_value", 0.0))
+        for d, v in enumerate(kw.get("velocity_value", (0.0, 0.0, 0.0))):
+            law.velocity_value[d] = float(v)
+        law.pressure_value = float(kw.get("pressure_value", 0.0))
+    return arr
 
 
 class NumericsDesc(ctypes.Structure):
@@ -104,6 +124,7 @@ def lib():
         L.sfg_set_metrics.argtypes = [_VP, _DP, ctypes.c_int]
         L.sfg_state_size.argtypes = [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]
         L.sfg_upload.argtypes = [_VP, _DP, ctypes.c_int, ctypes.c_double]
+        L.sfg_restore.argtypes = [_VP, _DP, ctypes.c_int, ctypes.c_double, ctypes.c_int64]
         L.sfg_download.argtypes = [_VP, _DP, ctypes.c_int]
         L.sfg_upload_device.argtypes = [_VP, _VP, ctypes.c_double]
         L.sfg_download_device.argtypes = [_VP, _VP]
@@ -133,6 +154,9 @@ def lib():
         L.sfg_batch_instance_bytes.argtypes = [_VP, PG, ctypes.POINTER(ctypes.c_size_t)]
         L.sfg_batch_add.argtypes = [_VP, PG, _DP, ctypes.c_double, ctypes.c_int64, ctypes.POINTER(ctypes.c_int)]
         L.sfg_batch_add_ex.argtypes = [_VP, PG, PN, _DP, ctypes.c_double, ctypes.c_int64, ctypes.POINTER(ctypes.c_int)]
+        PL = ctypes.POINTER(BoundaryLaw)
+        L.sfg_batch_add_laws.argtypes = [_VP, PG, PN, PL, _DP, ctypes.c_double, ctypes.c_int64,
+                                         ctypes.POINTER(ctypes.c_int)]
         L.sfg_batch_remove.argtypes = [_VP, ctypes.c_int]
         L.sfg_batch_step.argtypes = [_VP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
         L.sfg_batch_status.argtypes = [_VP, ctypes.c_int, _DP, I64P, ctypes.POINTER(ctypes.c_int),
@@ -147,6 +171,8 @@ def lib():
         L.sfg_server_destroy.argtypes = [_VP]
         L.sfg_server_submit.argtypes = [_VP, PG, _DP, ctypes.c_double, ctypes.c_int64, I64P]
         L.sfg_server_submit_ex.argtypes = [_VP, PG, PN, _DP, ctypes.c_double, ctypes.c_int64, I64P]
+        L.sfg_server_submit_laws.argtypes = [_VP, PG, PN, ctypes.POINTER(BoundaryLaw), _DP, ctypes.c_double,
+                                             ctypes.c_int64, I64P]
         L.sfg_server_poll.argtypes = [_VP, ctypes.c_int64, ctypes.POINTER(RequestInfo)]
         L.sfg_server_fetch.argtypes = [_VP, ctypes.c_int64, _DP]
         L.sfg_server_cancel.argtypes = [_VP, ctypes.c_int64]
@@ -236,6 +262,11 @@ class Solver:
 
     def upload(self, q: np.ndarray, time: float = 0.0, layout=LAYOUT_NODES):
         check(lib().sfg_upload(self._h, _dptr(q), layout, time))
+
+    def restore(self, q: np.ndarray, time: float, steps: int, layout=LAYOUT_NODES):
+        """Resume a run: the state, its time and its step count (as `time()`
+        reported them when the state was downloaded)."""
+        check(lib().sfg_restore(self._h, _dptr(q), layout, time, int(steps)))
 
     def download(self, layout=LAYOUT_NODES, out: np.ndarray | None = None) -> np.ndarray:
         if out is None:
@@ -364,13 +395,16 @@ class Batch:
         except Exception:
             pass
 
-    def add(self, case, t_end=None, max_steps=0, recipe=None, gamma=None, cfl=None, max_dt=None) -> int:
+    def add(self, case, t_end=None, max_steps=0, recipe=None, gamma=None, cfl=None, max_dt=None, laws=None) -> int:
+        """A grid with its own numerics where given; `laws` ({(axis, end):
+        dict}, see law_array) for its BC_LAW ends."""
         g = grid_desc(case.dim, case.n, case.h, case.bc_lo, case.bc_hi)
         slot = ctypes.c_int()
         q = np.ascontiguousarray(case.q, dtype=np.float64)
         nm = _own_numerics(self.defaults, recipe, gamma, cfl, max_dt)
-        check(lib().sfg_batch_add_ex(self._h, ctypes.byref(g), ctypes.byref(nm) if nm is not None else None, _dptr(q),
-                                     case.t_end if t_end is None else t_end, max_steps, ctypes.byref(slot)))
+        check(lib().sfg_batch_add_laws(self._h, ctypes.byref(g), ctypes.byref(nm) if nm is not None else None,
+                                       law_array(laws), _dptr(q), case.t_end if t_end is None else t_end, max_steps,
+                                       ctypes.byref(slot)))
         self.shapes[slot.value] = q.shape
         return slot.value
 
@@ -440,14 +474,15 @@ class Server:
         except Exception:
             pass
 
-    def submit(self, case, t_end=None, max_steps=0, recipe=None, gamma=None, cfl=None, max_dt=None) -> int:
+    def submit(self, case, t_end=None, max_steps=0, recipe=None, gamma=None, cfl=None, max_dt=None,
+               laws=None) -> int:
         g = grid_desc(case.dim, case.n, case.h, case.bc_lo, case.bc_hi)
         q = np.ascontiguousarray(case.q, dtype=np.float64)
         rid = ctypes.c_int64()
         nm = _own_numerics(self.defaults, recipe, gamma, cfl, max_dt)
-        check(lib().sfg_server_submit_ex(self._h, ctypes.byref(g), ctypes.byref(nm) if nm is not None else None,
-                                         _dptr(q), case.t_end if t_end is None else t_end, int(max_steps),
-                                         ctypes.byref(rid)))
+        check(lib().sfg_server_submit_laws(self._h, ctypes.byref(g), ctypes.byref(nm) if nm is not None else None,
+                                           law_array(laws), _dptr(q), case.t_end if t_end is None else t_end,
+                                           int(max_steps), ctypes.byref(rid)))
         self.shapes[rid.value] = q.shape
         return rid.value
 

@@ -18,15 +18,23 @@
 // contiguous ranges, and each stage runs one persistent kernel per group (the
 // recipe's template instance), the groups' kernels on parallel branches so
 // that one group's blocks fill the SMs that another's tail leaves idle.
+// A grid may have frozen ends (a patch without a condition) and law ends
+// (fixedValue / zeroGradient / symmetry laws per field) as a single-grid
+// solver has them: the instance's device grid carries the extra end nodes,
+// and a law kernel applies every law instance's laws at the points the
+// single-grid solver does (step start, before each stage's RHS, after the
+// last stage), with the same arithmetic (sfg_laws.cuh).
 // Host side: the batch step is captured once as a CUDA graph of G steps.
 // Adding or removing instances rewrites the table rows and the work list in
 // device memory between graph launches, so the graph needs recapture only
 // when a grid brings a recipe the batch has not run yet (continuous
 // batching).
 #include "../../include/sonicsolver_b200.h"
+#include "sfg_laws.cuh"
 #include "sfg_tile.cuh"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdarg>
 #include <cstring>
@@ -43,6 +51,7 @@ cudaError_t launch_aos_to_soa(const double* aos, double* soa, long long nodes, l
 struct BatchInst {
     GridView g;
     double *qn, *qa, *qb, *k;
+    const LawView* law;  // law ends (device copy in the slab), or null
     Clock clock;
     unsigned flags;
     int live;  // slot in use
@@ -54,6 +63,12 @@ struct WorkItem {
     int inst, x0, y0, dim;
 };
 
+// A run of up to LAW_CHUNK face points of one law instance.
+constexpr int LAW_CHUNK = 128;
+struct LawItem {
+    int inst, first, count, pad;
+};
+
 constexpr int kMaxGroups = 8;  // one per convection recipe the batch kernels provide
 constexpr int kCounters = 8 + 4 * kMaxGroups;
 
@@ -61,7 +76,7 @@ struct BatchCtl {
     int n_items;
     int n_inst;
     int active;  // instances stepping in the current step
-    int pad;
+    int n_law_items;
     // work stealing: [0] dt, [5] copy, [8 + 4 g + s] stage s of recipe group g
     int counters[kCounters];
     // tile range of group g in the work list: [2 g] first item, [2 g + 1] count
@@ -139,6 +154,32 @@ __global__ void __launch_bounds__(TILE_THREADS, F32 ? 4 : 2)
         if (flags) atomicOr(&b.flags, flags);
         if (last) flush_cfl_block(b.g, &b.clock, sr);
         __syncthreads();  // shared arrays are reused by the next tile
+    }
+}
+
+// The boundary laws of every stepping law instance, where the single-grid
+// solver applies them: phase 0 at the step's start (FlowStepPrepare, on qn),
+// phase 1 before stage `stage` reads its input (prepareBoundaryState; the
+// previous application's values sit in the previous stage's input), phase 2
+// on the last stage's output (FlowStepCommit).
+__global__ void __launch_bounds__(LAW_CHUNK)
+    batch_law_kernel(BatchInst* inst, const LawItem* items, BatchCtl* ctl, int phase, int stage, int time_id) {
+    const int n = ctl->n_law_items;
+    for (int k = blockIdx.x; k < n; k += gridDim.x) {
+        const LawItem w = items[k];
+        BatchInst& b = inst[w.inst];
+        if (!b.live || !b.clock.active || !b.law || (int)threadIdx.x >= w.count) continue;
+        const double* old = b.qn;
+        double* q = b.qn;
+        if (phase == 1) {
+            q = const_cast<double*>(batch_stage_view(b, stage, time_id).qs);
+            if (stage > 0) old = batch_stage_view(b, stage - 1, time_id).qs;
+        } else if (phase == 2) {
+            const StageView last = batch_stage_view(b, stage, time_id);
+            q = last.qout;
+            old = last.qs;
+        }
+        law_fill_point(b.g, *b.law, old, q, (long long)w.first + threadIdx.x, &b.flags);
     }
 }
 
@@ -349,6 +390,16 @@ struct sfg_batch_s {
     WorkItem* d_items = nullptr;
     size_t items_cap = 0;
     std::vector<WorkItem> h_items;
+    // per slot: the caller's grid and the device grid's offset (extra end
+    // nodes of frozen and law ends), its law view (count 0: none)
+    std::vector<sfg_grid_desc> inst_pub;
+    std::vector<std::array<int, 3>> inst_off;
+    std::vector<LawView> inst_law;
+    bool has_laws = false;  // a law instance was added: the step graph has the law launches
+    LawItem* d_law_items = nullptr;
+    size_t law_items_cap = 0;
+    std::vector<LawItem> h_law_items;
+    int law_grid = 0;
     BatchCtl* d_ctl = nullptr;
     BatchCtl* h_ctl = nullptr;  // pinned
     double* staging = nullptr;
@@ -403,6 +454,7 @@ int bind_kernels(sfg_batch_s* b) {
     int sms = 0;
     BCUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
     b->grid_items = sms * 4;
+    b->law_grid = sms * 8;
     if (b->graph) {
         cudaGraphExecDestroy(b->graph);
         b->graph = nullptr;
@@ -509,6 +561,32 @@ int publish_items(sfg_batch_s* b) {
     if (!b->h_items.empty())
         BCUDA(cudaMemcpyAsync(b->d_items, b->h_items.data(), b->h_items.size() * sizeof(WorkItem),
                               cudaMemcpyHostToDevice, b->stream));
+    // law points of the live law instances, in runs of LAW_CHUNK
+    b->h_law_items.clear();
+    for (int i = 0; i < (int)b->h_inst.size(); ++i) {
+        const BatchInst& r = b->h_inst[i];
+        if (!r.live || r.done || !r.law) continue;
+        const LawView& lv = b->inst_law[i];
+        const int pts = (int)lv.start[lv.count];
+        for (int f = 0; f < pts; f += LAW_CHUNK) b->h_law_items.push_back({i, f, std::min(LAW_CHUNK, pts - f), 0});
+    }
+    if (b->h_law_items.size() > b->law_items_cap) {
+        size_t cap = std::max<size_t>(b->h_law_items.size() * 2, 256);
+        if (b->d_law_items) cudaFree(b->d_law_items);
+        b->d_law_items = nullptr;
+        BCUDA(cudaMalloc((void**)&b->d_law_items, cap * sizeof(LawItem)));
+        b->law_items_cap = cap;
+        if (b->graph) {  // the graph holds the old list address
+            cudaGraphExecDestroy(b->graph);
+            b->graph = nullptr;
+        }
+    }
+    if (!b->h_law_items.empty())
+        BCUDA(cudaMemcpyAsync(b->d_law_items, b->h_law_items.data(), b->h_law_items.size() * sizeof(LawItem),
+                              cudaMemcpyHostToDevice, b->stream));
+    b->h_ctl->n_law_items = (int)b->h_law_items.size();
+    BCUDA(cudaMemcpyAsync(&b->d_ctl->n_law_items, &b->h_ctl->n_law_items, sizeof(int), cudaMemcpyHostToDevice,
+                          b->stream));
     b->h_ctl->n_items = (int)b->h_items.size();
     b->h_ctl->n_inst = (int)b->h_inst.size();
     BCUDA(cudaMemcpyAsync(&b->d_ctl->n_items, &b->h_ctl->n_items, 2 * sizeof(int), cudaMemcpyHostToDevice, b->stream));
@@ -525,7 +603,13 @@ int enqueue_batch_step(sfg_batch_s* b) {
     batch_finalize_kernel<<<(ni + 127) / 128, 128, 0, b->stream>>>(b->d_inst, b->d_ctl);
     const int ns = stage_count_of(b->num.time_recipe);
     const int ng = (int)b->groups.size();
+    auto laws = [&](int phase, int stage) {
+        batch_law_kernel<<<b->law_grid, LAW_CHUNK, 0, b->stream>>>(b->d_inst, b->d_law_items, b->d_ctl, phase, stage,
+                                                                 b->num.time_recipe);
+    };
+    if (b->has_laws) laws(0, 0);  // FlowStepPrepare
     for (int s = 0; s < ns; ++s) {
+        if (b->has_laws) laws(1, s);  // the stage input's boundary state
         // group 0 on the batch's stream, every other group on a branch
         // forked from it and joined back before the next stage
         if (ng > 1) BCUDA(cudaEventRecord(b->fork, b->stream));
@@ -539,6 +623,7 @@ int enqueue_batch_step(sfg_batch_s* b) {
         }
         for (int g = 1; g < ng; ++g) BCUDA(cudaStreamWaitEvent(b->stream, b->groups[g].joined, 0));
     }
+    if (b->has_laws) laws(2, ns - 1);  // FlowStepCommit on the last stage's output
     if (b->num.time_recipe == T_EULER) b->copy_k<<<b->grid_items, TILE_THREADS, 0, b->stream>>>(b->d_inst, b->d_items, b->d_ctl);
     batch_commit_kernel<<<(ni + 127) / 128, 128, 0, b->stream>>>(b->d_inst, b->d_ctl);
     BCUDA(cudaGetLastError());
@@ -561,12 +646,19 @@ int instance_numerics(const sfg_batch_s* b, const sfg_numerics_desc* n, const Re
     return SFG_OK;
 }
 
-int batch_grid_view(const sfg_grid_desc* d, const sfg_numerics_desc* n, int reach, GridView* out, long long* nodes) {
+// Device view of a grid: one extra node at every frozen and law end (it
+// holds the frozen ghost value, or the law's ghost value), as the
+// single-grid solver lays its grid out; off_lo: the offset of the caller's
+// node 0 on each axis.  *nodes: the device grid's node count.
+int batch_grid_view(const sfg_grid_desc* d, const sfg_numerics_desc* n, int reach, GridView* out, long long* nodes,
+                    int off_lo[3]) {
     if (!d) return bfail(SFG_ERR_ARG, "null grid");
     if (d->dim < 1 || d->dim > 2) return bfail(SFG_ERR_ARG, "batched grids are 1-D or 2-D (got %d)", d->dim);
     GridView g{};
     g.dim = d->dim;
+    auto extra_end = [](int bk) { return bk == SFG_BC_FROZEN || bk == SFG_BC_LAW; };
     for (int a = 0; a < 3; ++a) {
+        off_lo[a] = 0;
         if (!(d->h[a] > 0.0)) return bfail(SFG_ERR_ARG, "h[%d] must be > 0", a);
         g.n[a] = d->n[a];
         if (a >= d->dim) {
@@ -578,12 +670,19 @@ int batch_grid_view(const sfg_grid_desc* d, const sfg_numerics_desc* n, int reac
         const bool plo = d->bc_lo[a] == SFG_BC_PERIODIC, phi = d->bc_hi[a] == SFG_BC_PERIODIC;
         if (plo != phi) return bfail(SFG_ERR_ARG, "axis %d: periodic must be set on both ends", a);
         for (int bk : {d->bc_lo[a], d->bc_hi[a]})
-            if (bk != SFG_BC_TRANSMISSIVE && bk != SFG_BC_PERIODIC) return bfail(SFG_ERR_ARG, "unknown boundary kind");
-        if (plo ? d->n[a] < reach + 1 : d->n[a] < 3) return bfail(SFG_ERR_ARG, "axis %d has too few nodes", a);
-        g.bc_lo[a] = d->bc_lo[a];
-        g.bc_hi[a] = d->bc_hi[a];
-        g.lo[a] = plo ? 0 : 1;
-        g.hi[a] = plo ? d->n[a] : d->n[a] - 1;
+            if (bk != SFG_BC_TRANSMISSIVE && bk != SFG_BC_PERIODIC && bk != SFG_BC_FROZEN && bk != SFG_BC_LAW)
+                return bfail(SFG_ERR_ARG, "unknown boundary kind");
+        off_lo[a] = extra_end(d->bc_lo[a]) ? 1 : 0;
+        const int nd = d->n[a] + off_lo[a] + (extra_end(d->bc_hi[a]) ? 1 : 0);
+        if (plo ? d->n[a] < reach + 1 : nd < 3) return bfail(SFG_ERR_ARG, "axis %d has too few nodes", a);
+        g.n[a] = nd;
+        // a law end reads like a frozen one: ghosts clamp to its extra node
+        g.bc_lo[a] = d->bc_lo[a] == SFG_BC_LAW ? BC_FROZEN : d->bc_lo[a];
+        g.bc_hi[a] = d->bc_hi[a] == SFG_BC_LAW ? BC_FROZEN : d->bc_hi[a];
+        // transmissive and law boundary nodes and extra nodes are not advanced
+        g.lo[a] = plo ? 0 : (d->bc_lo[a] == SFG_BC_LAW ? 2 : 1);
+        g.hi[a] = plo ? nd : (d->bc_hi[a] == SFG_BC_LAW ? nd - 2 : nd - 1);
+        if (g.hi[a] <= g.lo[a]) return bfail(SFG_ERR_ARG, "axis %d has no solved node", a);
     }
     const double hx = d->h[0], hy = d->h[1], hz = d->h[2];
     g.jac = 1.0 / (hx * hy * hz);
@@ -594,10 +693,65 @@ int batch_grid_view(const sfg_grid_desc* d, const sfg_numerics_desc* n, int reac
     g.gamma = n->gamma;
     for (int a = 0; a < 3; ++a) g.h[a] = d->h[a];
     g.cfl = n->cfl;
-    *nodes = (long long)d->n[0] * d->n[1] * d->n[2];
+    *nodes = (long long)g.n[0] * g.n[1] * g.n[2];
     g.vs = (*nodes + 31) / 32 * 32;
     *out = g;
     return SFG_OK;
+}
+
+bool has_extra_nodes(const GridView& g, const sfg_grid_desc& pub) {
+    return g.n[0] != pub.n[0] || g.n[1] != pub.n[1] || g.n[2] != pub.n[2];
+}
+
+// Caller node layout -> device layout (AoS): an extra end node takes its
+// boundary node's value (the reference fills ghosts by clamping to the
+// interior, SF_mesh.cpp:544), as sfg_upload does.
+void to_device_layout(const sfg_grid_desc& pub, const GridView& g, const int off[3], const double* in,
+                      std::vector<double>& out) {
+    out.resize(5 * (size_t)g.n[0] * g.n[1] * g.n[2]);
+    for (int k = 0; k < g.n[2]; ++k)
+        for (int j = 0; j < g.n[1]; ++j)
+            for (int i = 0; i < g.n[0]; ++i) {
+                int c[3] = {i - off[0], j - off[1], k - off[2]};
+                for (int a = 0; a < 3; ++a) c[a] = std::min(std::max(c[a], 0), pub.n[a] - 1);
+                std::memcpy(&out[(((size_t)k * g.n[1] + j) * g.n[0] + i) * 5],
+                            in + (((size_t)c[2] * pub.n[1] + c[1]) * pub.n[0] + c[0]) * 5, 5 * sizeof(double));
+            }
+}
+
+// Device layout (AoS) -> caller node layout (drops the extra end nodes).
+void to_caller_layout(const sfg_grid_desc& pub, const GridView& g, const int off[3], const double* in, double* out) {
+    for (int k = 0; k < pub.n[2]; ++k)
+        for (int j = 0; j < pub.n[1]; ++j)
+            for (int i = 0; i < pub.n[0]; ++i)
+                std::memcpy(out + (((size_t)k * pub.n[1] + j) * pub.n[0] + i) * 5,
+                            in + (((size_t)(k + off[2]) * g.n[1] + (j + off[1])) * g.n[0] + (i + off[0])) * 5,
+                            5 * sizeof(double));
+}
+
+size_t align256(size_t x) { return (x + 255) / 256 * 256; }
+
+// Face points of a grid's law ends (over the solved range of the other axes).
+long long law_points(const sfg_grid_desc& pub, const GridView& g) {
+    long long pts = 0;
+    for (int a = 0; a < pub.dim; ++a)
+        for (int end = 0; end < 2; ++end) {
+            if ((end ? pub.bc_hi[a] : pub.bc_lo[a]) != SFG_BC_LAW) continue;
+            long long p = 1;
+            for (int d = 0; d < 3; ++d)
+                if (d != a) p *= g.hi[d] - g.lo[d];
+            pts += p;
+        }
+    return pts;
+}
+
+// Slab bytes of one instance: its state buffers, and for law ends the law
+// view and the state-cache codes.
+size_t instance_slab_bytes(const sfg_batch_s* b, const sfg_grid_desc& pub, const GridView& g) {
+    const size_t per = align256(sizeof(double) * 5 * (size_t)g.vs);
+    const int bufs = b->num.time_recipe == T_RK4 ? 4 : 3;
+    const long long pts = law_points(pub, g);
+    return per * bufs + (pts > 0 ? align256(sizeof(LawView)) + align256((size_t)pts) : 0);
 }
 
 }  // namespace
@@ -677,6 +831,7 @@ int sfg_batch_destroy(sfg_batch b) {
     if (b->slab) cudaFree(b->slab);
     if (b->d_inst) cudaFree(b->d_inst);
     if (b->d_items) cudaFree(b->d_items);
+    if (b->d_law_items) cudaFree(b->d_law_items);
     if (b->d_ctl) cudaFree(b->d_ctl);
     if (b->staging) cudaFree(b->staging);
     if (b->h_ctl) cudaFreeHost(b->h_ctl);
@@ -694,21 +849,27 @@ int sfg_batch_instance_bytes(sfg_batch b, const sfg_grid_desc* grid, size_t* byt
     if (!b || !grid || !bytes) return bfail(SFG_ERR_ARG, "null argument");
     GridView g;
     long long nodes = 0;
+    int off[3];
     const int reach = b->recipe->scheme == WENO3 ? 2 : (b->recipe->scheme == WENO7 ? 4 : 3);
-    int rc = batch_grid_view(grid, &b->num, reach, &g, &nodes);
+    int rc = batch_grid_view(grid, &b->num, reach, &g, &nodes, off);
     if (rc) return rc;
-    const int bufs = b->num.time_recipe == T_RK4 ? 4 : 3;
-    *bytes = ((sizeof(double) * 5 * (size_t)g.vs + 255) / 256 * 256) * bufs;
+    *bytes = instance_slab_bytes(b, *grid, g);
     return SFG_OK;
 }
 
 int sfg_batch_add(sfg_batch b, const sfg_grid_desc* grid, const double* host_nodes_aos, double t_end,
                   int64_t max_steps, int* slot) {
-    return sfg_batch_add_ex(b, grid, nullptr, host_nodes_aos, t_end, max_steps, slot);
+    return sfg_batch_add_laws(b, grid, nullptr, nullptr, host_nodes_aos, t_end, max_steps, slot);
 }
 
 int sfg_batch_add_ex(sfg_batch b, const sfg_grid_desc* grid, const sfg_numerics_desc* numerics,
                      const double* host_nodes_aos, double t_end, int64_t max_steps, int* slot) {
+    return sfg_batch_add_laws(b, grid, numerics, nullptr, host_nodes_aos, t_end, max_steps, slot);
+}
+
+int sfg_batch_add_laws(sfg_batch b, const sfg_grid_desc* grid, const sfg_numerics_desc* numerics,
+                       const sfg_boundary_law* laws, const double* host_nodes_aos, double t_end, int64_t max_steps,
+                       int* slot) {
     if (!b || !grid || !host_nodes_aos || !slot) return bfail(SFG_ERR_ARG, "null argument");
     const sfg_numerics_desc& num = numerics ? *numerics : b->num;
     const RecipeParts* rp = nullptr;
@@ -716,9 +877,24 @@ int sfg_batch_add_ex(sfg_batch b, const sfg_grid_desc* grid, const sfg_numerics_
     if (rc) return rc;
     GridView g;
     long long nodes = 0;
+    int off[3];
     const int reach = rp->scheme == WENO3 ? 2 : (rp->scheme == WENO7 ? 4 : 3);
-    rc = batch_grid_view(grid, &num, reach, &g, &nodes);
+    rc = batch_grid_view(grid, &num, reach, &g, &nodes, off);
     if (rc) return rc;
+    // law ends: every one needs its laws
+    const long long pts = law_points(*grid, g);
+    LawView lv{};
+    std::vector<unsigned char> codes;
+    if (pts > 0) {
+        if (!laws) return bfail(SFG_ERR_ARG, "a grid with SFG_BC_LAW ends needs its laws (sfg_batch_add_laws)");
+        for (int a = 0; a < grid->dim; ++a)
+            for (int end = 0; end < 2; ++end)
+                if ((end ? grid->bc_hi[a] : grid->bc_lo[a]) == SFG_BC_LAW)
+                    if (const char* why = law_problem(laws[2 * a + end]))
+                        return bfail(SFG_ERR_ARG, "axis %d end %d: %s", a, end, why);
+        grid_law_view(*grid, g, off, laws, reach, lv, codes);
+    }
+    const bool extra = has_extra_nodes(g, *grid);
     int group = 0;
     rc = group_of(b, rp, &group);
     if (rc) return rc;
@@ -735,11 +911,15 @@ int sfg_batch_add_ex(sfg_batch b, const sfg_grid_desc* grid, const sfg_numerics_
         b->inst_offset.push_back(0);
         b->inst_bytes.push_back(0);
         b->inst_group.push_back(0);
+        b->inst_pub.push_back(sfg_grid_desc{});
+        b->inst_off.push_back({0, 0, 0});
+        b->inst_law.push_back(LawView{});
     }
-    const size_t per = (sizeof(double) * 5 * (size_t)g.vs + 255) / 256 * 256;
+    const size_t per = align256(sizeof(double) * 5 * (size_t)g.vs);
     const int bufs = b->num.time_recipe == T_RK4 ? 4 : 3;
-    size_t off = 0;
-    rc = slab_alloc(b, per * bufs, &off);
+    const size_t slab_bytes = instance_slab_bytes(b, *grid, g);
+    size_t soff = 0;
+    rc = slab_alloc(b, slab_bytes, &soff);
     if (rc) return rc;
     const size_t aos_bytes = sizeof(double) * 5 * (size_t)nodes;
     if (aos_bytes > b->staging_cap) {
@@ -747,17 +927,33 @@ int sfg_batch_add_ex(sfg_batch b, const sfg_grid_desc* grid, const sfg_numerics_
         b->staging = nullptr;
         b->staging_cap = 0;
         if (cudaMalloc((void**)&b->staging, aos_bytes) != cudaSuccess) {
-            slab_free(b, off, per * bufs);
+            slab_free(b, soff, slab_bytes);
             return bfail(SFG_ERR_NOMEM, "staging allocation failed");
         }
         b->staging_cap = aos_bytes;
     }
     BatchInst r{};
     r.g = g;
-    r.qn = reinterpret_cast<double*>(b->slab + off);
-    r.qa = reinterpret_cast<double*>(b->slab + off + per);
-    r.qb = reinterpret_cast<double*>(b->slab + off + 2 * per);
-    r.k = bufs == 4 ? reinterpret_cast<double*>(b->slab + off + 3 * per) : nullptr;
+    r.qn = reinterpret_cast<double*>(b->slab + soff);
+    r.qa = reinterpret_cast<double*>(b->slab + soff + per);
+    r.qb = reinterpret_cast<double*>(b->slab + soff + 2 * per);
+    r.k = bufs == 4 ? reinterpret_cast<double*>(b->slab + soff + 3 * per) : nullptr;
+    r.law = nullptr;
+    if (pts > 0) {  // the law view and its codes after the state buffers
+        char* lbase = b->slab + soff + per * bufs;
+        unsigned char* dcodes = reinterpret_cast<unsigned char*>(lbase + align256(sizeof(LawView)));
+        lv.codes = dcodes;
+        BCUDA(cudaMemcpyAsync(dcodes, codes.data(), codes.size(), cudaMemcpyHostToDevice, b->stream));
+        BCUDA(cudaMemcpyAsync(lbase, &lv, sizeof lv, cudaMemcpyHostToDevice, b->stream));
+        r.law = reinterpret_cast<const LawView*>(lbase);
+        if (!b->has_laws) {  // the step graph gets its law launches
+            b->has_laws = true;
+            if (b->graph) {
+                cudaGraphExecDestroy(b->graph);
+                b->graph = nullptr;
+            }
+        }
+    }
     std::memset(&r.clock, 0, sizeof r.clock);
     r.clock.t = 0.0;
     r.clock.t_end = t_end;
@@ -769,14 +965,27 @@ int sfg_batch_add_ex(sfg_batch b, const sfg_grid_desc* grid, const sfg_numerics_
     r.clock.active = 0;
     r.flags = 0;
     r.live = 1;
-    BCUDA(cudaMemcpyAsync(b->staging, host_nodes_aos, aos_bytes, cudaMemcpyHostToDevice, b->stream));
+    std::vector<double> dev_layout;
+    if (extra) to_device_layout(*grid, g, off, host_nodes_aos, dev_layout);
+    BCUDA(cudaMemcpyAsync(b->staging, extra ? dev_layout.data() : host_nodes_aos, aos_bytes, cudaMemcpyHostToDevice,
+                          b->stream));
     if (launch_aos_to_soa(b->staging, r.qn, nodes, g.vs, b->stream) != cudaSuccess)
         return bfail(SFG_ERR_CUDA, "upload transpose failed");
+    if (extra) {
+        // stage kernels write solved nodes only, and stage outputs are read as
+        // the next state: every stage buffer holds the ghost value in its extra
+        // nodes, as on a single grid
+        BCUDA(cudaMemcpyAsync(r.qa, r.qn, per, cudaMemcpyDeviceToDevice, b->stream));
+        BCUDA(cudaMemcpyAsync(r.qb, r.qn, per, cudaMemcpyDeviceToDevice, b->stream));
+    }
     BCUDA(cudaMemcpyAsync(b->d_inst + idx, &r, sizeof r, cudaMemcpyHostToDevice, b->stream));
     b->h_inst[idx] = r;
-    b->inst_offset[idx] = off;
-    b->inst_bytes[idx] = per * bufs;
+    b->inst_offset[idx] = soff;
+    b->inst_bytes[idx] = slab_bytes;
     b->inst_group[idx] = group;
+    b->inst_pub[idx] = *grid;
+    b->inst_off[idx] = {off[0], off[1], off[2]};
+    b->inst_law[idx] = lv;
     rc = publish_items(b);  // synchronises the stream
     if (rc) return rc;
     *slot = idx;
@@ -878,8 +1087,16 @@ int sfg_batch_download(sfg_batch b, int slot, double* host_nodes_aos) {
     const size_t bytes = sizeof(double) * 5 * (size_t)nodes;
     if (launch_soa_to_aos(r.g, r.qn, b->staging, b->stream) != cudaSuccess)
         return bfail(SFG_ERR_CUDA, "download transpose failed");
-    BCUDA(cudaMemcpyAsync(host_nodes_aos, b->staging, bytes, cudaMemcpyDeviceToHost, b->stream));
+    const sfg_grid_desc& pub = b->inst_pub[slot];
+    if (!has_extra_nodes(r.g, pub)) {
+        BCUDA(cudaMemcpyAsync(host_nodes_aos, b->staging, bytes, cudaMemcpyDeviceToHost, b->stream));
+        BCUDA(cudaStreamSynchronize(b->stream));
+        return SFG_OK;
+    }
+    std::vector<double> dev((size_t)nodes * 5);
+    BCUDA(cudaMemcpyAsync(dev.data(), b->staging, bytes, cudaMemcpyDeviceToHost, b->stream));
     BCUDA(cudaStreamSynchronize(b->stream));
+    to_caller_layout(pub, r.g, b->inst_off[slot].data(), dev.data(), host_nodes_aos);
     return SFG_OK;
 }
 

@@ -5,6 +5,9 @@
 #include <stdint.h>
 
 #include <atomic>
+#include <vector>
+
+#include "../../include/sonicsolver_b200.h"
 
 namespace sfg {
 
@@ -124,6 +127,13 @@ struct ClusterRun {
     unsigned* flags;
     long long launch_steps;  // steps per launch at most (the host relaunches)
 };
+
+// Host helpers of the boundary laws (sfg_runtime.cu): the checks of one
+// end's laws (nullptr: valid), and the law view plus the reference
+// state-cache replay codes of a grid that is not a solver of its own.
+const char* law_problem(const sfg_boundary_law& law);
+void grid_law_view(const sfg_grid_desc& G, const GridView& gv, const int off_lo[3], const sfg_boundary_law* laws,
+                   int ng, LawView& lv, std::vector<unsigned char>& codes);
 
 // One-time kernel attribute setup per device: kernel attributes belong to a
 // device context, so each launcher keeps its own set of devices done (one bit

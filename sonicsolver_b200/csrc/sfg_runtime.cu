@@ -206,10 +206,8 @@ int validate(const sfg_grid_desc* g, const sfg_numerics_desc* n, const RecipeInf
 // pressure laws, face points with the last axis outermost, corners included
 // (SF_fixedValue.cpp:129-160, SF_thermodynamicClosure.cpp:219-285) -- and
 // records LAW_STATE_* for each face point the kernel updates.
-void simulate_law_cache(const sfg_solver_s* s, std::vector<unsigned char>& codes) {
-    const LawView& lv = s->lv;
-    const sfg_grid_desc& G = s->grid;
-    const int ng = s->ng;
+void simulate_law_cache(const LawView& lv, const sfg_grid_desc& G, const GridView& gv, const int off_lo[3], int ng,
+                        std::vector<unsigned char>& codes) {
     const long long mx = G.n[0] + 2LL * ng, my = G.n[1] + 2LL * ng, mz = G.n[2] + 2LL * ng;
     const long long cap = std::min<long long>(mx * my * mz, 4096);
     std::vector<long long> slot_cell((size_t)cap, -1);
@@ -227,8 +225,8 @@ void simulate_law_cache(const sfg_solver_s* s, std::vector<unsigned char>& codes
     };
     int pub_lo[3], pub_hi[3];
     for (int d = 0; d < 3; ++d) {
-        pub_lo[d] = s->gv.lo[d] - s->off_lo[d];
-        pub_hi[d] = s->gv.hi[d] - s->off_lo[d];
+        pub_lo[d] = gv.lo[d] - off_lo[d];
+        pub_hi[d] = gv.hi[d] - off_lo[d];
     }
     // Boundary nodes whose energy this application has not written yet: an
     // edge point's inner sample can be another end's boundary node, and the
@@ -283,17 +281,16 @@ void simulate_law_cache(const sfg_solver_s* s, std::vector<unsigned char>& codes
         }
 }
 
-// Law ends in the order x low, x high, y low, ...; face points over the
-// solved range of the other axes.
-void build_law_view(sfg_solver_s* s) {
-    LawView& lv = s->lv;
+// Law ends of a grid (`G`, caller layout; `g`, its device view) in the order
+// x low, x high, y low, ...; face points over the solved range of the other
+// axes; laws[2 axis + end] holds each end's laws.
+void make_law_view(const sfg_grid_desc& G, const GridView& g, const sfg_boundary_law* laws, LawView& lv) {
     lv = LawView{};
-    const GridView& g = s->gv;
-    for (int a = 0; a < s->grid.dim; ++a)
+    for (int a = 0; a < G.dim; ++a)
         for (int end = 0; end < 2; ++end) {
-            if ((end ? s->grid.bc_hi[a] : s->grid.bc_lo[a]) != SFG_BC_LAW) continue;
+            if ((end ? G.bc_hi[a] : G.bc_lo[a]) != SFG_BC_LAW) continue;
             const int e = lv.count++;
-            const sfg_boundary_law& law = s->laws[2 * a + end];
+            const sfg_boundary_law& law = laws[2 * a + end];
             lv.axis[e] = a;
             lv.end[e] = end;
             lv.rho[e] = law.rho;
@@ -307,7 +304,11 @@ void build_law_view(sfg_solver_s* s) {
                 if (d != a) pts *= g.hi[d] - g.lo[d];
             lv.start[e + 1] = lv.start[e] + pts;
         }
-    lv.codes = s->law_codes;
+}
+
+void build_law_view(sfg_solver_s* s) {
+    make_law_view(s->grid, s->gv, s->laws, s->lv);
+    s->lv.codes = s->law_codes;
 }
 
 // Device copy of the cache replay for the current laws (the number of face
@@ -315,7 +316,7 @@ void build_law_view(sfg_solver_s* s) {
 int upload_law_codes(sfg_solver_s* s) {
     if (!s->lv.count) return SFG_OK;
     std::vector<unsigned char> codes;
-    simulate_law_cache(s, codes);
+    simulate_law_cache(s->lv, s->grid, s->gv, s->off_lo, s->ng, codes);
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     if (!s->law_codes && cudaMalloc((void**)&s->law_codes, codes.size()) != cudaSuccess) {
         s->law_codes = nullptr;
@@ -614,6 +615,33 @@ void nodes_from_device_layout(const sfg_solver_s* s, const double* dev, double* 
 
 }  // namespace
 
+namespace sfg {
+
+// What is wrong with a law, or nullptr (the checks of sfg_set_boundary_law).
+const char* law_problem(const sfg_boundary_law& law) {
+    for (int k : {law.rho, law.velocity, law.pressure})
+        if (k != SFG_LAW_ZERO_GRADIENT && k != SFG_LAW_FIXED_VALUE && k != SFG_LAW_SYMMETRY)
+            return "unknown field law";
+    auto finite = [](double v) { return std::isfinite(v); };
+    if (!finite(law.rho_value) || !finite(law.pressure_value) || !finite(law.velocity_value[0]) ||
+        !finite(law.velocity_value[1]) || !finite(law.velocity_value[2]))
+        return "law values must be finite";
+    if (law.rho == SFG_LAW_FIXED_VALUE && !(law.rho_value > 0.0)) return "fixedValue density must be > 0";
+    if (law.pressure == SFG_LAW_FIXED_VALUE && !(law.pressure_value > 0.0)) return "fixedValue pressure must be > 0";
+    return nullptr;
+}
+
+// The law view and the state-cache replay of a grid that is not a solver of
+// its own (a batched grid): `G` in the caller's layout, `gv` its device view
+// with the extra end nodes (offset off_lo), ng the Field's ghost layers.
+void grid_law_view(const sfg_grid_desc& G, const GridView& gv, const int off_lo[3], const sfg_boundary_law* laws,
+                   int ng, LawView& lv, std::vector<unsigned char>& codes) {
+    make_law_view(G, gv, laws, lv);
+    simulate_law_cache(lv, G, gv, off_lo, ng, codes);
+}
+
+}  // namespace sfg
+
 extern "C" {
 
 const char* sfg_last_error(void) { return g_error.c_str(); }
@@ -722,17 +750,7 @@ int sfg_set_boundary_law(sfg_solver s, int axis, int end, const sfg_boundary_law
     if (axis < 0 || axis >= s->grid.dim || end < 0 || end > 1) return fail(SFG_ERR_ARG, "bad axis %d / end %d", axis, end);
     if ((end ? s->grid.bc_hi[axis] : s->grid.bc_lo[axis]) != SFG_BC_LAW)
         return fail(SFG_ERR_ARG, "axis %d end %d is not a SFG_BC_LAW end", axis, end);
-    for (int k : {law->rho, law->velocity, law->pressure})
-        if (k != SFG_LAW_ZERO_GRADIENT && k != SFG_LAW_FIXED_VALUE && k != SFG_LAW_SYMMETRY)
-            return fail(SFG_ERR_ARG, "unknown field law %d", k);
-    auto finite = [](double v) { return std::isfinite(v); };
-    if (!finite(law->rho_value) || !finite(law->pressure_value) || !finite(law->velocity_value[0]) ||
-        !finite(law->velocity_value[1]) || !finite(law->velocity_value[2]))
-        return fail(SFG_ERR_ARG, "law values must be finite");
-    if (law->rho == SFG_LAW_FIXED_VALUE && !(law->rho_value > 0.0))
-        return fail(SFG_ERR_ARG, "fixedValue density must be > 0");
-    if (law->pressure == SFG_LAW_FIXED_VALUE && !(law->pressure_value > 0.0))
-        return fail(SFG_ERR_ARG, "fixedValue pressure must be > 0");
+    if (const char* why = sfg::law_problem(*law)) return fail(SFG_ERR_ARG, "%s", why);
     s->laws[2 * axis + end] = *law;
     build_law_view(s);
     if (s->graph) {  // the captured launches hold the previous laws
@@ -887,6 +905,15 @@ int sfg_upload(sfg_solver s, const double* host, int layout, double time) {
         return fail(SFG_ERR_ARG, "unknown layout %d", layout);
     }
     return reset_time(s, time);
+}
+
+int sfg_restore(sfg_solver s, const double* host, int layout, double time, int64_t steps) {
+    if (!s || !host) return fail(SFG_ERR_ARG, "null argument");
+    if (!std::isfinite(time)) return fail(SFG_ERR_ARG, "time must be finite");
+    if (steps < 0) return fail(SFG_ERR_ARG, "steps must be >= 0");
+    if (int rc = sfg_upload(s, host, layout, time)) return rc;
+    s->host_clock->steps = steps;
+    return push_clock(s);
 }
 
 int sfg_upload_device(sfg_solver s, const double* dev_nodes_aos, double time) {

@@ -27,6 +27,7 @@
 namespace sfg {
 void set_last_error(const char* msg);
 int batch_check_numerics(sfg_batch b, const sfg_numerics_desc* n);
+const char* law_problem(const sfg_boundary_law& law);
 }
 
 namespace {
@@ -46,6 +47,8 @@ struct Request {
     sfg_grid_desc grid{};
     sfg_numerics_desc num{};  // the request's own numerics (has_num)
     bool has_num = false;
+    sfg_boundary_law laws[6] = {};  // [2 axis + end] of its SFG_BC_LAW ends (has_laws)
+    bool has_laws = false;
     std::vector<double> input, output;
     double t_end = 0.0;
     int64_t max_steps = 0;
@@ -132,8 +135,9 @@ void worker_loop(sfg_server_s* s) {
         }
         for (Request* r : admit) {
             int slot = -1;
-            int rc = sfg_batch_add_ex(s->batch, &r->grid, r->has_num ? &r->num : nullptr, r->input.data(), r->t_end,
-                                      r->max_steps, &slot);
+            int rc = sfg_batch_add_laws(s->batch, &r->grid, r->has_num ? &r->num : nullptr,
+                                        r->has_laws ? r->laws : nullptr, r->input.data(), r->t_end, r->max_steps,
+                                        &slot);
             std::lock_guard<std::mutex> lock(s->mu);
             if (rc == SFG_ERR_BUDGET) {  // fragmentation: retry at the queue head
                 s->queue.push_front(r->id);
@@ -244,11 +248,26 @@ int sfg_server_submit(sfg_server s, const sfg_grid_desc* grid, const double* hos
 
 int sfg_server_submit_ex(sfg_server s, const sfg_grid_desc* grid, const sfg_numerics_desc* numerics,
                          const double* host_nodes_aos, double t_end, int64_t max_steps, int64_t* request_id) {
+    return sfg_server_submit_laws(s, grid, numerics, nullptr, host_nodes_aos, t_end, max_steps, request_id);
+}
+
+int sfg_server_submit_laws(sfg_server s, const sfg_grid_desc* grid, const sfg_numerics_desc* numerics,
+                           const sfg_boundary_law* laws, const double* host_nodes_aos, double t_end,
+                           int64_t max_steps, int64_t* request_id) {
     if (!s || !grid || !host_nodes_aos || !request_id) return sfail(SFG_ERR_ARG, "null argument");
     if (numerics) {
         int rc = sfg::batch_check_numerics(s->batch, numerics);  // no device work
         if (rc) return rc;
     }
+    bool law_ends = false;
+    for (int a = 0; a < grid->dim && a < 3; ++a)
+        for (int end = 0; end < 2; ++end)
+            if ((end ? grid->bc_hi[a] : grid->bc_lo[a]) == SFG_BC_LAW) {
+                law_ends = true;
+                if (!laws) return sfail(SFG_ERR_ARG, "a grid with SFG_BC_LAW ends needs its laws");
+                if (const char* why = sfg::law_problem(laws[2 * a + end]))
+                    return sfail(SFG_ERR_ARG, "axis %d end %d: %s", a, end, why);
+            }
     size_t bytes = 0;
     int rc = sfg_batch_instance_bytes(s->batch, grid, &bytes);  // validates the grid; no device work
     if (rc) return rc;
@@ -262,6 +281,10 @@ int sfg_server_submit_ex(sfg_server s, const sfg_grid_desc* grid, const sfg_nume
     if (numerics) {
         r.num = *numerics;
         r.has_num = true;
+    }
+    if (law_ends) {
+        for (int k = 0; k < 2 * grid->dim && k < 6; ++k) r.laws[k] = laws[k];
+        r.has_laws = true;
     }
     r.input.assign(host_nodes_aos, host_nodes_aos + count);
     r.t_end = t_end;

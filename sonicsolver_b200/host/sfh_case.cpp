@@ -234,6 +234,24 @@ CaseSpec load_case(const std::string& dir) {
         if (!vb) continue;
         for (const auto& kv : vb->fields) {
             c.patch_bc[kv.first][var] = condition(kv.second, std::string(var) + "." + kv.first);
+            c.bc_order[var].push_back(kv.first);
+        }
+    }
+    // field declarations of the registry (its "fields" registry entries,
+    // src/infrastructure/io/case/SF_case.cpp:115-150): output switch and name
+    const std::string reg = join(dir, "fields/fields.yaml");
+    if (exists(reg)) {
+        const Node r = load_yaml_file(reg);
+        for (const auto& kv : r.fields) {
+            const std::string& k = kv.first;
+            if (k == "SonicFile" || k == "default" || k == "internalField" || k == "boundaries") continue;
+            CaseSpec::DeclaredField f;
+            f.name = f.output_name = k;
+            if (kv.second.is_map()) {
+                if (const Node* o = kv.second.get("output")) f.output = o->boolean();
+                if (const Node* on = kv.second.get("outputName")) f.output_name = on->str();
+            }
+            c.declared_fields.push_back(f);
         }
     }
     return c;

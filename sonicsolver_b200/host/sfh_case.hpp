@@ -67,6 +67,15 @@ struct CaseSpec {
     std::string write_control = "runTime", output_dir = "result", job_name;
     // patch -> field ("rho", "U", "p") -> condition
     std::map<std::string, std::map<std::string, FieldCondition>> patch_bc;
+    // field ("rho", "U", "p") -> its patches in file order (the order the
+    // reference's writer numbers boundary sets in)
+    std::map<std::string, std::vector<std::string>> bc_order;
+    // fields declared in the fields registry (fields/fields.yaml), file order
+    struct DeclaredField {
+        std::string name, output_name;
+        bool output = true;
+    };
+    std::vector<DeclaredField> declared_fields;
     InitialValue rho, U, p;
 };
 

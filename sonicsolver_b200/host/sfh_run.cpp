@@ -10,7 +10,8 @@
 //
 //   sfg_run CASE_DIR [--mode graph|plan] [--precision fp64|fp32flux]
 //                    [--graph-steps K] [--dump FILE] [--dump-points FILE]
-//                    [--dump-metrics FILE] [--no-write] [--describe]
+//                    [--dump-metrics FILE] [--checkpoint PREFIX] [--restart FILE]
+//                    [--no-write] [--describe]
 //
 // --mode plan executes the plan operation by operation (one C-ABI call per
 // operation, host synchronous).  --mode graph (default) lowers the time loop
@@ -22,18 +23,26 @@
 // per node, x fastest) and --dump-metrics the metrics handed to the provider
 // (10 per point of the Field layout: the recipe's ghost layers on every
 // axis), both as raw float64, also under --describe.
+// --checkpoint PREFIX writes a restart file PREFIX_NNNN.json at every output
+// time (NNNN: the output's number, as in the .vts names) and at the end of
+// the run (sfh_checkpoint.hpp); --restart FILE starts from such a file: its
+// state, time, step count and output clock replace the case's initial state
+// and start time, and the run continues with the bits of the run that wrote
+// it (sfg_restore).
 // Exit codes: 0 done, 1 error, 2 usage, 3 case not supported by the provider.
 #include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <limits>
 #include <string>
 #include <sys/stat.h>
 #include <vector>
 
 #include "../../include/sonicsolver_b200.h"
 #include "sfh_case.hpp"
+#include "sfh_checkpoint.hpp"
 #include "sfh_catalog.hpp"
 #include "sfh_plan.hpp"
 #include "sfh_vts.hpp"
@@ -44,7 +53,7 @@ namespace {
 using namespace sfh;
 
 struct Options {
-    std::string dir, mode = "graph", dump, dump_points, dump_metrics;
+    std::string dir, mode = "graph", dump, dump_points, dump_metrics, checkpoint, restart;
     int precision = SFG_PREC_FP64;
     int graph_steps = 32;
     bool write = true, describe_only = false;
@@ -53,7 +62,8 @@ struct Options {
 int usage() {
     std::fprintf(stderr,
                  "usage: sfg_run CASE_DIR [--mode graph|plan] [--precision fp64|fp32flux] [--graph-steps K]\n"
-                 "               [--dump FILE] [--dump-points FILE] [--dump-metrics FILE] [--no-write] [--describe]\n");
+                 "               [--dump FILE] [--dump-points FILE] [--dump-metrics FILE] [--checkpoint PREFIX]\n"
+                 "               [--restart FILE] [--no-write] [--describe]\n");
     return 2;
 }
 
@@ -83,7 +93,9 @@ struct Run {
     int outputs = 0;
     std::string out_dir;
     std::vector<double> host;
-    std::vector<double> points;  // node coordinates of a graded or curved block (else empty)
+    VtsLayout vts;               // the .vts output layout of the case
+    std::string checkpoint;      // restart-file prefix (empty: none)
+    const Checkpoint* restart = nullptr;  // the restart file this run starts from
 };
 
 // Ghost layers of the provider's Field layout for a recipe (WENO3: 2,
@@ -100,7 +112,8 @@ int recipe_ghosts(const std::string& convection) {
 // reference Field (the case's nGhost layers) at the same node offsets.  On
 // an inactive axis the provider's one node plane is the block's first.
 void block_geometry(const CaseSpec& c, const GridSetup& g, int ng_s, std::vector<double>& points,
-                    std::vector<double>& metrics, double* residual, double* tolerance) {
+                    std::vector<double>& all_points, std::vector<double>& metrics, double* residual,
+                    double* tolerance) {
     bool active[3];
     for (int d = 0; d < 3; ++d) active[d] = d < g.grid.dim;
     const int ng_c = c.ghost_layers;
@@ -122,6 +135,18 @@ void block_geometry(const CaseSpec& c, const GridSetup& g, int ng_s, std::vector
             for (int i = 0; i < n[0]; ++i) {
                 const long long t = F.at(i + ng_c, j + ng_c, k + ng_c);
                 double* p = &points[(((size_t)k * n[1] + j) * n[0] + i) * 3];
+                p[0] = F.x[t];
+                p[1] = F.y[t];
+                p[2] = F.z[t];
+            }
+    // every node of the block (the written output covers unsolved axes too)
+    const int nb[3] = {c.mesh.cells[0] + 1, c.mesh.cells[1] + 1, c.mesh.cells[2] + 1};
+    all_points.resize(size_t(nb[0]) * nb[1] * nb[2] * 3);
+    for (int k = 0; k < nb[2]; ++k)
+        for (int j = 0; j < nb[1]; ++j)
+            for (int i = 0; i < nb[0]; ++i) {
+                const long long t = F.at(i + ng_c, j + ng_c, k + ng_c);
+                double* p = &all_points[(((size_t)k * nb[1] + j) * nb[0] + i) * 3];
                 p[0] = F.x[t];
                 p[1] = F.y[t];
                 p[2] = F.z[t];
@@ -148,23 +173,45 @@ bool at_or_past(double t, double mark) {
     return t >= mark - 1e-11 * sc;
 }
 
+// A restart file of the current state (the host copy is current).
+int write_restart(Run& r, const std::string& path) {
+    Checkpoint c;
+    for (int d = 0; d < 3; ++d) c.nodes[d] = r.g->nodes[d];
+    if (int rc = sfg_time(r.s, &c.time, &c.steps)) return rc;
+    c.next_output = r.c->write_interval > 0.0 ? r.next_out : std::numeric_limits<double>::infinity();
+    c.outputs = r.outputs;
+    c.q = r.host;
+    if (!write_checkpoint(path, c)) {
+        std::fprintf(stderr, "sfg_run: cannot write the restart file %s\n", path.c_str());
+        return SFG_ERR_ARG;
+    }
+    std::printf("checkpoint t=%.17g %s\n", c.time, path.c_str());
+    return 0;
+}
+
+std::string restart_name(const Run& r, int number) {
+    char name[32];
+    std::snprintf(name, sizeof name, "_%04d.json", number);
+    return r.checkpoint + name;
+}
+
 int write_output(Run& r, double t) {
-    if (!r.write) return 0;
+    if (!r.write && r.checkpoint.empty()) return 0;
     if (int rc = sfg_download(r.s, r.host.data(), SFG_LAYOUT_NODES)) return rc;
+    if (!r.write) {
+        ++r.outputs;
+        return write_restart(r, restart_name(r, r.outputs - 1));
+    }
     char name[64];
     std::snprintf(name, sizeof name, "_%04d.vts", r.outputs);
     const std::string path = r.out_dir + "/" + r.c->job_name + name;
-    VtsGeometry geo{{r.g->nodes[0], r.g->nodes[1], r.g->nodes[2]},
-                    {r.g->origin[0], r.g->origin[1], r.g->origin[2]},
-                    {r.g->grid.h[0], r.g->grid.h[1], r.g->grid.h[2]},
-                    r.points.empty() ? nullptr : &r.points};
-    if (!write_vts(path, geo, r.host, r.c->gamma, t)) {
+    if (!write_vts(path, r.vts, r.host, r.c->gamma)) {
         std::fprintf(stderr, "sfg_run: cannot write %s\n", path.c_str());
         return SFG_ERR_ARG;
     }
     std::printf("write t=%.17g %s\n", t, path.c_str());
     ++r.outputs;
-    return 0;
+    return r.checkpoint.empty() ? 0 : write_restart(r, restart_name(r, r.outputs - 1));
 }
 
 // Clock end / output clipping of Time::Driver (the rule the device clock
@@ -184,6 +231,11 @@ bool remaining_limit(const Run& r, double t, double& limit) {
 
 // Output schedule and the initial write, before the time loop.
 int start_output(Run& r, double t) {
+    if (r.restart) {  // the output clock of the run that wrote the restart file
+        r.next_out = r.c->write_interval > 0.0 ? r.restart->next_output : 0.0;
+        r.outputs = r.restart->outputs;
+        return 0;
+    }
     r.next_out = r.c->write_interval > 0.0 ? t + r.c->write_interval : 0.0;
     return r.c->write_initial ? write_output(r, t) : 0;
 }
@@ -350,6 +402,8 @@ int main(int argc, char** argv) {
         else if (a == "--dump") o.dump = next();
         else if (a == "--dump-points") o.dump_points = next();
         else if (a == "--dump-metrics") o.dump_metrics = next();
+        else if (a == "--checkpoint") o.checkpoint = next();
+        else if (a == "--restart") o.restart = next();
         else if (a == "--no-write") o.write = false;
         else if (a == "--describe") o.describe_only = true;
         else if (!a.empty() && a[0] == '-') return usage();
@@ -394,10 +448,10 @@ int main(int argc, char** argv) {
                             L.velocity_value[1], L.velocity_value[2], law_name(L.pressure), L.pressure_value);
             }
         // a graded or curved block: the generator's node coordinates and metrics
-        std::vector<double> points, metrics;
+        std::vector<double> points, all_points, metrics;
         if (c.curvilinear) {
             double res = 0, tol = 0;
-            block_geometry(c, g, recipe_ghosts(c.convection), points, metrics, &res, &tol);
+            block_geometry(c, g, recipe_ghosts(c.convection), points, all_points, metrics, &res, &tol);
             std::printf("mesh curvilinear (%s): metric identity residual %.3g, tolerance %.3g\n",
                         c.mesh.edges.empty() ? "trilinear, graded" : "transfinite, arc edges", res, tol);
             if (!o.dump_points.empty()) write_doubles(o.dump_points, points);
@@ -418,7 +472,7 @@ int main(int argc, char** argv) {
         r.g = &g;
         r.write = o.write;
         r.host.resize(g.q.size());
-        r.points = points;
+        r.vts = vts_layout(c, g, all_points);
         r.out_dir = c.dir + "/" + c.output_dir;
         if (o.write) mkdir(r.out_dir.c_str(), 0755);
         if (sfg_create(&g.grid, &nd, nullptr, &r.s) != SFG_OK) {
@@ -438,9 +492,33 @@ int main(int argc, char** argv) {
             sfg_destroy(r.s);
             return 1;
         }
-        int rc = sfg_upload(r.s, g.q.data(), SFG_LAYOUT_NODES, c.start_time);
+        r.checkpoint = o.checkpoint;
+        Checkpoint restart;
         StepContext ctx;
         ctx.t = c.start_time;
+        int rc = 0;
+        if (!o.restart.empty()) {
+            // a restart file replaces the initial state and the start time
+            // (the case's ghost layers of unconditioned ends are re-made from
+            // the restart state, as the reference's restart does)
+            restart = read_checkpoint(o.restart);
+            for (int d = 0; d < 3; ++d)
+                if (restart.nodes[d] != g.nodes[d]) {
+                    std::fprintf(stderr, "sfg_run: %s holds %d x %d x %d nodes, the case %d x %d x %d\n",
+                                 o.restart.c_str(), restart.nodes[0], restart.nodes[1], restart.nodes[2], g.nodes[0],
+                                 g.nodes[1], g.nodes[2]);
+                    sfg_destroy(r.s);
+                    return 1;
+                }
+            r.restart = &restart;
+            rc = sfg_restore(r.s, restart.q.data(), SFG_LAYOUT_NODES, restart.time, restart.steps);
+            ctx.t = restart.time;
+            ctx.steps = restart.steps;
+            std::printf("restart t=%.17g steps=%lld from %s\n", restart.time, (long long)restart.steps,
+                        o.restart.c_str());
+        } else {
+            rc = sfg_upload(r.s, g.q.data(), SFG_LAYOUT_NODES, c.start_time);
+        }
         const auto w0 = std::chrono::steady_clock::now();
         if (!rc) {
             if (o.mode == "plan") {
@@ -457,6 +535,10 @@ int main(int argc, char** argv) {
         double totals[5] = {0, 0, 0, 0, 0};
         if (!rc) rc = sfg_status_word(r.s, &bits, 0);
         if (!rc) rc = sfg_conserved_totals(r.s, totals);
+        if (!rc && !o.checkpoint.empty()) {
+            rc = sfg_download(r.s, r.host.data(), SFG_LAYOUT_NODES);
+            if (!rc) rc = write_restart(r, o.checkpoint + "_end.json");
+        }
         if (!rc && !o.dump.empty()) {
             rc = sfg_download(r.s, r.host.data(), SFG_LAYOUT_NODES);
             std::ofstream f(o.dump, std::ios::binary);

@@ -26,6 +26,23 @@ def rel_linf(a: np.ndarray, b: np.ndarray) -> np.ndarray:
     return np.abs(a - b).max(axis=0) / scale
 
 
+def state_scale(q):
+    """Per conserved variable max |q|, one scale for the momentum vector (the
+    largest |component| over the three)."""
+    scale = np.abs(np.asarray(q).reshape(-1, 5)).max(axis=0)
+    scale[1:4] = scale[1:4].max()
+    return np.where(scale > 0, scale, 1.0)
+
+
+def rel_linf_vec(a, b):
+    """Relative L-infinity per conserved variable, the momentum components
+    measured against one scale (a component that is zero up to round-off,
+    such as rho v of a flow along x, is not compared with its own noise)."""
+    a = np.asarray(a).reshape(-1, 5)
+    b = np.asarray(b).reshape(-1, 5)
+    return np.abs(a - b).max(axis=0) / state_scale(b)
+
+
 @pytest.fixture(scope="session")
 def oracle():
     import pyoracle

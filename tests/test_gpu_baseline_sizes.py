@@ -42,6 +42,8 @@ import numpy as np
 import pytest
 
 import baseline_jobs as jobs
+from conftest import rel_linf_vec as rel_linf
+from conftest import state_scale
 from sonicsolver_b200 import capi, cases
 
 pytestmark = pytest.mark.gpu
@@ -68,21 +70,6 @@ def oracle_runs():
 
 def _result(runs, key):
     return runs["futures"][key].result(timeout=900)
-
-
-def state_scale(q):
-    """Per conserved variable max |q|, one scale for the momentum vector (the
-    largest |component| over the three)."""
-    scale = np.abs(np.asarray(q).reshape(-1, 5)).max(axis=0)
-    scale[1:4] = scale[1:4].max()
-    return np.where(scale > 0, scale, 1.0)
-
-
-def rel_linf(a, b):
-    """Relative L-infinity per conserved variable (momentum: one scale)."""
-    a = np.asarray(a).reshape(-1, 5)
-    b = np.asarray(b).reshape(-1, 5)
-    return np.abs(a - b).max(axis=0) / state_scale(b)
 
 
 # ----------------------------------------------------------------- c2: vortex 1024^2

@@ -291,3 +291,99 @@ def test_near_vacuum_request_stops_in_the_mix_where_the_oracle_stops():
         assert b.status(slot)["steps"] == steps
         assert rel_linf(b.download(slot), want).max() <= TOL
 
+
+
+# ---- frozen and law ends in batches and the server
+
+INFLOW = dict(rho=capi.LAW_FIXED_VALUE, velocity=capi.LAW_FIXED_VALUE, pressure=capi.LAW_FIXED_VALUE, rho_value=1.0,
+              velocity_value=(0.3, 0.0, 0.0), pressure_value=1.0)
+WALL = dict(rho=capi.LAW_ZERO_GRADIENT, velocity=capi.LAW_FIXED_VALUE, pressure=capi.LAW_ZERO_GRADIENT)
+SLIP = dict(rho=capi.LAW_ZERO_GRADIENT, velocity=capi.LAW_SYMMETRY, pressure=capi.LAW_SYMMETRY)
+
+
+def boundary_mix(t_end=0.04):
+    """Grids with every end kind a case directory gives: a Sod tube without
+    a Left condition (frozen), a tube with a fixedValue inflow and a noSlip
+    wall, a 2-D box with noSlip and slip walls, and one with a
+    frozen low y end, beside plain transmissive and periodic grids.
+    Returns [(case, laws)]."""
+    sod = cases.sod_1d(cells=600, t_end=t_end)
+    sod.bc_lo = (capi.BC_FROZEN, 0, 0)
+    tube = cases.sod_1d(cells=450, t_end=t_end)
+    tube.bc_lo = tube.bc_hi = (capi.BC_LAW, 0, 0)
+    box = cases.shock_tube_batch(count=8, seed=5, t_end=t_end, max_1d=800, max_2d=70)[-1]
+    assert box.dim == 2
+    walls = cases.Case(box.name + "_walls", 2, box.n, box.h, (capi.BC_LAW, capi.BC_LAW, 0),
+                       (capi.BC_LAW, capi.BC_LAW, 0), box.q.copy(), box.gamma, t_end, box.cfl)
+    frozen_y = cases.Case(box.name + "_frozen", 2, box.n, box.h, (0, capi.BC_FROZEN, 0), (0, 0, 0), box.q.copy(),
+                          box.gamma, t_end, box.cfl)
+    plain = cases.shock_tube_batch(count=3, seed=9, t_end=t_end, max_1d=700, max_2d=72)
+    vortex = cases.isentropic_vortex(40, recipe="weno5Rusanov", cfl=0.5, t_end=0.1)
+    return ([(sod, None), (tube, {(0, 0): INFLOW, (0, 1): WALL}),
+             (walls, {(0, 0): WALL, (0, 1): SLIP, (1, 0): SLIP, (1, 1): WALL}), (frozen_y, None)] +
+            [(c, None) for c in plain] + [(vortex, None)])
+
+
+def solo_laws(case, laws, precision, variant):
+    """The grid alone on the tile kernel of the batch's tile shape, with its
+    laws."""
+    s = capi.Solver(case.dim, case.n, case.h, case.bc_lo, case.bc_hi, recipe="weno5Rusanov", time_recipe="SSPRK3",
+                    precision=precision, cfl=case.cfl)
+    s.variant = variant if case.dim == 2 else 1
+    for (axis, end), kw in (laws or {}).items():
+        s.set_boundary_law(axis, end, **kw)
+    s.upload(np.ascontiguousarray(case.q))
+    st, _ = s.advance(case.t_end)
+    out = s.download().reshape(case.q.shape), st.steps
+    s.close()
+    return out
+
+
+@pytest.mark.parametrize("precision", [capi.PREC_FP64, capi.PREC_FP32_FLUX])
+@pytest.mark.parametrize("variant", [1, 2])
+def test_batch_with_frozen_and_law_ends_equals_solo(precision, variant):
+    """Law and frozen ends run in the batch exactly as on a single grid: the
+    same steps and the same bits (the batch runs the single-grid tile body
+    and law arithmetic on the same device layout)."""
+    grids = boundary_mix()
+    b = capi.Batch(1 << 30, 32, recipe="weno5Rusanov", precision=precision, cfl=0.5)
+    b.variant = variant
+    slots = [b.add(c, laws=laws) for c, laws in grids]
+    b.step(100000, graph_steps=8)
+    for (c, laws), slot in zip(grids, slots):
+        st = b.status(slot)
+        assert not st["running"] and st["flags"] == 0, c.name
+        want, steps = solo_laws(c, laws, precision, variant)
+        assert st["steps"] == steps, c.name
+        got = b.download(slot).reshape(c.q.shape)
+        assert np.array_equal(got, want), (c.name, rel_linf(got, want))
+    b.close()
+
+
+def test_server_with_law_requests_equals_solo():
+    grids = boundary_mix(t_end=0.03)
+    srv = capi.Server(1 << 30, 8, recipe="weno5Rusanov", precision=capi.PREC_FP64, cfl=0.5, graph_steps=4)
+    ids = [srv.submit(c, laws=laws) for c, laws in grids]
+    srv.drain(300)
+    for (c, laws), rid in zip(grids, ids):
+        info = srv.poll(rid)
+        assert info.state == capi.REQ_DONE, c.name
+        want, steps = solo_laws(c, laws, capi.PREC_FP64, 1)
+        assert info.steps == steps and np.array_equal(srv.fetch(rid).reshape(c.q.shape), want), c.name
+    srv.close()
+
+
+def test_law_ends_need_valid_laws():
+    tube = cases.sod_1d(cells=100, t_end=0.01)
+    tube.bc_lo = tube.bc_hi = (capi.BC_LAW, 0, 0)
+    b = capi.Batch(1 << 28, 4, recipe="weno5Rusanov", cfl=0.5)
+    with pytest.raises(capi.SolverError, match="needs its laws"):
+        b.add(tube)
+    bad = dict(INFLOW, rho_value=-1.0)
+    with pytest.raises(capi.SolverError, match="density must be > 0"):
+        b.add(tube, laws={(0, 0): bad, (0, 1): WALL})
+    srv = capi.Server(1 << 28, 4, recipe="weno5Rusanov", cfl=0.5)
+    with pytest.raises(capi.SolverError, match="needs its laws"):
+        srv.submit(tube)
+    srv.close()
+    b.close()

@@ -19,7 +19,7 @@ import pytest
 
 import pyoracle as po
 from case_dirs import write_case
-from conftest import rel_linf
+from conftest import rel_linf, rel_linf_vec
 
 pytestmark = pytest.mark.gpu
 
@@ -73,16 +73,66 @@ def test_plan_mode_equals_graph_mode(sod_dir):
     assert rel_linf(qp, qg).max() <= 1e-14
 
 
+def _vts_arrays(text):
+    """Name -> values of every DataArray of a .vts file (Points as "Points")."""
+    out = {}
+    pts = re.search(r"<Points>\s*<DataArray[^>]*>(.*?)</DataArray>", text, re.S)
+    out["Points"] = np.array(pts.group(1).split(), dtype=np.float64)
+    for m in re.finditer(r'<DataArray type="(\w+)" Name="([^"]+)"[^>]*>(.*?)</DataArray>', text, re.S):
+        out[m.group(2)] = np.array(m.group(3).split(), dtype=np.int64 if m.group(1) == "Int32" else np.float64)
+    return out
+
+
 def test_vts_output_carries_the_state(sod_dir):
+    """The output is the reference's result layout: the Field's nodes (the 1-D
+    tube's unsolved y and z axes as their two node planes each), the
+    boundary-set arrays, and Density / Pressure / Velocity (this case's
+    registry declares no fields) with 17 digits."""
     s, q, _ = run_case(sod_dir)
     path = os.path.join(sod_dir, "result", "sod_c1_0003.vts")
     text = open(path).read()
-    assert 'WholeExtent="0 1000 0 0 0 0"' in text
-    m = re.search(r'Name="rho" NumberOfComponents="1" format="ascii">\n(.*?)</DataArray>', text, re.S)
-    rho = np.array(m.group(1).split(), dtype=np.float64)
-    np.testing.assert_array_equal(rho, q.reshape(-1, 5)[:, 0])   # 17 digits round-trip exactly
-    t = float(re.search(r'Name="TIME"[^>]*>([^<]*)<', text).group(1))
-    assert abs(t - 0.2) <= 1e-14
+    assert 'WholeExtent="0 1000 0 1 0 1"' in text and "TIME" not in text
+    a = _vts_arrays(text)
+    names = re.findall(r'Name="([^"]+)"', text)
+    assert names == ["BC_ID", "BC_ID_rho", "BC_ID_U", "BC_ID_p", "Density", "Pressure", "Velocity"]
+    q = q.reshape(-1, 5)
+    rho = a["Density"].reshape(2, 2, 1001)
+    for k in range(2):
+        for j in range(2):
+            np.testing.assert_array_equal(rho[k, j], q[:, 0])   # 17 digits round-trip exactly
+    np.testing.assert_array_equal(a["Velocity"].reshape(2, 2, 1001, 3)[0, 0, :, 0], q[:, 1] / q[:, 0])
+    pts = a["Points"].reshape(2, 2, 1001, 3)
+    assert pts[1, 1, 1000].tolist() == [1.0, 0.1, 0.1] and pts[0, 0, 0].tolist() == [0.0, 0.0, 0.0]
+    # Left = 1, Right = 2, sideWalls = 3, frontBack = 4: the empty patches'
+    # node planes cover every node of the tube, the last-named set wins
+    assert (a["BC_ID"] == 4).all() and (a["BC_ID_rho"] == 4).all()
+    assert "1=Left, 2=Right, 3=sideWalls, 4=frontBack;" in text
+
+
+def test_vts_boundary_sets_and_declared_fields(tmp_path):
+    """A 2-D box whose registry declares U and rho for output and p not:
+    U and rho take those names, Pressure keeps its built-in name; boundary
+    sets are numbered by first appearance over the rho, U, p conditions and
+    a later condition wins on shared nodes."""
+    bnd = {"frontBack": "empty", "Left": "zeroGradient", "Right": "zeroGradient", "sideWalls": "zeroGradient"}
+    d = write_case(str(tmp_path), "sets", cells=(30, 10, 1), box_hi=(3.0, 1.0, 0.1), end_time=0.01,
+                   write_interval=0.01, boundaries=bnd)
+    with open(os.path.join(d, "fields", "fields.yaml"), "a") as f:
+        f.write("U:\n  type: vector\n  output: true\nrho:\n  type: scalar\n  output: true\n"
+                "p:\n  type: scalar\n  output: false\n")
+    s, q, _ = run_case(d)
+    vts = sorted(f for f in os.listdir(os.path.join(d, "result")) if f.endswith(".vts"))
+    text = open(os.path.join(d, "result", vts[-1])).read()
+    names = re.findall(r'Name="([^"]+)"', text)
+    assert names[4:] == ["Pressure", "U", "rho"]
+    a = _vts_arrays(text)
+    # frontBack = 1 (both node planes of the one-cell-deep box: every node),
+    # Left = 2, Right = 3, sideWalls = 4
+    assert "1=frontBack, 2=Left, 3=Right, 4=sideWalls;" in text
+    ids = a["BC_ID"].reshape(2, 11, 31)
+    assert ids[0, 5, 0] == 2 and ids[1, 5, 30] == 3 and ids[0, 10, 5] == 4 and ids[1, 5, 5] == 1
+    assert ids[0, 0, 0] == 4 and ids[1, 10, 30] == 4   # corners: sideWalls, the last condition, wins
+    np.testing.assert_array_equal(a["rho"].reshape(2, 11, 31)[1].ravel(), q.reshape(-1, 5)[:, 0])
 
 
 # ------------------------------------------------- frozen end (no condition)
@@ -297,7 +347,8 @@ def test_curved_block_case_directory_matches_oracle(tmp_path, block, mode):
     assert "mesh curvilinear" in out and s["status"] == 0
     want, dts, tf = curved_oracle(kw, fm)
     assert s["steps"] == len(dts) and abs(s["time"] - tf) <= 1e-14
-    assert rel_linf(q, want).max() <= 1e-11
+    # momentum against one scale: rho v of the graded box stays at round-off
+    assert rel_linf_vec(q, want).max() <= 1e-11
 
 
 def test_curved_block_vts_carries_the_generated_points(tmp_path):
@@ -310,6 +361,8 @@ def test_curved_block_vts_carries_the_generated_points(tmp_path):
     vts = sorted(f for f in os.listdir(os.path.join(d, "result")) if f.endswith(".vts"))
     with open(os.path.join(d, "result", vts[-1])) as f:
         text = f.read()
-    body = text.split("<Points>")[1].split(">", 1)[1].split("</DataArray>")[0]
-    pts = np.array(body.split(), dtype=np.float64)
-    assert np.array_equal(pts, np.fromfile(fp))
+    pts = _vts_arrays(text)["Points"].reshape(2, 21, 41, 3)   # both node planes of the one-cell-deep block
+    assert np.array_equal(pts[0].ravel(), np.fromfile(fp))
+    # the second plane: z = 0.01, the same x, y (to the round-off of the
+    # transfinite sums)
+    assert np.abs(pts[1, ..., 2] - 0.01).max() <= 1e-15 and np.abs(pts[1, ..., :2] - pts[0, ..., :2]).max() <= 1e-14
