@@ -8,10 +8,12 @@
 //     alone;
 //   * a work list of tiles (2-D: TX x TY nodes, 1-D: 511 nodes) covering the
 //     solved nodes of every live instance, with its length in device memory;
-//   * persistent kernels, one block per SM slot, that take tiles from the
-//     list with an atomic counter: CFL reduction (per-instance 64-bit
-//     atomicMin), then each stage (the fused tile bodies of sfg_tile.cuh),
-//     then the per-instance clock update.
+//   * a step of four launches: the per-instance dt (the CFL minimum was
+//     reduced by the previous step's last stage, per-instance 64-bit
+//     atomicMin; a grid's first one when it joins), each stage as persistent
+//     kernels, one block per SM slot, that take tiles from the list with an
+//     atomic counter (the fused tile bodies of sfg_tile.cuh), then the
+//     per-instance clock update.
 // Every grid carries its own numerics (convection recipe, gamma, CFL,
 // maxDeltaT), as every reference case directory selects its own TermRecipe.
 // Grids of one recipe form a group: the work list holds the groups' tiles in
@@ -59,6 +61,8 @@ struct BatchInst {
     int pad;
 };
 
+// A tile: 2-D, TX x TY nodes from (x0, y0); 1-D, y0 nodes (TILE1D, or
+// TILE1D_SHORT once the batch has drained) from x0.
 struct WorkItem {
     int inst, x0, y0, dim;
 };
@@ -75,9 +79,11 @@ constexpr int kCounters = 8 + 4 * kMaxGroups;
 struct BatchCtl {
     int n_items;
     int n_inst;
-    int active;  // instances stepping in the current step
+    int active;   // instances stepping in the current step (counted by finalize)
+    int stepped;  // instances that stepped in the last completed step (set by commit)
     int n_law_items;
-    // work stealing: [0] dt, [5] copy, [8 + 4 g + s] stage s of recipe group g
+    int pad;
+    // work stealing: [5] copy, [8 + 4 g + s] stage s of recipe group g
     int counters[kCounters];
     // tile range of group g in the work list: [2 g] first item, [2 g + 1] count
     int group_range[2 * kMaxGroups];
@@ -148,6 +154,8 @@ __global__ void __launch_bounds__(TILE_THREADS, F32 ? 4 : 2)
         if (w.dim == 2) {
             if constexpr (F32) tile2d_f32_body<SCHEME, FLUX, TX, TY>(b.g, sv, w.x0, w.y0, smem, flags, cut, cores, sr);
             else tile2d_body<SCHEME, FLUX, TX, TY>(b.g, sv, w.x0, w.y0, smem, flags, cut, cores, sr);
+        } else if (w.y0 == TILE1D_SHORT) {
+            tile1d_body<SCHEME, FLUX, Tt, TILE1D_SHORT>(b.g, sv, w.x0, smem, flags, cut, cores, sr);
         } else {
             tile1d_body<SCHEME, FLUX, Tt>(b.g, sv, w.x0, smem, flags, cut, cores, sr);
         }
@@ -183,36 +191,28 @@ __global__ void __launch_bounds__(LAW_CHUNK)
     }
 }
 
-// CFL step per instance over its tiles (RusanovEOS::deltaT).
-template <int TX, int TY>
-__global__ void __launch_bounds__(TILE_THREADS) batch_dt_kernel(BatchInst* inst, const WorkItem* items, BatchCtl* ctl) {
-    __shared__ int slot;
-    const int n_items = ctl->n_items;
-    for (;;) {
-        const int it = steal(&ctl->counters[0], &slot);
-        if (it >= n_items) break;
-        const WorkItem w = items[it];
-        BatchInst& b = inst[w.inst];
-        if (!b.live || b.done || b.clock.dt_ready) continue;  // ready: reduced by the last stage
-        const GridView& g = b.g;
-        const int cnt = w.dim == 2 ? TX * TY : TILE1D;
-        double best = 0.0;
-        unsigned fl = 0;
-        for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
-            const int i = w.dim == 2 ? w.x0 + t % TX : w.x0 + t;
-            const int j = w.dim == 2 ? w.y0 + t / TX : 0;
-            if (i >= g.hi[0] || (w.dim == 2 && j >= g.hi[1])) continue;
-            const long long node = (long long)j * g.n[0] + i;
-            const double* q = b.qn;
-            const double qq[5] = {q[node], q[g.vs + node], q[2 * g.vs + node], q[3 * g.vs + node], q[4 * g.vs + node]};
-            const double sr = cfl_rate(g, qq);
-            if (!(sr > 0.0) || !isfinite(sr)) fl |= FLAG_NONFINITE;
-            best = fmax(best, sr);
-        }
-        flush_cfl_block(g, &b.clock, best);
-        if (fl) atomicOr(&b.flags, fl);
-        __syncthreads();
+// CFL minimum of a grid's uploaded state (RusanovEOS::deltaT), once when it
+// joins the batch; from then on each step's last stage reduces the new
+// state's minimum (MODE_CFL), so the step itself has no CFL pass.
+__global__ void __launch_bounds__(TILE_THREADS) batch_initial_cfl_kernel(BatchInst* inst, int idx) {
+    BatchInst& b = inst[idx];
+    const GridView& g = b.g;
+    const int sx = g.hi[0] - g.lo[0], sy = g.hi[1] - g.lo[1];
+    const long long count = (long long)sx * sy;
+    double best = 0.0;
+    unsigned fl = 0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < count;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = g.lo[0] + (int)(t % sx), j = g.lo[1] + (int)(t / sx);
+        const long long node = (long long)j * g.n[0] + i;
+        const double* q = b.qn;
+        const double qq[5] = {q[node], q[g.vs + node], q[2 * g.vs + node], q[3 * g.vs + node], q[4 * g.vs + node]};
+        const double sr = cfl_rate(g, qq);
+        if (!(sr > 0.0) || !isfinite(sr)) fl |= FLAG_NONFINITE;
+        best = fmax(best, sr);
     }
+    flush_cfl_block(g, &b.clock, best);
+    if (fl) atomicOr(&b.flags, fl);
 }
 
 // FlowDtCompute + Time::Driver clipping per instance (one thread each).
@@ -255,7 +255,7 @@ __global__ void __launch_bounds__(TILE_THREADS) batch_copy_kernel(BatchInst* ins
         const WorkItem w = items[it];
         BatchInst& b = inst[w.inst];
         if (!b.live || !b.clock.active) continue;
-        const int cnt = w.dim == 2 ? TX * TY : TILE1D;
+        const int cnt = w.dim == 2 ? TX * TY : w.y0;
         for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
             const int i = w.dim == 2 ? w.x0 + t % TX : w.x0 + t;
             const int j = w.dim == 2 ? w.y0 + t / TX : 0;
@@ -283,11 +283,14 @@ __global__ void batch_commit_kernel(BatchInst* inst, BatchCtl* ctl) {
             c->dt_ready = c->active ? 1 : 0;  // the last stage reduced the new state's CFL minimum
         }
     }
-    if (blockIdx.x == 0)
+    if (blockIdx.x == 0) {
         for (int c = threadIdx.x; c < kCounters; c += blockDim.x) ctl->counters[c] = 0;
+        if (threadIdx.x == 0) {  // the next step's finalize counts afresh
+            ctl->stepped = ctl->active;
+            ctl->active = 0;
+        }
+    }
 }
-
-__global__ void batch_reset_active_kernel(BatchCtl* ctl) { ctl->active = 0; }
 
 }  // namespace sfg
 
@@ -405,7 +408,7 @@ struct sfg_batch_s {
     double* staging = nullptr;
     size_t staging_cap = 0;
     // kernels and graph
-    ItemKernel dt_k = nullptr, copy_k = nullptr;
+    ItemKernel copy_k = nullptr;
     int grid_items = 0;
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
@@ -437,12 +440,10 @@ int bind_group(sfg_batch_s* b, RecipeGroup& grp) {
 
 int bind_kernels(sfg_batch_s* b) {
     if (b->variant == 1) {
-        b->dt_k = batch_dt_kernel<32, 15>;
         b->copy_k = batch_copy_kernel<32, 15>;
         b->tx = 32;
         b->ty = 15;
     } else {
-        b->dt_k = batch_dt_kernel<22, 22>;
         b->copy_k = batch_copy_kernel<22, 22>;
         b->tx = 22;
         b->ty = 22;
@@ -531,6 +532,18 @@ void slab_free(sfg_batch_s* b, size_t off, size_t bytes) {
 // instance count) to device memory.
 int publish_items(sfg_batch_s* b) {
     b->h_items.clear();
+    // 1-D tiles of one face round once the live tiles no longer fill the
+    // SMs: a drained batch's last grids then take half the time per stage
+    long long long_tiles = 0;
+    for (int i = 0; i < (int)b->h_inst.size(); ++i) {
+        const BatchInst& r = b->h_inst[i];
+        if (!r.live || r.done) continue;
+        const GridView& g = r.g;
+        long_tiles += g.dim == 1 ? (g.hi[0] - g.lo[0] + TILE1D - 1) / TILE1D
+                                 : (long long)((g.hi[0] - g.lo[0] + b->tx - 1) / b->tx) *
+                                       ((g.hi[1] - g.lo[1] + b->ty - 1) / b->ty);
+    }
+    const int t1 = long_tiles < b->grid_items ? TILE1D_SHORT : TILE1D;
     for (int grp = 0; grp < kMaxGroups; ++grp) {
         const int first = (int)b->h_items.size();
         for (int i = 0; grp < (int)b->groups.size() && i < (int)b->h_inst.size(); ++i) {
@@ -538,7 +551,7 @@ int publish_items(sfg_batch_s* b) {
             if (!r.live || r.done || b->inst_group[i] != grp) continue;
             const GridView& g = r.g;
             if (g.dim == 1) {
-                for (int x = g.lo[0]; x < g.hi[0]; x += TILE1D) b->h_items.push_back({i, x, 0, 1});
+                for (int x = g.lo[0]; x < g.hi[0]; x += t1) b->h_items.push_back({i, x, t1, 1});
             } else {
                 for (int y = g.lo[1]; y < g.hi[1]; y += b->ty)
                     for (int x = g.lo[0]; x < g.hi[0]; x += b->tx) b->h_items.push_back({i, x, y, 2});
@@ -598,8 +611,6 @@ int publish_items(sfg_batch_s* b) {
 
 int enqueue_batch_step(sfg_batch_s* b) {
     const int ni = std::max<int>(1, b->max_inst);
-    batch_reset_active_kernel<<<1, 1, 0, b->stream>>>(b->d_ctl);
-    b->dt_k<<<b->grid_items, TILE_THREADS, 0, b->stream>>>(b->d_inst, b->d_items, b->d_ctl);
     batch_finalize_kernel<<<(ni + 127) / 128, 128, 0, b->stream>>>(b->d_inst, b->d_ctl);
     const int ns = stage_count_of(b->num.time_recipe);
     const int ng = (int)b->groups.size();
@@ -961,6 +972,7 @@ int sfg_batch_add_laws(sfg_batch b, const sfg_grid_desc* grid, const sfg_numeric
     r.clock.max_dt = num.max_dt > 0.0 ? num.max_dt : kInfB;
     r.clock.limit = kInfB;
     r.clock.dt_bits = 0x7FEFFFFFFFFFFFFFull;
+    r.clock.dt_ready = 1;  // reduced below, before the grid's first step
     r.clock.max_steps = max_steps > 0 ? max_steps : std::numeric_limits<long long>::max();
     r.clock.active = 0;
     r.flags = 0;
@@ -979,6 +991,12 @@ int sfg_batch_add_laws(sfg_batch b, const sfg_grid_desc* grid, const sfg_numeric
         BCUDA(cudaMemcpyAsync(r.qb, r.qn, per, cudaMemcpyDeviceToDevice, b->stream));
     }
     BCUDA(cudaMemcpyAsync(b->d_inst + idx, &r, sizeof r, cudaMemcpyHostToDevice, b->stream));
+    {
+        const long long solved = (long long)(g.hi[0] - g.lo[0]) * (g.hi[1] - g.lo[1]);
+        const int blocks = (int)std::min<long long>((solved + TILE_THREADS - 1) / TILE_THREADS, 1024);
+        batch_initial_cfl_kernel<<<blocks, TILE_THREADS, 0, b->stream>>>(b->d_inst, idx);
+        BCUDA(cudaGetLastError());
+    }
     b->h_inst[idx] = r;
     b->inst_offset[idx] = soff;
     b->inst_bytes[idx] = slab_bytes;
@@ -1034,7 +1052,7 @@ int sfg_batch_step(sfg_batch b, int steps, int graph_steps, int* active) {
         }
         BCUDA(cudaMemcpyAsync(b->h_ctl, b->d_ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, b->stream));
         BCUDA(cudaStreamSynchronize(b->stream));
-        const int now = b->h_ctl->active;
+        const int now = b->h_ctl->stepped;
         if (last_active < 0 || now < last_active) {
             // some instances finished: drop their tiles from the work list
             std::vector<BatchInst> tmp(b->h_inst.size());
@@ -1056,7 +1074,7 @@ int sfg_batch_step(sfg_batch b, int steps, int graph_steps, int* active) {
         if (now == 0) break;  // every live instance has finished
     }
     b->batch_steps += done;
-    if (active) *active = b->h_ctl->active;
+    if (active) *active = b->h_ctl->stepped;
     return SFG_OK;
 }
 

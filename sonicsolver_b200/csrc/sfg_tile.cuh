@@ -34,7 +34,8 @@
 namespace sfg {
 
 constexpr int TILE_THREADS = 256;
-constexpr int TILE1D = 511;  // 1-D tile: 512 faces = 2 rounds of 256
+constexpr int TILE1D = 511;        // 1-D tile: 512 faces = 2 rounds of 256
+constexpr int TILE1D_SHORT = 255;  // 1-D tile of one round (a batch's drained tail)
 
 template <int SCHEME, int TX, int TY>
 struct TileShape {
@@ -46,12 +47,12 @@ struct TileShape {
     static constexpr int ELEMS = 5 * SX * SY + 5 * NFX + 5 * NFY;  // shared elements
 };
 
-template <int SCHEME>
+template <int SCHEME, int T1 = TILE1D>
 struct Tile1Shape {
     static constexpr int NST = SchemeInfo<SCHEME>::NST;
     static constexpr int H = NST / 2;
-    static constexpr int SX = TILE1D + 2 * H;
-    static constexpr int NF = TILE1D + 1;
+    static constexpr int SX = T1 + 2 * H;
+    static constexpr int NF = T1 + 1;
     static constexpr int ELEMS = 5 * SX + 5 * NF;
 };
 
@@ -243,10 +244,12 @@ __device__ __forceinline__ void tile2d_f32_body(const GridView& g, const StageVi
 
 // ------------------------------------------------------------------ 1-D
 // T = double: FP64 stencil; T = float: FP32 deviations from the stage's reference node.
-template <int SCHEME, int FLUX, typename T>
+// T1 nodes per tile; every face and node gets the same bits whatever the
+// tile length (the FP32 reference is the stage's, not the tile's).
+template <int SCHEME, int FLUX, typename T, int T1 = TILE1D>
 __device__ __forceinline__ void tile1d_body(const GridView& g, const StageView& sv, int x0, T* smem, unsigned& flags,
                                             unsigned& cut, unsigned& cores, double& sr_max) {
-    using S = Tile1Shape<SCHEME>;
+    using S = Tile1Shape<SCHEME, T1>;
     constexpr int NST = S::NST, H = S::H, SX = S::SX, NF = S::NF;
     constexpr bool F32 = sizeof(T) == sizeof(float);
     T* sq = smem;          // [5][SX]
@@ -276,7 +279,7 @@ __device__ __forceinline__ void tile1d_body(const GridView& g, const StageView& 
     }
     __syncthreads();
     const double dt = sv.clock->dt;
-    for (int c = threadIdx.x; c < TILE1D; c += blockDim.x) {
+    for (int c = threadIdx.x; c < T1; c += blockDim.x) {
         const int gx = x0 + c;
         if (gx >= g.hi[0]) continue;
         double div[5], qn[5];
