@@ -71,6 +71,9 @@ def parse():
     ap.add_argument("--curv-t", type=float, default=1.0, help="curvilinear vortex run length (0: skip)")
     ap.add_argument("--all-kernels", action="store_true",
                     help="run every kernel family once on inputs larger than L2 (for a profiler launch list)")
+    ap.add_argument("--family", default="all",
+                    choices=["all", "vortex2d", "channel", "tube1d", "sod", "tgv3d", "curv", "batch"],
+                    help="with --all-kernels: one kernel family's workload only (small profiler captures)")
     return ap.parse_args()
 
 
@@ -813,6 +816,10 @@ def run_all_kernels(args):
     from sonicsolver_b200 import capi, cases
     F64, F32 = capi.PREC_FP64, capi.PREC_FP32_FLUX
     ran = []
+    fam = args.family
+
+    def want(f):
+        return fam in ("all", f)
 
     def steps(case, label, variants, precisions=(F64, F32)):
         for prec in precisions:
@@ -824,41 +831,49 @@ def run_all_kernels(args):
                 ran.append(f"{label} variant {v} {'fp64' if prec == F64 else 'fp32flux'}: one CFL step")
 
     # 2-D vortex 2048^2 (168 MB per state copy): axis sweeps, 32 x 15 and 22 x 22 tiles
-    vortex = cases.isentropic_vortex(2048)
-    steps(vortex, "2-D vortex 2048^2", (0, 1, 2))
-    s = vortex.solver()
-    s.totals()
-    s.teno_flips()
-    s.download()
-    r = s.residual()
-    s.stage_with_residual(0, 1e-4, r)
-    s.close()
-    ran.append("2-D vortex 2048^2: totals, TENO flip count, download, residual, stage from a given residual")
-    # 2-D channel with law ends (fixedValue inflow, zeroGradient outflow)
-    lo, hi = (capi.BC_LAW, capi.BC_TRANSMISSIVE, 0), (capi.BC_LAW, capi.BC_TRANSMISSIVE, 0)
-    s = capi.Solver(2, vortex.n, vortex.h, lo, hi, recipe="teno5Rusanov", cfl=0.4)
-    s.set_boundary_law(0, 0, rho=capi.LAW_FIXED_VALUE, velocity=capi.LAW_FIXED_VALUE, rho_value=1.0,
-                       velocity_value=(1.0, 0.0, 0.0))
-    s.set_boundary_law(0, 1)
-    s.upload(np.ascontiguousarray(vortex.q))
-    s.step()
-    s.close()
-    ran.append("2-D channel 2048^2 with law ends: one CFL step (law fill before each stage)")
-    del vortex
+    if want("vortex2d") or want("channel"):
+        vortex = cases.isentropic_vortex(2048)
+    if want("vortex2d"):
+        steps(vortex, "2-D vortex 2048^2", (0, 1, 2))
+        s = vortex.solver()
+        s.totals()
+        s.teno_flips()
+        s.download()
+        r = s.residual()
+        s.stage_with_residual(0, 1e-4, r)
+        s.close()
+        ran.append("2-D vortex 2048^2: totals, TENO flip count, download, residual, stage from a given residual")
+    if want("channel"):
+        # 2-D channel with law ends (fixedValue inflow, zeroGradient outflow)
+        lo, hi = (capi.BC_LAW, capi.BC_TRANSMISSIVE, 0), (capi.BC_LAW, capi.BC_TRANSMISSIVE, 0)
+        s = capi.Solver(2, vortex.n, vortex.h, lo, hi, recipe="teno5Rusanov", cfl=0.4)
+        s.set_boundary_law(0, 0, rho=capi.LAW_FIXED_VALUE, velocity=capi.LAW_FIXED_VALUE, rho_value=1.0,
+                           velocity_value=(1.0, 0.0, 0.0))
+        s.set_boundary_law(0, 1)
+        s.upload(np.ascontiguousarray(vortex.q))
+        s.step()
+        s.close()
+        ran.append("2-D channel 2048^2 with law ends: one CFL step (law fill before each stage)")
+    if want("vortex2d") or want("channel"):
+        del vortex
     # 1-D tube of 4 M nodes (168 MB): 511-node tiles; Sod 1000 cells: the whole-run cluster kernel
-    steps(cases.sod_1d((1 << 22) - 1), "1-D tube 4M nodes", (1,))
-    sod = cases.sod_1d(1000)
-    s = sod.solver()
-    s.advance(sod.t_end, max_steps=50)
-    s.close()
-    ran.append("Sod 1000 cells: 50 steps in one cluster launch")
+    if want("tube1d"):
+        steps(cases.sod_1d((1 << 22) - 1), "1-D tube 4M nodes", (1,))
+    if want("sod"):
+        sod = cases.sod_1d(1000)
+        s = sod.solver()
+        s.advance(sod.t_end, max_steps=50)
+        s.close()
+        ran.append("Sod 1000 cells: 50 steps in one cluster launch")
     # 3-D Taylor-Green 160^3 (164 MB): axis sweeps and z-marching tiles
-    steps(cases.taylor_green(160), "3-D Taylor-Green 160^3", (0, 1))
+    if want("tgv3d"):
+        steps(cases.taylor_green(160), "3-D Taylor-Green 160^3", (0, 1))
     # curvilinear vortex 1448^2 (84 MB state + 168 MB metrics): face launches and fused tiles
-    steps(cases.wavy_vortex(1448), "curvilinear vortex 1448^2", (0, 1))
+    if want("curv"):
+        steps(cases.wavy_vortex(1448), "curvilinear vortex 1448^2", (0, 1))
     # batch: every second tube of the batched workload
-    tubes = cases.shock_tube_batch(count=512, seed=2024, t_end=0.15)[::2]
-    for prec in (F64, F32):
+    tubes = cases.shock_tube_batch(count=512, seed=2024, t_end=0.15)[::2] if want("batch") else []
+    for prec in ((F64, F32) if want("batch") else ()):
         b = capi.Batch(4 << 30, len(tubes), recipe="weno5Rusanov", precision=prec, cfl=0.5)
         for c in tubes:
             b.add(c)

@@ -38,6 +38,7 @@
 #include <limits>
 #include <string>
 #include <sys/stat.h>
+#include <unistd.h>
 #include <vector>
 
 #include "../../include/sonicsolver_b200.h"
@@ -380,6 +381,41 @@ int selftest() {
         threw = true;
     }
     check(threw, "an operation is bound once");
+    // restart files: a written state reads back to the last bit, with its
+    // clock; a damaged one is refused
+    {
+        Checkpoint ck;
+        ck.nodes[0] = 7;
+        ck.nodes[1] = 3;
+        ck.time = 0.1 + 0.2;
+        ck.steps = 42;
+        ck.next_output = 1.0 / 3.0;
+        ck.outputs = 5;
+        for (int i = 0; i < 7 * 3 * 5; ++i) ck.q.push_back(std::ldexp(1.0 + i / 97.0, (i % 9) - 4) * (i % 2 ? -1 : 1));
+        char path[] = "/tmp/sfg_selftest_ckXXXXXX";
+        const int fd = mkstemp(path);
+        bool ok = fd >= 0 && write_checkpoint(path, ck);
+        if (fd >= 0) close(fd);
+        if (ok) {
+            const Checkpoint back = read_checkpoint(path);
+            ok = back.q == ck.q && back.time == ck.time && back.steps == 42 && back.next_output == ck.next_output &&
+                 back.outputs == 5 && back.nodes[0] == 7 && back.nodes[1] == 3 && back.nodes[2] == 1;
+        }
+        check(ok, "a restart file reads back bit for bit with its clock");
+        bool refused = false;
+        if (FILE* f = std::fopen(path, "w")) {
+            std::fputs("{\"formatVersion\": 1, \"fields\": {}, \"nodes\": [1, 1, 1], \"time\": 0, \"steps\": 0, "
+                       "\"outputs\": 0}", f);
+            std::fclose(f);
+            try {
+                read_checkpoint(path);
+            } catch (const std::runtime_error&) {
+                refused = true;
+            }
+        }
+        std::remove(path);
+        check(refused, "a restart file without its fields is refused");
+    }
     std::printf("%s\n", failed ? "selftest FAILED" : "selftest passed");
     return failed ? 1 : 0;
 }
