@@ -881,6 +881,7 @@ int sfg_batch_add_ex(sfg_batch b, const sfg_grid_desc* grid, const sfg_numerics_
 int sfg_batch_add_laws(sfg_batch b, const sfg_grid_desc* grid, const sfg_numerics_desc* numerics,
                        const sfg_boundary_law* laws, const double* host_nodes_aos, double t_end, int64_t max_steps,
                        int* slot) {
+    sfg::NvtxRange nvtx_("sfg_batch_add");
     if (!b || !grid || !host_nodes_aos || !slot) return bfail(SFG_ERR_ARG, "null argument");
     const sfg_numerics_desc& num = numerics ? *numerics : b->num;
     const RecipeParts* rp = nullptr;
@@ -1023,6 +1024,7 @@ int sfg_batch_remove(sfg_batch b, int slot) {
 }
 
 int sfg_batch_step(sfg_batch b, int steps, int graph_steps, int* active) {
+    sfg::NvtxRange nvtx_("sfg_batch_step");
     if (!b) return bfail(SFG_ERR_ARG, "null batch");
     if (graph_steps <= 0) graph_steps = 16;
     if (!b->graph || b->graph_steps != graph_steps) {
@@ -1097,6 +1099,7 @@ int sfg_batch_status(sfg_batch b, int slot, double* time, int64_t* steps, int* r
 }
 
 int sfg_batch_download(sfg_batch b, int slot, double* host_nodes_aos) {
+    sfg::NvtxRange nvtx_("sfg_batch_download");
     if (!b || !host_nodes_aos) return bfail(SFG_ERR_ARG, "null argument");
     if (slot < 0 || slot >= (int)b->h_inst.size() || !b->h_inst[slot].live)
         return bfail(SFG_ERR_NOT_FOUND, "no live instance in slot %d", slot);

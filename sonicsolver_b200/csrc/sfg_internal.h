@@ -7,6 +7,8 @@
 #include <atomic>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/sonicsolver_b200.h"
 
 namespace sfg {
@@ -134,6 +136,16 @@ struct ClusterRun {
 const char* law_problem(const sfg_boundary_law& law);
 void grid_law_view(const sfg_grid_desc& G, const GridView& gv, const int off_lo[3], const sfg_boundary_law* laws,
                    int ng, LawView& lv, std::vector<unsigned char>& codes);
+
+// A named NVTX range over a host scope: the C-ABI entries mark their work
+// for a timeline profiler (Nsight Systems) and for range filters (ncu
+// --nvtx-include).  Without a tool attached a push / pop costs a branch.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // One-time kernel attribute setup per device: kernel attributes belong to a
 // device context, so each launcher keeps its own set of devices done (one bit

@@ -873,6 +873,7 @@ static int reset_time(sfg_solver s, double time) {
 }
 
 int sfg_upload(sfg_solver s, const double* host, int layout, double time) {
+    sfg::NvtxRange nvtx_("sfg_upload");
     if (!s || !host) return fail(SFG_ERR_ARG, "null argument");
     if (layout == SFG_LAYOUT_NODES && !s->frozen) {
         int rc = upload_nodes_host(s, host);
@@ -908,6 +909,7 @@ int sfg_upload(sfg_solver s, const double* host, int layout, double time) {
 }
 
 int sfg_restore(sfg_solver s, const double* host, int layout, double time, int64_t steps) {
+    sfg::NvtxRange nvtx_("sfg_restore");
     if (!s || !host) return fail(SFG_ERR_ARG, "null argument");
     if (!std::isfinite(time)) return fail(SFG_ERR_ARG, "time must be finite");
     if (steps < 0) return fail(SFG_ERR_ARG, "steps must be >= 0");
@@ -932,6 +934,7 @@ int sfg_download_device(sfg_solver s, double* dev_nodes_aos) {
 }
 
 int sfg_download(sfg_solver s, double* host, int layout) {
+    sfg::NvtxRange nvtx_("sfg_download");
     if (!s || !host) return fail(SFG_ERR_ARG, "null argument");
     CUDA_TRY(launch_soa_to_aos(s->gv, s->qn, s->staging, s->stream));
     if (layout == SFG_LAYOUT_NODES && !s->frozen) {
@@ -970,6 +973,7 @@ int sfg_download(sfg_solver s, double* host, int layout) {
 }
 
 int sfg_compute_dt(sfg_solver s, double limit, double* dt) {
+    sfg::NvtxRange nvtx_("sfg_compute_dt");
     if (!s || !dt) return fail(SFG_ERR_ARG, "null argument");
     CUDA_TRY(launch_reset_min(s->clock, s->stream));
     CUDA_TRY(launch_dt(s->gv, s->qn, s->clock, s->flags, 0, s->stream));
@@ -985,6 +989,7 @@ int sfg_compute_dt(sfg_solver s, double limit, double* dt) {
 }
 
 int sfg_stage(sfg_solver s, int stage, double dt) {
+    sfg::NvtxRange nvtx_("sfg_stage");
     if (!s) return fail(SFG_ERR_ARG, "null solver");
     const int ns = stage_count(s->num.time_recipe);
     if (stage != s->next_stage || stage < 0 || stage >= ns)
@@ -1009,6 +1014,7 @@ int sfg_stage(sfg_solver s, int stage, double dt) {
 }
 
 int sfg_step(sfg_solver s, double dt, double limit) {
+    sfg::NvtxRange nvtx_("sfg_step");
     if (!s) return fail(SFG_ERR_ARG, "null solver");
     if (s->next_stage != 0) return fail(SFG_ERR_ARG, "a step is in progress (stage %d)", s->next_stage);
     if (dt > 0.0) {
@@ -1129,6 +1135,7 @@ static int advance_cluster(sfg_solver_s* s, float* ms, bool* ran) {
 
 int sfg_advance(sfg_solver s, double t_end, int64_t max_steps, double write_interval, int graph_steps,
                 double* dt_out, int64_t dt_capacity, sfg_stats* stats) {
+    sfg::NvtxRange nvtx_("sfg_advance");
     if (!s) return fail(SFG_ERR_ARG, "null solver");
     if (s->next_stage != 0) return fail(SFG_ERR_ARG, "a step is in progress");
     if (!(t_end == t_end)) return fail(SFG_ERR_ARG, "t_end is NaN");
@@ -1202,6 +1209,7 @@ int sfg_advance(sfg_solver s, double t_end, int64_t max_steps, double write_inte
 }
 
 int sfg_residual(sfg_solver s, double* host_nodes_aos) {
+    sfg::NvtxRange nvtx_("sfg_residual");
     if (!s || !host_nodes_aos) return fail(SFG_ERR_ARG, "null argument");
     CUDA_TRY(cudaMemsetAsync(s->r, 0, sizeof(double) * 5 * s->gv.vs, s->stream));
     int rc = enqueue_stage(s, 0, true, false);
