@@ -321,6 +321,12 @@ int sfg_batch_add_ex(sfg_batch b, const sfg_grid_desc* grid, const sfg_numerics_
 int sfg_batch_add_laws(sfg_batch b, const sfg_grid_desc* grid, const sfg_numerics_desc* numerics,
                        const sfg_boundary_law* laws, const double* host_nodes_aos, double t_end, int64_t max_steps,
                        int* slot);
+/* Output clipping of one grid, as sfg_advance's write_interval: its steps
+ * stop exactly at every write_interval after its current time (<= 0:
+ * none), so its dt sequence equals a single-grid run that writes output at
+ * those times (Time::Driver, src/solver/algorithm/time/SF_time.cpp:56-72).
+ * Call between steps. */
+int sfg_batch_set_write_interval(sfg_batch b, int slot, double write_interval);
 int sfg_batch_remove(sfg_batch b, int slot);
 /* Runs up to `steps` batch steps (graph of `graph_steps`, <= 0: 16); stops
  * early when no grid is running.  *active = grids that stepped last. */

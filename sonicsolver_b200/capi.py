@@ -158,6 +158,7 @@ def lib():
         L.sfg_batch_add_laws.argtypes = [_VP, PG, PN, PL, _DP, ctypes.c_double, ctypes.c_int64,
                                          ctypes.POINTER(ctypes.c_int)]
         L.sfg_batch_remove.argtypes = [_VP, ctypes.c_int]
+        L.sfg_batch_set_write_interval.argtypes = [_VP, ctypes.c_int, ctypes.c_double]
         L.sfg_batch_step.argtypes = [_VP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
         L.sfg_batch_status.argtypes = [_VP, ctypes.c_int, _DP, I64P, ctypes.POINTER(ctypes.c_int),
                                        ctypes.POINTER(ctypes.c_uint32)]
@@ -413,6 +414,10 @@ class Batch:
         b = ctypes.c_size_t()
         check(lib().sfg_batch_instance_bytes(self._h, ctypes.byref(g), ctypes.byref(b)))
         return b.value
+
+    def set_write_interval(self, slot, write_interval):
+        """Clip the grid's steps at every write_interval (as sfg_advance)."""
+        check(lib().sfg_batch_set_write_interval(self._h, slot, float(write_interval)))
 
     def remove(self, slot):
         check(lib().sfg_batch_remove(self._h, slot))

@@ -1011,6 +1011,23 @@ int sfg_batch_add_laws(sfg_batch b, const sfg_grid_desc* grid, const sfg_numeric
     return SFG_OK;
 }
 
+int sfg_batch_set_write_interval(sfg_batch b, int slot, double write_interval) {
+    if (!b || slot < 0 || slot >= (int)b->h_inst.size() || !b->h_inst[slot].live)
+        return bfail(SFG_ERR_NOT_FOUND, "no live instance in slot %d", slot);
+    if (!std::isfinite(write_interval)) return bfail(SFG_ERR_ARG, "write interval must be finite");
+    BatchInst r;
+    BCUDA(cudaMemcpyAsync(&r, b->d_inst + slot, sizeof r, cudaMemcpyDeviceToHost, b->stream));
+    BCUDA(cudaStreamSynchronize(b->stream));
+    const double wi = write_interval > 0.0 ? write_interval : 0.0;
+    r.clock.write_interval = wi;
+    r.clock.next_out = wi > 0.0 ? r.clock.t + wi : kInfB;
+    BCUDA(cudaMemcpyAsync(&b->d_inst[slot].clock, &r.clock, sizeof r.clock, cudaMemcpyHostToDevice, b->stream));
+    BCUDA(cudaStreamSynchronize(b->stream));
+    b->h_inst[slot].clock.write_interval = r.clock.write_interval;
+    b->h_inst[slot].clock.next_out = r.clock.next_out;
+    return SFG_OK;
+}
+
 int sfg_batch_remove(sfg_batch b, int slot) {
     if (!b || slot < 0 || slot >= (int)b->h_inst.size() || !b->h_inst[slot].live)
         return bfail(SFG_ERR_NOT_FOUND, "no live instance in slot %d", slot);

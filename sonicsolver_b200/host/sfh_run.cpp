@@ -8,6 +8,8 @@
 //      C-ABI call of this library, validate the bindings;
 //   4. run it, writing .vts output at the case's write times.
 //
+//   sfg_run --batch CASE_DIR... [--precision fp64|fp32flux] [--graph-steps K]
+//           [--variant 1|2] [--dump-dir DIR] [--no-write] [--describe]
 //   sfg_run CASE_DIR [--mode graph|plan] [--precision fp64|fp32flux]
 //                    [--graph-steps K] [--dump FILE] [--dump-points FILE]
 //                    [--dump-metrics FILE] [--checkpoint PREFIX] [--restart FILE]
@@ -29,6 +31,15 @@
 // state, time, step count and output clock replace the case's initial state
 // and start time, and the run continues with the bits of the run that wrote
 // it (sfg_restore).
+// --batch runs several case directories together on the batched provider
+// (sfg_batch_*): every case keeps its own recipe, gamma, CFL, maxDeltaT,
+// boundary laws and output clipping, cases of one time recipe share a
+// batch, and each ends at its own endTime with the steps and bits of its
+// single-case graph run.  It writes each case's final state
+// (<job>_final.vts in its output directory; with --dump-dir, <case name>.bin
+// there) and prints one JSON line per case.  A case the batched kernels do
+// not run (3-D, curvilinear, a start time, a flux other than Rusanov / Roe)
+// is reported as unsupported and the others run.
 // Exit codes: 0 done, 1 error, 2 usage, 3 case not supported by the provider.
 #include <chrono>
 #include <cmath>
@@ -36,6 +47,7 @@
 #include <cstring>
 #include <fstream>
 #include <limits>
+#include <map>
 #include <string>
 #include <sys/stat.h>
 #include <unistd.h>
@@ -54,7 +66,10 @@ namespace {
 using namespace sfh;
 
 struct Options {
-    std::string dir, mode = "graph", dump, dump_points, dump_metrics, checkpoint, restart;
+    std::string dir, mode = "graph", dump, dump_points, dump_metrics, checkpoint, restart, dump_dir;
+    std::vector<std::string> batch_dirs;
+    bool batch = false;
+    int variant = 0;
     int precision = SFG_PREC_FP64;
     int graph_steps = 32;
     bool write = true, describe_only = false;
@@ -64,7 +79,9 @@ int usage() {
     std::fprintf(stderr,
                  "usage: sfg_run CASE_DIR [--mode graph|plan] [--precision fp64|fp32flux] [--graph-steps K]\n"
                  "               [--dump FILE] [--dump-points FILE] [--dump-metrics FILE] [--checkpoint PREFIX]\n"
-                 "               [--restart FILE] [--no-write] [--describe]\n");
+                 "               [--restart FILE] [--no-write] [--describe]\n"
+                 "       sfg_run --batch CASE_DIR... [--precision fp64|fp32flux] [--graph-steps K] [--variant 1|2]\n"
+                 "               [--dump-dir DIR] [--no-write] [--describe]\n");
     return 2;
 }
 
@@ -422,6 +439,152 @@ int selftest() {
 
 }  // namespace
 
+// ---- several case directories on the batched provider
+
+struct BatchCase {
+    std::string dir;
+    CaseSpec c;
+    GridSetup g;
+    int recipe = -1, tid = -1, slot = -1;
+};
+
+// Why a case cannot run batched (empty: it can).
+std::string batch_obstacle(const BatchCase& b) {
+    if (b.g.grid.dim > 2) return "3-D grids run on single-grid solvers only";
+    if (b.c.curvilinear) return "graded or curved blocks run on single-grid solvers only";
+    if (b.c.start_time != 0.0) return "a start time other than 0 (restart cases run on single-grid solvers)";
+    const std::string& r = b.c.convection;
+    const bool flux_ok = r.size() > 5 && (r.compare(r.size() - 7, 7, "Rusanov") == 0 || r.compare(r.size() - 3, 3, "Roe") == 0);
+    if (!flux_ok) return "convection '" + r + "': the batched kernels provide Rusanov and Roe faces";
+    return {};
+}
+
+int run_batch(const Options& o) {
+    std::vector<BatchCase> cases;
+    int unsupported = 0;
+    for (const auto& dir : o.batch_dirs) {
+        BatchCase b;
+        b.dir = dir;
+        try {
+            b.c = load_case(dir);
+            b.g = build_grid(b.c);
+            int stages = 0;
+            b.tid = time_id(b.c.time_recipe, stages);
+            if (sfg_recipe_from_name(b.c.convection.c_str(), &b.recipe) != SFG_OK)
+                throw Unsupported("convection '" + b.c.convection + "' has no term provider");
+            const std::string why = batch_obstacle(b);
+            if (!why.empty()) throw Unsupported(why);
+        } catch (const Unsupported& e) {
+            std::fprintf(stderr, "sfg_run: unsupported: %s: %s\n", dir.c_str(), e.what());
+            ++unsupported;
+            continue;
+        } catch (const std::exception& e) {
+            std::fprintf(stderr, "sfg_run: error: %s: %s\n", dir.c_str(), e.what());
+            return 1;
+        }
+        cases.push_back(std::move(b));
+    }
+    // one batch per time recipe (a batch runs one time recipe and precision)
+    std::map<int, std::vector<size_t>> groups;
+    for (size_t k = 0; k < cases.size(); ++k) groups[cases[k].tid].push_back(k);
+    for (const auto& kv : groups) {
+        std::printf("batch time=%s cases=%zu:", cases[kv.second[0]].c.time_recipe.c_str(), kv.second.size());
+        for (size_t k : kv.second) std::printf(" %s(%s)", cases[k].c.name.c_str(), cases[k].c.convection.c_str());
+        std::printf("\n");
+    }
+    if (o.describe_only) return unsupported ? 3 : 0;
+    int rc_all = 0;
+    std::vector<std::string> results(cases.size());  // JSON lines, printed in the order given
+    for (const auto& kv : groups) {
+        const BatchCase& first = cases[kv.second[0]];
+        sfg_numerics_desc nd{first.recipe, kv.first, o.precision, first.c.gamma, first.c.cfl, first.c.max_dt};
+        // the slab: every grid's bytes (asked of a probe batch), plus room
+        size_t need = 0;
+        {
+            sfg_batch probe = nullptr;
+            if (sfg_batch_create(&nd, 1u << 20, 1, nullptr, &probe) != SFG_OK) {
+                std::fprintf(stderr, "sfg_run: %s\n", sfg_last_error());
+                return 1;
+            }
+            for (size_t k : kv.second) {
+                size_t bytes = 0;
+                if (sfg_batch_instance_bytes(probe, &cases[k].g.grid, &bytes) != SFG_OK) {
+                    std::fprintf(stderr, "sfg_run: %s: %s\n", cases[k].dir.c_str(), sfg_last_error());
+                    sfg_batch_destroy(probe);
+                    return 1;
+                }
+                need += bytes + 4096;
+            }
+            sfg_batch_destroy(probe);
+        }
+        sfg_batch b = nullptr;
+        if (sfg_batch_create(&nd, need + (64u << 20), int(kv.second.size()), nullptr, &b) != SFG_OK) {
+            std::fprintf(stderr, "sfg_run: %s\n", sfg_last_error());
+            return 1;
+        }
+        if (o.variant && sfg_batch_set_variant(b, o.variant) != SFG_OK) {
+            std::fprintf(stderr, "sfg_run: %s\n", sfg_last_error());
+            sfg_batch_destroy(b);
+            return 1;
+        }
+        const auto w0 = std::chrono::steady_clock::now();
+        for (size_t k : kv.second) {
+            BatchCase& bc = cases[k];
+            sfg_numerics_desc own{bc.recipe, bc.tid, o.precision, bc.c.gamma, bc.c.cfl, bc.c.max_dt};
+            if (sfg_batch_add_laws(b, &bc.g.grid, &own, bc.g.laws, bc.g.q.data(), bc.c.end_time, 0, &bc.slot) != SFG_OK ||
+                sfg_batch_set_write_interval(b, bc.slot, bc.c.write_interval) != SFG_OK) {
+                std::fprintf(stderr, "sfg_run: %s: %s\n", bc.dir.c_str(), sfg_last_error());
+                sfg_batch_destroy(b);
+                return 1;
+            }
+        }
+        int active = 0;
+        if (sfg_batch_step(b, std::numeric_limits<int>::max(), o.graph_steps, &active) != SFG_OK) {
+            std::fprintf(stderr, "sfg_run: %s\n", sfg_last_error());
+            sfg_batch_destroy(b);
+            return 1;
+        }
+        const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - w0).count();
+        for (size_t k : kv.second) {
+            BatchCase& bc = cases[k];
+            double t = 0;
+            int64_t steps = 0;
+            int running = 0;
+            uint32_t bits = 0;
+            int rc = sfg_batch_status(b, bc.slot, &t, &steps, &running, &bits);
+            std::vector<double> q(bc.g.q.size());
+            if (!rc) rc = sfg_batch_download(b, bc.slot, q.data());
+            if (!rc && bits) rc = SFG_ERR_STATE;
+            if (!rc && o.write) {
+                const std::string out_dir = bc.c.dir + "/" + bc.c.output_dir;
+                mkdir(out_dir.c_str(), 0755);
+                const std::string path = out_dir + "/" + bc.c.job_name + "_final.vts";
+                if (!write_vts(path, vts_layout(bc.c, bc.g, {}), q, bc.c.gamma)) rc = SFG_ERR_ARG;
+                else std::printf("write t=%.17g %s\n", t, path.c_str());
+            }
+            if (!rc && !o.dump_dir.empty()) {
+                std::ofstream f(o.dump_dir + "/" + bc.c.name + ".bin", std::ios::binary);
+                f.write(reinterpret_cast<const char*>(q.data()), std::streamsize(q.size() * sizeof(double)));
+                if (!f) rc = SFG_ERR_ARG;
+            }
+            if (rc) rc_all = 1;
+            char line[1024];
+            std::snprintf(line, sizeof line,
+                          "{\"case\": \"%s\", \"mode\": \"batch\", \"recipe\": \"%s\", \"time_recipe\": \"%s\", "
+                          "\"dim\": %d, \"nodes\": [%d, %d, %d], \"steps\": %lld, \"time\": %.17g, \"status\": %d, "
+                          "\"status_bits\": %u, \"batch_wall_s\": %.6f}",
+                          json_escape(bc.c.name).c_str(), bc.c.convection.c_str(), bc.c.time_recipe.c_str(),
+                          bc.g.grid.dim, bc.g.nodes[0], bc.g.nodes[1], bc.g.nodes[2], (long long)steps, t, rc, bits,
+                          wall);
+            results[k] = line;
+        }
+        sfg_batch_destroy(b);
+    }
+    for (const auto& line : results) std::printf("%s\n", line.c_str());
+    if (rc_all) return 1;
+    return unsupported ? 3 : 0;
+}
+
 int main(int argc, char** argv) {
     if (argc == 2 && std::strcmp(argv[1], "--selftest") == 0) return selftest();
     Options o;
@@ -442,9 +605,14 @@ int main(int argc, char** argv) {
         else if (a == "--restart") o.restart = next();
         else if (a == "--no-write") o.write = false;
         else if (a == "--describe") o.describe_only = true;
+        else if (a == "--batch") o.batch = true;
+        else if (a == "--dump-dir") o.dump_dir = next();
+        else if (a == "--variant") o.variant = std::atoi(next().c_str());
         else if (!a.empty() && a[0] == '-') return usage();
+        else if (o.batch) o.batch_dirs.push_back(a);
         else o.dir = a;
     }
+    if (o.batch) return o.batch_dirs.empty() ? usage() : run_batch(o);
     if (o.dir.empty() || (o.mode != "graph" && o.mode != "plan")) return usage();
     try {
         const CaseSpec c = load_case(o.dir);

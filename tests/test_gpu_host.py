@@ -366,3 +366,42 @@ def test_curved_block_vts_carries_the_generated_points(tmp_path):
     # the second plane: z = 0.01, the same x, y (to the round-off of the
     # transfinite sums)
     assert np.abs(pts[1, ..., 2] - 0.01).max() <= 1e-15 and np.abs(pts[1, ..., :2] - pts[0, ..., :2]).max() <= 1e-14
+
+
+# ---- several case directories on the batched provider
+
+def test_batch_mode_equals_single_case_runs(tmp_path):
+    """`sfg_run --batch` over case directories of every end kind (a law
+    tube, a tube without a Left condition, a 2-D box on TENO5 + Roe with its
+    own CFL, and a forwardEuler WENO7 case in a second batch): each ends at
+    its own endTime with the step count and the time of its single-case run
+    (output clipping included) and its final state within 1e-12 (the same
+    bits on the tile kernels; a 1-D FP64 case alone may take the whole-run
+    cluster kernel, equal to round-off)."""
+    root = str(tmp_path)
+    box = {"Left": "zeroGradient", "Right": "zeroGradient", "sideWalls": "zeroGradient", "frontBack": "empty"}
+    frozen = {"Right": "zeroGradient", "sideWalls": "empty", "frontBack": "empty"}
+    dirs = [write_case(root, "law", cells=(400, 1, 1), box_hi=(1.0, 0.1, 0.1), end_time=0.1, write_interval=0.05,
+                       boundaries=LAW_CASE),
+            write_case(root, "frozen", cells=(300, 1, 1), box_hi=(1.0, 0.1, 0.1), end_time=0.08, write_interval=0.03,
+                       boundaries=frozen),
+            write_case(root, "box", cells=(48, 24, 1), box_hi=(2.0, 1.0, 0.1), end_time=0.07, write_interval=0.02,
+                       cfl=0.4, convection="teno5Roe", boundaries=box),
+            write_case(root, "euler7", cells=(100, 20, 1), box_hi=(100.0, 20.0, 0.1), n_ghost=4, end_time=0.05,
+                       write_interval=0.05, convection="weno7Rusanov", time="forwardEuler",
+                       left=(1.0, 0.0, 1e5), right=(0.125, 0.0, 1e4),
+                       boundaries={"Right": "zeroGradient", "sideWalls": "zeroGradient", "frontBack": "empty"})]
+    dump = os.path.join(root, "dump")
+    os.makedirs(dump)
+    r = subprocess.run([RUNNER, "--batch", *dirs, "--dump-dir", dump, "--no-write"], capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    lines = [json.loads(l) for l in r.stdout.splitlines() if l.startswith("{")]
+    assert [l["case"] for l in lines] == ["law", "frozen", "box", "euler7"]
+    assert "batch time=SSPRK3 cases=3" in r.stdout and "batch time=forwardEuler cases=1" in r.stdout
+    for d, got in zip(dirs, lines):
+        alone, q, _ = run_case(d, "--no-write")
+        assert got["status"] == 0 and got["steps"] == alone["steps"], (got, alone)
+        assert abs(got["time"] - alone["time"]) <= 1e-14
+        qb = np.fromfile(os.path.join(dump, got["case"] + ".bin"))
+        assert rel_linf_vec(qb, q).max() <= 1e-12, got["case"]

@@ -300,3 +300,25 @@ def test_block_geometry_is_the_reference_generators(runner, tmp_path, name):
     assert np.array_equal(np.fromfile(fm).reshape(want.shape), want)
     line = out.split("metric identity residual ")[1].splitlines()[0]
     assert float(line.split(",")[0]) == float("%.3g" % res) and res <= tol
+
+
+def test_batch_mode_groups_cases_and_reports_the_rest(runner, tmp_path):
+    """`sfg_run --batch` groups case directories by time recipe (one batch
+    each) and reports the cases the batched kernels do not run, without a
+    GPU under --describe."""
+    a = write_case(str(tmp_path), "a", cells=(200, 1, 1), box_hi=(1.0, 0.1, 0.1))
+    b = write_case(str(tmp_path), "b", cells=(30, 20, 1), box_hi=(1.5, 1.0, 0.1), convection="teno5Roe",
+                   boundaries={"Left": "zeroGradient", "Right": "zeroGradient", "sideWalls": "zeroGradient",
+                               "frontBack": "empty"})
+    c = write_case(str(tmp_path), "c", cells=(100, 1, 1), box_hi=(1.0, 0.1, 0.1), convection="weno7Rusanov",
+                   time="forwardEuler")
+    d = write_case(str(tmp_path), "d", cells=(100, 1, 1), box_hi=(1.0, 0.1, 0.1), convection="weno5LaxFriedrichs")
+    e = write_case(str(tmp_path), "e", cells=(8, 8, 8), box_hi=(1, 1, 1), boundaries=ALL_ZG)
+    r = run(runner, "--batch", a, b, c, d, e, "--describe")
+    assert r.returncode == 3, r.stdout + r.stderr
+    assert "batch time=SSPRK3 cases=2: a(weno5Rusanov) b(teno5Roe)" in r.stdout
+    assert "batch time=forwardEuler cases=1: c(weno7Rusanov)" in r.stdout
+    assert "d: convection 'weno5LaxFriedrichs': the batched kernels provide Rusanov and Roe faces" in r.stderr
+    assert "e: 3-D grids run on single-grid solvers only" in r.stderr
+    r2 = run(runner, "--batch", a, c, "--describe")
+    assert r2.returncode == 0
