@@ -92,6 +92,86 @@ std::string convection_token(const Node& nu) {
     return scheme + flux;
 }
 
+bool switched_on(const Node& n, const std::string& key) {
+    const Node* v = n.get(key);
+    return v && v->is_scalar() && v->boolean();
+}
+
+// Terms a numerics file switches on beyond convection.  A `diffusion:
+// default:` scheme is live unless `transport: enable: false` turns it off
+// (SF_nativeBinding.cpp:454-462); `sources: default:` names the gravity /
+// MRF / wall-heat sources (SF_nativeDecode.cpp:1074-1078, parsed by
+// parseSourceKinds, SF_modelConfigParser.h:14-33, none/off/false naming
+// none).
+void numerics_physics(const Node& nu, std::vector<std::string>& out) {
+    bool disabled = false;
+    if (const Node* tr = nu.get("transport"))
+        if (const Node* en = tr->get("enable")) disabled = !en->boolean();
+    if (const Node* df = nu.get("diffusion"))
+        if (const Node* d = df->get("default"))
+            if (!disabled)
+                out.push_back("viscous terms (numerics diffusion '" + d->str() +
+                              "' without transport.enable: false): the provider implements the Euler equations");
+    if (const Node* src = nu.get("sources"))
+        if (const Node* d = src->get("default")) {
+            const std::string s = lower(d->str());
+            if (!s.empty() && s != "none" && s != "off" && s != "false")
+                out.push_back("source terms '" + d->str() + "' (numerics sources)");
+        }
+}
+
+// Switches of the model modules (models/models.yaml entries by type) and of
+// the equation system and ILW entries of solvers/solvers.yaml that select
+// physics beyond the inviscid single-fluid Euler equations.  Gravity and MRF
+// modules act only through numerics sources; geometry entries only through
+// an immersed boundary.
+void module_physics(const std::string& dir, std::vector<std::string>& out) {
+    std::vector<std::pair<std::string, std::string>> modules;  // type, file
+    const std::string reg = join(dir, "models/models.yaml");
+    if (exists(reg)) {
+        const Node r = load_yaml_file(reg);
+        for (const auto& kv : r.fields)
+            if (kv.second.is_map() && kv.second.get("type") && kv.second.get("file"))
+                modules.emplace_back(kv.second.at("type").str(), join(dir, kv.second.at("file").str()));
+    } else {
+        for (const char* t : {"IBM", "turbulence", "multiPhase", "phaseChange", "thermophysical"})
+            modules.emplace_back(t, join(dir, std::string("models/") + t + ".yaml"));
+    }
+    for (const auto& m : modules) {
+        if (!exists(m.second)) continue;
+        const Node f = load_yaml_file(m.second);
+        const Node* body = f.get(m.first);  // `IBM: {enabled: ...}` or top-level keys
+        const Node& b = body && body->is_map() ? *body : f;
+        if (m.first == "IBM" && switched_on(b, "enabled")) {
+            out.push_back("immersed boundary (" + m.second.substr(dir.size() + 1) + " enabled)");
+        } else if (m.first == "turbulence" && switched_on(b, "enabled")) {
+            const std::string st = b.get("simulationType") ? lower(b.at("simulationType").str()) : "";
+            if (st != "laminar" && st != "dns" && st != "none")
+                out.push_back("turbulence model (simulationType '" + b.at("simulationType").str() + "')");
+        } else if (m.first == "multiPhase" && switched_on(f, "multiPhases")) {
+            out.push_back("multiphase flow (" + m.second.substr(dir.size() + 1) + ")");
+        } else if (m.first == "phaseChange" && switched_on(b, "enabled")) {
+            out.push_back("phase change (" + m.second.substr(dir.size() + 1) + ")");
+        } else if (m.first == "thermophysical") {
+            if (const Node* t = f.get("temperature"))
+                if (switched_on(*t, "enabled")) out.push_back("temperature equation (thermophysical temperature.enabled)");
+        }
+    }
+    const std::string eq = registry_file(dir, "solvers/solvers.yaml", "equations", "solvers/equations.yaml");
+    if (exists(eq)) {
+        const Node e = load_yaml_file(eq);
+        if (const Node* p = e.get("preset"))
+            if (p->str() != "compressible")
+                out.push_back("equation preset '" + p->str() + "': the provider implements 'compressible'");
+    }
+    const std::string ilw = registry_file(dir, "solvers/solvers.yaml", "ILW", "solvers/ILW.yaml");
+    if (exists(ilw)) {
+        const Node f = load_yaml_file(ilw);
+        const Node* body = f.get("ILW");
+        if (body && switched_on(*body, "enabled")) out.push_back("inverse Lax-Wendroff boundaries (ILW enabled)");
+    }
+}
+
 // One patch entry: `zeroGradient`, `{type: fixedValue, value: V}` or the
 // compact `{fixedValue: V}` (compactBoundary, SF_case.cpp:22-29).
 FieldCondition condition(const Node& n, const std::string& what) {
@@ -147,8 +227,10 @@ CaseSpec load_case(const std::string& dir) {
     if (const Node* tr = nu.get("transport"))
         if (const Node* en = tr->get("enable"))
             if (en->boolean()) throw Unsupported("transport enabled: viscous terms are outside the explicit Euler path");
+    numerics_physics(nu, c.unsupported_physics);
     const std::string alg = registry_file(dir, "solvers/solvers.yaml", "algorithm", "solvers/algorithm.yaml");
     c.algorithm = exists(alg) ? load_yaml_file(alg).at("type").str() : "densityBase";
+    module_physics(dir, c.unsupported_physics);
     // ---- thermodynamics
     const std::string th = registry_file(dir, "models/models.yaml", "thermoDynamics", "models/thermoDynamics.yaml");
     if (exists(th)) {
@@ -345,6 +427,11 @@ int end_kind(const PatchConditions& pc, const char* patch, sfg_boundary_law& law
 GridSetup build_grid(const CaseSpec& c) {
     if (c.algorithm != "densityBase")
         throw Unsupported("algorithm '" + c.algorithm + "': the provider implements the densityBase explicit path");
+    if (!c.unsupported_physics.empty()) {
+        std::string why = c.unsupported_physics[0];
+        for (size_t i = 1; i < c.unsupported_physics.size(); ++i) why += "; " + c.unsupported_physics[i];
+        throw Unsupported(why);
+    }
     GridSetup g;
     bool active[3];
     for (int d = 0; d < 3; ++d) {

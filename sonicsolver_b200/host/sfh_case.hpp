@@ -5,7 +5,11 @@
 //   solvers/solvers.yaml -> runtime (startTime, endTime, CFL, writeControl,
 //     writeInterval, writeInitial, output.jobName / outputDir, maxDeltaT),
 //     numerics (time.default, terms.convection), algorithm (type);
-//   models/models.yaml -> thermoDynamics (perfectGas gamma, R);
+//   models/models.yaml -> thermoDynamics (perfectGas gamma, R, transport
+//     mu), and the switches of the IBM, MRF, turbulence, multiPhase,
+//     phaseChange and thermophysical modules (gravity and geometry entries
+//     are inert on the density-based path);
+//   solvers/solvers.yaml -> equations (preset), ILW (enabled);
 //   mesh/mesh.yaml -> generation (JSON: vertices, blocks[0].vertices /
 //     cells / grading, scale, nGhost, arc edges; one block: an axis-aligned
 //     box runs on the uniform Cartesian path, a graded or curved block with
@@ -77,6 +81,11 @@ struct CaseSpec {
     };
     std::vector<DeclaredField> declared_fields;
     InitialValue rho, U, p;
+    // enabled physics outside the inviscid single-fluid Euler equations (an
+    // immersed boundary, MRF, a turbulence model, multiphase, phase change, a
+    // temperature equation, viscous transport, ILW, a non-compressible
+    // equation preset), one reason each; build_grid refuses a case with any
+    std::vector<std::string> unsupported_physics;
 };
 
 CaseSpec load_case(const std::string& dir);
@@ -94,9 +103,10 @@ struct GridSetup {
 // keeps the initial ghost state there and advances the boundary node).
 // A patch whose rho, U and p are all zeroGradient is SFG_BC_TRANSMISSIVE;
 // one with fixedValue or symmetry laws is SFG_BC_LAW with those laws.
-// Throws Unsupported for what this provider does not run (periodic ends on
-// a graded or curved block; a patch with conditions for only some of rho, U,
-// p).
+// Throws Unsupported for what this provider does not run (an algorithm other
+// than densityBase; enabled physics listed in unsupported_physics; periodic
+// ends on a graded or curved block; a patch with conditions for only some of
+// rho, U, p).
 GridSetup build_grid(const CaseSpec& c);
 
 }  // namespace sfh

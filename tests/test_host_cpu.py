@@ -93,8 +93,10 @@ def test_parse_error_names_file_and_line(runner, tmp_path):
 def test_reference_case_directories(runner):
     """Every case directory of the reference's test tree is read without a
     parse error.  The three Sod cases (no Left condition: frozen ghosts;
-    TENO5 + Steger-Warming and WENO7 + Rusanov) resolve and plan; every other
-    case is reported as not supported by this provider, with its reason."""
+    TENO5 + Steger-Warming and WENO7 + Rusanov) and the inviscid GUI Sod case
+    resolve and plan; every other case is reported as not supported by this
+    provider, with its reason (the immersed-boundary, thermal and mixture
+    cases by the physics they switch on, although their meshes would run)."""
     dirs = sorted(os.path.dirname(os.path.join(dp, f)) for dp, _, fs in os.walk(REFERENCE_TESTS)
                   for f in fs if f == "case.yaml")
     assert len(dirs) > 10
@@ -110,8 +112,64 @@ def test_reference_case_directories(runner):
                 assert "bc=20/00/00" in r.stdout
         else:
             assert "unsupported:" in r.stderr
-    for case in ("sodCase", "sodCase_weno7", "sodCase_weno7_t0p2"):
-        assert os.path.join("Sod", case) in resolved
+    assert sorted(resolved) == sorted([os.path.join("Sod", c) for c in
+                                       ("sodCase", "sodCase_weno7", "sodCase_weno7_t0p2")] +
+                                      [os.path.join("guiCase", "sodGuiFromSfm")])
+    reasons = {"thermalCase": "temperature equation", "mixtureCase": "multiphase flow",
+               "variationalIBMCase": "immersed boundary",
+               os.path.join("IBM", "cylinderFlowPeskin"): "viscous terms"}
+    for rel, why in reasons.items():
+        r = run(runner, os.path.join(REFERENCE_TESTS, rel), "--describe")
+        assert r.returncode == 3 and why in r.stderr, (rel, r.stderr)
+
+
+def _add_module(d, name, body):
+    """Registers models/<name>.yaml (type <name>) with `body` in a case."""
+    with open(os.path.join(d, "models", "models.yaml"), "a") as f:
+        f.write(f"{name}:\n  type: {name}\n  file: models/{name}.yaml\n")
+    with open(os.path.join(d, "models", f"{name}.yaml"), "w") as f:
+        f.write(f"SonicFile:\n  object: models\n  type: {name}\n" + body)
+
+
+@pytest.mark.parametrize("module,body,why", [
+    ("IBM", "IBM:\n  enabled: true\n  type: ghost\n", "immersed boundary"),
+    ("turbulence", "enabled: true\nsimulationType: RAS\n", "turbulence model (simulationType 'RAS')"),
+    ("multiPhase", "multiPhases: true\n", "multiphase flow"),
+    ("phaseChange", "phaseChange:\n  enabled: true\n", "phase change"),
+    ("thermophysical", "temperature:\n  enabled: true\n  fieldName: T\n", "temperature equation"),
+])
+def test_physics_gate_refuses_enabled_modules(runner, tmp_path, module, body, why):
+    """A model module that switches on physics beyond the inviscid Euler
+    equations makes the case unsupported (exit 3, the reason on stderr)."""
+    d = write_case(str(tmp_path), "gate", cells=(40, 1, 1), box_hi=(1.0, 0.1, 0.1))
+    assert run(runner, d, "--describe").returncode == 0
+    _add_module(d, module, body)
+    r = run(runner, d, "--describe")
+    assert r.returncode == 3 and why in r.stderr, r.stderr
+
+
+def test_physics_gate_inert_modules(runner, tmp_path):
+    """Disabled modules, a laminar or DNS turbulence entry, gravity (which
+    acts only through numerics sources) and a diffusion scheme switched off
+    by transport.enable: false leave the case runnable; a live diffusion
+    scheme or a numerics source term does not."""
+    d = write_case(str(tmp_path), "inert", cells=(40, 1, 1), box_hi=(1.0, 0.1, 0.1), numerics_form="scheme")
+    _add_module(d, "IBM", "IBM:\n  enabled: false\n")
+    _add_module(d, "turbulence", "enabled: true\nsimulationType: DNS\n")
+    _add_module(d, "gravity", "value: [9.8, 0, 0]\n")
+    _add_module(d, "thermophysical", "temperature:\n  enabled: false\n")
+    r = run(runner, d, "--describe")
+    assert r.returncode == 0, r.stderr
+    num = os.path.join(d, "solvers", "numerics.yaml")
+    text = open(num).read()
+    with open(num, "w") as f:
+        f.write(text.replace("  enable: false\n", ""))
+    r = run(runner, d, "--describe")
+    assert r.returncode == 3 and "viscous terms" in r.stderr, r.stderr
+    with open(num, "w") as f:
+        f.write(text + "sources:\n  default: Gravity\n")
+    r = run(runner, d, "--describe")
+    assert r.returncode == 3 and "source terms 'Gravity'" in r.stderr, r.stderr
 
 
 LAW_BOUNDARIES = {
