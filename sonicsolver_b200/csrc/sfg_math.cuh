@@ -258,18 +258,57 @@ __device__ __forceinline__ T weno7_core(const T* v, unsigned& flags) {
 // keep_mask() is the cut-off decision alone (bit k set = sub-stencil k kept);
 // core() is the reconstruction built on it.  `cut` accumulates the number of
 // cut sub-stencils.
+//
+// The sub-stencil polynomials and smoothness indicators are written with
+// every rounding fixed (fma where two operations fuse, the _rn intrinsics
+// where they must not): left to the compiler, products shared between them
+// (2 v2, 3 v2, ...) fuse or not depending on the code around them, so the
+// same inputs could round differently in two call sites.
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+
+// 6 x the three sub-stencil reconstructions (p_k of the reference).
+template <typename T>
+__device__ __forceinline__ void teno_polys(const T* v, T& p0, T& p1, T& p2) {
+    p0 = fma(T(11), v[2], fma(T(-7), v[1], mul_rn(T(2), v[0])));
+    p1 = fma(T(2), v[3], fma(T(5), v[2], -v[1]));
+    p2 = add_rn(fma(T(5), v[3], mul_rn(T(2), v[2])), -v[4]);
+}
+
 template <typename T>
 __device__ __forceinline__ void teno_betas(const T* v, T& b0, T& b1, T& b2) {
-    const T t0 = v[0] - T(2) * v[1] + v[2], r0 = v[0] - T(4) * v[1] + T(3) * v[2];
-    const T t1 = v[1] - T(2) * v[2] + v[3], r1 = v[1] - v[3];
-    const T t2 = v[2] - T(2) * v[3] + v[4], r2 = T(3) * v[2] - T(4) * v[3] + v[4];
+    const T t0 = add_rn(fma(T(-2), v[1], v[0]), v[2]), r0 = fma(T(3), v[2], fma(T(-4), v[1], v[0]));
+    const T t1 = add_rn(fma(T(-2), v[2], v[1]), v[3]), r1 = add_rn(v[1], -v[3]);
+    const T t2 = add_rn(fma(T(-2), v[3], v[2]), v[4]), r2 = add_rn(fma(T(-4), v[3], mul_rn(T(3), v[2])), v[4]);
     const T c13 = T(13.0 / 12.0);
-    b0 = c13 * (t0 * t0) + T(0.25) * (r0 * r0);
-    b1 = c13 * (t1 * t1) + T(0.25) * (r1 * r1);
-    b2 = c13 * (t2 * t2) + T(0.25) * (r2 * r2);
+    b0 = fma(c13, mul_rn(t0, t0), mul_rn(T(0.25), mul_rn(r0, r0)));
+    b1 = fma(c13, mul_rn(t1, t1), mul_rn(T(0.25), mul_rn(r1, r1)));
+    b2 = fma(c13, mul_rn(t2, t2), mul_rn(T(0.25), mul_rn(r2, r2)));
 }
 
 template <typename T> struct Teno;
+
+// d0 p0 + d1 p1 + d2 p2 with its roundings fixed (one product, two fused
+// multiply-adds), so a weight set given as constants and the same set chosen
+// at run time round alike.
+__device__ __forceinline__ double teno_sum64(double d0, double d1, double d2, double p0, double p1, double p2) {
+    return fma(d2, p2, fma(d1, p1, d0 * p0));
+}
+
+// A smooth sub-stencil triple keeps all three sub-stencils, which the FP64
+// cut-off finds only after its division: with tau <= 4 e_min (e_k = b_k +
+// 1e-40) every g_k = 1 + tau/e_k lies in [1, 5] up to a few ulps, so G_k >=
+// 1 > lim = 1e-5 sum G <= 0.47 and the mask is 7.  b_max <= 1e30 keeps the
+// products e0 e1 e2 and the shared reciprocal of two of them finite and
+// normal, so the cut-off path raises no non-finite flag either; NaN or
+// infinite indicators fail the test.  The weights for mask 7 are then the
+// cut-off path's to the bit.
+__device__ __forceinline__ bool teno_smooth64(const double (&b)[3], double tau) {
+    const double em = fmin(b[0], fmin(b[1], b[2])) + 1e-40;
+    return tau <= 4.0 * em && fmax(b[0], fmax(b[1], b[2])) <= 1e30;
+}
 
 // FP64 keeps the reference's gamma_k = (1 + tau5/(b_k+eps))^6 and tests
 // gamma_k < CT * sum(gamma) (the reference divides; the comparison is the same
@@ -292,11 +331,11 @@ template <> struct Teno<double> {
         return int(!(G0 < lim)) | (int(!(G1 < lim)) << 1) | (int(!(G2 < lim)) << 2);
     }
     static __device__ __forceinline__ double core(const double* v, unsigned& flags, unsigned& cut) {
-        const double p0 = 2.0 * v[0] - 7.0 * v[1] + 11.0 * v[2];
-        const double p1 = -v[1] + 5.0 * v[2] + 2.0 * v[3];
-        const double p2 = 2.0 * v[2] + 5.0 * v[3] - v[4];
-        double b0, b1, b2;
+        double p0, p1, p2, b0, b1, b2;
+        teno_polys<double>(v, p0, p1, p2);
         teno_betas<double>(v, b0, b1, b2);
+        const double bb[3] = {b0, b1, b2};
+        if (teno_smooth64(bb, fabs(b0 - b2))) return teno_sum64(0.1, 0.6, 0.3, p0, p1, p2) * (1.0 / 6.0);  // mask 7
         const int m = keep_mask(b0, b1, b2, flags);
         cut += 3 - __popc(m);
         if (m == 0) { flags |= FLAG_TENO_CUTOFF; return 0.0; }
@@ -305,7 +344,7 @@ template <> struct Teno<double> {
         const double inv6act = m == 7 ? 1.0 / 6.0 : m == 6 ? 1.0 / 5.4 : m == 5 ? 1.0 / 2.4 : m == 4 ? 1.0 / 1.8
                              : m == 3 ? 1.0 / 4.2 : m == 2 ? 1.0 / 3.6 : 1.0 / 0.6;
         const double d0 = (m & 1) ? 0.1 : 0.0, d1 = (m & 2) ? 0.6 : 0.0, d2 = (m & 4) ? 0.3 : 0.0;
-        return (d0 * p0 + d1 * p1 + d2 * p2) * inv6act;
+        return teno_sum64(d0, d1, d2, p0, p1, p2) * inv6act;
     }
 };
 
@@ -339,6 +378,21 @@ __device__ __forceinline__ void teno_keep32x2(float2 b0, float2 b1, float2 b2, f
     keep[2] = f2(ge_one(G2.x, lim.x), ge_one(G2.y, lim.y));
 }
 
+// A smooth stencil pair keeps every sub-stencil, which the cut-off would
+// find only after its reciprocals: with tau = |B0 - B2| <= 4 e_min (e_min =
+// min B + eps <= 1e30) in both lanes, t = e_min / (e_min + tau) >= 0.2 up to
+// a few ulps, every x_k >= t, so G_k >= 6.39e-5 > 2 lim (lim = 1e-5 sum G <=
+// 3.0001e-5): teno_keep32x2 would return k = 1 for all three.  The test
+// fails for NaN or infinite indicators (they take the cut-off path and its
+// non-finite watch), and a pair that passes has finite differences, so the
+// weights computed with k = 1 are the cut-off path's to the bit.
+__device__ __forceinline__ bool teno_smooth2(const float2 (&B)[3]) {
+    const float2 em = add2(f2(fminf(B[0].x, fminf(B[1].x, B[2].x)), fminf(B[0].y, fminf(B[1].y, B[2].y))),
+                           f2(TENO32_EPS));
+    const float2 d02 = sub2(B[0], B[2]);
+    return fabsf(d02.x) <= 4.f * em.x && fabsf(d02.y) <= 4.f * em.y && em.x <= 1e30f && em.y <= 1e30f;
+}
+
 template <> struct Teno<float> {
     static __device__ __forceinline__ int keep_mask(float b0, float b1, float b2, unsigned& flags) {
         float2 k[3];
@@ -348,17 +402,18 @@ template <> struct Teno<float> {
         return int(k[0].x != 0.f) | (int(k[1].x != 0.f) << 1) | (int(k[2].x != 0.f) << 2);
     }
     static __device__ __forceinline__ float core(const float* v, unsigned& flags, unsigned& cut) {
-        const float p0 = 2.f * v[0] - 7.f * v[1] + 11.f * v[2];
-        const float p1 = -v[1] + 5.f * v[2] + 2.f * v[3];
-        const float p2 = 2.f * v[2] + 5.f * v[3] - v[4];
-        float b0, b1, b2;
+        float p0, p1, p2, b0, b1, b2;
+        teno_polys<float>(v, p0, p1, p2);
         teno_betas<float>(v, b0, b1, b2);
+        const float2 bb[3] = {f2(b0), f2(b1), f2(b2)};
+        if (teno_smooth2(bb))  // mask 7 (teno_smooth2 on both lanes of the broadcast)
+            return __fdividef(fmaf(0.3f, p2, fmaf(0.6f, p1, 0.1f * p0)), 6.f * ((0.1f + 0.6f) + 0.3f));
         const int m = keep_mask(b0, b1, b2, flags);
         cut += 3 - __popc(m);
         const float d0 = (m & 1) ? 0.1f : 0.f, d1 = (m & 2) ? 0.6f : 0.f, d2 = (m & 4) ? 0.3f : 0.f;
-        const float act = d0 + d1 + d2;
+        const float act = (d0 + d1) + d2;
         if (!(act > 0.f)) { flags |= FLAG_TENO_CUTOFF; return 0.f; }
-        return __fdividef(d0 * p0 + d1 * p1 + d2 * p2, 6.f * act);
+        return __fdividef(fmaf(d2, p2, fmaf(d1, p1, d0 * p0)), 6.f * act);
     }
 };
 
@@ -401,13 +456,17 @@ __device__ __forceinline__ void teno5_pair64(const double* l, const double* r, d
 #pragma unroll
     for (int side = 0; side < 2; ++side) {
         const double* v = v2[side];
-        p[side][0] = 2.0 * v[0] - 7.0 * v[1] + 11.0 * v[2];
-        p[side][1] = -v[1] + 5.0 * v[2] + 2.0 * v[3];
-        p[side][2] = 2.0 * v[2] + 5.0 * v[3] - v[4];
+        teno_polys<double>(v, p[side][0], p[side][1], p[side][2]);
         teno_betas<double>(v, b[side][0], b[side][1], b[side][2]);
         tau[side] = fabs(b[side][0] - b[side][2]);
         for (int k = 0; k < 3; ++k) e[side][k] = b[side][k] + 1e-40;
         prod[side] = e[side][0] * (e[side][1] * e[side][2]);
+    }
+    if (teno_smooth64(b[0], tau[0]) && teno_smooth64(b[1], tau[1])) {
+        // every sub-stencil kept on both sides: the m = 7 weights below
+        wl = teno_sum64(0.1, 0.6, 0.3, p[0][0], p[0][1], p[0][2]) * (1.0 / 6.0);
+        wr = teno_sum64(0.1, 0.6, 0.3, p[1][0], p[1][1], p[1][2]) * (1.0 / 6.0);
+        return;
     }
     const double inv = 1.0 / (prod[0] * prod[1]);
     double out[2];
@@ -428,7 +487,7 @@ __device__ __forceinline__ void teno5_pair64(const double* l, const double* r, d
         const double inv6act = m == 7 ? 1.0 / 6.0 : m == 6 ? 1.0 / 5.4 : m == 5 ? 1.0 / 2.4 : m == 4 ? 1.0 / 1.8
                              : m == 3 ? 1.0 / 4.2 : m == 2 ? 1.0 / 3.6 : m == 1 ? 1.0 / 0.6 : 0.0;
         const double d0 = (m & 1) ? 0.1 : 0.0, d1 = (m & 2) ? 0.6 : 0.0, d2 = (m & 4) ? 0.3 : 0.0;
-        out[side] = (d0 * p[side][0] + d1 * p[side][1] + d2 * p[side][2]) * inv6act;
+        out[side] = teno_sum64(d0, d1, d2, p[side][0], p[side][1], p[side][2]) * inv6act;
     }
     wl = out[0];
     wr = out[1];
@@ -752,17 +811,28 @@ __device__ __forceinline__ float2 weno5_core2(const float2* v, float2& bad) {
 // smoothness indicators, the cut-off (teno_keep32x2) and the weights.  With
 // `count` (a launch-uniform switch: the cut-off accounting of
 // sfg_set_counting), `kept` accumulates the kept sub-stencils of each lane.
+// TENO5 weights from the keep flags k (1 or 0 per lane): the kept linear
+// weights, renormalised.  No all-cut check: the sub-stencil with x = 1
+// always passes (G ~ 1 > lim <= 3e-5, and a NaN lim fails every '<'), so
+// act >= 0.6.
+__device__ __forceinline__ float2 teno5_weights2(const float2 (&k)[3], const float2 (&q)[3], float2 v2) {
+    const float2 d0 = mul2(f2(0.1f), k[0]), d1 = mul2(f2(0.6f), k[1]), d2 = mul2(f2(0.3f), k[2]);
+    const float2 act = fma2(f2(6.f), d0, fma2(f2(6.f), d1, mul2(f2(6.f), d2)));
+    const float2 num = fma2(d0, q[0], fma2(d1, q[1], mul2(d2, q[2])));
+    return fma2(num, rcp2(act), v2);
+}
+
 __device__ __forceinline__ float2 teno5_core2(const float2* v, float2& bad, bool count, float2& kept) {
     float2 B[3], q[3], k[3];
     stencil5x2(v, B, q);
+    if (teno_smooth2(B)) {
+        const float2 all[3] = {f2(1.f), f2(1.f), f2(1.f)};
+        if (count) kept = add2(kept, f2(3.f));
+        return teno5_weights2(all, q, v[2]);
+    }
     teno_keep32x2(B[0], B[1], B[2], k, bad);
     if (count) kept = add2(kept, add2(add2(k[0], k[1]), k[2]));
-    const float2 d0 = mul2(f2(0.1f), k[0]), d1 = mul2(f2(0.6f), k[1]), d2 = mul2(f2(0.3f), k[2]);
-    // No all-cut check: the sub-stencil with x = 1 always passes (G ~ 1 >
-    // lim <= 3e-5, and a NaN lim fails every '<'), so act >= 0.6.
-    const float2 act = fma2(f2(6.f), d0, fma2(f2(6.f), d1, mul2(f2(6.f), d2)));
-    const float2 num = fma2(d0, q[0], fma2(d1, q[1], mul2(d2, q[2])));
-    return fma2(num, rcp2(act), v[2]);
+    return teno5_weights2(k, q, v[2]);
 }
 
 // The eigen-structure as lane pairs, signs folded in, built once per face.
