@@ -290,6 +290,12 @@ __device__ __forceinline__ void teno_betas(const T* v, T& b0, T& b1, T& b2) {
 
 template <typename T> struct Teno;
 
+// The smooth-stencil shortcuts below are taken per warp, when every active
+// lane's stencils pass: a uniform branch, with no divergent paths to
+// reconverge.  A lane whose stencils are smooth but whose warp is not takes
+// the cut-off path, which gives it the same bits.
+__device__ __forceinline__ bool warp_all(bool p) { return __all_sync(__activemask(), p); }
+
 // d0 p0 + d1 p1 + d2 p2 with its roundings fixed (one product, two fused
 // multiply-adds), so a weight set given as constants and the same set chosen
 // at run time round alike.
@@ -335,7 +341,8 @@ template <> struct Teno<double> {
         teno_polys<double>(v, p0, p1, p2);
         teno_betas<double>(v, b0, b1, b2);
         const double bb[3] = {b0, b1, b2};
-        if (teno_smooth64(bb, fabs(b0 - b2))) return teno_sum64(0.1, 0.6, 0.3, p0, p1, p2) * (1.0 / 6.0);  // mask 7
+        if (warp_all(teno_smooth64(bb, fabs(b0 - b2))))
+            return teno_sum64(0.1, 0.6, 0.3, p0, p1, p2) * (1.0 / 6.0);  // mask 7
         const int m = keep_mask(b0, b1, b2, flags);
         cut += 3 - __popc(m);
         if (m == 0) { flags |= FLAG_TENO_CUTOFF; return 0.0; }
@@ -406,7 +413,7 @@ template <> struct Teno<float> {
         teno_polys<float>(v, p0, p1, p2);
         teno_betas<float>(v, b0, b1, b2);
         const float2 bb[3] = {f2(b0), f2(b1), f2(b2)};
-        if (teno_smooth2(bb))  // mask 7 (teno_smooth2 on both lanes of the broadcast)
+        if (warp_all(teno_smooth2(bb)))  // mask 7 (teno_smooth2 on both lanes of the broadcast)
             return __fdividef(fmaf(0.3f, p2, fmaf(0.6f, p1, 0.1f * p0)), 6.f * ((0.1f + 0.6f) + 0.3f));
         const int m = keep_mask(b0, b1, b2, flags);
         cut += 3 - __popc(m);
@@ -462,7 +469,7 @@ __device__ __forceinline__ void teno5_pair64(const double* l, const double* r, d
         for (int k = 0; k < 3; ++k) e[side][k] = b[side][k] + 1e-40;
         prod[side] = e[side][0] * (e[side][1] * e[side][2]);
     }
-    if (teno_smooth64(b[0], tau[0]) && teno_smooth64(b[1], tau[1])) {
+    if (warp_all(teno_smooth64(b[0], tau[0]) && teno_smooth64(b[1], tau[1]))) {
         // every sub-stencil kept on both sides: the m = 7 weights below
         wl = teno_sum64(0.1, 0.6, 0.3, p[0][0], p[0][1], p[0][2]) * (1.0 / 6.0);
         wr = teno_sum64(0.1, 0.6, 0.3, p[1][0], p[1][1], p[1][2]) * (1.0 / 6.0);
@@ -825,7 +832,7 @@ __device__ __forceinline__ float2 teno5_weights2(const float2 (&k)[3], const flo
 __device__ __forceinline__ float2 teno5_core2(const float2* v, float2& bad, bool count, float2& kept) {
     float2 B[3], q[3], k[3];
     stencil5x2(v, B, q);
-    if (teno_smooth2(B)) {
+    if (warp_all(teno_smooth2(B))) {
         const float2 all[3] = {f2(1.f), f2(1.f), f2(1.f)};
         if (count) kept = add2(kept, f2(3.f));
         return teno5_weights2(all, q, v[2]);
