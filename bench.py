@@ -39,12 +39,13 @@ sys.path.insert(0, ROOT)
 #   last axis (stage update): read q_s, R, q0, write q_out (+K RK4)   -> 160
 STATE_BYTES = 40
 # algorithmic FLOPs per face (reconstruction + flux), counted from the kernel
-# source: projection 12/pt, WENO5 core ~58 + 1 div, TENO5 core ~70 + 3 div,
+# source: projection 12/pt, WENO5 core ~58 + 1 div, TENO5 core ~70 + 3 div
+# (the full cut-off; a smooth stencil skips it and does fewer),
 # back-projection 24, Rusanov ~60 + 2 div + 2 sqrt, eigen ~30 + rsqrt.
 # DRAM bytes (read + write) of one stage-1 launch of the fused 2-D tile kernel
 # on the 1024^2 vortex (variant 1: 32 x 15 tiles, variant 2: 22 x 22), from
 # one ncu --set full capture per kernel of the same command line with --quick.
-PROFILED_DRAM_BYTES = {("tile2d", 1, 1024, "fp32flux"): 42.167e6 + 6.357e6,
+PROFILED_DRAM_BYTES = {("tile2d", 1, 1024, "fp32flux"): 42.263e6 + 7.677e6,
                        ("tile2d", 2, 1024, "fp32flux"): 42.036e6 + 4.637e6,
                        ("tile2d", 2, 1024, "fp64"): 42.113e6 + 5.318e6}
 FLOPS_PER_FACE = {"weno5": 6 * 12 + 10 * 59 + 24 + 64 + 34, "teno5": 6 * 12 + 10 * 73 + 24 + 64 + 34}
