@@ -950,20 +950,20 @@ __device__ __forceinline__ void phys_flux_dev(const Ref32& r, const float d[5], 
 // central part from phys_flux_dev, the dissipation from dR - dL.
 template <int AX>
 __device__ __forceinline__ void rusanov_dev(const Ref32& r, const float dL[5], const float dR[5], float gamma,
-                                            float F[5], unsigned& flags) {
+                                            float F[5], unsigned& flags, float scale = 1.f) {
     float fL[5], fR[5], unL, unR, cL, cR, pL, pR;
     phys_flux_dev<AX>(r, dL, gamma, fL, unL, cL, pL, flags);
     phys_flux_dev<AX>(r, dR, gamma, fR, unR, cR, pR, flags);
     const float hl = 0.5f * fmaxf(fabsf(unL) + cL, fabsf(unR) + cR);
 #pragma unroll
-    for (int v = 0; v < 5; ++v) F[v] = 0.5f * (fL[v] + fR[v]) - hl * (dR[v] - dL[v]);
+    for (int v = 0; v < 5; ++v) F[v] = (0.5f * (fL[v] + fR[v]) - hl * (dR[v] - dL[v])) * scale;
 }
 
 // Roe flux deviation: Roe average and eigen-structure from the absolute
 // states, jump dR - dL, central part from phys_flux_dev.
 template <int AX>
 __device__ __forceinline__ void roe_dev(const Ref32& r, const float dL[5], const float dR[5], float gamma, float F[5],
-                                        unsigned& flags) {
+                                        unsigned& flags, float scale = 1.f) {
     constexpr int N = AxisBasis<AX>::N;
     float qL[5], qR[5], fL[5], fR[5], unL, unR, cL, cR, pL, pR;
 #pragma unroll
@@ -1005,7 +1005,7 @@ __device__ __forceinline__ void roe_dev(const Ref32& r, const float dL[5], const
     }
     from_characteristic<AX, float>(e, s, diss);
 #pragma unroll
-    for (int v = 0; v < 5; ++v) F[v] = 0.5f * (fL[v] + fR[v] - diss[v]);
+    for (int v = 0; v < 5; ++v) F[v] = (fL[v] + fR[v] - diss[v]) * (0.5f * scale);
 }
 
 // phys_flux_dev for the (left, right) pair of face states.  Reciprocal and
@@ -1044,7 +1044,7 @@ __device__ __forceinline__ void phys_flux_dev2(const Ref32& r, const float2 d[5]
 
 template <int AX>
 __device__ __forceinline__ void rusanov_dev2(const Ref32& r, const float2 d[5], float gamma, float F[5],
-                                             unsigned& flags) {
+                                             unsigned& flags, float scale = 1.f) {
     float2 f[5], un, c;
     phys_flux_dev2<AX>(r, d, gamma, f, un, c, flags);
     // F = (f_L + f_R)/2 - lam/2 (d_R - d_L) = ((f_L + lam d_L) + (f_R - lam d_R)) / 2
@@ -1053,14 +1053,14 @@ __device__ __forceinline__ void rusanov_dev2(const Ref32& r, const float2 d[5], 
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
         const float2 g = fma2(lr, d[v], f[v]);
-        F[v] = 0.5f * (g.x + g.y);
+        F[v] = (g.x + g.y) * (0.5f * scale);
     }
 }
 
 // face_flux_dev32 with the left / right work paired in float2 (WENO5, TENO5).
 template <int AX, int SCHEME, int FLUX>
 __device__ __forceinline__ void face_flux_dev32x2(const float (&d)[6][5], const Ref32& ref, float gamma, float F[5],
-                                                  unsigned& flags, unsigned& cut, bool count) {
+                                                  unsigned& flags, unsigned& cut, bool count, float scale) {
     float dbar[5], qbar[5];
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
@@ -1097,7 +1097,7 @@ __device__ __forceinline__ void face_flux_dev32x2(const float (&d)[6][5], const 
 #pragma unroll
     for (int v = 0; v < 5; ++v) x2[v] = add2(f2(dbar[v]), dq[v]);  // (left, right) deviations from q_ref
     if constexpr (FLUX == RUSANOV) {
-        rusanov_dev2<AX>(ref, x2, gamma, F, flags);
+        rusanov_dev2<AX>(ref, x2, gamma, F, flags, scale);
     } else {
         float xl[5], xr[5];
 #pragma unroll
@@ -1105,7 +1105,7 @@ __device__ __forceinline__ void face_flux_dev32x2(const float (&d)[6][5], const 
             xl[v] = x2[v].x;
             xr[v] = x2[v].y;
         }
-        roe_dev<AX>(ref, xl, xr, gamma, F, flags);
+        roe_dev<AX>(ref, xl, xr, gamma, F, flags, scale);
     }
 }
 
@@ -1118,13 +1118,15 @@ __device__ __forceinline__ void face_flux_dev32x2(const float (&d)[6][5], const 
 // cancels exactly in every difference dF, so FP32 rounding scales with the
 // distance from the reference state, not with |F|.
 // `count`: the launch's TENO5 cut-off accounting is on (sfg_set_counting);
-// `cut` then receives the cut sub-stencils of the face.
+// `cut` then receives the cut sub-stencils of the face.  `scale` multiplies
+// the flux (a face area): folded into the flux's closing factor 1/2, which
+// is exact, so F * scale rounds as one multiply after the flux would.
 template <int AX, int SCHEME, int FLUX>
 __device__ __forceinline__ void face_flux_dev32(const float (&d)[SchemeInfo<SCHEME>::NST][5], const Ref32& ref,
                                                 float gamma, float F[5], unsigned& flags, unsigned& cut,
-                                                bool count = true) {
+                                                bool count = true, float scale = 1.f) {
     if constexpr (SCHEME == WENO5 || SCHEME == TENO5) {
-        face_flux_dev32x2<AX, SCHEME, FLUX>(d, ref, gamma, F, flags, cut, count);
+        face_flux_dev32x2<AX, SCHEME, FLUX>(d, ref, gamma, F, flags, cut, count, scale);
         return;
     }
     const float (&qref)[5] = ref.q;
@@ -1167,8 +1169,8 @@ __device__ __forceinline__ void face_flux_dev32(const float (&d)[SchemeInfo<SCHE
         xl[v] = dbar[v] + dl[v];
         xr[v] = dbar[v] + dr[v];
     }
-    if constexpr (FLUX == RUSANOV) rusanov_dev<AX>(ref, xl, xr, gamma, F, flags);
-    else roe_dev<AX>(ref, xl, xr, gamma, F, flags);
+    if constexpr (FLUX == RUSANOV) rusanov_dev<AX>(ref, xl, xr, gamma, F, flags, scale);
+    else roe_dev<AX>(ref, xl, xr, gamma, F, flags, scale);
 }
 
 }  // namespace sfg

@@ -178,9 +178,13 @@ __device__ __forceinline__ void tile2d_f32_body(const GridView& g, const StageVi
     float* fx = sq + 5 * SX * SY;   // [5][TY][TX+1]
     float* fy = fx + 5 * NFX;       // [5][TY+1][TX]
     const long long nx = g.n[0], vs = g.vs;
+    // the FP32 reference (velocity, pressure) is made once per tile by one
+    // thread; every face reads it after the staging barrier (the previous
+    // tile's faces are all done before thread 0 gets here again)
+    __shared__ Ref32 sref;
     double qref[5];
     load_ref(g, sv.qs, qref);
-    const Ref32 ref = make_ref32(qref, g.gamma);
+    if (threadIdx.x == 0) sref = make_ref32(qref, g.gamma);
     stage_rows<TX, TY, H>(g, x0, y0, [&](int t, long long at) {
         double q[5];
 #pragma unroll
@@ -189,6 +193,7 @@ __device__ __forceinline__ void tile2d_f32_body(const GridView& g, const StageVi
         for (int v = 0; v < 5; ++v) sq[v * SX * SY + t] = float(q[v] - qref[v]);
     });
     __syncthreads();
+    const Ref32 ref = sref;
     const float gamma = float(g.gamma);
     for (int f = threadIdx.x; f < NFXP + NFYP; f += blockDim.x) {
         float st[NST][5];
@@ -201,10 +206,10 @@ __device__ __forceinline__ void tile2d_f32_body(const GridView& g, const StageVi
             for (int s = 0; s < NST; ++s)
 #pragma unroll
                 for (int v = 0; v < 5; ++v) st[s][v] = base[v * SX * SY + s];
-            face_flux_dev32<0, SCHEME, FLUX>(st, ref, gamma, Ft, flags, cut, sv.counters != nullptr);
-            const float a = float(g.area[0]);
+            face_flux_dev32<0, SCHEME, FLUX>(st, ref, gamma, Ft, flags, cut, sv.counters != nullptr,
+                                             float(g.area[0]));
 #pragma unroll
-            for (int v = 0; v < 5; ++v) fx[v * NFX + f] = Ft[v] * a;
+            for (int v = 0; v < 5; ++v) fx[v * NFX + f] = Ft[v];
         } else {
             const int k = f - NFXP;
             if (k >= NFY) continue;
@@ -214,10 +219,10 @@ __device__ __forceinline__ void tile2d_f32_body(const GridView& g, const StageVi
             for (int s = 0; s < NST; ++s)
 #pragma unroll
                 for (int v = 0; v < 5; ++v) st[s][v] = base[v * SX * SY + s * SX];
-            face_flux_dev32<1, SCHEME, FLUX>(st, ref, gamma, Ft, flags, cut, sv.counters != nullptr);
-            const float a = float(g.area[1]);
+            face_flux_dev32<1, SCHEME, FLUX>(st, ref, gamma, Ft, flags, cut, sv.counters != nullptr,
+                                             float(g.area[1]));
 #pragma unroll
-            for (int v = 0; v < 5; ++v) fy[v * NFY + k] = Ft[v] * a;
+            for (int v = 0; v < 5; ++v) fy[v * NFY + k] = Ft[v];
         }
         if (SCHEME == TENO5) cores += 10;
     }
@@ -256,14 +261,18 @@ __device__ __forceinline__ void tile1d_body(const GridView& g, const StageView& 
     T* fx = sq + 5 * SX;   // [5][NF]
     const long long vs = g.vs;
     double qref[5] = {0, 0, 0, 0, 0};
-    if (F32) load_ref(g, sv.qs, qref);
-    const Ref32 ref = F32 ? make_ref32(qref, g.gamma) : Ref32{};
+    __shared__ Ref32 sref;  // FP32: made once per tile, read after the staging barrier
+    if (F32) {
+        load_ref(g, sv.qs, qref);
+        if (threadIdx.x == 0) sref = make_ref32(qref, g.gamma);
+    }
     for (int t = threadIdx.x; t < SX; t += blockDim.x) {
         const int gx = map_tile_index(x0 - H + t, g.n[0], g.bc_lo[0], g.bc_hi[0]);
 #pragma unroll
         for (int v = 0; v < 5; ++v) sq[v * SX + t] = T(__ldg(sv.qs + v * vs + gx) - qref[v]);
     }
     __syncthreads();
+    const Ref32 ref = F32 ? sref : Ref32{};
     for (int f = threadIdx.x; f < NF; f += blockDim.x) {
         T st[NST][5];
         T Ft[5];
@@ -271,10 +280,16 @@ __device__ __forceinline__ void tile1d_body(const GridView& g, const StageView& 
         for (int s = 0; s < NST; ++s)
 #pragma unroll
             for (int v = 0; v < 5; ++v) st[s][v] = sq[v * SX + f + s];
-        if constexpr (F32) face_flux_dev32<0, SCHEME, FLUX>(st, ref, T(g.gamma), Ft, flags, cut, sv.counters != nullptr);
-        else face_flux<0, SCHEME, FLUX, double>(st, g.gamma, Ft, flags, cut, FLUX == LAXW ? sv.clock->dt / g.h[0] : 0.0);
+        if constexpr (F32) {
+            face_flux_dev32<0, SCHEME, FLUX>(st, ref, T(g.gamma), Ft, flags, cut, sv.counters != nullptr,
+                                             T(g.area[0]));
 #pragma unroll
-        for (int v = 0; v < 5; ++v) fx[v * NF + f] = Ft[v] * T(g.area[0]);
+            for (int v = 0; v < 5; ++v) fx[v * NF + f] = Ft[v];
+        } else {
+            face_flux<0, SCHEME, FLUX, double>(st, g.gamma, Ft, flags, cut, FLUX == LAXW ? sv.clock->dt / g.h[0] : 0.0);
+#pragma unroll
+            for (int v = 0; v < 5; ++v) fx[v * NF + f] = Ft[v] * T(g.area[0]);
+        }
         if (SCHEME == TENO5) cores += 10;
     }
     __syncthreads();
