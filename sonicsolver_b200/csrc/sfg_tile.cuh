@@ -58,14 +58,21 @@ struct Tile1Shape {
 
 // Halo index mapping for tile loads.  A partial tile at the high end of an
 // axis reaches up to TX - 1 + H nodes past the last node, which can exceed
-// one period on small periodic grids, so periodic indices take a full modulo
-// (both ends are periodic or neither); transmissive ends clamp to the inner
-// neighbour of the boundary node, frozen ends to their extra end node.  Every
-// result lies in [0, n).
+// one period on small periodic grids, so periodic indices wrap by one period
+// and fall back to a full modulo only when that is not enough (both ends are
+// periodic or neither; an integer modulo by a run-time n costs tens of
+// instructions); transmissive ends clamp to the inner neighbour of the
+// boundary node, frozen ends to their extra end node.  Every result lies in
+// [0, n).
 __device__ __forceinline__ int map_tile_index(int i, int n, int bcl, int bch) {
     if (bcl == BC_PERIODIC) {
-        i %= n;
-        return i < 0 ? i + n : i;
+        if (i < 0) i += n;
+        else if (i >= n) i -= n;
+        if ((unsigned)i >= (unsigned)n) {
+            i %= n;
+            i = i < 0 ? i + n : i;
+        }
+        return i;
     }
     const int lo = bcl == BC_FROZEN ? 0 : 1;
     const int hi = bch == BC_FROZEN ? n - 1 : n - 2;
