@@ -191,14 +191,34 @@ __device__ __forceinline__ void recon_field(const CharBasisT<T>& e, const T (&st
         for (int k = 0; k < 5; ++k) acc += row[k] * st[s][k];
         ch[s] = acc;
     }
-    T sl[8], sr[8];
+    T wl, wr;
+    if constexpr (std::is_same<T, float>::value && (SCHEME == WENO5 || SCHEME == TENO5)) {
+        // FP32 WENO5 / TENO5: the left- and right-biased stencils as the two
+        // lanes of one paired core (the Cartesian kernels' cores)
+        float2 v[5];
 #pragma unroll
-    for (int s = 0; s < W; ++s) {
-        sl[s] = ch[s];
-        sr[s] = ch[NST - 1 - s];
+        for (int s = 0; s < 5; ++s) v[s] = make_float2(ch[s], ch[NST - 1 - s]);
+        float2 bad = f2(0.f), kept = f2(0.f);
+        float2 w;
+        if constexpr (SCHEME == TENO5) {
+            w = teno5_core2(v, bad, true, kept);
+            cut += 6u - unsigned(kept.x + kept.y);
+        } else {
+            w = weno5_core2(v, bad);
+        }
+        flag_bad(bad, flags);
+        wl = w.x;
+        wr = w.y;
+    } else {
+        T sl[8], sr[8];
+#pragma unroll
+        for (int s = 0; s < W; ++s) {
+            sl[s] = ch[s];
+            sr[s] = ch[NST - 1 - s];
+        }
+        wl = recon_core<SCHEME, T>(sl, flags, cut);
+        wr = recon_core<SCHEME, T>(sr, flags, cut);
     }
-    const T wl = recon_core<SCHEME, T>(sl, flags, cut);
-    const T wr = recon_core<SCHEME, T>(sr, flags, cut);
     T col[5];
     right_col<K, T>(e, col);
 #pragma unroll
