@@ -151,17 +151,22 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == sizeof(float) ? T3_
                 for (int s = 0; s < NST; ++s)
 #pragma unroll
                     for (int v = 0; v < 5; ++v) st[s][v] = base[v * SX * SY + s];
-                if constexpr (F32) face_flux_dev32<0, SCHEME, FLUX>(st, ref, float(g.gamma), Ft, flags, cut, sv.counters != nullptr);
-                else {
+                if constexpr (F32) {
+                    // the area rides in the flux's exact factor 1/2
+                    face_flux_dev32<0, SCHEME, FLUX>(st, ref, float(g.gamma), Ft, flags, cut, sv.counters != nullptr,
+                                                     float(g.area[0]));
+#pragma unroll
+                    for (int v = 0; v < 5; ++v) fx[v * NFX + f] = Ft[v];
+                } else {
                     double sd[NST][5];
 #pragma unroll
                     for (int s = 0; s < NST; ++s)
 #pragma unroll
                         for (int v = 0; v < 5; ++v) sd[s][v] = st[s][v];
                     face_flux<0, SCHEME, FLUX, double>(sd, g.gamma, Ft, flags, cut, lamx);
-                }
 #pragma unroll
-                for (int v = 0; v < 5; ++v) fx[v * NFX + f] = Ft[v] * T(g.area[0]);
+                    for (int v = 0; v < 5; ++v) fx[v * NFX + f] = Ft[v] * T(g.area[0]);
+                }
             } else {
                 const int kf = f - NFX;
                 const int r = kf / T3X, c = kf - r * T3X;
@@ -170,17 +175,22 @@ __global__ void __launch_bounds__(TILE_THREADS, sizeof(T) == sizeof(float) ? T3_
                 for (int s = 0; s < NST; ++s)
 #pragma unroll
                     for (int v = 0; v < 5; ++v) st[s][v] = base[v * SX * SY + s * SX];
-                if constexpr (F32) face_flux_dev32<1, SCHEME, FLUX>(st, ref, float(g.gamma), Ft, flags, cut, sv.counters != nullptr);
-                else {
+                if constexpr (F32) {
+                    // the area rides in the flux's exact factor 1/2
+                    face_flux_dev32<1, SCHEME, FLUX>(st, ref, float(g.gamma), Ft, flags, cut, sv.counters != nullptr,
+                                                     float(g.area[1]));
+#pragma unroll
+                    for (int v = 0; v < 5; ++v) fy[v * NFY + kf] = Ft[v];
+                } else {
                     double sd[NST][5];
 #pragma unroll
                     for (int s = 0; s < NST; ++s)
 #pragma unroll
                         for (int v = 0; v < 5; ++v) sd[s][v] = st[s][v];
                     face_flux<1, SCHEME, FLUX, double>(sd, g.gamma, Ft, flags, cut, lamy);
-                }
 #pragma unroll
-                for (int v = 0; v < 5; ++v) fy[v * NFY + kf] = Ft[v] * T(g.area[1]);
+                    for (int v = 0; v < 5; ++v) fy[v * NFY + kf] = Ft[v] * T(g.area[1]);
+                }
             }
             if (SCHEME == TENO5) cores += 10;
         }
